@@ -1,0 +1,136 @@
+/*
+ * h2dev.h — C ABI of the B200-native H^2 solver (libmxcb200.so).
+ *
+ * Plain pointers and sizes only.  Every entry point returns an int status
+ * (H2DEV_OK on success).  "Host" arrays are caller-owned host memory; the
+ * *_device variants take device pointers on the solver's device.  All
+ * vectors are column-major n x nrhs with leading dimension ld >= n, in the
+ * tree-sorted body order produced by h2_build_tree (the order the reference
+ * uses for every vector, solver.hpp:23).  One solver object per host thread
+ * at a time; calls on one handle are ordered on the handle's stream.
+ */
+#ifndef H2DEV_H
+#define H2DEV_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct h2dev_handle_s* h2dev_handle_t;
+typedef struct h2dev_solver_s* h2dev_solver_t;
+
+enum {
+  H2DEV_OK = 0,
+  H2DEV_ERR_ARG = 1,      /* invalid argument or size */
+  H2DEV_ERR_CUDA = 2,     /* CUDA runtime error (h2dev_last_error_message has it) */
+  H2DEV_ERR_OOM = 3,      /* device allocation failed */
+  H2DEV_ERR_STATE = 4,    /* call out of order (e.g. solve before factorize) */
+  H2DEV_ERR_SINGULAR = 5, /* a redundant block had |det| <= DBL_MIN (info > 0) */
+  H2DEV_ERR_NOCONV = 6    /* GMRES stopped at outer_iters above tol */
+};
+
+enum { H2DEV_KERNEL_LAPLACE = 0, H2DEV_KERNEL_YUKAWA = 1 };
+enum { H2DEV_FP64 = 0, H2DEV_FP32 = 1 };
+
+/* ---- host helpers (no device work) ---------------------------------- */
+
+/* test_funcs.hpp:31-41 uniform_unit_cube_rnd: std::mt19937(seed) bodies. */
+int h2_uniform_unit_cube_rnd(double* bodies, int64_t nbodies, double diameter, int64_t dim, unsigned seed);
+/* main.cpp:358-361: default-seeded std::mt19937_64 uniform[0,1) vector. */
+int h2_uniform_rhs(double* x, int64_t n);
+/* build_tree.cpp:93-125 buildBinaryTree: sorts bodies (n x 3) in place and
+ * fills 2^(levels+1)-1 cells: child[2], body[2] (int64) and R[3], C[3]. */
+int h2_build_tree(double* bodies, int64_t nbodies, int64_t levels, int64_t* cell_child, int64_t* cell_body,
+                  double* cell_R, double* cell_C);
+/* build_tree.cpp:67-84 CSR::CSR: kind 'N' (near) or 'F' (far) pair list over
+ * all cells.  row receives ncells+1 offsets; col up to cap column indices;
+ * *nnz the list length (call with col = NULL to size it). */
+int h2_pair_csr(char kind, int64_t ncells, const int64_t* cell_child, const int64_t* cell_body, const double* cell_R,
+                const double* cell_C, double theta, int64_t* row, int64_t* col, int64_t cap, int64_t* nnz);
+/* main.cpp:54-55: levels = floor(log2(N / min(N, leaf))). */
+int64_t h2_levels_for(int64_t nbodies, int64_t leaf);
+
+/* ---- device handle (gpu_handles.cu:54-62 initGpuEnvs / finalizeGpuEnvs) */
+int h2dev_handle_create(int device, h2dev_handle_t* out);
+int h2dev_handle_destroy(h2dev_handle_t h);
+int h2dev_handle_synchronize(h2dev_handle_t h);
+
+/* ---- solver (solver.hpp:11-47 H2MatrixSolver) ------------------------ */
+
+/* H2MatrixSolver::H2MatrixSolver (solver.cpp:59-88): builds the tree lists,
+ * the shared bases (compute_basis, h2matrix.cpp:70-120), near blocks and
+ * couplings of every level on the device.  epi > 0: operator mode (ID basis
+ * with relative threshold epi); epi == 0: fixed-rank orthogonal preconditioner
+ * mode with rank (levels - l) * leveled_rank + rank at level l and far lists
+ * from weak admissibility.  samples > 0 caps each box's far list (build
+ * extension); samples <= 0 uses every far body as the reference does.
+ * precision: H2DEV_FP64 or H2DEV_FP32 storage/arithmetic for this matrix.
+ * bodies: tree-sorted nbodies x 3 host array (as left by h2_build_tree). */
+int h2dev_solver_create(h2dev_handle_t h, int kernel, double singularity, double alpha, double epi, int64_t rank,
+                        int64_t leveled_rank, int64_t ncells, const int64_t* cell_child, const int64_t* cell_body,
+                        const double* cell_R, const double* cell_C, double theta, const double* bodies,
+                        int64_t nbodies, int64_t levels, int64_t samples, int precision, h2dev_solver_t* out);
+int h2dev_solver_destroy(h2dev_solver_t s);
+/* levels and lenX (= local_bodies.second - local_bodies.first). */
+int h2dev_solver_shape(h2dev_solver_t s, int64_t* levels, int64_t* lenX);
+/* Dims / DimsLr of one level (h2matrix.hpp:27-28), 2^level entries each. */
+int h2dev_solver_level_dims(h2dev_solver_t s, int64_t level, int64_t* dims, int64_t* ranks);
+
+/* matVecMul (solver.cpp:123-135): X <- A_H2 X, in place. */
+int h2dev_matvec(h2dev_solver_t s, int64_t nrhs, double* X, int64_t ldx);
+int h2dev_matvec_device(h2dev_solver_t s, int64_t nrhs, double* dX, int64_t ldx);
+
+/* factorizeM (solver.cpp:137-147): multilevel ULV factorization.
+ * info_per_level (optional, levels+1 ints) receives the singular-block
+ * count of each level; returns H2DEV_ERR_SINGULAR when any is nonzero. */
+int h2dev_factorize(h2dev_solver_t s, int* info_per_level);
+
+/* solvePrecondition (solver.cpp:168-179): X <- M^{-1} X, in place. */
+int h2dev_solve_precondition(h2dev_solver_t s, int64_t nrhs, double* X, int64_t ldx);
+int h2dev_solve_precondition_device(h2dev_solver_t s, int64_t nrhs, double* dX, int64_t ldx);
+
+/* solveGMRES (solver.cpp:191-248), one independent restarted GMRES per
+ * right-hand side: left preconditioner M (factored), true residual with A.
+ * X is the initial guess on entry and the solution on return.  resid
+ * ((outer+1) x nrhs, column-major) receives the relative residual history and
+ * iters (nrhs) the restart cycles taken.  early_exit != 0 ends a cycle's
+ * Arnoldi loop once every active Hessenberg residual estimate is below tol
+ * (the reference always runs inner steps); 0 reproduces the reference. */
+int h2dev_solve_gmres(h2dev_solver_t A, h2dev_solver_t M, double tol, int64_t nrhs, double* X, const double* B,
+                      int64_t ld, int64_t inner, int64_t outer, int early_exit, double* resid, int64_t* iters);
+int h2dev_solve_gmres_device(h2dev_solver_t A, h2dev_solver_t M, double tol, int64_t nrhs, double* dX,
+                             const double* dB, int64_t ld, int64_t inner, int64_t outer, int early_exit,
+                             double* resid, int64_t* iters);
+
+/* ---- dense kernel access (kernel.cpp:71-85 gen_matrix; main.cpp:83-84) */
+
+/* out (m x n column-major) = K(bi, bj), bodies xyz-interleaved host arrays;
+ * distances formed exactly as the reference's std::hypot. */
+int h2dev_gen_block(h2dev_handle_t h, int kernel, double singularity, double alpha, const double* bi, int64_t m,
+                    const double* bj, int64_t n, double* out);
+/* Y = A_dense X without storing A (host arrays, FP64). */
+int h2dev_dense_matvec(h2dev_handle_t h, int kernel, double singularity, double alpha, const double* bodies,
+                       int64_t n, int64_t nrhs, const double* X, double* Y, int64_t ld);
+int h2dev_dense_matvec_device(h2dev_handle_t h, int kernel, double singularity, double alpha,
+                              const double* dbodies, int64_t n, int64_t nrhs, const double* dX, double* dY,
+                              int64_t ld);
+
+/* ---- inspection (parity tests) -------------------------------------- */
+
+enum { H2DEV_EXPORT_S = 0, H2DEV_EXPORT_Q = 1, H2DEV_EXPORT_R = 2, H2DEV_EXPORT_A = 3, H2DEV_EXPORT_C = 4 };
+/* Number of doubles h2dev_solver_export writes for (level, what). */
+int h2dev_solver_export_size(h2dev_solver_t s, int64_t level, int what, int64_t* count);
+/* Copies one level's container (S: skeleton-ordered bodies, Q, R (V after
+ * factorize, stored transposed), A near blocks, C couplings) in box /
+ * block order, each block column-major, converted to double. */
+int h2dev_solver_export(h2dev_solver_t s, int64_t level, int what, double* out);
+
+const char* h2dev_last_error_message(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* H2DEV_H */

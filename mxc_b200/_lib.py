@@ -1,0 +1,95 @@
+"""ctypes binding of libmxcb200.so (the C ABI declared in include/h2dev.h).
+
+Loading fails loudly when the library has not been built: there is no
+Python or CPU fallback for any device entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmxcb200.so")
+
+H2DEV_OK = 0
+H2DEV_ERR_ARG = 1
+H2DEV_ERR_CUDA = 2
+H2DEV_ERR_OOM = 3
+H2DEV_ERR_STATE = 4
+H2DEV_ERR_SINGULAR = 5
+H2DEV_ERR_NOCONV = 6
+
+KERNEL_LAPLACE = 0
+KERNEL_YUKAWA = 1
+FP64 = 0
+FP32 = 1
+
+EXPORT_S, EXPORT_Q, EXPORT_R, EXPORT_A, EXPORT_C = range(5)
+
+_i64 = C.c_int64
+_dp = C.POINTER(C.c_double)
+_i64p = C.POINTER(C.c_int64)
+_vp = C.c_void_p
+
+# name -> (restype, argtypes); every symbol include/h2dev.h declares.
+SIGNATURES = {
+    "h2_uniform_unit_cube_rnd": (C.c_int, [_vp, _i64, C.c_double, _i64, C.c_uint]),
+    "h2_uniform_rhs": (C.c_int, [_vp, _i64]),
+    "h2_build_tree": (C.c_int, [_vp, _i64, _i64, _vp, _vp, _vp, _vp]),
+    "h2_levels_for": (_i64, [_i64, _i64]),
+    "h2_pair_csr": (C.c_int, [C.c_char, _i64, _vp, _vp, _vp, _vp, C.c_double, _vp, _vp, _i64, _i64p]),
+    "h2dev_handle_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
+    "h2dev_handle_destroy": (C.c_int, [_vp]),
+    "h2dev_handle_synchronize": (C.c_int, [_vp]),
+    "h2dev_solver_create": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double, C.c_double, _i64, _i64, _i64,
+                                      _vp, _vp, _vp, _vp, C.c_double, _vp, _i64, _i64, _i64, C.c_int,
+                                      C.POINTER(_vp)]),
+    "h2dev_solver_destroy": (C.c_int, [_vp]),
+    "h2dev_solver_shape": (C.c_int, [_vp, _i64p, _i64p]),
+    "h2dev_solver_level_dims": (C.c_int, [_vp, _i64, _vp, _vp]),
+    "h2dev_matvec": (C.c_int, [_vp, _i64, _vp, _i64]),
+    "h2dev_matvec_device": (C.c_int, [_vp, _i64, _vp, _i64]),
+    "h2dev_factorize": (C.c_int, [_vp, _vp]),
+    "h2dev_solve_precondition": (C.c_int, [_vp, _i64, _vp, _i64]),
+    "h2dev_solve_precondition_device": (C.c_int, [_vp, _i64, _vp, _i64]),
+    "h2dev_solve_gmres": (C.c_int, [_vp, _vp, C.c_double, _i64, _vp, _vp, _i64, _i64, _i64, C.c_int, _vp,
+                                    _vp]),
+    "h2dev_solve_gmres_device": (C.c_int, [_vp, _vp, C.c_double, _i64, _vp, _vp, _i64, _i64, _i64, C.c_int,
+                                           _vp, _vp]),
+    "h2dev_gen_block": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double, _vp, _i64, _vp, _i64, _vp]),
+    "h2dev_dense_matvec": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double, _vp, _i64, _i64, _vp, _vp, _i64]),
+    "h2dev_dense_matvec_device": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double, _vp, _i64, _i64, _vp, _vp,
+                                            _i64]),
+    "h2dev_solver_export_size": (C.c_int, [_vp, _i64, C.c_int, _i64p]),
+    "h2dev_solver_export": (C.c_int, [_vp, _i64, C.c_int, _vp]),
+    "h2dev_last_error_message": (C.c_char_p, []),
+}
+
+_lib = None
+
+
+class H2DevError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        super().__init__("%s failed with status %d: %s" % (where, code, msg))
+        self.code = code
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("libmxcb200.so is not built (run: python -m mxc_b200.build)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(code: int, where: str, allow=()) -> int:
+    if code != H2DEV_OK and code not in allow:
+        msg = lib().h2dev_last_error_message()
+        raise H2DevError(code, where, msg.decode() if msg else "")
+    return code

@@ -1,0 +1,100 @@
+// Shared device helpers for the H^2 solver kernels (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace h2b {
+
+typedef int64_t i64;
+
+enum KernelKind { KERNEL_LAPLACE = 0, KERNEL_YUKAWA = 1 };
+
+// K(d) for d != 0, and the value used where two bodies coincide
+// (kernel.hpp:28-50: Laplace 1/d, Yukawa exp(-alpha d)/d, diagonal 1/s).
+struct KernelParams {
+  int kind;
+  double diag;
+  double alpha;
+};
+
+// Distance exactly as libstdc++'s 3-argument std::hypot forms it
+// (a * sqrt((x/a)^2 + (y/a)^2 + (z/a)^2) with a the largest magnitude),
+// with every operation rounded separately so the result matches the
+// reference's host build bit for bit.
+__device__ __forceinline__ double hypot3_exact(double dx, double dy, double dz) {
+  double x = fabs(dx), y = fabs(dy), z = fabs(dz);
+  double a = x < y ? (y < z ? z : y) : (x < z ? z : x);
+  if (a == 0.) return 0.;
+  double sx = __ddiv_rn(x, a), sy = __ddiv_rn(y, a), sz = __ddiv_rn(z, a);
+  double s = __dadd_rn(__dadd_rn(__dmul_rn(sx, sx), __dmul_rn(sy, sy)), __dmul_rn(sz, sz));
+  return __dmul_rn(a, __dsqrt_rn(s));
+}
+
+__device__ __forceinline__ double kernel_exact(const KernelParams& kp, double dx, double dy, double dz) {
+  double d = hypot3_exact(dx, dy, dz);
+  if (d == 0.) return kp.diag;
+  if (kp.kind == KERNEL_LAPLACE) return __ddiv_rn(1., d);
+  return __ddiv_rn(exp(__dmul_rn(-kp.alpha, d)), d);
+}
+
+// Fast form for far-field samples and the dense verifier: one rsqrt of the
+// squared distance; differs from the exact form by a few ulp.
+__device__ __forceinline__ double kernel_fast(const KernelParams& kp, double dx, double dy, double dz) {
+  double r2 = dx * dx + dy * dy + dz * dz;
+  if (r2 == 0.) return kp.diag;
+  double inv = rsqrt(r2);
+  if (kp.kind == KERNEL_LAPLACE) return inv;
+  return exp(-kp.alpha * (r2 * inv)) * inv;
+}
+
+template <typename T>
+struct BlockReduce {
+  // Sum over a whole CTA (blockDim.x a multiple of 32, <= 1024).
+  static __device__ T sum(T v, T* sbuf) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sbuf[w] = v;
+    __syncthreads();
+    int nw = blockDim.x >> 5;
+    T r = (threadIdx.x < nw) ? sbuf[threadIdx.x] : T(0);
+    if (w == 0)
+      for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    if (threadIdx.x == 0) sbuf[0] = r;
+    __syncthreads();
+    T out = sbuf[0];
+    __syncthreads();
+    return out;
+  }
+};
+
+// CTA-wide argmax of a double with the first index winning ties.
+__device__ __forceinline__ void argmax_first(double& v, int& idx, double* sv, int* si) {
+  for (int o = 16; o > 0; o >>= 1) {
+    double ov = __shfl_xor_sync(0xffffffffu, v, o);
+    int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+    if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
+  }
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) { sv[w] = v; si[w] = idx; }
+  __syncthreads();
+  int nw = blockDim.x >> 5;
+  if (w == 0) {
+    double rv = (l < nw) ? sv[l] : -1.0;
+    int ri = (l < nw) ? si[l] : 0x7fffffff;
+    for (int o = 16; o > 0; o >>= 1) {
+      double ov = __shfl_xor_sync(0xffffffffu, rv, o);
+      int oi = __shfl_xor_sync(0xffffffffu, ri, o);
+      if (ov > rv || (ov == rv && oi < ri)) { rv = ov; ri = oi; }
+    }
+    if (l == 0) { sv[0] = rv; si[0] = ri; }
+  }
+  __syncthreads();
+  v = sv[0];
+  idx = si[0];
+  __syncthreads();
+}
+
+}  // namespace h2b

@@ -1,0 +1,1489 @@
+// C ABI and level drivers of the B200-native H^2 solver.
+//
+// Single process, single device: every box of every level is local, so the
+// reference's ColCommMPI reduces to identity collectives and all halo data
+// is read in place from HBM (comm-mpi.cpp:198-225 become no-ops).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "h2dev.h"
+#include "kernels.h"
+#include "plan.hpp"
+
+namespace h2b {
+
+struct H2Error {
+  int code;
+  std::string msg;
+};
+
+static thread_local std::string g_last_error;
+
+static void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    int code = (e == cudaErrorMemoryAllocation) ? H2DEV_ERR_OOM : H2DEV_ERR_CUDA;
+    cudaGetLastError();
+    throw H2Error{code, std::string(what) + ": " + cudaGetErrorString(e)};
+  }
+}
+
+static void require(bool ok, const char* what) {
+  if (!ok) throw H2Error{H2DEV_ERR_ARG, what};
+}
+
+template <typename T>
+struct DVec {
+  T* p = nullptr;
+  size_t n = 0;
+  DVec() = default;
+  DVec(const DVec&) = delete;
+  DVec& operator=(const DVec&) = delete;
+  DVec(DVec&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DVec& operator=(DVec&& o) noexcept {
+    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    return *this;
+  }
+  ~DVec() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    if (count == n && p) return;
+    release();
+    if (count) ck(cudaMalloc((void**)&p, count * sizeof(T)), "cudaMalloc");
+    n = count;
+  }
+  void zero(cudaStream_t st) {
+    if (n) ck(cudaMemsetAsync(p, 0, n * sizeof(T), st), "cudaMemsetAsync");
+  }
+  void upload(const std::vector<T>& v) {
+    alloc(v.size());
+    if (!v.empty()) ck(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+  }
+  std::vector<T> download(cudaStream_t st) const {
+    std::vector<T> v(n);
+    if (n) {
+      ck(cudaStreamSynchronize(st), "sync");
+      ck(cudaMemcpy(v.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost), "download");
+    }
+    return v;
+  }
+};
+
+// Host-built list of segmented-GEMM tasks, uploaded once and replayed.
+template <typename T>
+struct GemmPlan {
+  std::vector<GemmTask<T>> tasks;
+  std::vector<GemmEntry<T>> ents;
+  DVec<GemmTask<T>> d_tasks;
+  DVec<GemmEntry<T>> d_ents;
+  DVec<TileRef> d_tiles;
+  int ntiles = 0;
+  int shape = GEMM_BIG;
+  void add_task(T* C, i64 ldc, int m, int n, T beta) {
+    GemmTask<T> t;
+    t.C = C; t.ldc = ldc; t.m = m; t.n = n; t.beta = beta;
+    t.e0 = t.e1 = (int)ents.size();
+    tasks.push_back(t);
+  }
+  void add_entry(const T* A, i64 lda, int opA, const T* B, i64 ldb, int opB, int k, T alpha) {
+    if (k <= 0) return;
+    GemmEntry<T> e;
+    e.A = A; e.B = B; e.lda = lda; e.ldb = ldb; e.k = k; e.opA = opA; e.opB = opB; e.alpha = alpha;
+    ents.push_back(e);
+    tasks.back().e1 = (int)ents.size();
+  }
+  void finalize() {
+    int maxn = 0;
+    for (auto& t : tasks) maxn = std::max(maxn, t.n);
+    shape = maxn <= 16 ? GEMM_SKINNY : GEMM_BIG;
+    int bm = gemm_tile_m(shape), bn = gemm_tile_n(shape);
+    std::vector<TileRef> tiles;
+    for (int ti = 0; ti < (int)tasks.size(); ti++) {
+      const auto& t = tasks[ti];
+      if (t.m <= 0 || t.n <= 0) continue;
+      if (t.e0 == t.e1 && t.beta == T(1)) continue;  // nothing to do
+      for (int a = 0; a < (t.m + bm - 1) / bm; a++)
+        for (int b = 0; b < (t.n + bn - 1) / bn; b++) tiles.push_back(TileRef{ti, a, b});
+    }
+    ntiles = (int)tiles.size();
+    d_tasks.upload(tasks);
+    d_ents.upload(ents);
+    d_tiles.upload(tiles);
+    tasks.clear();
+    tasks.shrink_to_fit();
+    ents.clear();
+    ents.shrink_to_fit();
+  }
+  void run(cudaStream_t st) const { ck(launch_seg_gemm<T>(shape, d_tasks.p, d_ents.p, d_tiles.p, ntiles, st), "seg_gemm"); }
+};
+
+template <typename T>
+struct CopyPlan {
+  std::vector<CopyEntry<T>> ents;
+  DVec<CopyEntry<T>> d;
+  int n = 0;
+  void add(const T* src, i64 lds, T* dst, i64 ldd, int m, int nn, int trans = 0) {
+    if (m <= 0 || nn <= 0) return;
+    CopyEntry<T> e;
+    e.src = src; e.dst = dst; e.lds = lds; e.ldd = ldd; e.m = m; e.n = nn; e.trans = trans;
+    ents.push_back(e);
+  }
+  void finalize() {
+    n = (int)ents.size();
+    d.upload(ents);
+    ents.clear();
+    ents.shrink_to_fit();
+  }
+  void run(cudaStream_t st) const { ck(launch_batched_copy<T>(d.p, n, st), "batched_copy"); }
+};
+
+}  // namespace h2b
+
+struct h2dev_handle_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+};
+
+namespace h2b {
+
+template <typename T>
+struct Level {
+  int l = 0;
+  i64 nodes = 0, gbegin = 0;
+  std::vector<i64> arow, acol, crow, ccol, diag;
+  std::vector<i64> dims, ranks, xoff, zoff, qoff, aoff, coff;
+  i64 lenX = 0, lenZ = 0, maxM = 0;
+  DVec<i64> d_dims, d_ranks, d_xoff, d_qoff;
+  DVec<double> pts;  // lenX x 3, skeleton-first after the basis
+  DVec<T> Q, R, A, C;
+  std::vector<i64> na_off, na_ld;  // destination of each near block's ss part in the parent A
+  // factorization results
+  DVec<T> B, invT;
+  std::vector<i64> boff, ioff;
+  DVec<int> ipiv, info;
+  int info_count = 0;
+  // per-nrhs vectors
+  DVec<T> vX, vZ, vW;
+};
+
+class SolverBase {
+ public:
+  virtual ~SolverBase() {}
+  virtual i64 lenX() const = 0;
+  virtual i64 nlevels() const = 0;
+  virtual void matvec(i64 nrhs, double* dX, i64 ldx) = 0;
+  virtual void factorize(int* info) = 0;
+  virtual void precondition(i64 nrhs, double* dX, i64 ldx) = 0;
+  virtual void level_dims(i64 l, i64* dims, i64* ranks) const = 0;
+  virtual i64 export_size(i64 l, int what) const = 0;
+  virtual void export_to(i64 l, int what, double* out) = 0;
+  h2dev_handle_s* h = nullptr;
+};
+
+struct BuildArgs {
+  KernelParams kp;
+  double epi;
+  i64 rank, leveled_rank, levels, nbodies, samples;
+  double theta;
+  std::vector<Cell> cells;
+  const double* bodies;
+};
+
+template <typename T>
+class Solver : public SolverBase {
+ public:
+  KernelParams kp;
+  double epi = 0.;
+  bool fix_rank = false;
+  i64 rank = 0, leveled_rank = 0, levels = 0, N = 0, samples = 0;
+  std::vector<Cell> cells;
+  DVec<double> bodies;
+  std::vector<Level<T>> L;
+  bool factored = false;
+  // per-nrhs state
+  i64 cur_nrhs = -1;
+  DVec<T> vin, vout;
+  GemmPlan<T> mv_leaf;
+  std::vector<GemmPlan<T>> mv_up, mv_h, mv_down;
+  std::vector<GemmPlan<T>> pc_fx, pc_fz, pc_bx, pc_by;
+  std::vector<CopyPlan<T>> pc_fcopy, pc_bcopy;
+  bool mv_built = false, pc_built = false;
+
+  cudaStream_t st() const { return h->stream; }
+  i64 lenX() const override { return N; }
+  i64 nlevels() const override { return levels; }
+
+  void build(const BuildArgs& a) {
+    kp = a.kp;
+    epi = a.epi;
+    fix_rank = (a.epi == 0.);
+    rank = a.rank;
+    leveled_rank = a.leveled_rank;
+    levels = a.levels;
+    N = a.nbodies;
+    samples = a.samples;
+    cells = a.cells;
+    {
+      std::vector<double> hb(a.bodies, a.bodies + 3 * N);
+      bodies.upload(hb);
+    }
+    PairCSR nearL = build_pair_csr('N', cells, a.theta);
+    PairCSR farL = build_pair_csr('F', cells, a.theta);
+    PairCSR sampL = fix_rank ? build_pair_csr('F', cells, 0.) : farL;
+
+    // Far-body ranges per cell: the parent's list then the cell's own far
+    // boxes (h-matrix.cpp:83-98, 122-127); the root has none.
+    i64 ncells = (i64)cells.size();
+    std::vector<std::vector<std::pair<i64, i64>>> ranges(ncells);
+    for (i64 c = 1; c < ncells; c++) {
+      i64 parent = (c - 1) / 2;
+      ranges[c] = ranges[parent];
+      for (i64 k = sampL.row[c]; k < sampL.row[c + 1]; k++) {
+        i64 x = sampL.col[k];
+        ranges[c].emplace_back(cells[x].body[0], cells[x].body[1]);
+      }
+    }
+    if (ncells) ranges[0].clear();
+
+    L.resize(levels + 1);
+    for (i64 l = 0; l <= levels; l++) {
+      Level<T>& lv = L[l];
+      lv.l = (int)l;
+      lv.gbegin = ((i64)1 << l) - 1;
+      lv.nodes = (i64)1 << l;
+      i64 g0 = lv.gbegin, g1 = g0 + lv.nodes;
+      lv.arow.assign(lv.nodes + 1, 0);
+      lv.crow.assign(lv.nodes + 1, 0);
+      for (i64 i = 0; i < lv.nodes; i++) {
+        for (i64 k = nearL.row[g0 + i]; k < nearL.row[g0 + i + 1]; k++) lv.acol.push_back(nearL.col[k] - g0);
+        for (i64 k = farL.row[g0 + i]; k < farL.row[g0 + i + 1]; k++) lv.ccol.push_back(farL.col[k] - g0);
+        lv.arow[i + 1] = (i64)lv.acol.size();
+        lv.crow[i + 1] = (i64)lv.ccol.size();
+      }
+      (void)g1;
+      lv.diag.assign(lv.nodes, -1);
+      for (i64 i = 0; i < lv.nodes; i++)
+        for (i64 k = lv.arow[i]; k < lv.arow[i + 1]; k++)
+          if (lv.acol[k] == i) lv.diag[i] = k;
+      lv.na_off.assign(lv.acol.size(), -1);
+      lv.na_ld.assign(lv.acol.size(), 0);
+    }
+    for (i64 l = levels; l >= 0; l--) construct_level(l, ranges);
+  }
+
+  double level_epi(i64 l) const {
+    return fix_rank ? (double)((levels - l) * leveled_rank + rank) : epi;
+  }
+
+  // h2matrix.cpp:129-306 for one level.
+  void construct_level(i64 l, const std::vector<std::vector<std::pair<i64, i64>>>& ranges) {
+    Level<T>& lv = L[l];
+    Level<T>* low = (l < levels) ? &L[l + 1] : nullptr;
+    const i64 nodes = lv.nodes;
+    const i64 g0 = lv.gbegin;
+    lv.dims.assign(nodes, 0);
+    for (i64 i = 0; i < nodes; i++)
+      lv.dims[i] = low ? low->ranks[2 * i] + low->ranks[2 * i + 1] : cells[g0 + i].body[1] - cells[g0 + i].body[0];
+    lv.xoff.assign(nodes + 1, 0);
+    lv.qoff.assign(nodes + 1, 0);
+    for (i64 i = 0; i < nodes; i++) {
+      lv.xoff[i + 1] = lv.xoff[i] + lv.dims[i];
+      lv.qoff[i + 1] = lv.qoff[i] + lv.dims[i] * lv.dims[i];
+      lv.maxM = std::max(lv.maxM, lv.dims[i]);
+    }
+    require(lv.maxM <= 1024, "box dimension above 1024 is not supported");
+    lv.lenX = lv.xoff[nodes];
+    i64 nA = (i64)lv.acol.size();
+    lv.aoff.assign(nA + 1, 0);
+    for (i64 i = 0; i < nodes; i++)
+      for (i64 k = lv.arow[i]; k < lv.arow[i + 1]; k++) lv.aoff[k + 1] = lv.aoff[k] + lv.dims[i] * lv.dims[lv.acol[k]];
+    lv.d_dims.upload(lv.dims);
+    lv.d_xoff.upload(lv.xoff);
+    lv.d_qoff.upload(lv.qoff);
+    lv.pts.alloc(3 * lv.lenX);
+    lv.Q.alloc(lv.qoff[nodes]);
+    lv.R.alloc(lv.qoff[nodes]);
+    lv.A.alloc(lv.aoff[nA]);
+    lv.Q.zero(st());
+    lv.R.zero(st());
+    lv.A.zero(st());
+    lv.ranks.assign(nodes, 0);
+
+    if (lv.lenX > 0) {
+      if (!low) {
+        ck(cudaMemcpyAsync(lv.pts.p, bodies.p, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, st()), "pts");
+        ck(launch_set_identity<T>(lv.Q.p, lv.d_qoff.p, lv.d_dims.p, (int)nodes, st()), "identity");
+        std::vector<GenTask> gt;
+        for (i64 i = 0; i < nodes; i++)
+          for (i64 k = lv.arow[i]; k < lv.arow[i + 1]; k++) {
+            i64 j = lv.acol[k];
+            GenTask t;
+            t.bi = bodies.p + 3 * cells[g0 + i].body[0];
+            t.bj = bodies.p + 3 * cells[g0 + j].body[0];
+            t.m = (int)lv.dims[i];
+            t.n = (int)lv.dims[j];
+            t.out_off = lv.aoff[k];
+            t.ld = lv.dims[i];
+            gt.push_back(t);
+          }
+        DVec<GenTask> dg;
+        dg.upload(gt);
+        ck(launch_gen_blocks<T>(kp, dg.p, (int)gt.size(), 1, lv.A.p, st()), "gen near");
+        ck(cudaStreamSynchronize(st()), "sync");
+      } else {
+        CopyPlan<double> pcopy;
+        CopyPlan<T> qcopy, acopy;
+        for (i64 i = 0; i < nodes; i++) {
+          const i64 M = lv.dims[i];
+          i64 offy = 0;
+          for (i64 y = 2 * i; y <= 2 * i + 1; y++) {
+            const i64 ny = low->ranks[y];
+            pcopy.add(low->pts.p + 3 * low->xoff[y], 3 * ny, lv.pts.p + 3 * (lv.xoff[i] + offy), 3 * ny, (int)(3 * ny), 1);
+            qcopy.add(low->R.p + low->qoff[y], low->dims[y], lv.Q.p + lv.qoff[i] + offy + offy * M, M, (int)ny, (int)ny);
+            if (M > 0)
+              for (i64 k = lv.arow[i]; k < lv.arow[i + 1]; k++) {
+                i64 j = lv.acol[k];
+                i64 offx = 0;
+                for (i64 x = 2 * j; x <= 2 * j + 1; x++) {
+                  const i64 nx = low->ranks[x];
+                  i64 lowN = -1, lowC = -1;
+                  for (i64 q = low->arow[y]; q < low->arow[y + 1]; q++)
+                    if (low->acol[q] == x) lowN = q;
+                  if (lowN < 0)
+                    for (i64 q = low->crow[y]; q < low->crow[y + 1]; q++)
+                      if (low->ccol[q] == x) lowC = q;
+                  if (lowN >= 0) {
+                    low->na_off[lowN] = lv.aoff[k] + offy + offx * M;
+                    low->na_ld[lowN] = M;
+                  } else if (lowC >= 0) {
+                    acopy.add(low->C.p + low->coff[lowC], ny, lv.A.p + lv.aoff[k] + offy + offx * M, M, (int)ny, (int)nx);
+                  }
+                  offx += nx;
+                }
+              }
+            offy += ny;
+          }
+        }
+        pcopy.finalize();
+        qcopy.finalize();
+        acopy.finalize();
+        pcopy.run(st());
+        qcopy.run(st());
+        acopy.run(st());
+        ck(cudaStreamSynchronize(st()), "sync");
+      }
+
+      // Shared basis of every box (compute_basis, h2matrix.cpp:252-257).
+      std::vector<int> sidx, tmp;
+      std::vector<i64> soff(nodes + 1, 0), krows(nodes, 0);
+      for (i64 i = 0; i < nodes; i++) {
+        sample_far_list(ranges[g0 + i], samples, tmp);
+        sidx.insert(sidx.end(), tmp.begin(), tmp.end());
+        soff[i + 1] = (i64)sidx.size();
+        krows[i] = std::min<i64>(lv.dims[i], (i64)tmp.size());
+      }
+      DVec<int> d_sidx, d_perm, d_nonzero;
+      DVec<i64> d_soff, d_krows;
+      DVec<double> d_maxpiv;
+      d_sidx.upload(sidx);
+      d_soff.upload(soff);
+      d_krows.upload(krows);
+      d_perm.alloc(lv.lenX);
+      d_nonzero.alloc(nodes);
+      d_maxpiv.alloc(nodes);
+      lv.d_ranks.alloc(nodes);
+      DVec<T> Rws;
+      Rws.alloc(lv.qoff[nodes]);
+      Rws.zero(st());
+      const double e = level_epi(l);
+      const bool orth = 1. <= e;
+      ck(launch_sample_tsqr<T>(kp, bodies.p, lv.pts.p, lv.d_xoff.p, lv.d_dims.p, d_sidx.p, d_soff.p, Rws.p,
+                               lv.d_qoff.p, (int)nodes, (int)lv.maxM, st()),
+         "sample_tsqr");
+      i64 cap = -1;
+      if (e >= 1.) cap = (i64)std::floor(e);
+      ck(launch_cpqr<T>(lv.d_dims.p, d_krows.p, Rws.p, lv.d_qoff.p, d_perm.p, lv.d_xoff.p, d_maxpiv.p, d_nonzero.p,
+                        cap, (int)nodes, (int)lv.maxM, st()),
+         "cpqr");
+      ck(launch_basis_finish<T>(lv.d_dims.p, d_krows.p, Rws.p, lv.Q.p, lv.R.p, lv.d_qoff.p, d_perm.p, lv.d_xoff.p,
+                                d_maxpiv.p, d_nonzero.p, lv.pts.p, lv.d_ranks.p, e, orth ? 1 : 0, low ? 0 : 1,
+                                (int)nodes, (int)lv.maxM, st()),
+         "basis_finish");
+      lv.ranks = lv.d_ranks.download(st());
+    } else {
+      lv.d_ranks.alloc(nodes);
+      lv.d_ranks.zero(st());
+    }
+
+    lv.zoff.assign(nodes + 1, 0);
+    for (i64 i = 0; i < nodes; i++) lv.zoff[i + 1] = lv.zoff[i] + lv.ranks[i];
+    lv.lenZ = lv.zoff[nodes];
+    i64 nC = (i64)lv.ccol.size();
+    lv.coff.assign(nC + 1, 0);
+    for (i64 i = 0; i < nodes; i++)
+      for (i64 k = lv.crow[i]; k < lv.crow[i + 1]; k++) lv.coff[k + 1] = lv.coff[k] + lv.ranks[i] * lv.ranks[lv.ccol[k]];
+    lv.C.alloc(lv.coff[nC]);
+    if (lv.lenZ > 0 && nC > 0) {
+      // Couplings (h2matrix.cpp:279-299): K(S_y, S_x) on the skeletons,
+      // scaled by R_y on the left and R_x^T on the right in orthogonal mode.
+      const bool orth = 1. <= level_epi(l);
+      DVec<T> K;
+      T* kout = lv.C.p;
+      if (orth) {
+        K.alloc(lv.coff[nC]);
+        kout = K.p;
+      }
+      std::vector<GenTask> gt;
+      for (i64 i = 0; i < nodes; i++)
+        for (i64 k = lv.crow[i]; k < lv.crow[i + 1]; k++) {
+          i64 x = lv.ccol[k];
+          GenTask t;
+          t.bi = lv.pts.p + 3 * lv.xoff[i];
+          t.bj = lv.pts.p + 3 * lv.xoff[x];
+          t.m = (int)lv.ranks[i];
+          t.n = (int)lv.ranks[x];
+          t.out_off = lv.coff[k];
+          t.ld = lv.ranks[i];
+          gt.push_back(t);
+        }
+      DVec<GenTask> dg;
+      dg.upload(gt);
+      ck(launch_gen_blocks<T>(kp, dg.p, (int)gt.size(), 1, kout, st()), "gen couplings");
+      if (orth) {
+        DVec<T> T1;
+        T1.alloc(lv.coff[nC]);
+        GemmPlan<T> g1, g2;
+        for (i64 i = 0; i < nodes; i++)
+          for (i64 k = lv.crow[i]; k < lv.crow[i + 1]; k++) {
+            i64 x = lv.ccol[k];
+            int ry = (int)lv.ranks[i], rx = (int)lv.ranks[x];
+            g1.add_task(T1.p + lv.coff[k], ry, ry, rx, T(0));
+            g1.add_entry(lv.R.p + lv.qoff[i], lv.dims[i], 0, K.p + lv.coff[k], ry, 0, ry, T(1));
+            g2.add_task(lv.C.p + lv.coff[k], ry, ry, rx, T(0));
+            g2.add_entry(T1.p + lv.coff[k], ry, 0, lv.R.p + lv.qoff[x], lv.dims[x], 1, rx, T(1));
+          }
+        g1.finalize();
+        g2.finalize();
+        g1.run(st());
+        g2.run(st());
+        ck(cudaStreamSynchronize(st()), "sync");
+      } else {
+        ck(cudaStreamSynchronize(st()), "sync");
+      }
+    }
+  }
+
+  // ------------------------------------------------------------ vectors
+  void ensure_vectors(i64 nrhs) {
+    if (nrhs == cur_nrhs) return;
+    for (auto& lv : L) {
+      lv.vX.alloc(std::max<i64>(1, lv.lenX * nrhs));
+      lv.vZ.alloc(std::max<i64>(1, lv.lenZ * nrhs));
+      lv.vW.alloc(std::max<i64>(1, lv.lenZ * nrhs));
+    }
+    vin.alloc(std::max<i64>(1, N * nrhs));
+    vout.alloc(std::max<i64>(1, N * nrhs));
+    cur_nrhs = nrhs;
+    mv_built = false;
+    pc_built = false;
+  }
+
+  // H^2 matvec plans (h2matrix.cpp:308-401) for the current nrhs.
+  void build_matvec(i64 nrhs) {
+    const int nr = (int)nrhs;
+    mv_up.clear();
+    mv_h.clear();
+    mv_down.clear();
+    mv_up.resize(levels + 1);
+    mv_h.resize(levels + 1);
+    mv_down.resize(levels + 1);
+    for (i64 l = levels; l >= 0; l--) {
+      Level<T>& lv = L[l];
+      const T* X = (l == levels) ? vin.p : L[l + 1].vZ.p;
+      const i64 ldx = lv.lenX;
+      GemmPlan<T>& g = mv_up[l];
+      for (i64 i = 0; i < lv.nodes; i++) {
+        int M = (int)lv.dims[i], r = (int)lv.ranks[i];
+        if (r == 0) continue;
+        g.add_task(lv.vZ.p + lv.zoff[i], lv.lenZ, r, nr, T(0));
+        g.add_entry(lv.Q.p + lv.qoff[i], M, 1, X + lv.xoff[i], ldx, 0, M, T(1));
+      }
+      g.finalize();
+    }
+    for (i64 l = 0; l <= levels; l++) {
+      Level<T>& lv = L[l];
+      GemmPlan<T>& g = mv_h[l];
+      const T beta = (l == 0) ? T(0) : T(1);
+      for (i64 i = 0; i < lv.nodes; i++) {
+        int r = (int)lv.ranks[i];
+        if (r == 0) continue;
+        g.add_task(lv.vW.p + lv.zoff[i], lv.lenZ, r, nr, beta);
+        for (i64 k = lv.crow[i]; k < lv.crow[i + 1]; k++) {
+          i64 j = lv.ccol[k];
+          g.add_entry(lv.C.p + lv.coff[k], r, 0, lv.vZ.p + lv.zoff[j], lv.lenZ, 0, (int)lv.ranks[j], T(1));
+        }
+      }
+      g.finalize();
+      if (l < levels) {
+        GemmPlan<T>& d = mv_down[l];
+        Level<T>& nx = L[l + 1];  // Y_l lives in W_{l+1}
+        for (i64 i = 0; i < lv.nodes; i++) {
+          int M = (int)lv.dims[i], r = (int)lv.ranks[i];
+          d.add_task(nx.vW.p + lv.xoff[i], nx.lenZ, M, nr, T(0));
+          d.add_entry(lv.Q.p + lv.qoff[i], M, 0, lv.vW.p + lv.zoff[i], lv.lenZ, 0, r, T(1));
+        }
+        d.finalize();
+      }
+    }
+    {
+      Level<T>& lv = L[levels];
+      GemmPlan<T>& g = mv_leaf;
+      g = GemmPlan<T>();
+      for (i64 i = 0; i < lv.nodes; i++) {
+        int M = (int)lv.dims[i], r = (int)lv.ranks[i];
+        g.add_task(vout.p + lv.xoff[i], lv.lenX, M, nr, T(0));
+        g.add_entry(lv.Q.p + lv.qoff[i], M, 0, lv.vW.p + lv.zoff[i], lv.lenZ, 0, r, T(1));
+        for (i64 k = lv.arow[i]; k < lv.arow[i + 1]; k++) {
+          i64 j = lv.acol[k];
+          g.add_entry(lv.A.p + lv.aoff[k], M, 0, vin.p + lv.xoff[j], lv.lenX, 0, (int)lv.dims[j], T(1));
+        }
+      }
+      g.finalize();
+    }
+    mv_built = true;
+  }
+
+  void stage_in(i64 nrhs, const double* dX, i64 ldx) {
+    if (ldx == N) {
+      ck(launch_convert<double, T>(dX, vin.p, N * nrhs, st()), "convert in");
+    } else {
+      for (i64 c = 0; c < nrhs; c++) ck(launch_convert<double, T>(dX + c * ldx, vin.p + c * N, N, st()), "convert in");
+    }
+  }
+  void stage_out(i64 nrhs, double* dX, i64 ldx) {
+    if (ldx == N) {
+      ck(launch_convert<T, double>(vout.p, dX, N * nrhs, st()), "convert out");
+    } else {
+      for (i64 c = 0; c < nrhs; c++) ck(launch_convert<T, double>(vout.p + c * N, dX + c * ldx, N, st()), "convert out");
+    }
+  }
+
+  void matvec(i64 nrhs, double* dX, i64 ldx) override {
+    require(nrhs > 0 && ldx >= N, "matvec: bad nrhs/ld");
+    ensure_vectors(nrhs);
+    if (!mv_built) build_matvec(nrhs);
+    stage_in(nrhs, dX, ldx);
+    for (i64 l = levels; l >= 0; l--) mv_up[l].run(st());
+    for (i64 l = 0; l < levels; l++) {
+      mv_h[l].run(st());
+      mv_down[l].run(st());
+    }
+    mv_h[levels].run(st());
+    mv_leaf.run(st());
+    stage_out(nrhs, dX, ldx);
+  }
+
+  // ------------------------------------------------------------ factor
+  // h2matrix.cpp:403-482 for one level, then factorizeCopyNext (484-503).
+  void factor_level(i64 l) {
+    Level<T>& lv = L[l];
+    const i64 nodes = lv.nodes;
+    if (lv.lenX == 0) {
+      lv.info_count = 0;
+      return;
+    }
+    std::vector<i64>& D = lv.dims;
+    std::vector<i64>& Rk = lv.ranks;
+    DVec<T> T1;
+    T1.alloc(lv.qoff[nodes]);
+    lv.boff.assign(nodes + 1, 0);
+    lv.ioff.assign(nodes + 1, 0);
+    std::vector<i64> poff(nodes + 1, 0);
+    for (i64 i = 0; i < nodes; i++) {
+      i64 Mr = D[i] - Rk[i];
+      lv.boff[i + 1] = lv.boff[i] + Mr * D[i];
+      lv.ioff[i + 1] = lv.ioff[i] + Mr * Mr;
+      poff[i + 1] = poff[i] + Mr;
+    }
+    lv.B.alloc(std::max<i64>(1, lv.boff[nodes]));
+    lv.invT.alloc(std::max<i64>(1, lv.ioff[nodes]));
+    lv.ipiv.alloc(std::max<i64>(1, poff[nodes]));
+    lv.info.alloc(nodes);
+    lv.info.zero(st());
+    T* A = lv.A.p;
+    T* Q = lv.Q.p;
+    T* V = lv.R.p;  // V stored transposed: V^T column-major
+    // Steps 1-2: A_ii <- U^T A_ii U.
+    GemmPlan<T> s1, s2, s5, s6, s7, s8;
+    CopyPlan<T> c3, c8;
+    for (i64 i = 0; i < nodes; i++) {
+      const int M = (int)D[i];
+      if (M == 0) continue;
+      T* Aii = A + lv.aoff[lv.diag[i]];
+      s1.add_task(T1.p + lv.qoff[i], M, M, M, T(0));
+      s1.add_entry(Aii, M, 0, Q + lv.qoff[i], M, 0, M, T(1));
+      s2.add_task(Aii, M, M, M, T(0));
+      s2.add_entry(Q + lv.qoff[i], M, 1, T1.p + lv.qoff[i], M, 0, M, T(1));
+    }
+    s1.finalize();
+    s2.finalize();
+    s1.run(st());
+    s2.run(st());
+    // Step 3: V^T[:, :Ms] = U_s.  Step 4: LU and inverse of A_rr.
+    std::vector<LuTask<T>> lt;
+    for (i64 i = 0; i < nodes; i++) {
+      const int M = (int)D[i], Ms = (int)Rk[i], Mr = M - Ms;
+      if (M == 0) continue;
+      c3.add(Q + lv.qoff[i], M, V + lv.qoff[i], M, M, Ms);
+      LuTask<T> t;
+      t.A = A + lv.aoff[lv.diag[i]] + Ms + (i64)Ms * M;
+      t.lda = M;
+      t.n = Mr;
+      t.invT = lv.invT.p + lv.ioff[i];
+      t.ldinv = Mr > 0 ? Mr : 1;
+      t.ipiv = lv.ipiv.p + poff[i];
+      t.info = lv.info.p + i;
+      lt.push_back(t);
+    }
+    c3.finalize();
+    c3.run(st());
+    {
+      DVec<LuTask<T>> dl;
+      dl.upload(lt);
+      ck(launch_lu_inverse<T>(dl.p, (int)lt.size(), st()), "lu_inverse");
+      ck(cudaStreamSynchronize(st()), "sync");
+    }
+    // Step 5: V^T[:, Ms:] = U_r (A_rr^{-1})^T.
+    for (i64 i = 0; i < nodes; i++) {
+      const int M = (int)D[i], Ms = (int)Rk[i], Mr = M - Ms;
+      if (M == 0 || Mr == 0) continue;
+      s5.add_task(V + lv.qoff[i] + (i64)Ms * M, M, M, Mr, T(0));
+      s5.add_entry(Q + lv.qoff[i] + (i64)Ms * M, M, 0, lv.invT.p + lv.ioff[i], Mr, 0, Mr, T(1));
+    }
+    s5.finalize();
+    s5.run(st());
+    // Steps 6-8.
+    for (i64 i = 0; i < nodes; i++) {
+      const int M = (int)D[i], Ms = (int)Rk[i], Mr = M - Ms;
+      if (M == 0 || Mr == 0) continue;
+      T* Aii = A + lv.aoff[lv.diag[i]];
+      if (Ms > 0) {
+        s6.add_task(Aii + Ms, M, Mr, Ms, T(0));
+        s6.add_entry(V + lv.qoff[i] + (i64)Ms * M, M, 1, T1.p + lv.qoff[i], M, 0, M, T(1));
+        s7.add_task(Aii, M, Ms, Ms, T(1));
+        s7.add_entry(Aii + (i64)Ms * M, M, 0, Aii + Ms, M, 0, Mr, T(-1));
+      }
+      c8.add(Aii + Ms, M, lv.B.p + lv.boff[i], Mr, Mr, Ms);
+      s8.add_task(lv.B.p + lv.boff[i] + (i64)Ms * Mr, Mr, Mr, Mr, T(0));
+      s8.add_entry(V + lv.qoff[i] + (i64)Ms * M, M, 1, Q + lv.qoff[i] + (i64)Ms * M, M, 0, M, T(1));
+    }
+    s6.finalize();
+    s7.finalize();
+    s8.finalize();
+    c8.finalize();
+    s6.run(st());
+    s7.run(st());
+    c8.run(st());
+    s8.run(st());
+    // Step 9: off-diagonal transforms A_ij <- V_i A_ij U_j, in chunks of
+    // bounded scratch.
+    {
+      std::vector<i64> offd;
+      for (i64 i = 0; i < nodes; i++)
+        for (i64 k = lv.arow[i]; k < lv.arow[i + 1]; k++)
+          if (k != lv.diag[i]) offd.push_back(k);
+      std::vector<i64> rowof(lv.acol.size());
+      for (i64 i = 0; i < nodes; i++)
+        for (i64 k = lv.arow[i]; k < lv.arow[i + 1]; k++) rowof[k] = i;
+      const i64 cap = (i64)1 << 27;  // elements of scratch per chunk
+      size_t p = 0;
+      DVec<T> T2;
+      while (p < offd.size()) {
+        i64 used = 0;
+        size_t q = p;
+        while (q < offd.size()) {
+          i64 k = offd[q];
+          i64 sz = D[rowof[k]] * D[lv.acol[k]];
+          if (used > 0 && used + sz > cap) break;
+          used += sz;
+          q++;
+        }
+        T2.alloc(std::max<i64>(used, 1));
+        GemmPlan<T> a, b;
+        i64 o = 0;
+        for (size_t z = p; z < q; z++) {
+          i64 k = offd[z];
+          i64 i = rowof[k], j = lv.acol[k];
+          int Mi = (int)D[i], Nj = (int)D[j];
+          if (Mi == 0 || Nj == 0) continue;
+          T* Aij = A + lv.aoff[k];
+          a.add_task(T2.p + o, Mi, Mi, Nj, T(0));
+          a.add_entry(Aij, Mi, 0, Q + lv.qoff[j], Nj, 0, Nj, T(1));
+          b.add_task(Aij, Mi, Mi, Nj, T(0));
+          b.add_entry(V + lv.qoff[i], Mi, 1, T2.p + o, Mi, 0, Mi, T(1));
+          o += (i64)Mi * Nj;
+        }
+        a.finalize();
+        b.finalize();
+        a.run(st());
+        b.run(st());
+        ck(cudaStreamSynchronize(st()), "sync");
+        p = q;
+      }
+      // Steps 10-11: neighbour Schur updates of the skeleton blocks.
+      GemmPlan<T> s10, s11a, s11b;
+      std::vector<i64> t3off(lv.acol.size() + 1, 0);
+      for (i64 i = 0; i < nodes; i++)
+        for (i64 k = lv.arow[i]; k < lv.arow[i + 1]; k++) {
+          i64 j = lv.acol[k];
+          i64 add = (k != lv.diag[i]) ? Rk[i] * (D[j] - Rk[j]) : 0;
+          t3off[k + 1] = t3off[k] + add;
+        }
+      DVec<T> T3;
+      T3.alloc(std::max<i64>(1, t3off.back()));
+      for (i64 i = 0; i < nodes; i++) {
+        const int M = (int)D[i], Ms = (int)Rk[i], Mr = M - Ms;
+        if (Ms == 0) continue;
+        T* Aii = A + lv.aoff[lv.diag[i]];
+        bool any = false;
+        for (i64 k = lv.arow[i]; k < lv.arow[i + 1]; k++) {
+          if (k == lv.diag[i]) continue;
+          i64 j = lv.acol[k];
+          const int N = (int)D[j], Ns = (int)Rk[j], Nr = N - Ns;
+          T* Aij = A + lv.aoff[k];
+          if (Ns > 0) {
+            s10.add_task(Aij, M, Ms, Ns, T(1));
+            s10.add_entry(Aii + (i64)Ms * M, M, 0, Aij + Ms, M, 0, Mr, T(-1));
+            s10.add_entry(Aij + (i64)Ns * M, M, 0, lv.B.p + lv.boff[j], Nr, 0, Nr, T(-1));
+          }
+          if (Nr > 0) {
+            s11a.add_task(T3.p + t3off[k], Ms, Ms, Nr, T(0));
+            s11a.add_entry(Aij + (i64)Ns * M, M, 0, lv.B.p + lv.boff[j] + (i64)Ns * Nr, Nr, 0, Nr, T(1));
+            any = true;
+          }
+        }
+        if (any) {
+          s11b.add_task(Aii, M, Ms, Ms, T(1));
+          for (i64 k = lv.arow[i]; k < lv.arow[i + 1]; k++) {
+            if (k == lv.diag[i]) continue;
+            i64 j = lv.acol[k];
+            const int N = (int)D[j], Ns = (int)Rk[j], Nr = N - Ns;
+            if (Nr > 0) s11b.add_entry(T3.p + t3off[k], Ms, 0, A + lv.aoff[k] + (i64)Ns * M, M, 1, Nr, T(-1));
+          }
+        }
+      }
+      s10.finalize();
+      s11a.finalize();
+      s11b.finalize();
+      s11a.run(st());
+      s10.run(st());
+      s11b.run(st());
+      ck(cudaStreamSynchronize(st()), "sync");
+    }
+    std::vector<int> inf = lv.info.download(st());
+    lv.info_count = 0;
+    for (int v : inf) lv.info_count += v;
+  }
+
+  void copy_next(i64 l) {
+    Level<T>& lv = L[l];
+    Level<T>& up = L[l - 1];
+    CopyPlan<T> cp;
+    for (i64 i = 0; i < lv.nodes; i++)
+      for (i64 k = lv.arow[i]; k < lv.arow[i + 1]; k++) {
+        i64 j = lv.acol[k];
+        int Ms = (int)lv.ranks[i], Ns = (int)lv.ranks[j];
+        if (Ms > 0 && Ns > 0 && lv.na_off[k] >= 0)
+          cp.add(lv.A.p + lv.aoff[k], lv.dims[i], up.A.p + lv.na_off[k], lv.na_ld[k], Ms, Ns);
+      }
+    cp.finalize();
+    cp.run(st());
+    ck(cudaStreamSynchronize(st()), "sync");
+  }
+
+  void factorize(int* info) override {
+    require(!factored, "factorize: already factored");
+    for (i64 l = levels; l >= 0; l--) {
+      factor_level(l);
+      if (l > 0) copy_next(l);
+    }
+    for (i64 l = 0; l <= levels; l++) info[l] = L[l].info_count;
+    factored = true;
+    pc_built = false;
+  }
+
+  // ULV substitution plans (h2matrix.cpp:505-594).
+  void build_precondition(i64 nrhs) {
+    const int nr = (int)nrhs;
+    pc_fx.clear(); pc_fz.clear(); pc_bx.clear(); pc_by.clear(); pc_fcopy.clear(); pc_bcopy.clear();
+    pc_fx.resize(levels + 1); pc_fz.resize(levels + 1); pc_bx.resize(levels + 1); pc_by.resize(levels + 1);
+    pc_fcopy.resize(levels + 1); pc_bcopy.resize(levels + 1);
+    for (i64 l = 0; l <= levels; l++) {
+      Level<T>& lv = L[l];
+      const T* Yin = (l == levels) ? vin.p : L[l + 1].vZ.p;
+      T* Yout = (l == levels) ? vout.p : L[l + 1].vW.p;
+      const i64 ldx = lv.lenX, ldz = lv.lenZ;
+      T* X = lv.vX.p;
+      T* Z = lv.vZ.p;
+      T* W = lv.vW.p;
+      for (i64 i = 0; i < lv.nodes; i++) {
+        const int M = (int)lv.dims[i], Ms = (int)lv.ranks[i], Mr = M - Ms;
+        if (M == 0) continue;
+        // forward: X = V Y; Z = X_s - sum_j A_ij[:Ms, Ns:] X_j[Ns:]
+        pc_fx[l].add_task(X + lv.xoff[i], ldx, M, nr, T(0));
+        pc_fx[l].add_entry(lv.R.p + lv.qoff[i], M, 1, Yin + lv.xoff[i], ldx, 0, M, T(1));
+        if (Ms > 0) {
+          pc_fcopy[l].add(X + lv.xoff[i], ldx, Z + lv.zoff[i], ldz, Ms, nr);
+          pc_fz[l].add_task(Z + lv.zoff[i], ldz, Ms, nr, T(1));
+          for (i64 k = lv.arow[i]; k < lv.arow[i + 1]; k++) {
+            i64 j = lv.acol[k];
+            const int Nj = (int)lv.dims[j], Ns = (int)lv.ranks[j], Nr = Nj - Ns;
+            if (Nr > 0)
+              pc_fz[l].add_entry(lv.A.p + lv.aoff[k] + (i64)Ns * M, M, 0, X + lv.xoff[j] + Ns, ldx, 0, Nr, T(-1));
+          }
+        }
+        // backward: X_s = W; X_r -= sum_j A_ij[Ms:, :Ns] W_j; Y = U X
+        if (Ms > 0) pc_bcopy[l].add(W + lv.zoff[i], ldz, X + lv.xoff[i], ldx, Ms, nr);
+        if (Mr > 0) {
+          pc_bx[l].add_task(X + lv.xoff[i] + Ms, ldx, Mr, nr, T(1));
+          for (i64 k = lv.arow[i]; k < lv.arow[i + 1]; k++) {
+            i64 j = lv.acol[k];
+            const int Ns = (int)lv.ranks[j];
+            if (Ns > 0) pc_bx[l].add_entry(lv.A.p + lv.aoff[k] + Ms, M, 0, W + lv.zoff[j], ldz, 0, Ns, T(-1));
+          }
+        }
+        const i64 ldy = (l == levels) ? N : L[l + 1].lenZ;
+        pc_by[l].add_task(Yout + lv.xoff[i], ldy, M, nr, T(0));
+        pc_by[l].add_entry(lv.Q.p + lv.qoff[i], M, 0, X + lv.xoff[i], ldx, 0, M, T(1));
+      }
+      pc_fx[l].finalize(); pc_fz[l].finalize(); pc_bx[l].finalize(); pc_by[l].finalize();
+      pc_fcopy[l].finalize(); pc_bcopy[l].finalize();
+    }
+    pc_built = true;
+  }
+
+  void precondition(i64 nrhs, double* dX, i64 ldx) override {
+    if (!factored) throw H2Error{H2DEV_ERR_STATE, "solve_precondition before factorize"};
+    require(nrhs > 0 && ldx >= N, "precondition: bad nrhs/ld");
+    ensure_vectors(nrhs);
+    if (!pc_built) build_precondition(nrhs);
+    stage_in(nrhs, dX, ldx);
+    for (i64 l = levels; l >= 0; l--) {
+      pc_fx[l].run(st());
+      pc_fcopy[l].run(st());
+      pc_fz[l].run(st());
+    }
+    for (i64 l = 0; l <= levels; l++) {
+      pc_bcopy[l].run(st());
+      pc_bx[l].run(st());
+      pc_by[l].run(st());
+    }
+    stage_out(nrhs, dX, ldx);
+  }
+
+  void level_dims(i64 l, i64* dims, i64* ranks) const override {
+    require(l >= 0 && l <= levels, "level out of range");
+    for (i64 i = 0; i < L[l].nodes; i++) {
+      if (dims) dims[i] = L[l].dims[i];
+      if (ranks) ranks[i] = L[l].ranks[i];
+    }
+  }
+
+  i64 export_size(i64 l, int what) const override {
+    require(l >= 0 && l <= levels, "level out of range");
+    const Level<T>& lv = L[l];
+    switch (what) {
+      case H2DEV_EXPORT_S: return 3 * lv.lenX;
+      case H2DEV_EXPORT_Q:
+      case H2DEV_EXPORT_R: return lv.qoff.back();
+      case H2DEV_EXPORT_A: return lv.aoff.back();
+      case H2DEV_EXPORT_C: return lv.coff.back();
+    }
+    require(false, "export: unknown container");
+    return 0;
+  }
+
+  void export_to(i64 l, int what, double* out) override {
+    i64 n = export_size(l, what);
+    if (n == 0) return;
+    const Level<T>& lv = L[l];
+    if (what == H2DEV_EXPORT_S) {
+      ck(cudaStreamSynchronize(st()), "sync");
+      ck(cudaMemcpy(out, lv.pts.p, sizeof(double) * n, cudaMemcpyDeviceToHost), "export");
+      return;
+    }
+    const T* src = what == H2DEV_EXPORT_Q ? lv.Q.p : what == H2DEV_EXPORT_R ? lv.R.p : what == H2DEV_EXPORT_A ? lv.A.p : lv.C.p;
+    DVec<double> tmp;
+    tmp.alloc(n);
+    ck(launch_convert<T, double>(src, tmp.p, n, st()), "export convert");
+    ck(cudaStreamSynchronize(st()), "sync");
+    ck(cudaMemcpy(out, tmp.p, sizeof(double) * n, cudaMemcpyDeviceToHost), "export");
+  }
+};
+
+// Residual norm of min || beta e1 - H y || for an (rows x cols) Hessenberg
+// block of a column-major array with leading dimension ld.
+static double ls_residual(const double* Hin, int ld, int rows, int cols, double beta) {
+  std::vector<double> H((size_t)rows * cols), s(rows, 0.);
+  for (int j = 0; j < cols; j++)
+    for (int r = 0; r < rows; r++) H[r + (size_t)j * rows] = Hin[r + (size_t)j * ld];
+  s[0] = beta;
+  for (int k = 0; k < cols; k++) {
+    double a = H[k + (size_t)k * rows], b = H[k + 1 + (size_t)k * rows];
+    double r = std::hypot(a, b);
+    if (r == 0.) continue;
+    double c = a / r, sn = b / r;
+    for (int j = k; j < cols; j++) {
+      double x = H[k + (size_t)j * rows], y = H[k + 1 + (size_t)j * rows];
+      H[k + (size_t)j * rows] = c * x + sn * y;
+      H[k + 1 + (size_t)j * rows] = -sn * x + c * y;
+    }
+    double x = s[k], y = s[k + 1];
+    s[k] = c * x + sn * y;
+    s[k + 1] = -sn * x + c * y;
+  }
+  return std::fabs(s[cols]);
+}
+
+// ------------------------------------------------------------------ GMRES
+// solver.cpp:191-248 with one independent GMRES per right-hand side.
+static int gmres(SolverBase& A, SolverBase& M, double tol, i64 nrhs, double* dX, const double* dB, i64 ld, i64 inner,
+                 i64 outer, int early_exit, double* resid, i64* iters) {
+  require(A.lenX() == M.lenX(), "gmres: A and M sizes differ");
+  require(inner >= 1 && inner <= 16 && outer >= 0 && nrhs >= 1, "gmres: inner must be in [1,16]");
+  cudaStream_t st = A.h->stream;
+  const i64 N = A.lenX();
+  const int nr = (int)nrhs;
+  const int ldh = (int)inner + 1;
+  const i64 vstride = N * nrhs;
+  DVec<double> V, w, R, Bc, X, H, y, beta, nrm2, partial, normb, rvec, hcol;
+  DVec<int> active;
+  V.alloc((size_t)(inner + 1) * vstride);
+  w.alloc(vstride);
+  R.alloc(vstride);
+  Bc.alloc(vstride);
+  X.alloc(vstride);
+  H.alloc((size_t)ldh * inner * nrhs);
+  y.alloc((size_t)inner * nrhs);
+  beta.alloc(nrhs);
+  nrm2.alloc(nrhs);
+  normb.alloc(nrhs);
+  rvec.alloc(nrhs);
+  hcol.alloc((size_t)(inner + 1) * nrhs);
+  active.alloc(nrhs);
+  const int nch = dots_chunks(N);
+  partial.alloc((size_t)nch * (inner + 1) * nrhs);
+  for (i64 c = 0; c < nrhs; c++) {
+    ck(cudaMemcpyAsync(Bc.p + c * N, dB + c * ld, sizeof(double) * N, cudaMemcpyDeviceToDevice, st), "copy B");
+    ck(cudaMemcpyAsync(X.p + c * N, dX + c * ld, sizeof(double) * N, cudaMemcpyDeviceToDevice, st), "copy X");
+  }
+  ck(launch_dots(Bc.p, 0, 1, Bc.p, N, nr, partial.p, nch, nrm2.p, st), "dots");
+  std::vector<double> hn(nrhs);
+  {
+    std::vector<double> n2 = nrm2.download(st);
+    for (i64 c = 0; c < nrhs; c++) {
+      hn[c] = std::sqrt(n2[c]);
+      if (hn[c] == 0.) hn[c] = 1.;
+    }
+    ck(cudaMemcpy(normb.p, hn.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice), "normb");
+  }
+  ck(cudaMemcpyAsync(R.p, Bc.p, sizeof(double) * vstride, cudaMemcpyDeviceToDevice, st), "R=B");
+  std::vector<double> res((size_t)(outer + 1) * nrhs, 0.);
+  std::vector<i64> it(nrhs, 0);
+  std::vector<int> act(nrhs, 1);
+  for (i64 c = 0; c < nrhs; c++) {
+    res[c * (outer + 1)] = 1.;
+    act[c] = (0 < outer && tol <= 1.) ? 1 : 0;
+  }
+  // The reference starts from the given X with R = B (not B - A X) in its
+  // first cycle (solver.cpp:204); the initial guess is zero in every caller.
+  i64 cycle = 0;
+  while (true) {
+    bool any = false;
+    for (i64 c = 0; c < nrhs; c++) any |= act[c] != 0;
+    if (!any) break;
+    ck(cudaMemcpy(active.p, act.data(), sizeof(int) * nrhs, cudaMemcpyHostToDevice), "active");
+    M.precondition(nrhs, R.p, N);
+    ck(launch_dots(R.p, 0, 1, R.p, N, nr, partial.p, nch, nrm2.p, st), "dots");
+    ck(launch_scale_by_norm(R.p, V.p, nrm2.p, beta.p, 1, N, nr, st), "v0");
+    ck(cudaMemsetAsync(H.p, 0, sizeof(double) * H.n, st), "H=0");
+    i64 used = inner;
+    for (i64 i = 0; i < inner; i++) {
+      ck(cudaMemcpyAsync(w.p, V.p + i * vstride, sizeof(double) * vstride, cudaMemcpyDeviceToDevice, st), "w=v");
+      A.matvec(nrhs, w.p, N);
+      M.precondition(nrhs, w.p, N);
+      const int kv = (int)i + 1;
+      ck(launch_dots(V.p, vstride, kv, w.p, N, nr, partial.p, nch, hcol.p, st), "dots");
+      // H[:kv, i] for every rhs (rhs c block of H has stride ldh*inner)
+      ck(launch_gs_update(w.p, V.p, vstride, hcol.p, kv, kv, N, nr, -1.0, nullptr, st), "gs");
+      {
+        // scatter hcol into H column i
+        CopyPlan<double> cp;
+        for (int c = 0; c < nr; c++) cp.add(hcol.p + (i64)c * kv, kv, H.p + (i64)c * ldh * inner + i * ldh, ldh, kv, 1);
+        cp.finalize();
+        cp.run(st);
+        ck(launch_dots(w.p, 0, 1, w.p, N, nr, partial.p, nch, nrm2.p, st), "dots");
+        // H[i+1, i] and v_{i+1}; hout stride is per rhs block
+        DVec<double> hv;
+        hv.alloc(nrhs);
+        ck(launch_scale_by_norm(w.p, V.p + (i + 1) * vstride, nrm2.p, hv.p, 1, N, nr, st), "scale");
+        CopyPlan<double> cp2;
+        for (int c = 0; c < nr; c++) cp2.add(hv.p + c, 1, H.p + (i64)c * ldh * inner + i * ldh + i + 1, 1, 1, 1);
+        cp2.finalize();
+        cp2.run(st);
+      }
+      if (early_exit) {
+        // Hessenberg least-squares residual of the first i+1 steps, on the
+        // host (H is at most 17 x 16 per right-hand side).
+        std::vector<double> hh = H.download(st), bb = beta.download(st);
+        bool done = true;
+        for (i64 c = 0; c < nrhs && done; c++) {
+          if (!act[c]) continue;
+          double est = ls_residual(hh.data() + c * ldh * inner, ldh, (int)i + 2, (int)i + 1, bb[c]);
+          if (!(est / hn[c] < tol * 0.5)) done = false;
+        }
+        if (done) {
+          used = i + 1;
+          break;
+        }
+      }
+    }
+    if (used == inner) {
+      ck(launch_gmres_ls(H.p, ldh, (int)inner, beta.p, y.p, nr, st), "ls");
+    } else {
+      // Compact the leading used x used block per rhs for the final solve.
+      DVec<double> Hs;
+      Hs.alloc((size_t)(used + 1) * used * nrhs);
+      CopyPlan<double> cp;
+      for (int c = 0; c < nr; c++)
+        cp.add(H.p + (i64)c * ldh * inner, ldh, Hs.p + (i64)c * (used + 1) * used, used + 1, (int)used + 1, (int)used);
+      cp.finalize();
+      cp.run(st);
+      ck(launch_gmres_ls(Hs.p, (int)used + 1, (int)used, beta.p, y.p, nr, st), "ls");
+    }
+    ck(launch_gs_update(X.p, V.p, vstride, y.p, used, (int)used, N, nr, 1.0, active.p, st), "x update");
+    ck(cudaMemcpyAsync(R.p, X.p, sizeof(double) * vstride, cudaMemcpyDeviceToDevice, st), "R=X");
+    A.matvec(nrhs, R.p, N);
+    ck(launch_axpby(R.p, Bc.p, -1.0, 1.0, vstride, st), "R=B-AX");
+    ck(launch_dots(R.p, 0, 1, R.p, N, nr, partial.p, nch, nrm2.p, st), "dots");
+    ck(launch_residual_norm_finish(nrm2.p, normb.p, rvec.p, nr, st), "resid");
+    std::vector<double> rv = rvec.download(st);
+    cycle++;
+    for (i64 c = 0; c < nrhs; c++) {
+      if (!act[c]) continue;
+      it[c]++;
+      res[c * (outer + 1) + it[c]] = rv[c];
+      if (!(it[c] < outer && tol <= rv[c])) act[c] = 0;
+    }
+    // Columns that stopped keep their X; columns still running restart from
+    // the true residual.  Converged columns keep R (unused).
+  }
+  for (i64 c = 0; c < nrhs; c++)
+    ck(cudaMemcpyAsync(dX + c * ld, X.p + c * N, sizeof(double) * N, cudaMemcpyDeviceToDevice, st), "copy X out");
+  ck(cudaStreamSynchronize(st), "sync");
+  bool conv = true;
+  for (i64 c = 0; c < nrhs; c++) {
+    for (i64 k = 0; k <= outer; k++) resid[c * (outer + 1) + k] = res[c * (outer + 1) + k];
+    if (iters) iters[c] = it[c];
+    if (!(res[c * (outer + 1) + it[c]] < tol)) conv = false;
+  }
+  return conv ? H2DEV_OK : H2DEV_ERR_NOCONV;
+}
+
+}  // namespace h2b
+
+struct h2dev_solver_s {
+  std::unique_ptr<h2b::SolverBase> impl;
+};
+
+using namespace h2b;
+
+#define H2_API_BEGIN try {
+#define H2_API_END                                \
+  }                                               \
+  catch (const H2Error& e) {                      \
+    g_last_error = e.msg;                         \
+    return e.code;                                \
+  }                                               \
+  catch (const std::bad_alloc&) {                 \
+    g_last_error = "host allocation failed";      \
+    return H2DEV_ERR_OOM;                         \
+  }                                               \
+  catch (const std::exception& e) {               \
+    g_last_error = e.what();                      \
+    return H2DEV_ERR_ARG;                         \
+  }
+
+static KernelParams make_kp(int kernel, double singularity, double alpha) {
+  require(kernel == H2DEV_KERNEL_LAPLACE || kernel == H2DEV_KERNEL_YUKAWA, "unknown kernel");
+  require(singularity != 0., "singularity must be nonzero");
+  KernelParams kp;
+  kp.kind = kernel;
+  kp.diag = 1. / singularity;
+  kp.alpha = alpha;
+  return kp;
+}
+
+extern "C" {
+
+const char* h2dev_last_error_message(void) { return g_last_error.c_str(); }
+
+int h2_uniform_unit_cube_rnd(double* bodies, int64_t nbodies, double diameter, int64_t dim, unsigned seed) {
+  H2_API_BEGIN
+  require(bodies && nbodies >= 0, "bad arguments");
+  uniform_unit_cube_rnd(bodies, nbodies, diameter, dim, seed);
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2_uniform_rhs(double* x, int64_t n) {
+  H2_API_BEGIN
+  require(x && n >= 0, "bad arguments");
+  uniform_rhs(x, n);
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int64_t h2_levels_for(int64_t nbodies, int64_t leaf) {
+  if (nbodies <= 0 || leaf <= 0) return -1;
+  leaf = nbodies < leaf ? nbodies : leaf;
+  return (int64_t)std::log2((double)nbodies / leaf);
+}
+
+int h2_build_tree(double* bodies, int64_t nbodies, int64_t levels, int64_t* cell_child, int64_t* cell_body,
+                  double* cell_R, double* cell_C) {
+  H2_API_BEGIN
+  require(bodies && nbodies > 0 && levels >= 0 && levels < 40, "bad arguments");
+  require(((int64_t)1 << levels) <= nbodies, "more leaves than bodies");
+  int64_t ncells = ((int64_t)2 << levels) - 1;
+  std::vector<Cell> cells(ncells);
+  build_binary_tree(cells.data(), bodies, nbodies, levels);
+  for (int64_t c = 0; c < ncells; c++) {
+    for (int k = 0; k < 2; k++) {
+      if (cell_child) cell_child[2 * c + k] = cells[c].child[k];
+      if (cell_body) cell_body[2 * c + k] = cells[c].body[k];
+    }
+    for (int k = 0; k < 3; k++) {
+      if (cell_R) cell_R[3 * c + k] = cells[c].R[k];
+      if (cell_C) cell_C[3 * c + k] = cells[c].C[k];
+    }
+  }
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2_pair_csr(char kind, int64_t ncells, const int64_t* cell_child, const int64_t* cell_body, const double* cell_R,
+                const double* cell_C, double theta, int64_t* row, int64_t* col, int64_t cap, int64_t* nnz) {
+  H2_API_BEGIN
+  require(ncells > 0 && cell_child && cell_body && cell_R && cell_C && row && nnz, "bad arguments");
+  require(kind == 'N' || kind == 'n' || kind == 'F' || kind == 'f', "kind must be N or F");
+  std::vector<Cell> cells(ncells);
+  for (int64_t c = 0; c < ncells; c++) {
+    for (int k = 0; k < 2; k++) {
+      cells[c].child[k] = cell_child[2 * c + k];
+      cells[c].body[k] = cell_body[2 * c + k];
+    }
+    for (int k = 0; k < 3; k++) {
+      cells[c].R[k] = cell_R[3 * c + k];
+      cells[c].C[k] = cell_C[3 * c + k];
+    }
+  }
+  PairCSR csr = build_pair_csr(kind, cells, theta);
+  for (int64_t i = 0; i <= ncells; i++) row[i] = csr.row[i];
+  *nnz = (int64_t)csr.col.size();
+  if (col && cap >= *nnz)
+    for (size_t k = 0; k < csr.col.size(); k++) col[k] = csr.col[k];
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_handle_create(int device, h2dev_handle_t* out) {
+  H2_API_BEGIN
+  require(out != nullptr, "null out");
+  ck(cudaSetDevice(device), "cudaSetDevice");
+  auto* h = new h2dev_handle_s();
+  h->device = device;
+  cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete h;
+    ck(e, "cudaStreamCreate");
+  }
+  *out = h;
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_handle_destroy(h2dev_handle_t h) {
+  H2_API_BEGIN
+  if (!h) return H2DEV_OK;
+  cudaStreamSynchronize(h->stream);
+  cudaStreamDestroy(h->stream);
+  delete h;
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_handle_synchronize(h2dev_handle_t h) {
+  H2_API_BEGIN
+  require(h != nullptr, "null handle");
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_solver_create(h2dev_handle_t h, int kernel, double singularity, double alpha, double epi, int64_t rank,
+                        int64_t leveled_rank, int64_t ncells, const int64_t* cell_child, const int64_t* cell_body,
+                        const double* cell_R, const double* cell_C, double theta, const double* bodies,
+                        int64_t nbodies, int64_t levels, int64_t samples, int precision, h2dev_solver_t* out) {
+  H2_API_BEGIN
+  require(h && out && cell_child && cell_body && cell_R && cell_C && bodies, "null argument");
+  require(levels >= 0 && ncells == ((int64_t)2 << levels) - 1, "ncells must be 2^(levels+1)-1");
+  require(nbodies > 0 && epi >= 0., "bad sizes");
+  require(precision == H2DEV_FP64 || precision == H2DEV_FP32, "precision");
+  ck(cudaSetDevice(h->device), "cudaSetDevice");
+  BuildArgs a;
+  a.kp = make_kp(kernel, singularity, alpha);
+  a.epi = epi;
+  a.rank = rank;
+  a.leveled_rank = leveled_rank;
+  a.levels = levels;
+  a.nbodies = nbodies;
+  a.samples = samples;
+  a.theta = theta;
+  a.bodies = bodies;
+  a.cells.resize(ncells);
+  for (int64_t c = 0; c < ncells; c++) {
+    for (int k = 0; k < 2; k++) {
+      a.cells[c].child[k] = cell_child[2 * c + k];
+      a.cells[c].body[k] = cell_body[2 * c + k];
+    }
+    for (int k = 0; k < 3; k++) {
+      a.cells[c].R[k] = cell_R[3 * c + k];
+      a.cells[c].C[k] = cell_C[3 * c + k];
+    }
+  }
+  require(a.cells[0].body[0] == 0 && a.cells[0].body[1] == nbodies, "root cell must span all bodies");
+  std::unique_ptr<h2dev_solver_s> s(new h2dev_solver_s());
+  if (precision == H2DEV_FP64) {
+    auto* p = new Solver<double>();
+    s->impl.reset(p);
+    p->h = h;
+    p->build(a);
+  } else {
+    auto* p = new Solver<float>();
+    s->impl.reset(p);
+    p->h = h;
+    p->build(a);
+  }
+  *out = s.release();
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_solver_destroy(h2dev_solver_t s) {
+  H2_API_BEGIN
+  if (s) {
+    if (s->impl && s->impl->h) cudaStreamSynchronize(s->impl->h->stream);
+    delete s;
+  }
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_solver_shape(h2dev_solver_t s, int64_t* levels, int64_t* lenX) {
+  H2_API_BEGIN
+  require(s && s->impl, "null solver");
+  if (levels) *levels = s->impl->nlevels();
+  if (lenX) *lenX = s->impl->lenX();
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_solver_level_dims(h2dev_solver_t s, int64_t level, int64_t* dims, int64_t* ranks) {
+  H2_API_BEGIN
+  require(s && s->impl, "null solver");
+  s->impl->level_dims(level, dims, ranks);
+  return H2DEV_OK;
+  H2_API_END
+}
+
+static void with_device_copy(h2dev_handle_s* h, int64_t n, int64_t nrhs, double* X, int64_t ld,
+                             const std::function<void(double*)>& fn) {
+  DVec<double> d;
+  d.alloc((size_t)n * nrhs);
+  ck(cudaMemcpy2DAsync(d.p, sizeof(double) * n, X, sizeof(double) * ld, sizeof(double) * n, nrhs,
+                       cudaMemcpyHostToDevice, h->stream),
+     "H2D");
+  fn(d.p);
+  ck(cudaMemcpy2DAsync(X, sizeof(double) * ld, d.p, sizeof(double) * n, sizeof(double) * n, nrhs,
+                       cudaMemcpyDeviceToHost, h->stream),
+     "D2H");
+  ck(cudaStreamSynchronize(h->stream), "sync");
+}
+
+int h2dev_matvec(h2dev_solver_t s, int64_t nrhs, double* X, int64_t ldx) {
+  H2_API_BEGIN
+  require(s && s->impl && X, "null argument");
+  SolverBase* p = s->impl.get();
+  require(nrhs > 0 && ldx >= p->lenX(), "bad nrhs/ld");
+  with_device_copy(p->h, p->lenX(), nrhs, X, ldx, [&](double* d) { p->matvec(nrhs, d, p->lenX()); });
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_matvec_device(h2dev_solver_t s, int64_t nrhs, double* dX, int64_t ldx) {
+  H2_API_BEGIN
+  require(s && s->impl && dX, "null argument");
+  s->impl->matvec(nrhs, dX, ldx);
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_factorize(h2dev_solver_t s, int* info_per_level) {
+  H2_API_BEGIN
+  require(s && s->impl, "null solver");
+  std::vector<int> info(s->impl->nlevels() + 1, 0);
+  s->impl->factorize(info.data());
+  int any = 0;
+  for (size_t l = 0; l < info.size(); l++) {
+    if (info_per_level) info_per_level[l] = info[l];
+    any |= info[l] != 0;
+  }
+  return any ? H2DEV_ERR_SINGULAR : H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_solve_precondition(h2dev_solver_t s, int64_t nrhs, double* X, int64_t ldx) {
+  H2_API_BEGIN
+  require(s && s->impl && X, "null argument");
+  SolverBase* p = s->impl.get();
+  require(nrhs > 0 && ldx >= p->lenX(), "bad nrhs/ld");
+  with_device_copy(p->h, p->lenX(), nrhs, X, ldx, [&](double* d) { p->precondition(nrhs, d, p->lenX()); });
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_solve_precondition_device(h2dev_solver_t s, int64_t nrhs, double* dX, int64_t ldx) {
+  H2_API_BEGIN
+  require(s && s->impl && dX, "null argument");
+  s->impl->precondition(nrhs, dX, ldx);
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_solve_gmres_device(h2dev_solver_t A, h2dev_solver_t M, double tol, int64_t nrhs, double* dX,
+                             const double* dB, int64_t ld, int64_t inner, int64_t outer, int early_exit,
+                             double* resid, int64_t* iters) {
+  H2_API_BEGIN
+  require(A && A->impl && M && M->impl && dX && dB && resid, "null argument");
+  require(ld >= A->impl->lenX(), "bad ld");
+  return gmres(*A->impl, *M->impl, tol, nrhs, dX, dB, ld, inner, outer, early_exit, resid, iters);
+  H2_API_END
+}
+
+int h2dev_solve_gmres(h2dev_solver_t A, h2dev_solver_t M, double tol, int64_t nrhs, double* X, const double* B,
+                      int64_t ld, int64_t inner, int64_t outer, int early_exit, double* resid, int64_t* iters) {
+  H2_API_BEGIN
+  require(A && A->impl && M && M->impl && X && B && resid, "null argument");
+  SolverBase* a = A->impl.get();
+  const int64_t n = a->lenX();
+  require(nrhs > 0 && ld >= n, "bad nrhs/ld");
+  cudaStream_t st = a->h->stream;
+  DVec<double> dX, dB;
+  dX.alloc((size_t)n * nrhs);
+  dB.alloc((size_t)n * nrhs);
+  ck(cudaMemcpy2DAsync(dX.p, sizeof(double) * n, X, sizeof(double) * ld, sizeof(double) * n, nrhs,
+                       cudaMemcpyHostToDevice, st), "H2D");
+  ck(cudaMemcpy2DAsync(dB.p, sizeof(double) * n, B, sizeof(double) * ld, sizeof(double) * n, nrhs,
+                       cudaMemcpyHostToDevice, st), "H2D");
+  int rc = gmres(*a, *M->impl, tol, nrhs, dX.p, dB.p, n, inner, outer, early_exit, resid, iters);
+  ck(cudaMemcpy2DAsync(X, sizeof(double) * ld, dX.p, sizeof(double) * n, sizeof(double) * n, nrhs,
+                       cudaMemcpyDeviceToHost, st), "D2H");
+  ck(cudaStreamSynchronize(st), "sync");
+  return rc;
+  H2_API_END
+}
+
+int h2dev_gen_block(h2dev_handle_t h, int kernel, double singularity, double alpha, const double* bi, int64_t m,
+                    const double* bj, int64_t n, double* out) {
+  H2_API_BEGIN
+  require(h && bi && bj && out && m >= 0 && n >= 0, "bad arguments");
+  require(m * n < ((int64_t)1 << 31), "block too large");
+  KernelParams kp = make_kp(kernel, singularity, alpha);
+  if (m == 0 || n == 0) return H2DEV_OK;
+  DVec<double> di, dj, dout;
+  di.upload(std::vector<double>(bi, bi + 3 * m));
+  dj.upload(std::vector<double>(bj, bj + 3 * n));
+  dout.alloc((size_t)m * n);
+  std::vector<GenTask> gt(1);
+  gt[0].bi = di.p;
+  gt[0].bj = dj.p;
+  gt[0].m = (int)m;
+  gt[0].n = (int)n;
+  gt[0].out_off = 0;
+  gt[0].ld = m;
+  DVec<GenTask> dg;
+  dg.upload(gt);
+  int chunks = (int)std::min<int64_t>(4096, (m * n + 65535) / 65536);
+  ck(launch_gen_blocks<double>(kp, dg.p, 1, chunks, dout.p, h->stream), "gen");
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  ck(cudaMemcpy(out, dout.p, sizeof(double) * m * n, cudaMemcpyDeviceToHost), "D2H");
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_dense_matvec_device(h2dev_handle_t h, int kernel, double singularity, double alpha, const double* dbodies,
+                              int64_t n, int64_t nrhs, const double* dX, double* dY, int64_t ld) {
+  H2_API_BEGIN
+  require(h && dbodies && dX && dY && n > 0 && nrhs > 0 && ld >= n, "bad arguments");
+  KernelParams kp = make_kp(kernel, singularity, alpha);
+  ck(launch_dense_matvec(kp, dbodies, n, dX, ld, dY, ld, (int)nrhs, h->stream), "dense_matvec");
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_dense_matvec(h2dev_handle_t h, int kernel, double singularity, double alpha, const double* bodies,
+                       int64_t n, int64_t nrhs, const double* X, double* Y, int64_t ld) {
+  H2_API_BEGIN
+  require(h && bodies && X && Y && n > 0 && nrhs > 0 && ld >= n, "bad arguments");
+  KernelParams kp = make_kp(kernel, singularity, alpha);
+  DVec<double> db, dx, dy;
+  db.upload(std::vector<double>(bodies, bodies + 3 * n));
+  dx.alloc((size_t)n * nrhs);
+  dy.alloc((size_t)n * nrhs);
+  ck(cudaMemcpy2D(dx.p, sizeof(double) * n, X, sizeof(double) * ld, sizeof(double) * n, nrhs,
+                  cudaMemcpyHostToDevice), "H2D");
+  ck(launch_dense_matvec(kp, db.p, n, dx.p, n, dy.p, n, (int)nrhs, h->stream), "dense_matvec");
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  ck(cudaMemcpy2D(Y, sizeof(double) * ld, dy.p, sizeof(double) * n, sizeof(double) * n, nrhs,
+                  cudaMemcpyDeviceToHost), "D2H");
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_solver_export_size(h2dev_solver_t s, int64_t level, int what, int64_t* count) {
+  H2_API_BEGIN
+  require(s && s->impl && count, "null argument");
+  *count = s->impl->export_size(level, what);
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_solver_export(h2dev_solver_t s, int64_t level, int what, double* out) {
+  H2_API_BEGIN
+  require(s && s->impl && out, "null argument");
+  s->impl->export_to(level, what, out);
+  return H2DEV_OK;
+  H2_API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,483 @@
+// Shared-basis compression kernels (compute_basis, h2matrix.cpp:13-63).
+//
+// One CTA per box of a tree level.  Step 1 (k_sample_tsqr) forms the R
+// factor of the far-field sample block XF = K(far samples, box bodies)
+// without materialising XF: sample rows are generated 32 at a time into
+// shared memory and folded into R with Householder reflectors on
+// (row j of R, tile column j).  Step 2 (k_cpqr) runs the column-pivoted
+// Householder QR of R with Eigen 3.4's ColPivHouseholderQR pivot, norm
+// downdate and rank rules.  Step 3 (k_basis_finish) forms the interpolative
+// decomposition [I, R11^-1 R12], permutes the box bodies skeleton-first and
+// builds either the ID basis (operator mode) or the orthogonal basis with
+// completion plus the triangular R (preconditioner mode).
+#include "common.cuh"
+#include "kernels.h"
+
+#include <cfloat>
+
+namespace h2b {
+
+template <typename T> struct Tiny;
+template <> struct Tiny<double> { static __device__ double v() { return DBL_MIN; } };
+template <> struct Tiny<float> { static __device__ float v() { return FLT_MIN; } };
+
+constexpr int TS_THREADS = 256;
+constexpr int TS_MAXCOL = 4;  // columns owned per thread: M <= 1024
+
+// R (row-major M x M per box, zero on entry) of the sample block.
+template <typename T>
+__global__ void __launch_bounds__(TS_THREADS) k_sample_tsqr(
+    KernelParams kp, const double* __restrict__ bodies, const double* __restrict__ pts,
+    const i64* __restrict__ xoff, const i64* __restrict__ dims, const int* __restrict__ sidx,
+    const i64* __restrict__ soff, T* __restrict__ Rws, const i64* __restrict__ qoff) {
+  const int box = blockIdx.x;
+  const int M = (int)dims[box];
+  const i64 S = soff[box + 1] - soff[box];
+  if (M == 0 || S == 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* tile = reinterpret_cast<T*>(smem_raw);            // 32 x M, row-major
+  T* vbuf = tile + 32 * M;                             // 32
+  double* sp = reinterpret_cast<double*>(vbuf + 32);   // 32 x 3
+  __shared__ T s_tau;
+
+  T* R = Rws + qoff[box];
+  const int* my_sidx = sidx + soff[box];
+  const double* bp = pts + 3 * xoff[box];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+  double px[TS_MAXCOL], py[TS_MAXCOL], pz[TS_MAXCOL];
+#pragma unroll
+  for (int k = 0; k < TS_MAXCOL; k++) {
+    int c = tid + k * TS_THREADS;
+    px[k] = c < M ? bp[3 * c] : 0.;
+    py[k] = c < M ? bp[3 * c + 1] : 0.;
+    pz[k] = c < M ? bp[3 * c + 2] : 0.;
+  }
+
+  int rows = 0;  // rows of R that can be nonzero so far
+  for (i64 t0 = 0; t0 < S; t0 += 32) {
+    const int nrows = (int)((S - t0) < 32 ? (S - t0) : 32);
+    if (tid < nrows) {
+      const double* q = bodies + 3 * (i64)my_sidx[t0 + tid];
+      sp[3 * tid] = q[0];
+      sp[3 * tid + 1] = q[1];
+      sp[3 * tid + 2] = q[2];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < TS_MAXCOL; k++) {
+      int c = tid + k * TS_THREADS;
+      if (c < M)
+        for (int r = 0; r < 32; r++)
+          tile[r * M + c] = r < nrows ? (T)kernel_fast(kp, sp[3 * r] - px[k], sp[3 * r + 1] - py[k], sp[3 * r + 2] - pz[k]) : T(0);
+    }
+    __syncthreads();
+    const int jend = (rows + nrows) < M ? (rows + nrows) : M;
+    for (int j = 0; j < jend; j++) {
+      const int owner = j % TS_THREADS;
+      if (warp == (owner >> 5)) {
+        // Reflector on (R[j][j], tile[:, j]), computed by the owner's warp:
+        // lane r holds tile row r.
+        T x = lane < nrows ? tile[lane * M + j] : T(0);
+        T sig = x * x;
+        for (int o = 16; o > 0; o >>= 1) sig += __shfl_xor_sync(0xffffffffu, sig, o);
+        T alpha = R[(i64)j * M + j];
+        T tau = 0, scale = 0, beta = alpha;
+        if (sig > Tiny<T>::v()) {
+          T nrm = sqrt(alpha * alpha + sig);
+          beta = alpha >= T(0) ? -nrm : nrm;
+          tau = (beta - alpha) / beta;
+          scale = T(1) / (alpha - beta);
+        }
+        vbuf[lane] = x * scale;
+        if (lane == 0) {
+          s_tau = tau;
+          R[(i64)j * M + j] = beta;
+        }
+      }
+      __syncthreads();
+      const T tau = s_tau;
+      if (tau != T(0)) {
+#pragma unroll
+        for (int k = 0; k < TS_MAXCOL; k++) {
+          int c = tid + k * TS_THREADS;
+          if (c > j && c < M) {
+            T w = R[(i64)j * M + c];
+            for (int r = 0; r < nrows; r++) w += vbuf[r] * tile[r * M + c];
+            w *= tau;
+            R[(i64)j * M + c] -= w;
+            for (int r = 0; r < nrows; r++) tile[r * M + c] -= w * vbuf[r];
+          }
+        }
+      }
+      __syncthreads();
+    }
+    rows = jend;
+  }
+}
+
+// Column-pivoted Householder QR (Eigen 3.4 ColPivHouseholderQR::computeInPlace
+// restated) of the K x M row-major matrix in Rws.  ``steps`` bounds the
+// number of pivots taken (min(K, M) in threshold mode, the fixed rank in
+// fixed-rank mode; the first ``steps`` rows of R do not depend on later
+// steps).  Writes perm (position k holds the original column), maxpivot and
+// the nonzero-pivot count.
+template <typename T>
+__global__ void __launch_bounds__(256) k_cpqr(const i64* __restrict__ dims, const i64* __restrict__ krows,
+                                              T* __restrict__ Rws, const i64* __restrict__ qoff,
+                                              int* __restrict__ perm_out, const i64* __restrict__ xoff,
+                                              double* __restrict__ maxpiv_out, int* __restrict__ nonzero_out,
+                                              i64 step_cap) {
+  const int box = blockIdx.x;
+  const int M = (int)dims[box];
+  const int K = (int)krows[box];
+  if (M == 0 || K == 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* nu = reinterpret_cast<double*>(smem_raw);  // updated norms
+  double* nd = nu + M;                               // direct norms
+  T* ess = reinterpret_cast<T*>(nd + M);             // K
+  int* perm = reinterpret_cast<int*>(ess + K);       // M
+  __shared__ double red_v[32];
+  __shared__ int red_i[32];
+  __shared__ T red_t[32];
+  __shared__ int s_nonzero;
+  __shared__ double s_maxpiv;
+
+  T* W = Rws + qoff[box];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int size = K < M ? K : M;
+  int steps = size;
+  if (step_cap >= 0 && step_cap < steps) steps = (int)step_cap;
+
+  for (int c = tid; c < M; c += nt) {
+    double s = 0.;
+    for (int r = 0; r < K; r++) {
+      double v = (double)W[(i64)r * M + c];
+      s += v * v;
+    }
+    nu[c] = sqrt(s);
+    nd[c] = nu[c];
+    perm[c] = c;
+  }
+  __syncthreads();
+  double mx = 0.;
+  int mi = 0;
+  for (int c = tid; c < M; c += nt)
+    if (nu[c] > mx) { mx = nu[c]; mi = c; }
+  argmax_first(mx, mi, red_v, red_i);
+  const double eps = (sizeof(T) == 8) ? DBL_EPSILON : (double)FLT_EPSILON;
+  const double thr_helper = (mx * eps) * (mx * eps) / (double)K;
+  const double downdate_thr = sqrt(eps);
+  if (tid == 0) {
+    s_nonzero = size;
+    s_maxpiv = 0.;
+  }
+  __syncthreads();
+
+  for (int k = 0; k < steps; k++) {
+    double bv = -1.;
+    int bi = 0x7fffffff;
+    for (int c = k + tid; c < M; c += nt)
+      if (nu[c] > bv) { bv = nu[c]; bi = c; }
+    argmax_first(bv, bi, red_v, red_i);
+    if (tid == 0) {
+      if (s_nonzero == size && bv * bv < thr_helper * (double)(K - k)) s_nonzero = k;
+      if (bi != k) {
+        double t = nu[k]; nu[k] = nu[bi]; nu[bi] = t;
+        t = nd[k]; nd[k] = nd[bi]; nd[bi] = t;
+        int ti = perm[k]; perm[k] = perm[bi]; perm[bi] = ti;
+      }
+    }
+    if (bi != k)
+      for (int r = tid; r < K; r += nt) {
+        T t = W[(i64)r * M + k];
+        W[(i64)r * M + k] = W[(i64)r * M + bi];
+        W[(i64)r * M + bi] = t;
+      }
+    __syncthreads();
+    // Householder on column k, rows k..K-1.
+    T part = 0;
+    for (int r = k + 1 + tid; r < K; r += nt) {
+      T v = W[(i64)r * M + k];
+      part += v * v;
+    }
+    T tsq = BlockReduce<T>::sum(part, red_t);
+    T c0 = W[(i64)k * M + k];
+    T tau = 0, beta = c0, scale = 0;
+    if (tsq > Tiny<T>::v()) {
+      beta = sqrt(c0 * c0 + tsq);
+      if (c0 >= T(0)) beta = -beta;
+      scale = T(1) / (c0 - beta);
+      tau = (beta - c0) / beta;
+    }
+    for (int r = k + 1 + tid; r < K; r += nt) {
+      T e = W[(i64)r * M + k] * scale;
+      ess[r] = e;
+      W[(i64)r * M + k] = e;
+    }
+    if (tid == 0) {
+      W[(i64)k * M + k] = beta;
+      double ab = fabs((double)beta);
+      if (ab > s_maxpiv) s_maxpiv = ab;
+    }
+    __syncthreads();
+    for (int j = k + 1 + tid; j < M; j += nt) {
+      if (tau != T(0)) {
+        T w = W[(i64)k * M + j];
+        for (int r = k + 1; r < K; r++) w += ess[r] * W[(i64)r * M + j];
+        w *= tau;
+        W[(i64)k * M + j] -= w;
+        for (int r = k + 1; r < K; r++) W[(i64)r * M + j] -= w * ess[r];
+      }
+      if (nu[j] != 0.) {
+        double t = fabs((double)W[(i64)k * M + j]) / nu[j];
+        t = (1. + t) * (1. - t);
+        if (t < 0.) t = 0.;
+        double t2 = t * (nu[j] / nd[j]) * (nu[j] / nd[j]);
+        if (t2 <= downdate_thr) {
+          double s = 0.;
+          for (int r = k + 1; r < K; r++) {
+            double v = (double)W[(i64)r * M + j];
+            s += v * v;
+          }
+          nd[j] = sqrt(s);
+          nu[j] = nd[j];
+        } else {
+          nu[j] *= sqrt(t);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  for (int c = tid; c < M; c += nt) perm_out[xoff[box] + c] = perm[c];
+  if (tid == 0) {
+    maxpiv_out[box] = s_maxpiv;
+    nonzero_out[box] = s_nonzero;
+  }
+}
+
+// Interpolative decomposition and the box basis.  W holds the packed CPQR
+// (row-major); Q (col-major, in/out) holds the incoming Q (identity at a
+// leaf, the children's R blocks above); R (col-major, out, zero on entry).
+template <typename T>
+__global__ void __launch_bounds__(256) k_basis_finish(
+    const i64* __restrict__ dims, const i64* __restrict__ krows, T* __restrict__ Rws, T* __restrict__ Q,
+    T* __restrict__ Rm, const i64* __restrict__ qoff, const int* __restrict__ perm_in,
+    const i64* __restrict__ xoff, const double* __restrict__ maxpiv, const int* __restrict__ nonzero,
+    double* __restrict__ pts, i64* __restrict__ ranks_out, double epi, int orth, int qin_identity) {
+  const int box = blockIdx.x;
+  const int M = (int)dims[box];
+  const int K = (int)krows[box];
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  if (M == 0 || K == 0) {
+    if (tid == 0) ranks_out[box] = 0;
+    return;
+  }
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  int* perm = reinterpret_cast<int*>(smem_raw);                          // M
+  double* sp = reinterpret_cast<double*>(smem_raw + ((4 * M + 15) / 16) * 16);  // 3M
+  T* taus = reinterpret_cast<T*>(sp + 3 * M);                            // M
+  __shared__ int s_rank;
+  __shared__ T s_red[32];
+  T* W = Rws + qoff[box];
+  T* Qb = Q + qoff[box];
+  T* Rb = Rm + qoff[box];
+  for (int c = tid; c < M; c += nt) perm[c] = perm_in[xoff[box] + c];
+  if (tid == 0) {
+    int size = K < M ? K : M;
+    int r = (int)floor(epi);
+    r = size < r ? size : r;
+    if (epi < 1.) {
+      double thr = fabs(maxpiv[box]) * epi;
+      r = 0;
+      for (int i = 0; i < nonzero[box]; i++) r += fabs((double)W[(i64)i * M + i]) > thr;
+    }
+    s_rank = r;
+  }
+  __syncthreads();
+  const int rank = s_rank;
+  if (!(0 < rank && rank < M)) {
+    // R = upper triangle of the incoming Q, Q = identity (h2matrix.cpp:114-117).
+    for (i64 e = tid; e < (i64)M * M; e += nt) {
+      int r = (int)(e % M), c = (int)(e / M);
+      Rb[e] = r <= c ? Qb[e] : T(0);
+    }
+    __syncthreads();
+    for (i64 e = tid; e < (i64)M * M; e += nt) {
+      int r = (int)(e % M), c = (int)(e / M);
+      Qb[e] = r == c ? T(1) : T(0);
+    }
+    if (tid == 0) ranks_out[box] = rank;
+    return;
+  }
+  // T = R11^{-1} R12 in place (rows 0..rank-1, columns rank..M-1).
+  for (int c = rank + tid; c < M; c += nt) {
+    for (int i = rank - 1; i >= 0; i--) {
+      T s = W[(i64)i * M + c];
+      for (int k = i + 1; k < rank; k++) s -= W[(i64)i * M + k] * W[(i64)k * M + c];
+      W[(i64)i * M + c] = s / W[(i64)i * M + i];
+    }
+  }
+  // Skeleton-first order of the box bodies.
+  double* bp = pts + 3 * xoff[box];
+  for (int e = tid; e < 3 * M; e += nt) sp[e] = bp[e];
+  __syncthreads();
+  for (int k = tid; k < M; k += nt) {
+    int p = perm[k];
+    bp[3 * k] = sp[3 * p];
+    bp[3 * k + 1] = sp[3 * p + 1];
+    bp[3 * k + 2] = sp[3 * p + 2];
+  }
+  if (!orth) {
+    // Q = P [I; T^T] padded with zero columns, R = I (h2matrix.cpp:107-112).
+    for (i64 e = tid; e < (i64)M * M; e += nt) Qb[e] = T(0);
+    __syncthreads();
+    for (i64 e = tid; e < (i64)M * rank; e += nt) {
+      int k = (int)(e % M), i = (int)(e / M);
+      T v = k < rank ? (k == i ? T(1) : T(0)) : W[(i64)i * M + k];
+      Qb[(i64)perm[k] + (i64)i * M] = v;
+    }
+    for (int i = tid; i < rank; i += nt) Rb[(i64)i * M + i] = T(1);
+    if (tid == 0) ranks_out[box] = rank;
+    return;
+  }
+  // Orthogonal mode (h2matrix.cpp:100-106).  U_ID = P [I; T^T] (M x rank)
+  // goes to R's slot as scratch, RX2 = triu(Qin) U_ID to W (col-major now).
+  for (i64 e = tid; e < (i64)M * rank; e += nt) {
+    int k = (int)(e % M), i = (int)(e / M);
+    T v = k < rank ? (k == i ? T(1) : T(0)) : W[(i64)i * M + k];
+    Rb[(i64)perm[k] + (i64)i * M] = v;
+  }
+  __syncthreads();
+  for (i64 e = tid; e < (i64)M * rank; e += nt) {
+    int p = (int)(e % M), i = (int)(e / M);
+    T s;
+    if (qin_identity) {
+      s = Rb[e];
+    } else {
+      s = 0;
+      for (int l = p; l < M; l++) s += Qb[p + (i64)l * M] * Rb[l + (i64)i * M];
+    }
+    W[e] = s;
+  }
+  __syncthreads();
+  // Householder QR of RX2 (M x rank), column-major in W.  One warp per
+  // column for the reflector application.
+  for (int k = 0; k < rank; k++) {
+    T* colk = W + (i64)k * M;
+    T part = 0;
+    for (int r = k + 1 + tid; r < M; r += nt) part += colk[r] * colk[r];
+    T tsq = BlockReduce<T>::sum(part, s_red);
+    T c0 = colk[k];
+    T tau = 0, beta = c0, scale = 0;
+    if (tsq > Tiny<T>::v()) {
+      beta = sqrt(c0 * c0 + tsq);
+      if (c0 >= T(0)) beta = -beta;
+      scale = T(1) / (c0 - beta);
+      tau = (beta - c0) / beta;
+    }
+    __syncthreads();
+    for (int r = k + 1 + tid; r < M; r += nt) colk[r] *= scale;
+    if (tid == 0) {
+      colk[k] = beta;
+      taus[k] = tau;
+    }
+    __syncthreads();
+    if (tau != T(0))
+      for (int j = k + 1 + warp; j < rank; j += nw) {
+        T* colj = W + (i64)j * M;
+        T w = 0;
+        for (int r = k + 1 + lane; r < M; r += 32) w += colk[r] * colj[r];
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        w = (w + colj[k]) * tau;
+        if (lane == 0) colj[k] -= w;
+        for (int r = k + 1 + lane; r < M; r += 32) colj[r] -= w * colk[r];
+      }
+    __syncthreads();
+  }
+  // R = triu(RX2[:rank, :rank]) (R's slot was scratch: clear first).
+  for (i64 e = tid; e < (i64)M * M; e += nt) {
+    int r = (int)(e % M), c = (int)(e / M);
+    Rb[e] = (c < rank && r <= c) ? W[r + (i64)c * M] : T(0);
+  }
+  // Q = H_0 ... H_{rank-1} applied to the identity, accumulated backwards.
+  for (i64 e = tid; e < (i64)M * M; e += nt) {
+    int r = (int)(e % M), c = (int)(e / M);
+    Qb[e] = r == c ? T(1) : T(0);
+  }
+  __syncthreads();
+  for (int k = rank - 1; k >= 0; k--) {
+    const T tau = taus[k];
+    const T* colk = W + (i64)k * M;
+    if (tau != T(0))
+      for (int j = k + warp; j < M; j += nw) {
+        T* qj = Qb + (i64)j * M;
+        T w = 0;
+        for (int r = k + 1 + lane; r < M; r += 32) w += colk[r] * qj[r];
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        w = (w + qj[k]) * tau;
+        if (lane == 0) qj[k] -= w;
+        for (int r = k + 1 + lane; r < M; r += 32) qj[r] -= w * colk[r];
+      }
+    __syncthreads();
+  }
+  if (tid == 0) ranks_out[box] = rank;
+}
+
+// ---------------------------------------------------------------- launchers
+
+template <typename T>
+cudaError_t launch_sample_tsqr(const KernelParams& kp, const double* bodies, const double* pts, const i64* xoff,
+                               const i64* dims, const int* sidx, const i64* soff, T* Rws, const i64* qoff,
+                               int nboxes, int maxM, cudaStream_t st) {
+  if (nboxes == 0) return cudaSuccess;
+  size_t smem = sizeof(T) * (32 * (size_t)maxM + 32) + sizeof(double) * 96;
+  if (smem > 220 * 1024) return cudaErrorInvalidValue;  // box too large for one tile in shared memory
+  auto fn = k_sample_tsqr<T>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  fn<<<nboxes, TS_THREADS, smem, st>>>(kp, bodies, pts, xoff, dims, sidx, soff, Rws, qoff);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_cpqr(const i64* dims, const i64* krows, T* Rws, const i64* qoff, int* perm, const i64* xoff,
+                        double* maxpiv, int* nonzero, i64 step_cap, int nboxes, int maxM, cudaStream_t st) {
+  if (nboxes == 0) return cudaSuccess;
+  size_t smem = 2 * sizeof(double) * maxM + sizeof(T) * maxM + sizeof(int) * maxM + 64;
+  auto fn = k_cpqr<T>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  fn<<<nboxes, 256, smem, st>>>(dims, krows, Rws, qoff, perm, xoff, maxpiv, nonzero, step_cap);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_basis_finish(const i64* dims, const i64* krows, T* Rws, T* Q, T* R, const i64* qoff,
+                                const int* perm, const i64* xoff, const double* maxpiv, const int* nonzero,
+                                double* pts, i64* ranks, double epi, int orth, int qin_identity, int nboxes,
+                                int maxM, cudaStream_t st) {
+  if (nboxes == 0) return cudaSuccess;
+  size_t smem = ((4 * (size_t)maxM + 15) / 16) * 16 + sizeof(double) * 3 * maxM + sizeof(T) * (maxM + 32) + 64;
+  auto fn = k_basis_finish<T>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  fn<<<nboxes, 256, smem, st>>>(dims, krows, Rws, Q, R, qoff, perm, xoff, maxpiv, nonzero, pts, ranks, epi, orth,
+                                qin_identity);
+  return cudaGetLastError();
+}
+
+#define INST(T)                                                                                                     \
+  template cudaError_t launch_sample_tsqr<T>(const KernelParams&, const double*, const double*, const i64*,       \
+                                             const i64*, const int*, const i64*, T*, const i64*, int, int,       \
+                                             cudaStream_t);                                                       \
+  template cudaError_t launch_cpqr<T>(const i64*, const i64*, T*, const i64*, int*, const i64*, double*, int*,    \
+                                      i64, int, int, cudaStream_t);                                               \
+  template cudaError_t launch_basis_finish<T>(const i64*, const i64*, T*, T*, T*, const i64*, const int*,         \
+                                              const i64*, const double*, const int*, double*, i64*, double, int,  \
+                                              int, int, int, cudaStream_t);
+INST(double)
+INST(float)
+#undef INST
+
+}  // namespace h2b

@@ -1,0 +1,186 @@
+// FP64 vector kernels of the batched GMRES (solver.cpp:144-201): dot
+// products with a deterministic two-pass reduction, classical Gram-Schmidt
+// update, normalisation, the small Hessenberg least-squares solve and
+// precision conversion for the preconditioner apply.  Every right-hand side
+// (column) runs its own independent GMRES; one launch covers all of them.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace h2b {
+
+template <typename Ts, typename Td>
+__global__ void k_convert(const Ts* __restrict__ s, Td* __restrict__ d, i64 n) {
+  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) d[i] = (Td)s[i];
+}
+template <typename Ts, typename Td>
+cudaError_t launch_convert(const Ts* src, Td* dst, i64 n, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  int grid = (int)((n + 255) / 256);
+  grid = grid > 148 * 16 ? 148 * 16 : grid;
+  k_convert<Ts, Td><<<grid, 256, 0, st>>>(src, dst, n);
+  return cudaGetLastError();
+}
+template cudaError_t launch_convert<double, float>(const double*, float*, i64, cudaStream_t);
+template cudaError_t launch_convert<float, double>(const float*, double*, i64, cudaStream_t);
+template cudaError_t launch_convert<double, double>(const double*, double*, i64, cudaStream_t);
+
+constexpr int DOT_THREADS = 256;
+constexpr i64 DOT_ROWS = 8192;  // rows per chunk
+int dots_chunks(i64 n) { return (int)((n + DOT_ROWS - 1) / DOT_ROWS); }
+
+// partial[(g * kvec + j) * nrhs + c] = sum over rows of chunk g of V_j[:, c] * w[:, c]
+__global__ void __launch_bounds__(DOT_THREADS) k_dots_partial(const double* __restrict__ V, i64 vstride, int kvec,
+                                                              const double* __restrict__ w, i64 n, int nrhs,
+                                                              double* __restrict__ partial) {
+  __shared__ double red[32];
+  const int g = blockIdx.x, c = blockIdx.y;
+  const i64 r0 = (i64)g * DOT_ROWS;
+  const i64 r1 = r0 + DOT_ROWS < n ? r0 + DOT_ROWS : n;
+  const double* wc = w + (i64)c * n;
+  for (int j = 0; j < kvec; j++) {
+    const double* vc = V + (i64)j * vstride + (i64)c * n;
+    double s = 0.;
+    for (i64 r = r0 + threadIdx.x; r < r1; r += DOT_THREADS) s += vc[r] * wc[r];
+    s = BlockReduce<double>::sum(s, red);
+    if (threadIdx.x == 0) partial[((i64)g * kvec + j) * nrhs + c] = s;
+  }
+}
+
+__global__ void k_dots_final(const double* __restrict__ partial, int nchunks, int kvec, int nrhs, double* __restrict__ out) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= kvec * nrhs) return;
+  int j = idx / nrhs, c = idx % nrhs;
+  double s = 0.;
+  for (int g = 0; g < nchunks; g++) s += partial[((i64)g * kvec + j) * nrhs + c];
+  out[(i64)c * kvec + j] = s;  // column c holds the kvec dots of rhs c
+}
+
+cudaError_t launch_dots(const double* V, i64 vstride, int kvec, const double* w, i64 n, int nrhs, double* partial,
+                        int nchunks, double* out, cudaStream_t st) {
+  dim3 grid(nchunks, nrhs);
+  k_dots_partial<<<grid, DOT_THREADS, 0, st>>>(V, vstride, kvec, w, n, nrhs, partial);
+  int tot = kvec * nrhs;
+  k_dots_final<<<(tot + 127) / 128, 128, 0, st>>>(partial, nchunks, kvec, nrhs, out);
+  return cudaGetLastError();
+}
+
+// w[:, c] += sign * sum_j V_j[:, c] * h[c * hstride + j]   (active[c] != 0)
+__global__ void k_gs_update(double* __restrict__ w, const double* __restrict__ V, i64 vstride,
+                            const double* __restrict__ h, i64 hstride, int kvec, i64 n, int nrhs, double sign,
+                            const int* __restrict__ active) {
+  const int c = blockIdx.y;
+  if (active && !active[c]) return;
+  const double* hc = h + (i64)c * hstride;
+  for (i64 r = (i64)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (i64)gridDim.x * blockDim.x) {
+    double s = 0.;
+    for (int j = 0; j < kvec; j++) s += V[(i64)j * vstride + (i64)c * n + r] * hc[j];
+    w[(i64)c * n + r] += sign * s;
+  }
+}
+
+cudaError_t launch_gs_update(double* w, const double* V, i64 vstride, const double* h, i64 hstride, int kvec, i64 n,
+                             int nrhs, double sign, const int* active, cudaStream_t st) {
+  int gx = (int)((n + 255) / 256);
+  gx = gx > 1024 ? 1024 : gx;
+  dim3 grid(gx, nrhs);
+  k_gs_update<<<grid, 256, 0, st>>>(w, V, vstride, h, hstride, kvec, n, nrhs, sign, active);
+  return cudaGetLastError();
+}
+
+// hout[c * hstride] = sqrt(nrm2[c]); vout[:, c] = w[:, c] / hout (zero when the norm is zero)
+__global__ void k_scale_by_norm(const double* __restrict__ w, double* __restrict__ vout, const double* __restrict__ nrm2,
+                                double* __restrict__ hout, i64 hstride, i64 n, int nrhs) {
+  const int c = blockIdx.y;
+  const double nv = sqrt(nrm2[c]);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && hout) hout[(i64)c * hstride] = nv;
+  const double inv = 1. / nv;
+  for (i64 r = (i64)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (i64)gridDim.x * blockDim.x)
+    vout[(i64)c * n + r] = w[(i64)c * n + r] * inv;
+}
+
+cudaError_t launch_scale_by_norm(const double* w, double* vout, const double* nrm2, double* hout, i64 hstride, i64 n,
+                                 int nrhs, cudaStream_t st) {
+  int gx = (int)((n + 255) / 256);
+  gx = gx > 1024 ? 1024 : gx;
+  dim3 grid(gx, nrhs);
+  k_scale_by_norm<<<grid, 256, 0, st>>>(w, vout, nrm2, hout, hstride, n, nrhs);
+  return cudaGetLastError();
+}
+
+// min || beta e1 - H y || for each rhs (H: ld x inner column-major per rhs,
+// stride ld * inner); Householder QR in one thread per rhs (the reference
+// solves the same problem with HouseholderQR::solve, solver.cpp:190).
+__global__ void k_gmres_ls(const double* __restrict__ Hall, int ld, int inner, const double* __restrict__ beta,
+                           double* __restrict__ yall, int nrhs) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nrhs) return;
+  double H[17 * 16];
+  double s[17];
+  if (ld > 17 || inner > 16) return;
+  const double* Hc = Hall + (i64)c * ld * inner;
+  for (int i = 0; i < ld * inner; i++) H[i] = Hc[i];
+  for (int i = 0; i < ld; i++) s[i] = 0.;
+  s[0] = beta[c];
+  for (int k = 0; k < inner; k++) {
+    double nrm = 0.;
+    for (int r = k; r < ld; r++) nrm += H[r + k * ld] * H[r + k * ld];
+    nrm = sqrt(nrm);
+    if (nrm == 0.) continue;
+    double a = H[k + k * ld];
+    double bta = a >= 0. ? -nrm : nrm;
+    double v[17];
+    for (int r = 0; r < ld; r++) v[r] = 0.;
+    v[k] = a - bta;
+    for (int r = k + 1; r < ld; r++) v[r] = H[r + k * ld];
+    double vn = 0.;
+    for (int r = k; r < ld; r++) vn += v[r] * v[r];
+    if (vn == 0.) continue;
+    for (int j = k; j < inner; j++) {
+      double d = 0.;
+      for (int r = k; r < ld; r++) d += v[r] * H[r + j * ld];
+      d = 2. * d / vn;
+      for (int r = k; r < ld; r++) H[r + j * ld] -= d * v[r];
+    }
+    double d = 0.;
+    for (int r = k; r < ld; r++) d += v[r] * s[r];
+    d = 2. * d / vn;
+    for (int r = k; r < ld; r++) s[r] -= d * v[r];
+  }
+  double* y = yall + (i64)c * inner;
+  for (int i = inner - 1; i >= 0; i--) {
+    double t = s[i];
+    for (int j = i + 1; j < inner; j++) t -= H[i + j * ld] * y[j];
+    y[i] = H[i + i * ld] != 0. ? t / H[i + i * ld] : 0.;
+  }
+}
+
+cudaError_t launch_gmres_ls(const double* H, int ld, int inner, const double* beta, double* y, int nrhs,
+                            cudaStream_t st) {
+  k_gmres_ls<<<(nrhs + 31) / 32, 32, 0, st>>>(H, ld, inner, beta, y, nrhs);
+  return cudaGetLastError();
+}
+
+// y = a * y + b * x
+__global__ void k_axpby(double* __restrict__ y, const double* __restrict__ x, double a, double b, i64 n) {
+  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
+    y[i] = a * y[i] + b * x[i];
+}
+cudaError_t launch_axpby(double* y, const double* x, double a, double b, i64 n, cudaStream_t st) {
+  int grid = (int)((n + 255) / 256);
+  grid = grid > 148 * 16 ? 148 * 16 : grid;
+  k_axpby<<<grid, 256, 0, st>>>(y, x, a, b, n);
+  return cudaGetLastError();
+}
+
+__global__ void k_resid_finish(const double* __restrict__ nrm2, const double* __restrict__ normb, double* __restrict__ resid,
+                               int nrhs) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < nrhs) resid[c] = sqrt(nrm2[c]) / normb[c];
+}
+cudaError_t launch_residual_norm_finish(const double* nrm2, const double* normb, double* resid, int nrhs,
+                                        cudaStream_t st) {
+  k_resid_finish<<<(nrhs + 127) / 128, 128, 0, st>>>(nrm2, normb, resid, nrhs);
+  return cudaGetLastError();
+}
+
+}  // namespace h2b

@@ -1,0 +1,110 @@
+// Launch interfaces of the device kernels (host-callable, no torch types).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace h2b {
+
+// ---------------------------------------------------------------- gen
+struct GenTask {
+  const double* bi;  // m bodies, xyz interleaved
+  const double* bj;  // n bodies
+  int m, n;
+  i64 out_off;  // element offset of the column-major m x n output
+  i64 ld;
+};
+template <typename T>
+cudaError_t launch_gen_blocks(const KernelParams& kp, const GenTask* d_tasks, int ntasks, int chunks, T* out,
+                              cudaStream_t st);
+cudaError_t launch_dense_matvec(const KernelParams& kp, const double* bodies, i64 n, const double* X, i64 ldx,
+                                double* Y, i64 ldy, int nrhs, cudaStream_t st);
+
+// ---------------------------------------------------------------- basis
+template <typename T>
+cudaError_t launch_sample_tsqr(const KernelParams& kp, const double* bodies, const double* pts, const i64* xoff,
+                               const i64* dims, const int* sidx, const i64* soff, T* Rws, const i64* qoff,
+                               int nboxes, int maxM, cudaStream_t st);
+template <typename T>
+cudaError_t launch_cpqr(const i64* dims, const i64* krows, T* Rws, const i64* qoff, int* perm, const i64* xoff,
+                        double* maxpiv, int* nonzero, i64 step_cap, int nboxes, int maxM, cudaStream_t st);
+template <typename T>
+cudaError_t launch_basis_finish(const i64* dims, const i64* krows, T* Rws, T* Q, T* R, const i64* qoff,
+                                const int* perm, const i64* xoff, const double* maxpiv, const int* nonzero,
+                                double* pts, i64* ranks, double epi, int orth, int qin_identity, int nboxes,
+                                int maxM, cudaStream_t st);
+
+// ---------------------------------------------------------------- gemm
+// C_task = beta * C_task + sum_{e in task} alpha_e * op(A_e) * op(B_e)
+template <typename T>
+struct GemmEntry {
+  const T* A;
+  const T* B;
+  i64 lda, ldb;
+  int k;
+  int opA, opB;  // 0: as stored (column-major), 1: transposed
+  T alpha;
+};
+template <typename T>
+struct GemmTask {
+  T* C;
+  i64 ldc;
+  int m, n;
+  int e0, e1;
+  T beta;
+};
+struct TileRef {
+  int task, tm, tn;
+};
+enum GemmShape { GEMM_BIG = 0, GEMM_SKINNY = 1 };
+template <typename T>
+cudaError_t launch_seg_gemm(int shape, const GemmTask<T>* d_tasks, const GemmEntry<T>* d_ents, const TileRef* d_tiles,
+                            int ntiles, cudaStream_t st);
+int gemm_tile_m(int shape);
+int gemm_tile_n(int shape);
+
+template <typename T>
+struct CopyEntry {
+  const T* src;
+  T* dst;
+  i64 lds, ldd;
+  int m, n;
+  int trans;  // dst(r, c) = trans ? src(c, r) : src(r, c)
+};
+template <typename T>
+cudaError_t launch_batched_copy(const CopyEntry<T>* d_ents, int n, cudaStream_t st);
+template <typename T>
+cudaError_t launch_set_identity(T* base, const i64* qoff, const i64* dims, int nboxes, cudaStream_t st);
+
+// ---------------------------------------------------------------- lu
+template <typename T>
+struct LuTask {
+  T* A;      // n x n column-major, factored in place
+  i64 lda;
+  int n;
+  T* invT;   // receives A^{-1} transposed (column-major, ld = ldinv)
+  i64 ldinv;
+  int* ipiv;  // n
+  int* info;  // 1 when |det| <= DBL_MIN (h2matrix.cpp:441)
+};
+template <typename T>
+cudaError_t launch_lu_inverse(const LuTask<T>* d_tasks, int ntasks, cudaStream_t st);
+
+// ---------------------------------------------------------------- vectors
+template <typename Ts, typename Td>
+cudaError_t launch_convert(const Ts* src, Td* dst, i64 n, cudaStream_t st);
+cudaError_t launch_dots(const double* V, i64 vstride, int kvec, const double* w, i64 n, int nrhs, double* partial,
+                        int nchunks, double* out, cudaStream_t st);
+int dots_chunks(i64 n);
+cudaError_t launch_gs_update(double* w, const double* V, i64 vstride, const double* h, i64 hstride, int kvec, i64 n,
+                             int nrhs, double sign, const int* active, cudaStream_t st);
+cudaError_t launch_scale_by_norm(const double* w, double* vout, const double* nrm2, double* hout, i64 hstride,
+                                 i64 n, int nrhs, cudaStream_t st);
+cudaError_t launch_gmres_ls(const double* H, int ld, int inner, const double* beta, double* y, int nrhs,
+                            cudaStream_t st);
+cudaError_t launch_axpby(double* y, const double* x, double a, double b, i64 n, cudaStream_t st);
+cudaError_t launch_residual_norm_finish(const double* nrm2, const double* normb, double* resid, int nrhs,
+                                        cudaStream_t st);
+
+}  // namespace h2b

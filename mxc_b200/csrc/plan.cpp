@@ -1,0 +1,134 @@
+// Host plan layer: the reference's geometry / tree / list rules restated.
+#include "plan.hpp"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <random>
+
+namespace h2b {
+
+i64 PairCSR::lookup(i64 i, i64 j) const {
+  if (i < 0 || (i64)row.size() <= i + 1) return -1;
+  for (i64 k = row[i]; k < row[i + 1]; k++)
+    if (col[k] == j) return k;
+  return -1;
+}
+
+void uniform_unit_cube_rnd(double* bodies, i64 n, double diameter, i64 dim, unsigned seed) {
+  // test_funcs.hpp:31-41: one generator, coordinates drawn in body order.
+  std::mt19937 gen(seed);
+  std::uniform_real_distribution<double> dist(0., diameter);
+  for (i64 i = 0; i < n; i++)
+    for (int k = 0; k < 3; k++) bodies[3 * i + k] = k < dim ? dist(gen) : 0.;
+}
+
+void uniform_rhs(double* x, i64 n) {
+  std::mt19937_64 gen;
+  std::uniform_real_distribution<double> dist(0., 1.);
+  for (i64 i = 0; i < n; i++) x[i] = dist(gen);
+}
+
+// Centre and half-extent of a body range, build_tree.cpp:8-22.
+static void bounds(const double* b, i64 n, double R[3], double C[3]) {
+  for (int k = 0; k < 3; k++) {
+    double lo = b[k], hi = b[k];
+    for (i64 i = 1; i < n; i++) {
+      double v = b[3 * i + k];
+      lo = v < lo ? v : lo;
+      hi = hi < v ? v : hi;
+    }
+    C[k] = (lo + hi) * 0.5;
+    R[k] = (lo == hi && lo == 0.) ? 0. : ((hi - lo) * 0.5 + 1.e-8);
+  }
+}
+
+void build_binary_tree(Cell* cells, double* bodies, i64 nbodies, i64 levels) {
+  cells[0].body[0] = 0;
+  cells[0].body[1] = nbodies;
+  bounds(bodies, nbodies, cells[0].R, cells[0].C);
+  i64 nleaf = (i64)1 << levels;
+  typedef std::array<double, 3> P3;
+  for (i64 i = 0; i + 1 < nleaf; i++) {
+    Cell& ci = cells[i];
+    int sdim = 0;  // first maximum of the half extents
+    for (int k = 1; k < 3; k++)
+      if (ci.R[sdim] < ci.R[k]) sdim = k;
+    i64 b0 = ci.body[0], b1 = ci.body[1];
+    P3* first = reinterpret_cast<P3*>(bodies + 3 * b0);
+    P3* last = reinterpret_cast<P3*>(bodies + 3 * b1);
+    // Same comparator and the same std::sort as the reference, so equal
+    // keys (which random inputs do not produce) would also land the same.
+    std::sort(first, last, [=](P3& a, P3& b) { return a[sdim] < b[sdim]; });
+    i64 c0 = 2 * i + 1;
+    ci.child[0] = c0;
+    ci.child[1] = c0 + 2;
+    i64 mid = b0 + (b1 - b0) / 2;
+    cells[c0].body[0] = b0;
+    cells[c0].body[1] = mid;
+    cells[c0 + 1].body[0] = mid;
+    cells[c0 + 1].body[1] = b1;
+    bounds(bodies + 3 * b0, mid - b0, cells[c0].R, cells[c0].C);
+    bounds(bodies + 3 * mid, b1 - mid, cells[c0 + 1].R, cells[c0 + 1].C);
+  }
+}
+
+PairCSR build_pair_csr(char kind, const std::vector<Cell>& cells, double theta) {
+  // Dual-tree descent from (0, 0), taken one tree level at a time; the
+  // emitted pairs are sorted afterwards exactly as CSR::CSR sorts them.
+  std::vector<std::pair<i64, i64>> out, cur{{0, 0}}, next;
+  bool want_far = kind == 'F' || kind == 'f';
+  while (!cur.empty()) {
+    next.clear();
+    for (auto& p : cur) {
+      const Cell& a = cells[p.first];
+      const Cell& b = cells[p.second];
+      double dC = 0., dR1 = 0., dR2 = 0.;
+      for (int k = 0; k < 3; k++) {
+        double d = a.C[k] - b.C[k];
+        dC = dC + d * d;
+      }
+      for (int k = 0; k < 3; k++) dR1 = dR1 + a.R[k] * a.R[k];
+      for (int k = 0; k < 3; k++) dR2 = dR2 + b.R[k] * b.R[k];
+      bool admis = dC > theta * (dR1 + dR2);
+      if (admis == want_far) out.push_back(p);
+      if (!admis && a.child[0] >= 0 && b.child[0] >= 0)
+        for (i64 k = a.child[0]; k < a.child[1]; k++)
+          for (i64 l = b.child[0]; l < b.child[1]; l++) next.emplace_back(k, l);
+    }
+    cur.swap(next);
+  }
+  std::sort(out.begin(), out.end());
+  PairCSR csr;
+  i64 nc = (i64)cells.size();
+  csr.row.assign(nc + 1, 0);
+  csr.col.resize(out.size());
+  for (size_t k = 0; k < out.size(); k++) {
+    csr.row[out[k].first + 1]++;
+    csr.col[k] = out[k].second;
+  }
+  for (i64 i = 0; i < nc; i++) csr.row[i + 1] += csr.row[i];
+  return csr;
+}
+
+void sample_far_list(const std::vector<std::pair<i64, i64>>& ranges, i64 samples, std::vector<int>& out) {
+  i64 total = 0;
+  for (auto& r : ranges) total += r.second - r.first;
+  out.clear();
+  if (total == 0) return;
+  i64 keep = (samples <= 0 || samples >= total) ? total : samples;
+  out.resize(keep);
+  // Walk the concatenated list once; targets are increasing.
+  size_t ri = 0;
+  i64 base = 0;
+  for (i64 j = 0; j < keep; j++) {
+    i64 t = (keep == total) ? j : (j * total) / samples;
+    while (t >= base + (ranges[ri].second - ranges[ri].first)) {
+      base += ranges[ri].second - ranges[ri].first;
+      ri++;
+    }
+    out[j] = (int)(ranges[ri].first + (t - base));
+  }
+}
+
+}  // namespace h2b

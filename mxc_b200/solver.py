@@ -1,0 +1,261 @@
+"""Python mirror of the reference's solver interface (solver.hpp:11-47).
+
+``H2MatrixSolver`` keeps the reference's method names and argument meaning:
+``matVecMul``, ``factorizeM``, ``solvePrecondition``, ``solveGMRES`` and the
+static ``solveRelErr``; every vector is in tree-sorted body order and the
+operations work in place.  All numerical work runs in libmxcb200.so on the
+GPU; this module only moves arrays across the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib as L
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Tree:
+    """Cells of buildBinaryTree (build_tree.cpp:93-125) as flat arrays."""
+
+    def __init__(self, levels: int, child: np.ndarray, body: np.ndarray, R: np.ndarray, Cc: np.ndarray):
+        self.levels = levels
+        self.child = child
+        self.body = body
+        self.R = R
+        self.C = Cc
+
+    @property
+    def ncells(self) -> int:
+        return self.child.shape[0]
+
+
+def uniform_unit_cube_rnd(n: int, seed: int, diameter: float = 1.0, dim: int = 3) -> np.ndarray:
+    """test_funcs.hpp:31-41 (std::mt19937, run in the library's host code)."""
+    b = np.empty((n, 3), dtype=np.float64)
+    L.check(L.lib().h2_uniform_unit_cube_rnd(_ptr(b), n, diameter, dim, seed), "h2_uniform_unit_cube_rnd")
+    return b
+
+
+def uniform_rhs(n: int) -> np.ndarray:
+    """main.cpp:358-361 (default-seeded std::mt19937_64, uniform[0,1))."""
+    x = np.empty(n, dtype=np.float64)
+    L.check(L.lib().h2_uniform_rhs(_ptr(x), n), "h2_uniform_rhs")
+    return x
+
+
+def levels_for(n: int, leaf: int) -> int:
+    return int(L.lib().h2_levels_for(n, leaf))
+
+
+def build_tree(bodies: np.ndarray, levels: int) -> Tree:
+    """buildBinaryTree: sorts ``bodies`` (n x 3, C-contiguous float64) in place."""
+    assert bodies.dtype == np.float64 and bodies.flags.c_contiguous and bodies.shape[1] == 3
+    nc = (2 << levels) - 1
+    child = np.empty((nc, 2), dtype=np.int64)
+    body = np.empty((nc, 2), dtype=np.int64)
+    R = np.empty((nc, 3))
+    Cc = np.empty((nc, 3))
+    L.check(L.lib().h2_build_tree(_ptr(bodies), bodies.shape[0], levels, _ptr(child), _ptr(body), _ptr(R),
+                                  _ptr(Cc)), "h2_build_tree")
+    return Tree(levels, child, body, R, Cc)
+
+
+def pair_csr(kind: str, tree: Tree, theta: float):
+    """CSR::CSR (build_tree.cpp:67-84): (RowIndex, ColIndex) of the near or far pairs."""
+    row = np.zeros(tree.ncells + 1, dtype=np.int64)
+    nnz = C.c_int64()
+    args = (kind.encode(), tree.ncells, _ptr(tree.child), _ptr(tree.body), _ptr(tree.R), _ptr(tree.C), theta)
+    L.check(L.lib().h2_pair_csr(*args, _ptr(row), None, 0, C.byref(nnz)), "h2_pair_csr")
+    col = np.zeros(nnz.value, dtype=np.int64)
+    L.check(L.lib().h2_pair_csr(*args, _ptr(row), _ptr(col), nnz.value, C.byref(nnz)), "h2_pair_csr")
+    return row, col
+
+
+class Handle:
+    """deviceHandle (gpu_handles.cuh:10-15): one stream on one device."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        L.check(L.lib().h2dev_handle_create(device, C.byref(h)), "h2dev_handle_create")
+        self.h = h
+
+    def synchronize(self):
+        L.check(L.lib().h2dev_handle_synchronize(self.h), "h2dev_handle_synchronize")
+
+    def close(self):
+        if self.h:
+            L.lib().h2dev_handle_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Kernel:
+    """Laplace3D(s) / Yukawa3D(s, alpha) of kernel.hpp:28-50."""
+
+    def __init__(self, kind: int = L.KERNEL_LAPLACE, singularity: float = 1.0, alpha: float = 1.0):
+        self.kind = kind
+        self.singularity = singularity
+        self.alpha = alpha
+
+
+def Laplace3D(s: float = 1.0) -> Kernel:
+    return Kernel(L.KERNEL_LAPLACE, s, 0.0)
+
+
+def Yukawa3D(s: float = 1.0, a: float = 1.0) -> Kernel:
+    return Kernel(L.KERNEL_YUKAWA, s, a)
+
+
+def _as_cols(X: np.ndarray):
+    """(n,) or (n, nrhs) float64 -> Fortran-ordered 2-D view + nrhs + ld."""
+    if X.ndim == 1:
+        return X.reshape(-1, 1, order="F"), 1, X.shape[0]
+    assert X.flags.f_contiguous, "multi-RHS arrays must be column-major (order='F')"
+    return X, X.shape[1], X.shape[0]
+
+
+class H2MatrixSolver:
+    """H2MatrixSolver (solver.hpp:11-47) on one B200.
+
+    eps > 0: operator (ID basis, relative threshold eps); eps == 0:
+    fixed-rank orthogonal-basis preconditioner.  ``samples`` caps each box's
+    far list (<= 0: every far body, as the reference).  ``precision``:
+    FP64 or FP32 storage and arithmetic of this matrix.
+    """
+
+    def __init__(self, handle: Handle, kernel: Kernel, eps: float, rank: int, leveled_rank: int, tree: Tree,
+                 theta: float, bodies: np.ndarray, samples: int = 0, precision: int = L.FP64):
+        s = C.c_void_p()
+        self.handle = handle
+        self.levels = tree.levels
+        n = bodies.shape[0]
+        L.check(L.lib().h2dev_solver_create(handle.h, kernel.kind, kernel.singularity, kernel.alpha, eps, rank,
+                                            leveled_rank, tree.ncells, _ptr(tree.child), _ptr(tree.body),
+                                            _ptr(tree.R), _ptr(tree.C), theta, _ptr(bodies), n, tree.levels,
+                                            samples, precision, C.byref(s)), "h2dev_solver_create")
+        self.s = s
+        self.local_bodies = (0, n)
+        self.resid = None
+        self.iters = 0
+        self.info = None
+
+    # ------------------------------------------------------------ reference API
+    def matVecMul(self, X: np.ndarray) -> None:
+        A, nrhs, ld = _as_cols(X)
+        L.check(L.lib().h2dev_matvec(self.s, nrhs, _ptr(A), ld), "h2dev_matvec")
+
+    def factorizeM(self) -> list:
+        info = np.zeros(self.levels + 1, dtype=np.int32)
+        rc = L.lib().h2dev_factorize(self.s, _ptr(info))
+        L.check(rc, "h2dev_factorize", allow=(L.H2DEV_ERR_SINGULAR,))
+        self.info = [int(v) for v in info]
+        for lvl in range(self.levels, -1, -1):
+            if self.info[lvl]:
+                print("singularity detected at level %d." % lvl)
+        return self.info
+
+    def solvePrecondition(self, X: np.ndarray) -> None:
+        A, nrhs, ld = _as_cols(X)
+        L.check(L.lib().h2dev_solve_precondition(self.s, nrhs, _ptr(A), ld), "h2dev_solve_precondition")
+
+    def solveGMRES(self, tol: float, M: "H2MatrixSolver", X: np.ndarray, B: np.ndarray, inner_iters: int,
+                   outer_iters: int, early_exit: bool = False) -> int:
+        Xa, nrhs, ld = _as_cols(X)
+        Ba, nb, ldb = _as_cols(np.asarray(B, dtype=np.float64, order="F"))
+        assert nb == nrhs and ldb == ld
+        resid = np.zeros((outer_iters + 1, nrhs), order="F")
+        iters = np.zeros(nrhs, dtype=np.int64)
+        rc = L.lib().h2dev_solve_gmres(self.s, M.s, tol, nrhs, _ptr(Xa), _ptr(Ba), ld, inner_iters, outer_iters,
+                                       1 if early_exit else 0, _ptr(resid), _ptr(iters))
+        L.check(rc, "h2dev_solve_gmres", allow=(L.H2DEV_ERR_NOCONV,))
+        self.resid = resid if nrhs > 1 else resid[:, 0]
+        self.iters = iters if nrhs > 1 else int(iters[0])
+        return rc
+
+    @staticmethod
+    def solveRelErr(X: np.ndarray, ref: np.ndarray) -> float:
+        """solver.cpp:276-285 (host-side reduction of two vectors)."""
+        d = np.asarray(X) - np.asarray(ref)
+        return math.sqrt(float(np.sum(d * d)) / float(np.sum(np.asarray(ref) ** 2)))
+
+    # ------------------------------------------------------------ device-pointer API
+    def matvec_device(self, ptr: int, nrhs: int, ld: int) -> None:
+        L.check(L.lib().h2dev_matvec_device(self.s, nrhs, C.c_void_p(ptr), ld), "h2dev_matvec_device")
+
+    def precondition_device(self, ptr: int, nrhs: int, ld: int) -> None:
+        L.check(L.lib().h2dev_solve_precondition_device(self.s, nrhs, C.c_void_p(ptr), ld),
+                "h2dev_solve_precondition_device")
+
+    def gmres_device(self, M: "H2MatrixSolver", tol: float, xptr: int, bptr: int, nrhs: int, ld: int, inner: int,
+                     outer: int, early_exit: bool = False):
+        resid = np.zeros((outer + 1, nrhs), order="F")
+        iters = np.zeros(nrhs, dtype=np.int64)
+        rc = L.lib().h2dev_solve_gmres_device(self.s, M.s, tol, nrhs, C.c_void_p(xptr), C.c_void_p(bptr), ld,
+                                              inner, outer, 1 if early_exit else 0, _ptr(resid), _ptr(iters))
+        L.check(rc, "h2dev_solve_gmres_device", allow=(L.H2DEV_ERR_NOCONV,))
+        return rc, resid, iters
+
+    # ------------------------------------------------------------ inspection
+    def shape(self):
+        lv = C.c_int64()
+        n = C.c_int64()
+        L.check(L.lib().h2dev_solver_shape(self.s, C.byref(lv), C.byref(n)), "h2dev_solver_shape")
+        return lv.value, n.value
+
+    def level_dims(self, level: int):
+        nodes = 1 << level
+        d = np.zeros(nodes, dtype=np.int64)
+        r = np.zeros(nodes, dtype=np.int64)
+        L.check(L.lib().h2dev_solver_level_dims(self.s, level, _ptr(d), _ptr(r)), "h2dev_solver_level_dims")
+        return d, r
+
+    def export(self, level: int, what: int) -> np.ndarray:
+        cnt = C.c_int64()
+        L.check(L.lib().h2dev_solver_export_size(self.s, level, what, C.byref(cnt)), "export_size")
+        out = np.zeros(cnt.value)
+        if cnt.value:
+            L.check(L.lib().h2dev_solver_export(self.s, level, what, _ptr(out)), "export")
+        return out
+
+    def close(self):
+        if getattr(self, "s", None):
+            L.lib().h2dev_solver_destroy(self.s)
+            self.s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def gen_block(handle: Handle, kernel: Kernel, bi: np.ndarray, bj: np.ndarray) -> np.ndarray:
+    """gen_matrix (kernel.cpp:71-85) on the device; returns an (m, n) array."""
+    bi = np.ascontiguousarray(bi, dtype=np.float64)
+    bj = np.ascontiguousarray(bj, dtype=np.float64)
+    m, n = bi.shape[0], bj.shape[0]
+    out = np.zeros((m, n), order="F")
+    L.check(L.lib().h2dev_gen_block(handle.h, kernel.kind, kernel.singularity, kernel.alpha, _ptr(bi), m, _ptr(bj),
+                                    n, _ptr(out)), "h2dev_gen_block")
+    return out
+
+
+def dense_matvec(handle: Handle, kernel: Kernel, bodies: np.ndarray, X: np.ndarray) -> np.ndarray:
+    """Y = A_dense X (FP64, matrix-free on the device)."""
+    bodies = np.ascontiguousarray(bodies, dtype=np.float64)
+    Xa, nrhs, ld = _as_cols(np.asarray(X, dtype=np.float64, order="F"))
+    Y = np.zeros_like(Xa, order="F")
+    L.check(L.lib().h2dev_dense_matvec(handle.h, kernel.kind, kernel.singularity, kernel.alpha, _ptr(bodies),
+                                       bodies.shape[0], nrhs, _ptr(Xa), _ptr(Y), ld), "h2dev_dense_matvec")
+    return Y.reshape(X.shape) if np.asarray(X).ndim == 1 else Y

@@ -1,0 +1,266 @@
+"""GPU parity of the CUDA path (through the C ABI) against the FP64 oracle.
+
+Tolerances: kernel blocks are bit-exact (Laplace) or within 4 ulp (Yukawa);
+everything downstream of a QR is compared in relative 2-norm with bounds
+stated per test.  The preconditioned system is ill-conditioned (the dense
+matrix has condition ~1e5-1e6 at these sizes), which is what the looser
+substitution bounds reflect.
+"""
+import numpy as np
+import pytest
+
+import h2_oracle as O
+import mxc_b200 as m
+from conftest import golden_cases, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
+
+
+def problem(N, leaf=256, seed=999):
+    L = m.levels_for(N, leaf)
+    b = m.uniform_unit_cube_rnd(N, seed)
+    t = m.build_tree(b, L)
+    bo = O.uniform_unit_cube_rnd(N, seed)
+    cells = O.build_binary_tree(bo, L)
+    assert np.array_equal(b, bo)
+    return b, t, cells, L
+
+
+# ---------------------------------------------------------------- kernels
+
+def test_gen_block_bitexact_vs_reference(handle):
+    g = load_golden(golden_cases()[0])
+    b = gold_b = g["bodies"]
+    ij = g["probe_ij"]
+    lap = m.Laplace3D(1.0)
+    full = m.gen_block(handle, lap, b[:64], b)
+    vals = np.array([full[i, j] for i, j in ij])
+    assert np.array_equal(vals, g["probe_laplace"])
+    yuk = m.Yukawa3D(1.0, 1.0)
+    fy = m.gen_block(handle, yuk, b[:64], gold_b)
+    vy = np.array([fy[i, j] for i, j in ij])
+    np.testing.assert_allclose(vy, g["probe_yukawa"], rtol=1e-15, atol=0)
+
+
+def test_gen_block_matches_oracle_ragged(handle):
+    rng = np.random.default_rng(1)
+    bi = rng.random((313, 3))
+    bj = np.vstack([rng.random((17, 3)), bi[:5]])  # coincident bodies hit the diagonal value
+    for k, ok in ((m.Laplace3D(2.0), O.Kernel(O.LAPLACE, 2.0)), (m.Yukawa3D(1.0, 0.7), O.Kernel(O.YUKAWA, 1.0, 0.7))):
+        got = m.gen_block(handle, k, bi, bj)
+        exp = O.gen_matrix(ok, bi, bj)
+        if k.kind == m.KERNEL_LAPLACE:
+            assert np.array_equal(got, exp)
+        else:
+            np.testing.assert_allclose(got, exp, rtol=1e-15)
+    assert m.gen_block(handle, m.Laplace3D(), bi[:0], bj).shape == (0, 22)
+
+
+def test_dense_matvec_vs_oracle(handle):
+    N = 3000
+    b = m.uniform_unit_cube_rnd(N, 5)
+    X = np.asfortranarray(np.random.default_rng(2).random((N, 3)))
+    got = m.dense_matvec(handle, m.Laplace3D(), b, X)
+    exp = O.dense_matvec(O.Kernel(), b, X)
+    assert rel(got, exp) < 1e-13
+    x1 = X[:, 0].copy()
+    assert rel(m.dense_matvec(handle, m.Laplace3D(), b, x1), exp[:, 0]) < 1e-13
+
+
+# ---------------------------------------------------------------- H^2 operator
+
+@pytest.fixture(scope="module")
+def op2048(handle):
+    N = 2048
+    b, t, cells, L = problem(N)
+    k = m.Laplace3D()
+    A = m.H2MatrixSolver(handle, k, 1e-10, 100, 0, t, 2.0, b, samples=2000)
+    Ao = O.H2MatrixSolver(O.Kernel(), 1e-10, 100, 0, cells, 2.0, O.uniform_unit_cube_rnd(N, 999) if False else b.copy(), L, 2000)
+    return A, Ao, b, t, cells, L
+
+
+def test_operator_ranks_match_oracle(op2048):
+    A, Ao, b, t, cells, L = op2048
+    for lvl in range(L + 1):
+        d, r = A.level_dims(lvl)
+        assert np.array_equal(d, Ao.A[lvl].Dims), lvl
+        diff = np.abs(r - Ao.A[lvl].DimsLr)
+        assert diff.max() <= 1 and (diff > 0).sum() <= max(1, len(r) // 8), (lvl, r, Ao.A[lvl].DimsLr)
+
+
+def test_operator_matvec_vs_oracle_and_dense(op2048, handle):
+    A, Ao, b, t, cells, L = op2048
+    x = m.uniform_rhs(b.shape[0])
+    y = x.copy()
+    A.matVecMul(y)
+    yo = Ao.matvec(x)
+    yd = m.dense_matvec(handle, m.Laplace3D(), b, x)
+    assert rel(y, yo) < 1e-10
+    assert rel(y, yd) < 1e-10
+
+
+def test_operator_matvec_multi_rhs(op2048):
+    A, Ao, b, t, cells, L = op2048
+    N = b.shape[0]
+    X = np.asfortranarray(np.random.default_rng(3).random((N, 5)))
+    Y = X.copy(order="F")
+    A.matVecMul(Y)
+    for c in range(5):
+        y1 = X[:, c].copy()
+        A.matVecMul(y1)
+        assert rel(Y[:, c], y1) < 1e-14
+
+
+# ---------------------------------------------------------------- preconditioner
+
+@pytest.fixture(scope="module")
+def pre2048(handle):
+    N = 2048
+    b, t, cells, L = problem(N)
+    M = m.H2MatrixSolver(handle, m.Laplace3D(), 0.0, 100, 0, t, 2.0, b, samples=2000)
+    Mo = O.H2MatrixSolver(O.Kernel(), 0.0, 100, 0, cells, 2.0, b.copy(), L, 2000)
+    return M, Mo, b, t, cells, L
+
+
+def test_precond_basis_matches_oracle(pre2048):
+    M, Mo, b, t, cells, L = pre2048
+    lvl = L
+    S = M.export(lvl, m._lib.EXPORT_S).reshape(-1, 3)
+    So = np.vstack(Mo.A[lvl].S)
+    assert np.array_equal(S, So), "skeleton order differs"
+    Q = M.export(lvl, m._lib.EXPORT_Q)
+    Qo = np.concatenate([q.ravel(order="F") for q in Mo.A[lvl].Q])
+    # Columns of the orthogonal completion are unique up to rounding (same
+    # Householder convention on both sides).
+    assert rel(Q, Qo) < 1e-9
+    C = M.export(lvl, m._lib.EXPORT_C)
+    Co = np.concatenate([c.ravel(order="F") for c in Mo.A[lvl].C]) if Mo.A[lvl].C else np.zeros(0)
+    assert rel(C, Co) < 1e-9
+
+
+def test_precond_factor_and_substitution(pre2048):
+    M, Mo, b, t, cells, L = pre2048
+    info = M.factorizeM()
+    info_o = Mo.factorize()
+    assert info == info_o
+    N = b.shape[0]
+    x = m.uniform_rhs(N)
+    z = x.copy()
+    M.solvePrecondition(z)
+    zo = Mo.solve_precondition(x)
+    assert rel(z, zo) < 1e-7
+
+
+def test_precond_before_factorize_is_an_error(handle):
+    b, t, cells, L = problem(1024, leaf=128)
+    M = m.H2MatrixSolver(handle, m.Laplace3D(), 0.0, 64, 0, t, 2.0, b, samples=500)
+    with pytest.raises(m.H2DevError) as e:
+        M.solvePrecondition(np.ones(1024))
+    assert e.value.code == m._lib.H2DEV_ERR_STATE
+
+
+# ---------------------------------------------------------------- GMRES
+
+def test_gmres_fp64_matches_oracle_and_dense(op2048, pre2048, handle):
+    A, Ao, b, t, cells, L = op2048
+    M, Mo, *_ = pre2048
+    if M.info is None:
+        M.factorizeM()
+        Mo.factorize()
+    N = b.shape[0]
+    xt = m.uniform_rhs(N)
+    B = m.dense_matvec(handle, m.Laplace3D(), b, xt)
+    X = np.zeros(N)
+    rc = A.solveGMRES(1e-10, M, X, B, 10, 50)
+    assert rc == 0
+    xo, reso, ito = Ao.solve_gmres(1e-10, Mo, np.zeros(N), B, 10, 50)
+    assert A.iters == ito
+    assert A.resid[A.iters] < 1e-10
+    np.testing.assert_allclose(A.resid[:ito + 1], reso, rtol=1e-3, atol=1e-13)
+    assert rel(X, xo) < 1e-8
+    r = B - m.dense_matvec(handle, m.Laplace3D(), b, X)
+    assert np.linalg.norm(r) / np.linalg.norm(B) < 1e-10
+
+
+def test_gmres_multi_rhs_equals_single(op2048, pre2048, handle):
+    A, Ao, b, t, cells, L = op2048
+    M = pre2048[0]
+    if M.info is None:
+        M.factorizeM()
+    N = b.shape[0]
+    rng = np.random.default_rng(4)
+    Xt = np.asfortranarray(rng.random((N, 3)))
+    B = m.dense_matvec(handle, m.Laplace3D(), b, Xt)
+    X = np.zeros((N, 3), order="F")
+    A.solveGMRES(1e-10, M, X, B, 10, 50)
+    for c in range(3):
+        x1 = np.zeros(N)
+        A2 = A  # same operator object, single column
+        A2.solveGMRES(1e-10, M, x1, B[:, c].copy(), 10, 50)
+        assert rel(X[:, c], x1) < 1e-12
+
+
+def test_gmres_fp32_preconditioner_reaches_fp64_tolerance(op2048, handle):
+    A, Ao, b, t, cells, L = op2048
+    M32 = m.H2MatrixSolver(handle, m.Laplace3D(), 0.0, 100, 0, t, 2.0, b, samples=2000, precision=m.FP32)
+    M32.factorizeM()
+    N = b.shape[0]
+    xt = m.uniform_rhs(N)
+    B = m.dense_matvec(handle, m.Laplace3D(), b, xt)
+    X = np.zeros(N)
+    rc = A.solveGMRES(1e-10, M32, X, B, 10, 50)
+    assert rc == 0
+    r = B - m.dense_matvec(handle, m.Laplace3D(), b, X)
+    assert np.linalg.norm(r) / np.linalg.norm(B) < 1e-10
+
+
+# ---------------------------------------------------------------- edge cases
+
+def test_single_box_tree(handle):
+    """N < leaf: one box, no far field; the preconditioner is a dense LU."""
+    g = load_golden([c for c in golden_cases() if "n300" in c][0])
+    N = int(g["N"])
+    b = m.uniform_unit_cube_rnd(N, int(g["seed"]))
+    t = m.build_tree(b, 0)
+    A = m.H2MatrixSolver(handle, m.Laplace3D(), 1e-10, 50, 0, t, 2.0, b)
+    M = m.H2MatrixSolver(handle, m.Laplace3D(), 0.0, 50, 0, t, 2.0, b)
+    M.factorizeM()
+    xt = m.uniform_rhs(N)
+    B = m.dense_matvec(handle, m.Laplace3D(), b, xt)
+    y = xt.copy()
+    A.matVecMul(y)
+    assert rel(y, B) < 1e-14
+    z = B.copy()
+    M.solvePrecondition(z)
+    assert rel(z, xt) < 1e-8
+    X = np.zeros(N)
+    assert A.solveGMRES(1e-10, M, X, B, 10, 5) == 0
+    assert A.iters == 1
+
+
+def test_hss_mode_ulv_is_exact_inverse(handle):
+    """theta = 0 (mode "hss", main.cpp:139-140): the ULV inverts its own H^2 matrix."""
+    b, t, cells, L = problem(2048)
+    M = m.H2MatrixSolver(handle, m.Laplace3D(), 0.0, 100, 0, t, 0.0, b, samples=2000)
+    x = m.uniform_rhs(2048)
+    y = x.copy()
+    M.matVecMul(y)
+    M.factorizeM()
+    M.solvePrecondition(y)
+    assert rel(y, x) < 1e-7
+
+
+def test_ragged_leaves_and_full_far_lists(handle):
+    """N = 2000 (leaves of 250), every far body used (samples <= 0)."""
+    N = 2000
+    b, t, cells, L = problem(N)
+    A = m.H2MatrixSolver(handle, m.Laplace3D(), 1e-9, 100, 0, t, 2.0, b, samples=0)
+    Ao = O.H2MatrixSolver(O.Kernel(), 1e-9, 100, 0, cells, 2.0, b.copy(), L, 0)
+    x = m.uniform_rhs(N)
+    y = x.copy()
+    A.matVecMul(y)
+    assert rel(y, Ao.matvec(x)) < 1e-9
