@@ -1,0 +1,424 @@
+#!/usr/bin/env python
+"""Benchmark of the H^2 factor + solve hot path on B200.
+
+One step = build the ULV preconditioner (shared bases, near blocks,
+couplings), factor it, and solve all right-hand sides with
+ULV-preconditioned GMRES to the relative residual tolerance, for one batch of
+synthetic inputs (the H^2 operator and the right-hand sides are set up once,
+outside the timed region).  Default workload: 262,144 uniform points in the
+unit cube (seed 999), Laplace 1/r, theta 2, leaf 256, preconditioner rank 128,
+4000 far samples per box, 16 right-hand sides, FP32 preconditioner with FP64
+GMRES and FP64 operator, tolerance 1e-10.
+
+Prints one JSON line.  --impl reference times the FP64 CPU restatement of the
+reference path (oracle/h2_oracle.py) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "factor+solve s to 1e-10 residual (mixed FP32 preconditioner / FP64 GMRES), 1 B200"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=262144)
+    ap.add_argument("--leaf", type=int, default=256)
+    ap.add_argument("--theta", type=float, default=2.0)
+    ap.add_argument("--rank", type=int, default=128)
+    ap.add_argument("--samples", type=int, default=4000)
+    ap.add_argument("--op-samples", type=int, default=4000)
+    ap.add_argument("--op-eps", type=float, default=1e-11)
+    ap.add_argument("--nrhs", type=int, default=16)
+    ap.add_argument("--singularity", type=float, default=0.01,
+                    help="Laplace3D(s): value 1/s where bodies coincide (kernel.hpp:28-38)")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--inner", type=int, default=10)
+    ap.add_argument("--outer", type=int, default=50)
+    ap.add_argument("--early-exit", type=int, default=1)
+    ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-only", action="store_true", help="one profiled step, no timing (for ncu)")
+    return ap.parse_args()
+
+
+def workload(a) -> dict:
+    return {"workload": "H2 ULV-preconditioned GMRES, N=%d uniform unit cube (seed 999), Laplace 1/r diag 1/s s=%g, "
+                        "theta=%g, leaf=%d, precond rank=%d, samples=%d, operator eps=%g samples=%d, nrhs=%d, tol=%g"
+                        % (a.n, a.singularity, a.theta, a.leaf, a.rank, a.samples, a.op_eps, a.op_samples, a.nrhs,
+                           a.tol),
+            "n": a.n, "nrhs": a.nrhs, "leaf": a.leaf, "theta": a.theta, "rank": a.rank, "samples": a.samples,
+            "singularity": a.singularity, "precond_precision": "fp32" if a.precision == "mixed" else "fp64",
+            "gmres": "fp64, inner %d, outer <= %d, early exit %d" % (a.inner, a.outer, a.early_exit),
+            "l2": "inputs (HBM working set of GBs) exceed the 126 MB L2 every step"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names[1:], f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(a):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def dist_max(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def rhs_matrix(n: int, nrhs: int):
+    import numpy as np
+
+    import mxc_b200 as m
+
+    X = np.empty((n, nrhs), order="F")
+    X[:, 0] = m.uniform_rhs(n)  # main.cpp:358-361
+    if nrhs > 1:
+        X[:, 1:] = np.random.default_rng(20261203).random((n, nrhs - 1))
+    return X
+
+
+def run_ours(a):
+    import numpy as np
+    import torch
+
+    import mxc_b200 as m
+
+    ws, rank, local = dist_setup(a)
+    torch.cuda.set_device(local)
+    h = m.Handle(local)
+    k = m.Laplace3D(a.singularity)
+    L = m.levels_for(a.n, a.leaf)
+    b = m.uniform_unit_cube_rnd(a.n, 999)
+    tree = m.build_tree(b, L)
+    prec = m.FP32 if a.precision == "mixed" else m.FP64
+    t0 = time.time()
+    A = m.H2MatrixSolver(h, k, a.op_eps, a.rank, 0, tree, a.theta, b, samples=a.op_samples, precision=m.FP64)
+    op_build_s = time.time() - t0
+    Xt = rhs_matrix(a.n, a.nrhs)
+    dXt = torch.from_numpy(Xt.T.copy()).cuda()  # (nrhs, n) row-major == column-major n x nrhs
+    dB = torch.empty_like(dXt)
+    dbod = torch.from_numpy(b).cuda()
+    torch.cuda.synchronize()
+    m._lib.check(m.lib().h2dev_dense_matvec_device(h.h, k.kind, k.singularity, k.alpha,
+                                                   m.solver.C.c_void_p(dbod.data_ptr()), a.n, a.nrhs,
+                                                   m.solver.C.c_void_p(dXt.data_ptr()),
+                                                   m.solver.C.c_void_p(dB.data_ptr()), a.n), "dense")
+    h.synchronize()
+    dX = torch.zeros_like(dXt)
+    torch.cuda.synchronize()
+
+    def step(precision, profile=False):
+        dX.zero_()
+        torch.cuda.synchronize()
+        if profile:
+            h.profile(True)
+        h.timer_start()
+        M = m.H2MatrixSolver(h, k, 0.0, a.rank, 0, tree, a.theta, b, samples=a.samples, precision=precision)
+        t_build = h.timer_stop()
+        h.timer_start()
+        M.factorizeM()
+        t_fact = h.timer_stop()
+        h.timer_start()
+        rc, resid, iters = A.gmres_device(M, a.tol, dX.data_ptr(), dB.data_ptr(), a.nrhs, a.n, a.inner, a.outer,
+                                          bool(a.early_exit))
+        t_solve = h.timer_stop()
+        M.close()
+        final = [float(resid[int(iters[c]), c]) for c in range(a.nrhs)]
+        return {"build_ms": t_build, "factor_ms": t_fact, "solve_ms": t_solve,
+                "total_ms": t_build + t_fact + t_solve, "rc": rc, "iters": [int(v) for v in iters],
+                "resid": final}
+
+    if a.profile_only:
+        r = step(prec, profile=False)
+        print(json.dumps({"profile_only": True, **{k_: v for k_, v in r.items() if k_ != "resid"}}))
+        return
+
+    for _ in range(a.warmup):
+        step(prec)
+    clocks = ClockSampler(local)
+    dist_barrier(ws)
+    torch.cuda.synchronize()
+    clocks.start()
+    runs = [step(prec) for _ in range(a.steps)]
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    dist_barrier(ws)
+    ms = [r["total_ms"] for r in runs]
+    ms_step = sum(ms) / len(ms)
+    ms_step_max = dist_max(ms_step, ws)
+
+    # End to end through the public host-array API (H2D of X0 and B and D2H
+    # of X inside the timed region, every step).
+    Bh = np.asfortranarray(dB.cpu().numpy().T)
+    e2e_ms = []
+    for _ in range(max(1, a.steps)):
+        X = np.zeros((a.n, a.nrhs), order="F")
+        h.synchronize()
+        t0 = time.perf_counter()
+        M = m.H2MatrixSolver(h, k, 0.0, a.rank, 0, tree, a.theta, b, samples=a.samples, precision=prec)
+        M.factorizeM()
+        A.solveGMRES(a.tol, M, X, Bh, a.inner, a.outer, early_exit=bool(a.early_exit))
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        M.close()
+    e2e_step = dist_max(sum(e2e_ms) / len(e2e_ms), ws)
+
+    # Dense-matvec verification of the last solution (FP64, matrix-free).
+    Xs = np.asfortranarray(dX.cpu().numpy().T)
+    R = m.dense_matvec(h, k, b, Xs)
+    dense_res = [float(np.linalg.norm(Bh[:, c] - R[:, c]) / np.linalg.norm(Bh[:, c])) for c in range(a.nrhs)]
+    xerr = [float(np.linalg.norm(Xs[:, c] - Xt[:, c]) / np.linalg.norm(Xt[:, c])) for c in range(a.nrhs)]
+
+    # FP64-factor comparison (BASELINE: mixed vs FP64 on the same GPU).
+    fp64 = None
+    if a.precision == "mixed" and not a.no_fp64_compare:
+        r64 = step(m.FP64)
+        X64 = np.asfortranarray(dX.cpu().numpy().T)
+        fp64 = {"ms_per_step": r64["total_ms"], "build_ms": r64["build_ms"], "factor_ms": r64["factor_ms"],
+                "solve_ms": r64["solve_ms"], "iters": r64["iters"],
+                "max_rel_diff_vs_mixed": float(max(np.linalg.norm(X64[:, c] - Xs[:, c]) / np.linalg.norm(X64[:, c])
+                                                   for c in range(a.nrhs)))}
+
+    # Profiled step: per-kernel device time, algorithmic work, launch count.
+    step(prec, profile=True)
+    rep = h.profile_report()
+    h.profile(False)
+    launches = sum(v[0] for v in rep.values())
+    dom = max(rep.items(), key=lambda kv: kv[1][1])
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    fp64_peak = h.fma_peak_tflops(m.FP64)
+    fp32_peak = h.fma_peak_tflops(m.FP32)
+    name, (nl, dms, fl, by) = dom
+    compute = fl > 0 and (fl / max(by, 1.0)) > 2.0
+    if compute:
+        is32 = (prec == m.FP32 and name in ("sample_tsqr", "cpqr", "gemm_factor", "lu_inverse", "basis_finish"))
+        peak = fp32_peak if is32 else fp64_peak
+        achieved = fl / (dms * 1e-3) / 1e12
+        roof = {"kernel": name, "bound": "fp32_simt" if is32 else "fp64_simt", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
+                "peak_source": "measured FMA-throughput probe on this device (h2dev_probe_fma_peak); "
+                               "MEASURED_PEAKS.json has no FP64/FP32 SIMT figure",
+                "launches": nl, "ms_per_launch": dms / nl}
+    else:
+        achieved = by / (dms * 1e-3) / 1e9
+        roof = {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": None, "peak_source": "MEASURED_PEAKS.json hbm_gbs",
+                "launches": nl, "ms_per_launch": dms / nl}
+    kernels = {kk: {"launches": v[0], "ms": round(v[1], 3), "gflop": round(v[2] / 1e9, 3), "gb": round(v[3] / 1e9, 3)}
+               for kk, v in sorted(rep.items(), key=lambda kv: -kv[1][1])}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(a, runs[-1]["iters"], budget_s=25.0)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": ms_step_max / 1e3,
+            "unit": "s",
+            "n_gpus": ws,
+            "steps": a.steps,
+            "warmup": a.warmup,
+            "ms_per_step": ms_step_max,
+            "higher_is_better": False,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 preconditioner / f64 GMRES+operator" if a.precision == "mixed" else "f64",
+            "data": "synthetic (seeded uniform cube points, uniform[0,1) solutions; B = A_dense X)",
+            "config": workload(a),
+            "phases_ms": {"build": sum(r["build_ms"] for r in runs) / len(runs),
+                          "factor": sum(r["factor_ms"] for r in runs) / len(runs),
+                          "solve": sum(r["solve_ms"] for r in runs) / len(runs)},
+            "gmres_cycles": runs[-1]["iters"],
+            "converged": all(r["rc"] == 0 for r in runs),
+            "h2_resid_max": max(runs[-1]["resid"]),
+            "dense_resid_max": max(dense_res),
+            "x_true_err_max": max(xerr),
+            "operator_build_s": op_build_s,
+            "e2e": {"value": e2e_step / 1e3, "unit": "s", "h2d_bytes_per_step": 2 * 8 * a.n * a.nrhs,
+                    "d2h_bytes_per_step": 8 * a.n * a.nrhs},
+            "gpu_launches": launches,
+            "roofline": roof,
+            "kernels": kernels,
+            "fp64_factor": fp64,
+            "cpu_baseline": cpu,
+            "clocks": ck,
+        }
+        print(json.dumps(line))
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def cpu_baseline(a, gpu_cycles, budget_s=25.0):
+    """Oracle (FP64 numpy/OpenBLAS restatement) on a bounded sample, scaled to the full workload.
+
+    Sample: the same pipeline (preconditioner build + factor + one GMRES
+    restart cycle of ``inner`` steps, one right-hand side) at the largest
+    N_s = 2^k * leaf that fits the time budget.  The preconditioner build and
+    factor are O(N) per level-box work, so they scale by N/N_s; the solve
+    scales by N/N_s per cycle, times the cycles each right-hand side took on
+    the GPU, times the number of right-hand sides.
+    """
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+
+    import h2_oracle as O
+
+    cores = os.cpu_count()
+    ns = max(2 * a.leaf, 4096)
+    t_total = None
+    while True:
+        L = O.levels_for(ns, a.leaf)
+        bo = O.uniform_unit_cube_rnd(ns, 999)
+        cells = O.build_binary_tree(bo, L)
+        k = O.Kernel(O.LAPLACE, a.singularity)
+        t0 = time.perf_counter()
+        M = O.H2MatrixSolver(k, 0.0, a.rank, 0, cells, a.theta, bo, L, a.samples)
+        M.factorize()
+        t_bf = time.perf_counter() - t0
+        A = O.H2MatrixSolver(k, a.op_eps, a.rank, 0, cells, a.theta, bo, L, a.op_samples)
+        x = O.xbody_uniform(ns)
+        B = O.dense_matvec(k, bo, x)
+        t0 = time.perf_counter()
+        A.solve_gmres(a.tol, M, np.zeros(ns), B, a.inner, 1)
+        t_cycle = time.perf_counter() - t0
+        t_total = t_bf + t_cycle
+        if t_total * 2.5 > budget_s or ns * 2 > a.n:
+            break
+        ns *= 2
+    scale = a.n / ns
+    cycles = sum(max(1, c) for c in gpu_cycles)
+    est = t_bf * scale + t_cycle * scale * cycles
+    return {"value": est, "unit": "s", "cores": cores, "kind": "port",
+            "sample": "oracle/h2_oracle.py at N_s=%d (same leaf/rank/samples/theta): preconditioner build+factor "
+                      "%.2f s and one %d-step GMRES cycle %.2f s, scaled by N/N_s=%.0f and by the %d GMRES cycles "
+                      "(summed over %d RHS) the GPU run took; OpenBLAS threads=%s"
+                      % (ns, t_bf, a.inner, t_cycle, scale, cycles, a.nrhs,
+                         os.environ.get("OPENBLAS_NUM_THREADS", "default")),
+            "measured_s": t_total}
+
+
+def run_reference(a):
+    ws, rank, local = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    budget = 20.0
+    vals = []
+    for _ in range(a.warmup):
+        pass
+    t_start = time.time()
+    for i in range(max(1, a.steps)):
+        c = cpu_baseline(a, [1] * a.nrhs, budget_s=budget)
+        vals.append(c)
+        if time.time() - t_start > 240:
+            break
+    v = sum(c["value"] for c in vals) / len(vals)
+    line = {"metric": METRIC, "value": v, "unit": "s", "n_gpus": ws, "steps": len(vals), "warmup": a.warmup,
+            "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": workload(a), "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "s", "cores": vals[-1]["cores"], "kind": "port",
+                             "sample": vals[-1]["sample"] + " (one GMRES cycle per RHS assumed)"},
+            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -127,6 +127,24 @@ int h2dev_solver_export_size(h2dev_solver_t s, int64_t level, int what, int64_t*
  * block order, each block column-major, converted to double. */
 int h2dev_solver_export(h2dev_solver_t s, int64_t level, int what, double* out);
 
+/* ---- instrumentation (CUDA events on the handle's stream) ------------ */
+
+/* Turns per-launch timing on/off (clears earlier records).  While on, every
+ * kernel launch is bracketed by a pair of events; MPI_Wtime phase timers and
+ * the comm stopwatch (main.cpp, comm-mpi.cpp:247-262) have no other analogue. */
+int h2dev_profile_enable(h2dev_handle_t h, int on);
+/* Aggregates the records by kernel name: up to cap rows of names (48 bytes
+ * each), launch counts, total device ms, algorithmic FLOPs and bytes;
+ * *count receives the number of distinct kernels. */
+int h2dev_profile_report(h2dev_handle_t h, int64_t cap, char* names, int64_t* launches, double* ms, double* flops,
+                         double* bytes, int64_t* count);
+/* Measured FMA throughput (TFLOP/s, 2 flops per FMA) of plain FP64 or FP32
+ * SIMT code on this device: the denominator for the FP64/FP32 kernels. */
+int h2dev_probe_fma_peak(h2dev_handle_t h, int precision, double* tflops);
+/* Event pair on the handle's stream: device time between start and stop. */
+int h2dev_timer_start(h2dev_handle_t h);
+int h2dev_timer_stop(h2dev_handle_t h, double* ms);
+
 const char* h2dev_last_error_message(void);
 
 #ifdef __cplusplus

@@ -62,6 +62,11 @@ SIGNATURES = {
                                             _i64]),
     "h2dev_solver_export_size": (C.c_int, [_vp, _i64, C.c_int, _i64p]),
     "h2dev_solver_export": (C.c_int, [_vp, _i64, C.c_int, _vp]),
+    "h2dev_profile_enable": (C.c_int, [_vp, C.c_int]),
+    "h2dev_profile_report": (C.c_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _i64p]),
+    "h2dev_probe_fma_peak": (C.c_int, [_vp, C.c_int, _dp]),
+    "h2dev_timer_start": (C.c_int, [_vp]),
+    "h2dev_timer_stop": (C.c_int, [_vp, _dp]),
     "h2dev_last_error_message": (C.c_char_p, []),
 }
 

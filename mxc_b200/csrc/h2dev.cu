@@ -16,7 +16,69 @@
 #include "kernels.h"
 #include "plan.hpp"
 
+// Per-launch device timing, recorded only while profiling is enabled on the
+// handle: a pair of events around each launch on the handle's stream plus
+// the launch's algorithmic FLOP and byte counts.
+struct ProfRec {
+  const char* name;
+  cudaEvent_t a, b;
+  double flops, bytes;
+};
+
+struct h2dev_handle_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool prof = false;
+  std::vector<ProfRec> recs;
+  std::vector<cudaEvent_t> pool;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  cudaEvent_t take() {
+    if (!pool.empty()) {
+      cudaEvent_t e = pool.back();
+      pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+  }
+  void clear() {
+    for (auto& r : recs) {
+      pool.push_back(r.a);
+      pool.push_back(r.b);
+    }
+    recs.clear();
+  }
+};
+
 namespace h2b {
+
+static thread_local h2dev_handle_s* g_cur = nullptr;
+
+struct CurHandle {
+  h2dev_handle_s* prev;
+  explicit CurHandle(h2dev_handle_s* h) : prev(g_cur) { g_cur = h; }
+  ~CurHandle() { g_cur = prev; }
+};
+
+struct Prof {
+  h2dev_handle_s* h;
+  ProfRec r;
+  Prof(const char* name, double flops, double bytes) : h(g_cur && g_cur->prof ? g_cur : nullptr) {
+    if (!h) return;
+    r.name = name;
+    r.flops = flops;
+    r.bytes = bytes;
+    r.a = h->take();
+    r.b = h->take();
+    cudaEventRecord(r.a, h->stream);
+  }
+  ~Prof() {
+    if (!h) return;
+    cudaEventRecord(r.b, h->stream);
+    h->recs.push_back(r);
+  }
+};
 
 struct H2Error {
   int code;
@@ -88,6 +150,8 @@ struct GemmPlan {
   DVec<TileRef> d_tiles;
   int ntiles = 0;
   int shape = GEMM_BIG;
+  const char* name = "seg_gemm";
+  double flops = 0., bytes = 0.;  // algorithmic work of one run
   void add_task(T* C, i64 ldc, int m, int n, T beta) {
     GemmTask<T> t;
     t.C = C; t.ldc = ldc; t.m = m; t.n = n; t.beta = beta;
@@ -115,6 +179,15 @@ struct GemmPlan {
         for (int b = 0; b < (t.n + bn - 1) / bn; b++) tiles.push_back(TileRef{ti, a, b});
     }
     ntiles = (int)tiles.size();
+    flops = bytes = 0.;
+    for (const auto& t : tasks) {
+      if (t.m <= 0 || t.n <= 0) continue;
+      bytes += (double)t.m * t.n * sizeof(T) * (t.beta == T(0) ? 1. : 2.);
+      for (int e = t.e0; e < t.e1; e++) {
+        flops += 2. * t.m * t.n * ents[e].k;
+        bytes += ((double)t.m * ents[e].k + (double)ents[e].k * t.n) * sizeof(T);
+      }
+    }
     d_tasks.upload(tasks);
     d_ents.upload(ents);
     d_tiles.upload(tiles);
@@ -123,7 +196,10 @@ struct GemmPlan {
     ents.clear();
     ents.shrink_to_fit();
   }
-  void run(cudaStream_t st) const { ck(launch_seg_gemm<T>(shape, d_tasks.p, d_ents.p, d_tiles.p, ntiles, st), "seg_gemm"); }
+  void run(cudaStream_t st) const {
+    Prof p(name, flops, bytes);
+    ck(launch_seg_gemm<T>(shape, d_tasks.p, d_ents.p, d_tiles.p, ntiles, st), "seg_gemm");
+  }
 };
 
 template <typename T>
@@ -139,19 +215,20 @@ struct CopyPlan {
   }
   void finalize() {
     n = (int)ents.size();
+    bytes = 0.;
+    for (const auto& e : ents) bytes += 2. * e.m * e.n * sizeof(T);
     d.upload(ents);
     ents.clear();
     ents.shrink_to_fit();
   }
-  void run(cudaStream_t st) const { ck(launch_batched_copy<T>(d.p, n, st), "batched_copy"); }
+  double bytes = 0.;
+  void run(cudaStream_t st) const {
+    Prof p("batched_copy", 0., bytes);
+    ck(launch_batched_copy<T>(d.p, n, st), "batched_copy");
+  }
 };
 
 }  // namespace h2b
-
-struct h2dev_handle_s {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-};
 
 namespace h2b {
 
@@ -337,7 +414,10 @@ class Solver : public SolverBase {
           }
         DVec<GenTask> dg;
         dg.upload(gt);
-        ck(launch_gen_blocks<T>(kp, dg.p, (int)gt.size(), 1, lv.A.p, st()), "gen near");
+        {
+          Prof pf("gen_near_blocks", 0., (double)lv.aoff[nA] * sizeof(T));
+          ck(launch_gen_blocks<T>(kp, dg.p, (int)gt.size(), 1, lv.A.p, st()), "gen near");
+        }
         ck(cudaStreamSynchronize(st()), "sync");
       } else {
         CopyPlan<double> pcopy;
@@ -406,14 +486,33 @@ class Solver : public SolverBase {
       Rws.zero(st());
       const double e = level_epi(l);
       const bool orth = 1. <= e;
-      ck(launch_sample_tsqr<T>(kp, bodies.p, lv.pts.p, lv.d_xoff.p, lv.d_dims.p, d_sidx.p, d_soff.p, Rws.p,
-                               lv.d_qoff.p, (int)nodes, (int)lv.maxM, st()),
-         "sample_tsqr");
+      {
+        double fl = 0.;
+        for (i64 i = 0; i < nodes; i++) {
+          double S = (double)(soff[i + 1] - soff[i]), Md = (double)lv.dims[i];
+          fl += S >= Md ? 2. * S * Md * Md - 2. / 3. * Md * Md * Md : 2. * Md * S * S - 2. / 3. * S * S * S;
+        }
+        Prof pf("sample_tsqr", fl, (double)sidx.size() * 28.);
+        ck(launch_sample_tsqr<T>(kp, bodies.p, lv.pts.p, lv.d_xoff.p, lv.d_dims.p, d_sidx.p, d_soff.p, Rws.p,
+                                 lv.d_qoff.p, (int)nodes, (int)lv.maxM, st()),
+           "sample_tsqr");
+      }
       i64 cap = -1;
       if (e >= 1.) cap = (i64)std::floor(e);
-      ck(launch_cpqr<T>(lv.d_dims.p, d_krows.p, Rws.p, lv.d_qoff.p, d_perm.p, lv.d_xoff.p, d_maxpiv.p, d_nonzero.p,
-                        cap, (int)nodes, (int)lv.maxM, st()),
-         "cpqr");
+      {
+        double fl = 0.;
+        for (i64 i = 0; i < nodes; i++) {
+          double K = (double)krows[i], Md = (double)lv.dims[i];
+          double st_ = std::min(K, Md);
+          if (cap >= 0) st_ = std::min(st_, (double)cap);
+          fl += 4. * K * Md * st_ - 2. * (K + Md) * st_ * st_ + 4. / 3. * st_ * st_ * st_;
+        }
+        Prof pf("cpqr", fl, 0.);
+        ck(launch_cpqr<T>(lv.d_dims.p, d_krows.p, Rws.p, lv.d_qoff.p, d_perm.p, lv.d_xoff.p, d_maxpiv.p,
+                          d_nonzero.p, cap, (int)nodes, (int)lv.maxM, st()),
+           "cpqr");
+      }
+      Prof pfin("basis_finish", 0., (double)lv.qoff[nodes] * sizeof(T) * 3.);
       ck(launch_basis_finish<T>(lv.d_dims.p, d_krows.p, Rws.p, lv.Q.p, lv.R.p, lv.d_qoff.p, d_perm.p, lv.d_xoff.p,
                                 d_maxpiv.p, d_nonzero.p, lv.pts.p, lv.d_ranks.p, e, orth ? 1 : 0, low ? 0 : 1,
                                 (int)nodes, (int)lv.maxM, st()),
@@ -457,7 +556,10 @@ class Solver : public SolverBase {
         }
       DVec<GenTask> dg;
       dg.upload(gt);
-      ck(launch_gen_blocks<T>(kp, dg.p, (int)gt.size(), 1, kout, st()), "gen couplings");
+      {
+        Prof pf("gen_couplings", 0., (double)lv.coff[nC] * sizeof(T));
+        ck(launch_gen_blocks<T>(kp, dg.p, (int)gt.size(), 1, kout, st()), "gen couplings");
+      }
       if (orth) {
         DVec<T> T1;
         T1.alloc(lv.coff[nC]);
@@ -471,6 +573,7 @@ class Solver : public SolverBase {
             g2.add_task(lv.C.p + lv.coff[k], ry, ry, rx, T(0));
             g2.add_entry(T1.p + lv.coff[k], ry, 0, lv.R.p + lv.qoff[x], lv.dims[x], 1, rx, T(1));
           }
+        g1.name = g2.name = "gemm_coupling";
         g1.finalize();
         g2.finalize();
         g1.run(st());
@@ -511,6 +614,7 @@ class Solver : public SolverBase {
       const T* X = (l == levels) ? vin.p : L[l + 1].vZ.p;
       const i64 ldx = lv.lenX;
       GemmPlan<T>& g = mv_up[l];
+      g.name = "gemm_matvec";
       for (i64 i = 0; i < lv.nodes; i++) {
         int M = (int)lv.dims[i], r = (int)lv.ranks[i];
         if (r == 0) continue;
@@ -522,6 +626,7 @@ class Solver : public SolverBase {
     for (i64 l = 0; l <= levels; l++) {
       Level<T>& lv = L[l];
       GemmPlan<T>& g = mv_h[l];
+      g.name = "gemm_matvec";
       const T beta = (l == 0) ? T(0) : T(1);
       for (i64 i = 0; i < lv.nodes; i++) {
         int r = (int)lv.ranks[i];
@@ -535,6 +640,7 @@ class Solver : public SolverBase {
       g.finalize();
       if (l < levels) {
         GemmPlan<T>& d = mv_down[l];
+        d.name = "gemm_matvec";
         Level<T>& nx = L[l + 1];  // Y_l lives in W_{l+1}
         for (i64 i = 0; i < lv.nodes; i++) {
           int M = (int)lv.dims[i], r = (int)lv.ranks[i];
@@ -548,6 +654,7 @@ class Solver : public SolverBase {
       Level<T>& lv = L[levels];
       GemmPlan<T>& g = mv_leaf;
       g = GemmPlan<T>();
+      g.name = "gemm_matvec";
       for (i64 i = 0; i < lv.nodes; i++) {
         int M = (int)lv.dims[i], r = (int)lv.ranks[i];
         g.add_task(vout.p + lv.xoff[i], lv.lenX, M, nr, T(0));
@@ -563,6 +670,7 @@ class Solver : public SolverBase {
   }
 
   void stage_in(i64 nrhs, const double* dX, i64 ldx) {
+    Prof pf("stage_convert", 0., (8. + sizeof(T)) * N * nrhs);
     if (ldx == N) {
       ck(launch_convert<double, T>(dX, vin.p, N * nrhs, st()), "convert in");
     } else {
@@ -570,6 +678,7 @@ class Solver : public SolverBase {
     }
   }
   void stage_out(i64 nrhs, double* dX, i64 ldx) {
+    Prof pf("stage_convert", 0., (8. + sizeof(T)) * N * nrhs);
     if (ldx == N) {
       ck(launch_convert<T, double>(vout.p, dX, N * nrhs, st()), "convert out");
     } else {
@@ -634,7 +743,9 @@ class Solver : public SolverBase {
       s2.add_task(Aii, M, M, M, T(0));
       s2.add_entry(Q + lv.qoff[i], M, 1, T1.p + lv.qoff[i], M, 0, M, T(1));
     }
+    s1.name = "gemm_factor";
     s1.finalize();
+    s2.name = "gemm_factor";
     s2.finalize();
     s1.run(st());
     s2.run(st());
@@ -659,7 +770,12 @@ class Solver : public SolverBase {
     {
       DVec<LuTask<T>> dl;
       dl.upload(lt);
-      ck(launch_lu_inverse<T>(dl.p, (int)lt.size(), st()), "lu_inverse");
+      double fl = 0.;
+      for (const auto& t : lt) fl += 8. / 3. * (double)t.n * t.n * t.n;
+      {
+        Prof pf("lu_inverse", fl, 0.);
+        ck(launch_lu_inverse<T>(dl.p, (int)lt.size(), st()), "lu_inverse");
+      }
       ck(cudaStreamSynchronize(st()), "sync");
     }
     // Step 5: V^T[:, Ms:] = U_r (A_rr^{-1})^T.
@@ -669,6 +785,7 @@ class Solver : public SolverBase {
       s5.add_task(V + lv.qoff[i] + (i64)Ms * M, M, M, Mr, T(0));
       s5.add_entry(Q + lv.qoff[i] + (i64)Ms * M, M, 0, lv.invT.p + lv.ioff[i], Mr, 0, Mr, T(1));
     }
+    s5.name = "gemm_factor";
     s5.finalize();
     s5.run(st());
     // Steps 6-8.
@@ -686,8 +803,11 @@ class Solver : public SolverBase {
       s8.add_task(lv.B.p + lv.boff[i] + (i64)Ms * Mr, Mr, Mr, Mr, T(0));
       s8.add_entry(V + lv.qoff[i] + (i64)Ms * M, M, 1, Q + lv.qoff[i] + (i64)Ms * M, M, 0, M, T(1));
     }
+    s6.name = "gemm_factor";
     s6.finalize();
+    s7.name = "gemm_factor";
     s7.finalize();
+    s8.name = "gemm_factor";
     s8.finalize();
     c8.finalize();
     s6.run(st());
@@ -732,6 +852,7 @@ class Solver : public SolverBase {
           b.add_entry(V + lv.qoff[i], Mi, 1, T2.p + o, Mi, 0, Mi, T(1));
           o += (i64)Mi * Nj;
         }
+        a.name = b.name = "gemm_factor";
         a.finalize();
         b.finalize();
         a.run(st());
@@ -781,9 +902,12 @@ class Solver : public SolverBase {
           }
         }
       }
-      s10.finalize();
-      s11a.finalize();
-      s11b.finalize();
+      s10.name = "gemm_factor";
+    s10.finalize();
+      s11a.name = "gemm_factor";
+    s11a.finalize();
+      s11b.name = "gemm_factor";
+    s11b.finalize();
       s11a.run(st());
       s10.run(st());
       s11b.run(st());
@@ -865,6 +989,7 @@ class Solver : public SolverBase {
         pc_by[l].add_task(Yout + lv.xoff[i], ldy, M, nr, T(0));
         pc_by[l].add_entry(lv.Q.p + lv.qoff[i], M, 0, X + lv.xoff[i], ldx, 0, M, T(1));
       }
+      pc_fx[l].name = pc_fz[l].name = pc_bx[l].name = pc_by[l].name = "gemm_precond";
       pc_fx[l].finalize(); pc_fz[l].finalize(); pc_bx[l].finalize(); pc_by[l].finalize();
       pc_fcopy[l].finalize(); pc_bcopy[l].finalize();
     }
@@ -1022,9 +1147,9 @@ static int gmres(SolverBase& A, SolverBase& M, double tol, i64 nrhs, double* dX,
       A.matvec(nrhs, w.p, N);
       M.precondition(nrhs, w.p, N);
       const int kv = (int)i + 1;
-      ck(launch_dots(V.p, vstride, kv, w.p, N, nr, partial.p, nch, hcol.p, st), "dots");
+      { Prof pf("gmres_dots", 2. * N * kv * nr, 8. * (kv + 1) * N * nr); ck(launch_dots(V.p, vstride, kv, w.p, N, nr, partial.p, nch, hcol.p, st), "dots"); }
       // H[:kv, i] for every rhs (rhs c block of H has stride ldh*inner)
-      ck(launch_gs_update(w.p, V.p, vstride, hcol.p, kv, kv, N, nr, -1.0, nullptr, st), "gs");
+      { Prof pf("gmres_gs_update", 2. * N * kv * nr, 8. * (kv + 2) * N * nr); ck(launch_gs_update(w.p, V.p, vstride, hcol.p, kv, kv, N, nr, -1.0, nullptr, st), "gs"); }
       {
         // scatter hcol into H column i
         CopyPlan<double> cp;
@@ -1226,6 +1351,10 @@ int h2dev_handle_destroy(h2dev_handle_t h) {
   H2_API_BEGIN
   if (!h) return H2DEV_OK;
   cudaStreamSynchronize(h->stream);
+  h->clear();
+  for (cudaEvent_t e : h->pool) cudaEventDestroy(e);
+  if (h->t0) cudaEventDestroy(h->t0);
+  if (h->t1) cudaEventDestroy(h->t1);
   cudaStreamDestroy(h->stream);
   delete h;
   return H2DEV_OK;
@@ -1250,6 +1379,7 @@ int h2dev_solver_create(h2dev_handle_t h, int kernel, double singularity, double
   require(nbodies > 0 && epi >= 0., "bad sizes");
   require(precision == H2DEV_FP64 || precision == H2DEV_FP32, "precision");
   ck(cudaSetDevice(h->device), "cudaSetDevice");
+  CurHandle ch(h);
   BuildArgs a;
   a.kp = make_kp(kernel, singularity, alpha);
   a.epi = epi;
@@ -1334,6 +1464,7 @@ int h2dev_matvec(h2dev_solver_t s, int64_t nrhs, double* X, int64_t ldx) {
   H2_API_BEGIN
   require(s && s->impl && X, "null argument");
   SolverBase* p = s->impl.get();
+  CurHandle ch(p->h);
   require(nrhs > 0 && ldx >= p->lenX(), "bad nrhs/ld");
   with_device_copy(p->h, p->lenX(), nrhs, X, ldx, [&](double* d) { p->matvec(nrhs, d, p->lenX()); });
   return H2DEV_OK;
@@ -1343,6 +1474,7 @@ int h2dev_matvec(h2dev_solver_t s, int64_t nrhs, double* X, int64_t ldx) {
 int h2dev_matvec_device(h2dev_solver_t s, int64_t nrhs, double* dX, int64_t ldx) {
   H2_API_BEGIN
   require(s && s->impl && dX, "null argument");
+  CurHandle ch(s->impl->h);
   s->impl->matvec(nrhs, dX, ldx);
   return H2DEV_OK;
   H2_API_END
@@ -1351,6 +1483,7 @@ int h2dev_matvec_device(h2dev_solver_t s, int64_t nrhs, double* dX, int64_t ldx)
 int h2dev_factorize(h2dev_solver_t s, int* info_per_level) {
   H2_API_BEGIN
   require(s && s->impl, "null solver");
+  CurHandle ch(s->impl->h);
   std::vector<int> info(s->impl->nlevels() + 1, 0);
   s->impl->factorize(info.data());
   int any = 0;
@@ -1366,6 +1499,7 @@ int h2dev_solve_precondition(h2dev_solver_t s, int64_t nrhs, double* X, int64_t 
   H2_API_BEGIN
   require(s && s->impl && X, "null argument");
   SolverBase* p = s->impl.get();
+  CurHandle ch(p->h);
   require(nrhs > 0 && ldx >= p->lenX(), "bad nrhs/ld");
   with_device_copy(p->h, p->lenX(), nrhs, X, ldx, [&](double* d) { p->precondition(nrhs, d, p->lenX()); });
   return H2DEV_OK;
@@ -1375,6 +1509,7 @@ int h2dev_solve_precondition(h2dev_solver_t s, int64_t nrhs, double* X, int64_t 
 int h2dev_solve_precondition_device(h2dev_solver_t s, int64_t nrhs, double* dX, int64_t ldx) {
   H2_API_BEGIN
   require(s && s->impl && dX, "null argument");
+  CurHandle ch(s->impl->h);
   s->impl->precondition(nrhs, dX, ldx);
   return H2DEV_OK;
   H2_API_END
@@ -1386,6 +1521,7 @@ int h2dev_solve_gmres_device(h2dev_solver_t A, h2dev_solver_t M, double tol, int
   H2_API_BEGIN
   require(A && A->impl && M && M->impl && dX && dB && resid, "null argument");
   require(ld >= A->impl->lenX(), "bad ld");
+  CurHandle ch(A->impl->h);
   return gmres(*A->impl, *M->impl, tol, nrhs, dX, dB, ld, inner, outer, early_exit, resid, iters);
   H2_API_END
 }
@@ -1395,6 +1531,7 @@ int h2dev_solve_gmres(h2dev_solver_t A, h2dev_solver_t M, double tol, int64_t nr
   H2_API_BEGIN
   require(A && A->impl && M && M->impl && X && B && resid, "null argument");
   SolverBase* a = A->impl.get();
+  CurHandle ch(a->h);
   const int64_t n = a->lenX();
   require(nrhs > 0 && ld >= n, "bad nrhs/ld");
   cudaStream_t st = a->h->stream;
@@ -1446,6 +1583,8 @@ int h2dev_dense_matvec_device(h2dev_handle_t h, int kernel, double singularity, 
   H2_API_BEGIN
   require(h && dbodies && dX && dY && n > 0 && nrhs > 0 && ld >= n, "bad arguments");
   KernelParams kp = make_kp(kernel, singularity, alpha);
+  CurHandle ch(h);
+  Prof pf("dense_matvec", 2. * (double)n * n * nrhs, 16. * n * nrhs);
   ck(launch_dense_matvec(kp, dbodies, n, dX, ld, dY, ld, (int)nrhs, h->stream), "dense_matvec");
   return H2DEV_OK;
   H2_API_END
@@ -1466,6 +1605,107 @@ int h2dev_dense_matvec(h2dev_handle_t h, int kernel, double singularity, double 
   ck(cudaStreamSynchronize(h->stream), "sync");
   ck(cudaMemcpy2D(Y, sizeof(double) * ld, dy.p, sizeof(double) * n, sizeof(double) * n, nrhs,
                   cudaMemcpyDeviceToHost), "D2H");
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_profile_enable(h2dev_handle_t h, int on) {
+  H2_API_BEGIN
+  require(h != nullptr, "null handle");
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  h->clear();
+  h->prof = on != 0;
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_profile_report(h2dev_handle_t h, int64_t cap, char* names, int64_t* launches, double* ms, double* flops,
+                         double* bytes, int64_t* count) {
+  H2_API_BEGIN
+  require(h && count, "null argument");
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  std::vector<std::string> keys;
+  std::vector<int64_t> nl;
+  std::vector<double> t, f, b;
+  for (const auto& r : h->recs) {
+    float e = 0.f;
+    ck(cudaEventElapsedTime(&e, r.a, r.b), "cudaEventElapsedTime");
+    size_t k = 0;
+    while (k < keys.size() && keys[k] != r.name) k++;
+    if (k == keys.size()) {
+      keys.push_back(r.name);
+      nl.push_back(0);
+      t.push_back(0.);
+      f.push_back(0.);
+      b.push_back(0.);
+    }
+    nl[k]++;
+    t[k] += e;
+    f[k] += r.flops;
+    b[k] += r.bytes;
+  }
+  *count = (int64_t)keys.size();
+  for (size_t k = 0; k < keys.size() && (int64_t)k < cap; k++) {
+    if (names) {
+      std::strncpy(names + 48 * k, keys[k].c_str(), 47);
+      names[48 * k + 47] = 0;
+    }
+    if (launches) launches[k] = nl[k];
+    if (ms) ms[k] = t[k];
+    if (flops) flops[k] = f[k];
+    if (bytes) bytes[k] = b[k];
+  }
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_probe_fma_peak(h2dev_handle_t h, int precision, double* tflops) {
+  H2_API_BEGIN
+  require(h && tflops && (precision == H2DEV_FP64 || precision == H2DEV_FP32), "bad arguments");
+  int sms = 0;
+  ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device), "attr");
+  const int blocks = sms * 8, iters = precision == H2DEV_FP64 ? 4096 : 16384;
+  DVec<double> out;
+  out.alloc((size_t)blocks * 256);
+  cudaEvent_t a, b;
+  ck(cudaEventCreate(&a), "event");
+  ck(cudaEventCreate(&b), "event");
+  double best = 0.;
+  for (int rep = 0; rep < 4; rep++) {
+    ck(cudaEventRecord(a, h->stream), "record");
+    ck(launch_fma_probe(precision, blocks, iters, out.p, h->stream), "fma probe");
+    ck(cudaEventRecord(b, h->stream), "record");
+    ck(cudaEventSynchronize(b), "sync");
+    float ms = 0.f;
+    ck(cudaEventElapsedTime(&ms, a, b), "elapsed");
+    double fl = 2. * 8. * iters * (double)blocks * 256;
+    if (rep > 0) best = std::max(best, fl / (ms * 1e-3) / 1e12);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *tflops = best;
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_timer_start(h2dev_handle_t h) {
+  H2_API_BEGIN
+  require(h != nullptr, "null handle");
+  if (!h->t0) ck(cudaEventCreate(&h->t0), "event");
+  if (!h->t1) ck(cudaEventCreate(&h->t1), "event");
+  ck(cudaEventRecord(h->t0, h->stream), "record");
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_timer_stop(h2dev_handle_t h, double* ms) {
+  H2_API_BEGIN
+  require(h && ms && h->t0 && h->t1, "timer not started");
+  ck(cudaEventRecord(h->t1, h->stream), "record");
+  ck(cudaEventSynchronize(h->t1), "sync");
+  float e = 0.f;
+  ck(cudaEventElapsedTime(&e, h->t0, h->t1), "elapsed");
+  *ms = e;
   return H2DEV_OK;
   H2_API_END
 }

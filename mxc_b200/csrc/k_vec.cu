@@ -184,3 +184,31 @@ cudaError_t launch_residual_norm_finish(const double* nrm2, const double* normb,
 }
 
 }  // namespace h2b
+
+namespace h2b {
+
+// Peak FMA throughput probe: independent FMA chains per thread, no memory
+// traffic in the loop.  Used to give FP64 / FP32 SIMT kernels a measured
+// denominator.
+template <typename T>
+__global__ void __launch_bounds__(256) k_fma_probe(T* out, int iters, T seed) {
+  T a0 = seed + threadIdx.x, a1 = a0 + T(1), a2 = a0 + T(2), a3 = a0 + T(3);
+  T a4 = a0 + T(4), a5 = a0 + T(5), a6 = a0 + T(6), a7 = a0 + T(7);
+  const T m = T(0.999999), c = T(1e-7);
+  for (int i = 0; i < iters; i++) {
+    a0 = a0 * m + c; a1 = a1 * m + c; a2 = a2 * m + c; a3 = a3 * m + c;
+    a4 = a4 * m + c; a5 = a5 * m + c; a6 = a6 * m + c; a7 = a7 * m + c;
+  }
+  T s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (s == T(-1234.5)) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+cudaError_t launch_fma_probe(int precision, int blocks, int iters, void* out, cudaStream_t st) {
+  if (precision == 0)
+    k_fma_probe<double><<<blocks, 256, 0, st>>>((double*)out, iters, 1.0);
+  else
+    k_fma_probe<float><<<blocks, 256, 0, st>>>((float*)out, iters, 1.0f);
+  return cudaGetLastError();
+}
+
+}  // namespace h2b

@@ -107,4 +107,6 @@ cudaError_t launch_axpby(double* y, const double* x, double a, double b, i64 n, 
 cudaError_t launch_residual_norm_finish(const double* nrm2, const double* normb, double* resid, int nrhs,
                                         cudaStream_t st);
 
+cudaError_t launch_fma_probe(int precision, int blocks, int iters, void* out, cudaStream_t st);
+
 }  // namespace h2b

@@ -88,6 +88,41 @@ class Handle:
     def synchronize(self):
         L.check(L.lib().h2dev_handle_synchronize(self.h), "h2dev_handle_synchronize")
 
+    def profile(self, on: bool = True):
+        L.check(L.lib().h2dev_profile_enable(self.h, 1 if on else 0), "h2dev_profile_enable")
+
+    def profile_report(self) -> dict:
+        """{kernel: (launches, device ms, algorithmic flops, algorithmic bytes)}."""
+        cnt = C.c_int64()
+        L.check(L.lib().h2dev_profile_report(self.h, 0, None, None, None, None, None, C.byref(cnt)),
+                "h2dev_profile_report")
+        n = cnt.value
+        names = C.create_string_buffer(48 * max(n, 1))
+        nl = np.zeros(max(n, 1), dtype=np.int64)
+        ms = np.zeros(max(n, 1))
+        fl = np.zeros(max(n, 1))
+        by = np.zeros(max(n, 1))
+        L.check(L.lib().h2dev_profile_report(self.h, n, names, _ptr(nl), _ptr(ms), _ptr(fl), _ptr(by), C.byref(cnt)),
+                "h2dev_profile_report")
+        out = {}
+        for k in range(n):
+            nm = names.raw[48 * k:48 * k + 48].split(b"\0", 1)[0].decode()
+            out[nm] = (int(nl[k]), float(ms[k]), float(fl[k]), float(by[k]))
+        return out
+
+    def fma_peak_tflops(self, precision: int = L.FP64) -> float:
+        v = C.c_double()
+        L.check(L.lib().h2dev_probe_fma_peak(self.h, precision, C.byref(v)), "h2dev_probe_fma_peak")
+        return v.value
+
+    def timer_start(self):
+        L.check(L.lib().h2dev_timer_start(self.h), "h2dev_timer_start")
+
+    def timer_stop(self) -> float:
+        ms = C.c_double()
+        L.check(L.lib().h2dev_timer_stop(self.h, C.byref(ms)), "h2dev_timer_stop")
+        return ms.value
+
     def close(self):
         if self.h:
             L.lib().h2dev_handle_destroy(self.h)
