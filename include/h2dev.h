@@ -31,7 +31,11 @@ enum {
   H2DEV_ERR_NOCONV = 6    /* GMRES stopped at outer_iters above tol */
 };
 
-enum { H2DEV_KERNEL_LAPLACE = 0, H2DEV_KERNEL_YUKAWA = 1 };
+/* Laplace3D 1/d and Yukawa3D exp(-alpha d)/d (kernel.hpp:28-50); QUADRATIC
+ * d^2 + alpha has exactly low-rank off-diagonal blocks (no counterpart in the
+ * reference: used to verify that the ULV factorization is an exact inverse
+ * when no fill is dropped).  Every kernel takes the value 1/s at d == 0. */
+enum { H2DEV_KERNEL_LAPLACE = 0, H2DEV_KERNEL_YUKAWA = 1, H2DEV_KERNEL_QUADRATIC = 2 };
 enum { H2DEV_FP64 = 0, H2DEV_FP32 = 1 };
 
 /* ---- host helpers (no device work) ---------------------------------- */

@@ -8,7 +8,10 @@ namespace h2b {
 
 typedef int64_t i64;
 
-enum KernelKind { KERNEL_LAPLACE = 0, KERNEL_YUKAWA = 1 };
+// KERNEL_QUADRATIC, K(d) = d^2 + alpha, has exactly low-rank (<= 6)
+// off-diagonal blocks; with it the ULV factorization has no dropped fill and
+// must reproduce the inverse, which is how the multilevel logic is verified.
+enum KernelKind { KERNEL_LAPLACE = 0, KERNEL_YUKAWA = 1, KERNEL_QUADRATIC = 2 };
 
 // K(d) for d != 0, and the value used where two bodies coincide
 // (kernel.hpp:28-50: Laplace 1/d, Yukawa exp(-alpha d)/d, diagonal 1/s).
@@ -35,6 +38,7 @@ __device__ __forceinline__ double kernel_exact(const KernelParams& kp, double dx
   double d = hypot3_exact(dx, dy, dz);
   if (d == 0.) return kp.diag;
   if (kp.kind == KERNEL_LAPLACE) return __ddiv_rn(1., d);
+  if (kp.kind == KERNEL_QUADRATIC) return __dadd_rn(__dmul_rn(d, d), kp.alpha);
   return __ddiv_rn(exp(__dmul_rn(-kp.alpha, d)), d);
 }
 
@@ -43,6 +47,7 @@ __device__ __forceinline__ double kernel_exact(const KernelParams& kp, double dx
 __device__ __forceinline__ double kernel_fast(const KernelParams& kp, double dx, double dy, double dz) {
   double r2 = dx * dx + dy * dy + dz * dz;
   if (r2 == 0.) return kp.diag;
+  if (kp.kind == KERNEL_QUADRATIC) return r2 + kp.alpha;
   double inv = rsqrt(r2);
   if (kp.kind == KERNEL_LAPLACE) return inv;
   return exp(-kp.alpha * (r2 * inv)) * inv;

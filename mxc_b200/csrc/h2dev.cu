@@ -1249,7 +1249,8 @@ using namespace h2b;
   }
 
 static KernelParams make_kp(int kernel, double singularity, double alpha) {
-  require(kernel == H2DEV_KERNEL_LAPLACE || kernel == H2DEV_KERNEL_YUKAWA, "unknown kernel");
+  require(kernel == H2DEV_KERNEL_LAPLACE || kernel == H2DEV_KERNEL_YUKAWA || kernel == H2DEV_KERNEL_QUADRATIC,
+          "unknown kernel");
   require(singularity != 0., "singularity must be nonzero");
   KernelParams kp;
   kp.kind = kernel;

@@ -152,6 +152,11 @@ def Yukawa3D(s: float = 1.0, a: float = 1.0) -> Kernel:
     return Kernel(L.KERNEL_YUKAWA, s, a)
 
 
+def Quadratic(s: float = 1.0, a: float = 1.0) -> Kernel:
+    """d^2 + a off the diagonal: exactly low-rank off-diagonal blocks (ULV exactness checks)."""
+    return Kernel(L.KERNEL_QUADRATIC, s, a)
+
+
 def _as_cols(X: np.ndarray):
     """(n,) or (n, nrhs) float64 -> Fortran-ordered 2-D view + nrhs + ld."""
     if X.ndim == 1:

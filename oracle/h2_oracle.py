@@ -115,7 +115,7 @@ def xbody_uniform(n: int) -> np.ndarray:
 # Kernels (kernel.hpp:28-50, kernel.cpp:71-85)
 # --------------------------------------------------------------------------
 
-LAPLACE, YUKAWA = 0, 1
+LAPLACE, YUKAWA, QUADRATIC = 0, 1, 2
 
 
 @dataclass
@@ -130,6 +130,9 @@ class Kernel:
                 v = 1.0 / d
             elif self.kind == YUKAWA:
                 v = np.exp(-self.alpha * d) / d
+            elif self.kind == QUADRATIC:
+                # not a reference kernel: exactly low-rank off-diagonal blocks
+                v = d * d + self.alpha
             else:
                 raise ValueError("kernel kind")
         return np.where(d == 0.0, 1.0 / self.singularity, v)

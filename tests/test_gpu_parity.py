@@ -274,3 +274,28 @@ def test_ragged_leaves_and_full_far_lists(handle):
     y = x.copy()
     A.matVecMul(y)
     assert rel(y, Ao.matvec(x)) < 1e-9
+
+
+def test_ulv_exact_inverse_low_rank_kernel_multilevel(handle):
+    """K = d^2 + 1 (exactly low-rank off-diagonal blocks): the device ULV is an
+    exact inverse through every level under strong admissibility, in FP64."""
+    N, leaf, theta, rank = 4096, 128, 2.0, 16
+    b, t, cells, L = problem(N, leaf)
+    k = m.Quadratic(1.0 / 50.0, 1.0)
+    M = m.H2MatrixSolver(handle, k, 0.0, rank, 0, t, theta, b)
+    xt = m.uniform_rhs(N)
+    A = O.gen_matrix(O.Kernel(O.QUADRATIC, 1.0 / 50.0, 1.0), b, b)
+    B = A @ xt
+    y = xt.copy()
+    M.matVecMul(y)
+    assert rel(y, B) < 1e-12
+    M.factorizeM()
+    z = B.copy()
+    M.solvePrecondition(z)
+    assert rel(z, xt) < 1e-9
+    # FP32 storage: exact up to single precision
+    M32 = m.H2MatrixSolver(handle, k, 0.0, rank, 0, t, theta, b, precision=m.FP32)
+    M32.factorizeM()
+    z = B.copy()
+    M32.solvePrecondition(z)
+    assert rel(z, xt) < 5e-3
