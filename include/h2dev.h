@@ -60,6 +60,15 @@ int64_t h2_levels_for(int64_t nbodies, int64_t leaf);
 int h2dev_handle_create(int device, h2dev_handle_t* out);
 int h2dev_handle_destroy(h2dev_handle_t h);
 int h2dev_handle_synchronize(h2dev_handle_t h);
+/* Handle options (apply to solvers created afterwards on this handle).
+ * H2DEV_OPT_BASIS: 0 (default) forms fixed-rank orthogonal bases from the
+ * Gram matrix of the far samples with a pivoted Cholesky (same pivots and R
+ * as the column-pivoted QR in exact arithmetic); 1 uses the Householder
+ * sample-tile QR + Eigen-rule column-pivoted QR for every basis, the
+ * reference's own sequence (h2matrix.cpp:76-89).  Threshold (operator) bases
+ * always use the Householder path. */
+enum { H2DEV_OPT_BASIS = 0 };
+int h2dev_set_option(h2dev_handle_t h, int option, int64_t value);
 
 /* ---- solver (solver.hpp:11-47 H2MatrixSolver) ------------------------ */
 
@@ -107,6 +116,13 @@ int h2dev_solve_gmres(h2dev_solver_t A, h2dev_solver_t M, double tol, int64_t nr
 int h2dev_solve_gmres_device(h2dev_solver_t A, h2dev_solver_t M, double tol, int64_t nrhs, double* dX,
                              const double* dB, int64_t ld, int64_t inner, int64_t outer, int early_exit,
                              double* resid, int64_t* iters);
+
+/* H2MatrixSolver::solveRelErr (solver.cpp:276-285) for each of nrhs
+ * columns of device arrays X and ref (leading dimension ld):
+ * err[c] = sqrt(sum (x - ref)^2 / sum ref^2), written to host memory.  The
+ * per-chunk partial sums live in a device scratch buffer allocated per call. */
+int h2dev_solve_rel_err_device(h2dev_handle_t h, int64_t n, int64_t nrhs, const double* dX, const double* dRef,
+                               int64_t ld, double* err);
 
 /* ---- dense kernel access (kernel.cpp:71-85 gen_matrix; main.cpp:83-84) */
 

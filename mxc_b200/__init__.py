@@ -5,4 +5,4 @@ A drop-in for delta-leader/mxc's solver path: the C ABI in include/h2dev.h
 """
 from ._lib import (FP32, FP64, KERNEL_LAPLACE, KERNEL_QUADRATIC, KERNEL_YUKAWA, H2DevError, LIB_PATH, lib)  # noqa: F401
 from .solver import (H2MatrixSolver, Handle, Kernel, Laplace3D, Quadratic, Tree, Yukawa3D, build_tree,  # noqa: F401
-                     dense_matvec, gen_block, levels_for, pair_csr, uniform_rhs, uniform_unit_cube_rnd)
+                     dense_matvec, gen_block, levels_for, pair_csr, rel_err_device, uniform_rhs, uniform_unit_cube_rnd)

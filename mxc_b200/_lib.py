@@ -25,6 +25,9 @@ KERNEL_QUADRATIC = 2
 FP64 = 0
 FP32 = 1
 
+OPT_BASIS = 0
+BASIS_GRAM, BASIS_HOUSEHOLDER = 0, 1
+
 EXPORT_S, EXPORT_Q, EXPORT_R, EXPORT_A, EXPORT_C = range(5)
 
 _i64 = C.c_int64
@@ -42,6 +45,7 @@ SIGNATURES = {
     "h2dev_handle_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
     "h2dev_handle_destroy": (C.c_int, [_vp]),
     "h2dev_handle_synchronize": (C.c_int, [_vp]),
+    "h2dev_set_option": (C.c_int, [_vp, C.c_int, _i64]),
     "h2dev_solver_create": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double, C.c_double, _i64, _i64, _i64,
                                       _vp, _vp, _vp, _vp, C.c_double, _vp, _i64, _i64, _i64, C.c_int,
                                       C.POINTER(_vp)]),
@@ -57,6 +61,7 @@ SIGNATURES = {
                                     _vp]),
     "h2dev_solve_gmres_device": (C.c_int, [_vp, _vp, C.c_double, _i64, _vp, _vp, _i64, _i64, _i64, C.c_int,
                                            _vp, _vp]),
+    "h2dev_solve_rel_err_device": (C.c_int, [_vp, _i64, _i64, _vp, _vp, _i64, _vp]),
     "h2dev_gen_block": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double, _vp, _i64, _vp, _i64, _vp]),
     "h2dev_dense_matvec": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double, _vp, _i64, _i64, _vp, _vp, _i64]),
     "h2dev_dense_matvec_device": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double, _vp, _i64, _i64, _vp, _vp,

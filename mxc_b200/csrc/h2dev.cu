@@ -10,6 +10,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "h2dev.h"
@@ -29,6 +30,7 @@ struct h2dev_handle_s {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool prof = false;
+  int basis_mode = 0;  // 0: Gram + pivoted Cholesky for fixed-rank bases; 1: Householder TSQR everywhere
   std::vector<ProfRec> recs;
   std::vector<cudaEvent_t> pool;
   cudaEvent_t t0 = nullptr, t1 = nullptr;
@@ -481,42 +483,47 @@ class Solver : public SolverBase {
       d_nonzero.alloc(nodes);
       d_maxpiv.alloc(nodes);
       lv.d_ranks.alloc(nodes);
-      DVec<T> Rws;
-      Rws.alloc(lv.qoff[nodes]);
-      Rws.zero(st());
       const double e = level_epi(l);
       const bool orth = 1. <= e;
-      {
-        double fl = 0.;
-        for (i64 i = 0; i < nodes; i++) {
-          double S = (double)(soff[i + 1] - soff[i]), Md = (double)lv.dims[i];
-          fl += S >= Md ? 2. * S * Md * Md - 2. / 3. * Md * Md * Md : 2. * Md * S * S - 2. / 3. * S * S * S;
-        }
-        Prof pf("sample_tsqr", fl, (double)sidx.size() * 28.);
-        ck(launch_sample_tsqr<T>(kp, bodies.p, lv.pts.p, lv.d_xoff.p, lv.d_dims.p, d_sidx.p, d_soff.p, Rws.p,
-                                 lv.d_qoff.p, (int)nodes, (int)lv.maxM, st()),
-           "sample_tsqr");
-      }
       i64 cap = -1;
       if (e >= 1.) cap = (i64)std::floor(e);
-      {
-        double fl = 0.;
-        for (i64 i = 0; i < nodes; i++) {
-          double K = (double)krows[i], Md = (double)lv.dims[i];
-          double st_ = std::min(K, Md);
-          if (cap >= 0) st_ = std::min(st_, (double)cap);
-          fl += 4. * K * Md * st_ - 2. * (K + Md) * st_ * st_ + 4. / 3. * st_ * st_ * st_;
+      if (orth && h->basis_mode == 0) {
+        basis_gram(lv, low == nullptr, soff, d_sidx, d_krows, d_perm, d_maxpiv, d_nonzero, e, cap);
+      } else {
+        DVec<T> Rws;
+        Rws.alloc(lv.qoff[nodes]);
+        Rws.zero(st());
+        {
+          double fl = 0.;
+          for (i64 i = 0; i < nodes; i++) {
+            double S = (double)(soff[i + 1] - soff[i]), Md = (double)lv.dims[i];
+            fl += S >= Md ? 2. * S * Md * Md - 2. / 3. * Md * Md * Md : 2. * Md * S * S - 2. / 3. * S * S * S;
+          }
+          Prof pf("sample_tsqr", fl, (double)sidx.size() * 28.);
+          ck(launch_sample_tsqr<T>(kp, bodies.p, lv.pts.p, lv.d_xoff.p, lv.d_dims.p, d_sidx.p, d_soff.p, Rws.p,
+                                   lv.d_qoff.p, (int)nodes, (int)lv.maxM, st()),
+             "sample_tsqr");
         }
-        Prof pf("cpqr", fl, 0.);
-        ck(launch_cpqr<T>(lv.d_dims.p, d_krows.p, Rws.p, lv.d_qoff.p, d_perm.p, lv.d_xoff.p, d_maxpiv.p,
-                          d_nonzero.p, cap, (int)nodes, (int)lv.maxM, st()),
-           "cpqr");
+        {
+          double fl = 0.;
+          for (i64 i = 0; i < nodes; i++) {
+            double K = (double)krows[i], Md = (double)lv.dims[i];
+            double st_ = std::min(K, Md);
+            if (cap >= 0) st_ = std::min(st_, (double)cap);
+            fl += 4. * K * Md * st_ - 2. * (K + Md) * st_ * st_ + 4. / 3. * st_ * st_ * st_;
+          }
+          Prof pf("cpqr", fl, 0.);
+          ck(launch_cpqr<T>(lv.d_dims.p, d_krows.p, Rws.p, lv.d_qoff.p, d_perm.p, lv.d_xoff.p, d_maxpiv.p,
+                            d_nonzero.p, cap, (int)nodes, (int)lv.maxM, st()),
+             "cpqr");
+        }
+        Prof pfin("basis_finish", 0., (double)lv.qoff[nodes] * sizeof(T) * 3.);
+        ck(launch_basis_finish<T>(lv.d_dims.p, d_krows.p, Rws.p, lv.Q.p, lv.R.p, lv.d_qoff.p, d_perm.p,
+                                  lv.d_xoff.p, d_maxpiv.p, d_nonzero.p, lv.pts.p, lv.d_ranks.p, e, orth ? 1 : 0,
+                                  low ? 0 : 1, (int)nodes, (int)lv.maxM, st()),
+           "basis_finish");
+        ck(cudaStreamSynchronize(st()), "sync");
       }
-      Prof pfin("basis_finish", 0., (double)lv.qoff[nodes] * sizeof(T) * 3.);
-      ck(launch_basis_finish<T>(lv.d_dims.p, d_krows.p, Rws.p, lv.Q.p, lv.R.p, lv.d_qoff.p, d_perm.p, lv.d_xoff.p,
-                                d_maxpiv.p, d_nonzero.p, lv.pts.p, lv.d_ranks.p, e, orth ? 1 : 0, low ? 0 : 1,
-                                (int)nodes, (int)lv.maxM, st()),
-         "basis_finish");
       lv.ranks = lv.d_ranks.download(st());
     } else {
       lv.d_ranks.alloc(nodes);
@@ -583,6 +590,101 @@ class Solver : public SolverBase {
         ck(cudaStreamSynchronize(st()), "sync");
       }
     }
+  }
+
+  // Fixed-rank orthogonal mode: far-sample block XF generated into HBM in
+  // bounded chunks, Gram matrix G = XF^T XF by the segmented GEMM (FP64),
+  // pivoted Cholesky of G (the pivots and R rows of ColPivHouseholderQR in
+  // exact arithmetic, h2matrix.cpp:78-89), then the same ID / completion step
+  // as the Householder path, in FP64, converted to T at the end.
+  void basis_gram(Level<T>& lv, bool leaf, const std::vector<i64>& soff, DVec<int>& d_sidx, DVec<i64>& d_krows,
+                  DVec<int>& d_perm, DVec<double>& d_maxpiv, DVec<int>& d_nonzero, double e, i64 cap) {
+    const i64 nodes = lv.nodes;
+    DVec<double> spts, G, XF, Rws;
+    spts.alloc(std::max<i64>(3, 3 * soff[nodes]));
+    ck(launch_gather_points(bodies.p, d_sidx.p, soff[nodes], spts.p, st()), "gather samples");
+    G.alloc(lv.qoff[nodes]);
+    const i64 cap_elems = (i64)1 << 28;
+    std::vector<std::pair<i64, i64>> chunks;
+    i64 maxchunk = 1;
+    for (i64 i0 = 0; i0 < nodes;) {
+      i64 used = 0, i1 = i0;
+      while (i1 < nodes) {
+        i64 sz = (soff[i1 + 1] - soff[i1]) * lv.dims[i1];
+        if (used > 0 && used + sz > cap_elems) break;
+        used += sz;
+        i1++;
+      }
+      chunks.emplace_back(i0, i1);
+      maxchunk = std::max(maxchunk, used);
+      i0 = i1;
+    }
+    XF.alloc(maxchunk);
+    for (auto& ch : chunks) {
+      std::vector<GenTask> gt;
+      GemmPlan<double> gp;
+      gp.name = "gemm_gram";
+      i64 o = 0;
+      for (i64 i = ch.first; i < ch.second; i++) {
+        const i64 S = soff[i + 1] - soff[i], M = lv.dims[i];
+        if (S == 0 || M == 0) continue;
+        GenTask t;
+        t.bi = spts.p + 3 * soff[i];
+        t.bj = lv.pts.p + 3 * lv.xoff[i];
+        t.m = (int)S;
+        t.n = (int)M;
+        t.out_off = o;
+        t.ld = S;
+        gt.push_back(t);
+        gp.add_task(G.p + lv.qoff[i], M, (int)M, (int)M, 0.);
+        gp.add_entry(XF.p + o, S, 1, XF.p + o, S, 0, (int)S, 1.);
+        o += S * M;
+      }
+      if (gt.empty()) continue;
+      DVec<GenTask> dg;
+      dg.upload(gt);
+      {
+        Prof pf("gen_samples", 0., 8. * o);
+        ck(launch_gen_blocks<double>(kp, dg.p, (int)gt.size(), 4, XF.p, st(), 1), "gen samples");
+      }
+      gp.finalize();
+      gp.run(st());
+      ck(cudaStreamSynchronize(st()), "sync");
+    }
+    Rws.alloc(lv.qoff[nodes]);
+    Rws.zero(st());
+    {
+      double fl = 0.;
+      for (i64 i = 0; i < nodes; i++) {
+        double Md = (double)lv.dims[i], st_ = std::min(Md, (double)(cap >= 0 ? cap : lv.dims[i]));
+        fl += 2. * (Md * Md * st_ - Md * st_ * st_ + st_ * st_ * st_ / 3.);
+      }
+      Prof pf("pivchol", fl, 0.);
+      ck(launch_pivchol(lv.d_dims.p, d_krows.p, G.p, Rws.p, lv.d_qoff.p, d_perm.p, lv.d_xoff.p, cap, (int)nodes,
+                        (int)lv.maxM, st()),
+         "pivchol");
+    }
+    Prof pfin("basis_finish", 0., (double)lv.qoff[nodes] * 24.);
+    if (std::is_same<T, double>::value) {
+      ck(launch_basis_finish<double>(lv.d_dims.p, d_krows.p, Rws.p, reinterpret_cast<double*>(lv.Q.p),
+                                     reinterpret_cast<double*>(lv.R.p), lv.d_qoff.p, d_perm.p, lv.d_xoff.p,
+                                     d_maxpiv.p, d_nonzero.p, lv.pts.p, lv.d_ranks.p, e, 1, leaf ? 1 : 0,
+                                     (int)nodes, (int)lv.maxM, st()),
+         "basis_finish");
+    } else {
+      DVec<double> Qd, Rd;
+      Qd.alloc(lv.qoff[nodes]);
+      Rd.alloc(lv.qoff[nodes]);
+      Rd.zero(st());
+      ck(launch_convert<T, double>(lv.Q.p, Qd.p, lv.qoff[nodes], st()), "convert");
+      ck(launch_basis_finish<double>(lv.d_dims.p, d_krows.p, Rws.p, Qd.p, Rd.p, lv.d_qoff.p, d_perm.p,
+                                     lv.d_xoff.p, d_maxpiv.p, d_nonzero.p, lv.pts.p, lv.d_ranks.p, e, 1,
+                                     leaf ? 1 : 0, (int)nodes, (int)lv.maxM, st()),
+         "basis_finish");
+      ck(launch_convert<double, T>(Qd.p, lv.Q.p, lv.qoff[nodes], st()), "convert");
+      ck(launch_convert<double, T>(Rd.p, lv.R.p, lv.qoff[nodes], st()), "convert");
+    }
+    ck(cudaStreamSynchronize(st()), "sync");
   }
 
   // ------------------------------------------------------------ vectors
@@ -1689,6 +1791,19 @@ int h2dev_probe_fma_peak(h2dev_handle_t h, int precision, double* tflops) {
   H2_API_END
 }
 
+int h2dev_set_option(h2dev_handle_t h, int option, int64_t value) {
+  H2_API_BEGIN
+  require(h != nullptr, "null handle");
+  if (option == H2DEV_OPT_BASIS) {
+    require(value == 0 || value == 1, "basis option must be 0 or 1");
+    h->basis_mode = (int)value;
+    return H2DEV_OK;
+  }
+  require(false, "unknown option");
+  return H2DEV_ERR_ARG;
+  H2_API_END
+}
+
 int h2dev_timer_start(h2dev_handle_t h) {
   H2_API_BEGIN
   require(h != nullptr, "null handle");
@@ -1707,6 +1822,24 @@ int h2dev_timer_stop(h2dev_handle_t h, double* ms) {
   float e = 0.f;
   ck(cudaEventElapsedTime(&e, h->t0, h->t1), "elapsed");
   *ms = e;
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_solve_rel_err_device(h2dev_handle_t h, int64_t n, int64_t nrhs, const double* dX, const double* dRef,
+                                int64_t ld, double* err) {
+  H2_API_BEGIN
+  require(h && dX && dRef && err && n > 0 && nrhs > 0 && ld >= n, "bad arguments");
+  CurHandle ch(h);
+  DVec<double> partial, out;
+  partial.alloc((size_t)2 * relerr_chunks(n) * nrhs);
+  out.alloc(nrhs);
+  {
+    Prof pf("rel_err", 3. * n * nrhs, 16. * n * nrhs);
+    ck(launch_relerr(dX, dRef, n, ld, (int)nrhs, partial.p, out.p, h->stream), "rel_err");
+  }
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  ck(cudaMemcpy(err, out.p, sizeof(double) * nrhs, cudaMemcpyDeviceToHost), "D2H");
   return H2DEV_OK;
   H2_API_END
 }

@@ -481,3 +481,106 @@ INST(float)
 #undef INST
 
 }  // namespace h2b
+
+namespace h2b {
+
+// Right-looking pivoted Cholesky of the Gram matrix G = XF^T XF (M x M,
+// symmetric, row = column major) of each box, stopped after ``steps``
+// pivots.  The pivot is the largest remaining Schur-complement diagonal
+// (the squared column norm that a column-pivoted QR of XF would pick), so
+// the pivots and the rows of R equal those of ColPivHouseholderQR in exact
+// arithmetic (h2matrix.cpp:84); R goes to Rws row-major in pivoted column
+// order, exactly where k_cpqr leaves it, for k_basis_finish.
+__global__ void __launch_bounds__(256) k_pivchol(const i64* __restrict__ dims, const i64* __restrict__ krows,
+                                                 double* __restrict__ G, double* __restrict__ Rws,
+                                                 const i64* __restrict__ qoff, int* __restrict__ perm_out,
+                                                 const i64* __restrict__ xoff, i64 step_cap) {
+  const int box = blockIdx.x;
+  const int M = (int)dims[box];
+  const int K = (int)krows[box];
+  if (M == 0 || K == 0) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  int* perm = reinterpret_cast<int*>(smem_raw);
+  __shared__ double red_v[32];
+  __shared__ int red_i[32];
+  double* g = G + qoff[box];
+  double* R = Rws + qoff[box];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  int steps = K < M ? K : M;
+  if (step_cap >= 0 && step_cap < steps) steps = (int)step_cap;
+  for (int c = tid; c < M; c += nt) perm[c] = c;
+  __syncthreads();
+  for (int k = 0; k < steps; k++) {
+    double bv = -1.;
+    int bi = 0x7fffffff;
+    for (int j = k + tid; j < M; j += nt) {
+      double v = g[(i64)j * M + j];
+      if (v > bv) { bv = v; bi = j; }
+    }
+    argmax_first(bv, bi, red_v, red_i);
+    if (bi != k) {
+      for (int c = tid; c < M; c += nt) {  // swap rows k, bi
+        double t = g[(i64)k * M + c];
+        g[(i64)k * M + c] = g[(i64)bi * M + c];
+        g[(i64)bi * M + c] = t;
+      }
+      __syncthreads();
+      for (int r = tid; r < M; r += nt) {  // swap columns k, bi
+        double t = g[(i64)r * M + k];
+        g[(i64)r * M + k] = g[(i64)r * M + bi];
+        g[(i64)r * M + bi] = t;
+      }
+      for (int r = tid; r < k; r += nt) {  // earlier rows of R follow the column swap
+        double t = R[(i64)r * M + k];
+        R[(i64)r * M + k] = R[(i64)r * M + bi];
+        R[(i64)r * M + bi] = t;
+      }
+      if (tid == 0) {
+        int t = perm[k]; perm[k] = perm[bi]; perm[bi] = t;
+      }
+    }
+    __syncthreads();
+    const double d = g[(i64)k * M + k];
+    const double rkk = d > 0. ? sqrt(d) : 0.;
+    const double inv = rkk > 0. ? 1. / rkk : 0.;
+    for (int j = k + tid; j < M; j += nt) R[(i64)k * M + j] = (j == k) ? rkk : g[(i64)k * M + j] * inv;
+    __syncthreads();
+    const int rem = M - k - 1;
+    const i64 tot = (i64)rem * rem;
+    for (i64 e = tid; e < tot; e += nt) {
+      int i = k + 1 + (int)(e / rem), j = k + 1 + (int)(e % rem);
+      g[(i64)i * M + j] -= R[(i64)k * M + i] * R[(i64)k * M + j];
+    }
+    __syncthreads();
+  }
+  for (int c = tid; c < M; c += nt) perm_out[xoff[box] + c] = perm[c];
+}
+
+cudaError_t launch_pivchol(const i64* dims, const i64* krows, double* G, double* Rws, const i64* qoff, int* perm,
+                           const i64* xoff, i64 step_cap, int nboxes, int maxM, cudaStream_t st) {
+  if (nboxes == 0) return cudaSuccess;
+  size_t smem = sizeof(int) * (size_t)maxM + 16;
+  k_pivchol<<<nboxes, 256, smem, st>>>(dims, krows, G, Rws, qoff, perm, xoff, step_cap);
+  return cudaGetLastError();
+}
+
+// Gathers each box's far-sample bodies into one contiguous array.
+__global__ void k_gather_points(const double* __restrict__ bodies, const int* __restrict__ idx, i64 n,
+                                double* __restrict__ out) {
+  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+    const double* p = bodies + 3 * (i64)idx[i];
+    out[3 * i] = p[0];
+    out[3 * i + 1] = p[1];
+    out[3 * i + 2] = p[2];
+  }
+}
+
+cudaError_t launch_gather_points(const double* bodies, const int* idx, i64 n, double* out, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  int grid = (int)((n + 255) / 256);
+  grid = grid > 4096 ? 4096 : grid;
+  k_gather_points<<<grid, 256, 0, st>>>(bodies, idx, n, out);
+  return cudaGetLastError();
+}
+
+}  // namespace h2b

@@ -8,7 +8,7 @@ namespace h2b {
 
 // Column-major blocks K(bi[r], bj[c]); grid.x = task, grid.y = chunk of
 // the block's elements.  Consecutive threads write consecutive rows.
-template <typename T>
+template <typename T, bool FAST>
 __global__ void __launch_bounds__(256) k_gen_blocks(KernelParams kp, const GenTask* __restrict__ tasks, T* __restrict__ out) {
   GenTask t = tasks[blockIdx.x];
   i64 total = (i64)t.m * t.n;
@@ -20,20 +20,26 @@ __global__ void __launch_bounds__(256) k_gen_blocks(KernelParams kp, const GenTa
     int r = (int)(e % t.m), c = (int)(e / t.m);
     const double* a = t.bi + 3 * r;
     const double* b = t.bj + 3 * c;
-    o[r + (i64)c * t.ld] = (T)kernel_exact(kp, a[0] - b[0], a[1] - b[1], a[2] - b[2]);
+    o[r + (i64)c * t.ld] = FAST ? (T)kernel_fast(kp, a[0] - b[0], a[1] - b[1], a[2] - b[2])
+                                : (T)kernel_exact(kp, a[0] - b[0], a[1] - b[1], a[2] - b[2]);
   }
 }
 
 template <typename T>
 cudaError_t launch_gen_blocks(const KernelParams& kp, const GenTask* d_tasks, int ntasks, int chunks, T* out,
-                              cudaStream_t st) {
+                              cudaStream_t st, int fast) {
   if (ntasks == 0) return cudaSuccess;
   dim3 grid(ntasks, chunks < 1 ? 1 : chunks);
-  k_gen_blocks<T><<<grid, 256, 0, st>>>(kp, d_tasks, out);
+  if (fast)
+    k_gen_blocks<T, true><<<grid, 256, 0, st>>>(kp, d_tasks, out);
+  else
+    k_gen_blocks<T, false><<<grid, 256, 0, st>>>(kp, d_tasks, out);
   return cudaGetLastError();
 }
-template cudaError_t launch_gen_blocks<double>(const KernelParams&, const GenTask*, int, int, double*, cudaStream_t);
-template cudaError_t launch_gen_blocks<float>(const KernelParams&, const GenTask*, int, int, float*, cudaStream_t);
+template cudaError_t launch_gen_blocks<double>(const KernelParams&, const GenTask*, int, int, double*, cudaStream_t,
+                                               int);
+template cudaError_t launch_gen_blocks<float>(const KernelParams&, const GenTask*, int, int, float*, cudaStream_t,
+                                              int);
 
 // Y = A_dense X for up to NR right-hand sides per pass.  Each thread owns a
 // row; columns stream through shared memory in tiles of 256 bodies.

@@ -212,3 +212,53 @@ cudaError_t launch_fma_probe(int precision, int blocks, int iters, void* out, cu
 }
 
 }  // namespace h2b
+
+namespace h2b {
+
+// solveRelErr (solver.cpp:276-285) per column: partial sums of (x - ref)^2
+// and ref^2 over row chunks, then a fixed-order final sum (deterministic).
+constexpr i64 RELERR_ROWS = 16384;
+int relerr_chunks(i64 n) { return (int)((n + RELERR_ROWS - 1) / RELERR_ROWS); }
+
+__global__ void __launch_bounds__(256) k_relerr_partial(const double* __restrict__ X, const double* __restrict__ ref,
+                                                        i64 n, i64 ld, double* __restrict__ partial) {
+  __shared__ double red[32];
+  const int g = blockIdx.x, c = blockIdx.y, nch = gridDim.x;
+  const i64 r0 = (i64)g * RELERR_ROWS, r1 = r0 + RELERR_ROWS < n ? r0 + RELERR_ROWS : n;
+  const double* x = X + (i64)c * ld;
+  const double* f = ref + (i64)c * ld;
+  double se = 0., sr = 0.;
+  for (i64 r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+    double d = x[r] - f[r];
+    se += d * d;
+    sr += f[r] * f[r];
+  }
+  se = BlockReduce<double>::sum(se, red);
+  sr = BlockReduce<double>::sum(sr, red);
+  if (threadIdx.x == 0) {
+    partial[(i64)c * 2 * nch + 2 * g] = se;
+    partial[(i64)c * 2 * nch + 2 * g + 1] = sr;
+  }
+}
+
+__global__ void k_relerr_final(const double* __restrict__ partial, int nch, int nrhs, double* __restrict__ out) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nrhs) return;
+  double se = 0., sr = 0.;
+  for (int g = 0; g < nch; g++) {
+    se += partial[(i64)c * 2 * nch + 2 * g];
+    sr += partial[(i64)c * 2 * nch + 2 * g + 1];
+  }
+  out[c] = sqrt(se / sr);
+}
+
+cudaError_t launch_relerr(const double* X, const double* ref, i64 n, i64 ld, int nrhs, double* partial, double* out,
+                          cudaStream_t st) {
+  const int nch = relerr_chunks(n);
+  dim3 grid(nch, nrhs);
+  k_relerr_partial<<<grid, 256, 0, st>>>(X, ref, n, ld, partial);
+  k_relerr_final<<<(nrhs + 127) / 128, 128, 0, st>>>(partial, nch, nrhs, out);
+  return cudaGetLastError();
+}
+
+}  // namespace h2b

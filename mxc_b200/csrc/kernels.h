@@ -17,7 +17,7 @@ struct GenTask {
 };
 template <typename T>
 cudaError_t launch_gen_blocks(const KernelParams& kp, const GenTask* d_tasks, int ntasks, int chunks, T* out,
-                              cudaStream_t st);
+                              cudaStream_t st, int fast = 0);
 cudaError_t launch_dense_matvec(const KernelParams& kp, const double* bodies, i64 n, const double* X, i64 ldx,
                                 double* Y, i64 ldy, int nrhs, cudaStream_t st);
 
@@ -34,6 +34,10 @@ cudaError_t launch_basis_finish(const i64* dims, const i64* krows, T* Rws, T* Q,
                                 const int* perm, const i64* xoff, const double* maxpiv, const int* nonzero,
                                 double* pts, i64* ranks, double epi, int orth, int qin_identity, int nboxes,
                                 int maxM, cudaStream_t st);
+
+cudaError_t launch_pivchol(const i64* dims, const i64* krows, double* G, double* Rws, const i64* qoff, int* perm,
+                           const i64* xoff, i64 step_cap, int nboxes, int maxM, cudaStream_t st);
+cudaError_t launch_gather_points(const double* bodies, const int* idx, i64 n, double* out, cudaStream_t st);
 
 // ---------------------------------------------------------------- gemm
 // C_task = beta * C_task + sum_{e in task} alpha_e * op(A_e) * op(B_e)
@@ -107,6 +111,10 @@ cudaError_t launch_axpby(double* y, const double* x, double a, double b, i64 n, 
 cudaError_t launch_residual_norm_finish(const double* nrm2, const double* normb, double* resid, int nrhs,
                                         cudaStream_t st);
 
+int relerr_chunks(i64 n);
+// partial: 2 * relerr_chunks(n) * nrhs doubles of scratch; out: nrhs doubles (device)
+cudaError_t launch_relerr(const double* X, const double* ref, i64 n, i64 ld, int nrhs, double* partial, double* out,
+                          cudaStream_t st);
 cudaError_t launch_fma_probe(int precision, int blocks, int iters, void* out, cudaStream_t st);
 
 }  // namespace h2b

@@ -88,6 +88,10 @@ class Handle:
     def synchronize(self):
         L.check(L.lib().h2dev_handle_synchronize(self.h), "h2dev_handle_synchronize")
 
+    def set_basis_mode(self, mode: int):
+        """BASIS_GRAM (default) or BASIS_HOUSEHOLDER for fixed-rank bases of solvers created next."""
+        L.check(L.lib().h2dev_set_option(self.h, L.OPT_BASIS, mode), "h2dev_set_option")
+
     def profile(self, on: bool = True):
         L.check(L.lib().h2dev_profile_enable(self.h, 1 if on else 0), "h2dev_profile_enable")
 
@@ -278,6 +282,14 @@ class H2MatrixSolver:
             self.close()
         except Exception:
             pass
+
+
+def rel_err_device(handle: Handle, xptr: int, refptr: int, n: int, nrhs: int, ld: int) -> np.ndarray:
+    """solveRelErr (solver.cpp:276-285) of nrhs device columns; returns host values."""
+    out = np.zeros(nrhs)
+    L.check(L.lib().h2dev_solve_rel_err_device(handle.h, n, nrhs, C.c_void_p(xptr), C.c_void_p(refptr), ld, _ptr(out)),
+            "h2dev_solve_rel_err_device")
+    return out
 
 
 def gen_block(handle: Handle, kernel: Kernel, bi: np.ndarray, bj: np.ndarray) -> np.ndarray:

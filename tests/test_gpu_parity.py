@@ -119,9 +119,15 @@ def test_operator_matvec_multi_rhs(op2048):
 
 @pytest.fixture(scope="module")
 def pre2048(handle):
+    """Preconditioner built with the reference's own sequence (Householder
+    sample QR + Eigen-rule column-pivoted QR)."""
     N = 2048
     b, t, cells, L = problem(N)
-    M = m.H2MatrixSolver(handle, m.Laplace3D(), 0.0, 100, 0, t, 2.0, b, samples=2000)
+    handle.set_basis_mode(m._lib.BASIS_HOUSEHOLDER)
+    try:
+        M = m.H2MatrixSolver(handle, m.Laplace3D(), 0.0, 100, 0, t, 2.0, b, samples=2000)
+    finally:
+        handle.set_basis_mode(m._lib.BASIS_GRAM)
     Mo = O.H2MatrixSolver(O.Kernel(), 0.0, 100, 0, cells, 2.0, b.copy(), L, 2000)
     return M, Mo, b, t, cells, L
 
@@ -299,3 +305,49 @@ def test_ulv_exact_inverse_low_rank_kernel_multilevel(handle):
     z = B.copy()
     M32.solvePrecondition(z)
     assert rel(z, xt) < 5e-3
+
+
+
+def test_gram_basis_matches_householder_basis_and_oracle(handle, pre2048):
+    """Default fixed-rank path (Gram + pivoted Cholesky) selects the same
+    skeletons as the column-pivoted QR and gives the same preconditioner."""
+    Mh, Mo, b, t, cells, L = pre2048
+    Mg = m.H2MatrixSolver(handle, m.Laplace3D(), 0.0, 100, 0, t, 2.0, b, samples=2000)
+    for lvl in range(L + 1):
+        dg, rg = Mg.level_dims(lvl)
+        assert np.array_equal(dg, Mo.A[lvl].Dims) and np.array_equal(rg, Mo.A[lvl].DimsLr)
+    Sg = Mg.export(L, m._lib.EXPORT_S).reshape(-1, 3)
+    dims, ranks = Mg.level_dims(L)
+    off, same = 0, 0
+    for i, (d, r) in enumerate(zip(dims, ranks)):
+        same += np.array_equal(Sg[off:off + r], Mo.A[L].S[i][:r])
+        off += d
+    assert same >= len(dims) - 1
+    Qg = Mg.export(L, m._lib.EXPORT_Q)
+    Qo = np.concatenate([q.ravel(order="F") for q in Mo.A[L].Q])
+    assert rel(Qg, Qo) < 1e-7
+    Mg.factorizeM()
+    if Mh.info is None:
+        Mh.factorizeM()
+        Mo.factorize()
+    x = m.uniform_rhs(b.shape[0])
+    zg, zh = x.copy(), x.copy()
+    Mg.solvePrecondition(zg)
+    Mh.solvePrecondition(zh)
+    assert rel(zg, zh) < 1e-5
+
+
+def test_rel_err_device_matches_host(handle):
+    import torch
+
+    rng = np.random.default_rng(9)
+    n, nrhs = 70001, 3
+    X = rng.random((nrhs, n))
+    R = X + 1e-6 * rng.standard_normal((nrhs, n))
+    dX = torch.from_numpy(X).cuda()
+    dR = torch.from_numpy(R).cuda()
+    torch.cuda.synchronize()
+    got = m.rel_err_device(handle, dX.data_ptr(), dR.data_ptr(), n, nrhs, n)
+    for c in range(nrhs):
+        exp = m.H2MatrixSolver.solveRelErr(X[c], R[c])
+        assert abs(got[c] - exp) <= 1e-12 * exp
