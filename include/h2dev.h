@@ -124,6 +124,23 @@ int h2dev_solve_gmres_device(h2dev_solver_t A, h2dev_solver_t M, double tol, int
 int h2dev_solve_rel_err_device(h2dev_handle_t h, int64_t n, int64_t nrhs, const double* dX, const double* dRef,
                                int64_t ld, double* err);
 
+/* No counterpart in the reference.  The same relative errors as
+ * h2dev_solve_rel_err_device, for callers that must not allocate device
+ * memory: a serving loop whose HBM is handed out entirely by its own budgeted
+ * pool (an allocation behind its back can fail or break the budget), or a
+ * latency-critical path that cannot take the device-wide synchronisation
+ * cudaMalloc / cudaFree may imply.  Nothing is allocated: the partial sums go
+ * to a fixed 16384-double (128 KiB) device array inside the library, held by
+ * every GPU that loads it until the process exits, and err[c] is written to
+ * the caller's device array dErr (nrhs doubles) asynchronously on the
+ * handle's stream.  Limit: 2 * ceil(n / 16384) * nrhs <= 16384 (for example
+ * n up to 134,217,728 with one column, 8,388,608 with 16); larger requests
+ * return H2DEV_ERR_ARG.  The first call on a device looks up the array's
+ * device address, so make it before any stream capture.  All calls share the
+ * array: calls whose work overlaps on the GPU (two streams at once) race. */
+int h2dev_solve_rel_err_device_noalloc(h2dev_handle_t h, int64_t n, int64_t nrhs, const double* dX,
+                                       const double* dRef, int64_t ld, double* dErr);
+
 /* ---- dense kernel access (kernel.cpp:71-85 gen_matrix; main.cpp:83-84) */
 
 /* out (m x n column-major) = K(bi, bj), bodies xyz-interleaved host arrays;

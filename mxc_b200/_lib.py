@@ -62,6 +62,7 @@ SIGNATURES = {
     "h2dev_solve_gmres_device": (C.c_int, [_vp, _vp, C.c_double, _i64, _vp, _vp, _i64, _i64, _i64, C.c_int,
                                            _vp, _vp]),
     "h2dev_solve_rel_err_device": (C.c_int, [_vp, _i64, _i64, _vp, _vp, _i64, _vp]),
+    "h2dev_solve_rel_err_device_noalloc": (C.c_int, [_vp, _i64, _i64, _vp, _vp, _i64, _vp]),
     "h2dev_gen_block": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double, _vp, _i64, _vp, _i64, _vp]),
     "h2dev_dense_matvec": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double, _vp, _i64, _i64, _vp, _vp, _i64]),
     "h2dev_dense_matvec_device": (C.c_int, [_vp, C.c_int, C.c_double, C.c_double, _vp, _i64, _i64, _vp, _vp,

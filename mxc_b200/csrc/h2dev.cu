@@ -1827,3 +1827,69 @@ int h2dev_solver_export(h2dev_solver_t s, int64_t level, int what, double* out) 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free solveRelErr.  Same two reduction kernels as
+// h2dev_solve_rel_err_device; only the partial-sum scratch and the output
+// differ: the scratch is a file-scope device array, the output is the
+// caller's device array.
+
+#include <cstdio>
+#include <mutex>
+
+namespace h2b {
+
+// Partial-sum scratch of h2dev_solve_rel_err_device_noalloc: 16384 doubles
+// (128 KiB).  Every GPU that loads this library keeps it until the process
+// exits.
+constexpr i64 NOALLOC_SCRATCH_DOUBLES = 16384;
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_SCRATCH_DOUBLES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static double* g_noalloc_ptr[NOALLOC_MAX_DEVICES];
+static std::mutex g_noalloc_mu;
+
+// Device address of the scratch on ``dev``.  In host code the array's name
+// only stands in for the symbol; the address is looked up once per device,
+// with that device current, and cached.
+static cudaError_t noalloc_scratch(int dev, double** out) {
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    int prev = 0;
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e != cudaSuccess) return e;
+    if (prev != dev && (e = cudaSetDevice(dev)) != cudaSuccess) return e;
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (prev != dev) cudaSetDevice(prev);
+    if (e != cudaSuccess) return e;
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return cudaSuccess;
+}
+
+}  // namespace h2b
+
+extern "C" int h2dev_solve_rel_err_device_noalloc(h2dev_handle_t h, int64_t n, int64_t nrhs, const double* dX,
+                                                  const double* dRef, int64_t ld, double* dErr) {
+  H2_API_BEGIN
+  require(h && dX && dRef && dErr && n > 0 && nrhs > 0 && ld >= n, "bad arguments");
+  const int64_t need = 2 * (int64_t)relerr_chunks(n) * nrhs;
+  if (need > NOALLOC_SCRATCH_DOUBLES) {
+    char msg[200];
+    snprintf(msg, sizeof(msg),
+             "h2dev_solve_rel_err_device_noalloc: n=%lld, nrhs=%lld needs %lld scratch doubles; the fixed limit is "
+             "%lld (2 * ceil(n / 16384) * nrhs)",
+             (long long)n, (long long)nrhs, (long long)need, (long long)NOALLOC_SCRATCH_DOUBLES);
+    throw H2Error{H2DEV_ERR_ARG, msg};
+  }
+  double* scratch = nullptr;
+  ck(noalloc_scratch(h->device, &scratch), "cudaGetSymbolAddress(scratch)");
+  // Every scratch slot the second pass reads is written by the first pass of
+  // this same call, so nothing has to be cleared between calls.
+  ck(launch_relerr(dX, dRef, n, ld, (int)nrhs, scratch, dErr, h->stream), "rel_err (no-alloc)");
+  return H2DEV_OK;
+  H2_API_END
+}
