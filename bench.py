@@ -279,7 +279,7 @@ def run_ours(a):
     name, (nl, dms, fl, by) = dom
     compute = fl > 0 and (fl / max(by, 1.0)) > 2.0
     if compute:
-        is32 = (prec == m.FP32 and name in ("sample_tsqr", "cpqr", "gemm_factor", "lu_inverse", "basis_finish"))
+        is32 = (prec == m.FP32 and name in ("sample_tsqr", "cpqr", "gemm_factor", "lu_inverse", "basis_finish", "pivchol"))
         peak = fp32_peak if is32 else fp64_peak
         achieved = fl / (dms * 1e-3) / 1e12
         roof = {"kernel": name, "bound": "fp32_simt" if is32 else "fp64_simt", "achieved": achieved, "peak": peak,

@@ -67,7 +67,10 @@ int h2dev_handle_synchronize(h2dev_handle_t h);
  * sample-tile QR + Eigen-rule column-pivoted QR for every basis, the
  * reference's own sequence (h2matrix.cpp:76-89).  Threshold (operator) bases
  * always use the Householder path. */
-enum { H2DEV_OPT_BASIS = 0 };
+/* H2DEV_OPT_SKINNY_TILED: 1 makes plans built afterwards (in this process)
+ * run every multi-right-hand-side apply on the tiled segmented GEMM instead
+ * of the register-streaming kernel; 0 (default) restores the latter. */
+enum { H2DEV_OPT_BASIS = 0, H2DEV_OPT_SKINNY_TILED = 1 };
 int h2dev_set_option(h2dev_handle_t h, int option, int64_t value);
 
 /* ---- solver (solver.hpp:11-47 H2MatrixSolver) ------------------------ */

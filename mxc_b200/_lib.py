@@ -26,6 +26,7 @@ FP64 = 0
 FP32 = 1
 
 OPT_BASIS = 0
+OPT_SKINNY_TILED = 1
 BASIS_GRAM, BASIS_HOUSEHOLDER = 0, 1
 
 EXPORT_S, EXPORT_Q, EXPORT_R, EXPORT_A, EXPORT_C = range(5)

@@ -108,6 +108,11 @@ struct DVec {
   }
 };
 
+// Process-wide choice of the apply kernel for skinny plans (handle option
+// H2DEV_OPT_SKINNY_TILED, used to compare the two kernels).
+static bool g_force_tiled = false;
+static bool force_tiled() { return g_force_tiled; }
+
 // Host-built list of segmented-GEMM tasks, uploaded once and replayed.
 template <typename T>
 struct GemmPlan {
@@ -120,6 +125,13 @@ struct GemmPlan {
   int shape = GEMM_BIG;
   const char* name = "seg_gemm";
   double flops = 0., bytes = 0.;  // algorithmic work of one run
+  bool skinny_nn = false;          // use k_skinny_nn instead of the tiled kernel
+  int nr = 0;
+  DVec<int2> d_rtiles;
+  DVec<T> parts_buf;               // partial results of split tasks
+  DVec<SumTask<T>> d_sums;
+  int nsums = 0;
+  double sum_bytes = 0.;
   void add_task(T* C, i64 ldc, int m, int n, T beta) {
     GemmTask<T> t;
     t.C = C; t.ldc = ldc; t.m = m; t.n = n; t.beta = beta;
@@ -137,6 +149,22 @@ struct GemmPlan {
     int maxn = 0;
     for (auto& t : tasks) maxn = std::max(maxn, t.n);
     shape = maxn <= 16 ? GEMM_SKINNY : GEMM_BIG;
+    bool nn = true;
+    for (const auto& e : ents) nn = nn && e.opA == 0 && e.opB == 0;
+    skinny_nn = nn && maxn <= 16 && !force_tiled();
+    nr = maxn;
+    if (skinny_nn) split_tasks();
+    if (skinny_nn) {
+      const int rb = skinny_rows_per_cta();
+      std::vector<int2> rt;
+      for (int ti = 0; ti < (int)tasks.size(); ti++) {
+        const auto& t = tasks[ti];
+        if (t.m <= 0 || t.n <= 0) continue;
+        if (t.e0 == t.e1 && t.beta == T(1)) continue;
+        for (int a = 0; a < (t.m + rb - 1) / rb; a++) rt.push_back(make_int2(ti, a));
+      }
+      d_rtiles.upload(rt);
+    }
     int bm = gemm_tile_m(shape), bn = gemm_tile_n(shape);
     std::vector<TileRef> tiles;
     for (int ti = 0; ti < (int)tasks.size(); ti++) {
@@ -156,6 +184,7 @@ struct GemmPlan {
         bytes += ((double)t.m * ents[e].k + (double)ents[e].k * t.n) * sizeof(T);
       }
     }
+    bytes += sum_bytes;
     d_tasks.upload(tasks);
     d_ents.upload(ents);
     d_tiles.upload(tiles);
@@ -164,9 +193,81 @@ struct GemmPlan {
     ents.clear();
     ents.shrink_to_fit();
   }
+  // Spreads tasks with many entries over several CTAs: a task whose A
+  // elements exceed an even share of the plan's total is cut at entry
+  // boundaries into parts that write m x n partials; k_sum_parts adds them in
+  // order into the task's C afterwards.  Upper tree levels have few boxes
+  // with many large couplings, so without this a few CTAs would stream most
+  // of the bytes.
+  void split_tasks() {
+    double total = 0.;
+    for (const auto& t : tasks)
+      for (int e = t.e0; e < t.e1; e++) total += (double)t.m * ents[e].k;
+    const double cap = std::max(total / 4096., 65536.);
+    std::vector<GemmTask<T>> out;
+    struct Pending { int first; int parts; GemmTask<T> orig; i64 off; };
+    std::vector<Pending> pend;
+    i64 scratch = 0;
+    for (const auto& t : tasks) {
+      double w = 0.;
+      for (int e = t.e0; e < t.e1; e++) w += (double)t.m * ents[e].k;
+      if (w <= cap || t.e1 - t.e0 < 2 || t.m <= 0 || t.n <= 0) {
+        out.push_back(t);
+        continue;
+      }
+      Pending pd;
+      pd.first = (int)out.size();
+      pd.orig = t;
+      pd.off = scratch;
+      pd.parts = 0;
+      int e = t.e0;
+      while (e < t.e1) {
+        GemmTask<T> part = t;
+        part.e0 = e;
+        double wp = 0.;
+        while (e < t.e1 && (wp == 0. || wp + (double)t.m * ents[e].k <= cap)) {
+          wp += (double)t.m * ents[e].k;
+          e++;
+        }
+        part.e1 = e;
+        part.beta = T(0);
+        part.ldc = t.m;
+        part.C = nullptr;  // set once the scratch exists
+        out.push_back(part);
+        pd.parts++;
+      }
+      scratch += (i64)pd.parts * t.m * t.n;
+      pend.push_back(pd);
+    }
+    if (pend.empty()) return;
+    parts_buf.alloc(scratch);
+    std::vector<SumTask<T>> sums;
+    for (const auto& pd : pend) {
+      const i64 mn = (i64)pd.orig.m * pd.orig.n;
+      for (int p = 0; p < pd.parts; p++) out[pd.first + p].C = parts_buf.p + pd.off + p * mn;
+      SumTask<T> st_;
+      st_.dst = pd.orig.C;
+      st_.ldd = pd.orig.ldc;
+      st_.src = parts_buf.p + pd.off;
+      st_.m = pd.orig.m;
+      st_.n = pd.orig.n;
+      st_.parts = pd.parts;
+      st_.beta = pd.orig.beta;
+      sums.push_back(st_);
+      sum_bytes += (double)(pd.parts + 1) * mn * sizeof(T);
+    }
+    tasks.swap(out);
+    nsums = (int)sums.size();
+    d_sums.upload(sums);
+  }
+
   void run(cudaStream_t st) const {
     Prof p(name, flops, bytes);
-    ck(launch_seg_gemm<T>(shape, d_tasks.p, d_ents.p, d_tiles.p, ntiles, st), "seg_gemm");
+    if (skinny_nn) {
+      ck(launch_skinny_nn<T>(nr, d_tasks.p, d_ents.p, d_rtiles.p, (int)d_rtiles.n, st), "skinny_nn");
+      if (nsums) ck(launch_sum_parts<T>(d_sums.p, nsums, st), "sum_parts");
+    } else
+      ck(launch_seg_gemm<T>(shape, d_tasks.p, d_ents.p, d_tiles.p, ntiles, st), "seg_gemm");
   }
 };
 
@@ -345,7 +446,7 @@ class Solver : public SolverBase {
       lv.qoff[i + 1] = lv.qoff[i] + lv.dims[i] * lv.dims[i];
       lv.maxM = std::max(lv.maxM, lv.dims[i]);
     }
-    require(lv.maxM <= 1024, "box dimension above 1024 is not supported");
+    require(lv.maxM <= 2048, "box dimension above 2048 is not supported");
     lv.lenX = lv.xoff[nodes];
     i64 nA = (i64)lv.acol.size();
     lv.aoff.assign(nA + 1, 0);
@@ -682,7 +783,7 @@ class Solver : public SolverBase {
       const T* X = (l == levels) ? vin.p : L[l + 1].vZ.p;
       const i64 ldx = lv.lenX;
       GemmPlan<T>& g = mv_up[l];
-      g.name = "gemm_matvec";
+      g.name = "gemm_matvec_up";
       for (i64 i = 0; i < lv.nodes; i++) {
         int M = (int)lv.dims[i], r = (int)lv.ranks[i];
         if (r == 0) continue;
@@ -694,7 +795,7 @@ class Solver : public SolverBase {
     for (i64 l = 0; l <= levels; l++) {
       Level<T>& lv = L[l];
       GemmPlan<T>& g = mv_h[l];
-      g.name = "gemm_matvec";
+      g.name = l == levels ? "gemm_matvec_far_leaf" : "gemm_matvec_far_upper";
       const T beta = (l == 0) ? T(0) : T(1);
       for (i64 i = 0; i < lv.nodes; i++) {
         int r = (int)lv.ranks[i];
@@ -708,7 +809,7 @@ class Solver : public SolverBase {
       g.finalize();
       if (l < levels) {
         GemmPlan<T>& d = mv_down[l];
-        d.name = "gemm_matvec";
+        d.name = "gemm_matvec_down";
         Level<T>& nx = L[l + 1];  // Y_l lives in W_{l+1}
         for (i64 i = 0; i < lv.nodes; i++) {
           int M = (int)lv.dims[i], r = (int)lv.ranks[i];
@@ -722,7 +823,7 @@ class Solver : public SolverBase {
       Level<T>& lv = L[levels];
       GemmPlan<T>& g = mv_leaf;
       g = GemmPlan<T>();
-      g.name = "gemm_matvec";
+      g.name = "gemm_matvec_near";
       for (i64 i = 0; i < lv.nodes; i++) {
         int M = (int)lv.dims[i], r = (int)lv.ranks[i];
         g.add_task(vout.p + lv.xoff[i], lv.lenX, M, nr, T(0));
@@ -1760,6 +1861,11 @@ int h2dev_probe_fma_peak(h2dev_handle_t h, int precision, double* tflops) {
 int h2dev_set_option(h2dev_handle_t h, int option, int64_t value) {
   H2_API_BEGIN
   require(h != nullptr, "null handle");
+  if (option == H2DEV_OPT_SKINNY_TILED) {
+    require(value == 0 || value == 1, "skinny option must be 0 or 1");
+    g_force_tiled = value != 0;
+    return H2DEV_OK;
+  }
   if (option == H2DEV_OPT_BASIS) {
     require(value == 0 || value == 1, "basis option must be 0 or 1");
     h->basis_mode = (int)value;

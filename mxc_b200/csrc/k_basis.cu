@@ -22,10 +22,12 @@ template <> struct Tiny<double> { static __device__ double v() { return DBL_MIN;
 template <> struct Tiny<float> { static __device__ float v() { return FLT_MIN; } };
 
 constexpr int TS_THREADS = 256;
-constexpr int TS_MAXCOL = 4;  // columns owned per thread: M <= 1024
+constexpr int TS_MAXCOL = 8;  // columns owned per thread: M <= 2048
 
-// R (row-major M x M per box, zero on entry) of the sample block.
-template <typename T>
+// R (row-major M x M per box, zero on entry) of the sample block.  TR
+// sample rows per tile (32, or 16 / 8 for wide boxes so the tile fits in
+// shared memory); lane r of the reflector warp holds tile row r.
+template <typename T, int TR>
 __global__ void __launch_bounds__(TS_THREADS) k_sample_tsqr(
     KernelParams kp, const double* __restrict__ bodies, const double* __restrict__ pts,
     const i64* __restrict__ xoff, const i64* __restrict__ dims, const int* __restrict__ sidx,
@@ -36,7 +38,7 @@ __global__ void __launch_bounds__(TS_THREADS) k_sample_tsqr(
   if (M == 0 || S == 0) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* tile = reinterpret_cast<T*>(smem_raw);            // 32 x M, row-major
-  T* vbuf = tile + 32 * M;                             // 32
+  T* vbuf = tile + TR * M;                             // 32
   double* sp = reinterpret_cast<double*>(vbuf + 32);   // 32 x 3
   __shared__ T s_tau;
 
@@ -55,8 +57,8 @@ __global__ void __launch_bounds__(TS_THREADS) k_sample_tsqr(
   }
 
   int rows = 0;  // rows of R that can be nonzero so far
-  for (i64 t0 = 0; t0 < S; t0 += 32) {
-    const int nrows = (int)((S - t0) < 32 ? (S - t0) : 32);
+  for (i64 t0 = 0; t0 < S; t0 += TR) {
+    const int nrows = (int)((S - t0) < TR ? (S - t0) : TR);
     if (tid < nrows) {
       const double* q = bodies + 3 * (i64)my_sidx[t0 + tid];
       sp[3 * tid] = q[0];
@@ -68,7 +70,7 @@ __global__ void __launch_bounds__(TS_THREADS) k_sample_tsqr(
     for (int k = 0; k < TS_MAXCOL; k++) {
       int c = tid + k * TS_THREADS;
       if (c < M)
-        for (int r = 0; r < 32; r++)
+        for (int r = 0; r < TR; r++)
           tile[r * M + c] = r < nrows ? (T)kernel_fast(kp, sp[3 * r] - px[k], sp[3 * r + 1] - py[k], sp[3 * r + 2] - pz[k]) : T(0);
     }
     __syncthreads();
@@ -180,6 +182,9 @@ __global__ void __launch_bounds__(256) k_cpqr(const i64* __restrict__ dims, cons
     for (int c = k + tid; c < M; c += nt)
       if (nu[c] > bv) { bv = nu[c]; bi = c; }
     argmax_first(bv, bi, red_v, red_i);
+    // No candidate compares greater when every norm is NaN: keep column k
+    // rather than index outside the matrix.
+    if (bi < k || bi >= M) bi = k;
     if (tid == 0) {
       if (s_nonzero == size && bv * bv < thr_helper * (double)(K - k)) s_nonzero = k;
       if (bi != k) {
@@ -431,9 +436,12 @@ cudaError_t launch_sample_tsqr(const KernelParams& kp, const double* bodies, con
                                const i64* dims, const int* sidx, const i64* soff, T* Rws, const i64* qoff,
                                int nboxes, int maxM, cudaStream_t st) {
   if (nboxes == 0) return cudaSuccess;
-  size_t smem = sizeof(T) * (32 * (size_t)maxM + 32) + sizeof(double) * 96;
+  if (maxM > TS_THREADS * TS_MAXCOL) return cudaErrorInvalidValue;
+  int tr = 32;
+  while (tr > 8 && sizeof(T) * (tr * (size_t)maxM + 32) + sizeof(double) * 96 > 200 * 1024) tr /= 2;
+  size_t smem = sizeof(T) * (tr * (size_t)maxM + 32) + sizeof(double) * 96;
   if (smem > 220 * 1024) return cudaErrorInvalidValue;  // box too large for one tile in shared memory
-  auto fn = k_sample_tsqr<T>;
+  auto fn = tr == 32 ? k_sample_tsqr<T, 32> : tr == 16 ? k_sample_tsqr<T, 16> : k_sample_tsqr<T, 8>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   fn<<<nboxes, TS_THREADS, smem, st>>>(kp, bodies, pts, xoff, dims, sidx, soff, Rws, qoff);
@@ -509,6 +517,23 @@ __global__ void __launch_bounds__(256) k_pivchol(const i64* __restrict__ dims, c
   int steps = K < M ? K : M;
   if (step_cap >= 0 && step_cap < steps) steps = (int)step_cap;
   for (int c = tid; c < M; c += nt) perm[c] = c;
+  // Smallest pivot kept: sqrt(eps) * ||XF|| (the resolution of an FP64 Gram
+  // matrix).  Columns below it are numerically dependent; flooring their
+  // pivot keeps R11^{-1} R12 finite and O(1) for them while the rows that
+  // carry the range of XF are unaffected.
+  double dmax = 0.;
+  int dmi = 0;
+  for (int j = tid; j < M; j += nt) {
+    double v = g[(i64)j * M + j];
+    if (v > dmax) { dmax = v; dmi = j; }
+  }
+  argmax_first(dmax, dmi, red_v, red_i);
+  double rfloor = sqrt(DBL_EPSILON * dmax);
+  if (!(rfloor > 0.)) rfloor = DBL_MIN;
+  // Schur diagonals at or below this are rounding noise of the FP64 Gram
+  // matrix (its resolution is ~sqrt(eps) in singular values).
+  const double noise = 16. * DBL_EPSILON * dmax;
+  bool noise_mode = false;
   __syncthreads();
   for (int k = 0; k < steps; k++) {
     double bv = -1.;
@@ -518,6 +543,7 @@ __global__ void __launch_bounds__(256) k_pivchol(const i64* __restrict__ dims, c
       if (v > bv) { bv = v; bi = j; }
     }
     argmax_first(bv, bi, red_v, red_i);
+    if (bi < k || bi >= M) bi = k;  // every diagonal NaN: no swap
     if (bi != k) {
       for (int c = tid; c < M; c += nt) {  // swap rows k, bi
         double t = g[(i64)k * M + c];
@@ -541,8 +567,18 @@ __global__ void __launch_bounds__(256) k_pivchol(const i64* __restrict__ dims, c
     }
     __syncthreads();
     const double d = g[(i64)k * M + k];
-    const double rkk = d > 0. ? sqrt(d) : 0.;
-    const double inv = rkk > 0. ? 1. / rkk : 0.;
+    // Once the remaining columns are numerically dependent, the pivots that
+    // still have to be taken (fixed rank) get the row [floor, 0, ..., 0]:
+    // their interpolation coefficients come out exactly zero and the rows
+    // that carry the range of XF solve their own system unchanged.
+    if (!(d > noise)) noise_mode = true;
+    if (noise_mode) {
+      for (int j = k + tid; j < M; j += nt) R[(i64)k * M + j] = (j == k) ? rfloor : 0.;
+      __syncthreads();
+      continue;
+    }
+    const double rkk = sqrt(d);
+    const double inv = 1. / rkk;
     for (int j = k + tid; j < M; j += nt) R[(i64)k * M + j] = (j == k) ? rkk : g[(i64)k * M + j] * inv;
     __syncthreads();
     const int rem = M - k - 1;

@@ -31,6 +31,9 @@ __global__ void __launch_bounds__(256) k_lu_inverse(const LuTask<T>* __restrict_
       if (v > bv) { bv = v; bi = r; }
     }
     argmax_first(bv, bi, red_v, red_i);
+    // A column of NaNs gives no maximum: keep row k rather than swap with a
+    // row outside the block.
+    if (bi < k || bi >= n) bi = k;
     if (tid == 0) t.ipiv[k] = bi;
     if (bi != k)
       for (int c = tid; c < n; c += nt) {

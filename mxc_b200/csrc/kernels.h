@@ -66,6 +66,25 @@ template <typename T>
 cudaError_t launch_seg_gemm(int shape, const GemmTask<T>* d_tasks, const GemmEntry<T>* d_ents, const TileRef* d_tiles,
                             int ntiles, cudaStream_t st);
 int gemm_tile_m(int shape);
+// Plans whose entries all use A and B as stored and whose outputs have at
+// most 16 columns: rows of A streamed from HBM into registers, one CTA per
+// skinny_rows_per_cta() rows of a task (tile = {task, row block}).
+template <typename T>
+cudaError_t launch_skinny_nn(int nr, const GemmTask<T>* d_tasks, const GemmEntry<T>* d_ents, const int2* d_tiles,
+                             int ntiles, cudaStream_t st);
+int skinny_rows_per_cta();
+// Reduction of a split task: dst (m x n, ld ldd) = beta dst + sum of `parts`
+// consecutive m x n partial results at src.
+template <typename T>
+struct SumTask {
+  T* dst;
+  i64 ldd;
+  const T* src;
+  int m, n, parts;
+  T beta;
+};
+template <typename T>
+cudaError_t launch_sum_parts(const SumTask<T>* d_tasks, int ntasks, cudaStream_t st);
 int gemm_tile_n(int shape);
 
 template <typename T>

@@ -88,6 +88,9 @@ class Handle:
     def synchronize(self):
         L.check(L.lib().h2dev_handle_synchronize(self.h), "h2dev_handle_synchronize")
 
+    def set_option(self, option: int, value: int):
+        L.check(L.lib().h2dev_set_option(self.h, option, value), "h2dev_set_option")
+
     def set_basis_mode(self, mode: int):
         """BASIS_GRAM (default) or BASIS_HOUSEHOLDER for fixed-rank bases of solvers created next."""
         L.check(L.lib().h2dev_set_option(self.h, L.OPT_BASIS, mode), "h2dev_set_option")
