@@ -41,10 +41,10 @@ def parse():
     ap.add_argument("--theta", type=float, default=2.0)
     ap.add_argument("--rank", type=int, default=128)
     ap.add_argument("--samples", type=int, default=4000)
-    ap.add_argument("--op-samples", type=int, default=4000)
+    ap.add_argument("--op-samples", type=int, default=16000)
     ap.add_argument("--op-eps", type=float, default=1e-11)
     ap.add_argument("--nrhs", type=int, default=16)
-    ap.add_argument("--singularity", type=float, default=0.01,
+    ap.add_argument("--singularity", type=float, default=1e-4,
                     help="Laplace3D(s): value 1/s where bodies coincide (kernel.hpp:28-38)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--tol", type=float, default=1e-10)

@@ -70,7 +70,11 @@ int h2dev_handle_synchronize(h2dev_handle_t h);
 /* H2DEV_OPT_SKINNY_TILED: 1 makes plans built afterwards (in this process)
  * run every multi-right-hand-side apply on the tiled segmented GEMM instead
  * of the register-streaming kernel; 0 (default) restores the latter. */
-enum { H2DEV_OPT_BASIS = 0, H2DEV_OPT_SKINNY_TILED = 1 };
+/* H2DEV_OPT_SAMPLING: how `samples` caps a box's far list.  0 (default):
+ * rows floor(j * total / samples) of the whole list.  1: level-geometric —
+ * the far boxes of the box's own level (the nearest) get half of the budget,
+ * each level further out half of what remains, each group strided as in 0. */
+enum { H2DEV_OPT_BASIS = 0, H2DEV_OPT_SKINNY_TILED = 1, H2DEV_OPT_SAMPLING = 2 };
 int h2dev_set_option(h2dev_handle_t h, int option, int64_t value);
 
 /* ---- solver (solver.hpp:11-47 H2MatrixSolver) ------------------------ */
@@ -178,6 +182,12 @@ int h2dev_profile_enable(h2dev_handle_t h, int on);
  * *count receives the number of distinct kernels. */
 int h2dev_profile_report(h2dev_handle_t h, int64_t cap, char* names, int64_t* launches, double* ms, double* flops,
                          double* bytes, int64_t* count);
+/* Per-launch records since profiling was enabled, in launch order: names
+ * (48 bytes each), start (ms after the first record's start) and device
+ * duration; idle gaps between records show host-side stalls.  *count
+ * receives the number of records. */
+int h2dev_profile_timeline(h2dev_handle_t h, int64_t cap, char* names, double* start_ms, double* dur_ms,
+                           int64_t* count);
 /* Measured FMA throughput (TFLOP/s, 2 flops per FMA) of plain FP64 or FP32
  * SIMT code on this device: the denominator for the FP64/FP32 kernels. */
 int h2dev_probe_fma_peak(h2dev_handle_t h, int precision, double* tflops);

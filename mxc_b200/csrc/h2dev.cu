@@ -67,28 +67,115 @@ static void require(bool ok, const char* what) {
   if (!ok) throw H2Error{H2DEV_ERR_ARG, what};
 }
 
+// Host->device copy through the handle's pinned staging buffer: the host
+// bytes are copied into pinned memory at once and the DMA is queued on the
+// handle's stream.  A full buffer is reused when its last copy has run,
+// otherwise replaced by one twice the size (the old one is freed once its
+// copies are done); past 512 MB the call waits for the buffer instead.
+static void stage_copy(h2dev_handle_s* h, void* dst, const void* src, size_t bytes) {
+  const size_t need = (bytes + 255) & ~(size_t)255;
+  for (size_t k = 0; k < h->stage_retired.size();) {
+    auto& r = h->stage_retired[k];
+    if (cudaEventQuery(r.second) == cudaSuccess) {
+      cudaFreeHost(r.first);
+      cudaEventDestroy(r.second);
+      h->stage_retired.erase(h->stage_retired.begin() + (long)k);
+    } else {
+      cudaGetLastError();
+      k++;
+    }
+  }
+  if (h->stage_head + need > h->stage_cap) {
+    bool reuse = false;
+    if (h->stage && need <= h->stage_cap) {
+      cudaError_t q = cudaEventQuery(h->stage_ev);
+      if (q == cudaSuccess) {
+        reuse = true;
+      } else if (h->stage_cap >= ((size_t)512 << 20)) {
+        cudaGetLastError();
+        ck(cudaEventSynchronize(h->stage_ev), "stage wait");
+        reuse = true;
+      } else {
+        cudaGetLastError();
+      }
+    }
+    if (reuse) {
+      h->stage_head = 0;
+    } else {
+      if (h->stage) h->stage_retired.emplace_back(h->stage, h->stage_ev);
+      h->stage = nullptr;
+      h->stage_ev = nullptr;
+      const size_t cap = std::max(std::max(need, 2 * h->stage_cap), (size_t)8 << 20);
+      h->stage_cap = 0;
+      h->stage_head = 0;
+      ck(cudaHostAlloc((void**)&h->stage, cap, cudaHostAllocDefault), "cudaHostAlloc");
+      ck(cudaEventCreateWithFlags(&h->stage_ev, cudaEventDisableTiming), "cudaEventCreate");
+      h->stage_cap = cap;
+    }
+  }
+  char* buf = h->stage + h->stage_head;
+  std::memcpy(buf, src, bytes);
+  ck(cudaMemcpyAsync(dst, buf, bytes, cudaMemcpyHostToDevice, h->stream), "upload");
+  ck(cudaEventRecord(h->stage_ev, h->stream), "cudaEventRecord");
+  h->stage_head += need;
+}
+
+static void stage_release(h2dev_handle_s* h) {
+  for (auto& r : h->stage_retired) {
+    cudaFreeHost(r.first);
+    cudaEventDestroy(r.second);
+  }
+  h->stage_retired.clear();
+  if (h->stage) cudaFreeHost(h->stage);
+  if (h->stage_ev) cudaEventDestroy(h->stage_ev);
+  h->stage = nullptr;
+  h->stage_ev = nullptr;
+  h->stage_cap = h->stage_head = 0;
+}
+
+// Device array.  Inside an API call (a current handle) memory comes from the
+// device's stream-ordered pool on the handle's stream and is returned to it
+// in stream order, so temporaries need no synchronisation before they go.
 template <typename T>
 struct DVec {
   T* p = nullptr;
   size_t n = 0;
+  cudaStream_t s = nullptr;  // stream of a stream-ordered allocation
+  bool ordered = false;
   DVec() = default;
   DVec(const DVec&) = delete;
   DVec& operator=(const DVec&) = delete;
-  DVec(DVec&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DVec(DVec&& o) noexcept : p(o.p), n(o.n), s(o.s), ordered(o.ordered) { o.p = nullptr; o.n = 0; }
   DVec& operator=(DVec&& o) noexcept {
-    if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    if (this != &o) {
+      release();
+      p = o.p; n = o.n; s = o.s; ordered = o.ordered;
+      o.p = nullptr; o.n = 0;
+    }
     return *this;
   }
   ~DVec() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      if (!ordered || cudaFreeAsync(p, s) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(p);
+      }
+    }
     p = nullptr;
     n = 0;
   }
   void alloc(size_t count) {
     if (count == n && p) return;
     release();
-    if (count) ck(cudaMalloc((void**)&p, count * sizeof(T)), "cudaMalloc");
+    ordered = g_cur != nullptr;
+    s = ordered ? g_cur->stream : nullptr;
+    if (count) {
+      if (ordered)
+        ck(cudaMallocAsync((void**)&p, count * sizeof(T), s), "cudaMallocAsync");
+      else
+        ck(cudaMalloc((void**)&p, count * sizeof(T)), "cudaMalloc");
+    }
     n = count;
   }
   void zero(cudaStream_t st) {
@@ -96,7 +183,11 @@ struct DVec {
   }
   void upload(const std::vector<T>& v) {
     alloc(v.size());
-    if (!v.empty()) ck(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+    if (v.empty()) return;
+    if (ordered && g_cur && g_cur->stream == s)
+      stage_copy(g_cur, p, v.data(), v.size() * sizeof(T));
+    else
+      ck(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
   }
   std::vector<T> download(cudaStream_t st) const {
     std::vector<T> v(n);
@@ -355,6 +446,8 @@ class Solver : public SolverBase {
   DVec<double> bodies;
   std::vector<Level<T>> L;
   bool factored = false;
+  int sampling_mode = 0;                 // 0: strided, 1: level-geometric far-list cap
+  std::vector<std::vector<i64>> gstart;  // per cell: first range of each level group
   // per-nrhs state
   i64 cur_nrhs = -1;
   DVec<T> vin, vout;
@@ -377,6 +470,7 @@ class Solver : public SolverBase {
     levels = a.levels;
     N = a.nbodies;
     samples = a.samples;
+    sampling_mode = h->sampling_mode;
     cells = a.cells;
     {
       std::vector<double> hb(a.bodies, a.bodies + 3 * N);
@@ -390,9 +484,12 @@ class Solver : public SolverBase {
     // boxes (h-matrix.cpp:83-98, 122-127); the root has none.
     i64 ncells = (i64)cells.size();
     std::vector<std::vector<std::pair<i64, i64>>> ranges(ncells);
+    gstart.assign(ncells, std::vector<i64>());
     for (i64 c = 1; c < ncells; c++) {
       i64 parent = (c - 1) / 2;
       ranges[c] = ranges[parent];
+      gstart[c] = gstart[parent];
+      gstart[c].push_back((i64)ranges[parent].size());
       for (i64 k = sampL.row[c]; k < sampL.row[c + 1]; k++) {
         i64 x = sampL.col[k];
         ranges[c].emplace_back(cells[x].body[0], cells[x].body[1]);
@@ -487,7 +584,6 @@ class Solver : public SolverBase {
           Prof pf("gen_near_blocks", 0., (double)lv.aoff[nA] * sizeof(T));
           ck(launch_gen_blocks<T>(kp, dg.p, (int)gt.size(), 1, lv.A.p, st()), "gen near");
         }
-        ck(cudaStreamSynchronize(st()), "sync");
       } else {
         CopyPlan<double> pcopy;
         CopyPlan<T> qcopy, acopy;
@@ -528,14 +624,16 @@ class Solver : public SolverBase {
         pcopy.run(st());
         qcopy.run(st());
         acopy.run(st());
-        ck(cudaStreamSynchronize(st()), "sync");
       }
 
       // Shared basis of every box (compute_basis, h2matrix.cpp:252-257).
       std::vector<int> sidx, tmp;
       std::vector<i64> soff(nodes + 1, 0), krows(nodes, 0);
       for (i64 i = 0; i < nodes; i++) {
-        sample_far_list(ranges[g0 + i], samples, tmp);
+        if (sampling_mode == 1)
+          sample_far_list_geometric(ranges[g0 + i], gstart[g0 + i], samples, tmp);
+        else
+          sample_far_list(ranges[g0 + i], samples, tmp);
         sidx.insert(sidx.end(), tmp.begin(), tmp.end());
         soff[i + 1] = (i64)sidx.size();
         krows[i] = std::min<i64>(lv.dims[i], (i64)tmp.size());
@@ -584,12 +682,16 @@ class Solver : public SolverBase {
                             d_nonzero.p, cap, (int)nodes, (int)lv.maxM, st()),
              "cpqr");
         }
-        Prof pfin("basis_finish", 0., (double)lv.qoff[nodes] * sizeof(T) * 3.);
-        ck(launch_basis_finish<T>(lv.d_dims.p, d_krows.p, Rws.p, lv.Q.p, lv.R.p, lv.d_qoff.p, d_perm.p,
-                                  lv.d_xoff.p, d_maxpiv.p, d_nonzero.p, lv.pts.p, lv.d_ranks.p, e, orth ? 1 : 0,
-                                  low ? 0 : 1, (int)nodes, (int)lv.maxM, st()),
-           "basis_finish");
-        ck(cudaStreamSynchronize(st()), "sync");
+        DVec<T> taus;
+        if (orth) taus.alloc(std::max<i64>(1, lv.lenX));
+        {
+          Prof pfin("basis_finish", 0., (double)lv.qoff[nodes] * sizeof(T) * 3.);
+          ck(launch_basis_finish<T>(lv.d_dims.p, d_krows.p, Rws.p, lv.Q.p, lv.R.p, lv.d_qoff.p, d_perm.p,
+                                    lv.d_xoff.p, d_maxpiv.p, d_nonzero.p, lv.pts.p, lv.d_ranks.p, e, orth ? 1 : 0,
+                                    low ? 0 : 1, (int)nodes, (int)lv.maxM, st(), orth ? taus.p : nullptr),
+             "basis_finish");
+        }
+        if (orth) blocked_orth_qr<T>(lv, Rws.p, lv.Q.p, lv.R.p, taus.p, lv.d_ranks.download(st()), low == nullptr);
       }
       lv.ranks = lv.d_ranks.download(st());
     } else {
@@ -652,9 +754,6 @@ class Solver : public SolverBase {
         g2.finalize();
         g1.run(st());
         g2.run(st());
-        ck(cudaStreamSynchronize(st()), "sync");
-      } else {
-        ck(cudaStreamSynchronize(st()), "sync");
       }
     }
   }
@@ -716,42 +815,249 @@ class Solver : public SolverBase {
       }
       gp.finalize();
       gp.run(st());
-      ck(cudaStreamSynchronize(st()), "sync");
     }
     Rws.alloc(lv.qoff[nodes]);
     Rws.zero(st());
     {
+      // Blocked pivoted Cholesky: panels of 32 pivots per box, each followed
+      // by one batched rank-32 update of every trailing Gram matrix.
+      const int nb = 32;
+      std::vector<i64> steps(nodes, 0);
+      i64 maxsteps = 0;
       double fl = 0.;
       for (i64 i = 0; i < nodes; i++) {
-        double Md = (double)lv.dims[i], st_ = std::min(Md, (double)(cap >= 0 ? cap : lv.dims[i]));
-        fl += 2. * (Md * Md * st_ - Md * st_ * st_ + st_ * st_ * st_ / 3.);
+        i64 K = std::min<i64>(lv.dims[i], soff[i + 1] - soff[i]);
+        steps[i] = cap >= 0 ? std::min<i64>(K, cap) : K;
+        maxsteps = std::max(maxsteps, steps[i]);
+        double Md = (double)lv.dims[i], sd = (double)steps[i];
+        fl += 2. * (Md * Md * sd - Md * sd * sd + sd * sd * sd / 3.);
       }
+      DVec<i64> d_steps;
+      DVec<double> state;
+      d_steps.upload(steps);
+      state.alloc(3 * nodes);
       Prof pf("pivchol", fl, 0.);
-      ck(launch_pivchol(lv.d_dims.p, d_krows.p, G.p, Rws.p, lv.d_qoff.p, d_perm.p, lv.d_xoff.p, cap, (int)nodes,
-                        (int)lv.maxM, st()),
-         "pivchol");
+      for (i64 k0 = 0; k0 < maxsteps; k0 += nb) {
+        ck(launch_pivchol_panel(lv.d_dims.p, d_steps.p, G.p, Rws.p, lv.d_qoff.p, d_perm.p, lv.d_xoff.p, state.p,
+                                (int)k0, nb, (int)nodes, (int)lv.maxM, st()),
+           "pivchol panel");
+        const i64 k1 = k0 + nb;
+        if (k1 >= maxsteps) break;
+        GemmPlan<double> up;
+        up.name = "gemm_pivchol_update";
+        for (i64 i = 0; i < nodes; i++) {
+          const i64 M = lv.dims[i];
+          if (steps[i] <= k1 || M <= k1) continue;
+          double* Rb = Rws.p + lv.qoff[i];
+          up.add_task(G.p + lv.qoff[i] + k1 + k1 * M, M, (int)(M - k1), (int)(M - k1), 1.);
+          up.add_entry(Rb + k0 * M + k1, M, 0, Rb + k0 * M + k1, M, 1, nb, -1.);
+        }
+        up.finalize();
+        up.run(st());
+      }
     }
-    Prof pfin("basis_finish", 0., (double)lv.qoff[nodes] * 24.);
+    DVec<double> taus;
+    taus.alloc(std::max<i64>(1, lv.lenX));
     if (std::is_same<T, double>::value) {
-      ck(launch_basis_finish<double>(lv.d_dims.p, d_krows.p, Rws.p, reinterpret_cast<double*>(lv.Q.p),
-                                     reinterpret_cast<double*>(lv.R.p), lv.d_qoff.p, d_perm.p, lv.d_xoff.p,
-                                     d_maxpiv.p, d_nonzero.p, lv.pts.p, lv.d_ranks.p, e, 1, leaf ? 1 : 0,
-                                     (int)nodes, (int)lv.maxM, st()),
-         "basis_finish");
+      {
+        Prof pfin("basis_finish", 0., (double)lv.qoff[nodes] * 24.);
+        ck(launch_basis_finish<double>(lv.d_dims.p, d_krows.p, Rws.p, reinterpret_cast<double*>(lv.Q.p),
+                                       reinterpret_cast<double*>(lv.R.p), lv.d_qoff.p, d_perm.p, lv.d_xoff.p,
+                                       d_maxpiv.p, d_nonzero.p, lv.pts.p, lv.d_ranks.p, e, 1, leaf ? 1 : 0,
+                                       (int)nodes, (int)lv.maxM, st(), taus.p),
+           "basis_finish");
+      }
+      blocked_orth_qr<double>(lv, Rws.p, reinterpret_cast<double*>(lv.Q.p), reinterpret_cast<double*>(lv.R.p),
+                              taus.p, lv.d_ranks.download(st()), leaf);
     } else {
       DVec<double> Qd, Rd;
       Qd.alloc(lv.qoff[nodes]);
       Rd.alloc(lv.qoff[nodes]);
       Rd.zero(st());
       ck(launch_convert<T, double>(lv.Q.p, Qd.p, lv.qoff[nodes], st()), "convert");
-      ck(launch_basis_finish<double>(lv.d_dims.p, d_krows.p, Rws.p, Qd.p, Rd.p, lv.d_qoff.p, d_perm.p,
-                                     lv.d_xoff.p, d_maxpiv.p, d_nonzero.p, lv.pts.p, lv.d_ranks.p, e, 1,
-                                     leaf ? 1 : 0, (int)nodes, (int)lv.maxM, st()),
-         "basis_finish");
+      {
+        Prof pfin("basis_finish", 0., (double)lv.qoff[nodes] * 24.);
+        ck(launch_basis_finish<double>(lv.d_dims.p, d_krows.p, Rws.p, Qd.p, Rd.p, lv.d_qoff.p, d_perm.p,
+                                       lv.d_xoff.p, d_maxpiv.p, d_nonzero.p, lv.pts.p, lv.d_ranks.p, e, 1,
+                                       leaf ? 1 : 0, (int)nodes, (int)lv.maxM, st(), taus.p),
+           "basis_finish");
+      }
+      blocked_orth_qr<double>(lv, Rws.p, Qd.p, Rd.p, taus.p, lv.d_ranks.download(st()), leaf);
       ck(launch_convert<double, T>(Qd.p, lv.Q.p, lv.qoff[nodes], st()), "convert");
       ck(launch_convert<double, T>(Rd.p, lv.R.p, lv.qoff[nodes], st()), "convert");
     }
-    ck(cudaStreamSynchronize(st()), "sync");
+  }
+
+  // Orthogonal completion (h2matrix.cpp:100-106) for every box with
+  // 0 < rank < M, after the finish kernel left U_ID = P [I; T^T] in R's slot
+  // and Q_in (upper triangular) in Q: W = Q_in U_ID (M x rank, ld M), a
+  // blocked Householder QR of W (panels factored in shared memory, the
+  // trailing columns updated by three batched GEMMs per panel,
+  // A -= V (T^T (V^T A))), R = triu(W[:rank, :rank]) and
+  // Q = H_0 ... H_{rank-1} in compact-WY form.
+  template <typename U>
+  void blocked_orth_qr(Level<T>& lv, U* W, U* Q, U* R, U* taus, const std::vector<i64>& ranks, bool leaf) {
+    std::vector<i64> box;
+    i64 maxM = 0, maxr = 0, ysz = 0;
+    for (i64 i = 0; i < lv.nodes; i++) {
+      const i64 M = lv.dims[i], r = ranks[i];
+      if (!(0 < r && r < M)) continue;
+      box.push_back(i);
+      maxM = std::max(maxM, M);
+      maxr = std::max(maxr, r);
+    }
+    if (box.empty()) return;
+    int nb = 32;
+    while (nb > 1 && sizeof(U) * ((size_t)maxM * nb + 2 * nb + (size_t)nb * nb) > 190 * 1024) nb--;
+    for (i64 i : box) ysz += (i64)nb * ranks[i];
+    {
+      double fl = 0.;
+      for (i64 i : box) fl += leaf ? 0. : (double)lv.dims[i] * lv.dims[i] * ranks[i];
+      if (leaf) {
+        CopyPlan<U> cp;
+        for (i64 i : box) cp.add(R + lv.qoff[i], lv.dims[i], W + lv.qoff[i], lv.dims[i], (int)lv.dims[i], (int)ranks[i]);
+        cp.finalize();
+        cp.run(st());
+      } else {
+        GemmPlan<U> g;
+        g.name = "gemm_qr";
+        for (i64 i : box) {
+          const i64 M = lv.dims[i];
+          g.add_task(W + lv.qoff[i], M, (int)M, (int)ranks[i], U(0));
+          g.add_entry(Q + lv.qoff[i], M, 0, R + lv.qoff[i], M, 0, (int)M, U(1));
+        }
+        g.finalize();
+        g.run(st());
+      }
+    }
+    DVec<U> Vp, Tp, Y, Y2;
+    Vp.alloc((i64)box.size() * maxM * nb);
+    Tp.alloc((i64)box.size() * nb * nb);
+    Y.alloc(ysz);
+    Y2.alloc(ysz);
+    for (i64 k0 = 0; k0 < maxr; k0 += nb) {
+      std::vector<QrPanelTask<U>> pt;
+      GemmPlan<U> gy, gt, ga;
+      gy.name = gt.name = ga.name = "gemm_qr";
+      i64 yo = 0;
+      int maxm = 0;
+      double fl = 0.;
+      for (size_t z = 0; z < box.size(); z++) {
+        const i64 i = box[z], M = lv.dims[i], r = ranks[i];
+        if (k0 >= r) continue;
+        const int w = (int)std::min<i64>(nb, r - k0), m = (int)(M - k0);
+        U* vp = Vp.p + (i64)z * maxM * nb;
+        U* tp = Tp.p + (i64)z * nb * nb;
+        QrPanelTask<U> t;
+        t.W = W + lv.qoff[i];
+        t.Vp = vp;
+        t.Tp = tp;
+        t.taus = taus + lv.xoff[i];
+        t.M = (int)M;
+        t.k0 = (int)k0;
+        t.nb = w;
+        pt.push_back(t);
+        maxm = std::max(maxm, m);
+        fl += 2. * m * w * w;
+        const i64 n2 = r - k0 - w;
+        if (n2 <= 0) continue;
+        U* At = W + lv.qoff[i] + k0 + (k0 + w) * M;
+        gy.add_task(Y.p + yo, w, w, (int)n2, U(0));
+        gy.add_entry(vp, m, 1, At, M, 0, m, U(1));
+        gt.add_task(Y2.p + yo, w, w, (int)n2, U(0));
+        gt.add_entry(tp, w, 1, Y.p + yo, w, 0, w, U(1));
+        ga.add_task(At, M, m, (int)n2, U(1));
+        ga.add_entry(vp, m, 0, Y2.p + yo, w, 0, w, U(-1));
+        yo += (i64)w * n2;
+      }
+      DVec<QrPanelTask<U>> dpt;
+      dpt.upload(pt);
+      {
+        Prof pf("qr_panel", fl, 0.);
+        ck(launch_qr_panel<U>(dpt.p, (int)pt.size(), maxm, nb, st()), "qr_panel");
+      }
+      if (yo > 0) {
+        gy.finalize();
+        gt.finalize();
+        ga.finalize();
+        gy.run(st());
+        gt.run(st());
+        ga.run(st());
+      }
+    }
+    std::vector<QrExtractTask<U>> et;
+    for (i64 i : box) {
+      QrExtractTask<U> t;
+      t.W = W + lv.qoff[i];
+      t.R = R + lv.qoff[i];
+      t.Q = Q + lv.qoff[i];
+      t.M = (int)lv.dims[i];
+      t.rank = (int)ranks[i];
+      et.push_back(t);
+    }
+    DVec<QrExtractTask<U>> det;
+    det.upload(et);
+    {
+      Prof pf("qr_extract", 0., 0.);
+      ck(launch_qr_extract<U>(det.p, (int)et.size(), st()), "qr_extract");
+    }
+    wy_form_q<U>(lv, W, Q, taus, ranks);
+  }
+
+  // Q = H_0 ... H_{r-1} = I - V T V^T for every box whose orthogonal basis
+  // was completed by a Householder QR (0 < rank < M): S = V^T V and the two
+  // products are batched GEMMs over the level, T comes from k_wy_t.  W holds
+  // the explicit V (M x rank, column-major at the box's qoff), Q the identity.
+  template <typename U>
+  void wy_form_q(Level<T>& lv, U* W, U* Q, U* taus, const std::vector<i64>& ranks) {
+    std::vector<i64> so(1, 0), wo(1, 0);
+    std::vector<i64> box;
+    int maxr = 0;
+    for (i64 i = 0; i < lv.nodes; i++) {
+      const i64 M = lv.dims[i], r = ranks[i];
+      if (!(0 < r && r < M)) continue;
+      box.push_back(i);
+      so.push_back(so.back() + r * r);
+      wo.push_back(wo.back() + r * M);
+      maxr = std::max<int>(maxr, (int)r);
+    }
+    if (box.empty()) return;
+    DVec<U> Sb, Tb, W2;
+    Sb.alloc(so.back());
+    Tb.alloc(so.back());
+    W2.alloc(wo.back());
+    GemmPlan<U> gs, gw, gq;
+    gs.name = gw.name = gq.name = "gemm_wy";
+    std::vector<WyTask<U>> wt;
+    for (size_t z = 0; z < box.size(); z++) {
+      const i64 i = box[z], M = lv.dims[i];
+      const int r = (int)ranks[i];
+      U* Wi = W + lv.qoff[i];
+      gs.add_task(Sb.p + so[z], r, r, r, U(0));
+      gs.add_entry(Wi, M, 1, Wi, M, 0, (int)M, U(1));
+      WyTask<U> t;
+      t.S = Sb.p + so[z];
+      t.taus = taus + lv.xoff[i];
+      t.Tm = Tb.p + so[z];
+      t.r = r;
+      wt.push_back(t);
+      gw.add_task(W2.p + wo[z], r, r, (int)M, U(0));
+      gw.add_entry(Tb.p + so[z], r, 0, Wi, M, 1, r, U(1));
+      gq.add_task(Q + lv.qoff[i], M, (int)M, (int)M, U(1));
+      gq.add_entry(Wi, M, 0, W2.p + wo[z], r, 0, r, U(-1));
+    }
+    gs.finalize();
+    gw.finalize();
+    gq.finalize();
+    DVec<WyTask<U>> dwt;
+    dwt.upload(wt);
+    gs.run(st());
+    {
+      Prof pf("wy_t", 0., 0.);
+      ck(launch_wy_t<U>(dwt.p, (int)wt.size(), maxr, st()), "wy_t");
+    }
+    gw.run(st());
+    gq.run(st());
   }
 
   // ------------------------------------------------------------ vectors
@@ -945,7 +1251,6 @@ class Solver : public SolverBase {
         Prof pf("lu_inverse", fl, 0.);
         ck(launch_lu_inverse<T>(dl.p, (int)lt.size(), st()), "lu_inverse");
       }
-      ck(cudaStreamSynchronize(st()), "sync");
     }
     // Step 5: V^T[:, Ms:] = U_r (A_rr^{-1})^T.
     for (i64 i = 0; i < nodes; i++) {
@@ -1026,7 +1331,6 @@ class Solver : public SolverBase {
         b.finalize();
         a.run(st());
         b.run(st());
-        ck(cudaStreamSynchronize(st()), "sync");
         p = q;
       }
       // Steps 10-11: neighbour Schur updates of the skeleton blocks.
@@ -1080,11 +1384,7 @@ class Solver : public SolverBase {
       s11a.run(st());
       s10.run(st());
       s11b.run(st());
-      ck(cudaStreamSynchronize(st()), "sync");
     }
-    std::vector<int> inf = lv.info.download(st());
-    lv.info_count = 0;
-    for (int v : inf) lv.info_count += v;
   }
 
   void copy_next(i64 l) {
@@ -1100,7 +1400,6 @@ class Solver : public SolverBase {
       }
     cp.finalize();
     cp.run(st());
-    ck(cudaStreamSynchronize(st()), "sync");
   }
 
   void factorize(int* info) override {
@@ -1109,7 +1408,13 @@ class Solver : public SolverBase {
       factor_level(l);
       if (l > 0) copy_next(l);
     }
-    for (i64 l = 0; l <= levels; l++) info[l] = L[l].info_count;
+    // Singular-block counts per level, read once after the last level.
+    for (i64 l = 0; l <= levels; l++) {
+      std::vector<int> inf = L[l].info.download(st());
+      L[l].info_count = 0;
+      for (int v : inf) L[l].info_count += v;
+      info[l] = L[l].info_count;
+    }
     factored = true;
     pc_built = false;
   }
@@ -1512,21 +1817,36 @@ int h2dev_handle_create(int device, h2dev_handle_t* out) {
     delete h;
     ck(e, "cudaStreamCreate");
   }
+  // Keep up to 32 GB of freed stream-ordered memory in this process's pool
+  // between calls (the default returns it to the driver at every sync).
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = (uint64_t)32 << 30;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
   *out = h;
   return H2DEV_OK;
   H2_API_END
 }
 
-int h2dev_handle_destroy(h2dev_handle_t h) {
-  H2_API_BEGIN
-  if (!h) return H2DEV_OK;
+// Drops one reference; the last one frees the stream, events and staging.
+static void handle_release(h2dev_handle_s* h) {
+  if (!h || --h->refs > 0) return;
+  cudaSetDevice(h->device);
   cudaStreamSynchronize(h->stream);
+  stage_release(h);
   h->clear();
   for (cudaEvent_t e : h->pool) cudaEventDestroy(e);
   if (h->t0) cudaEventDestroy(h->t0);
   if (h->t1) cudaEventDestroy(h->t1);
   cudaStreamDestroy(h->stream);
   delete h;
+}
+
+int h2dev_handle_destroy(h2dev_handle_t h) {
+  H2_API_BEGIN
+  handle_release(h);
   return H2DEV_OK;
   H2_API_END
 }
@@ -1584,6 +1904,7 @@ int h2dev_solver_create(h2dev_handle_t h, int kernel, double singularity, double
     p->h = h;
     p->build(a);
   }
+  h->refs++;
   *out = s.release();
   return H2DEV_OK;
   H2_API_END
@@ -1592,8 +1913,16 @@ int h2dev_solver_create(h2dev_handle_t h, int kernel, double singularity, double
 int h2dev_solver_destroy(h2dev_solver_t s) {
   H2_API_BEGIN
   if (s) {
-    if (s->impl && s->impl->h) cudaStreamSynchronize(s->impl->h->stream);
-    delete s;
+    h2dev_handle_s* h = s->impl ? s->impl->h : nullptr;
+    if (h) {
+      cudaSetDevice(h->device);
+      CurHandle ch(h);
+      delete s;
+      cudaStreamSynchronize(h->stream);
+    } else {
+      delete s;
+    }
+    handle_release(h);
   }
   return H2DEV_OK;
   H2_API_END
@@ -1829,6 +2158,28 @@ int h2dev_profile_report(h2dev_handle_t h, int64_t cap, char* names, int64_t* la
   H2_API_END
 }
 
+int h2dev_profile_timeline(h2dev_handle_t h, int64_t cap, char* names, double* start_ms, double* dur_ms,
+                           int64_t* count) {
+  H2_API_BEGIN
+  require(h && count, "null argument");
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  *count = (int64_t)h->recs.size();
+  for (size_t k = 0; k < h->recs.size() && (int64_t)k < cap; k++) {
+    const ProfRec& r = h->recs[k];
+    float a = 0.f, d = 0.f;
+    ck(cudaEventElapsedTime(&a, h->recs[0].a, r.a), "cudaEventElapsedTime");
+    ck(cudaEventElapsedTime(&d, r.a, r.b), "cudaEventElapsedTime");
+    if (names) {
+      std::strncpy(names + 48 * k, r.name, 47);
+      names[48 * k + 47] = 0;
+    }
+    if (start_ms) start_ms[k] = a;
+    if (dur_ms) dur_ms[k] = d;
+  }
+  return H2DEV_OK;
+  H2_API_END
+}
+
 int h2dev_probe_fma_peak(h2dev_handle_t h, int precision, double* tflops) {
   H2_API_BEGIN
   require(h && tflops && (precision == H2DEV_FP64 || precision == H2DEV_FP32), "bad arguments");
@@ -1864,6 +2215,11 @@ int h2dev_set_option(h2dev_handle_t h, int option, int64_t value) {
   if (option == H2DEV_OPT_SKINNY_TILED) {
     require(value == 0 || value == 1, "skinny option must be 0 or 1");
     g_force_tiled = value != 0;
+    return H2DEV_OK;
+  }
+  if (option == H2DEV_OPT_SAMPLING) {
+    require(value == 0 || value == 1, "sampling option must be 0 or 1");
+    h->sampling_mode = (int)value;
     return H2DEV_OK;
   }
   if (option == H2DEV_OPT_BASIS) {

@@ -13,6 +13,7 @@
 #include "common.cuh"
 #include "kernels.h"
 
+#include <algorithm>
 #include <cfloat>
 
 namespace h2b {
@@ -269,7 +270,8 @@ __global__ void __launch_bounds__(256) k_basis_finish(
     const i64* __restrict__ dims, const i64* __restrict__ krows, T* __restrict__ Rws, T* __restrict__ Q,
     T* __restrict__ Rm, const i64* __restrict__ qoff, const int* __restrict__ perm_in,
     const i64* __restrict__ xoff, const double* __restrict__ maxpiv, const int* __restrict__ nonzero,
-    double* __restrict__ pts, i64* __restrict__ ranks_out, double epi, int orth, int qin_identity) {
+    double* __restrict__ pts, i64* __restrict__ ranks_out, double epi, int orth, int qin_identity,
+    T* __restrict__ wy_taus, int xcap) {
   const int box = blockIdx.x;
   const int M = (int)dims[box];
   const int K = (int)krows[box];
@@ -315,12 +317,29 @@ __global__ void __launch_bounds__(256) k_basis_finish(
     if (tid == 0) ranks_out[box] = rank;
     return;
   }
-  // T = R11^{-1} R12 in place (rows 0..rank-1, columns rank..M-1).
-  for (int c = rank + tid; c < M; c += nt) {
-    for (int i = rank - 1; i >= 0; i--) {
-      T s = W[(i64)i * M + c];
-      for (int k = i + 1; k < rank; k++) s -= W[(i64)i * M + k] * W[(i64)k * M + c];
-      W[(i64)i * M + c] = s / W[(i64)i * M + i];
+  // T = R11^{-1} R12 in place (rows 0..rank-1, columns rank..M-1), by
+  // column chunks staged in shared memory: back substitution with the whole
+  // CTA updating the rows above the current one (one barrier per row).
+  {
+    T* X = taus + M;  // rank x nc, row-major
+    const int nc = min(32, xcap / rank);
+    for (int c0 = rank; c0 < M; c0 += nc) {
+      const int w = min(nc, M - c0);
+      for (int e = tid; e < rank * w; e += nt) X[e] = W[(i64)(e / w) * M + c0 + e % w];
+      __syncthreads();
+      for (int i = rank - 1; i >= 0; i--) {
+        const T rii = W[(i64)i * M + i];
+        for (int e = tid; e < i * w; e += nt) {
+          const int k = e / w, c = e % w;
+          X[e] -= W[(i64)k * M + i] * (X[i * w + c] / rii);
+        }
+        __syncthreads();
+      }
+      for (int e = tid; e < rank * w; e += nt) {
+        const int i = e / w;
+        W[(i64)i * M + c0 + e % w] = X[e] / W[(i64)i * M + i];
+      }
+      __syncthreads();
     }
   }
   // Skeleton-first order of the box bodies.
@@ -354,6 +373,12 @@ __global__ void __launch_bounds__(256) k_basis_finish(
     Rb[(i64)perm[k] + (i64)i * M] = v;
   }
   __syncthreads();
+  if (wy_taus) {
+    // Blocked completion on the host side: U_ID is in R's slot, Q still
+    // holds Q_in; the caller forms triu(Q_in) U_ID, its QR and Q.
+    if (tid == 0) ranks_out[box] = rank;
+    return;
+  }
   for (i64 e = tid; e < (i64)M * rank; e += nt) {
     int p = (int)(e % M), i = (int)(e / M);
     T s;
@@ -405,7 +430,7 @@ __global__ void __launch_bounds__(256) k_basis_finish(
     int r = (int)(e % M), c = (int)(e / M);
     Rb[e] = (c < rank && r <= c) ? W[r + (i64)c * M] : T(0);
   }
-  // Q = H_0 ... H_{rank-1} applied to the identity, accumulated backwards.
+  // Q = H_0 ... H_{rank-1} applied to the identity.
   for (i64 e = tid; e < (i64)M * M; e += nt) {
     int r = (int)(e % M), c = (int)(e / M);
     Qb[e] = r == c ? T(1) : T(0);
@@ -464,14 +489,16 @@ template <typename T>
 cudaError_t launch_basis_finish(const i64* dims, const i64* krows, T* Rws, T* Q, T* R, const i64* qoff,
                                 const int* perm, const i64* xoff, const double* maxpiv, const int* nonzero,
                                 double* pts, i64* ranks, double epi, int orth, int qin_identity, int nboxes,
-                                int maxM, cudaStream_t st) {
+                                int maxM, cudaStream_t st, T* wy_taus) {
   if (nboxes == 0) return cudaSuccess;
-  size_t smem = ((4 * (size_t)maxM + 15) / 16) * 16 + sizeof(double) * 3 * maxM + sizeof(T) * (maxM + 32) + 64;
+  // Back-substitution chunk: up to 32 columns of rank rows, at most 96 KB.
+  const int xcap = (int)std::min<size_t>((size_t)maxM * 32, 96 * 1024 / sizeof(T));
+  size_t smem = ((4 * (size_t)maxM + 15) / 16) * 16 + sizeof(double) * 3 * maxM + sizeof(T) * (maxM + xcap) + 64;
   auto fn = k_basis_finish<T>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   fn<<<nboxes, 256, smem, st>>>(dims, krows, Rws, Q, R, qoff, perm, xoff, maxpiv, nonzero, pts, ranks, epi, orth,
-                                qin_identity);
+                                qin_identity, wy_taus, xcap);
   return cudaGetLastError();
 }
 
@@ -483,7 +510,7 @@ cudaError_t launch_basis_finish(const i64* dims, const i64* krows, T* Rws, T* Q,
                                       i64, int, int, cudaStream_t);                                               \
   template cudaError_t launch_basis_finish<T>(const i64*, const i64*, T*, T*, T*, const i64*, const int*,         \
                                               const i64*, const double*, const int*, double*, i64*, double, int,  \
-                                              int, int, int, cudaStream_t);
+                                              int, int, int, cudaStream_t, T*);
 INST(double)
 INST(float)
 #undef INST
@@ -618,5 +645,304 @@ cudaError_t launch_gather_points(const double* bodies, const int* idx, i64 n, do
   k_gather_points<<<grid, 256, 0, st>>>(bodies, idx, n, out);
   return cudaGetLastError();
 }
+
+}  // namespace h2b
+
+namespace h2b {
+
+// One 32-pivot panel of the blocked pivoted Cholesky of G = XF^T XF.  G (M x M
+// per box, symmetric) already carries the trailing updates of earlier panels;
+// the pivots of this panel are taken left-looking: the Schur diagonal of the
+// remaining columns lives in shared memory and loses R[k][j]^2 after every
+// pivot, and row k of R is G[k][j] minus the panel's earlier rows.  The
+// caller applies G_trail -= R_panel^T R_panel (one batched GEMM) afterwards.
+// Pivot rule, noise rule and R layout are those of k_pivchol.
+__global__ void __launch_bounds__(256) k_pivchol_panel(const i64* __restrict__ dims, const i64* __restrict__ steps_box,
+                                                       double* __restrict__ G, double* __restrict__ Rws,
+                                                       const i64* __restrict__ qoff, int* __restrict__ perm_g,
+                                                       const i64* __restrict__ xoff, double* __restrict__ state,
+                                                       int k0, int nb) {
+  const int box = blockIdx.x;
+  const int M = (int)dims[box];
+  const int steps = (int)steps_box[box];
+  if (M == 0 || k0 >= steps) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* dsch = reinterpret_cast<double*>(smem_raw);  // M
+  __shared__ double red_v[32];
+  __shared__ int red_i[32];
+  double* g = G + qoff[box];
+  double* R = Rws + qoff[box];
+  int* perm = perm_g + xoff[box];
+  double* st = state + 3 * (i64)box;  // [rfloor, noise threshold, noise flag]
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (k0 == 0) {
+    for (int c = tid; c < M; c += nt) perm[c] = c;
+    double dmax = 0.;
+    int dmi = 0;
+    for (int j = tid; j < M; j += nt) {
+      double v = g[(i64)j * M + j];
+      if (v > dmax) { dmax = v; dmi = j; }
+    }
+    argmax_first(dmax, dmi, red_v, red_i);
+    if (tid == 0) {
+      double rf = sqrt(DBL_EPSILON * dmax);
+      st[0] = rf > 0. ? rf : DBL_MIN;
+      st[1] = 16. * DBL_EPSILON * dmax;
+      st[2] = 0.;
+    }
+    __syncthreads();
+  }
+  const double rfloor = st[0], noise = st[1];
+  bool noise_mode = st[2] != 0.;
+  for (int j = tid; j < M; j += nt) dsch[j] = j >= k0 ? g[(i64)j * M + j] : 0.;
+  __syncthreads();
+  const int kend = (k0 + nb < steps) ? k0 + nb : steps;
+  for (int k = k0; k < kend; k++) {
+    double bv = -1.;
+    int bi = 0x7fffffff;
+    for (int j = k + tid; j < M; j += nt)
+      if (dsch[j] > bv) { bv = dsch[j]; bi = j; }
+    argmax_first(bv, bi, red_v, red_i);
+    if (bi < k || bi >= M) bi = k;
+    if (bi != k) {
+      // Rows/columns k0.. of G are the live trailing matrix; earlier rows of
+      // R (all panels) follow the column exchange.
+      for (int c = k0 + tid; c < M; c += nt) {
+        double t = g[(i64)k * M + c];
+        g[(i64)k * M + c] = g[(i64)bi * M + c];
+        g[(i64)bi * M + c] = t;
+      }
+      __syncthreads();
+      for (int r = k0 + tid; r < M; r += nt) {
+        double t = g[(i64)r * M + k];
+        g[(i64)r * M + k] = g[(i64)r * M + bi];
+        g[(i64)r * M + bi] = t;
+      }
+      for (int r = tid; r < k; r += nt) {
+        double t = R[(i64)r * M + k];
+        R[(i64)r * M + k] = R[(i64)r * M + bi];
+        R[(i64)r * M + bi] = t;
+      }
+      if (tid == 0) {
+        double t = dsch[k]; dsch[k] = dsch[bi]; dsch[bi] = t;
+        int ti = perm[k]; perm[k] = perm[bi]; perm[bi] = ti;
+      }
+    }
+    __syncthreads();
+    const double d = dsch[k];
+    if (!(d > noise)) noise_mode = true;
+    if (noise_mode) {
+      for (int j = k + tid; j < M; j += nt) R[(i64)k * M + j] = (j == k) ? rfloor : 0.;
+      __syncthreads();
+      continue;
+    }
+    const double rkk = sqrt(d);
+    const double inv = 1. / rkk;
+    for (int j = k + tid; j < M; j += nt) {
+      double v;
+      if (j == k) {
+        v = rkk;
+      } else {
+        v = g[(i64)k * M + j];
+        for (int p = k0; p < k; p++) v -= R[(i64)p * M + k] * R[(i64)p * M + j];
+        v *= inv;
+        dsch[j] -= v * v;
+      }
+      R[(i64)k * M + j] = v;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) st[2] = noise_mode ? 1. : 0.;
+}
+
+cudaError_t launch_pivchol_panel(const i64* dims, const i64* steps_box, double* G, double* Rws, const i64* qoff,
+                                 int* perm, const i64* xoff, double* state, int k0, int nb, int nboxes, int maxM,
+                                 cudaStream_t st) {
+  if (nboxes == 0) return cudaSuccess;
+  size_t smem = sizeof(double) * (size_t)maxM + 16;
+  k_pivchol_panel<<<nboxes, 256, smem, st>>>(dims, steps_box, G, Rws, qoff, perm, xoff, state, k0, nb);
+  return cudaGetLastError();
+}
+
+}  // namespace h2b
+
+namespace h2b {
+
+// T of the compact-WY form Q = H_0 ... H_{r-1} = I - V T V^T (forward,
+// column by column: T[i][i] = tau_i, T[0:i, i] = -tau_i T[0:i,0:i] S[0:i, i]
+// with S = V^T V), one CTA per box, r x r column-major at Tb + toff[box].
+template <typename T>
+__global__ void __launch_bounds__(256) k_wy_t(const WyTask<T>* __restrict__ tasks) {
+  const WyTask<T> t = tasks[blockIdx.x];
+  const int r = t.r;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* col = reinterpret_cast<T*>(smem_raw);  // r
+  for (i64 e = threadIdx.x; e < (i64)r * r; e += blockDim.x) t.Tm[e] = T(0);
+  __syncthreads();
+  for (int i = 0; i < r; i++) {
+    const T tau = t.taus[i];
+    for (int j = threadIdx.x; j < i; j += blockDim.x) col[j] = -tau * t.S[j + (i64)i * r];
+    __syncthreads();
+    for (int j = threadIdx.x; j < i; j += blockDim.x) {
+      T v = T(0);
+      for (int l = j; l < i; l++) v += t.Tm[j + (i64)l * r] * col[l];
+      t.Tm[j + (i64)i * r] = v;
+    }
+    if (threadIdx.x == 0) t.Tm[i + (i64)i * r] = tau;
+    __syncthreads();
+  }
+}
+
+template <typename T>
+cudaError_t launch_wy_t(const WyTask<T>* d_tasks, int ntasks, int maxr, cudaStream_t st) {
+  if (ntasks == 0) return cudaSuccess;
+  k_wy_t<T><<<ntasks, 256, sizeof(T) * (size_t)(maxr + 2), st>>>(d_tasks);
+  return cudaGetLastError();
+}
+template cudaError_t launch_wy_t<double>(const WyTask<double>*, int, int, cudaStream_t);
+template cudaError_t launch_wy_t<float>(const WyTask<float>*, int, int, cudaStream_t);
+
+}  // namespace h2b
+
+namespace h2b {
+
+// One Householder panel of the M x rank matrix W (column-major, ld M) of a
+// box: columns k0..k0+nb-1, rows k0..M-1, factored in shared memory with the
+// same reflector convention as k_basis_finish (beta = -sign(c0) * norm).
+// Writes back R (upper) and the reflector tails (lower), the explicit unit
+// lower-trapezoidal V of the panel to Vp ((M-k0) x nb), the panel's
+// compact-WY T (nb x nb, I - V T V^T = H_k0 ... H_k0+nb-1) to Tp and its
+// taus.  The caller applies the panel to the trailing columns with GEMMs.
+template <typename T>
+__global__ void __launch_bounds__(256) k_qr_panel(const QrPanelTask<T>* __restrict__ tasks) {
+  const QrPanelTask<T> t = tasks[blockIdx.x];
+  const int m = t.M - t.k0, nb = t.nb;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* P = reinterpret_cast<T*>(smem_raw);  // m x nb, ld m
+  T* tau = P + (size_t)m * nb;            // nb
+  T* Tl = tau + nb;                       // nb x nb
+  T* sc = Tl + (size_t)nb * nb;           // nb
+  __shared__ T red[32];
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  T* Wp = t.W + (i64)t.k0 + (i64)t.k0 * t.M;
+  for (i64 e = tid; e < (i64)m * nb; e += nt) {
+    int r = (int)(e % m), j = (int)(e / m);
+    P[e] = Wp[r + (i64)j * t.M];
+  }
+  __syncthreads();
+  for (int j = 0; j < nb; j++) {
+    T* cj = P + (size_t)j * m;
+    T part = 0;
+    for (int r = j + 1 + tid; r < m; r += nt) part += cj[r] * cj[r];
+    T tsq = BlockReduce<T>::sum(part, red);
+    T c0 = cj[j];
+    T tj = 0, beta = c0, scale = 0;
+    if (tsq > Tiny<T>::v()) {
+      beta = sqrt(c0 * c0 + tsq);
+      if (c0 >= T(0)) beta = -beta;
+      scale = T(1) / (c0 - beta);
+      tj = (beta - c0) / beta;
+    }
+    __syncthreads();
+    for (int r = j + 1 + tid; r < m; r += nt) cj[r] *= scale;
+    if (tid == 0) {
+      cj[j] = beta;
+      tau[j] = tj;
+    }
+    __syncthreads();
+    if (tj != T(0))
+      for (int jj = j + 1 + warp; jj < nb; jj += nw) {
+        T* c2 = P + (size_t)jj * m;
+        T w = 0;
+        for (int r = j + 1 + lane; r < m; r += 32) w += cj[r] * c2[r];
+        for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        w = (w + c2[j]) * tj;
+        if (lane == 0) c2[j] -= w;
+        for (int r = j + 1 + lane; r < m; r += 32) c2[r] -= w * cj[r];
+      }
+    __syncthreads();
+  }
+  // S[l][i] = V(:,l)^T V(:,i) for l < i (V unit lower: V[i][i] = 1, zero above).
+  for (int pr = warp; pr < nb * nb; pr += nw) {
+    int l = pr % nb, i = pr / nb;
+    if (l >= i) continue;
+    T s = 0;
+    for (int r = i + 1 + lane; r < m; r += 32) s += P[r + (size_t)l * m] * P[r + (size_t)i * m];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) Tl[l + i * nb] = s + P[i + (size_t)l * m];  // row i of V(:,l) times V[i][i] = 1
+  }
+  __syncthreads();
+  // T recurrence, one warp: column i of S is staged in sc, then
+  // T[:i, i] = -tau_i T[:i,:i] S[:i, i] and T[i][i] = tau_i.
+  if (warp == 0) {
+    for (int i = 0; i < nb; i++) {
+      for (int j = lane; j < i; j += 32) sc[j] = Tl[j + i * nb];
+      __syncwarp();
+      for (int j = lane; j < i; j += 32) {
+        T v = 0;
+        for (int l = j; l < i; l++) v += Tl[j + l * nb] * sc[l];
+        Tl[j + i * nb] = -tau[i] * v;
+      }
+      if (lane == 0) Tl[i + i * nb] = tau[i];
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  for (i64 e = tid; e < (i64)m * nb; e += nt) {
+    int r = (int)(e % m), j = (int)(e / m);
+    Wp[r + (i64)j * t.M] = P[e];
+    t.Vp[e] = r < j ? T(0) : (r == j ? T(1) : P[e]);
+  }
+  for (int e = tid; e < nb * nb; e += nt) {
+    int r = e % nb, c = e / nb;
+    t.Tp[e] = r <= c ? Tl[e] : T(0);
+  }
+  for (int j = tid; j < nb; j += nt) t.taus[t.k0 + j] = tau[j];
+}
+
+template <typename T>
+cudaError_t launch_qr_panel(const QrPanelTask<T>* d_tasks, int ntasks, int maxm, int nb, cudaStream_t st) {
+  if (ntasks == 0) return cudaSuccess;
+  size_t smem = sizeof(T) * ((size_t)maxm * nb + 2 * nb + (size_t)nb * nb) + 16;
+  auto fn = k_qr_panel<T>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  fn<<<ntasks, 256, smem, st>>>(d_tasks);
+  return cudaGetLastError();
+}
+template cudaError_t launch_qr_panel<double>(const QrPanelTask<double>*, int, int, int, cudaStream_t);
+template cudaError_t launch_qr_panel<float>(const QrPanelTask<float>*, int, int, int, cudaStream_t);
+
+}  // namespace h2b
+
+namespace h2b {
+
+// After the blocked QR of W (M x rank): R's slot gets triu(W[:rank, :rank]),
+// W becomes the explicit unit lower-trapezoidal V, Q the identity (for the
+// compact-WY formation that follows).
+template <typename T>
+__global__ void __launch_bounds__(256) k_qr_extract(const QrExtractTask<T>* __restrict__ tasks) {
+  const QrExtractTask<T> t = tasks[blockIdx.x];
+  const int M = t.M, r = t.rank;
+  for (i64 e = threadIdx.x; e < (i64)M * M; e += blockDim.x) {
+    int i = (int)(e % M), c = (int)(e / M);
+    t.R[e] = (c < r && i <= c) ? t.W[i + (i64)c * M] : T(0);
+    t.Q[e] = i == c ? T(1) : T(0);
+  }
+  __syncthreads();
+  for (i64 e = threadIdx.x; e < (i64)M * r; e += blockDim.x) {
+    int i = (int)(e % M), c = (int)(e / M);
+    if (i <= c) t.W[e] = i == c ? T(1) : T(0);
+  }
+}
+
+template <typename T>
+cudaError_t launch_qr_extract(const QrExtractTask<T>* d_tasks, int ntasks, cudaStream_t st) {
+  if (ntasks == 0) return cudaSuccess;
+  k_qr_extract<T><<<ntasks, 256, 0, st>>>(d_tasks);
+  return cudaGetLastError();
+}
+template cudaError_t launch_qr_extract<double>(const QrExtractTask<double>*, int, cudaStream_t);
+template cudaError_t launch_qr_extract<float>(const QrExtractTask<float>*, int, cudaStream_t);
 
 }  // namespace h2b

@@ -155,11 +155,11 @@ namespace h2b {
 // one coalesced row of loads, eight columns in flight per thread); B chunks
 // of KC rows are staged in shared memory and read as broadcasts; all NR
 // columns accumulate in registers.  One CTA covers NT*TM rows of one task.
-template <typename T, int NR, int TM>
-__global__ void __launch_bounds__(128) k_skinny_nn(const GemmTask<T>* __restrict__ tasks,
-                                                   const GemmEntry<T>* __restrict__ ents,
-                                                   const int2* __restrict__ tiles) {
-  constexpr int NT = 128, BM = NT * TM, KC = 128, U = 8;
+template <typename T, int NR, int TM, int NT, int U>
+__global__ void __launch_bounds__(NT) k_skinny_nn(const GemmTask<T>* __restrict__ tasks,
+                                                  const GemmEntry<T>* __restrict__ ents,
+                                                  const int2* __restrict__ tiles) {
+  constexpr int BM = NT * TM, KC = 128;
   __shared__ __align__(16) T Bs[KC][NR];
   const int2 tl = tiles[blockIdx.x];
   const GemmTask<T> task = tasks[tl.x];
@@ -272,16 +272,18 @@ template <typename T>
 cudaError_t launch_skinny_nn(int nr, const GemmTask<T>* d_tasks, const GemmEntry<T>* d_ents, const int2* d_tiles,
                              int ntiles, cudaStream_t st) {
   if (ntiles == 0) return cudaSuccess;
+  // Every variant covers 256 rows per CTA: 2 rows per thread, deep load
+  // batches (HBM-latency bound).
   if (nr <= 1)
-    k_skinny_nn<T, 1, 2><<<ntiles, 128, 0, st>>>(d_tasks, d_ents, d_tiles);
+    k_skinny_nn<T, 1, 2, 128, 8><<<ntiles, 128, 0, st>>>(d_tasks, d_ents, d_tiles);
   else if (nr <= 2)
-    k_skinny_nn<T, 2, 2><<<ntiles, 128, 0, st>>>(d_tasks, d_ents, d_tiles);
+    k_skinny_nn<T, 2, 2, 128, 8><<<ntiles, 128, 0, st>>>(d_tasks, d_ents, d_tiles);
   else if (nr <= 4)
-    k_skinny_nn<T, 4, 2><<<ntiles, 128, 0, st>>>(d_tasks, d_ents, d_tiles);
+    k_skinny_nn<T, 4, 2, 128, 8><<<ntiles, 128, 0, st>>>(d_tasks, d_ents, d_tiles);
   else if (nr <= 8)
-    k_skinny_nn<T, 8, 2><<<ntiles, 128, 0, st>>>(d_tasks, d_ents, d_tiles);
+    k_skinny_nn<T, 8, 2, 128, 8><<<ntiles, 128, 0, st>>>(d_tasks, d_ents, d_tiles);
   else if (nr <= 16)
-    k_skinny_nn<T, 16, 2><<<ntiles, 128, 0, st>>>(d_tasks, d_ents, d_tiles);
+    k_skinny_nn<T, 16, 2, 128, 8><<<ntiles, 128, 0, st>>>(d_tasks, d_ents, d_tiles);
   else
     return cudaErrorInvalidValue;
   return cudaGetLastError();

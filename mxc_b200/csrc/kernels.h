@@ -33,10 +33,45 @@ template <typename T>
 cudaError_t launch_basis_finish(const i64* dims, const i64* krows, T* Rws, T* Q, T* R, const i64* qoff,
                                 const int* perm, const i64* xoff, const double* maxpiv, const int* nonzero,
                                 double* pts, i64* ranks, double epi, int orth, int qin_identity, int nboxes,
-                                int maxM, cudaStream_t st);
+                                int maxM, cudaStream_t st, T* wy_taus = nullptr);
+// Compact-WY T matrix per box (see k_wy_t).
+template <typename T>
+struct WyTask {
+  const T* S;     // r x r, V^T V
+  const T* taus;  // r
+  T* Tm;          // r x r output (upper triangular)
+  int r;
+};
+// One Householder panel per box (k_qr_panel).
+template <typename T>
+struct QrPanelTask {
+  T* W;      // M x rank, column-major (ld M)
+  T* Vp;     // (M - k0) x nb explicit V of the panel
+  T* Tp;     // nb x nb
+  T* taus;   // per box, indexed by column
+  int M, k0, nb;
+};
+template <typename T>
+cudaError_t launch_qr_panel(const QrPanelTask<T>* d_tasks, int ntasks, int maxm, int nb, cudaStream_t st);
+template <typename T>
+struct QrExtractTask {
+  T* W;
+  T* R;
+  T* Q;
+  int M, rank;
+};
+template <typename T>
+cudaError_t launch_qr_extract(const QrExtractTask<T>* d_tasks, int ntasks, cudaStream_t st);
+template <typename T>
+cudaError_t launch_wy_t(const WyTask<T>* d_tasks, int ntasks, int maxr, cudaStream_t st);
 
 cudaError_t launch_pivchol(const i64* dims, const i64* krows, double* G, double* Rws, const i64* qoff, int* perm,
                            const i64* xoff, i64 step_cap, int nboxes, int maxM, cudaStream_t st);
+// Blocked pivoted Cholesky: one panel of nb pivots starting at k0 for every
+// box (steps_box[i] pivots in all); state holds 3 doubles per box.
+cudaError_t launch_pivchol_panel(const i64* dims, const i64* steps_box, double* G, double* Rws, const i64* qoff,
+                                 int* perm, const i64* xoff, double* state, int k0, int nb, int nboxes, int maxM,
+                                 cudaStream_t st);
 cudaError_t launch_gather_points(const double* bodies, const int* idx, i64 n, double* out, cudaStream_t st);
 
 // ---------------------------------------------------------------- gemm

@@ -132,3 +132,48 @@ void sample_far_list(const std::vector<std::pair<i64, i64>>& ranges, i64 samples
 }
 
 }  // namespace h2b
+
+namespace h2b {
+
+void sample_far_list_geometric(const std::vector<std::pair<i64, i64>>& ranges, const std::vector<i64>& gstart,
+                               i64 samples, std::vector<int>& out) {
+  const int G = (int)gstart.size();
+  std::vector<i64> gsize(G, 0), alloc(G, 0);
+  i64 total = 0;
+  for (int g = 0; g < G; g++) {
+    i64 r1 = g + 1 < G ? gstart[g + 1] : (i64)ranges.size();
+    for (i64 r = gstart[g]; r < r1; r++) gsize[g] += ranges[r].second - ranges[r].first;
+    total += gsize[g];
+  }
+  out.clear();
+  if (total == 0) return;
+  if (samples <= 0 || samples >= total) {
+    sample_far_list(ranges, 0, out);
+    return;
+  }
+  // Nearest group (the box's own level, last in the list) first: half of
+  // what is left, then half again for each level further out; the farthest
+  // group takes the rest.  Shares a small group cannot use move outward
+  // first and then inward.
+  i64 rem = samples;
+  for (int g = G - 1; g >= 0; g--) {
+    i64 share = g == 0 ? rem : (rem + 1) / 2;
+    alloc[g] = std::min(gsize[g], share);
+    rem -= alloc[g];
+  }
+  for (int g = G - 1; g >= 0 && rem > 0; g--) {
+    i64 extra = std::min(gsize[g] - alloc[g], rem);
+    alloc[g] += extra;
+    rem -= extra;
+  }
+  for (int g = 0; g < G; g++) {
+    if (alloc[g] == 0) continue;
+    i64 r1 = g + 1 < G ? gstart[g + 1] : (i64)ranges.size();
+    std::vector<std::pair<i64, i64>> sub(ranges.begin() + gstart[g], ranges.begin() + r1);
+    std::vector<int> part;
+    sample_far_list(sub, alloc[g] == gsize[g] ? 0 : alloc[g], part);
+    out.insert(out.end(), part.begin(), part.end());
+  }
+}
+
+}  // namespace h2b

@@ -41,6 +41,12 @@ PairCSR build_pair_csr(char kind, const std::vector<Cell>& cells, double theta);
 // keep all, the reference behaviour): row j of the sample is entry
 // floor(j * total / samples) of the concatenated list.
 void sample_far_list(const std::vector<std::pair<i64, i64>>& ranges, i64 samples, std::vector<int>& out_idx);
+// Level-geometric cap: gstart[g] is the first range appended at tree level
+// g+1 (g = 0 farthest, last = the box's own level).  The own-level group gets
+// half of the budget, each level further out half of what is left, the
+// farthest the rest; each group is then strided as in sample_far_list.
+void sample_far_list_geometric(const std::vector<std::pair<i64, i64>>& ranges, const std::vector<i64>& gstart,
+                               i64 samples, std::vector<int>& out_idx);
 
 // Per-level box structure of one H^2 matrix (the single-process view of
 // ColCommMPI: every box of a level is local, comm-mpi.cpp:49-150).

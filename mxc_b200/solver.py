@@ -117,6 +117,19 @@ class Handle:
             out[nm] = (int(nl[k]), float(ms[k]), float(fl[k]), float(by[k]))
         return out
 
+    def profile_timeline(self) -> list:
+        """[(kernel, start ms, device ms)] for every profiled launch, in order."""
+        cnt = C.c_int64()
+        L.check(L.lib().h2dev_profile_timeline(self.h, 0, None, None, None, C.byref(cnt)), "h2dev_profile_timeline")
+        n = cnt.value
+        names = C.create_string_buffer(48 * max(n, 1))
+        t0 = np.zeros(max(n, 1))
+        dt = np.zeros(max(n, 1))
+        L.check(L.lib().h2dev_profile_timeline(self.h, n, names, _ptr(t0), _ptr(dt), C.byref(cnt)),
+                "h2dev_profile_timeline")
+        return [(names.raw[48 * k:48 * k + 48].split(b"\0", 1)[0].decode(), float(t0[k]), float(dt[k]))
+                for k in range(n)]
+
     def fma_peak_tflops(self, precision: int = L.FP64) -> float:
         v = C.c_double()
         L.check(L.lib().h2dev_probe_fma_peak(self.h, precision, C.byref(v)), "h2dev_probe_fma_peak")

@@ -314,12 +314,59 @@ def sample_indices(total: int, samples: int) -> np.ndarray:
     return (j * total) // samples
 
 
-def far_bodies(bodies: np.ndarray, ranges, samples: int) -> np.ndarray:
+def far_body_groups(cells: Cells, far: CSR, levels: int):
+    """{cell: [first range index of each tree-level group]} matching far_body_lists."""
+    lists = far_body_lists(cells, far, levels)
+    groups = {0: []}
+    for l in range(1, levels + 1):
+        for c in range((1 << l) - 1, (1 << (l + 1)) - 1):
+            parent = (c - 1) // 2
+            groups[c] = list(groups[parent]) + [len(lists[parent]) if parent else 0]
+    return groups
+
+
+def geometric_allocation(gsize, samples: int):
+    """Level-geometric split of ``samples`` over groups (last = nearest)."""
+    G = len(gsize)
+    alloc = [0] * G
+    rem = samples
+    for g in range(G - 1, -1, -1):
+        share = rem if g == 0 else (rem + 1) // 2
+        alloc[g] = min(gsize[g], share)
+        rem -= alloc[g]
+    for g in range(G - 1, -1, -1):
+        if rem <= 0:
+            break
+        extra = min(gsize[g] - alloc[g], rem)
+        alloc[g] += extra
+        rem -= extra
+    return alloc
+
+
+def far_bodies(bodies: np.ndarray, ranges, samples: int, gstart=None, mode: int = 0) -> np.ndarray:
+    """Rows of a box's far list kept under ``samples``: mode 0 strided over the
+    whole list, mode 1 level-geometric (build extensions; samples <= 0 keeps all)."""
     if not ranges:
         return np.zeros((0, 3))
     idx = np.concatenate([np.arange(b0, b1, dtype=np.int64) for b0, b1 in ranges])
-    keep = sample_indices(len(idx), samples)
-    return bodies[idx[keep]]
+    total = len(idx)
+    if mode == 0 or samples <= 0 or samples >= total:
+        keep = sample_indices(total, samples)
+        return bodies[idx[keep]]
+    bounds = list(gstart) + [len(ranges)]
+    parts = []
+    gidx = []
+    for g in range(len(gstart)):
+        sub = ranges[bounds[g]:bounds[g + 1]]
+        gidx.append(np.concatenate([np.arange(b0, b1, dtype=np.int64) for b0, b1 in sub]) if sub
+                    else np.zeros(0, dtype=np.int64))
+    alloc = geometric_allocation([len(x) for x in gidx], samples)
+    for g, x in enumerate(gidx):
+        if alloc[g] == 0:
+            continue
+        keep = sample_indices(len(x), 0 if alloc[g] == len(x) else alloc[g])
+        parts.append(x[keep])
+    return bodies[np.concatenate(parts)]
 
 
 # --------------------------------------------------------------------------
@@ -519,7 +566,7 @@ class H2MatrixSolver:
     """
 
     def __init__(self, kern: Kernel, epi: float, rank: int, leveled_rank: int, cells: Cells,
-                 theta: float, bodies: np.ndarray, levels: int, samples: int = 0):
+                 theta: float, bodies: np.ndarray, levels: int, samples: int = 0, sampling: int = 0):
         self.kern = kern
         self.levels = levels
         self.cells = cells
@@ -530,6 +577,8 @@ class H2MatrixSolver:
         far_list_csr = build_csr("F", cells, 0.0) if fix_rank else far
         self.near, self.far = near, far
         ranges = far_body_lists(cells, far_list_csr, levels)
+        self.gstart = far_body_groups(cells, far_list_csr, levels)
+        self.sampling = sampling
         self.A: list[Level] = []
         for l in range(levels + 1):
             ar, ac = _level_csr(near, l)
@@ -603,7 +652,8 @@ class H2MatrixSolver:
                         lev.A[ij][:] = gen_matrix(kern, bodies[b0:b1], bodies[cells.body[cj, 0]:cells.body[cj, 1]])
 
             for i in range(nodes):
-                fb = far_bodies(bodies, ranges.get(g0 + i, []), samples)
+                fb = far_bodies(bodies, ranges.get(g0 + i, []), samples, self.gstart.get(g0 + i, []),
+                                self.sampling)
                 rank, c = compute_basis(kern, epi, lev.S[i], fb, lev.Q[i], 1.0 <= epi)
                 lev.R[i] = c
                 lev.DimsLr[i] = rank
