@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="one profiled step, no timing (for ncu)")
+    ap.add_argument("--profile-phase", default="step", choices=["step", "build", "factor", "solve"],
+                    help="with --profile-only: the part of the step bracketed by cudaProfilerStart/Stop "
+                         "(for ncu --profile-from-start off)")
     return ap.parse_args()
 
 
@@ -194,21 +197,33 @@ def run_ours(a):
     dX = torch.zeros_like(dXt)
     torch.cuda.synchronize()
 
+    def bracket(phase, on):
+        # cudaProfilerStart/Stop around the selected phase of a --profile-only step.
+        if a.profile_only and a.profile_phase in ("step", phase):
+            h.synchronize()
+            (torch.cuda.profiler.start if on else torch.cuda.profiler.stop)()
+
     def step(precision, profile=False):
         dX.zero_()
         torch.cuda.synchronize()
         if profile:
             h.profile(True)
+        bracket("build", True)
         h.timer_start()
         M = m.H2MatrixSolver(h, k, 0.0, a.rank, 0, tree, a.theta, b, samples=a.samples, precision=precision)
         t_build = h.timer_stop()
+        bracket("build", False)
+        bracket("factor", True)
         h.timer_start()
         M.factorizeM()
         t_fact = h.timer_stop()
+        bracket("factor", False)
+        bracket("solve", True)
         h.timer_start()
         rc, resid, iters = A.gmres_device(M, a.tol, dX.data_ptr(), dB.data_ptr(), a.nrhs, a.n, a.inner, a.outer,
                                           bool(a.early_exit))
         t_solve = h.timer_stop()
+        bracket("solve", False)
         M.close()
         final = [float(resid[int(iters[c]), c]) for c in range(a.nrhs)]
         return {"build_ms": t_build, "factor_ms": t_fact, "solve_ms": t_solve,

@@ -5,6 +5,7 @@
 // is read in place from HBM (comm-mpi.cpp:198-225 become no-ops).
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <functional>
 #include <memory>
@@ -1817,11 +1818,12 @@ int h2dev_handle_create(int device, h2dev_handle_t* out) {
     delete h;
     ck(e, "cudaStreamCreate");
   }
-  // Keep up to 32 GB of freed stream-ordered memory in this process's pool
-  // between calls (the default returns it to the driver at every sync).
+  // Keep freed stream-ordered memory in this process's pool between calls
+  // (the default returns it to the driver at every synchronisation, and the
+  // next factorization maps it again); the last handle destroyed trims it.
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-    uint64_t keep = (uint64_t)32 << 30;
+    uint64_t keep = UINT64_MAX;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
   }
   cudaGetLastError();
@@ -1841,6 +1843,9 @@ static void handle_release(h2dev_handle_s* h) {
   if (h->t0) cudaEventDestroy(h->t0);
   if (h->t1) cudaEventDestroy(h->t1);
   cudaStreamDestroy(h->stream);
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, h->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+  cudaGetLastError();
   delete h;
 }
 

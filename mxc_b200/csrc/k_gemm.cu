@@ -8,6 +8,8 @@
 #include "common.cuh"
 #include "kernels.h"
 
+#include <cstdint>
+
 namespace h2b {
 
 template <typename T, int BM, int BN, int BK, int TM, int TN>
@@ -150,89 +152,159 @@ namespace h2b {
 // Multi-right-hand-side block-sparse apply: C_task (m x n, n <= NR) =
 // beta C + sum_e alpha_e A_e B_e with A_e and B_e as stored (column-major).
 // This is the shape of every H^2 matvec pass and every ULV substitution
-// step except the transposed ones.  A is read once, straight from HBM into
-// registers (consecutive threads own consecutive rows, so each k column is
-// one coalesced row of loads, eight columns in flight per thread); B chunks
-// of KC rows are staged in shared memory and read as broadcasts; all NR
-// columns accumulate in registers.  One CTA covers NT*TM rows of one task.
-template <typename T, int NR, int TM, int NT, int U>
-__global__ void __launch_bounds__(NT) k_skinny_nn(const GemmTask<T>* __restrict__ tasks,
-                                                  const GemmEntry<T>* __restrict__ ents,
-                                                  const int2* __restrict__ tiles) {
-  constexpr int BM = NT * TM, KC = 128;
-  __shared__ __align__(16) T Bs[KC][NR];
+// step except the transposed ones, and it is bound by streaming A from HBM
+// once.  One CTA (128 threads) covers 256 rows of a task.  The (entry,
+// k-slab) sequence of the task is one stream of stages: each stage is a
+// 256 x KS slab of A and the KS x NR slab of B, copied by cp.async into a
+// ST-deep shared-memory ring (16-byte copies where the column starts are
+// 16-byte aligned, element copies otherwise; rows past m and k past K are
+// zero-filled), so ST-1 slabs are in flight while one is multiplied.  Each
+// thread owns two adjacent rows and all NR columns; B rows are read as
+// shared-memory broadcasts.  alpha_e != 1 scales the B slab in place.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp_async_16(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes));
+}
+template <int N>
+__device__ __forceinline__ void cp_async_ca(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(smem_u32(dst)), "l"(src), "n"(N),
+               "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+template <typename T>
+struct StreamCfg;
+template <>
+struct StreamCfg<double> { static constexpr int KS = 16, ST = 3; };
+template <>
+struct StreamCfg<float> { static constexpr int KS = 32, ST = 3; };
+
+constexpr int STREAM_NT = 128, STREAM_BM = 256;
+
+template <typename T, int NR>
+constexpr size_t stream_smem() {
+  return sizeof(T) * (size_t)StreamCfg<T>::ST * StreamCfg<T>::KS * (STREAM_BM + NR);
+}
+
+template <typename T, int NR>
+__global__ void __launch_bounds__(STREAM_NT) k_stream_nn(const GemmTask<T>* __restrict__ tasks,
+                                                         const GemmEntry<T>* __restrict__ ents,
+                                                         const int2* __restrict__ tiles) {
+  constexpr int KS = StreamCfg<T>::KS, ST = StreamCfg<T>::ST, BM = STREAM_BM, NT = STREAM_NT;
+  constexpr int V = 16 / sizeof(T);  // elements per 16-byte copy
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* As = reinterpret_cast<T*>(smem_raw);  // [ST][KS][BM]
+  T* Bs = As + (size_t)ST * KS * BM;       // [ST][KS][NR]
   const int2 tl = tiles[blockIdx.x];
   const GemmTask<T> task = tasks[tl.x];
   const int m0 = tl.y * BM;
+  const int mrows = min(BM, task.m - m0);
   const int tid = threadIdx.x;
-  T acc[TM][NR];
+
+  // Producer cursor: next (entry, k0) to stage.
+  int pe = task.e0, pk = 0;
+  while (pe < task.e1 && ents[pe].k <= 0) pe++;
+  auto issue = [&](int slot) {
+    if (pe < task.e1) {
+      const GemmEntry<T> en = ents[pe];
+      T* as = As + (size_t)slot * KS * BM;
+      T* bs = Bs + (size_t)slot * KS * NR;
+      const bool vec = ((reinterpret_cast<uintptr_t>(en.A) & 15) == 0) && (en.lda % V == 0);
+      if (vec) {
+        for (int c = tid; c < KS * (BM / V); c += NT) {
+          const int k = c / (BM / V), r = (c % (BM / V)) * V;
+          int valid = mrows - r;
+          valid = valid < 0 ? 0 : (valid > V ? V : valid);
+          if (pk + k >= en.k) valid = 0;
+          const T* src = valid ? en.A + (i64)(m0 + r) + (i64)(pk + k) * en.lda : en.A;
+          cp_async_16(as + k * BM + r, src, valid * (int)sizeof(T));
+        }
+      } else {
+        for (int c = tid; c < KS * BM; c += NT) {
+          const int k = c / BM, r = c % BM;
+          const bool ok = r < mrows && pk + k < en.k;
+          const T* src = ok ? en.A + (i64)(m0 + r) + (i64)(pk + k) * en.lda : en.A;
+          cp_async_ca<sizeof(T)>(as + k * BM + r, src, ok ? (int)sizeof(T) : 0);
+        }
+      }
+      for (int c = tid; c < KS * NR; c += NT) {
+        const int k = c / NR, j = c % NR;
+        const bool ok = j < task.n && pk + k < en.k;
+        const T* src = ok ? en.B + (i64)(pk + k) + (i64)j * en.ldb : en.B;
+        cp_async_ca<sizeof(T)>(bs + c, src, ok ? (int)sizeof(T) : 0);
+      }
+      pk += KS;
+      if (pk >= en.k) {
+        pk = 0;
+        pe++;
+        while (pe < task.e1 && ents[pe].k <= 0) pe++;
+      }
+    }
+    cp_async_commit();
+  };
+
+  T acc[2][NR];
 #pragma unroll
-  for (int t = 0; t < TM; t++)
+  for (int t = 0; t < 2; t++)
 #pragma unroll
     for (int j = 0; j < NR; j++) acc[t][j] = T(0);
-  bool rv[TM];
-#pragma unroll
-  for (int t = 0; t < TM; t++) rv[t] = (m0 + tid + t * NT) < task.m;
 
-  for (int e = task.e0; e < task.e1; e++) {
-    const GemmEntry<T> en = ents[e];
-    const int K = en.k;
-    const T* Ab = en.A + (m0 + tid);
-    for (int k0 = 0; k0 < K; k0 += KC) {
-      const int kc = (K - k0) < KC ? (K - k0) : KC;
-      for (int idx = tid; idx < KC * NR; idx += NT) {
-        int kk = idx % KC, j = idx / KC;
-        Bs[kk][j] = (kk < kc && j < task.n) ? en.B[(i64)(k0 + kk) + (i64)j * en.ldb] : T(0);
-      }
-      __syncthreads();
-      // Two register batches of U columns of A: the loads of the next batch
-      // are in flight while the current one is multiplied.
-      T a0[U][TM], a1[U][TM];
 #pragma unroll
-      for (int u = 0; u < U; u++)
-#pragma unroll
-        for (int t = 0; t < TM; t++)
-          a0[u][t] = (u < kc && rv[t]) ? en.alpha * Ab[(i64)(k0 + u) * en.lda + t * NT] : T(0);
-      for (int kb = 0; kb < kc; kb += 2 * U) {
-#pragma unroll
-        for (int u = 0; u < U; u++)
-#pragma unroll
-          for (int t = 0; t < TM; t++)
-            a1[u][t] = (kb + U + u < kc && rv[t]) ? en.alpha * Ab[(i64)(k0 + kb + U + u) * en.lda + t * NT] : T(0);
-#pragma unroll
-        for (int u = 0; u < U; u++)
-#pragma unroll
-          for (int j = 0; j < NR; j++) {
-            const T bj = Bs[kb + u][j];
-#pragma unroll
-            for (int t = 0; t < TM; t++) acc[t][j] += a0[u][t] * bj;
-          }
-#pragma unroll
-        for (int u = 0; u < U; u++)
-#pragma unroll
-          for (int t = 0; t < TM; t++)
-            a0[u][t] = (kb + 2 * U + u < kc && rv[t]) ? en.alpha * Ab[(i64)(k0 + kb + 2 * U + u) * en.lda + t * NT]
-                                                       : T(0);
-#pragma unroll
-        for (int u = 0; u < U; u++)
-#pragma unroll
-          for (int j = 0; j < NR; j++) {
-            const T bj = Bs[(kb + U + u) < KC ? kb + U + u : KC - 1][j];
-#pragma unroll
-            for (int t = 0; t < TM; t++) acc[t][j] += a1[u][t] * bj;
-          }
-      }
-      __syncthreads();
+  for (int s = 0; s < ST - 1; s++) issue(s);
+  // Consumer cursor.
+  int ce = task.e0, ck = 0;
+  while (ce < task.e1 && ents[ce].k <= 0) ce++;
+  int slot = 0;
+  while (ce < task.e1) {
+    const T alpha = ents[ce].alpha;
+    cp_async_wait<ST - 2>();
+    if (alpha != T(1)) {
+      // Scale the B elements this thread copied into the slot.
+      T* bs = Bs + (size_t)slot * KS * NR;
+      for (int c = tid; c < KS * NR; c += NT) bs[c] *= alpha;
     }
-  }
+    __syncthreads();
+    issue((slot + ST - 1) % ST);
+    const T* as = As + (size_t)slot * KS * BM + 2 * tid;
+    const T* bs = Bs + (size_t)slot * KS * NR;
+#pragma unroll 4
+    for (int k = 0; k < KS; k++) {
+      T a0, a1;
+      if constexpr (sizeof(T) == 8) {
+        const double2 v = *reinterpret_cast<const double2*>(as + k * BM);
+        a0 = v.x;
+        a1 = v.y;
+      } else {
+        const float2 v = *reinterpret_cast<const float2*>(as + k * BM);
+        a0 = v.x;
+        a1 = v.y;
+      }
 #pragma unroll
-  for (int t = 0; t < TM; t++) {
-    if (!rv[t]) continue;
-    const int r = m0 + tid + t * NT;
+      for (int j = 0; j < NR; j++) {
+        const T bj = bs[k * NR + j];
+        acc[0][j] += a0 * bj;
+        acc[1][j] += a1 * bj;
+      }
+    }
+    ck += KS;
+    if (ck >= ents[ce].k) {
+      ck = 0;
+      ce++;
+      while (ce < task.e1 && ents[ce].k <= 0) ce++;
+    }
+    slot = (slot + 1) % ST;
+  }
+  cp_async_wait<0>();
+#pragma unroll
+  for (int t = 0; t < 2; t++) {
+    const int r = 2 * tid + t;
+    if (r >= mrows) continue;
 #pragma unroll
     for (int j = 0; j < NR; j++) {
       if (j >= task.n) break;
-      T* p = task.C + r + (i64)j * task.ldc;
+      T* p = task.C + (m0 + r) + (i64)j * task.ldc;
       *p = (task.beta == T(0)) ? acc[t][j] : task.beta * (*p) + acc[t][j];
     }
   }
@@ -272,21 +344,19 @@ template <typename T>
 cudaError_t launch_skinny_nn(int nr, const GemmTask<T>* d_tasks, const GemmEntry<T>* d_ents, const int2* d_tiles,
                              int ntiles, cudaStream_t st) {
   if (ntiles == 0) return cudaSuccess;
-  // Every variant covers 256 rows per CTA: 2 rows per thread, deep load
-  // batches (HBM-latency bound).
-  if (nr <= 1)
-    k_skinny_nn<T, 1, 2, 128, 8><<<ntiles, 128, 0, st>>>(d_tasks, d_ents, d_tiles);
-  else if (nr <= 2)
-    k_skinny_nn<T, 2, 2, 128, 8><<<ntiles, 128, 0, st>>>(d_tasks, d_ents, d_tiles);
-  else if (nr <= 4)
-    k_skinny_nn<T, 4, 2, 128, 8><<<ntiles, 128, 0, st>>>(d_tasks, d_ents, d_tiles);
-  else if (nr <= 8)
-    k_skinny_nn<T, 8, 2, 128, 8><<<ntiles, 128, 0, st>>>(d_tasks, d_ents, d_tiles);
-  else if (nr <= 16)
-    k_skinny_nn<T, 16, 2, 128, 8><<<ntiles, 128, 0, st>>>(d_tasks, d_ents, d_tiles);
-  else
-    return cudaErrorInvalidValue;
-  return cudaGetLastError();
+  // Every variant covers 256 rows per CTA (two per thread).
+  auto go = [&](auto kern, size_t smem) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<ntiles, STREAM_NT, smem, st>>>(d_tasks, d_ents, d_tiles);
+    return cudaGetLastError();
+  };
+  if (nr <= 1) return go(k_stream_nn<T, 1>, stream_smem<T, 1>());
+  if (nr <= 2) return go(k_stream_nn<T, 2>, stream_smem<T, 2>());
+  if (nr <= 4) return go(k_stream_nn<T, 4>, stream_smem<T, 4>());
+  if (nr <= 8) return go(k_stream_nn<T, 8>, stream_smem<T, 8>());
+  if (nr <= 16) return go(k_stream_nn<T, 16>, stream_smem<T, 16>());
+  return cudaErrorInvalidValue;
 }
 template cudaError_t launch_skinny_nn<double>(int, const GemmTask<double>*, const GemmEntry<double>*, const int2*, int,
                                               cudaStream_t);
