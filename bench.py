@@ -332,6 +332,8 @@ def run_ours(a):
             "phases_ms": {"build": sum(r["build_ms"] for r in runs) / len(runs),
                           "factor": sum(r["factor_ms"] for r in runs) / len(runs),
                           "solve": sum(r["solve_ms"] for r in runs) / len(runs)},
+            "steps_ms": [[round(r["build_ms"], 2), round(r["factor_ms"], 2), round(r["solve_ms"], 2)] for r in runs],
+            "e2e_steps_ms": [round(v, 2) for v in e2e_ms],
             "gmres_cycles": runs[-1]["iters"],
             "converged": all(r["rc"] == 0 for r in runs),
             "h2_resid_max": max(runs[-1]["resid"]),

@@ -74,7 +74,10 @@ int h2dev_handle_synchronize(h2dev_handle_t h);
  * rows floor(j * total / samples) of the whole list.  1: level-geometric —
  * the far boxes of the box's own level (the nearest) get half of the budget,
  * each level further out half of what remains, each group strided as in 0. */
-enum { H2DEV_OPT_BASIS = 0, H2DEV_OPT_SKINNY_TILED = 1, H2DEV_OPT_SAMPLING = 2 };
+/* H2DEV_OPT_TENSOR_CORES: 1 (default) runs the FP32 block contractions of
+ * plans built afterwards (in this process) on the tcgen05 tensor cores with
+ * a 3-term TF32 split (FP32 accuracy); 0 runs them on the SIMT kernel. */
+enum { H2DEV_OPT_BASIS = 0, H2DEV_OPT_SKINNY_TILED = 1, H2DEV_OPT_SAMPLING = 2, H2DEV_OPT_TENSOR_CORES = 3 };
 int h2dev_set_option(h2dev_handle_t h, int option, int64_t value);
 
 /* ---- solver (solver.hpp:11-47 H2MatrixSolver) ------------------------ */
@@ -182,6 +185,16 @@ int h2dev_profile_enable(h2dev_handle_t h, int on);
  * *count receives the number of distinct kernels. */
 int h2dev_profile_report(h2dev_handle_t h, int64_t cap, char* names, int64_t* launches, double* ms, double* flops,
                          double* bytes, int64_t* count);
+/* Strided-batched GEMM through the solver's segmented-GEMM engine (device
+ * pointers, column-major, element type by `precision`): for b < batch,
+ * C_b = beta C_b + alpha sum_{t < nterms} op(A_{b,t}) op(B_{b,t}), where
+ * X_{b,t} = X + (b * nterms + t) * strideX, op(X) = X (op 0) or X^T (op 1),
+ * op(A) m x k, op(B) k x n.  The contraction engine of the factorization,
+ * exposed for testing and reuse; no reference counterpart. */
+int h2dev_batched_gemm_device(h2dev_handle_t h, int precision, int64_t batch, int64_t nterms, int64_t m, int64_t n,
+                              int64_t k, int opA, int opB, double alpha, const void* A, int64_t lda, int64_t strideA,
+                              const void* B, int64_t ldb, int64_t strideB, double beta, void* C, int64_t ldc,
+                              int64_t strideC);
 /* Per-launch records since profiling was enabled, in launch order: names
  * (48 bytes each), start (ms after the first record's start) and device
  * duration; idle gaps between records show host-side stalls.  *count

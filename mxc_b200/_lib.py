@@ -28,6 +28,7 @@ FP32 = 1
 OPT_BASIS = 0
 OPT_SKINNY_TILED = 1
 OPT_SAMPLING = 2
+OPT_TENSOR_CORES = 3
 BASIS_GRAM, BASIS_HOUSEHOLDER = 0, 1
 
 EXPORT_S, EXPORT_Q, EXPORT_R, EXPORT_A, EXPORT_C = range(5)
@@ -74,6 +75,8 @@ SIGNATURES = {
     "h2dev_profile_enable": (C.c_int, [_vp, C.c_int]),
     "h2dev_profile_report": (C.c_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _i64p]),
     "h2dev_profile_timeline": (C.c_int, [_vp, _i64, _vp, _vp, _vp, _i64p]),
+    "h2dev_batched_gemm_device": (C.c_int, [_vp, C.c_int, _i64, _i64, _i64, _i64, _i64, C.c_int, C.c_int, C.c_double,
+                                            _vp, _i64, _i64, _vp, _i64, _i64, C.c_double, _vp, _i64, _i64]),
     "h2dev_probe_fma_peak": (C.c_int, [_vp, C.c_int, _dp]),
     "h2dev_timer_start": (C.c_int, [_vp]),
     "h2dev_timer_stop": (C.c_int, [_vp, _dp]),

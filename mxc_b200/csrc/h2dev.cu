@@ -11,6 +11,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -68,89 +69,150 @@ static void require(bool ok, const char* what) {
   if (!ok) throw H2Error{H2DEV_ERR_ARG, what};
 }
 
-// Host->device copy through the handle's pinned staging buffer: the host
-// bytes are copied into pinned memory at once and the DMA is queued on the
-// handle's stream.  A full buffer is reused when its last copy has run,
-// otherwise replaced by one twice the size (the old one is freed once its
-// copies are done); past 512 MB the call waits for the buffer instead.
-static void stage_copy(h2dev_handle_s* h, void* dst, const void* src, size_t bytes) {
-  const size_t need = (bytes + 255) & ~(size_t)255;
-  for (size_t k = 0; k < h->stage_retired.size();) {
-    auto& r = h->stage_retired[k];
-    if (cudaEventQuery(r.second) == cudaSuccess) {
-      cudaFreeHost(r.first);
-      cudaEventDestroy(r.second);
-      h->stage_retired.erase(h->stage_retired.begin() + (long)k);
-    } else {
+// Host->device copy through the handle's pinned ring (64 MB): the bytes are
+// copied into pinned memory at once and the DMA is queued on the handle's
+// stream.  When the ring has no room, the call waits for the oldest copy in
+// flight to finish; uploads larger than half the ring go in pieces.
+constexpr size_t STAGE_BYTES = (size_t)64 << 20;
+
+static void stage_reclaim(h2dev_handle_s* h) {
+  while (!h->stage_inflight.empty()) {
+    cudaError_t q = cudaEventQuery(h->stage_inflight.front().ev);
+    if (q == cudaErrorNotReady) {
       cudaGetLastError();
-      k++;
+      return;
     }
+    ck(q, "stage event");
+    h->stage_events.push_back(h->stage_inflight.front().ev);
+    h->stage_inflight.pop_front();
   }
-  if (h->stage_head + need > h->stage_cap) {
-    bool reuse = false;
-    if (h->stage && need <= h->stage_cap) {
-      cudaError_t q = cudaEventQuery(h->stage_ev);
-      if (q == cudaSuccess) {
-        reuse = true;
-      } else if (h->stage_cap >= ((size_t)512 << 20)) {
-        cudaGetLastError();
-        ck(cudaEventSynchronize(h->stage_ev), "stage wait");
-        reuse = true;
-      } else {
-        cudaGetLastError();
+}
+
+static char* stage_reserve(h2dev_handle_s* h, size_t need) {
+  if (!h->stage) {
+    ck(cudaHostAlloc((void**)&h->stage, STAGE_BYTES, cudaHostAllocDefault), "cudaHostAlloc");
+    h->stage_cap = STAGE_BYTES;
+    h->stage_head = 0;
+  }
+  for (;;) {
+    stage_reclaim(h);
+    if (h->stage_inflight.empty()) h->stage_head = 0;
+    const size_t head = h->stage_head, cap = h->stage_cap;
+    size_t pos = SIZE_MAX;
+    if (h->stage_inflight.empty()) {
+      pos = 0;
+    } else {
+      const size_t tail = h->stage_inflight.front().start;
+      if (head > tail) {
+        if (cap - head >= need) pos = head;
+        else if (tail >= need) pos = 0;
+      } else if (head < tail && tail - head >= need) {
+        pos = head;
       }
     }
-    if (reuse) {
-      h->stage_head = 0;
-    } else {
-      if (h->stage) h->stage_retired.emplace_back(h->stage, h->stage_ev);
-      h->stage = nullptr;
-      h->stage_ev = nullptr;
-      const size_t cap = std::max(std::max(need, 2 * h->stage_cap), (size_t)8 << 20);
-      h->stage_cap = 0;
-      h->stage_head = 0;
-      ck(cudaHostAlloc((void**)&h->stage, cap, cudaHostAllocDefault), "cudaHostAlloc");
-      ck(cudaEventCreateWithFlags(&h->stage_ev, cudaEventDisableTiming), "cudaEventCreate");
-      h->stage_cap = cap;
+    if (pos != SIZE_MAX) {
+      h->stage_head = pos + need;
+      return h->stage + pos;
     }
+    // No room: wait for the oldest copy in flight.
+    ck(cudaEventSynchronize(h->stage_inflight.front().ev), "stage wait");
   }
-  char* buf = h->stage + h->stage_head;
-  std::memcpy(buf, src, bytes);
-  ck(cudaMemcpyAsync(dst, buf, bytes, cudaMemcpyHostToDevice, h->stream), "upload");
-  ck(cudaEventRecord(h->stage_ev, h->stream), "cudaEventRecord");
-  h->stage_head += need;
+}
+
+static void stage_copy(h2dev_handle_s* h, void* dst, const void* src, size_t bytes) {
+  const size_t piece = STAGE_BYTES / 2;
+  for (size_t o = 0; o < bytes; o += piece) {
+    const size_t nb = std::min(piece, bytes - o);
+    const size_t need = (nb + 255) & ~(size_t)255;
+    char* buf = stage_reserve(h, need);
+    std::memcpy(buf, static_cast<const char*>(src) + o, nb);
+    ck(cudaMemcpyAsync(static_cast<char*>(dst) + o, buf, nb, cudaMemcpyHostToDevice, h->stream), "upload");
+    cudaEvent_t ev;
+    if (!h->stage_events.empty()) {
+      ev = h->stage_events.back();
+      h->stage_events.pop_back();
+    } else {
+      ck(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+    }
+    ck(cudaEventRecord(ev, h->stream), "cudaEventRecord");
+    h->stage_inflight.push_back(h2dev_handle_s::StageRec{(size_t)(buf - h->stage), (size_t)(buf - h->stage) + need, ev});
+  }
 }
 
 static void stage_release(h2dev_handle_s* h) {
-  for (auto& r : h->stage_retired) {
-    cudaFreeHost(r.first);
-    cudaEventDestroy(r.second);
+  for (auto& r : h->stage_inflight) {
+    cudaEventSynchronize(r.ev);
+    cudaEventDestroy(r.ev);
   }
-  h->stage_retired.clear();
+  h->stage_inflight.clear();
+  for (cudaEvent_t e : h->stage_events) cudaEventDestroy(e);
+  h->stage_events.clear();
   if (h->stage) cudaFreeHost(h->stage);
-  if (h->stage_ev) cudaEventDestroy(h->stage_ev);
   h->stage = nullptr;
-  h->stage_ev = nullptr;
   h->stage_cap = h->stage_head = 0;
 }
 
+// Size classes of the handle's device-memory cache: four per octave (at
+// most 25% rounding), 512 bytes at least.
+static size_t cache_class(size_t bytes) {
+  size_t b = std::max<size_t>(bytes, 512);
+  int p = 63 - __builtin_clzll((unsigned long long)b);
+  if (b == ((size_t)1 << p)) return b;
+  const size_t step = (size_t)1 << (p - 2);
+  return (b + step - 1) / step * step;
+}
+
+// Returns every cached block to the driver (after the stream drains).
+static void cache_trim(h2dev_handle_s* h) {
+  if (h->cached_bytes == 0) return;
+  cudaStreamSynchronize(h->stream);
+  for (auto& kv : h->cache)
+    for (void* p : kv.second) cudaFree(p);
+  h->cache.clear();
+  h->cached_bytes = 0;
+}
+
+static void* cache_alloc(h2dev_handle_s* h, size_t cls) {
+  auto it = h->cache.find(cls);
+  if (it != h->cache.end() && !it->second.empty()) {
+    void* p = it->second.back();
+    it->second.pop_back();
+    h->cached_bytes -= cls;
+    return p;
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, cls);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    cache_trim(h);
+    e = cudaMalloc(&p, cls);
+  }
+  ck(e, "cudaMalloc");
+  return p;
+}
+
+static void cache_free(h2dev_handle_s* h, void* p, size_t cls) {
+  h->cache[cls].push_back(p);
+  h->cached_bytes += cls;
+}
+
 // Device array.  Inside an API call (a current handle) memory comes from the
-// device's stream-ordered pool on the handle's stream and is returned to it
-// in stream order, so temporaries need no synchronisation before they go.
+// handle's cache and goes back to it when released; all its users are on the
+// handle's stream, so temporaries need no synchronisation before they go.
 template <typename T>
 struct DVec {
   T* p = nullptr;
   size_t n = 0;
-  cudaStream_t s = nullptr;  // stream of a stream-ordered allocation
-  bool ordered = false;
+  h2dev_handle_s* owner = nullptr;  // cache the block came from (none: plain cudaMalloc)
+  size_t cls = 0;
   DVec() = default;
   DVec(const DVec&) = delete;
   DVec& operator=(const DVec&) = delete;
-  DVec(DVec&& o) noexcept : p(o.p), n(o.n), s(o.s), ordered(o.ordered) { o.p = nullptr; o.n = 0; }
+  DVec(DVec&& o) noexcept : p(o.p), n(o.n), owner(o.owner), cls(o.cls) { o.p = nullptr; o.n = 0; }
   DVec& operator=(DVec&& o) noexcept {
     if (this != &o) {
       release();
-      p = o.p; n = o.n; s = o.s; ordered = o.ordered;
+      p = o.p; n = o.n; owner = o.owner; cls = o.cls;
       o.p = nullptr; o.n = 0;
     }
     return *this;
@@ -158,10 +220,10 @@ struct DVec {
   ~DVec() { release(); }
   void release() {
     if (p) {
-      if (!ordered || cudaFreeAsync(p, s) != cudaSuccess) {
-        cudaGetLastError();
+      if (owner)
+        cache_free(owner, p, cls);
+      else
         cudaFree(p);
-      }
     }
     p = nullptr;
     n = 0;
@@ -169,13 +231,14 @@ struct DVec {
   void alloc(size_t count) {
     if (count == n && p) return;
     release();
-    ordered = g_cur != nullptr;
-    s = ordered ? g_cur->stream : nullptr;
+    owner = g_cur;
     if (count) {
-      if (ordered)
-        ck(cudaMallocAsync((void**)&p, count * sizeof(T), s), "cudaMallocAsync");
-      else
+      if (owner) {
+        cls = cache_class(count * sizeof(T));
+        p = static_cast<T*>(cache_alloc(owner, cls));
+      } else {
         ck(cudaMalloc((void**)&p, count * sizeof(T)), "cudaMalloc");
+      }
     }
     n = count;
   }
@@ -185,7 +248,7 @@ struct DVec {
   void upload(const std::vector<T>& v) {
     alloc(v.size());
     if (v.empty()) return;
-    if (ordered && g_cur && g_cur->stream == s)
+    if (owner && g_cur == owner)
       stage_copy(g_cur, p, v.data(), v.size() * sizeof(T));
     else
       ck(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
@@ -204,6 +267,16 @@ struct DVec {
 // H2DEV_OPT_SKINNY_TILED, used to compare the two kernels).
 static bool g_force_tiled = false;
 static bool force_tiled() { return g_force_tiled; }
+// Process-wide switch for the tcgen05 FP32 contractions (H2DEV_OPT_TENSOR_CORES).
+static bool g_tensor_cores = true;
+
+// Throws when a tensor-core GEMM launched since the last check reported an
+// expired wait (synchronises the stream).
+static void check_tc(cudaStream_t st) {
+  int flag = 0;
+  ck(tc_gemm_take_error(&flag, st), "tensor-core GEMM status");
+  if (flag) throw H2Error{H2DEV_ERR_CUDA, "tensor-core GEMM: an mbarrier wait expired"};
+}
 
 // Host-built list of segmented-GEMM tasks, uploaded once and replayed.
 template <typename T>
@@ -241,6 +314,7 @@ struct GemmPlan {
     int maxn = 0;
     for (auto& t : tasks) maxn = std::max(maxn, t.n);
     shape = maxn <= 16 ? GEMM_SKINNY : GEMM_BIG;
+    if (std::is_same<T, float>::value && shape == GEMM_BIG && g_tensor_cores) shape = GEMM_TC;
     bool nn = true;
     for (const auto& e : ents) nn = nn && e.opA == 0 && e.opB == 0;
     skinny_nn = nn && maxn <= 16 && !force_tiled();
@@ -257,7 +331,8 @@ struct GemmPlan {
       }
       d_rtiles.upload(rt);
     }
-    int bm = gemm_tile_m(shape), bn = gemm_tile_n(shape);
+    int bm = shape == GEMM_TC ? tc_gemm_tile() : gemm_tile_m(shape);
+    int bn = shape == GEMM_TC ? tc_gemm_tile() : gemm_tile_n(shape);
     std::vector<TileRef> tiles;
     for (int ti = 0; ti < (int)tasks.size(); ti++) {
       const auto& t = tasks[ti];
@@ -358,8 +433,12 @@ struct GemmPlan {
     if (skinny_nn) {
       ck(launch_skinny_nn<T>(nr, d_tasks.p, d_ents.p, d_rtiles.p, (int)d_rtiles.n, st), "skinny_nn");
       if (nsums) ck(launch_sum_parts<T>(d_sums.p, nsums, st), "sum_parts");
-    } else
+    } else if (shape == GEMM_TC) {
+      if constexpr (std::is_same<T, float>::value)
+        ck(launch_tc_gemm(d_tasks.p, d_ents.p, d_tiles.p, ntiles, st), "tc_gemm");
+    } else {
       ck(launch_seg_gemm<T>(shape, d_tasks.p, d_ents.p, d_tiles.p, ntiles, st), "seg_gemm");
+    }
   }
 };
 
@@ -412,6 +491,23 @@ struct Level {
   // per-nrhs vectors
   DVec<T> vX, vZ, vW;
 };
+
+template <typename T>
+void batched_gemm(int64_t batch, int64_t nterms, int64_t m, int64_t n, int64_t k, int opA, int opB,
+                         double alpha, const T* A, int64_t lda, int64_t sA, const T* B, int64_t ldb, int64_t sB,
+                         double beta, T* C, int64_t ldc, int64_t sC, cudaStream_t st) {
+  GemmPlan<T> g;
+  g.name = "batched_gemm";
+  for (int64_t b = 0; b < batch; b++) {
+    g.add_task(C + b * sC, ldc, (int)m, (int)n, (T)beta);
+    for (int64_t t = 0; t < nterms; t++)
+      g.add_entry(A + (b * nterms + t) * sA, lda, opA, B + (b * nterms + t) * sB, ldb, opB, (int)k, (T)alpha);
+  }
+  g.finalize();
+  g.run(st);
+  check_tc(st);
+}
+
 
 class SolverBase {
  public:
@@ -522,6 +618,7 @@ class Solver : public SolverBase {
       lv.na_ld.assign(lv.acol.size(), 0);
     }
     for (i64 l = levels; l >= 0; l--) construct_level(l, ranges);
+    check_tc(st());
   }
 
   double level_epi(i64 l) const {
@@ -628,16 +725,35 @@ class Solver : public SolverBase {
       }
 
       // Shared basis of every box (compute_basis, h2matrix.cpp:252-257).
-      std::vector<int> sidx, tmp;
+      // Far-sample lists of all boxes, built by up to 8 host threads over
+      // contiguous box ranges and concatenated in box order.
+      std::vector<int> sidx;
       std::vector<i64> soff(nodes + 1, 0), krows(nodes, 0);
-      for (i64 i = 0; i < nodes; i++) {
-        if (sampling_mode == 1)
-          sample_far_list_geometric(ranges[g0 + i], gstart[g0 + i], samples, tmp);
-        else
-          sample_far_list(ranges[g0 + i], samples, tmp);
-        sidx.insert(sidx.end(), tmp.begin(), tmp.end());
-        soff[i + 1] = (i64)sidx.size();
-        krows[i] = std::min<i64>(lv.dims[i], (i64)tmp.size());
+      {
+        const int nth = (int)std::max<i64>(1, std::min<i64>({8, (i64)std::thread::hardware_concurrency(), nodes / 16}));
+        std::vector<std::vector<int>> part(nth);
+        std::vector<i64> cnt(nodes, 0);
+        auto work = [&](int t) {
+          std::vector<int> tmp;
+          for (i64 i = nodes * t / nth; i < nodes * (t + 1) / nth; i++) {
+            if (sampling_mode == 1)
+              sample_far_list_geometric(ranges[g0 + i], gstart[g0 + i], samples, tmp);
+            else
+              sample_far_list(ranges[g0 + i], samples, tmp);
+            part[t].insert(part[t].end(), tmp.begin(), tmp.end());
+            cnt[i] = (i64)tmp.size();
+          }
+        };
+        std::vector<std::thread> th;
+        for (int t = 1; t < nth; t++) th.emplace_back(work, t);
+        work(0);
+        for (auto& x : th) x.join();
+        for (i64 i = 0; i < nodes; i++) {
+          soff[i + 1] = soff[i] + cnt[i];
+          krows[i] = std::min<i64>(lv.dims[i], cnt[i]);
+        }
+        sidx.reserve(soff[nodes]);
+        for (auto& v : part) sidx.insert(sidx.end(), v.begin(), v.end());
       }
       DVec<int> d_sidx, d_perm, d_nonzero;
       DVec<i64> d_soff, d_krows;
@@ -1409,6 +1525,7 @@ class Solver : public SolverBase {
       factor_level(l);
       if (l > 0) copy_next(l);
     }
+    check_tc(st());
     // Singular-block counts per level, read once after the last level.
     for (i64 l = 0; l <= levels; l++) {
       std::vector<int> inf = L[l].info.download(st());
@@ -1818,15 +1935,6 @@ int h2dev_handle_create(int device, h2dev_handle_t* out) {
     delete h;
     ck(e, "cudaStreamCreate");
   }
-  // Keep freed stream-ordered memory in this process's pool between calls
-  // (the default returns it to the driver at every synchronisation, and the
-  // next factorization maps it again); the last handle destroyed trims it.
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-    uint64_t keep = UINT64_MAX;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-  }
-  cudaGetLastError();
   *out = h;
   return H2DEV_OK;
   H2_API_END
@@ -1842,10 +1950,8 @@ static void handle_release(h2dev_handle_s* h) {
   for (cudaEvent_t e : h->pool) cudaEventDestroy(e);
   if (h->t0) cudaEventDestroy(h->t0);
   if (h->t1) cudaEventDestroy(h->t1);
+  cache_trim(h);
   cudaStreamDestroy(h->stream);
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, h->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
-  cudaGetLastError();
   delete h;
 }
 
@@ -2163,6 +2269,31 @@ int h2dev_profile_report(h2dev_handle_t h, int64_t cap, char* names, int64_t* la
   H2_API_END
 }
 
+int h2dev_batched_gemm_device(h2dev_handle_t h, int precision, int64_t batch, int64_t nterms, int64_t m, int64_t n,
+                              int64_t k, int opA, int opB, double alpha, const void* A, int64_t lda, int64_t strideA,
+                              const void* B, int64_t ldb, int64_t strideB, double beta, void* C, int64_t ldc,
+                              int64_t strideC) {
+  H2_API_BEGIN
+  require(h && A && B && C, "null argument");
+  require(precision == H2DEV_FP64 || precision == H2DEV_FP32, "precision");
+  require(batch >= 0 && nterms >= 0 && m >= 0 && n >= 0 && k >= 0, "negative size");
+  require(m < (1 << 30) && n < (1 << 30) && k < (1 << 30), "size too large");
+  require((opA == 0 || opA == 1) && (opB == 0 || opB == 1), "op must be 0 or 1");
+  require(lda >= std::max<int64_t>(1, opA ? k : m) && ldb >= std::max<int64_t>(1, opB ? n : k) &&
+              ldc >= std::max<int64_t>(1, m),
+          "leading dimension too small");
+  ck(cudaSetDevice(h->device), "cudaSetDevice");
+  CurHandle ch(h);
+  if (precision == H2DEV_FP64)
+    batched_gemm<double>(batch, nterms, m, n, k, opA, opB, alpha, (const double*)A, lda, strideA, (const double*)B,
+                         ldb, strideB, beta, (double*)C, ldc, strideC, h->stream);
+  else
+    batched_gemm<float>(batch, nterms, m, n, k, opA, opB, alpha, (const float*)A, lda, strideA, (const float*)B, ldb,
+                        strideB, beta, (float*)C, ldc, strideC, h->stream);
+  return H2DEV_OK;
+  H2_API_END
+}
+
 int h2dev_profile_timeline(h2dev_handle_t h, int64_t cap, char* names, double* start_ms, double* dur_ms,
                            int64_t* count) {
   H2_API_BEGIN
@@ -2220,6 +2351,11 @@ int h2dev_set_option(h2dev_handle_t h, int option, int64_t value) {
   if (option == H2DEV_OPT_SKINNY_TILED) {
     require(value == 0 || value == 1, "skinny option must be 0 or 1");
     g_force_tiled = value != 0;
+    return H2DEV_OK;
+  }
+  if (option == H2DEV_OPT_TENSOR_CORES) {
+    require(value == 0 || value == 1, "tensor-core option must be 0 or 1");
+    g_tensor_cores = value != 0;
     return H2DEV_OK;
   }
   if (option == H2DEV_OPT_SAMPLING) {

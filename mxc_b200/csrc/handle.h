@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include <deque>
+#include <unordered_map>
 #include <utility>
 #include <vector>
 
@@ -27,12 +29,24 @@ struct h2dev_handle_s {
   // One reference held by the caller plus one per live solver: the stream
   // (and the stream-ordered memory freed on it) outlives every solver.
   int refs = 1;
-  // Pinned staging buffer for host->device uploads of launch plans, so an
-  // upload is stream-ordered and never waits for queued kernels.
+  // Pinned ring buffer for host->device uploads of launch plans, so an
+  // upload is stream-ordered and does not wait for queued kernels.  Each
+  // copy in flight is a FIFO record (its byte range and an event recorded
+  // after it); space is reclaimed as those events complete.
+  struct StageRec {
+    size_t start, end;
+    cudaEvent_t ev;
+  };
   char* stage = nullptr;
   size_t stage_cap = 0, stage_head = 0;
-  cudaEvent_t stage_ev = nullptr;  // recorded after the latest copy out of `stage`
-  std::vector<std::pair<char*, cudaEvent_t>> stage_retired;
+  std::deque<StageRec> stage_inflight;
+  std::vector<cudaEvent_t> stage_events;  // completed records' events, for reuse
+  // Device memory cache: blocks freed by this handle's solvers and
+  // temporaries, by size class.  Every block is used only on `stream`, so a
+  // block freed in stream order is reusable at once by later work; steady
+  // state factorizations then make no driver allocation calls.
+  std::unordered_map<size_t, std::vector<void*>> cache;
+  size_t cached_bytes = 0;
   std::vector<ProfRec> recs;
   std::vector<cudaEvent_t> pool;
   cudaEvent_t t0 = nullptr, t1 = nullptr;

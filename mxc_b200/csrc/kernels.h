@@ -96,7 +96,7 @@ struct GemmTask {
 struct TileRef {
   int task, tm, tn;
 };
-enum GemmShape { GEMM_BIG = 0, GEMM_SKINNY = 1 };
+enum GemmShape { GEMM_BIG = 0, GEMM_SKINNY = 1, GEMM_TC = 2 };
 template <typename T>
 cudaError_t launch_seg_gemm(int shape, const GemmTask<T>* d_tasks, const GemmEntry<T>* d_ents, const TileRef* d_tiles,
                             int ntiles, cudaStream_t st);
@@ -121,6 +121,12 @@ struct SumTask {
 template <typename T>
 cudaError_t launch_sum_parts(const SumTask<T>* d_tasks, int ntasks, cudaStream_t st);
 int gemm_tile_n(int shape);
+// FP32 segmented GEMM on the tcgen05 tensor cores (3-term TF32 split),
+// 128 x 128 output tiles (TileRef over tc_gemm_tile()-sized tiles).
+cudaError_t launch_tc_gemm(const GemmTask<float>* d_tasks, const GemmEntry<float>* d_ents, const TileRef* d_tiles,
+                           int ntiles, cudaStream_t st);
+int tc_gemm_tile();
+cudaError_t tc_gemm_take_error(int* flag, cudaStream_t st);
 
 template <typename T>
 struct CopyEntry {
