@@ -201,6 +201,9 @@ int h2dev_batched_gemm_device(h2dev_handle_t h, int precision, int64_t batch, in
  * receives the number of records. */
 int h2dev_profile_timeline(h2dev_handle_t h, int64_t cap, char* names, double* start_ms, double* dur_ms,
                            int64_t* count);
+/* Number of kernels this library has launched in this process so far (all
+ * handles); the difference across a region counts its launches. */
+int h2dev_launch_count(int64_t* count);
 /* Measured FMA throughput (TFLOP/s, 2 flops per FMA) of plain FP64 or FP32
  * SIMT code on this device: the denominator for the FP64/FP32 kernels. */
 int h2dev_probe_fma_peak(h2dev_handle_t h, int precision, double* tflops);

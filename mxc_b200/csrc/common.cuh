@@ -102,4 +102,9 @@ __device__ __forceinline__ void argmax_first(double& v, int& idx, double* sv, in
   __syncthreads();
 }
 
+// Host-side count of kernel launches made by this library (process-wide);
+// every launcher calls note_launch() once per kernel it launches.
+void note_launch();
+long long launch_count();
+
 }  // namespace h2b

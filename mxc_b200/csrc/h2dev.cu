@@ -292,7 +292,7 @@ struct GemmPlan {
   double flops = 0., bytes = 0.;  // algorithmic work of one run
   bool skinny_nn = false;          // use k_skinny_nn instead of the tiled kernel
   int nr = 0;
-  DVec<int2> d_rtiles;
+  DVec<int2> d_rtiles, d_rtiles_w;  // row tiles of the 128- and 256-row streaming variants
   DVec<T> parts_buf;               // partial results of split tasks
   DVec<SumTask<T>> d_sums;
   int nsums = 0;
@@ -321,15 +321,19 @@ struct GemmPlan {
     nr = maxn;
     if (skinny_nn) split_tasks();
     if (skinny_nn) {
-      const int rb = skinny_rows_per_cta();
-      std::vector<int2> rt;
+      // Tasks of at most 128 rows go to the 128-row variant, the rest to
+      // the 256-row one (two launches back to back).
+      std::vector<int2> rt[2];
       for (int ti = 0; ti < (int)tasks.size(); ti++) {
         const auto& t = tasks[ti];
         if (t.m <= 0 || t.n <= 0) continue;
         if (t.e0 == t.e1 && t.beta == T(1)) continue;
-        for (int a = 0; a < (t.m + rb - 1) / rb; a++) rt.push_back(make_int2(ti, a));
+        const int wide = t.m > skinny_rows_per_cta(0) ? 1 : 0;
+        const int rb = skinny_rows_per_cta(wide);
+        for (int a = 0; a < (t.m + rb - 1) / rb; a++) rt[wide].push_back(make_int2(ti, a));
       }
-      d_rtiles.upload(rt);
+      d_rtiles.upload(rt[0]);
+      d_rtiles_w.upload(rt[1]);
     }
     int bm = shape == GEMM_TC ? tc_gemm_tile() : gemm_tile_m(shape);
     int bn = shape == GEMM_TC ? tc_gemm_tile() : gemm_tile_n(shape);
@@ -431,7 +435,8 @@ struct GemmPlan {
   void run(cudaStream_t st) const {
     Prof p(name, flops, bytes);
     if (skinny_nn) {
-      ck(launch_skinny_nn<T>(nr, d_tasks.p, d_ents.p, d_rtiles.p, (int)d_rtiles.n, st), "skinny_nn");
+      ck(launch_skinny_nn<T>(nr, 1, d_tasks.p, d_ents.p, d_rtiles_w.p, (int)d_rtiles_w.n, st), "skinny_nn");
+      ck(launch_skinny_nn<T>(nr, 0, d_tasks.p, d_ents.p, d_rtiles.p, (int)d_rtiles.n, st), "skinny_nn");
       if (nsums) ck(launch_sum_parts<T>(d_sums.p, nsums, st), "sum_parts");
     } else if (shape == GEMM_TC) {
       if constexpr (std::is_same<T, float>::value)
@@ -488,6 +493,12 @@ struct Level {
   std::vector<i64> boff, ioff;
   DVec<int> ipiv, info;
   int info_count = 0;
+  // Transposed copies for the multi-RHS applies, so every apply streams
+  // its matrix as stored: Qt = Q[:, :rank]^T (rank x M per box at qtoff) for
+  // the upward pass, Rt = (factor's R slot)^T (M x M at qoff) for the ULV
+  // forward substitution.
+  DVec<T> Qt, Rt;
+  std::vector<i64> qtoff;
   // per-nrhs vectors
   DVec<T> vX, vZ, vW;
 };
@@ -548,8 +559,8 @@ class Solver : public SolverBase {
   // per-nrhs state
   i64 cur_nrhs = -1;
   DVec<T> vin, vout;
-  GemmPlan<T> mv_leaf;
-  std::vector<GemmPlan<T>> mv_up, mv_h, mv_down;
+  GemmPlan<T> mv_leaf, mv_far;
+  std::vector<GemmPlan<T>> mv_up, mv_down;
   std::vector<GemmPlan<T>> pc_fx, pc_fz, pc_bx, pc_by;
   std::vector<CopyPlan<T>> pc_fcopy, pc_bcopy;
   bool mv_built = false, pc_built = false;
@@ -1193,14 +1204,31 @@ class Solver : public SolverBase {
   }
 
   // H^2 matvec plans (h2matrix.cpp:308-401) for the current nrhs.
+  // Multi-RHS H^2 matvec plans (h2matrix.cpp:303-344): upward pass
+  // Z_l = Q_l^T X_l (from the transposed copies), one launch for the far
+  // couplings of every level W_l = sum_j C_ij Z_j (all levels read finished
+  // upward results and write their own W), then the downward pass
+  // W_{l+1} += Q_l W_l level by level and the leaf Y = Q W + sum_j A_ij X_j.
   void build_matvec(i64 nrhs) {
     const int nr = (int)nrhs;
     mv_up.clear();
-    mv_h.clear();
     mv_down.clear();
     mv_up.resize(levels + 1);
-    mv_h.resize(levels + 1);
     mv_down.resize(levels + 1);
+    {
+      CopyPlan<T> tp;
+      for (i64 l = 0; l <= levels; l++) {
+        Level<T>& lv = L[l];
+        lv.qtoff.assign(lv.nodes + 1, 0);
+        for (i64 i = 0; i < lv.nodes; i++) lv.qtoff[i + 1] = lv.qtoff[i] + lv.ranks[i] * lv.dims[i];
+        lv.Qt.alloc(std::max<i64>(1, lv.qtoff[lv.nodes]));
+        for (i64 i = 0; i < lv.nodes; i++)
+          tp.add(lv.Q.p + lv.qoff[i], lv.dims[i], lv.Qt.p + lv.qtoff[i], lv.ranks[i], (int)lv.ranks[i],
+                 (int)lv.dims[i], 1);
+      }
+      tp.finalize();
+      tp.run(st());
+    }
     for (i64 l = levels; l >= 0; l--) {
       Level<T>& lv = L[l];
       const T* X = (l == levels) ? vin.p : L[l + 1].vZ.p;
@@ -1211,36 +1239,36 @@ class Solver : public SolverBase {
         int M = (int)lv.dims[i], r = (int)lv.ranks[i];
         if (r == 0) continue;
         g.add_task(lv.vZ.p + lv.zoff[i], lv.lenZ, r, nr, T(0));
-        g.add_entry(lv.Q.p + lv.qoff[i], M, 1, X + lv.xoff[i], ldx, 0, M, T(1));
+        g.add_entry(lv.Qt.p + lv.qtoff[i], r, 0, X + lv.xoff[i], ldx, 0, M, T(1));
       }
       g.finalize();
     }
+    mv_far = GemmPlan<T>();
+    mv_far.name = "gemm_matvec_far";
     for (i64 l = 0; l <= levels; l++) {
       Level<T>& lv = L[l];
-      GemmPlan<T>& g = mv_h[l];
-      g.name = l == levels ? "gemm_matvec_far_leaf" : "gemm_matvec_far_upper";
-      const T beta = (l == 0) ? T(0) : T(1);
       for (i64 i = 0; i < lv.nodes; i++) {
         int r = (int)lv.ranks[i];
         if (r == 0) continue;
-        g.add_task(lv.vW.p + lv.zoff[i], lv.lenZ, r, nr, beta);
+        mv_far.add_task(lv.vW.p + lv.zoff[i], lv.lenZ, r, nr, T(0));
         for (i64 k = lv.crow[i]; k < lv.crow[i + 1]; k++) {
           i64 j = lv.ccol[k];
-          g.add_entry(lv.C.p + lv.coff[k], r, 0, lv.vZ.p + lv.zoff[j], lv.lenZ, 0, (int)lv.ranks[j], T(1));
+          mv_far.add_entry(lv.C.p + lv.coff[k], r, 0, lv.vZ.p + lv.zoff[j], lv.lenZ, 0, (int)lv.ranks[j], T(1));
         }
       }
-      g.finalize();
-      if (l < levels) {
-        GemmPlan<T>& d = mv_down[l];
-        d.name = "gemm_matvec_down";
-        Level<T>& nx = L[l + 1];  // Y_l lives in W_{l+1}
-        for (i64 i = 0; i < lv.nodes; i++) {
-          int M = (int)lv.dims[i], r = (int)lv.ranks[i];
-          d.add_task(nx.vW.p + lv.xoff[i], nx.lenZ, M, nr, T(0));
-          d.add_entry(lv.Q.p + lv.qoff[i], M, 0, lv.vW.p + lv.zoff[i], lv.lenZ, 0, r, T(1));
-        }
-        d.finalize();
+    }
+    mv_far.finalize();
+    for (i64 l = 0; l < levels; l++) {
+      Level<T>& lv = L[l];
+      GemmPlan<T>& d = mv_down[l];
+      d.name = "gemm_matvec_down";
+      Level<T>& nx = L[l + 1];  // Y_l lives in W_{l+1}
+      for (i64 i = 0; i < lv.nodes; i++) {
+        int M = (int)lv.dims[i], r = (int)lv.ranks[i];
+        d.add_task(nx.vW.p + lv.xoff[i], nx.lenZ, M, nr, T(1));
+        d.add_entry(lv.Q.p + lv.qoff[i], M, 0, lv.vW.p + lv.zoff[i], lv.lenZ, 0, r, T(1));
       }
+      d.finalize();
     }
     {
       Level<T>& lv = L[levels];
@@ -1284,11 +1312,8 @@ class Solver : public SolverBase {
     if (!mv_built) build_matvec(nrhs);
     stage_in(nrhs, dX, ldx);
     for (i64 l = levels; l >= 0; l--) mv_up[l].run(st());
-    for (i64 l = 0; l < levels; l++) {
-      mv_h[l].run(st());
-      mv_down[l].run(st());
-    }
-    mv_h[levels].run(st());
+    mv_far.run(st());
+    for (i64 l = 0; l < levels; l++) mv_down[l].run(st());
     mv_leaf.run(st());
     stage_out(nrhs, dX, ldx);
   }
@@ -1543,6 +1568,17 @@ class Solver : public SolverBase {
     pc_fx.clear(); pc_fz.clear(); pc_bx.clear(); pc_by.clear(); pc_fcopy.clear(); pc_bcopy.clear();
     pc_fx.resize(levels + 1); pc_fz.resize(levels + 1); pc_bx.resize(levels + 1); pc_by.resize(levels + 1);
     pc_fcopy.resize(levels + 1); pc_bcopy.resize(levels + 1);
+    {
+      CopyPlan<T> tp;
+      for (i64 l = 0; l <= levels; l++) {
+        Level<T>& lv = L[l];
+        lv.Rt.alloc(std::max<i64>(1, lv.qoff[lv.nodes]));
+        for (i64 i = 0; i < lv.nodes; i++)
+          tp.add(lv.R.p + lv.qoff[i], lv.dims[i], lv.Rt.p + lv.qoff[i], lv.dims[i], (int)lv.dims[i], (int)lv.dims[i], 1);
+      }
+      tp.finalize();
+      tp.run(st());
+    }
     for (i64 l = 0; l <= levels; l++) {
       Level<T>& lv = L[l];
       const T* Yin = (l == levels) ? vin.p : L[l + 1].vZ.p;
@@ -1556,7 +1592,7 @@ class Solver : public SolverBase {
         if (M == 0) continue;
         // forward: X = V Y; Z = X_s - sum_j A_ij[:Ms, Ns:] X_j[Ns:]
         pc_fx[l].add_task(X + lv.xoff[i], ldx, M, nr, T(0));
-        pc_fx[l].add_entry(lv.R.p + lv.qoff[i], M, 1, Yin + lv.xoff[i], ldx, 0, M, T(1));
+        pc_fx[l].add_entry(lv.Rt.p + lv.qoff[i], M, 0, Yin + lv.xoff[i], ldx, 0, M, T(1));
         if (Ms > 0) {
           pc_fcopy[l].add(X + lv.xoff[i], ldx, Z + lv.zoff[i], ldz, Ms, nr);
           pc_fz[l].add_task(Z + lv.zoff[i], ldz, Ms, nr, T(1));
@@ -2312,6 +2348,14 @@ int h2dev_profile_timeline(h2dev_handle_t h, int64_t cap, char* names, double* s
     if (start_ms) start_ms[k] = a;
     if (dur_ms) dur_ms[k] = d;
   }
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_launch_count(int64_t* count) {
+  H2_API_BEGIN
+  require(count != nullptr, "null argument");
+  *count = (int64_t)launch_count();
   return H2DEV_OK;
   H2_API_END
 }

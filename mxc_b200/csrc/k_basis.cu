@@ -469,6 +469,7 @@ cudaError_t launch_sample_tsqr(const KernelParams& kp, const double* bodies, con
   auto fn = tr == 32 ? k_sample_tsqr<T, 32> : tr == 16 ? k_sample_tsqr<T, 16> : k_sample_tsqr<T, 8>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  note_launch();
   fn<<<nboxes, TS_THREADS, smem, st>>>(kp, bodies, pts, xoff, dims, sidx, soff, Rws, qoff);
   return cudaGetLastError();
 }
@@ -481,6 +482,7 @@ cudaError_t launch_cpqr(const i64* dims, const i64* krows, T* Rws, const i64* qo
   auto fn = k_cpqr<T>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  note_launch();
   fn<<<nboxes, 256, smem, st>>>(dims, krows, Rws, qoff, perm, xoff, maxpiv, nonzero, step_cap);
   return cudaGetLastError();
 }
@@ -497,6 +499,7 @@ cudaError_t launch_basis_finish(const i64* dims, const i64* krows, T* Rws, T* Q,
   auto fn = k_basis_finish<T>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  note_launch();
   fn<<<nboxes, 256, smem, st>>>(dims, krows, Rws, Q, R, qoff, perm, xoff, maxpiv, nonzero, pts, ranks, epi, orth,
                                 qin_identity, wy_taus, xcap);
   return cudaGetLastError();
@@ -519,114 +522,6 @@ INST(float)
 
 namespace h2b {
 
-// Right-looking pivoted Cholesky of the Gram matrix G = XF^T XF (M x M,
-// symmetric, row = column major) of each box, stopped after ``steps``
-// pivots.  The pivot is the largest remaining Schur-complement diagonal
-// (the squared column norm that a column-pivoted QR of XF would pick), so
-// the pivots and the rows of R equal those of ColPivHouseholderQR in exact
-// arithmetic (h2matrix.cpp:84); R goes to Rws row-major in pivoted column
-// order, exactly where k_cpqr leaves it, for k_basis_finish.
-__global__ void __launch_bounds__(256) k_pivchol(const i64* __restrict__ dims, const i64* __restrict__ krows,
-                                                 double* __restrict__ G, double* __restrict__ Rws,
-                                                 const i64* __restrict__ qoff, int* __restrict__ perm_out,
-                                                 const i64* __restrict__ xoff, i64 step_cap) {
-  const int box = blockIdx.x;
-  const int M = (int)dims[box];
-  const int K = (int)krows[box];
-  if (M == 0 || K == 0) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  int* perm = reinterpret_cast<int*>(smem_raw);
-  __shared__ double red_v[32];
-  __shared__ int red_i[32];
-  double* g = G + qoff[box];
-  double* R = Rws + qoff[box];
-  const int tid = threadIdx.x, nt = blockDim.x;
-  int steps = K < M ? K : M;
-  if (step_cap >= 0 && step_cap < steps) steps = (int)step_cap;
-  for (int c = tid; c < M; c += nt) perm[c] = c;
-  // Smallest pivot kept: sqrt(eps) * ||XF|| (the resolution of an FP64 Gram
-  // matrix).  Columns below it are numerically dependent; flooring their
-  // pivot keeps R11^{-1} R12 finite and O(1) for them while the rows that
-  // carry the range of XF are unaffected.
-  double dmax = 0.;
-  int dmi = 0;
-  for (int j = tid; j < M; j += nt) {
-    double v = g[(i64)j * M + j];
-    if (v > dmax) { dmax = v; dmi = j; }
-  }
-  argmax_first(dmax, dmi, red_v, red_i);
-  double rfloor = sqrt(DBL_EPSILON * dmax);
-  if (!(rfloor > 0.)) rfloor = DBL_MIN;
-  // Schur diagonals at or below this are rounding noise of the FP64 Gram
-  // matrix (its resolution is ~sqrt(eps) in singular values).
-  const double noise = 16. * DBL_EPSILON * dmax;
-  bool noise_mode = false;
-  __syncthreads();
-  for (int k = 0; k < steps; k++) {
-    double bv = -1.;
-    int bi = 0x7fffffff;
-    for (int j = k + tid; j < M; j += nt) {
-      double v = g[(i64)j * M + j];
-      if (v > bv) { bv = v; bi = j; }
-    }
-    argmax_first(bv, bi, red_v, red_i);
-    if (bi < k || bi >= M) bi = k;  // every diagonal NaN: no swap
-    if (bi != k) {
-      for (int c = tid; c < M; c += nt) {  // swap rows k, bi
-        double t = g[(i64)k * M + c];
-        g[(i64)k * M + c] = g[(i64)bi * M + c];
-        g[(i64)bi * M + c] = t;
-      }
-      __syncthreads();
-      for (int r = tid; r < M; r += nt) {  // swap columns k, bi
-        double t = g[(i64)r * M + k];
-        g[(i64)r * M + k] = g[(i64)r * M + bi];
-        g[(i64)r * M + bi] = t;
-      }
-      for (int r = tid; r < k; r += nt) {  // earlier rows of R follow the column swap
-        double t = R[(i64)r * M + k];
-        R[(i64)r * M + k] = R[(i64)r * M + bi];
-        R[(i64)r * M + bi] = t;
-      }
-      if (tid == 0) {
-        int t = perm[k]; perm[k] = perm[bi]; perm[bi] = t;
-      }
-    }
-    __syncthreads();
-    const double d = g[(i64)k * M + k];
-    // Once the remaining columns are numerically dependent, the pivots that
-    // still have to be taken (fixed rank) get the row [floor, 0, ..., 0]:
-    // their interpolation coefficients come out exactly zero and the rows
-    // that carry the range of XF solve their own system unchanged.
-    if (!(d > noise)) noise_mode = true;
-    if (noise_mode) {
-      for (int j = k + tid; j < M; j += nt) R[(i64)k * M + j] = (j == k) ? rfloor : 0.;
-      __syncthreads();
-      continue;
-    }
-    const double rkk = sqrt(d);
-    const double inv = 1. / rkk;
-    for (int j = k + tid; j < M; j += nt) R[(i64)k * M + j] = (j == k) ? rkk : g[(i64)k * M + j] * inv;
-    __syncthreads();
-    const int rem = M - k - 1;
-    const i64 tot = (i64)rem * rem;
-    for (i64 e = tid; e < tot; e += nt) {
-      int i = k + 1 + (int)(e / rem), j = k + 1 + (int)(e % rem);
-      g[(i64)i * M + j] -= R[(i64)k * M + i] * R[(i64)k * M + j];
-    }
-    __syncthreads();
-  }
-  for (int c = tid; c < M; c += nt) perm_out[xoff[box] + c] = perm[c];
-}
-
-cudaError_t launch_pivchol(const i64* dims, const i64* krows, double* G, double* Rws, const i64* qoff, int* perm,
-                           const i64* xoff, i64 step_cap, int nboxes, int maxM, cudaStream_t st) {
-  if (nboxes == 0) return cudaSuccess;
-  size_t smem = sizeof(int) * (size_t)maxM + 16;
-  k_pivchol<<<nboxes, 256, smem, st>>>(dims, krows, G, Rws, qoff, perm, xoff, step_cap);
-  return cudaGetLastError();
-}
-
 // Gathers each box's far-sample bodies into one contiguous array.
 __global__ void k_gather_points(const double* __restrict__ bodies, const int* __restrict__ idx, i64 n,
                                 double* __restrict__ out) {
@@ -642,6 +537,7 @@ cudaError_t launch_gather_points(const double* bodies, const int* idx, i64 n, do
   if (n == 0) return cudaSuccess;
   int grid = (int)((n + 255) / 256);
   grid = grid > 4096 ? 4096 : grid;
+  note_launch();
   k_gather_points<<<grid, 256, 0, st>>>(bodies, idx, n, out);
   return cudaGetLastError();
 }
@@ -650,13 +546,21 @@ cudaError_t launch_gather_points(const double* bodies, const int* idx, i64 n, do
 
 namespace h2b {
 
-// One 32-pivot panel of the blocked pivoted Cholesky of G = XF^T XF.  G (M x M
-// per box, symmetric) already carries the trailing updates of earlier panels;
-// the pivots of this panel are taken left-looking: the Schur diagonal of the
-// remaining columns lives in shared memory and loses R[k][j]^2 after every
-// pivot, and row k of R is G[k][j] minus the panel's earlier rows.  The
-// caller applies G_trail -= R_panel^T R_panel (one batched GEMM) afterwards.
-// Pivot rule, noise rule and R layout are those of k_pivchol.
+// One 32-pivot panel of the blocked pivoted Cholesky of the Gram matrix
+// G = XF^T XF (M x M per box, symmetric), stopped after ``steps`` pivots in
+// all.  The pivot is the largest remaining Schur-complement diagonal (the
+// squared column norm a column-pivoted QR of XF would pick), so pivots and
+// rows of R equal those of ColPivHouseholderQR in exact arithmetic
+// (h2matrix.cpp:84); R goes to Rws row-major in pivoted column order, where
+// k_cpqr leaves it, for k_basis_finish.  Once the Schur diagonal falls to
+// rounding noise of the FP64 Gram matrix (16 eps max diag), the pivots
+// still to be taken get the row [floor, 0, ..., 0] with floor =
+// sqrt(eps max diag): their interpolation coefficients come out exactly zero.
+// G already carries the trailing updates of earlier panels; this panel's
+// pivots are taken left-looking: the Schur diagonal of the remaining
+// columns lives in shared memory and loses R[k][j]^2 after every pivot, and
+// row k of R is G[k][j] minus the panel's earlier rows.  The caller applies
+// G_trail -= R_panel^T R_panel (one batched GEMM) afterwards.
 __global__ void __launch_bounds__(256) k_pivchol_panel(const i64* __restrict__ dims, const i64* __restrict__ steps_box,
                                                        double* __restrict__ G, double* __restrict__ Rws,
                                                        const i64* __restrict__ qoff, int* __restrict__ perm_g,
@@ -760,6 +664,7 @@ cudaError_t launch_pivchol_panel(const i64* dims, const i64* steps_box, double* 
                                  cudaStream_t st) {
   if (nboxes == 0) return cudaSuccess;
   size_t smem = sizeof(double) * (size_t)maxM + 16;
+  note_launch();
   k_pivchol_panel<<<nboxes, 256, smem, st>>>(dims, steps_box, G, Rws, qoff, perm, xoff, state, k0, nb);
   return cudaGetLastError();
 }
@@ -796,6 +701,7 @@ __global__ void __launch_bounds__(256) k_wy_t(const WyTask<T>* __restrict__ task
 template <typename T>
 cudaError_t launch_wy_t(const WyTask<T>* d_tasks, int ntasks, int maxr, cudaStream_t st) {
   if (ntasks == 0) return cudaSuccess;
+  note_launch();
   k_wy_t<T><<<ntasks, 256, sizeof(T) * (size_t)(maxr + 2), st>>>(d_tasks);
   return cudaGetLastError();
 }
@@ -907,6 +813,7 @@ cudaError_t launch_qr_panel(const QrPanelTask<T>* d_tasks, int ntasks, int maxm,
   auto fn = k_qr_panel<T>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
+  note_launch();
   fn<<<ntasks, 256, smem, st>>>(d_tasks);
   return cudaGetLastError();
 }
@@ -939,6 +846,7 @@ __global__ void __launch_bounds__(256) k_qr_extract(const QrExtractTask<T>* __re
 template <typename T>
 cudaError_t launch_qr_extract(const QrExtractTask<T>* d_tasks, int ntasks, cudaStream_t st) {
   if (ntasks == 0) return cudaSuccess;
+  note_launch();
   k_qr_extract<T><<<ntasks, 256, 0, st>>>(d_tasks);
   return cudaGetLastError();
 }

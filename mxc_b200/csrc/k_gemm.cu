@@ -98,10 +98,13 @@ template <typename T>
 cudaError_t launch_seg_gemm(int shape, const GemmTask<T>* d_tasks, const GemmEntry<T>* d_ents, const TileRef* d_tiles,
                             int ntiles, cudaStream_t st) {
   if (ntiles == 0) return cudaSuccess;
-  if (shape == GEMM_BIG)
+  if (shape == GEMM_BIG) {
+    note_launch();
     k_seg_gemm<T, 64, 64, 16, 4, 4><<<ntiles, 256, 0, st>>>(d_tasks, d_ents, d_tiles);
-  else
+  } else {
+    note_launch();
     k_seg_gemm<T, 128, 16, 16, 4, 2><<<ntiles, 256, 0, st>>>(d_tasks, d_ents, d_tiles);
+  }
   return cudaGetLastError();
 }
 template cudaError_t launch_seg_gemm<double>(int, const GemmTask<double>*, const GemmEntry<double>*, const TileRef*,
@@ -122,6 +125,7 @@ __global__ void __launch_bounds__(256) k_batched_copy(const CopyEntry<T>* __rest
 template <typename T>
 cudaError_t launch_batched_copy(const CopyEntry<T>* d_ents, int n, cudaStream_t st) {
   if (n == 0) return cudaSuccess;
+  note_launch();
   k_batched_copy<T><<<n, 256, 0, st>>>(d_ents);
   return cudaGetLastError();
 }
@@ -139,6 +143,7 @@ __global__ void __launch_bounds__(256) k_set_identity(T* base, const i64* __rest
 template <typename T>
 cudaError_t launch_set_identity(T* base, const i64* qoff, const i64* dims, int nboxes, cudaStream_t st) {
   if (nboxes == 0) return cudaSuccess;
+  note_launch();
   k_set_identity<T><<<nboxes, 256, 0, st>>>(base, qoff, dims);
   return cudaGetLastError();
 }
@@ -153,9 +158,10 @@ namespace h2b {
 // beta C + sum_e alpha_e A_e B_e with A_e and B_e as stored (column-major).
 // This is the shape of every H^2 matvec pass and every ULV substitution
 // step except the transposed ones, and it is bound by streaming A from HBM
-// once.  One CTA (128 threads) covers 256 rows of a task.  The (entry,
-// k-slab) sequence of the task is one stream of stages: each stage is a
-// 256 x KS slab of A and the KS x NR slab of B, copied by cp.async into a
+// once.  One CTA (BM / 2 threads) covers BM = 128 or 256 rows of a task
+// (tasks of at most 128 rows take the narrow variant).  The (entry, k-slab)
+// sequence of the task is one stream of stages: each stage is a BM x KS
+// slab of A and the KS x NR slab of B, copied by cp.async into a
 // ST-deep shared-memory ring (16-byte copies where the column starts are
 // 16-byte aligned, element copies otherwise; rows past m and k past K are
 // zero-filled), so ST-1 slabs are in flight while one is multiplied.  Each
@@ -177,22 +183,20 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 template <typename T>
 struct StreamCfg;
 template <>
-struct StreamCfg<double> { static constexpr int KS = 16, ST = 3; };
+struct StreamCfg<double> { static constexpr int KS = 8, ST = 3; };
 template <>
-struct StreamCfg<float> { static constexpr int KS = 32, ST = 3; };
+struct StreamCfg<float> { static constexpr int KS = 16, ST = 3; };
 
-constexpr int STREAM_NT = 128, STREAM_BM = 256;
-
-template <typename T, int NR>
+template <typename T, int NR, int BM>
 constexpr size_t stream_smem() {
-  return sizeof(T) * (size_t)StreamCfg<T>::ST * StreamCfg<T>::KS * (STREAM_BM + NR);
+  return sizeof(T) * (size_t)StreamCfg<T>::ST * StreamCfg<T>::KS * (BM + NR);
 }
 
-template <typename T, int NR>
-__global__ void __launch_bounds__(STREAM_NT) k_stream_nn(const GemmTask<T>* __restrict__ tasks,
-                                                         const GemmEntry<T>* __restrict__ ents,
-                                                         const int2* __restrict__ tiles) {
-  constexpr int KS = StreamCfg<T>::KS, ST = StreamCfg<T>::ST, BM = STREAM_BM, NT = STREAM_NT;
+template <typename T, int NR, int BM>
+__global__ void __launch_bounds__(BM / 2, 1024 / BM) k_stream_nn(const GemmTask<T>* __restrict__ tasks,
+                                                      const GemmEntry<T>* __restrict__ ents,
+                                                      const int2* __restrict__ tiles) {
+  constexpr int KS = StreamCfg<T>::KS, ST = StreamCfg<T>::ST, NT = BM / 2;
   constexpr int V = 16 / sizeof(T);  // elements per 16-byte copy
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* As = reinterpret_cast<T*>(smem_raw);  // [ST][KS][BM]
@@ -269,7 +273,7 @@ __global__ void __launch_bounds__(STREAM_NT) k_stream_nn(const GemmTask<T>* __re
     issue((slot + ST - 1) % ST);
     const T* as = As + (size_t)slot * KS * BM + 2 * tid;
     const T* bs = Bs + (size_t)slot * KS * NR;
-#pragma unroll 4
+#pragma unroll
     for (int k = 0; k < KS; k++) {
       T a0, a1;
       if constexpr (sizeof(T) == 8) {
@@ -328,6 +332,7 @@ __global__ void __launch_bounds__(256) k_sum_parts(const SumTask<T>* __restrict_
 template <typename T>
 cudaError_t launch_sum_parts(const SumTask<T>* d_tasks, int ntasks, cudaStream_t st) {
   if (ntasks == 0) return cudaSuccess;
+  note_launch();
   k_sum_parts<T><<<ntasks, 256, 0, st>>>(d_tasks);
   return cudaGetLastError();
 }
@@ -338,29 +343,35 @@ template cudaError_t launch_sum_parts<float>(const SumTask<float>*, int, cudaStr
 
 namespace h2b {
 
-int skinny_rows_per_cta() { return 256; }
+int skinny_rows_per_cta(int wide) { return wide ? 256 : 128; }
 
 template <typename T>
-cudaError_t launch_skinny_nn(int nr, const GemmTask<T>* d_tasks, const GemmEntry<T>* d_ents, const int2* d_tiles,
-                             int ntiles, cudaStream_t st) {
+cudaError_t launch_skinny_nn(int nr, int wide, const GemmTask<T>* d_tasks, const GemmEntry<T>* d_ents,
+                             const int2* d_tiles, int ntiles, cudaStream_t st) {
   if (ntiles == 0) return cudaSuccess;
-  // Every variant covers 256 rows per CTA (two per thread).
-  auto go = [&](auto kern, size_t smem) {
+  auto go = [&](auto kern, size_t smem, int threads) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<ntiles, STREAM_NT, smem, st>>>(d_tasks, d_ents, d_tiles);
+    note_launch();
+    kern<<<ntiles, threads, smem, st>>>(d_tasks, d_ents, d_tiles);
     return cudaGetLastError();
   };
-  if (nr <= 1) return go(k_stream_nn<T, 1>, stream_smem<T, 1>());
-  if (nr <= 2) return go(k_stream_nn<T, 2>, stream_smem<T, 2>());
-  if (nr <= 4) return go(k_stream_nn<T, 4>, stream_smem<T, 4>());
-  if (nr <= 8) return go(k_stream_nn<T, 8>, stream_smem<T, 8>());
-  if (nr <= 16) return go(k_stream_nn<T, 16>, stream_smem<T, 16>());
+#define H2B_STREAM(NRV)                                                                  \
+  if (nr <= NRV) {                                                                      \
+    if (wide) return go(k_stream_nn<T, NRV, 256>, stream_smem<T, NRV, 256>(), 128);    \
+    return go(k_stream_nn<T, NRV, 128>, stream_smem<T, NRV, 128>(), 64);               \
+  }
+  H2B_STREAM(1)
+  H2B_STREAM(2)
+  H2B_STREAM(4)
+  H2B_STREAM(8)
+  H2B_STREAM(16)
+#undef H2B_STREAM
   return cudaErrorInvalidValue;
 }
-template cudaError_t launch_skinny_nn<double>(int, const GemmTask<double>*, const GemmEntry<double>*, const int2*, int,
-                                              cudaStream_t);
-template cudaError_t launch_skinny_nn<float>(int, const GemmTask<float>*, const GemmEntry<float>*, const int2*, int,
-                                             cudaStream_t);
+template cudaError_t launch_skinny_nn<double>(int, int, const GemmTask<double>*, const GemmEntry<double>*, const int2*,
+                                              int, cudaStream_t);
+template cudaError_t launch_skinny_nn<float>(int, int, const GemmTask<float>*, const GemmEntry<float>*, const int2*,
+                                             int, cudaStream_t);
 
 }  // namespace h2b

@@ -30,10 +30,13 @@ cudaError_t launch_gen_blocks(const KernelParams& kp, const GenTask* d_tasks, in
                               cudaStream_t st, int fast) {
   if (ntasks == 0) return cudaSuccess;
   dim3 grid(ntasks, chunks < 1 ? 1 : chunks);
-  if (fast)
+  if (fast) {
+    note_launch();
     k_gen_blocks<T, true><<<grid, 256, 0, st>>>(kp, d_tasks, out);
-  else
+  } else {
+    note_launch();
     k_gen_blocks<T, false><<<grid, 256, 0, st>>>(kp, d_tasks, out);
+  }
   return cudaGetLastError();
 }
 template cudaError_t launch_gen_blocks<double>(const KernelParams&, const GenTask*, int, int, double*, cudaStream_t,
@@ -89,14 +92,19 @@ cudaError_t launch_dense_matvec(const KernelParams& kp, const double* bodies, i6
     int nr = nrhs - c0 < 16 ? nrhs - c0 : 16;
     const double* x = X + (i64)c0 * ldx;
     double* y = Y + (i64)c0 * ldy;
-    if (nr == 1)
+    if (nr == 1) {
+      note_launch();
       k_dense_mv<1><<<grid, DM_THREADS, 0, st>>>(kp, bodies, n, x, ldx, y, ldy, nr);
-    else if (nr <= 4)
+    } else if (nr <= 4) {
+      note_launch();
       k_dense_mv<4><<<grid, DM_THREADS, 0, st>>>(kp, bodies, n, x, ldx, y, ldy, nr);
-    else if (nr <= 8)
+    } else if (nr <= 8) {
+      note_launch();
       k_dense_mv<8><<<grid, DM_THREADS, 0, st>>>(kp, bodies, n, x, ldx, y, ldy, nr);
-    else
+    } else {
+      note_launch();
       k_dense_mv<16><<<grid, DM_THREADS, 0, st>>>(kp, bodies, n, x, ldx, y, ldy, nr);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }

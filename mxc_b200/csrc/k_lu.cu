@@ -97,6 +97,7 @@ template <typename T>
 cudaError_t launch_lu_inverse(const LuTask<T>* d_tasks, int ntasks, cudaStream_t st) {
   if (ntasks == 0) return cudaSuccess;
   // Largest n is bounded by the caller (box dims <= 4096).
+  note_launch();
   k_lu_inverse<T><<<ntasks, 256, 4096 * sizeof(int), st>>>(d_tasks);
   return cudaGetLastError();
 }

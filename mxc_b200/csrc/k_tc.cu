@@ -391,6 +391,7 @@ cudaError_t launch_tc_gemm(const GemmTask<float>* d_tasks, const GemmEntry<float
   if (ntiles == 0) return cudaSuccess;
   cudaError_t e = cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
   if (e != cudaSuccess) return e;
+  note_launch();
   k_tc_gemm<<<ntiles, TC_NT, TC_SMEM, st>>>(d_tasks, d_ents, d_tiles);
   return cudaGetLastError();
 }

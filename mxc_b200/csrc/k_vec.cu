@@ -6,7 +6,14 @@
 #include "common.cuh"
 #include "kernels.h"
 
+#include <atomic>
+
 namespace h2b {
+
+static std::atomic<long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
 
 template <typename Ts, typename Td>
 __global__ void k_convert(const Ts* __restrict__ s, Td* __restrict__ d, i64 n) {
@@ -17,6 +24,7 @@ cudaError_t launch_convert(const Ts* src, Td* dst, i64 n, cudaStream_t st) {
   if (n == 0) return cudaSuccess;
   int grid = (int)((n + 255) / 256);
   grid = grid > 148 * 16 ? 148 * 16 : grid;
+  note_launch();
   k_convert<Ts, Td><<<grid, 256, 0, st>>>(src, dst, n);
   return cudaGetLastError();
 }
@@ -58,8 +66,10 @@ __global__ void k_dots_final(const double* __restrict__ partial, int nchunks, in
 cudaError_t launch_dots(const double* V, i64 vstride, int kvec, const double* w, i64 n, int nrhs, double* partial,
                         int nchunks, double* out, cudaStream_t st) {
   dim3 grid(nchunks, nrhs);
+  note_launch();
   k_dots_partial<<<grid, DOT_THREADS, 0, st>>>(V, vstride, kvec, w, n, nrhs, partial);
   int tot = kvec * nrhs;
+  note_launch();
   k_dots_final<<<(tot + 127) / 128, 128, 0, st>>>(partial, nchunks, kvec, nrhs, out);
   return cudaGetLastError();
 }
@@ -83,6 +93,7 @@ cudaError_t launch_gs_update(double* w, const double* V, i64 vstride, const doub
   int gx = (int)((n + 255) / 256);
   gx = gx > 1024 ? 1024 : gx;
   dim3 grid(gx, nrhs);
+  note_launch();
   k_gs_update<<<grid, 256, 0, st>>>(w, V, vstride, h, hstride, kvec, n, nrhs, sign, active);
   return cudaGetLastError();
 }
@@ -103,6 +114,7 @@ cudaError_t launch_scale_by_norm(const double* w, double* vout, const double* nr
   int gx = (int)((n + 255) / 256);
   gx = gx > 1024 ? 1024 : gx;
   dim3 grid(gx, nrhs);
+  note_launch();
   k_scale_by_norm<<<grid, 256, 0, st>>>(w, vout, nrm2, hout, hstride, n, nrhs);
   return cudaGetLastError();
 }
@@ -156,6 +168,7 @@ __global__ void k_gmres_ls(const double* __restrict__ Hall, int ld, int inner, c
 
 cudaError_t launch_gmres_ls(const double* H, int ld, int inner, const double* beta, double* y, int nrhs,
                             cudaStream_t st) {
+  note_launch();
   k_gmres_ls<<<(nrhs + 31) / 32, 32, 0, st>>>(H, ld, inner, beta, y, nrhs);
   return cudaGetLastError();
 }
@@ -168,6 +181,7 @@ __global__ void k_axpby(double* __restrict__ y, const double* __restrict__ x, do
 cudaError_t launch_axpby(double* y, const double* x, double a, double b, i64 n, cudaStream_t st) {
   int grid = (int)((n + 255) / 256);
   grid = grid > 148 * 16 ? 148 * 16 : grid;
+  note_launch();
   k_axpby<<<grid, 256, 0, st>>>(y, x, a, b, n);
   return cudaGetLastError();
 }
@@ -179,6 +193,7 @@ __global__ void k_resid_finish(const double* __restrict__ nrm2, const double* __
 }
 cudaError_t launch_residual_norm_finish(const double* nrm2, const double* normb, double* resid, int nrhs,
                                         cudaStream_t st) {
+  note_launch();
   k_resid_finish<<<(nrhs + 127) / 128, 128, 0, st>>>(nrm2, normb, resid, nrhs);
   return cudaGetLastError();
 }
@@ -204,10 +219,13 @@ __global__ void __launch_bounds__(256) k_fma_probe(T* out, int iters, T seed) {
 }
 
 cudaError_t launch_fma_probe(int precision, int blocks, int iters, void* out, cudaStream_t st) {
-  if (precision == 0)
+  if (precision == 0) {
+    note_launch();
     k_fma_probe<double><<<blocks, 256, 0, st>>>((double*)out, iters, 1.0);
-  else
+  } else {
+    note_launch();
     k_fma_probe<float><<<blocks, 256, 0, st>>>((float*)out, iters, 1.0f);
+  }
   return cudaGetLastError();
 }
 
@@ -256,7 +274,9 @@ cudaError_t launch_relerr(const double* X, const double* ref, i64 n, i64 ld, int
                           cudaStream_t st) {
   const int nch = relerr_chunks(n);
   dim3 grid(nch, nrhs);
+  note_launch();
   k_relerr_partial<<<grid, 256, 0, st>>>(X, ref, n, ld, partial);
+  note_launch();
   k_relerr_final<<<(nrhs + 127) / 128, 128, 0, st>>>(partial, nch, nrhs, out);
   return cudaGetLastError();
 }

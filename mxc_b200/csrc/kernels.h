@@ -65,8 +65,6 @@ cudaError_t launch_qr_extract(const QrExtractTask<T>* d_tasks, int ntasks, cudaS
 template <typename T>
 cudaError_t launch_wy_t(const WyTask<T>* d_tasks, int ntasks, int maxr, cudaStream_t st);
 
-cudaError_t launch_pivchol(const i64* dims, const i64* krows, double* G, double* Rws, const i64* qoff, int* perm,
-                           const i64* xoff, i64 step_cap, int nboxes, int maxM, cudaStream_t st);
 // Blocked pivoted Cholesky: one panel of nb pivots starting at k0 for every
 // box (steps_box[i] pivots in all); state holds 3 doubles per box.
 cudaError_t launch_pivchol_panel(const i64* dims, const i64* steps_box, double* G, double* Rws, const i64* qoff,
@@ -102,12 +100,13 @@ cudaError_t launch_seg_gemm(int shape, const GemmTask<T>* d_tasks, const GemmEnt
                             int ntiles, cudaStream_t st);
 int gemm_tile_m(int shape);
 // Plans whose entries all use A and B as stored and whose outputs have at
-// most 16 columns: rows of A streamed from HBM into registers, one CTA per
-// skinny_rows_per_cta() rows of a task (tile = {task, row block}).
+// most 16 columns: A streamed from HBM through a cp.async shared-memory
+// ring, one CTA per skinny_rows_per_cta(wide) rows of a task (tile = {task,
+// row block}); wide = 0 for tasks of at most 128 rows, 1 otherwise.
 template <typename T>
-cudaError_t launch_skinny_nn(int nr, const GemmTask<T>* d_tasks, const GemmEntry<T>* d_ents, const int2* d_tiles,
-                             int ntiles, cudaStream_t st);
-int skinny_rows_per_cta();
+cudaError_t launch_skinny_nn(int nr, int wide, const GemmTask<T>* d_tasks, const GemmEntry<T>* d_ents,
+                             const int2* d_tiles, int ntiles, cudaStream_t st);
+int skinny_rows_per_cta(int wide);
 // Reduction of a split task: dst (m x n, ld ldd) = beta dst + sum of `parts`
 // consecutive m x n partial results at src.
 template <typename T>

@@ -130,6 +130,13 @@ class Handle:
         return [(names.raw[48 * k:48 * k + 48].split(b"\0", 1)[0].decode(), float(t0[k]), float(dt[k]))
                 for k in range(n)]
 
+    @staticmethod
+    def launch_count() -> int:
+        """Kernels launched by the library in this process so far."""
+        v = C.c_int64()
+        L.check(L.lib().h2dev_launch_count(C.byref(v)), "h2dev_launch_count")
+        return v.value
+
     def fma_peak_tflops(self, precision: int = L.FP64) -> float:
         v = C.c_double()
         L.check(L.lib().h2dev_probe_fma_peak(self.h, precision, C.byref(v)), "h2dev_probe_fma_peak")
