@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--inner", type=int, default=10)
     ap.add_argument("--outer", type=int, default=50)
     ap.add_argument("--early-exit", type=int, default=1)
+    ap.add_argument("--tensor-cores", type=int, default=1, choices=[0, 1, 2],
+                    help="FP32 contractions: 1 tcgen05 3-term TF32 split (default), 2 one TF32 product, 0 SIMT")
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="one profiled step, no timing (for ncu)")
@@ -67,6 +69,8 @@ def workload(a) -> dict:
                            a.tol),
             "n": a.n, "nrhs": a.nrhs, "leaf": a.leaf, "theta": a.theta, "rank": a.rank, "samples": a.samples,
             "singularity": a.singularity, "precond_precision": "fp32" if a.precision == "mixed" else "fp64",
+            "fp32_contractions": {0: "simt fp32", 1: "tcgen05 3-term tf32 split", 2: "tcgen05 single tf32"}[
+                getattr(a, "tensor_cores", 1)],
             "gmres": "fp64, inner %d, outer <= %d, early exit %d" % (a.inner, a.outer, a.early_exit),
             "l2": "inputs (HBM working set of GBs) exceed the 126 MB L2 every step"}
 
@@ -176,6 +180,7 @@ def run_ours(a):
     ws, rank, local = dist_setup(a)
     torch.cuda.set_device(local)
     h = m.Handle(local)
+    h.set_option(m._lib.OPT_TENSOR_CORES, a.tensor_cores)
     k = m.Laplace3D(a.singularity)
     L = m.levels_for(a.n, a.leaf)
     b = m.uniform_unit_cube_rnd(a.n, 999)
@@ -298,7 +303,8 @@ def run_ours(a):
     # FP32 block contractions run on the tcgen05 tensor cores as three TF32
     # products (hi*hi + hi*lo + lo*hi): their ceiling in algorithmic FP32
     # flops is the dense TF32 rate (half the measured BF16 rate) / 3.
-    tc_kernels = ("gemm_factor", "gemm_coupling") if prec == m.FP32 else ()
+    tc_kernels = ("gemm_factor", "gemm_coupling") if prec == m.FP32 and a.tensor_cores else ()
+    tc_div = 3.0 if a.tensor_cores == 1 else 1.0
     simt32 = ("sample_tsqr", "cpqr", "lu_inverse", "basis_finish") if prec == m.FP32 else ()
 
     def roofline(name, nl, dms, fl, by):
@@ -307,8 +313,9 @@ def run_ours(a):
         # in the unit of that bound.
         t = dms * 1e-3
         if name in tc_kernels:
-            cbound, cpeak = "tensor", bf16 / 2.0 / 3.0
-            csrc = "MEASURED_PEAKS.json bf16_tflops / 2 (dense TF32) / 3 (three TF32 products per FP32 product)"
+            cbound, cpeak = "tensor", bf16 / 2.0 / tc_div
+            csrc = ("MEASURED_PEAKS.json bf16_tflops / 2 (dense TF32) / 3 (three TF32 products per FP32 product)"
+                    if tc_div == 3.0 else "MEASURED_PEAKS.json bf16_tflops / 2 (dense TF32)")
         elif name in simt32:
             cbound, cpeak = "fp32_simt", fp32_peak
             csrc = "measured FMA-throughput probe (h2dev_probe_fma_peak); no FP32 SIMT figure in MEASURED_PEAKS.json"

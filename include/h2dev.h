@@ -76,7 +76,8 @@ int h2dev_handle_synchronize(h2dev_handle_t h);
  * each level further out half of what remains, each group strided as in 0. */
 /* H2DEV_OPT_TENSOR_CORES: 1 (default) runs the FP32 block contractions of
  * plans built afterwards (in this process) on the tcgen05 tensor cores with
- * a 3-term TF32 split (FP32 accuracy); 0 runs them on the SIMT kernel. */
+ * a 3-term TF32 split (FP32 accuracy); 2 with one TF32 product (about 1e-3
+ * relative, for accuracy ablations); 0 runs them on the SIMT kernel. */
 enum { H2DEV_OPT_BASIS = 0, H2DEV_OPT_SKINNY_TILED = 1, H2DEV_OPT_SAMPLING = 2, H2DEV_OPT_TENSOR_CORES = 3 };
 int h2dev_set_option(h2dev_handle_t h, int option, int64_t value);
 

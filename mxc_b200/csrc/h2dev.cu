@@ -267,8 +267,9 @@ struct DVec {
 // H2DEV_OPT_SKINNY_TILED, used to compare the two kernels).
 static bool g_force_tiled = false;
 static bool force_tiled() { return g_force_tiled; }
-// Process-wide switch for the tcgen05 FP32 contractions (H2DEV_OPT_TENSOR_CORES).
-static bool g_tensor_cores = true;
+// Process-wide mode of the FP32 contractions (H2DEV_OPT_TENSOR_CORES):
+// 0 SIMT, 1 tcgen05 with the 3-term TF32 split, 2 tcgen05 single TF32.
+static int g_tensor_cores = 1;
 
 // Throws when a tensor-core GEMM launched since the last check reported an
 // expired wait (synchronises the stream).
@@ -288,6 +289,7 @@ struct GemmPlan {
   DVec<TileRef> d_tiles;
   int ntiles = 0;
   int shape = GEMM_BIG;
+  int tc_mode = 0;  // GEMM_TC: 1 three-term TF32 split, 2 single TF32
   const char* name = "seg_gemm";
   double flops = 0., bytes = 0.;  // algorithmic work of one run
   bool skinny_nn = false;          // use k_skinny_nn instead of the tiled kernel
@@ -314,21 +316,26 @@ struct GemmPlan {
     int maxn = 0;
     for (auto& t : tasks) maxn = std::max(maxn, t.n);
     shape = maxn <= 16 ? GEMM_SKINNY : GEMM_BIG;
-    if (std::is_same<T, float>::value && shape == GEMM_BIG && g_tensor_cores) shape = GEMM_TC;
+    if (std::is_same<T, float>::value && shape == GEMM_BIG && g_tensor_cores) {
+      shape = GEMM_TC;
+      tc_mode = g_tensor_cores;
+    }
     bool nn = true;
     for (const auto& e : ents) nn = nn && e.opA == 0 && e.opB == 0;
     skinny_nn = nn && maxn <= 16 && !force_tiled();
     nr = maxn;
     if (skinny_nn) split_tasks();
     if (skinny_nn) {
-      // Tasks of at most 128 rows go to the 128-row variant, the rest to
-      // the 256-row one (two launches back to back).
+      // A task takes 256-row tiles when they leave no more padding rows
+      // than 128-row tiles would, else 128-row tiles (two launches back to
+      // back; the padding rows are streamed as zeros but cost compute).
       std::vector<int2> rt[2];
       for (int ti = 0; ti < (int)tasks.size(); ti++) {
         const auto& t = tasks[ti];
         if (t.m <= 0 || t.n <= 0) continue;
         if (t.e0 == t.e1 && t.beta == T(1)) continue;
-        const int wide = t.m > skinny_rows_per_cta(0) ? 1 : 0;
+        const int n1 = skinny_rows_per_cta(0), n2 = skinny_rows_per_cta(1);
+        const int wide = ((t.m + n2 - 1) / n2) * n2 == ((t.m + n1 - 1) / n1) * n1 ? 1 : 0;
         const int rb = skinny_rows_per_cta(wide);
         for (int a = 0; a < (t.m + rb - 1) / rb; a++) rt[wide].push_back(make_int2(ti, a));
       }
@@ -440,7 +447,7 @@ struct GemmPlan {
       if (nsums) ck(launch_sum_parts<T>(d_sums.p, nsums, st), "sum_parts");
     } else if (shape == GEMM_TC) {
       if constexpr (std::is_same<T, float>::value)
-        ck(launch_tc_gemm(d_tasks.p, d_ents.p, d_tiles.p, ntiles, st), "tc_gemm");
+        ck(launch_tc_gemm(d_tasks.p, d_ents.p, d_tiles.p, ntiles, tc_mode == 1 ? 1 : 0, st), "tc_gemm");
     } else {
       ck(launch_seg_gemm<T>(shape, d_tasks.p, d_ents.p, d_tiles.p, ntiles, st), "seg_gemm");
     }
@@ -2398,8 +2405,8 @@ int h2dev_set_option(h2dev_handle_t h, int option, int64_t value) {
     return H2DEV_OK;
   }
   if (option == H2DEV_OPT_TENSOR_CORES) {
-    require(value == 0 || value == 1, "tensor-core option must be 0 or 1");
-    g_tensor_cores = value != 0;
+    require(value >= 0 && value <= 2, "tensor-core option must be 0, 1 or 2");
+    g_tensor_cores = (int)value;
     return H2DEV_OK;
   }
   if (option == H2DEV_OPT_SAMPLING) {

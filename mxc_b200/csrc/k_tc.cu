@@ -8,18 +8,22 @@
 // in tensor memory (the dropped A_lo B_lo term and the TF32 truncation of lo
 // are below 2^-21 relative).
 //
-// One CTA (128 threads) owns a 128 x 128 output tile; its accumulator is 128
-// TMEM lanes x 128 columns.  The task's (entry, 32-wide k slab) sequence is
-// double buffered in shared memory: all threads load slab s+1 from global
-// memory into registers while the tensor cores multiply slab s, then split
-// it into hi / lo and store it in the canonical no-swizzle K-major UMMA
-// layout (operands stored with rows contiguous are transposed 4 x 4 in
-// registers on the way; every global load is a 16-byte vector of
-// consecutive elements and every shared store is conflict-free).  One
-// thread issues the 12 MMAs of a slab (4 k-steps x 3 products) and commits
-// them to the slab's mbarrier; the buffer is refilled after that barrier
-// completes.  Every mbarrier wait is bounded (about a second of clock
-// cycles); on expiry the kernel records an error code and leaves.
+// One CTA (128 threads, two per SM) owns a 128 x 128 output tile; its
+// accumulator is 128 TMEM lanes x 128 columns.  The task's (entry, 16-wide
+// k slab) sequence flows through three stages:
+//  1. raw ring (3 slots): every thread issues cp.async copies of the slab's
+//     A and B tiles in their global orientation (16-byte chunks, XOR-swizzled
+//     so the reads of stage 2 are bank-conflict-free; rows past m / n and k
+//     past K are zero-filled), two slabs ahead of the one being converted;
+//  2. conversion: the slab is read back, scaled by alpha (A), split into hi
+//     and lo and stored in the canonical no-swizzle K-major UMMA layout (row-
+//     contiguous operands are transposed 4 x 4 in registers), into one of two
+//     operand buffers;
+//  3. one thread issues the slab's 6 MMAs (2 k-steps x 3 products) and
+//     commits them to the buffer's mbarrier; the buffer is converted into
+//     again once that barrier completes.
+// Every mbarrier wait is bounded (about two seconds of clock cycles); on
+// expiry the kernel records an error flag for the host and leaves.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -29,19 +33,27 @@ namespace h2b {
 
 namespace {
 
-constexpr int TC_BM = 128, TC_BN = 128, TC_KT = 32, TC_NT = 128;
-constexpr int TC_TILE = TC_BM * TC_KT * 4;  // bytes of one 128 x 32 FP32 operand tile
-constexpr int TC_STAGE = 4 * TC_TILE;       // A hi, A lo, B hi, B lo
-constexpr int TC_STAGES = 2;
-constexpr int TC_SMEM = TC_STAGES * TC_STAGE + 128;
+constexpr int TC_BM = 128, TC_BN = 128, TC_KT = 16, TC_NT = 128;
+constexpr int TC_KC = TC_KT / 4;            // 16-byte k-chunks per row
+constexpr int TC_TILE = TC_BM * TC_KT * 4;  // bytes of one 128 x 16 FP32 operand tile
+constexpr int TC_RAW = 2 * TC_TILE;         // raw slot: A, B
+constexpr int TC_HL = 4 * TC_TILE;          // operand buffer: A hi, A lo, B hi, B lo
+constexpr int TC_RS = 3, TC_HS = 2;
+constexpr int TC_SMEM = TC_RS * TC_RAW + TC_HS * TC_HL;
 constexpr long long TC_WAIT_CYCLES = 4000000000LL;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// Canonical no-swizzle K-major layout (byte offsets inside a 128 x 32
+// Canonical no-swizzle K-major layout (byte offsets inside a 128 x 16
 // tile): core matrix = 8 rows x 16 bytes (4 k); k-chunks 128 B apart
-// (leading byte offset), 8-row groups 1024 B apart (stride byte offset).
-__device__ __forceinline__ int off_kmajor(int r, int kc) { return (r >> 3) * 1024 + kc * 128 + (r & 7) * 16; }
+// (leading byte offset), 8-row groups 512 B apart (stride byte offset).
+constexpr int TC_SBO = TC_KC * 128;
+__device__ __forceinline__ int off_kmajor(int r, int kc) { return (r >> 3) * TC_SBO + kc * 128 + (r & 7) * 16; }
+// Raw layouts.  k contiguous: row r is 64 bytes (4 chunks of 4 k), chunk
+// kc stored at slot kc ^ ((r >> 1) & 3).  Rows contiguous: k-row k is 512
+// bytes (32 chunks of 4 rows), chunk q stored at slot q ^ (2 ((k >> 2) & 3)).
+__device__ __forceinline__ int raw_kc(int r, int kc) { return r * 64 + ((kc ^ ((r >> 1) & 3)) << 4); }
+__device__ __forceinline__ int raw_rc(int q, int k) { return k * 512 + ((q ^ (((k >> 2) & 3) << 1)) << 4); }
 
 __device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
   uint64_t d = 0;
@@ -94,6 +106,18 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   return true;
 }
 
+__device__ __forceinline__ void cp16(uint32_t dst, const void* src, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp4(uint32_t dst, const void* src, int bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 __device__ __forceinline__ float tf32_hi(float x) {
   uint32_t u;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(x));
@@ -101,7 +125,7 @@ __device__ __forceinline__ float tf32_hi(float x) {
 }
 
 // One operand of a slab: 128 rows (of op(X), rows of the output tile) by
-// 32 k.  kcontig: element (r, k) at X[k + r * ld]; otherwise at X[r + k * ld].
+// 16 k.  kcontig: element (r, k) at X[k + r * ld]; otherwise at X[r + k * ld].
 struct OperandRef {
   const float* X;
   i64 ld;
@@ -109,76 +133,56 @@ struct OperandRef {
   int r0;    // tile origin in rows
   int k0, K;
   int kcontig;
-  int vec;   // 16-byte vector loads are aligned
-  float scale;
+  int vec;  // 16-byte copies are aligned
 };
 
-// Thread-to-chunk maps of a 128 x 32 operand tile (1024 chunks of 16 bytes,
-// 8 per thread).  Both store into the K-major layout; each 8-lane phase of a
-// 16-byte shared store covers 8 distinct rows mod 8, so stores are
-// conflict-free.
-//  - k contiguous in global memory: chunk c = tid + 128 i holds row
-//    ((c >> 6) << 3) | (c & 7), k-chunk (c >> 3) & 7, one 16-byte load.
-//  - rows contiguous: lane = 8p + 2a + b loads, for warp task wt = warp + 4i
-//    (i < 2), rows 4q..4q+3 with q = 8 (wt & 3) + 2p + b at the four k of
-//    k-chunk kc = 4 (wt >> 2) + a (four 16-byte loads along the rows), and
-//    stores the transposed 4 x 4 block row by row, starting at row
-//    (t + a) & 3 in step t so the eight lanes of a phase hit eight rows.
-__device__ __forceinline__ float pick(const float4& v, int j) {
-  return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w));
-}
-
-__device__ __forceinline__ void load_operand(const OperandRef& o, float4 (&v)[8], int tid) {
-  if (o.kcontig) {
+// Issues this thread's copies (4 chunks of 16 bytes) of a raw operand tile.
+// k contiguous: chunk c = tid + 128 i is row c >> 2, k-chunk c & 3 (a warp
+// reads 8 rows x 64 contiguous bytes).  Rows contiguous: chunk c is row
+// quad c & 31 of k-row c >> 5 (a warp reads 512 contiguous bytes).
+__device__ __forceinline__ void issue_operand(const OperandRef& o, uint32_t raw, int tid) {
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-      const int c = tid + TC_NT * i;
-      const int r = ((c >> 6) << 3) | (c & 7), k = ((c >> 3) & 7) * 4;
-      const int gk = o.k0 + k;
-      float e[4] = {0.f, 0.f, 0.f, 0.f};
-      if (r < o.rows) {
-        const float* p = o.X + (i64)gk + (i64)(o.r0 + r) * o.ld;
-        if (o.vec && gk + 3 < o.K) {
-          const float4 t = __ldg(reinterpret_cast<const float4*>(p));
-          e[0] = t.x; e[1] = t.y; e[2] = t.z; e[3] = t.w;
-        } else {
+  for (int i = 0; i < TC_KC; i++) {
+    const int c = tid + TC_NT * i;
+    if (o.kcontig) {
+      const int r = c >> 2, kc = c & 3;
+      const int gk = o.k0 + kc * 4;
+      const uint32_t dst = raw + raw_kc(r, kc);
+      const bool rowok = r < o.rows;
+      int nk = o.K - gk;
+      nk = nk < 0 ? 0 : (nk > 4 ? 4 : nk);
+      if (!rowok) nk = 0;
+      const float* p = o.X + (i64)gk + (i64)(o.r0 + r) * o.ld;
+      if (o.vec) {
+        cp16(dst, nk ? (const void*)p : (const void*)o.X, nk * 4);
+      } else {
 #pragma unroll
-          for (int j = 0; j < 4; j++)
-            if (gk + j < o.K) e[j] = __ldg(p + j);
-        }
+        for (int j = 0; j < 4; j++) cp4(dst + 4 * j, j < nk ? (const void*)(p + j) : (const void*)o.X, j < nk ? 4 : 0);
       }
-      v[i] = make_float4(e[0] * o.scale, e[1] * o.scale, e[2] * o.scale, e[3] * o.scale);
-    }
-  } else {
-    const int lane = tid & 31, warp = tid >> 5;
-    const int p = lane >> 3, a = (lane >> 1) & 3, b = lane & 1;
+    } else {
+      const int q = c & 31, k = c >> 5;
+      const int gk = o.k0 + k, r = 4 * q;
+      const uint32_t dst = raw + raw_rc(q, k);
+      int nr = o.rows - r;
+      nr = nr < 0 ? 0 : (nr > 4 ? 4 : nr);
+      if (gk >= o.K) nr = 0;
+      const float* p = o.X + (i64)(o.r0 + r) + (i64)gk * o.ld;
+      if (o.vec) {
+        cp16(dst, nr ? (const void*)p : (const void*)o.X, nr * 4);
+      } else {
 #pragma unroll
-    for (int i = 0; i < 2; i++) {
-      const int wt = warp + 4 * i;
-      const int r = 4 * ((wt & 3) * 8 + 2 * p + b);
-      const int kc = (wt >> 2) * 4 + a;
-#pragma unroll
-      for (int t = 0; t < 4; t++) {
-        const int gk = o.k0 + 4 * kc + t;
-        float e[4] = {0.f, 0.f, 0.f, 0.f};
-        if (gk < o.K) {
-          const float* q = o.X + (i64)(o.r0 + r) + (i64)gk * o.ld;
-          if (o.vec && r + 3 < o.rows) {
-            const float4 x = __ldg(reinterpret_cast<const float4*>(q));
-            e[0] = x.x; e[1] = x.y; e[2] = x.z; e[3] = x.w;
-          } else {
-#pragma unroll
-            for (int j = 0; j < 4; j++)
-              if (r + j < o.rows) e[j] = __ldg(q + j);
-          }
-        }
-        v[4 * i + t] = make_float4(e[0] * o.scale, e[1] * o.scale, e[2] * o.scale, e[3] * o.scale);
+        for (int j = 0; j < 4; j++) cp4(dst + 4 * j, j < nr ? (const void*)(p + j) : (const void*)o.X, j < nr ? 4 : 0);
       }
     }
   }
 }
 
-__device__ __forceinline__ void store_split(unsigned char* hi, unsigned char* lo, int off, const float4& x) {
+__device__ __forceinline__ float pick(const float4& v, int j) {
+  return j == 0 ? v.x : (j == 1 ? v.y : (j == 2 ? v.z : v.w));
+}
+
+__device__ __forceinline__ void store_split(unsigned char* hi, unsigned char* lo, int off, float4 x, float scale) {
+  x.x *= scale; x.y *= scale; x.z *= scale; x.w *= scale;
   float4 h, l;
   h.x = tf32_hi(x.x); l.x = x.x - h.x;
   h.y = tf32_hi(x.y); l.y = x.y - h.y;
@@ -188,29 +192,37 @@ __device__ __forceinline__ void store_split(unsigned char* hi, unsigned char* lo
   *reinterpret_cast<float4*>(lo + off) = l;
 }
 
-// Splits the chunks into hi / lo and stores them K-major.
-__device__ __forceinline__ void store_operand(const float4 (&v)[8], int kcontig, unsigned char* hi,
-                                              unsigned char* lo, int tid) {
+// Converts a raw operand tile into hi / lo K-major tiles.  Each 8-lane
+// phase of the 16-byte shared loads and stores touches 8 distinct bank
+// groups.  k contiguous: chunk c = tid + 128 i is row 8 (c >> 5) + (c & 7),
+// k-chunk (c >> 3) & 3.  Rows contiguous: lane = 8p + 2a + b of warp w
+// reads rows 4q..4q+3 (q = 8w + 2p + b) at the four k of k-chunk a and
+// stores the transposed 4 x 4 block row by row, starting at row (t + a) & 3
+// in step t.
+__device__ __forceinline__ void convert_operand(const unsigned char* raw, int kcontig, float scale,
+                                                unsigned char* hi, unsigned char* lo, int tid) {
   if (kcontig) {
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
+    for (int i = 0; i < TC_KC; i++) {
       const int c = tid + TC_NT * i;
-      store_split(hi, lo, off_kmajor(((c >> 6) << 3) | (c & 7), (c >> 3) & 7), v[i]);
+      const int r = ((c >> 5) << 3) | (c & 7), kc = (c >> 3) & 3;
+      const float4 x = *reinterpret_cast<const float4*>(raw + raw_kc(r, kc));
+      store_split(hi, lo, off_kmajor(r, kc), x, scale);
     }
   } else {
     const int lane = tid & 31, warp = tid >> 5;
     const int p = lane >> 3, a = (lane >> 1) & 3, b = lane & 1;
+    {
+      const int q = warp * 8 + 2 * p + b;
+      const int kc = a;
+      float4 v[4];
 #pragma unroll
-    for (int i = 0; i < 2; i++) {
-      const int wt = warp + 4 * i;
-      const int r = 4 * ((wt & 3) * 8 + 2 * p + b);
-      const int kc = (wt >> 2) * 4 + a;
+      for (int t = 0; t < 4; t++) v[t] = *reinterpret_cast<const float4*>(raw + raw_rc(q, 4 * kc + t));
 #pragma unroll
       for (int t = 0; t < 4; t++) {
         const int j = (t + a) & 3;
-        const float4 x = make_float4(pick(v[4 * i], j), pick(v[4 * i + 1], j), pick(v[4 * i + 2], j),
-                                     pick(v[4 * i + 3], j));
-        store_split(hi, lo, off_kmajor(r + j, kc), x);
+        store_split(hi, lo, off_kmajor(4 * q + j, kc), make_float4(pick(v[0], j), pick(v[1], j), pick(v[2], j),
+                                                                  pick(v[3], j)), scale);
       }
     }
   }
@@ -224,16 +236,25 @@ __device__ __forceinline__ void skip_empty(const GemmEntry<float>* ents, int e1,
   while (c.e < e1 && ents[c.e].k <= 0) c.e++;
 }
 
+__device__ __forceinline__ void advance(const GemmEntry<float>* ents, int e1, SlabCursor& c) {
+  c.k0 += TC_KT;
+  if (c.k0 >= ents[c.e].k) {
+    c.k0 = 0;
+    c.e++;
+    skip_empty(ents, e1, c);
+  }
+}
+
 }  // namespace
 
 // Set when an mbarrier wait expired (read and cleared by the host).
 __device__ int g_tc_err = 0;
 
-__global__ void __launch_bounds__(TC_NT, 1)
+__global__ void __launch_bounds__(TC_NT, 2)
     k_tc_gemm(const GemmTask<float>* __restrict__ tasks, const GemmEntry<float>* __restrict__ ents,
-              const TileRef* __restrict__ tiles) {
+              const TileRef* __restrict__ tiles, int split) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bars[TC_STAGES];
+  __shared__ __align__(8) uint64_t bars[TC_HS];
   __shared__ uint32_t tmem_slot;
   __shared__ int wait_ok;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -242,9 +263,11 @@ __global__ void __launch_bounds__(TC_NT, 1)
   const int m0 = tl.tm * TC_BM, n0 = tl.tn * TC_BN;
   const int mrows = min(TC_BM, task.m - m0), ncols = min(TC_BN, task.n - n0);
   const int nmma = ((ncols + 15) / 16) * 16;  // MMA N: multiple of 16, >= 16
+  unsigned char* raw_base = smem;
+  unsigned char* hl_base = smem + TC_RS * TC_RAW;
 
   if (tid == 0) {
-    for (int s = 0; s < TC_STAGES; s++)
+    for (int s = 0; s < TC_HS; s++)
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bars[s])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -259,84 +282,87 @@ __global__ void __launch_bounds__(TC_NT, 1)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
 
-  SlabCursor cur{task.e0, 0};
-  skip_empty(ents, task.e1, cur);
-  const bool any = cur.e < task.e1;
+  SlabCursor prod{task.e0, 0}, cons{task.e0, 0};
+  skip_empty(ents, task.e1, prod);
+  skip_empty(ents, task.e1, cons);
+  const bool any = cons.e < task.e1;
   bool ok = true;
   int s = 0;
   if (any) {
-    float4 va[8], vb[8];
-    int a_kc = 0, b_kc = 0;
-    auto fetch = [&](const SlabCursor& c) {
-      const GemmEntry<float> en = ents[c.e];
-      OperandRef a, b;
-      a.X = en.A; a.ld = en.lda; a.rows = mrows; a.r0 = m0; a.k0 = c.k0; a.K = en.k;
-      a.kcontig = en.opA;  // op(A)(m, k) = A[k + m lda] when transposed
-      a.vec = ((reinterpret_cast<uintptr_t>(en.A) & 15) == 0) && (en.lda % 4 == 0);
-      a.scale = en.alpha;
-      b.X = en.B; b.ld = en.ldb; b.rows = ncols; b.r0 = n0; b.k0 = c.k0; b.K = en.k;
-      b.kcontig = en.opB ? 0 : 1;  // op(B)(k, n) = B[k + n ldb] when not transposed
-      b.vec = ((reinterpret_cast<uintptr_t>(en.B) & 15) == 0) && (en.ldb % 4 == 0);
-      b.scale = 1.f;
-      load_operand(a, va, tid);
-      load_operand(b, vb, tid);
-      a_kc = a.kcontig;
-      b_kc = b.kcontig;
+    // Copies of the slab at the producer cursor into raw slot `slot`; one
+    // commit group per call (empty once the cursor is past the end).
+    auto produce = [&](int slot) {
+      if (prod.e < task.e1) {
+        const GemmEntry<float> en = ents[prod.e];
+        const uint32_t raw = smem_addr(raw_base + slot * TC_RAW);
+        OperandRef a, b;
+        a.X = en.A; a.ld = en.lda; a.rows = mrows; a.r0 = m0; a.k0 = prod.k0; a.K = en.k;
+        a.kcontig = en.opA;  // op(A)(m, k) = A[k + m lda] when transposed
+        a.vec = ((reinterpret_cast<uintptr_t>(en.A) & 15) == 0) && (en.lda % 4 == 0);
+        b.X = en.B; b.ld = en.ldb; b.rows = ncols; b.r0 = n0; b.k0 = prod.k0; b.K = en.k;
+        b.kcontig = en.opB ? 0 : 1;  // op(B)(k, n) = B[k + n ldb] when not transposed
+        b.vec = ((reinterpret_cast<uintptr_t>(en.B) & 15) == 0) && (en.ldb % 4 == 0);
+        issue_operand(a, raw, tid);
+        issue_operand(b, raw + TC_TILE, tid);
+        advance(ents, task.e1, prod);
+      }
+      cp_commit();
     };
-    fetch(cur);
-    uint32_t phase[TC_STAGES] = {0u, 0u};
-    for (;;) {
-      const int buf = s & 1;
-      unsigned char* st = smem + buf * TC_STAGE;
-      if (s >= TC_STAGES) {
-        // The MMAs that read this buffer two slabs ago must have finished
-        // (one thread waits; the verdict is shared so all leave together).
-        if (tid == 0) wait_ok = mbar_wait(smem_addr(&bars[buf]), phase[buf]) ? 1 : 0;
-        __syncthreads();
+#pragma unroll
+    for (int j = 0; j < TC_RS - 1; j++) produce(j);
+    uint32_t phase[TC_HS] = {0u, 0u};
+    while (cons.e < task.e1) {
+      const int hb = s & 1;
+      cp_wait<TC_RS - 2>();  // this thread's copies of slab s have landed
+      if (s >= TC_HS && tid == 0) wait_ok = mbar_wait(smem_addr(&bars[hb]), phase[hb]) ? 1 : 0;
+      __syncthreads();  // slab s visible to all; slot (s - 1) % RS free
+      if (s >= TC_HS) {
         if (!wait_ok) {
           ok = false;
           break;
         }
-        phase[buf] ^= 1u;
+        phase[hb] ^= 1u;
       }
-      store_operand(va, a_kc, st, st + TC_TILE, tid);
-      store_operand(vb, b_kc, st + 2 * TC_TILE, st + 3 * TC_TILE, tid);
+      produce((s + TC_RS - 1) % TC_RS);
+      const GemmEntry<float> en = ents[cons.e];
+      const unsigned char* raw = raw_base + (s % TC_RS) * TC_RAW;
+      unsigned char* hl = hl_base + hb * TC_HL;
+      const int a_kc = en.opA, b_kc = en.opB ? 0 : 1;
+      convert_operand(raw, a_kc, en.alpha, hl, hl + TC_TILE, tid);
+      convert_operand(raw + TC_TILE, b_kc, 1.f, hl + 2 * TC_TILE, hl + 3 * TC_TILE, tid);
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncthreads();
       if (tid == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t idesc = make_idesc(nmma);
-        const uint32_t base = smem_addr(st);
+        const uint32_t base = smem_addr(hl);
 #pragma unroll
         for (int ks = 0; ks < TC_KT / 8; ks++) {
           uint64_t ad[2], bd[2];
 #pragma unroll
           for (int h = 0; h < 2; h++) {
-            ad[h] = make_desc(base + h * TC_TILE + ks * 256, 128, 1024);
-            bd[h] = make_desc(base + (2 + h) * TC_TILE + ks * 256, 128, 1024);
+            ad[h] = make_desc(base + h * TC_TILE + ks * 256, 128, TC_SBO);
+            bd[h] = make_desc(base + (2 + h) * TC_TILE + ks * 256, 128, TC_SBO);
           }
           const uint32_t first = (s == 0 && ks == 0) ? 0u : 1u;
-          mma_tf32(tmem, ad[1], bd[0], idesc, first);  // lo x hi
-          mma_tf32(tmem, ad[0], bd[1], idesc, 1u);     // hi x lo
-          mma_tf32(tmem, ad[0], bd[0], idesc, 1u);     // hi x hi
+          if (split) {
+            mma_tf32(tmem, ad[1], bd[0], idesc, first);  // lo x hi
+            mma_tf32(tmem, ad[0], bd[1], idesc, 1u);     // hi x lo
+            mma_tf32(tmem, ad[0], bd[0], idesc, 1u);     // hi x hi
+          } else {
+            mma_tf32(tmem, ad[0], bd[0], idesc, first);  // one TF32 product
+          }
         }
-        mma_commit(smem_addr(&bars[buf]));
+        mma_commit(smem_addr(&bars[hb]));
       }
-      // Next slab.
-      cur.k0 += TC_KT;
-      if (cur.k0 >= ents[cur.e].k) {
-        cur.k0 = 0;
-        cur.e++;
-        skip_empty(ents, task.e1, cur);
-      }
+      advance(ents, task.e1, cons);
       s++;
-      if (cur.e >= task.e1) break;
-      fetch(cur);
     }
+    cp_wait<0>();
     if (ok) {
       // Wait for the last slab's MMAs (all earlier ones complete before it).
-      const int buf = (s - 1) & 1;
-      if (tid == 0) wait_ok = mbar_wait(smem_addr(&bars[buf]), phase[buf]) ? 1 : 0;
+      const int hb = (s - 1) & 1;
+      if (tid == 0) wait_ok = mbar_wait(smem_addr(&bars[hb]), phase[hb]) ? 1 : 0;
       __syncthreads();
       ok = wait_ok != 0;
     }
@@ -387,12 +413,12 @@ __global__ void __launch_bounds__(TC_NT, 1)
 int tc_gemm_tile() { return TC_BM; }
 
 cudaError_t launch_tc_gemm(const GemmTask<float>* d_tasks, const GemmEntry<float>* d_ents, const TileRef* d_tiles,
-                           int ntiles, cudaStream_t st) {
+                           int ntiles, int split, cudaStream_t st) {
   if (ntiles == 0) return cudaSuccess;
   cudaError_t e = cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
   if (e != cudaSuccess) return e;
   note_launch();
-  k_tc_gemm<<<ntiles, TC_NT, TC_SMEM, st>>>(d_tasks, d_ents, d_tiles);
+  k_tc_gemm<<<ntiles, TC_NT, TC_SMEM, st>>>(d_tasks, d_ents, d_tiles, split);
   return cudaGetLastError();
 }
 

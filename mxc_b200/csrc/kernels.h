@@ -120,10 +120,11 @@ struct SumTask {
 template <typename T>
 cudaError_t launch_sum_parts(const SumTask<T>* d_tasks, int ntasks, cudaStream_t st);
 int gemm_tile_n(int shape);
-// FP32 segmented GEMM on the tcgen05 tensor cores (3-term TF32 split),
-// 128 x 128 output tiles (TileRef over tc_gemm_tile()-sized tiles).
+// FP32 segmented GEMM on the tcgen05 tensor cores, 128 x 128 output tiles
+// (TileRef over tc_gemm_tile()-sized tiles); split = 1: 3-term TF32 split
+// (FP32 accuracy), 0: one TF32 product.
 cudaError_t launch_tc_gemm(const GemmTask<float>* d_tasks, const GemmEntry<float>* d_ents, const TileRef* d_tiles,
-                           int ntiles, cudaStream_t st);
+                           int ntiles, int split, cudaStream_t st);
 int tc_gemm_tile();
 cudaError_t tc_gemm_take_error(int* flag, cudaStream_t st);
 
