@@ -319,6 +319,10 @@ def run_ours(a):
         elif name in simt32:
             cbound, cpeak = "fp32_simt", fp32_peak
             csrc = "measured FMA-throughput probe (h2dev_probe_fma_peak); no FP32 SIMT figure in MEASURED_PEAKS.json"
+        elif name == "gram":
+            cbound, cpeak = "fp64_tensor", fp64_peak
+            csrc = ("FP64 mma.sync; denominator = measured FP64 FMA-throughput probe (h2dev_probe_fma_peak), "
+                    "no FP64 figure in MEASURED_PEAKS.json")
         else:
             cbound, cpeak = "fp64_simt", fp64_peak
             csrc = "measured FMA-throughput probe (h2dev_probe_fma_peak); no FP64 figure in MEASURED_PEAKS.json"

@@ -921,14 +921,20 @@ class Solver : public SolverBase {
       i0 = i1;
     }
     XF.alloc(maxchunk);
+    const int gt_w = gram_tile();
     for (auto& ch : chunks) {
       std::vector<GenTask> gt;
-      GemmPlan<double> gp;
-      gp.name = "gemm_gram";
+      std::vector<GramTask> gm;
+      std::vector<int4> tiles;
+      double gfl = 0.;
       i64 o = 0;
       for (i64 i = ch.first; i < ch.second; i++) {
         const i64 S = soff[i + 1] - soff[i], M = lv.dims[i];
-        if (S == 0 || M == 0) continue;
+        if (M == 0) continue;
+        if (S == 0) {
+          ck(cudaMemsetAsync(G.p + lv.qoff[i], 0, sizeof(double) * M * M, st()), "gram zero");
+          continue;
+        }
         GenTask t;
         t.bi = spts.p + 3 * soff[i];
         t.bj = lv.pts.p + 3 * lv.xoff[i];
@@ -937,8 +943,18 @@ class Solver : public SolverBase {
         t.out_off = o;
         t.ld = S;
         gt.push_back(t);
-        gp.add_task(G.p + lv.qoff[i], M, (int)M, (int)M, 0.);
-        gp.add_entry(XF.p + o, S, 1, XF.p + o, S, 0, (int)S, 1.);
+        GramTask g;
+        g.X = XF.p + o;
+        g.ld = S;
+        g.S = (int)S;
+        g.M = (int)M;
+        g.G = G.p + lv.qoff[i];
+        g.ldg = M;
+        const int tn = (int)((M + gt_w - 1) / gt_w);
+        for (int a = 0; a < tn; a++)
+          for (int b = a; b < tn; b++) tiles.push_back(make_int4((int)gm.size(), a, b, 0));
+        gm.push_back(g);
+        gfl += (double)S * M * (M + 1);  // symmetric rank-S product
         o += S * M;
       }
       if (gt.empty()) continue;
@@ -948,8 +964,14 @@ class Solver : public SolverBase {
         Prof pf("gen_samples", 0., 8. * o);
         ck(launch_gen_blocks<double>(kp, dg.p, (int)gt.size(), 4, XF.p, st(), 1), "gen samples");
       }
-      gp.finalize();
-      gp.run(st());
+      DVec<GramTask> dgm;
+      DVec<int4> dtl;
+      dgm.upload(gm);
+      dtl.upload(tiles);
+      {
+        Prof pf("gram", gfl, 8. * o);
+        ck(launch_gram(dgm.p, dtl.p, (int)tiles.size(), st()), "gram");
+      }
     }
     Rws.alloc(lv.qoff[nodes]);
     Rws.zero(st());

@@ -71,6 +71,17 @@ cudaError_t launch_pivchol_panel(const i64* dims, const i64* steps_box, double* 
                                  int* perm, const i64* xoff, double* state, int k0, int nb, int nboxes, int maxM,
                                  cudaStream_t st);
 cudaError_t launch_gather_points(const double* bodies, const int* idx, i64 n, double* out, cudaStream_t st);
+// Gram matrix G = X^T X of one box (k_gram): X is S x M column-major.
+struct GramTask {
+  const double* X;
+  i64 ld;
+  int S, M;
+  double* G;
+  i64 ldg;
+};
+// tiles: {task, tile row, tile col} with tile row <= tile col, gram_tile() wide.
+cudaError_t launch_gram(const GramTask* d_tasks, const int4* d_tiles, int ntiles, cudaStream_t st);
+int gram_tile();
 
 // ---------------------------------------------------------------- gemm
 // C_task = beta * C_task + sum_{e in task} alpha_e * op(A_e) * op(B_e)
