@@ -314,6 +314,140 @@ __global__ void __launch_bounds__(BM / 2, 1024 / BM) k_stream_nn(const GemmTask<
   }
 }
 
+// FP64 variant of the streaming apply on the FP64 tensor cores (mma.sync
+// m8n8k4 .f64) for 8 or 16 right-hand sides.  Same ring and cursors as
+// k_stream_nn; each warp owns 32 rows x NR columns as 4 x (NR / 8) m8n8k4
+// accumulators.  A slabs are stored [k][BM + 4] and B slabs [k][NR + 4]
+// (doubles): the padding makes the fragment loads of a half-warp (4 k x 4
+// rows or columns) hit 16 distinct bank pairs.  One MMA replaces 8 DFMA
+// instructions per thread, so the apply is no longer issue-bound.
+constexpr int SD_KS = 8, SD_ST = 3;
+
+template <int NR, int BM>
+constexpr size_t stream_dmma_smem() {
+  return sizeof(double) * (size_t)SD_ST * SD_KS * ((BM + 4) + (NR + 4));
+}
+
+template <int NR, int BM>
+__global__ void __launch_bounds__(BM, BM == 256 ? 3 : 6)
+    k_stream_dmma(const GemmTask<double>* __restrict__ tasks, const GemmEntry<double>* __restrict__ ents,
+                  const int2* __restrict__ tiles) {
+  constexpr int NT = BM, AS = BM + 4, BS = NR + 4, NF = NR / 8;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* As = reinterpret_cast<double*>(smem_raw);  // [ST][KS][AS]
+  double* Bs = As + (size_t)SD_ST * SD_KS * AS;       // [ST][KS][BS]
+  const int2 tl = tiles[blockIdx.x];
+  const GemmTask<double> task = tasks[tl.x];
+  const int m0 = tl.y * BM;
+  const int mrows = min(BM, task.m - m0);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+  int pe = task.e0, pk = 0;
+  while (pe < task.e1 && ents[pe].k <= 0) pe++;
+  auto issue = [&](int slot) {
+    if (pe < task.e1) {
+      const GemmEntry<double> en = ents[pe];
+      double* as = As + (size_t)slot * SD_KS * AS;
+      double* bs = Bs + (size_t)slot * SD_KS * BS;
+      const bool vec = ((reinterpret_cast<uintptr_t>(en.A) & 15) == 0) && (en.lda % 2 == 0);
+      if (vec) {
+        for (int c = tid; c < SD_KS * (BM / 2); c += NT) {
+          const int k = c / (BM / 2), r = (c % (BM / 2)) * 2;
+          int valid = mrows - r;
+          valid = valid < 0 ? 0 : (valid > 2 ? 2 : valid);
+          if (pk + k >= en.k) valid = 0;
+          const double* src = valid ? en.A + (i64)(m0 + r) + (i64)(pk + k) * en.lda : en.A;
+          cp_async_16(as + k * AS + r, src, valid * 8);
+        }
+      } else {
+        for (int c = tid; c < SD_KS * BM; c += NT) {
+          const int k = c / BM, r = c % BM;
+          const bool ok = r < mrows && pk + k < en.k;
+          const double* src = ok ? en.A + (i64)(m0 + r) + (i64)(pk + k) * en.lda : en.A;
+          cp_async_ca<8>(as + k * AS + r, src, ok ? 8 : 0);
+        }
+      }
+      for (int c = tid; c < SD_KS * NR; c += NT) {
+        const int k = c / NR, j = c % NR;
+        const bool ok = j < task.n && pk + k < en.k;
+        const double* src = ok ? en.B + (i64)(pk + k) + (i64)j * en.ldb : en.B;
+        cp_async_ca<8>(bs + k * BS + j, src, ok ? 8 : 0);
+      }
+      pk += SD_KS;
+      if (pk >= en.k) {
+        pk = 0;
+        pe++;
+        while (pe < task.e1 && ents[pe].k <= 0) pe++;
+      }
+    }
+    cp_async_commit();
+  };
+
+  double acc[4][NF][2];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < NF; j++) acc[i][j][0] = acc[i][j][1] = 0.;
+
+#pragma unroll
+  for (int s = 0; s < SD_ST - 1; s++) issue(s);
+  int ce = task.e0, ck = 0;
+  while (ce < task.e1 && ents[ce].k <= 0) ce++;
+  int slot = 0;
+  const int fr = lane >> 2, fk = lane & 3;
+  while (ce < task.e1) {
+    const double alpha = ents[ce].alpha;
+    cp_async_wait<SD_ST - 2>();
+    if (alpha != 1.) {
+      double* bs = Bs + (size_t)slot * SD_KS * BS;
+      for (int c = tid; c < SD_KS * NR; c += NT) bs[(c / NR) * BS + c % NR] *= alpha;
+    }
+    __syncthreads();
+    issue((slot + SD_ST - 1) % SD_ST);
+    const double* as = As + (size_t)slot * SD_KS * AS + fk * AS + warp * 32 + fr;
+    const double* bs = Bs + (size_t)slot * SD_KS * BS + fk * BS + fr;
+#pragma unroll
+    for (int ks = 0; ks < SD_KS; ks += 4) {
+      double a[4], b[NF];
+#pragma unroll
+      for (int i = 0; i < 4; i++) a[i] = as[ks * AS + i * 8];
+#pragma unroll
+      for (int j = 0; j < NF; j++) b[j] = bs[ks * BS + j * 8];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < NF; j++)
+          asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                       : "+d"(acc[i][j][0]), "+d"(acc[i][j][1])
+                       : "d"(a[i]), "d"(b[j]));
+    }
+    ck += SD_KS;
+    if (ck >= ents[ce].k) {
+      ck = 0;
+      ce++;
+      while (ce < task.e1 && ents[ce].k <= 0) ce++;
+    }
+    slot = (slot + 1) % SD_ST;
+  }
+  cp_async_wait<0>();
+  // D fragment: lane holds row lane >> 2, columns 2 (lane & 3) + {0, 1}.
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int r = warp * 32 + i * 8 + fr;
+    if (r >= mrows) continue;
+#pragma unroll
+    for (int j = 0; j < NF; j++)
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int c = j * 8 + 2 * fk + h;
+        if (c < task.n) {
+          double* p = task.C + (m0 + r) + (i64)c * task.ldc;
+          *p = (task.beta == 0.) ? acc[i][j][h] : task.beta * (*p) + acc[i][j][h];
+        }
+      }
+  }
+}
+
 // dst = beta * dst + sum_{p < parts} src_p, the parts of one split task
 // summed in a fixed order (deterministic).
 template <typename T>
@@ -356,6 +490,17 @@ cudaError_t launch_skinny_nn(int nr, int wide, const GemmTask<T>* d_tasks, const
     kern<<<ntiles, threads, smem, st>>>(d_tasks, d_ents, d_tiles);
     return cudaGetLastError();
   };
+  if constexpr (sizeof(T) == 8) {
+    // FP64 with 5..16 right-hand sides: tensor-core variant, BM threads.
+    if (nr > 4 && nr <= 8) {
+      if (wide) return go(k_stream_dmma<8, 256>, stream_dmma_smem<8, 256>(), 256);
+      return go(k_stream_dmma<8, 128>, stream_dmma_smem<8, 128>(), 128);
+    }
+    if (nr > 8 && nr <= 16) {
+      if (wide) return go(k_stream_dmma<16, 256>, stream_dmma_smem<16, 256>(), 256);
+      return go(k_stream_dmma<16, 128>, stream_dmma_smem<16, 128>(), 128);
+    }
+  }
 #define H2B_STREAM(NRV)                                                                  \
   if (nr <= NRV) {                                                                      \
     if (wide) return go(k_stream_nn<T, NRV, 256>, stream_smem<T, NRV, 256>(), 128);    \
