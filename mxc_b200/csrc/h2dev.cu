@@ -1420,7 +1420,9 @@ class Solver : public SolverBase {
       for (const auto& t : lt) fl += 8. / 3. * (double)t.n * t.n * t.n;
       {
         Prof pf("lu_inverse", fl, 0.);
-        ck(launch_lu_inverse<T>(dl.p, (int)lt.size(), st()), "lu_inverse");
+        int maxn = 0;
+        for (const auto& x : lt) maxn = std::max(maxn, x.n);
+        ck(launch_lu_inverse<T>(dl.p, (int)lt.size(), maxn, st()), "lu_inverse");
       }
     }
     // Step 5: V^T[:, Ms:] = U_r (A_rr^{-1})^T.

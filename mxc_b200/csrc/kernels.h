@@ -155,7 +155,7 @@ cudaError_t launch_set_identity(T* base, const i64* qoff, const i64* dims, int n
 // ---------------------------------------------------------------- lu
 template <typename T>
 struct LuTask {
-  T* A;      // n x n column-major, factored in place
+  T* A;      // n x n column-major (read only)
   i64 lda;
   int n;
   T* invT;   // receives A^{-1} transposed (column-major, ld = ldinv)
@@ -164,7 +164,7 @@ struct LuTask {
   int* info;  // 1 when |det| <= DBL_MIN (h2matrix.cpp:441)
 };
 template <typename T>
-cudaError_t launch_lu_inverse(const LuTask<T>* d_tasks, int ntasks, cudaStream_t st);
+cudaError_t launch_lu_inverse(const LuTask<T>* d_tasks, int ntasks, int maxn, cudaStream_t st);
 
 // ---------------------------------------------------------------- vectors
 template <typename Ts, typename Td>
