@@ -115,6 +115,161 @@ __global__ void __launch_bounds__(256) k_gj_inverse(const LuTask<T>* __restrict_
   }
 }
 
+// Register-resident Gauss-Jordan for n <= NP (NP = 128 with 256 threads,
+// FP32 NP = 256 with 1024 threads; the block is padded with the identity):
+// warp w owns columns w + W j (j < CPW = NP / W), lane l owns rows l + 32 i
+// (i < RPL = NP / 32), so each thread holds 64 values and a step costs two
+// barriers (pivot column to shared memory, pivot index back) instead of a
+// block-wide sweep through memory.  Row swaps and the pivot row travel by
+// warp shuffles; pivot order, ipiv, the determinant rule and the column
+// unscrambling are those of k_gj_inverse.
+template <typename T, int NP>
+__global__ void __launch_bounds__(NP * NP / 64) k_gj_reg(const LuTask<T>* __restrict__ tasks) {
+  constexpr int NT = NP * NP / 64, W = NT / 32, CPW = NP / W, RPL = NP / 32;
+  const LuTask<T> t = tasks[blockIdx.x];
+  const int n = t.n;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  __shared__ T colk[2][NP];
+  __shared__ int s_piv[NP];
+  __shared__ int s_pos[NP];
+  __shared__ int s_p;
+  __shared__ double s_det;
+  __shared__ int s_swaps;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* stage = reinterpret_cast<T*>(smem_raw);  // 32 x (NP + 1) output staging
+  if (n <= 0) {
+    if (tid == 0) *t.info = 0;
+    return;
+  }
+  T x[CPW][RPL];
+#pragma unroll
+  for (int j = 0; j < CPW; j++) {
+    const int c = warp + W * j;
+#pragma unroll
+    for (int i = 0; i < RPL; i++) {
+      const int r = lane + 32 * i;
+      x[j][i] = (r < n && c < n) ? t.A[r + (i64)c * t.lda] : (r == c ? T(1) : T(0));
+    }
+  }
+  if (tid == 0) {
+    s_det = 1.;
+    s_swaps = 0;
+  }
+  for (int k = 0; k < n; k++) {
+    const int wk = k % W, jk = k / W, lk = k & 31, ik = k >> 5;
+    T* ck = colk[k & 1];
+    // 1. The owner warp publishes column k.
+    if (warp == wk) {
+#pragma unroll
+      for (int j = 0; j < CPW; j++)
+        if (j == jk)
+#pragma unroll
+          for (int i = 0; i < RPL; i++) ck[lane + 32 * i] = x[j][i];
+    }
+    __syncthreads();
+    // 2. Warp 0 finds the pivot: first row of largest magnitude, rows k..n-1.
+    if (warp == 0) {
+      double bv = -1.;
+      int bi = 0x7fffffff;
+      for (int r = k + lane; r < n; r += 32) {
+        const double v = fabs((double)ck[r]);
+        if (v > bv) { bv = v; bi = r; }
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+      }
+      if (bi < k || bi >= n) bi = k;  // a column of NaNs: no swap
+      if (lane == 0) {
+        s_p = bi;
+        s_piv[k] = bi;
+        s_det *= (double)ck[bi];
+        s_swaps += bi != k;
+      }
+    }
+    __syncthreads();
+    const int p = s_p, lp = p & 31, ip = p >> 5;
+    const T piv = ck[p];
+    const T inv = piv != T(0) ? T(1) / piv : T(0);
+    // 3. Swap rows k and p of every owned column, then scale row k and
+    //    broadcast it within the warp.
+    T rowk[CPW];
+#pragma unroll
+    for (int j = 0; j < CPW; j++) {
+      T vk = x[j][0], vp = x[j][0];
+#pragma unroll
+      for (int i = 1; i < RPL; i++) {
+        if (i == ik) vk = x[j][i];
+        if (i == ip) vp = x[j][i];
+      }
+      const T a_k = __shfl_sync(0xffffffffu, vk, lk);  // old row k
+      const T a_p = __shfl_sync(0xffffffffu, vp, lp);  // old row p (new row k)
+      const int c = warp + W * j;
+      if (p != k) {
+#pragma unroll
+        for (int i = 0; i < RPL; i++) {
+          if (i == ip && lane == lp) x[j][i] = a_k;
+        }
+      }
+      const T nk = (c == k ? T(1) : a_p) * inv;  // new row k, scaled
+#pragma unroll
+      for (int i = 0; i < RPL; i++)
+        if (i == ik && lane == lk) x[j][i] = nk;
+      rowk[j] = nk;
+    }
+    // 4. Eliminate column k from every other row (multipliers from the
+    //    published column, with rows k and p exchanged).
+#pragma unroll
+    for (int i = 0; i < RPL; i++) {
+      const int r = lane + 32 * i;
+      if (r == k) continue;
+      const T m = r == p ? ck[k] : ck[r];
+#pragma unroll
+      for (int j = 0; j < CPW; j++) {
+        const int c = warp + W * j;
+        x[j][i] = (c == k ? T(0) : x[j][i]) - m * rowk[j];
+      }
+    }
+  }
+  __syncthreads();
+  // Unscramble: position q of the inverse holds elimination column idx[q]
+  // after the swaps (k, piv[k]) for k = n-1..0; s_pos[c] = position of c.
+  if (tid == 0) {
+    int* idx = s_pos;  // reused below as the inverse map
+    for (int c = 0; c < NP; c++) idx[c] = c;
+    for (int k = n - 1; k >= 0; k--) {
+      const int q = s_piv[k];
+      const int tmp = idx[k]; idx[k] = idx[q]; idx[q] = tmp;
+    }
+    // Invert idx in place through colk (free now) as scratch.
+    int* inv_map = reinterpret_cast<int*>(colk);
+    for (int q = 0; q < NP; q++) inv_map[idx[q]] = q;
+    for (int c = 0; c < NP; c++) s_pos[c] = inv_map[c];
+    const double det = (s_swaps & 1) ? -s_det : s_det;
+    *t.info = fabs(det) <= DBL_MIN ? 1 : 0;
+  }
+  __syncthreads();
+  for (int k = tid; k < n; k += NT) t.ipiv[k] = s_piv[k];
+  // invT[r * ldinv + q] = A^{-1}[r][q], 32 rows at a time through shared
+  // memory so the global stores run along q.
+#pragma unroll
+  for (int i = 0; i < RPL; i++) {
+    if (32 * i >= n) break;
+#pragma unroll
+    for (int j = 0; j < CPW; j++) {
+      const int c = warp + W * j;
+      if (c < n) stage[lane * (NP + 1) + s_pos[c]] = x[j][i];
+    }
+    __syncthreads();
+    for (int e = tid; e < 32 * NP; e += NT) {
+      const int rr = e / NP, q = e % NP, r = 32 * i + rr;
+      if (r < n && q < n) t.invT[(i64)r * t.ldinv + q] = stage[rr * (NP + 1) + q];
+    }
+    __syncthreads();
+  }
+}
+
 template <typename T>
 size_t gj_smem(int n) {
   return sizeof(T) * ((size_t)n * (n + 1) + n) + sizeof(int) * (size_t)n + 16;
@@ -123,6 +278,18 @@ size_t gj_smem(int n) {
 template <typename T>
 cudaError_t launch_lu_inverse(const LuTask<T>* d_tasks, int ntasks, int maxn, cudaStream_t st) {
   if (ntasks == 0) return cudaSuccess;
+  if (maxn <= (sizeof(T) == 4 ? 256 : 128)) {
+    auto go = [&](auto kern, int np) {
+      const size_t smem = sizeof(T) * 32 * (size_t)(np + 1);
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      note_launch();
+      kern<<<ntasks, np * np / 64, smem, st>>>(d_tasks);
+      return cudaGetLastError();
+    };
+    if (maxn <= 128) return go(k_gj_reg<T, 128>, 128);
+    if constexpr (sizeof(T) == 4) return go(k_gj_reg<float, 256>, 256);
+  }
   if (gj_smem<T>(maxn) <= 200 * 1024) {
     const size_t smem = gj_smem<T>(maxn);
     cudaError_t e = cudaFuncSetAttribute(k_gj_inverse<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
