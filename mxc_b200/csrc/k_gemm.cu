@@ -448,6 +448,175 @@ __global__ void __launch_bounds__(BM, BM == 256 ? 3 : 6)
   }
 }
 
+// FP32 variant of the streaming apply on the tensor cores through warp-level
+// mma.sync m16n8k8 TF32 with the 3-term split (hi*hi + hi*lo + lo*hi, FP32
+// accumulation: FP32 accuracy) for 8 or 16 right-hand sides.  Same ring and
+// cursors as k_stream_nn; each warp owns 32 rows x NR columns as 2 x (NR / 8)
+// m16n8 accumulators.  A slabs are stored [k][BM + 8] and B slabs [k][NR + 8]
+// (floats) so each fragment load of a warp (8 rows x 4 k) hits 32 distinct
+// banks.  The split happens in registers as fragments are loaded.
+constexpr int SF_KS = 16, SF_ST = 3;
+
+template <int NR, int BM>
+constexpr size_t stream_tf32_smem() {
+  return sizeof(float) * (size_t)SF_ST * SF_KS * ((BM + 8) + (NR + 8));
+}
+
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+  uint32_t h;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+  h &= 0xFFFFE000u;
+  hi = h;
+  lo = __float_as_uint(x - __uint_as_float(h));
+}
+
+__device__ __forceinline__ void mma_tf32_16x8x8(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+template <int NR, int BM>
+__global__ void __launch_bounds__(BM, BM == 256 ? 3 : 6)
+    k_stream_tf32(const GemmTask<float>* __restrict__ tasks, const GemmEntry<float>* __restrict__ ents,
+                  const int2* __restrict__ tiles) {
+  constexpr int NT = BM, AS = BM + 8, BS = NR + 8, NF = NR / 8;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* As = reinterpret_cast<float*>(smem_raw);  // [ST][KS][AS]
+  float* Bs = As + (size_t)SF_ST * SF_KS * AS;      // [ST][KS][BS]
+  const int2 tl = tiles[blockIdx.x];
+  const GemmTask<float> task = tasks[tl.x];
+  const int m0 = tl.y * BM;
+  const int mrows = min(BM, task.m - m0);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+  int pe = task.e0, pk = 0;
+  while (pe < task.e1 && ents[pe].k <= 0) pe++;
+  auto issue = [&](int slot) {
+    if (pe < task.e1) {
+      const GemmEntry<float> en = ents[pe];
+      float* as = As + (size_t)slot * SF_KS * AS;
+      float* bs = Bs + (size_t)slot * SF_KS * BS;
+      const bool vec = ((reinterpret_cast<uintptr_t>(en.A) & 15) == 0) && (en.lda % 4 == 0);
+      if (vec) {
+        for (int c = tid; c < SF_KS * (BM / 4); c += NT) {
+          const int k = c / (BM / 4), r = (c % (BM / 4)) * 4;
+          int valid = mrows - r;
+          valid = valid < 0 ? 0 : (valid > 4 ? 4 : valid);
+          if (pk + k >= en.k) valid = 0;
+          const float* src = valid ? en.A + (i64)(m0 + r) + (i64)(pk + k) * en.lda : en.A;
+          cp_async_16(as + k * AS + r, src, valid * 4);
+        }
+      } else {
+        for (int c = tid; c < SF_KS * BM; c += NT) {
+          const int k = c / BM, r = c % BM;
+          const bool ok = r < mrows && pk + k < en.k;
+          const float* src = ok ? en.A + (i64)(m0 + r) + (i64)(pk + k) * en.lda : en.A;
+          cp_async_ca<4>(as + k * AS + r, src, ok ? 4 : 0);
+        }
+      }
+      for (int c = tid; c < SF_KS * NR; c += NT) {
+        const int k = c / NR, j = c % NR;
+        const bool ok = j < task.n && pk + k < en.k;
+        const float* src = ok ? en.B + (i64)(pk + k) + (i64)j * en.ldb : en.B;
+        cp_async_ca<4>(bs + k * BS + j, src, ok ? 4 : 0);
+      }
+      pk += SF_KS;
+      if (pk >= en.k) {
+        pk = 0;
+        pe++;
+        while (pe < task.e1 && ents[pe].k <= 0) pe++;
+      }
+    }
+    cp_async_commit();
+  };
+
+  float acc[2][NF][4];
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < NF; j++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[i][j][q] = 0.f;
+
+#pragma unroll
+  for (int s = 0; s < SF_ST - 1; s++) issue(s);
+  int ce = task.e0, ck = 0;
+  while (ce < task.e1 && ents[ce].k <= 0) ce++;
+  int slot = 0;
+  const int g = lane >> 2, t4 = lane & 3;
+  while (ce < task.e1) {
+    const float alpha = ents[ce].alpha;
+    cp_async_wait<SF_ST - 2>();
+    if (alpha != 1.f) {
+      float* bs = Bs + (size_t)slot * SF_KS * BS;
+      for (int c = tid; c < SF_KS * NR; c += NT) bs[(c / NR) * BS + c % NR] *= alpha;
+    }
+    __syncthreads();
+    issue((slot + SF_ST - 1) % SF_ST);
+    const float* as = As + (size_t)slot * SF_KS * AS + warp * 32 + g;
+    const float* bs = Bs + (size_t)slot * SF_KS * BS + g;
+#pragma unroll
+    for (int ks = 0; ks < SF_KS; ks += 8) {
+      // A fragment of m16n8k8 (row): a0 (g, t), a1 (g + 8, t), a2 (g, t + 4), a3 (g + 8, t + 4).
+      uint32_t ah[2][4], al[2][4];
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const float* ap = as + i * 16 + (ks + t4) * AS;
+        split_tf32(ap[0], ah[i][0], al[i][0]);
+        split_tf32(ap[8], ah[i][1], al[i][1]);
+        split_tf32(ap[4 * AS], ah[i][2], al[i][2]);
+        split_tf32(ap[4 * AS + 8], ah[i][3], al[i][3]);
+      }
+      // B fragment (col): b0 (k = t, n = g), b1 (k = t + 4, n = g).
+      uint32_t bh[NF][2], bl[NF][2];
+#pragma unroll
+      for (int j = 0; j < NF; j++) {
+        const float* bp = bs + j * 8 + (ks + t4) * BS;
+        split_tf32(bp[0], bh[j][0], bl[j][0]);
+        split_tf32(bp[4 * BS], bh[j][1], bl[j][1]);
+      }
+#pragma unroll
+      for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < NF; j++) {
+          mma_tf32_16x8x8(acc[i][j], al[i], bh[j]);
+          mma_tf32_16x8x8(acc[i][j], ah[i], bl[j]);
+          mma_tf32_16x8x8(acc[i][j], ah[i], bh[j]);
+        }
+    }
+    ck += SF_KS;
+    if (ck >= ents[ce].k) {
+      ck = 0;
+      ce++;
+      while (ce < task.e1 && ents[ce].k <= 0) ce++;
+    }
+    slot = (slot + 1) % SF_ST;
+  }
+  cp_async_wait<0>();
+  // C fragment: c0 (g, 2t), c1 (g, 2t + 1), c2 (g + 8, 2t), c3 (g + 8, 2t + 1).
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int hh = 0; hh < 2; hh++) {
+      const int r = warp * 32 + i * 16 + g + 8 * hh;
+      if (r >= mrows) continue;
+#pragma unroll
+      for (int j = 0; j < NF; j++)
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+          const int c = j * 8 + 2 * t4 + q;
+          if (c < task.n) {
+            float* p = task.C + (m0 + r) + (i64)c * task.ldc;
+            const float v = acc[i][j][2 * hh + q];
+            *p = (task.beta == 0.f) ? v : task.beta * (*p) + v;
+          }
+        }
+    }
+}
+
 // dst = beta * dst + sum_{p < parts} src_p, the parts of one split task
 // summed in a fixed order (deterministic).
 template <typename T>
@@ -490,6 +659,17 @@ cudaError_t launch_skinny_nn(int nr, int wide, const GemmTask<T>* d_tasks, const
     kern<<<ntiles, threads, smem, st>>>(d_tasks, d_ents, d_tiles);
     return cudaGetLastError();
   };
+  if constexpr (sizeof(T) == 4) {
+    // FP32 with 5..16 right-hand sides: TF32 tensor-core variant (3-term split), BM threads.
+    if (nr > 4 && nr <= 8) {
+      if (wide) return go(k_stream_tf32<8, 256>, stream_tf32_smem<8, 256>(), 256);
+      return go(k_stream_tf32<8, 128>, stream_tf32_smem<8, 128>(), 128);
+    }
+    if (nr > 8 && nr <= 16) {
+      if (wide) return go(k_stream_tf32<16, 256>, stream_tf32_smem<16, 256>(), 256);
+      return go(k_stream_tf32<16, 128>, stream_tf32_smem<16, 128>(), 128);
+    }
+  }
   if constexpr (sizeof(T) == 8) {
     // FP64 with 5..16 right-hand sides: tensor-core variant, BM threads.
     if (nr > 4 && nr <= 8) {
