@@ -60,6 +60,12 @@ int64_t h2_levels_for(int64_t nbodies, int64_t leaf);
 int h2dev_handle_create(int device, h2dev_handle_t* out);
 int h2dev_handle_destroy(h2dev_handle_t h);
 int h2dev_handle_synchronize(h2dev_handle_t h);
+/* Device memory of the handle: bytes held by its live solvers, plans and
+ * temporaries, and bytes freed into its cache for reuse (no reference
+ * counterpart; used for HBM-budget admission by a serving loop). */
+int h2dev_handle_memory(h2dev_handle_t h, int64_t* live_bytes, int64_t* cached_bytes);
+/* Returns the handle's cached (free) device blocks to the driver. */
+int h2dev_handle_trim(h2dev_handle_t h);
 /* Handle options (apply to solvers created afterwards on this handle).
  * H2DEV_OPT_BASIS: 0 (default) forms fixed-rank orthogonal bases from the
  * Gram matrix of the far samples with a pivoted Cholesky (same pivots and R

@@ -178,6 +178,7 @@ static void* cache_alloc(h2dev_handle_s* h, size_t cls) {
     void* p = it->second.back();
     it->second.pop_back();
     h->cached_bytes -= cls;
+    h->live_bytes += cls;
     return p;
   }
   void* p = nullptr;
@@ -188,12 +189,14 @@ static void* cache_alloc(h2dev_handle_s* h, size_t cls) {
     e = cudaMalloc(&p, cls);
   }
   ck(e, "cudaMalloc");
+  h->live_bytes += cls;
   return p;
 }
 
 static void cache_free(h2dev_handle_s* h, void* p, size_t cls) {
   h->cache[cls].push_back(p);
   h->cached_bytes += cls;
+  h->live_bytes -= cls;
 }
 
 // Device array.  Inside an API call (a current handle) memory comes from the
@@ -2025,6 +2028,24 @@ static void handle_release(h2dev_handle_s* h) {
 int h2dev_handle_destroy(h2dev_handle_t h) {
   H2_API_BEGIN
   handle_release(h);
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_handle_memory(h2dev_handle_t h, int64_t* live_bytes, int64_t* cached_bytes) {
+  H2_API_BEGIN
+  require(h != nullptr, "null handle");
+  if (live_bytes) *live_bytes = (int64_t)h->live_bytes;
+  if (cached_bytes) *cached_bytes = (int64_t)h->cached_bytes;
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_handle_trim(h2dev_handle_t h) {
+  H2_API_BEGIN
+  require(h != nullptr, "null handle");
+  ck(cudaSetDevice(h->device), "cudaSetDevice");
+  cache_trim(h);
   return H2DEV_OK;
   H2_API_END
 }

@@ -47,6 +47,7 @@ struct h2dev_handle_s {
   // state factorizations then make no driver allocation calls.
   std::unordered_map<size_t, std::vector<void*>> cache;
   size_t cached_bytes = 0;
+  size_t live_bytes = 0;  // blocks handed out (solvers, plans, temporaries)
   std::vector<ProfRec> recs;
   std::vector<cudaEvent_t> pool;
   cudaEvent_t t0 = nullptr, t1 = nullptr;

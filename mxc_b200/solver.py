@@ -130,6 +130,16 @@ class Handle:
         return [(names.raw[48 * k:48 * k + 48].split(b"\0", 1)[0].decode(), float(t0[k]), float(dt[k]))
                 for k in range(n)]
 
+    def memory(self) -> tuple:
+        """(live bytes, cached free bytes) of this handle's device memory."""
+        live, cached = C.c_int64(), C.c_int64()
+        L.check(L.lib().h2dev_handle_memory(self.h, C.byref(live), C.byref(cached)), "h2dev_handle_memory")
+        return live.value, cached.value
+
+    def trim(self) -> None:
+        """Return the handle's cached device blocks to the driver."""
+        L.check(L.lib().h2dev_handle_trim(self.h), "h2dev_handle_trim")
+
     @staticmethod
     def launch_count() -> int:
         """Kernels launched by the library in this process so far."""
