@@ -8,7 +8,7 @@
 // in tensor memory (the dropped A_lo B_lo term and the TF32 truncation of lo
 // are below 2^-21 relative).
 //
-// One CTA (128 threads, two per SM) owns a 128 x 128 output tile; its
+// One CTA (256 threads, two per SM) owns a 128 x 128 output tile; its
 // accumulator is 128 TMEM lanes x 128 columns.  The task's (entry, 16-wide
 // k slab) sequence flows through three stages:
 //  1. raw ring (3 slots): every thread issues cp.async copies of the slab's
@@ -33,7 +33,8 @@ namespace h2b {
 
 namespace {
 
-constexpr int TC_BM = 128, TC_BN = 128, TC_KT = 16, TC_NT = 128;
+constexpr int TC_BM = 128, TC_BN = 128, TC_KT = 16, TC_NT = 256;
+constexpr int TC_CPT = TC_BM * TC_KT / 4 / TC_NT;  // 16-byte chunks per thread per operand
 constexpr int TC_KC = TC_KT / 4;            // 16-byte k-chunks per row
 constexpr int TC_TILE = TC_BM * TC_KT * 4;  // bytes of one 128 x 16 FP32 operand tile
 constexpr int TC_RAW = 2 * TC_TILE;         // raw slot: A, B
@@ -136,13 +137,13 @@ struct OperandRef {
   int vec;  // 16-byte copies are aligned
 };
 
-// Issues this thread's copies (4 chunks of 16 bytes) of a raw operand tile.
-// k contiguous: chunk c = tid + 128 i is row c >> 2, k-chunk c & 3 (a warp
+// Issues this thread's copies (2 chunks of 16 bytes) of a raw operand tile.
+// k contiguous: chunk c = tid + 256 i is row c >> 2, k-chunk c & 3 (a warp
 // reads 8 rows x 64 contiguous bytes).  Rows contiguous: chunk c is row
 // quad c & 31 of k-row c >> 5 (a warp reads 512 contiguous bytes).
 __device__ __forceinline__ void issue_operand(const OperandRef& o, uint32_t raw, int tid) {
 #pragma unroll
-  for (int i = 0; i < TC_KC; i++) {
+  for (int i = 0; i < TC_CPT; i++) {
     const int c = tid + TC_NT * i;
     if (o.kcontig) {
       const int r = c >> 2, kc = c & 3;
@@ -194,16 +195,16 @@ __device__ __forceinline__ void store_split(unsigned char* hi, unsigned char* lo
 
 // Converts a raw operand tile into hi / lo K-major tiles.  Each 8-lane
 // phase of the 16-byte shared loads and stores touches 8 distinct bank
-// groups.  k contiguous: chunk c = tid + 128 i is row 8 (c >> 5) + (c & 7),
+// groups.  k contiguous: chunk c = tid + 256 i is row 8 (c >> 5) + (c & 7),
 // k-chunk (c >> 3) & 3.  Rows contiguous: lane = 8p + 2a + b of warp w
-// reads rows 4q..4q+3 (q = 8w + 2p + b) at the four k of k-chunk a and
-// stores the transposed 4 x 4 block row by row, starting at row (t + a) & 3
-// in step t.
+// reads rows 4q..4q+3 (q = 8 (w & 3) + 2p + b) at the four k of k-chunk a
+// and stores two rows of the transposed 4 x 4 block (steps t = 2 (w >> 2)
+// and t + 1, row (t + a) & 3 in step t; warps w and w + 4 share a block).
 __device__ __forceinline__ void convert_operand(const unsigned char* raw, int kcontig, float scale,
                                                 unsigned char* hi, unsigned char* lo, int tid) {
   if (kcontig) {
 #pragma unroll
-    for (int i = 0; i < TC_KC; i++) {
+    for (int i = 0; i < TC_CPT; i++) {
       const int c = tid + TC_NT * i;
       const int r = ((c >> 5) << 3) | (c & 7), kc = (c >> 3) & 3;
       const float4 x = *reinterpret_cast<const float4*>(raw + raw_kc(r, kc));
@@ -213,13 +214,15 @@ __device__ __forceinline__ void convert_operand(const unsigned char* raw, int kc
     const int lane = tid & 31, warp = tid >> 5;
     const int p = lane >> 3, a = (lane >> 1) & 3, b = lane & 1;
     {
-      const int q = warp * 8 + 2 * p + b;
+      const int q = (warp & 3) * 8 + 2 * p + b;
       const int kc = a;
       float4 v[4];
 #pragma unroll
       for (int t = 0; t < 4; t++) v[t] = *reinterpret_cast<const float4*>(raw + raw_rc(q, 4 * kc + t));
+      const int t0 = 2 * (warp >> 2);
 #pragma unroll
-      for (int t = 0; t < 4; t++) {
+      for (int tt = 0; tt < 2; tt++) {
+        const int t = t0 + tt;
         const int j = (t + a) & 3;
         store_split(hi, lo, off_kmajor(4 * q + j, kc), make_float4(pick(v[0], j), pick(v[1], j), pick(v[2], j),
                                                                   pick(v[3], j)), scale);
@@ -370,15 +373,17 @@ __global__ void __launch_bounds__(TC_NT, 2)
   }
   if (!ok && tid == 0) atomicExch(&g_tc_err, 1);
 
-  // Epilogue: warp w reads TMEM lanes 32w..32w+31 (tile rows), 32 columns
-  // per load; C = beta C + acc, coalesced along the rows of a column.
-  const int row = warp * 32 + lane;
-  for (int c0 = 0; c0 < TC_BN; c0 += 32) {
+  // Epilogue: warp w reads TMEM lanes 32 (w & 3) .. +31 (tile rows; a warp
+  // may only read its lane quarter), warps 0-3 columns 0-63 and warps 4-7
+  // columns 64-127, 32 per load; C = beta C + acc, coalesced along the rows
+  // of a column.
+  const int row = (warp & 3) * 32 + lane;
+  for (int c0 = (warp >> 2) * (TC_BN / 2); c0 < (warp >> 2 ? TC_BN : TC_BN / 2); c0 += 32) {
     if (c0 >= ncols) break;
     float acc[32];
     if (any && ok) {
       uint32_t r[32];
-      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+      const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)c0;
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
           "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
