@@ -84,11 +84,13 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
-__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+// mbarrier.try_wait suspends the thread in hardware until the phase
+// completes or a system-dependent time limit passes.
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}\n"
       : "=r"(ok)
       : "r"(bar), "r"(parity)
@@ -98,11 +100,9 @@ __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
 
 // Bounded wait for the given phase parity of an mbarrier.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  if (mbar_test(bar, parity)) return true;
   const long long t0 = clock64();
-  while (!mbar_test(bar, parity)) {
+  while (!mbar_try(bar, parity)) {
     if (clock64() - t0 > TC_WAIT_CYCLES) return false;
-    __nanosleep(64);
   }
   return true;
 }
@@ -253,19 +253,44 @@ __device__ __forceinline__ void advance(const GemmEntry<float>* ents, int e1, Sl
 // Set when an mbarrier wait expired (read and cleared by the host).
 __device__ int g_tc_err = 0;
 
+// Position in a CTA's stream of (tile, entry, k slab): the CTA owns tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ...
+struct TileCursor {
+  int tile, e, e1, k0;
+};
+
+__device__ __forceinline__ void tile_begin(const GemmTask<float>* tasks, const GemmEntry<float>* ents,
+                                           const TileRef* tiles, int ntiles, TileCursor& c) {
+  while (c.tile < ntiles) {
+    const GemmTask<float>& t = tasks[tiles[c.tile].task];
+    c.e = t.e0;
+    c.e1 = t.e1;
+    c.k0 = 0;
+    while (c.e < c.e1 && ents[c.e].k <= 0) c.e++;
+    return;
+  }
+}
+
+// Next slab; moves on to the CTA's next tile after the last one of a tile.
+__device__ __forceinline__ bool slab_next(const GemmTask<float>* tasks, const GemmEntry<float>* ents,
+                                          const TileRef* tiles, int ntiles, TileCursor& c) {
+  c.k0 += TC_KT;
+  if (c.k0 >= ents[c.e].k) {
+    c.k0 = 0;
+    c.e++;
+    while (c.e < c.e1 && ents[c.e].k <= 0) c.e++;
+  }
+  return c.e < c.e1;
+}
+
 __global__ void __launch_bounds__(TC_NT, 2)
     k_tc_gemm(const GemmTask<float>* __restrict__ tasks, const GemmEntry<float>* __restrict__ ents,
-              const TileRef* __restrict__ tiles, int split) {
+              const TileRef* __restrict__ tiles, int ntiles, int split) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t bars[TC_HS];
   __shared__ uint32_t tmem_slot;
   __shared__ int wait_ok;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const TileRef tl = tiles[blockIdx.x];
-  const GemmTask<float> task = tasks[tl.task];
-  const int m0 = tl.tm * TC_BM, n0 = tl.tn * TC_BN;
-  const int mrows = min(TC_BM, task.m - m0), ncols = min(TC_BN, task.n - n0);
-  const int nmma = ((ncols + 15) / 16) * 16;  // MMA N: multiple of 16, >= 16
   unsigned char* raw_base = smem;
   unsigned char* hl_base = smem + TC_RS * TC_RAW;
 
@@ -285,130 +310,157 @@ __global__ void __launch_bounds__(TC_NT, 2)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
 
-  SlabCursor prod{task.e0, 0}, cons{task.e0, 0};
-  skip_empty(ents, task.e1, prod);
-  skip_empty(ents, task.e1, cons);
-  const bool any = cons.e < task.e1;
-  bool ok = true;
-  int s = 0;
-  if (any) {
-    // Copies of the slab at the producer cursor into raw slot `slot`; one
-    // commit group per call (empty once the cursor is past the end).
-    auto produce = [&](int slot) {
-      if (prod.e < task.e1) {
-        const GemmEntry<float> en = ents[prod.e];
-        const uint32_t raw = smem_addr(raw_base + slot * TC_RAW);
-        OperandRef a, b;
-        a.X = en.A; a.ld = en.lda; a.rows = mrows; a.r0 = m0; a.k0 = prod.k0; a.K = en.k;
-        a.kcontig = en.opA;  // op(A)(m, k) = A[k + m lda] when transposed
-        a.vec = ((reinterpret_cast<uintptr_t>(en.A) & 15) == 0) && (en.lda % 4 == 0);
-        b.X = en.B; b.ld = en.ldb; b.rows = ncols; b.r0 = n0; b.k0 = prod.k0; b.K = en.k;
-        b.kcontig = en.opB ? 0 : 1;  // op(B)(k, n) = B[k + n ldb] when not transposed
-        b.vec = ((reinterpret_cast<uintptr_t>(en.B) & 15) == 0) && (en.ldb % 4 == 0);
-        issue_operand(a, raw, tid);
-        issue_operand(b, raw + TC_TILE, tid);
-        advance(ents, task.e1, prod);
+  // Producer: copies of the slab at its cursor into raw slot `slot`, one
+  // commit group per call (empty once the CTA's tiles are exhausted).  It
+  // runs two slabs ahead of the consumer, across tile boundaries.
+  TileCursor prod{(int)blockIdx.x, 0, 0, 0};
+  tile_begin(tasks, ents, tiles, ntiles, prod);
+  auto produce = [&](int slot) {
+    while (prod.tile < ntiles && prod.e >= prod.e1) {  // tiles without slabs
+      prod.tile += gridDim.x;
+      tile_begin(tasks, ents, tiles, ntiles, prod);
+    }
+    if (prod.tile < ntiles) {
+      const TileRef tl = tiles[prod.tile];
+      const GemmTask<float> task = tasks[tl.task];
+      const int m0 = tl.tm * TC_BM, n0 = tl.tn * TC_BN;
+      const GemmEntry<float> en = ents[prod.e];
+      const uint32_t raw = smem_addr(raw_base + slot * TC_RAW);
+      OperandRef a, b;
+      a.X = en.A; a.ld = en.lda; a.rows = min(TC_BM, task.m - m0); a.r0 = m0; a.k0 = prod.k0; a.K = en.k;
+      a.kcontig = en.opA;  // op(A)(m, k) = A[k + m lda] when transposed
+      a.vec = ((reinterpret_cast<uintptr_t>(en.A) & 15) == 0) && (en.lda % 4 == 0);
+      b.X = en.B; b.ld = en.ldb; b.rows = min(TC_BN, task.n - n0); b.r0 = n0; b.k0 = prod.k0; b.K = en.k;
+      b.kcontig = en.opB ? 0 : 1;  // op(B)(k, n) = B[k + n ldb] when not transposed
+      b.vec = ((reinterpret_cast<uintptr_t>(en.B) & 15) == 0) && (en.ldb % 4 == 0);
+      issue_operand(a, raw, tid);
+      issue_operand(b, raw + TC_TILE, tid);
+      if (!slab_next(tasks, ents, tiles, ntiles, prod)) {
+        prod.tile += gridDim.x;
+        tile_begin(tasks, ents, tiles, ntiles, prod);
       }
-      cp_commit();
-    };
+    }
+    cp_commit();
+  };
 #pragma unroll
-    for (int j = 0; j < TC_RS - 1; j++) produce(j);
-    uint32_t phase[TC_HS] = {0u, 0u};
-    while (cons.e < task.e1) {
-      const int hb = s & 1;
-      cp_wait<TC_RS - 2>();  // this thread's copies of slab s have landed
-      if (s >= TC_HS && tid == 0) wait_ok = mbar_wait(smem_addr(&bars[hb]), phase[hb]) ? 1 : 0;
-      __syncthreads();  // slab s visible to all; slot (s - 1) % RS free
-      if (s >= TC_HS) {
-        if (!wait_ok) {
+  for (int j = 0; j < TC_RS - 1; j++) produce(j);
+
+  bool ok = true;
+  int s = 0;  // slabs consumed by this CTA (all tiles)
+  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const TileRef tl = tiles[tile];
+    const GemmTask<float> task = tasks[tl.task];
+    const int m0 = tl.tm * TC_BM, n0 = tl.tn * TC_BN;
+    const int mrows = min(TC_BM, task.m - m0), ncols = min(TC_BN, task.n - n0);
+    const int nmma = ((ncols + 15) / 16) * 16;  // MMA N: multiple of 16, >= 16
+    TileCursor cons{tile, 0, 0, 0};
+    tile_begin(tasks, ents, tiles, ntiles, cons);
+    const bool any = cons.e < cons.e1;
+    if (any) {
+      bool more = true;
+      bool first_slab = true;
+      while (more) {
+        const int hb = s & 1;
+        cp_wait<TC_RS - 2>();  // this thread's copies of slab s have landed
+        // Slab s - 2 used the operand buffer hb; its MMAs must have finished
+        // (phase (s - 2) / 2 of that buffer's barrier).
+        if (s >= TC_HS && tid == 0)
+          wait_ok = mbar_wait(smem_addr(&bars[hb]), (uint32_t)(((s - TC_HS) >> 1) & 1)) ? 1 : 0;
+        __syncthreads();  // slab s visible to all; slot (s - 1) % RS free
+        if (s >= TC_HS && !wait_ok) {
           ok = false;
           break;
         }
-        phase[hb] ^= 1u;
-      }
-      produce((s + TC_RS - 1) % TC_RS);
-      const GemmEntry<float> en = ents[cons.e];
-      const unsigned char* raw = raw_base + (s % TC_RS) * TC_RAW;
-      unsigned char* hl = hl_base + hb * TC_HL;
-      const int a_kc = en.opA, b_kc = en.opB ? 0 : 1;
-      convert_operand(raw, a_kc, en.alpha, hl, hl + TC_TILE, tid);
-      convert_operand(raw + TC_TILE, b_kc, 1.f, hl + 2 * TC_TILE, hl + 3 * TC_TILE, tid);
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      __syncthreads();
-      if (tid == 0) {
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t idesc = make_idesc(nmma);
-        const uint32_t base = smem_addr(hl);
+        produce((s + TC_RS - 1) % TC_RS);
+        const GemmEntry<float> en = ents[cons.e];
+        const unsigned char* raw = raw_base + (s % TC_RS) * TC_RAW;
+        unsigned char* hl = hl_base + hb * TC_HL;
+        const int a_kc = en.opA, b_kc = en.opB ? 0 : 1;
+        convert_operand(raw, a_kc, en.alpha, hl, hl + TC_TILE, tid);
+        convert_operand(raw + TC_TILE, b_kc, 1.f, hl + 2 * TC_TILE, hl + 3 * TC_TILE, tid);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t idesc = make_idesc(nmma);
+          const uint32_t base = smem_addr(hl);
 #pragma unroll
-        for (int ks = 0; ks < TC_KT / 8; ks++) {
-          uint64_t ad[2], bd[2];
+          for (int ks = 0; ks < TC_KT / 8; ks++) {
+            uint64_t ad[2], bd[2];
 #pragma unroll
-          for (int h = 0; h < 2; h++) {
-            ad[h] = make_desc(base + h * TC_TILE + ks * 256, 128, TC_SBO);
-            bd[h] = make_desc(base + (2 + h) * TC_TILE + ks * 256, 128, TC_SBO);
+            for (int h = 0; h < 2; h++) {
+              ad[h] = make_desc(base + h * TC_TILE + ks * 256, 128, TC_SBO);
+              bd[h] = make_desc(base + (2 + h) * TC_TILE + ks * 256, 128, TC_SBO);
+            }
+            const uint32_t first = (first_slab && ks == 0) ? 0u : 1u;
+            if (split) {
+              mma_tf32(tmem, ad[1], bd[0], idesc, first);  // lo x hi
+              mma_tf32(tmem, ad[0], bd[1], idesc, 1u);     // hi x lo
+              mma_tf32(tmem, ad[0], bd[0], idesc, 1u);     // hi x hi
+            } else {
+              mma_tf32(tmem, ad[0], bd[0], idesc, first);  // one TF32 product
+            }
           }
-          const uint32_t first = (s == 0 && ks == 0) ? 0u : 1u;
-          if (split) {
-            mma_tf32(tmem, ad[1], bd[0], idesc, first);  // lo x hi
-            mma_tf32(tmem, ad[0], bd[1], idesc, 1u);     // hi x lo
-            mma_tf32(tmem, ad[0], bd[0], idesc, 1u);     // hi x hi
-          } else {
-            mma_tf32(tmem, ad[0], bd[0], idesc, first);  // one TF32 product
+          mma_commit(smem_addr(&bars[hb]));
+        }
+        first_slab = false;
+        more = slab_next(tasks, ents, tiles, ntiles, cons);
+        s++;
+      }
+      if (ok) {
+        // The tile's last slab (s - 1): its MMAs and all earlier ones done.
+        if (tid == 0) wait_ok = mbar_wait(smem_addr(&bars[(s - 1) & 1]), (uint32_t)(((s - 1) >> 1) & 1)) ? 1 : 0;
+        __syncthreads();
+        ok = wait_ok != 0;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    }
+    if (!ok) break;
+
+    // Epilogue: warp w reads TMEM lanes 32 (w & 3) .. +31 (tile rows; a warp
+    // may only read its lane quarter), warps 0-3 columns 0-63 and warps 4-7
+    // columns 64-127, 32 per load; C = beta C + acc, coalesced along the rows
+    // of a column.
+    const int row = (warp & 3) * 32 + lane;
+    for (int c0 = (warp >> 2) * (TC_BN / 2); c0 < (warp >> 2 ? TC_BN : TC_BN / 2); c0 += 32) {
+      if (c0 >= ncols) break;
+      float acc[32];
+      if (any) {
+        uint32_t r[32];
+        const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)c0;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+              "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+              "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int j = 0; j < 32; j++) acc[j] = __uint_as_float(r[j]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 32; j++) acc[j] = 0.f;
+      }
+      if (row < mrows) {
+#pragma unroll
+        for (int j = 0; j < 32; j++) {
+          if (c0 + j < ncols) {
+            float* p = task.C + (i64)(m0 + row) + (i64)(n0 + c0 + j) * task.ldc;
+            *p = (task.beta == 0.f) ? acc[j] : task.beta * (*p) + acc[j];
           }
         }
-        mma_commit(smem_addr(&bars[hb]));
       }
-      advance(ents, task.e1, cons);
-      s++;
     }
-    cp_wait<0>();
-    if (ok) {
-      // Wait for the last slab's MMAs (all earlier ones complete before it).
-      const int hb = (s - 1) & 1;
-      if (tid == 0) wait_ok = mbar_wait(smem_addr(&bars[hb]), phase[hb]) ? 1 : 0;
-      __syncthreads();
-      ok = wait_ok != 0;
-    }
+    // The next tile's first MMA overwrites the accumulator: every warp's
+    // tcgen05.ld must be complete first.
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   }
+  cp_wait<0>();
   if (!ok && tid == 0) atomicExch(&g_tc_err, 1);
-
-  // Epilogue: warp w reads TMEM lanes 32 (w & 3) .. +31 (tile rows; a warp
-  // may only read its lane quarter), warps 0-3 columns 0-63 and warps 4-7
-  // columns 64-127, 32 per load; C = beta C + acc, coalesced along the rows
-  // of a column.
-  const int row = (warp & 3) * 32 + lane;
-  for (int c0 = (warp >> 2) * (TC_BN / 2); c0 < (warp >> 2 ? TC_BN : TC_BN / 2); c0 += 32) {
-    if (c0 >= ncols) break;
-    float acc[32];
-    if (any && ok) {
-      uint32_t r[32];
-      const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)c0;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-          "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-            "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-            "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-          : "r"(taddr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-      for (int j = 0; j < 32; j++) acc[j] = __uint_as_float(r[j]);
-    } else {
-#pragma unroll
-      for (int j = 0; j < 32; j++) acc[j] = 0.f;
-    }
-    if (row < mrows) {
-#pragma unroll
-      for (int j = 0; j < 32; j++) {
-        if (c0 + j < ncols) {
-          float* p = task.C + (i64)(m0 + row) + (i64)(n0 + c0 + j) * task.ldc;
-          *p = (task.beta == 0.f) ? acc[j] : task.beta * (*p) + acc[j];
-        }
-      }
-    }
-  }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
@@ -422,8 +474,16 @@ cudaError_t launch_tc_gemm(const GemmTask<float>* d_tasks, const GemmEntry<float
   if (ntiles == 0) return cudaSuccess;
   cudaError_t e = cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
   if (e != cudaSuccess) return e;
+  // Persistent: two CTAs per SM walk the tile list with a stride of the grid.
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  }
+  const int grid = ntiles < 2 * sms ? ntiles : 2 * sms;
   note_launch();
-  k_tc_gemm<<<ntiles, TC_NT, TC_SMEM, st>>>(d_tasks, d_ents, d_tiles, split);
+  k_tc_gemm<<<grid, TC_NT, TC_SMEM, st>>>(d_tasks, d_ents, d_tiles, ntiles, split);
   return cudaGetLastError();
 }
 

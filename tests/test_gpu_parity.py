@@ -470,3 +470,41 @@ def test_c1_configuration_matches_oracle_fixture(handle):
     # in the third digit, rounding amplified by the weak preconditioner).
     assert np.max(np.abs(np.asarray(A.resid[:A.iters + 1]) - 1.0)) < 1e-2
     assert np.max(np.abs(g["resid"] - 1.0)) < 1e-2
+
+
+def test_yukawa_system_matches_oracle(handle):
+    """Yukawa e^{-alpha r} / r (kernel.hpp:40-50) through the whole path at
+    N = 2048: operator ranks, matvec, factorization, substitution and GMRES
+    against the oracle."""
+    N = 2048
+    b, t, cells, L = problem(N)
+    k = m.Yukawa3D(1.0, 1.0)
+    ko = O.Kernel(O.YUKAWA, 1.0, 1.0)
+    A = m.H2MatrixSolver(handle, k, 1e-10, 100, 0, t, 2.0, b, samples=2000)
+    Ao = O.H2MatrixSolver(ko, 1e-10, 100, 0, cells, 2.0, b.copy(), L, 2000)
+    handle.set_basis_mode(m._lib.BASIS_HOUSEHOLDER)
+    try:
+        M = m.H2MatrixSolver(handle, k, 0.0, 100, 0, t, 2.0, b, samples=2000)
+    finally:
+        handle.set_basis_mode(m._lib.BASIS_GRAM)
+    Mo = O.H2MatrixSolver(ko, 0.0, 100, 0, cells, 2.0, b.copy(), L, 2000)
+    for lvl in range(L + 1):
+        d, r = A.level_dims(lvl)
+        assert np.array_equal(d, Ao.A[lvl].Dims)
+        assert np.abs(r - Ao.A[lvl].DimsLr).max() <= 1
+    x = m.uniform_rhs(N)
+    y = x.copy()
+    A.matVecMul(y)
+    assert rel(y, Ao.matvec(x)) < 1e-10
+    assert rel(y, m.dense_matvec(handle, k, b, x)) < 1e-9
+    assert M.factorizeM() == Mo.factorize()
+    z = x.copy()
+    M.solvePrecondition(z)
+    assert rel(z, Mo.solve_precondition(x)) < 1e-7
+    B = m.dense_matvec(handle, k, b, x)
+    X = np.zeros(N)
+    A.solveGMRES(1e-10, M, X, B, 10, 50)
+    xo, reso, ito = Ao.solve_gmres(1e-10, Mo, np.zeros(N), B, 10, 50)
+    assert A.iters == ito
+    np.testing.assert_allclose(A.resid[:ito + 1], reso, rtol=1e-3, atol=1e-13)
+    assert rel(X, xo) < 1e-8
