@@ -331,7 +331,8 @@ struct GemmPlan {
     if (skinny_nn) {
       // A task takes 256-row tiles when they leave no more padding rows
       // than 128-row tiles would, else 128-row tiles (two launches back to
-      // back; the padding rows are streamed as zeros but cost compute).
+      // back; padding rows are zero-filled copies whose tensor-core work is
+      // skipped, but a mostly empty CTA still walks every stage).
       std::vector<int2> rt[2];
       for (int ti = 0; ti < (int)tasks.size(); ti++) {
         const auto& t = tasks[ti];

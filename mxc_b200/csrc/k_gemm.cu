@@ -406,6 +406,9 @@ __global__ void __launch_bounds__(BM, BM == 256 ? 3 : 6)
     issue((slot + SD_ST - 1) % SD_ST);
     const double* as = As + (size_t)slot * SD_KS * AS + fk * AS + warp * 32 + fr;
     const double* bs = Bs + (size_t)slot * SD_KS * BS + fk * BS + fr;
+    // Row blocks past the task's last row hold zeros: their MMAs are skipped
+    // (8-row granularity), so padded tiles cost no tensor-pipe time.
+    const int mf = min(4, max(0, (mrows - warp * 32 + 7) / 8));
 #pragma unroll
     for (int ks = 0; ks < SD_KS; ks += 4) {
       double a[4], b[NF];
@@ -415,11 +418,12 @@ __global__ void __launch_bounds__(BM, BM == 256 ? 3 : 6)
       for (int j = 0; j < NF; j++) b[j] = bs[ks * BS + j * 8];
 #pragma unroll
       for (int i = 0; i < 4; i++)
+        if (i < mf)
 #pragma unroll
-        for (int j = 0; j < NF; j++)
-          asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-                       : "+d"(acc[i][j][0]), "+d"(acc[i][j][1])
-                       : "d"(a[i]), "d"(b[j]));
+          for (int j = 0; j < NF; j++)
+            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                         : "+d"(acc[i][j][0]), "+d"(acc[i][j][1])
+                         : "d"(a[i]), "d"(b[j]));
     }
     ck += SD_KS;
     if (ck >= ents[ce].k) {
@@ -558,6 +562,7 @@ __global__ void __launch_bounds__(BM, BM == 256 ? 3 : 6)
     issue((slot + SF_ST - 1) % SF_ST);
     const float* as = As + (size_t)slot * SF_KS * AS + warp * 32 + g;
     const float* bs = Bs + (size_t)slot * SF_KS * BS + g;
+    const int mf = min(2, max(0, (mrows - warp * 32 + 15) / 16));  // live 16-row blocks
 #pragma unroll
     for (int ks = 0; ks < SF_KS; ks += 8) {
       // A fragment of m16n8k8 (row): a0 (g, t), a1 (g + 8, t), a2 (g, t + 4), a3 (g + 8, t + 4).
@@ -580,12 +585,13 @@ __global__ void __launch_bounds__(BM, BM == 256 ? 3 : 6)
       }
 #pragma unroll
       for (int i = 0; i < 2; i++)
+        if (i < mf)
 #pragma unroll
-        for (int j = 0; j < NF; j++) {
-          mma_tf32_16x8x8(acc[i][j], al[i], bh[j]);
-          mma_tf32_16x8x8(acc[i][j], ah[i], bl[j]);
-          mma_tf32_16x8x8(acc[i][j], ah[i], bh[j]);
-        }
+          for (int j = 0; j < NF; j++) {
+            mma_tf32_16x8x8(acc[i][j], al[i], bh[j]);
+            mma_tf32_16x8x8(acc[i][j], ah[i], bl[j]);
+            mma_tf32_16x8x8(acc[i][j], ah[i], bh[j]);
+          }
     }
     ck += SF_KS;
     if (ck >= ents[ce].k) {
