@@ -452,6 +452,9 @@ struct GemmPlan {
     } else if (shape == GEMM_TC) {
       if constexpr (std::is_same<T, float>::value)
         ck(launch_tc_gemm(d_tasks.p, d_ents.p, d_tiles.p, ntiles, tc_mode == 1 ? 1 : 0, st), "tc_gemm");
+    } else if (std::is_same<T, double>::value && shape == GEMM_BIG && g_tensor_cores) {
+      if constexpr (std::is_same<T, double>::value)
+        ck(launch_dgemm(d_tasks.p, d_ents.p, d_tiles.p, ntiles, st), "dgemm");
     } else {
       ck(launch_seg_gemm<T>(shape, d_tasks.p, d_ents.p, d_tiles.p, ntiles, st), "seg_gemm");
     }
@@ -702,7 +705,9 @@ class Solver : public SolverBase {
         dg.upload(gt);
         {
           Prof pf("gen_near_blocks", 0., (double)lv.aoff[nA] * sizeof(T));
-          ck(launch_gen_blocks<T>(kp, dg.p, (int)gt.size(), 1, lv.A.p, st()), "gen near");
+          // FP64 blocks use the std::hypot-exact distance (bit-exact with the
+          // reference); FP32 blocks the rsqrt path, rounded to FP32 anyway.
+          ck(launch_gen_blocks<T>(kp, dg.p, (int)gt.size(), 1, lv.A.p, st(), sizeof(T) == 4 ? 1 : 0), "gen near");
         }
       } else {
         CopyPlan<double> pcopy;
@@ -873,7 +878,7 @@ class Solver : public SolverBase {
       dg.upload(gt);
       {
         Prof pf("gen_couplings", 0., (double)lv.coff[nC] * sizeof(T));
-        ck(launch_gen_blocks<T>(kp, dg.p, (int)gt.size(), 1, kout, st()), "gen couplings");
+        ck(launch_gen_blocks<T>(kp, dg.p, (int)gt.size(), 1, kout, st(), sizeof(T) == 4 ? 1 : 0), "gen couplings");
       }
       if (orth) {
         DVec<T> T1;

@@ -143,3 +143,182 @@ cudaError_t launch_gram(const GramTask* d_tasks, const int4* d_tiles, int ntiles
 }
 
 }  // namespace h2b
+
+namespace h2b {
+
+// Segmented FP64 GEMM on the FP64 tensor cores: C_task = beta C_task + sum_e
+// alpha_e op(A_e) op(B_e) over 64 x 64 output tiles (the FP64 plans of the
+// factorization and basis completion).  Same ring and fragments as k_gram;
+// each operand slab (32 k) is staged in the orientation it has in memory:
+// k contiguous -> [row][36] (rows of 32 k, padded), rows contiguous ->
+// [k][68] (k-rows of 64 rows, padded), so every cp.async is a 16-byte
+// vector of consecutive elements and every fragment load of a half-warp hits
+// 16 distinct bank pairs.
+namespace {
+
+constexpr int DG_T = 64, DG_KS = 32, DG_ST = 3, DG_NT = 128;
+constexpr int DG_RK = 36;  // [row][k] stride (doubles)
+constexpr int DG_KR = 68;  // [k][row] stride (doubles)
+constexpr int DG_OP = DG_T * DG_RK > DG_KS * DG_KR ? DG_T * DG_RK : DG_KS * DG_KR;  // doubles per operand
+constexpr int DG_SMEM = DG_ST * 2 * DG_OP * 8;
+
+struct DgOperand {
+  const double* X;
+  i64 ld;
+  int rows, r0, k0, K;
+  int kcontig;  // element (r, k) at X[k + r ld]; otherwise X[r + k ld]
+  int vec;
+};
+
+__device__ __forceinline__ void dg_issue(const DgOperand& o, double* dst, int tid) {
+  if (o.kcontig) {
+    for (int c = tid; c < DG_T * (DG_KS / 2); c += DG_NT) {
+      const int r = c >> 4, kk = (c & 15) * 2;
+      const int k = o.k0 + kk;
+      int nk = o.K - k;
+      nk = nk < 0 ? 0 : (nk > 2 ? 2 : nk);
+      if (r >= o.rows) nk = 0;
+      const double* src = o.X + (i64)k + (i64)(o.r0 + r) * o.ld;
+      const uint32_t d = gsmem(dst + r * DG_RK + kk);
+      if (o.vec) {
+        gcp16(d, nk ? (const void*)src : (const void*)o.X, nk * 8);
+      } else {
+        gcp8(d, nk > 0 ? (const void*)src : (const void*)o.X, nk > 0 ? 8 : 0);
+        gcp8(d + 8, nk > 1 ? (const void*)(src + 1) : (const void*)o.X, nk > 1 ? 8 : 0);
+      }
+    }
+  } else {
+    for (int c = tid; c < DG_KS * (DG_T / 2); c += DG_NT) {
+      const int kk = c >> 5, r = (c & 31) * 2;
+      const int k = o.k0 + kk;
+      int nr = o.rows - r;
+      nr = nr < 0 ? 0 : (nr > 2 ? 2 : nr);
+      if (k >= o.K) nr = 0;
+      const double* src = o.X + (i64)(o.r0 + r) + (i64)k * o.ld;
+      const uint32_t d = gsmem(dst + kk * DG_KR + r);
+      if (o.vec) {
+        gcp16(d, nr ? (const void*)src : (const void*)o.X, nr * 8);
+      } else {
+        gcp8(d, nr > 0 ? (const void*)src : (const void*)o.X, nr > 0 ? 8 : 0);
+        gcp8(d + 8, nr > 1 ? (const void*)(src + 1) : (const void*)o.X, nr > 1 ? 8 : 0);
+      }
+    }
+  }
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(DG_NT, 2) k_dgemm(const GemmTask<double>* __restrict__ tasks,
+                                                   const GemmEntry<double>* __restrict__ ents,
+                                                   const TileRef* __restrict__ tiles) {
+  extern __shared__ __align__(16) double dsm[];
+  const TileRef tl = tiles[blockIdx.x];
+  const GemmTask<double> task = tasks[tl.task];
+  const int m0 = tl.tm * DG_T, n0 = tl.tn * DG_T;
+  const int mrows = min(DG_T, task.m - m0), ncols = min(DG_T, task.n - n0);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  const int fr = lane >> 2, fk = lane & 3;
+
+  int pe = task.e0, pk = 0;
+  while (pe < task.e1 && ents[pe].k <= 0) pe++;
+  auto produce = [&](int slot) {
+    if (pe < task.e1) {
+      const GemmEntry<double> en = ents[pe];
+      double* base = dsm + (size_t)slot * 2 * DG_OP;
+      DgOperand a, b;
+      a.X = en.A; a.ld = en.lda; a.rows = mrows; a.r0 = m0; a.k0 = pk; a.K = en.k;
+      a.kcontig = en.opA;  // op(A)(m, k) = A[k + m lda] when transposed
+      a.vec = ((reinterpret_cast<uintptr_t>(en.A) & 15) == 0) && (en.lda % 2 == 0);
+      b.X = en.B; b.ld = en.ldb; b.rows = ncols; b.r0 = n0; b.k0 = pk; b.K = en.k;
+      b.kcontig = en.opB ? 0 : 1;  // op(B)(k, n) = B[k + n ldb] when not transposed
+      b.vec = ((reinterpret_cast<uintptr_t>(en.B) & 15) == 0) && (en.ldb % 2 == 0);
+      dg_issue(a, base, tid);
+      dg_issue(b, base + DG_OP, tid);
+      pk += DG_KS;
+      if (pk >= en.k) {
+        pk = 0;
+        pe++;
+        while (pe < task.e1 && ents[pe].k <= 0) pe++;
+      }
+    }
+    gcommit();
+  };
+
+  double acc[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.;
+
+#pragma unroll
+  for (int s = 0; s < DG_ST - 1; s++) produce(s);
+  int ce = task.e0, ck = 0, slot = 0;
+  while (ce < task.e1 && ents[ce].k <= 0) ce++;
+  while (ce < task.e1) {
+    gwait<DG_ST - 2>();
+    __syncthreads();
+    produce((slot + DG_ST - 1) % DG_ST);
+    const GemmEntry<double> en = ents[ce];
+    const double* as = dsm + (size_t)slot * 2 * DG_OP;
+    const double* bs = as + DG_OP;
+    const int a_kc = en.opA, b_kc = en.opB ? 0 : 1;
+    const double alpha = en.alpha;
+#pragma unroll
+    for (int ks = 0; ks < DG_KS; ks += 4) {
+      double a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int r = wm * 32 + i * 8 + fr, k = ks + fk;
+        a[i] = alpha * (a_kc ? as[r * DG_RK + k] : as[k * DG_KR + r]);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int r = wn * 32 + j * 8 + fr, k = ks + fk;
+        b[j] = b_kc ? bs[r * DG_RK + k] : bs[k * DG_KR + r];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) dmma(acc[i][j], a[i], b[j]);
+    }
+    ck += DG_KS;
+    if (ck >= en.k) {
+      ck = 0;
+      ce++;
+      while (ce < task.e1 && ents[ce].k <= 0) ce++;
+    }
+    slot = (slot + 1) % DG_ST;
+  }
+  gwait<0>();
+  // D fragment of m8n8k4: lane holds row lane >> 2, columns 2 (lane & 3) + {0, 1}.
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int r = wm * 32 + i * 8 + fr;
+    if (r >= mrows) continue;
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int c = wn * 32 + j * 8 + 2 * fk + h;
+        if (c < ncols) {
+          double* p = task.C + (i64)(m0 + r) + (i64)(n0 + c) * task.ldc;
+          *p = (task.beta == 0.) ? acc[i][j][h] : task.beta * (*p) + acc[i][j][h];
+        }
+      }
+  }
+}
+
+int dgemm_tile() { return DG_T; }
+
+cudaError_t launch_dgemm(const GemmTask<double>* d_tasks, const GemmEntry<double>* d_ents, const TileRef* d_tiles,
+                         int ntiles, cudaStream_t st) {
+  if (ntiles == 0) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(k_dgemm, cudaFuncAttributeMaxDynamicSharedMemorySize, DG_SMEM);
+  if (e != cudaSuccess) return e;
+  note_launch();
+  k_dgemm<<<ntiles, DG_NT, DG_SMEM, st>>>(d_tasks, d_ents, d_tiles);
+  return cudaGetLastError();
+}
+
+}  // namespace h2b

@@ -138,6 +138,11 @@ cudaError_t launch_tc_gemm(const GemmTask<float>* d_tasks, const GemmEntry<float
                            int ntiles, int split, cudaStream_t st);
 int tc_gemm_tile();
 cudaError_t tc_gemm_take_error(int* flag, cudaStream_t st);
+// FP64 segmented GEMM on the FP64 tensor cores (mma.sync m8n8k4), 64 x 64
+// output tiles (TileRef over dgemm_tile()-sized tiles).
+cudaError_t launch_dgemm(const GemmTask<double>* d_tasks, const GemmEntry<double>* d_ents, const TileRef* d_tiles,
+                         int ntiles, cudaStream_t st);
+int dgemm_tile();
 
 template <typename T>
 struct CopyEntry {

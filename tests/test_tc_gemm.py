@@ -8,7 +8,9 @@ miss this by two orders of magnitude), the same bound the SIMT kernel
 meets.  Covered: the four transpose combinations, ragged tiles (m, n
 not multiples of 128, k not a multiple of 32), leading dimensions that are
 not multiples of 4 (scalar-load path), several terms per output, alpha and
-beta, and tensor cores on versus off.
+beta, and tensor cores on versus off.  FP64 plans run on the FP64 tensor
+cores (mma.sync m8n8k4, 64 x 64 tiles) over the same cases, or on the SIMT
+kernel with tensor cores off, both to 1e-14 of the same magnitude bound.
 """
 import ctypes as C
 
@@ -94,7 +96,17 @@ def test_fp32_simt_gemm_same_bound(handle, case):
     assert worst < 1e-5, worst
 
 
-@pytest.mark.parametrize("case", CASES[:4], ids=[str(i) for i in range(4)])
-def test_fp64_gemm(handle, case):
+@pytest.mark.parametrize("case", CASES, ids=[str(i) for i in range(len(CASES))])
+def test_fp64_tensor_core_gemm(handle, case):
     worst = _run(handle, _lib.FP64, *case, seed=9)
+    assert worst < 1e-14, worst
+
+
+@pytest.mark.parametrize("case", CASES[:2], ids=[str(i) for i in range(2)])
+def test_fp64_simt_gemm(handle, case):
+    handle.set_option(_lib.OPT_TENSOR_CORES, 0)
+    try:
+        worst = _run(handle, _lib.FP64, *case, seed=9)
+    finally:
+        handle.set_option(_lib.OPT_TENSOR_CORES, 1)
     assert worst < 1e-14, worst
