@@ -497,6 +497,10 @@ struct Level {
   i64 nodes = 0, gbegin = 0;
   std::vector<i64> arow, acol, crow, ccol, diag;
   std::vector<i64> dims, ranks, xoff, zoff, qoff, aoff, coff;
+  // Leading dimension of box i's coupling blocks C_ij (rank_i x rank_j at
+  // coff): rank_i rounded up to 4, so that every column starts on a
+  // 32-byte boundary and the streaming applies copy whole 16-byte vectors.
+  std::vector<i64> cld;
   i64 lenX = 0, lenZ = 0, maxM = 0;
   DVec<i64> d_dims, d_ranks, d_xoff, d_qoff;
   DVec<double> pts;  // lenX x 3, skeleton-first after the basis
@@ -508,9 +512,10 @@ struct Level {
   DVec<int> ipiv, info;
   int info_count = 0;
   // Transposed copies for the multi-RHS applies, so every apply streams
-  // its matrix as stored: Qt = Q[:, :rank]^T (rank x M per box at qtoff) for
-  // the upward pass, Rt = (factor's R slot)^T (M x M at qoff) for the ULV
-  // forward substitution.
+  // its matrix as stored: Qt = Q[:, :rank]^T (rank x M per box at qtoff,
+  // leading dimension rank rounded up to 4) for the upward pass,
+  // Rt = (factor's R slot)^T (M x M at qoff) for the ULV forward
+  // substitution.
   DVec<T> Qt, Rt;
   std::vector<i64> qtoff;
   // per-nrhs vectors
@@ -735,7 +740,7 @@ class Solver : public SolverBase {
                     low->na_off[lowN] = lv.aoff[k] + offy + offx * M;
                     low->na_ld[lowN] = M;
                   } else if (lowC >= 0) {
-                    acopy.add(low->C.p + low->coff[lowC], ny, lv.A.p + lv.aoff[k] + offy + offx * M, M, (int)ny, (int)nx);
+                    acopy.add(low->C.p + low->coff[lowC], low->cld[y], lv.A.p + lv.aoff[k] + offy + offx * M, M, (int)ny, (int)nx);
                   }
                   offx += nx;
                 }
@@ -848,8 +853,11 @@ class Solver : public SolverBase {
     lv.lenZ = lv.zoff[nodes];
     i64 nC = (i64)lv.ccol.size();
     lv.coff.assign(nC + 1, 0);
-    for (i64 i = 0; i < nodes; i++)
-      for (i64 k = lv.crow[i]; k < lv.crow[i + 1]; k++) lv.coff[k + 1] = lv.coff[k] + lv.ranks[i] * lv.ranks[lv.ccol[k]];
+    lv.cld.assign(nodes, 0);
+    for (i64 i = 0; i < nodes; i++) {
+      lv.cld[i] = (lv.ranks[i] + 3) / 4 * 4;
+      for (i64 k = lv.crow[i]; k < lv.crow[i + 1]; k++) lv.coff[k + 1] = lv.coff[k] + lv.cld[i] * lv.ranks[lv.ccol[k]];
+    }
     lv.C.alloc(lv.coff[nC]);
     if (lv.lenZ > 0 && nC > 0) {
       // Couplings (h2matrix.cpp:279-299): K(S_y, S_x) on the skeletons,
@@ -871,7 +879,7 @@ class Solver : public SolverBase {
           t.m = (int)lv.ranks[i];
           t.n = (int)lv.ranks[x];
           t.out_off = lv.coff[k];
-          t.ld = lv.ranks[i];
+          t.ld = lv.cld[i];
           gt.push_back(t);
         }
       DVec<GenTask> dg;
@@ -888,10 +896,11 @@ class Solver : public SolverBase {
           for (i64 k = lv.crow[i]; k < lv.crow[i + 1]; k++) {
             i64 x = lv.ccol[k];
             int ry = (int)lv.ranks[i], rx = (int)lv.ranks[x];
-            g1.add_task(T1.p + lv.coff[k], ry, ry, rx, T(0));
-            g1.add_entry(lv.R.p + lv.qoff[i], lv.dims[i], 0, K.p + lv.coff[k], ry, 0, ry, T(1));
-            g2.add_task(lv.C.p + lv.coff[k], ry, ry, rx, T(0));
-            g2.add_entry(T1.p + lv.coff[k], ry, 0, lv.R.p + lv.qoff[x], lv.dims[x], 1, rx, T(1));
+            const i64 ld = lv.cld[i];
+            g1.add_task(T1.p + lv.coff[k], ld, ry, rx, T(0));
+            g1.add_entry(lv.R.p + lv.qoff[i], lv.dims[i], 0, K.p + lv.coff[k], ld, 0, ry, T(1));
+            g2.add_task(lv.C.p + lv.coff[k], ld, ry, rx, T(0));
+            g2.add_entry(T1.p + lv.coff[k], ld, 0, lv.R.p + lv.qoff[x], lv.dims[x], 1, rx, T(1));
           }
         g1.name = g2.name = "gemm_coupling";
         g1.finalize();
@@ -1258,10 +1267,11 @@ class Solver : public SolverBase {
       for (i64 l = 0; l <= levels; l++) {
         Level<T>& lv = L[l];
         lv.qtoff.assign(lv.nodes + 1, 0);
-        for (i64 i = 0; i < lv.nodes; i++) lv.qtoff[i + 1] = lv.qtoff[i] + lv.ranks[i] * lv.dims[i];
+        // Leading dimension rank_i rounded up to 4 (32-byte column starts).
+        for (i64 i = 0; i < lv.nodes; i++) lv.qtoff[i + 1] = lv.qtoff[i] + (lv.ranks[i] + 3) / 4 * 4 * lv.dims[i];
         lv.Qt.alloc(std::max<i64>(1, lv.qtoff[lv.nodes]));
         for (i64 i = 0; i < lv.nodes; i++)
-          tp.add(lv.Q.p + lv.qoff[i], lv.dims[i], lv.Qt.p + lv.qtoff[i], lv.ranks[i], (int)lv.ranks[i],
+          tp.add(lv.Q.p + lv.qoff[i], lv.dims[i], lv.Qt.p + lv.qtoff[i], (lv.ranks[i] + 3) / 4 * 4, (int)lv.ranks[i],
                  (int)lv.dims[i], 1);
       }
       tp.finalize();
@@ -1277,7 +1287,7 @@ class Solver : public SolverBase {
         int M = (int)lv.dims[i], r = (int)lv.ranks[i];
         if (r == 0) continue;
         g.add_task(lv.vZ.p + lv.zoff[i], lv.lenZ, r, nr, T(0));
-        g.add_entry(lv.Qt.p + lv.qtoff[i], r, 0, X + lv.xoff[i], ldx, 0, M, T(1));
+        g.add_entry(lv.Qt.p + lv.qtoff[i], (r + 3) / 4 * 4, 0, X + lv.xoff[i], ldx, 0, M, T(1));
       }
       g.finalize();
     }
@@ -1291,7 +1301,7 @@ class Solver : public SolverBase {
         mv_far.add_task(lv.vW.p + lv.zoff[i], lv.lenZ, r, nr, T(0));
         for (i64 k = lv.crow[i]; k < lv.crow[i + 1]; k++) {
           i64 j = lv.ccol[k];
-          mv_far.add_entry(lv.C.p + lv.coff[k], r, 0, lv.vZ.p + lv.zoff[j], lv.lenZ, 0, (int)lv.ranks[j], T(1));
+          mv_far.add_entry(lv.C.p + lv.coff[k], lv.cld[i], 0, lv.vZ.p + lv.zoff[j], lv.lenZ, 0, (int)lv.ranks[j], T(1));
         }
       }
     }
@@ -1699,7 +1709,12 @@ class Solver : public SolverBase {
       case H2DEV_EXPORT_Q:
       case H2DEV_EXPORT_R: return lv.qoff.back();
       case H2DEV_EXPORT_A: return lv.aoff.back();
-      case H2DEV_EXPORT_C: return lv.coff.back();
+      case H2DEV_EXPORT_C: {
+        i64 n = 0;  // packed: each block rank_i x rank_j with leading dimension rank_i
+        for (i64 i = 0; i < lv.nodes; i++)
+          for (i64 k = lv.crow[i]; k < lv.crow[i + 1]; k++) n += lv.ranks[i] * lv.ranks[lv.ccol[k]];
+        return n;
+      }
     }
     require(false, "export: unknown container");
     return 0;
@@ -1715,11 +1730,25 @@ class Solver : public SolverBase {
       return;
     }
     const T* src = what == H2DEV_EXPORT_Q ? lv.Q.p : what == H2DEV_EXPORT_R ? lv.R.p : what == H2DEV_EXPORT_A ? lv.A.p : lv.C.p;
+    const i64 stored = what == H2DEV_EXPORT_C ? lv.coff.back() : n;
     DVec<double> tmp;
-    tmp.alloc(n);
-    ck(launch_convert<T, double>(src, tmp.p, n, st()), "export convert");
+    tmp.alloc(stored);
+    ck(launch_convert<T, double>(src, tmp.p, stored, st()), "export convert");
     ck(cudaStreamSynchronize(st()), "sync");
-    ck(cudaMemcpy(out, tmp.p, sizeof(double) * n, cudaMemcpyDeviceToHost), "export");
+    if (what != H2DEV_EXPORT_C) {
+      ck(cudaMemcpy(out, tmp.p, sizeof(double) * n, cudaMemcpyDeviceToHost), "export");
+      return;
+    }
+    // Couplings are stored with leading dimension cld[i] >= rank_i: repack.
+    std::vector<double> h(stored);
+    ck(cudaMemcpy(h.data(), tmp.p, sizeof(double) * stored, cudaMemcpyDeviceToHost), "export");
+    i64 o = 0;
+    for (i64 i = 0; i < lv.nodes; i++)
+      for (i64 k = lv.crow[i]; k < lv.crow[i + 1]; k++) {
+        const i64 ri = lv.ranks[i], rj = lv.ranks[lv.ccol[k]];
+        for (i64 c = 0; c < rj; c++)
+          for (i64 r = 0; r < ri; r++) out[o++] = h[lv.coff[k] + r + c * lv.cld[i]];
+      }
   }
 };
 

@@ -3,27 +3,12 @@
 // C_task = beta C_task + sum_e alpha_e op(A_e) op(B_e), the same task /
 // entry lists as the SIMT segmented GEMM, for the FP32 contractions of the
 // ULV factorization.  FP32 accuracy on TF32 tensor cores by the 3-term split
-// x = hi + lo (hi = x rounded to TF32, lo = x - hi exactly in FP32):
-// A B ~= A_hi B_hi + A_hi B_lo + A_lo B_hi, every product accumulated in FP32
-// in tensor memory (the dropped A_lo B_lo term and the TF32 truncation of lo
-// are below 2^-21 relative).
+// x = hi + lo: A B ~= A_hi B_hi + A_hi B_lo + A_lo B_hi, every product
+// accumulated in FP32 in tensor memory (the dropped A_lo B_lo term and the
+// TF32 truncation of lo are below 2^-20 relative).
 //
-// One CTA (256 threads, two per SM) owns a 128 x 128 output tile; its
-// accumulator is 128 TMEM lanes x 128 columns.  The task's (entry, 16-wide
-// k slab) sequence flows through three stages:
-//  1. raw ring (3 slots): every thread issues cp.async copies of the slab's
-//     A and B tiles in their global orientation (16-byte chunks, XOR-swizzled
-//     so the reads of stage 2 are bank-conflict-free; rows past m / n and k
-//     past K are zero-filled), two slabs ahead of the one being converted;
-//  2. conversion: the slab is read back, scaled by alpha (A), split into hi
-//     and lo and stored in the canonical no-swizzle K-major UMMA layout (row-
-//     contiguous operands are transposed 4 x 4 in registers), into one of two
-//     operand buffers;
-//  3. one thread issues the slab's 6 MMAs (2 k-steps x 3 products) and
-//     commits them to the buffer's mbarrier; the buffer is converted into
-//     again once that barrier completes.
-// Every mbarrier wait is bounded (about two seconds of clock cycles); on
-// expiry the kernel records an error flag for the host and leaves.
+// 128 x 128 output tiles, 16-wide k slabs; one persistent warp-specialised
+// CTA per SM (see k_tc_gemm_ws below for the roles and the stage ring).
 #include "common.cuh"
 #include "kernels.h"
 
@@ -33,14 +18,12 @@ namespace h2b {
 
 namespace {
 
-constexpr int TC_BM = 128, TC_BN = 128, TC_KT = 16, TC_NT = 256;
-constexpr int TC_CPT = TC_BM * TC_KT / 4 / TC_NT;  // 16-byte chunks per thread per operand
+constexpr int TC_BM = 128, TC_BN = 128, TC_KT = 16;
+// Row-contiguous B conversion: 256 threads, 2 chunks of 16 bytes per thread.
+constexpr int TC_NT = 256;
+constexpr int TC_CPT = TC_BM * TC_KT / 4 / TC_NT;
 constexpr int TC_KC = TC_KT / 4;            // 16-byte k-chunks per row
 constexpr int TC_TILE = TC_BM * TC_KT * 4;  // bytes of one 128 x 16 FP32 operand tile
-constexpr int TC_RAW = 2 * TC_TILE;         // raw slot: A, B
-constexpr int TC_HL = 4 * TC_TILE;          // operand buffer: A hi, A lo, B hi, B lo
-constexpr int TC_RS = 3, TC_HS = 2;
-constexpr int TC_SMEM = TC_RS * TC_RAW + TC_HS * TC_HL;
 constexpr long long TC_WAIT_CYCLES = 4000000000LL;
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -68,16 +51,6 @@ __device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo, uint
 // Instruction descriptor: D FP32, A and B TF32 (both K-major), M = 128, N = n.
 __device__ __forceinline__ uint32_t make_idesc(int n) {
   return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                         uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t"
-      "}\n" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
@@ -113,69 +86,16 @@ __device__ __forceinline__ void cp16(uint32_t dst, const void* src, int bytes) {
 __device__ __forceinline__ void cp4(uint32_t dst, const void* src, int bytes) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
 }
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// x rounded to the nearest TF32 value (10 explicit mantissa bits; ties away
+// from zero): add half a TF32 ulp to the magnitude bits, clear the 13 low
+// bits.  Integer ALU work only; inputs are finite and far below FLT_MAX.
 __device__ __forceinline__ float tf32_hi(float x) {
-  uint32_t u;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(x));
-  return __uint_as_float(u & 0xFFFFE000u);
-}
-
-// One operand of a slab: 128 rows (of op(X), rows of the output tile) by
-// 16 k.  kcontig: element (r, k) at X[k + r * ld]; otherwise at X[r + k * ld].
-struct OperandRef {
-  const float* X;
-  i64 ld;
-  int rows;  // valid rows in the tile (from the tile origin)
-  int r0;    // tile origin in rows
-  int k0, K;
-  int kcontig;
-  int vec;  // 16-byte copies are aligned
-};
-
-// Issues this thread's copies (2 chunks of 16 bytes) of a raw operand tile.
-// k contiguous: chunk c = tid + 256 i is row c >> 2, k-chunk c & 3 (a warp
-// reads 8 rows x 64 contiguous bytes).  Rows contiguous: chunk c is row
-// quad c & 31 of k-row c >> 5 (a warp reads 512 contiguous bytes).
-__device__ __forceinline__ void issue_operand(const OperandRef& o, uint32_t raw, int tid) {
-#pragma unroll
-  for (int i = 0; i < TC_CPT; i++) {
-    const int c = tid + TC_NT * i;
-    if (o.kcontig) {
-      const int r = c >> 2, kc = c & 3;
-      const int gk = o.k0 + kc * 4;
-      const uint32_t dst = raw + raw_kc(r, kc);
-      const bool rowok = r < o.rows;
-      int nk = o.K - gk;
-      nk = nk < 0 ? 0 : (nk > 4 ? 4 : nk);
-      if (!rowok) nk = 0;
-      const float* p = o.X + (i64)gk + (i64)(o.r0 + r) * o.ld;
-      if (o.vec) {
-        cp16(dst, nk ? (const void*)p : (const void*)o.X, nk * 4);
-      } else {
-#pragma unroll
-        for (int j = 0; j < 4; j++) cp4(dst + 4 * j, j < nk ? (const void*)(p + j) : (const void*)o.X, j < nk ? 4 : 0);
-      }
-    } else {
-      const int q = c & 31, k = c >> 5;
-      const int gk = o.k0 + k, r = 4 * q;
-      const uint32_t dst = raw + raw_rc(q, k);
-      int nr = o.rows - r;
-      nr = nr < 0 ? 0 : (nr > 4 ? 4 : nr);
-      if (gk >= o.K) nr = 0;
-      const float* p = o.X + (i64)(o.r0 + r) + (i64)gk * o.ld;
-      if (o.vec) {
-        cp16(dst, nr ? (const void*)p : (const void*)o.X, nr * 4);
-      } else {
-#pragma unroll
-        for (int j = 0; j < 4; j++) cp4(dst + 4 * j, j < nr ? (const void*)(p + j) : (const void*)o.X, j < nr ? 4 : 0);
-      }
-    }
-  }
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
 __device__ __forceinline__ float pick(const float4& v, int j) {
@@ -231,77 +151,218 @@ __device__ __forceinline__ void convert_operand(const unsigned char* raw, int kc
   }
 }
 
-struct SlabCursor {
-  int e, k0;
-};
-
-__device__ __forceinline__ void skip_empty(const GemmEntry<float>* ents, int e1, SlabCursor& c) {
-  while (c.e < e1 && ents[c.e].k <= 0) c.e++;
-}
-
-__device__ __forceinline__ void advance(const GemmEntry<float>* ents, int e1, SlabCursor& c) {
-  c.k0 += TC_KT;
-  if (c.k0 >= ents[c.e].k) {
-    c.k0 = 0;
-    c.e++;
-    skip_empty(ents, e1, c);
-  }
-}
-
 }  // namespace
 
 // Set when an mbarrier wait expired (read and cleared by the host).
 __device__ int g_tc_err = 0;
 
-// Position in a CTA's stream of (tile, entry, k slab): the CTA owns tiles
-// blockIdx.x, blockIdx.x + gridDim.x, ...
-struct TileCursor {
-  int tile, e, e1, k0;
+// Warp-specialised variant, one CTA per SM (21 warps, 512 TMEM columns),
+// A operand in tensor memory, double-buffered accumulator.
+//
+// The tensor core reads a TF32 operand from a 32-bit container by ignoring
+// its 13 low mantissa bits, so the split needs no rounding pass: hi = x as
+// stored (truncated by the hardware), lo = x - trunc(x) (exact in FP32).
+// Per slab the work is therefore: copy A raw and B (k-contiguous B straight
+// into its K-major hi tile), then the converters write A_hi / A_lo from
+// registers into TMEM (tcgen05.st; lane = tile row, column = k) and compute
+// B_lo from B_hi in place.  Row-contiguous B is copied raw and converted
+// (transposed, rounded split) as in the kernel above.  The MMAs read A from
+// TMEM and only B from shared memory.
+//
+// Stage ring (WS_ST stages of 32 KB: A raw, B raw, B hi, B lo; TMEM A
+// buffer of 32 columns per stage at 256 + 32 s):
+//  warps 0-3   producers: wait stage_free (the MMAs of the stage's previous
+//              slab done), cp.async the slab, cp.async.mbarrier.arrive on
+//              full.
+//  warps 4-11  converters: wait full; warp w writes A rows 32 (w & 3) ..
+//              +31, k 8 h .. +7 (h = (w - 4) >> 2) to TMEM and its share of
+//              B lo; signal conv_full.
+//  warps 12-19 epilogue: wait acc_full, read TMEM lane quarter w & 3,
+//              columns 64 ((w - 12) >> 2) .. +63, release the accumulator
+//              (acc_empty), write C.
+//  warp 20     one thread: wait conv_full (and, before a tile's first slab,
+//              acc_empty of its accumulator), issue the slab's MMAs, commit
+//              to stage_free and, after a tile's last slab, to acc_full.
+// Every wait is bounded; an expired wait sets a CTA-wide abort flag that
+// ends every role's loop.  Waits are taken by one lane and broadcast, so
+// warp-collective instructions stay convergent; no named barrier is used
+// inside the loops.
+namespace {
+constexpr int WS_NT = 672;
+constexpr int WS_ST = 6;
+constexpr int WS_STAGE = 4 * TC_TILE;  // A raw, B raw, B hi, B lo
+constexpr int WS_SMEM = WS_ST * WS_STAGE;
+constexpr int WS_TMEM_COLS = 512;
+constexpr int WS_ACOL = 2 * TC_BN;  // first A buffer column
+constexpr uint32_t TF32_MASK = 0xFFFFE000u;
+
+// try_wait with a suspend-time hint (ns): a waiting thread sleeps in
+// hardware until the phase completes instead of spinning on issue slots.
+__device__ __forceinline__ bool mbar_try_sleep(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity), "r"(1000000u)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ bool ws_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+  if (mbar_try_sleep(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_sleep(bar, parity)) {
+    if (*abort_flag) return false;
+    if (clock64() - t0 > TC_WAIT_CYCLES) {
+      *abort_flag = 1;
+      return false;
+    }
+  }
+  return true;
+}
+
+// Lane 0 waits, the warp learns the outcome (warp-uniform).
+__device__ __forceinline__ bool warp_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int lane) {
+  int ok = 1;
+  if (lane == 0) ok = ws_wait(bar, parity, abort_flag) ? 1 : 0;
+  return __shfl_sync(0xffffffffu, ok, 0) != 0;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mma_tf32_ta(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t"
+      "}\n" ::"r"(tmem_d),
+      "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&v)[8]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr), "r"(v[0]),
+               "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+               : "memory");
+}
+
+struct WsTile {
+  int m0, n0, mrows, ncols, e0, e1;
+  GemmTask<float> task;
 };
 
-__device__ __forceinline__ void tile_begin(const GemmTask<float>* tasks, const GemmEntry<float>* ents,
-                                           const TileRef* tiles, int ntiles, TileCursor& c) {
-  while (c.tile < ntiles) {
-    const GemmTask<float>& t = tasks[tiles[c.tile].task];
-    c.e = t.e0;
-    c.e1 = t.e1;
-    c.k0 = 0;
-    while (c.e < c.e1 && ents[c.e].k <= 0) c.e++;
-    return;
-  }
+__device__ __forceinline__ WsTile ws_tile(const GemmTask<float>* tasks, const GemmEntry<float>* ents,
+                                          const TileRef* tiles, int tile) {
+  WsTile w;
+  const TileRef tl = tiles[tile];
+  w.task = tasks[tl.task];
+  w.m0 = tl.tm * TC_BM;
+  w.n0 = tl.tn * TC_BN;
+  w.mrows = min(TC_BM, w.task.m - w.m0);
+  w.ncols = min(TC_BN, w.task.n - w.n0);
+  w.e0 = w.task.e0;
+  w.e1 = w.task.e1;
+  while (w.e0 < w.e1 && ents[w.e0].k <= 0) w.e0++;
+  return w;
 }
 
-// Next slab; moves on to the CTA's next tile after the last one of a tile.
-__device__ __forceinline__ bool slab_next(const GemmTask<float>* tasks, const GemmEntry<float>* ents,
-                                          const TileRef* tiles, int ntiles, TileCursor& c) {
-  c.k0 += TC_KT;
-  if (c.k0 >= ents[c.e].k) {
-    c.k0 = 0;
-    c.e++;
-    while (c.e < c.e1 && ents[c.e].k <= 0) c.e++;
+// A producer thread's four 16-byte chunks of one operand tile (the chunks
+// c = ptid + 128 j of the tile's 512), resolved once per entry: per slab only
+// the k offset changes.  k contiguous: chunk j is row (ptid >> 2) + 32 j,
+// k-chunk ptid & 3, stored in the raw layout or, with kmajor, directly in
+// the canonical K-major layout; rows contiguous: chunk j is row quad
+// ptid & 31 of k-row (ptid >> 5) + 4 j (raw layout).
+struct ProdChunks {
+  const float* X;
+  const float* src[4];  // element (row, k = k0 + kofs) at src + k0 * kstep
+  uint32_t dst[4];
+  i64 kstep;
+  int kofs[4];
+  int nrow[4];  // k contiguous: 4 if the row is in the tile else 0; rows contiguous: valid rows of the quad
+  int kcontig, vec, K;
+};
+
+__device__ __forceinline__ void prod_prepare(ProdChunks& pc, const float* X, i64 ld, int rows, int r0, int K,
+                                             int kcontig, int kmajor, uint32_t base, int ptid) {
+  pc.X = X;
+  pc.K = K;
+  pc.kcontig = kcontig;
+  pc.vec = ((reinterpret_cast<uintptr_t>(X) & 15) == 0) && (ld % 4 == 0);
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    if (kcontig) {
+      const int r = (ptid >> 2) + 32 * j, kc = ptid & 3;
+      pc.kofs[j] = 4 * kc;
+      pc.nrow[j] = r < rows ? 4 : 0;
+      pc.src[j] = X + (i64)(r0 + r) * ld + 4 * kc;
+      pc.dst[j] = base + (kmajor ? off_kmajor(r, kc) : raw_kc(r, kc));
+    } else {
+      const int q = ptid & 31, k = (ptid >> 5) + 4 * j;
+      int nr = rows - 4 * q;
+      pc.kofs[j] = k;
+      pc.nrow[j] = nr < 0 ? 0 : (nr > 4 ? 4 : nr);
+      pc.src[j] = X + (i64)(r0 + 4 * q) + (i64)k * ld;
+      pc.dst[j] = base + raw_rc(q, k);
+    }
   }
-  return c.e < c.e1;
+  pc.kstep = kcontig ? 1 : ld;
 }
 
-__global__ void __launch_bounds__(TC_NT, 2)
-    k_tc_gemm(const GemmTask<float>* __restrict__ tasks, const GemmEntry<float>* __restrict__ ents,
-              const TileRef* __restrict__ tiles, int ntiles, int split) {
+// Issues the four chunks of the slab at k0 into stage offset `stage_off`.
+__device__ __forceinline__ void prod_issue(const ProdChunks& pc, int k0, uint32_t stage_off) {
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    const int k = k0 + pc.kofs[j];
+    int n;
+    if (pc.kcontig) {
+      n = pc.K - k;
+      n = n < 0 ? 0 : (n > 4 ? 4 : n);
+      if (!pc.nrow[j]) n = 0;
+    } else {
+      n = k < pc.K ? pc.nrow[j] : 0;
+    }
+    const float* p = pc.src[j] + (i64)k0 * pc.kstep;
+    const uint32_t d = pc.dst[j] + stage_off;
+    if (pc.vec) {
+      cp16(d, n ? (const void*)p : (const void*)pc.X, n * 4);
+    } else {  // the four elements of a chunk are adjacent in memory in both layouts
+#pragma unroll
+      for (int t = 0; t < 4; t++) cp4(d + 4 * t, t < n ? (const void*)(p + t) : (const void*)pc.X, t < n ? 4 : 0);
+    }
+  }
+}
+}  // namespace
+
+__global__ void __launch_bounds__(WS_NT, 1)
+    k_tc_gemm_ws(const GemmTask<float>* __restrict__ tasks, const GemmEntry<float>* __restrict__ ents,
+                 const TileRef* __restrict__ tiles, int ntiles, int split) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ __align__(8) uint64_t bars[TC_HS];
+  __shared__ __align__(8) uint64_t full[WS_ST], conv_full[WS_ST], stage_free[WS_ST], acc_full[2], acc_empty[2], drain;
   __shared__ uint32_t tmem_slot;
-  __shared__ int wait_ok;
+  __shared__ volatile int abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  unsigned char* raw_base = smem;
-  unsigned char* hl_base = smem + TC_RS * TC_RAW;
 
   if (tid == 0) {
-    for (int s = 0; s < TC_HS; s++)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bars[s])) : "memory");
+    for (int s = 0; s < WS_ST; s++) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(smem_addr(&full[s])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 8;" ::"r"(smem_addr(&conv_full[s])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&stage_free[s])) : "memory");
+    }
+    for (int s = 0; s < 2; s++) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&acc_full[s])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 8;" ::"r"(smem_addr(&acc_empty[s])) : "memory");
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&drain)) : "memory");
+    abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
-                 "r"(TC_BN)
+                 "r"(WS_TMEM_COLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -310,161 +371,231 @@ __global__ void __launch_bounds__(TC_NT, 2)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
 
-  // Producer: copies of the slab at its cursor into raw slot `slot`, one
-  // commit group per call (empty once the CTA's tiles are exhausted).  It
-  // runs two slabs ahead of the consumer, across tile boundaries.
-  TileCursor prod{(int)blockIdx.x, 0, 0, 0};
-  tile_begin(tasks, ents, tiles, ntiles, prod);
-  auto produce = [&](int slot) {
-    while (prod.tile < ntiles && prod.e >= prod.e1) {  // tiles without slabs
-      prod.tile += gridDim.x;
-      tile_begin(tasks, ents, tiles, ntiles, prod);
-    }
-    if (prod.tile < ntiles) {
-      const TileRef tl = tiles[prod.tile];
-      const GemmTask<float> task = tasks[tl.task];
-      const int m0 = tl.tm * TC_BM, n0 = tl.tn * TC_BN;
-      const GemmEntry<float> en = ents[prod.e];
-      const uint32_t raw = smem_addr(raw_base + slot * TC_RAW);
-      OperandRef a, b;
-      a.X = en.A; a.ld = en.lda; a.rows = min(TC_BM, task.m - m0); a.r0 = m0; a.k0 = prod.k0; a.K = en.k;
-      a.kcontig = en.opA;  // op(A)(m, k) = A[k + m lda] when transposed
-      a.vec = ((reinterpret_cast<uintptr_t>(en.A) & 15) == 0) && (en.lda % 4 == 0);
-      b.X = en.B; b.ld = en.ldb; b.rows = min(TC_BN, task.n - n0); b.r0 = n0; b.k0 = prod.k0; b.K = en.k;
-      b.kcontig = en.opB ? 0 : 1;  // op(B)(k, n) = B[k + n ldb] when not transposed
-      b.vec = ((reinterpret_cast<uintptr_t>(en.B) & 15) == 0) && (en.ldb % 4 == 0);
-      issue_operand(a, raw, tid);
-      issue_operand(b, raw + TC_TILE, tid);
-      if (!slab_next(tasks, ents, tiles, ntiles, prod)) {
-        prod.tile += gridDim.x;
-        tile_begin(tasks, ents, tiles, ntiles, prod);
+  if (warp < 4) {
+    // ---------------------------------------------------------- producers
+    int g = 0;
+    bool ok = true;
+    const uint32_t st0 = smem_addr(smem);
+    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+      const WsTile w = ws_tile(tasks, ents, tiles, tile);
+      for (int e = w.e0; e < w.e1 && ok; e++) {
+        const GemmEntry<float> en = ents[e];
+        if (en.k <= 0) continue;
+        const int b_kc = en.opB ? 0 : 1;
+        ProdChunks pa, pb;
+        prod_prepare(pa, en.A, en.lda, w.mrows, w.m0, en.k, en.opA, 0, st0, tid);
+        prod_prepare(pb, en.B, en.ldb, w.ncols, w.n0, en.k, b_kc, b_kc, st0 + (b_kc ? 2 : 1) * TC_TILE, tid);
+        for (int k0 = 0; k0 < en.k; k0 += TC_KT) {
+          const int s = g % WS_ST;
+          if (g >= WS_ST && !ws_wait(smem_addr(&stage_free[s]), (uint32_t)(((g / WS_ST) - 1) & 1), &abort_flag)) {
+            ok = false;
+            break;
+          }
+          prod_issue(pa, k0, (uint32_t)(s * WS_STAGE));
+          prod_issue(pb, k0, (uint32_t)(s * WS_STAGE));
+          asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_addr(&full[s])) : "memory");
+          g++;
+        }
       }
     }
-    cp_commit();
-  };
+    cp_wait<0>();
+  } else if (warp < 12) {
+    // --------------------------------------------------------- converters
+    const int ctid = tid - 128;
+    const int q = warp & 3, kh = (warp - 4) >> 2;
+    const int r = q * 32 + lane;  // A row (TMEM lane) of this thread
+    const uint32_t tmem_row = tmem + ((uint32_t)(q * 32) << 16);
+    int g = 0;
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+      const WsTile w = ws_tile(tasks, ents, tiles, tile);
+      for (int e = w.e0; e < w.e1 && ok; e++) {
+        const GemmEntry<float> en = ents[e];
+        if (en.k <= 0) continue;
+        const int b_kc = en.opB ? 0 : 1;
+        const bool unit = en.alpha == 1.f;
+        for (int k0 = 0; k0 < en.k; k0 += TC_KT) {
+          const int s = g % WS_ST;
+          if (!warp_wait(smem_addr(&full[s]), (uint32_t)((g / WS_ST) & 1), &abort_flag, lane)) {
+            ok = false;
+            break;
+          }
+          unsigned char* st = smem + s * WS_STAGE;
+          // A row r, k 8 kh .. 8 kh + 7 -> TMEM (hi = x, lo = x - trunc(x)).
+          float v[8];
+          if (en.opA) {
 #pragma unroll
-  for (int j = 0; j < TC_RS - 1; j++) produce(j);
-
-  bool ok = true;
-  int s = 0;  // slabs consumed by this CTA (all tiles)
-  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    const TileRef tl = tiles[tile];
-    const GemmTask<float> task = tasks[tl.task];
-    const int m0 = tl.tm * TC_BM, n0 = tl.tn * TC_BN;
-    const int mrows = min(TC_BM, task.m - m0), ncols = min(TC_BN, task.n - n0);
-    const int nmma = ((ncols + 15) / 16) * 16;  // MMA N: multiple of 16, >= 16
-    TileCursor cons{tile, 0, 0, 0};
-    tile_begin(tasks, ents, tiles, ntiles, cons);
-    const bool any = cons.e < cons.e1;
-    if (any) {
-      bool more = true;
-      bool first_slab = true;
-      while (more) {
-        const int hb = s & 1;
-        cp_wait<TC_RS - 2>();  // this thread's copies of slab s have landed
-        // Slab s - 2 used the operand buffer hb; its MMAs must have finished
-        // (phase (s - 2) / 2 of that buffer's barrier).
-        if (s >= TC_HS && tid == 0)
-          wait_ok = mbar_wait(smem_addr(&bars[hb]), (uint32_t)(((s - TC_HS) >> 1) & 1)) ? 1 : 0;
-        __syncthreads();  // slab s visible to all; slot (s - 1) % RS free
-        if (s >= TC_HS && !wait_ok) {
-          ok = false;
-          break;
+            for (int c = 0; c < 2; c++) {
+              const float4 x = *reinterpret_cast<const float4*>(st + raw_kc(r, 2 * kh + c));
+              v[4 * c] = x.x; v[4 * c + 1] = x.y; v[4 * c + 2] = x.z; v[4 * c + 3] = x.w;
+            }
+          } else {
+#pragma unroll
+            for (int k = 0; k < 8; k++) v[k] = *reinterpret_cast<const float*>(st + raw_rc(r >> 2, 8 * kh + k) + (r & 3) * 4);
+          }
+          uint32_t hi[8], lo[8];
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            const float x = unit ? v[k] : v[k] * en.alpha;
+            hi[k] = __float_as_uint(x);
+            lo[k] = __float_as_uint(x - __uint_as_float(hi[k] & TF32_MASK));
+          }
+          const uint32_t acol = (uint32_t)(WS_ACOL + s * 32 + 8 * kh);
+          tmem_st8(tmem_row + acol, hi);
+          tmem_st8(tmem_row + acol + 16, lo);
+          // B lo (k-contiguous B: from the hi tile the copies filled).
+          unsigned char* bhi = st + 2 * TC_TILE;
+          unsigned char* blo = st + 3 * TC_TILE;
+          if (b_kc) {
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+              const int off = (ctid + 256 * i) * 16;
+              const float4 x = *reinterpret_cast<const float4*>(bhi + off);
+              float4 l;
+              l.x = x.x - __uint_as_float(__float_as_uint(x.x) & TF32_MASK);
+              l.y = x.y - __uint_as_float(__float_as_uint(x.y) & TF32_MASK);
+              l.z = x.z - __uint_as_float(__float_as_uint(x.z) & TF32_MASK);
+              l.w = x.w - __uint_as_float(__float_as_uint(x.w) & TF32_MASK);
+              *reinterpret_cast<float4*>(blo + off) = l;
+            }
+          } else {
+            convert_operand(st + TC_TILE, 0, 1.f, bhi, blo, ctid);
+          }
+          asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) mbar_arrive(smem_addr(&conv_full[s]));
+          g++;
         }
-        produce((s + TC_RS - 1) % TC_RS);
-        const GemmEntry<float> en = ents[cons.e];
-        const unsigned char* raw = raw_base + (s % TC_RS) * TC_RAW;
-        unsigned char* hl = hl_base + hb * TC_HL;
-        const int a_kc = en.opA, b_kc = en.opB ? 0 : 1;
-        convert_operand(raw, a_kc, en.alpha, hl, hl + TC_TILE, tid);
-        convert_operand(raw + TC_TILE, b_kc, 1.f, hl + 2 * TC_TILE, hl + 3 * TC_TILE, tid);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) {
+      }
+    }
+  } else if (warp < 20) {
+    // ---------------------------------------------------------- epilogue
+    const int q = warp & 3, ch = (warp - 12) >> 2;
+    const int row = q * 32 + lane;
+    int t = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+      const WsTile w = ws_tile(tasks, ents, tiles, tile);
+      const bool any = w.e0 < w.e1;
+      const int ab = t & 1;
+      const int cbeg = ch * 64;
+      if (any && !warp_wait(smem_addr(&acc_full[ab]), (uint32_t)((t >> 1) & 1), &abort_flag, lane)) break;
+      if (cbeg >= w.ncols) {
+        // No columns for this warp; still hand the accumulator back.
+        if (any) {
+          if (lane == 0) mbar_arrive(smem_addr(&acc_empty[ab]));
+          t++;
+        }
+        continue;
+      }
+      if (any) asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int cend = min(w.ncols, cbeg + 64);
+      const float beta = w.task.beta;
+      const bool rowok = row < w.mrows;
+      for (int c0 = cbeg; c0 < cend; c0 += 32) {
+        float acc[32];
+        if (any) {
+          uint32_t rr[32];
+          const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * TC_BN + c0);
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+              "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+              : "=r"(rr[0]), "=r"(rr[1]), "=r"(rr[2]), "=r"(rr[3]), "=r"(rr[4]), "=r"(rr[5]), "=r"(rr[6]),
+                "=r"(rr[7]), "=r"(rr[8]), "=r"(rr[9]), "=r"(rr[10]), "=r"(rr[11]), "=r"(rr[12]), "=r"(rr[13]),
+                "=r"(rr[14]), "=r"(rr[15]), "=r"(rr[16]), "=r"(rr[17]), "=r"(rr[18]), "=r"(rr[19]), "=r"(rr[20]),
+                "=r"(rr[21]), "=r"(rr[22]), "=r"(rr[23]), "=r"(rr[24]), "=r"(rr[25]), "=r"(rr[26]), "=r"(rr[27]),
+                "=r"(rr[28]), "=r"(rr[29]), "=r"(rr[30]), "=r"(rr[31])
+              : "r"(taddr));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+          for (int j = 0; j < 32; j++) acc[j] = __uint_as_float(rr[j]);
+          if (c0 + 32 >= cend) {
+            // Last read of this warp: hand the accumulator back.
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_addr(&acc_empty[ab]));
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; j++) acc[j] = 0.f;
+        }
+        if (rowok) {
+          float* cp = w.task.C + (i64)(w.m0 + row) + (i64)(w.n0 + c0) * w.task.ldc;
+          const i64 ldc = w.task.ldc;
+          if (c0 + 32 <= w.ncols && beta == 0.f) {
+#pragma unroll
+            for (int j = 0; j < 32; j++) cp[(i64)j * ldc] = acc[j];
+          } else {
+#pragma unroll
+            for (int j = 0; j < 32; j++) {
+              if (c0 + j < w.ncols) {
+                float* p = cp + (i64)j * ldc;
+                *p = (beta == 0.f) ? acc[j] : beta * (*p) + acc[j];
+              }
+            }
+          }
+        }
+      }
+      if (any) t++;
+    }
+  } else if (lane == 0) {
+    // ------------------------------------------------------- MMA issuer
+    int g = 0, t = 0;
+    bool ok = true;
+    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+      const WsTile w = ws_tile(tasks, ents, tiles, tile);
+      if (w.e0 >= w.e1) continue;
+      const int ab = t & 1;
+      const uint32_t idesc = make_idesc(((w.ncols + 15) / 16) * 16);
+      const uint32_t dacc = tmem + (uint32_t)(ab * TC_BN);
+      if (t >= 2 && !ws_wait(smem_addr(&acc_empty[ab]), (uint32_t)(((t >> 1) - 1) & 1), &abort_flag)) break;
+      bool first = true;
+      for (int e = w.e0; e < w.e1 && ok; e++) {
+        const int K = ents[e].k;
+        if (K <= 0) continue;
+        int enext = e + 1;
+        while (enext < w.e1 && ents[enext].k <= 0) enext++;
+        for (int k0 = 0; k0 < K; k0 += TC_KT) {
+          const int s = g % WS_ST;
+          if (!ws_wait(smem_addr(&conv_full[s]), (uint32_t)((g / WS_ST) & 1), &abort_flag)) {
+            ok = false;
+            break;
+          }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          const uint32_t idesc = make_idesc(nmma);
-          const uint32_t base = smem_addr(hl);
+          const uint32_t base = smem_addr(smem + s * WS_STAGE + 2 * TC_TILE);
+          const uint32_t acol = (uint32_t)(WS_ACOL + s * 32);
 #pragma unroll
           for (int ks = 0; ks < TC_KT / 8; ks++) {
-            uint64_t ad[2], bd[2];
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-              ad[h] = make_desc(base + h * TC_TILE + ks * 256, 128, TC_SBO);
-              bd[h] = make_desc(base + (2 + h) * TC_TILE + ks * 256, 128, TC_SBO);
-            }
-            const uint32_t first = (first_slab && ks == 0) ? 0u : 1u;
+            const uint64_t bh = make_desc(base + ks * 256, 128, TC_SBO);
+            const uint64_t bl = make_desc(base + TC_TILE + ks * 256, 128, TC_SBO);
+            const uint32_t ah = tmem + acol + ks * 8, al = tmem + acol + 16 + ks * 8;
+            const uint32_t accf = (first && ks == 0) ? 0u : 1u;
             if (split) {
-              mma_tf32(tmem, ad[1], bd[0], idesc, first);  // lo x hi
-              mma_tf32(tmem, ad[0], bd[1], idesc, 1u);     // hi x lo
-              mma_tf32(tmem, ad[0], bd[0], idesc, 1u);     // hi x hi
+              mma_tf32_ta(dacc, al, bh, idesc, accf);
+              mma_tf32_ta(dacc, ah, bl, idesc, 1u);
+              mma_tf32_ta(dacc, ah, bh, idesc, 1u);
             } else {
-              mma_tf32(tmem, ad[0], bd[0], idesc, first);  // one TF32 product
+              mma_tf32_ta(dacc, ah, bh, idesc, accf);
             }
           }
-          mma_commit(smem_addr(&bars[hb]));
-        }
-        first_slab = false;
-        more = slab_next(tasks, ents, tiles, ntiles, cons);
-        s++;
-      }
-      if (ok) {
-        // The tile's last slab (s - 1): its MMAs and all earlier ones done.
-        if (tid == 0) wait_ok = mbar_wait(smem_addr(&bars[(s - 1) & 1]), (uint32_t)(((s - 1) >> 1) & 1)) ? 1 : 0;
-        __syncthreads();
-        ok = wait_ok != 0;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    }
-    if (!ok) break;
-
-    // Epilogue: warp w reads TMEM lanes 32 (w & 3) .. +31 (tile rows; a warp
-    // may only read its lane quarter), warps 0-3 columns 0-63 and warps 4-7
-    // columns 64-127, 32 per load; C = beta C + acc, coalesced along the rows
-    // of a column.
-    const int row = (warp & 3) * 32 + lane;
-    for (int c0 = (warp >> 2) * (TC_BN / 2); c0 < (warp >> 2 ? TC_BN : TC_BN / 2); c0 += 32) {
-      if (c0 >= ncols) break;
-      float acc[32];
-      if (any) {
-        uint32_t r[32];
-        const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)c0;
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-            "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-              "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-              "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-            : "r"(taddr));
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-        for (int j = 0; j < 32; j++) acc[j] = __uint_as_float(r[j]);
-      } else {
-#pragma unroll
-        for (int j = 0; j < 32; j++) acc[j] = 0.f;
-      }
-      if (row < mrows) {
-#pragma unroll
-        for (int j = 0; j < 32; j++) {
-          if (c0 + j < ncols) {
-            float* p = task.C + (i64)(m0 + row) + (i64)(n0 + c0 + j) * task.ldc;
-            *p = (task.beta == 0.f) ? acc[j] : task.beta * (*p) + acc[j];
-          }
+          mma_commit(smem_addr(&stage_free[s]));
+          if (enext >= w.e1 && k0 + TC_KT >= K) mma_commit(smem_addr(&acc_full[ab]));
+          first = false;
+          g++;
         }
       }
+      t++;
     }
-    // The next tile's first MMA overwrites the accumulator: every warp's
-    // tcgen05.ld must be complete first.
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // Every MMA this thread issued has completed before TMEM is freed.
+    mma_commit(smem_addr(&drain));
+    mbar_wait(smem_addr(&drain), 0);
   }
-  cp_wait<0>();
-  if (!ok && tid == 0) atomicExch(&g_tc_err, 1);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
+  if (tid == 0 && abort_flag) atomicExch(&g_tc_err, 1);
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BN) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(WS_TMEM_COLS) : "memory");
 }
 
 int tc_gemm_tile() { return TC_BM; }
@@ -472,18 +603,18 @@ int tc_gemm_tile() { return TC_BM; }
 cudaError_t launch_tc_gemm(const GemmTask<float>* d_tasks, const GemmEntry<float>* d_ents, const TileRef* d_tiles,
                            int ntiles, int split, cudaStream_t st) {
   if (ntiles == 0) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+  cudaError_t e = cudaFuncSetAttribute(k_tc_gemm_ws, cudaFuncAttributeMaxDynamicSharedMemorySize, WS_SMEM);
   if (e != cudaSuccess) return e;
-  // Persistent: two CTAs per SM walk the tile list with a stride of the grid.
+  // Persistent: one CTA per SM walks the tile list with a stride of the grid.
   static int sms = 0;
   if (sms == 0) {
     int dev = 0;
     cudaGetDevice(&dev);
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
   }
-  const int grid = ntiles < 2 * sms ? ntiles : 2 * sms;
+  const int grid = ntiles < sms ? ntiles : sms;
   note_launch();
-  k_tc_gemm<<<grid, TC_NT, TC_SMEM, st>>>(d_tasks, d_ents, d_tiles, ntiles, split);
+  k_tc_gemm_ws<<<grid, WS_NT, WS_SMEM, st>>>(d_tasks, d_ents, d_tiles, ntiles, split);
   return cudaGetLastError();
 }
 
