@@ -300,7 +300,7 @@ struct GemmPlan {
   DVec<int2> d_rtiles, d_rtiles_w;  // row tiles of the 128- and 256-row streaming variants
   DVec<T> parts_buf;               // partial results of split tasks
   DVec<SumTask<T>> d_sums;
-  int nsums = 0;
+  int nsums = 0, sum_maxmn = 0;
   double sum_bytes = 0.;
   void add_task(T* C, i64 ldc, int m, int n, T beta) {
     GemmTask<T> t;
@@ -385,14 +385,54 @@ struct GemmPlan {
     double total = 0.;
     for (const auto& t : tasks)
       for (int e = t.e0; e < t.e1; e++) total += (double)t.m * ents[e].k;
-    const double cap = std::max(total / 4096., 65536.);
+    // Plans with fewer row tiles than about four CTAs per SM (the upper
+    // tree levels: U^T x, U y and the ULV substitution blocks of few large
+    // boxes) are latency-bound on the streaming rate of single CTAs: there
+    // an entry longer than a part is first cut along k into entries of a
+    // multiple of 16 columns of A (rows of B; these plans are all NN), so
+    // one-entry tasks spread over several CTAs too.  Larger plans keep
+    // whole entries (partials would only add traffic).
+    double rowtiles = 0.;
+    for (const auto& t : tasks) rowtiles += (t.m + 127) / 128;
+    constexpr double kCtaTarget = 4. * 148.;
+    const bool cut_k = rowtiles < kCtaTarget;
+    const double cap = cut_k ? std::max(total / kCtaTarget, 16384.) : std::max(total / 4096., 65536.);
+    if (cut_k) {
+      std::vector<GemmEntry<T>> cut;
+      cut.reserve(ents.size());
+      for (auto& t : tasks) {
+        const int e0 = (int)cut.size();
+        for (int e = t.e0; e < t.e1; e++) {
+          const GemmEntry<T>& en = ents[e];
+          const int mcta = std::min(t.m, 256);  // rows one CTA streams
+          if (t.m <= 0 || (double)mcta * en.k <= cap || en.opA || en.opB) {
+            cut.push_back(en);
+            continue;
+          }
+          const int kc = std::max(16, (int)(cap / mcta) / 16 * 16);
+          for (int k0 = 0; k0 < en.k; k0 += kc) {
+            GemmEntry<T> piece = en;
+            piece.A = en.A + (i64)k0 * en.lda;
+            piece.B = en.B + k0;
+            piece.k = std::min(kc, en.k - k0);
+            cut.push_back(piece);
+          }
+        }
+        t.e0 = e0;
+        t.e1 = (int)cut.size();
+      }
+      ents.swap(cut);
+    }
     std::vector<GemmTask<T>> out;
     struct Pending { int first; int parts; GemmTask<T> orig; i64 off; };
     std::vector<Pending> pend;
     i64 scratch = 0;
     for (const auto& t : tasks) {
+      // Part weight: A elements one CTA streams (rows capped at a 256-row
+      // tile when entries were cut, else the whole task's rows).
+      const double mw = cut_k ? std::min(t.m, 256) : t.m;
       double w = 0.;
-      for (int e = t.e0; e < t.e1; e++) w += (double)t.m * ents[e].k;
+      for (int e = t.e0; e < t.e1; e++) w += mw * ents[e].k;
       if (w <= cap || t.e1 - t.e0 < 2 || t.m <= 0 || t.n <= 0) {
         out.push_back(t);
         continue;
@@ -407,8 +447,8 @@ struct GemmPlan {
         GemmTask<T> part = t;
         part.e0 = e;
         double wp = 0.;
-        while (e < t.e1 && (wp == 0. || wp + (double)t.m * ents[e].k <= cap)) {
-          wp += (double)t.m * ents[e].k;
+        while (e < t.e1 && (wp == 0. || wp + mw * ents[e].k <= cap)) {
+          wp += mw * ents[e].k;
           e++;
         }
         part.e1 = e;
@@ -436,6 +476,7 @@ struct GemmPlan {
       st_.parts = pd.parts;
       st_.beta = pd.orig.beta;
       sums.push_back(st_);
+      sum_maxmn = std::max(sum_maxmn, (int)mn);
       sum_bytes += (double)(pd.parts + 1) * mn * sizeof(T);
     }
     tasks.swap(out);
@@ -448,7 +489,7 @@ struct GemmPlan {
     if (skinny_nn) {
       ck(launch_skinny_nn<T>(nr, 1, d_tasks.p, d_ents.p, d_rtiles_w.p, (int)d_rtiles_w.n, st), "skinny_nn");
       ck(launch_skinny_nn<T>(nr, 0, d_tasks.p, d_ents.p, d_rtiles.p, (int)d_rtiles.n, st), "skinny_nn");
-      if (nsums) ck(launch_sum_parts<T>(d_sums.p, nsums, st), "sum_parts");
+      if (nsums) ck(launch_sum_parts<T>(d_sums.p, nsums, sum_maxmn, st), "sum_parts");
     } else if (shape == GEMM_TC) {
       if constexpr (std::is_same<T, float>::value)
         ck(launch_tc_gemm(d_tasks.p, d_ents.p, d_tiles.p, ntiles, tc_mode == 1 ? 1 : 0, st), "tc_gemm");

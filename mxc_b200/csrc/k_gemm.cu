@@ -624,29 +624,37 @@ __global__ void __launch_bounds__(BM, BM == 256 ? 3 : 6)
 }
 
 // dst = beta * dst + sum_{p < parts} src_p, the parts of one split task
-// summed in a fixed order (deterministic).
+// summed in a fixed order (deterministic).  blockIdx.y strides over the
+// tasks, blockIdx.x is a chunk of 1024 of a task's m x n elements
+// (column-major).
 template <typename T>
-__global__ void __launch_bounds__(256) k_sum_parts(const SumTask<T>* __restrict__ tasks) {
-  const SumTask<T> t = tasks[blockIdx.x];
-  const i64 mn = (i64)t.m * t.n;
-  for (i64 e = threadIdx.x; e < mn; e += blockDim.x) {
-    const int r = (int)(e % t.m), c = (int)(e / t.m);
-    T s = T(0);
-    for (int p = 0; p < t.parts; p++) s += t.src[(i64)p * mn + e];
-    T* d = t.dst + r + (i64)c * t.ldd;
-    *d = (t.beta == T(0)) ? s : t.beta * (*d) + s;
+__global__ void __launch_bounds__(256) k_sum_parts(const SumTask<T>* __restrict__ tasks, int ntasks) {
+  for (int ti = blockIdx.y; ti < ntasks; ti += gridDim.y) {
+    const SumTask<T> t = tasks[ti];
+    const int mn = t.m * t.n;
+    const int e0 = blockIdx.x * 1024;
+    if (e0 >= mn) continue;
+    const int e1 = min(mn, e0 + 1024);
+    for (int e = e0 + (int)threadIdx.x; e < e1; e += blockDim.x) {
+      const int c = e / t.m, r = e - c * t.m;
+      T s = T(0);
+      for (int p = 0; p < t.parts; p++) s += t.src[(i64)p * mn + e];
+      T* d = t.dst + r + (i64)c * t.ldd;
+      *d = (t.beta == T(0)) ? s : t.beta * (*d) + s;
+    }
   }
 }
 
 template <typename T>
-cudaError_t launch_sum_parts(const SumTask<T>* d_tasks, int ntasks, cudaStream_t st) {
-  if (ntasks == 0) return cudaSuccess;
+cudaError_t launch_sum_parts(const SumTask<T>* d_tasks, int ntasks, int maxmn, cudaStream_t st) {
+  if (ntasks == 0 || maxmn <= 0) return cudaSuccess;
   note_launch();
-  k_sum_parts<T><<<ntasks, 256, 0, st>>>(d_tasks);
+  const dim3 grid((maxmn + 1023) / 1024, ntasks < 65535 ? ntasks : 65535);
+  k_sum_parts<T><<<grid, 256, 0, st>>>(d_tasks, ntasks);
   return cudaGetLastError();
 }
-template cudaError_t launch_sum_parts<double>(const SumTask<double>*, int, cudaStream_t);
-template cudaError_t launch_sum_parts<float>(const SumTask<float>*, int, cudaStream_t);
+template cudaError_t launch_sum_parts<double>(const SumTask<double>*, int, int, cudaStream_t);
+template cudaError_t launch_sum_parts<float>(const SumTask<float>*, int, int, cudaStream_t);
 
 }  // namespace h2b
 

@@ -129,7 +129,7 @@ struct SumTask {
   T beta;
 };
 template <typename T>
-cudaError_t launch_sum_parts(const SumTask<T>* d_tasks, int ntasks, cudaStream_t st);
+cudaError_t launch_sum_parts(const SumTask<T>* d_tasks, int ntasks, int maxmn, cudaStream_t st);
 int gemm_tile_n(int shape);
 // FP32 segmented GEMM on the tcgen05 tensor cores, 128 x 128 output tiles
 // (TileRef over tc_gemm_tile()-sized tiles); split = 1: 3-term TF32 split
