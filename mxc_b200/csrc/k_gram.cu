@@ -5,9 +5,9 @@
 // Only the upper-triangle 64 x 64 tiles of each G are computed; each
 // off-diagonal tile is also written transposed.  One CTA (4 warps, each a
 // 32 x 32 quadrant as 4 x 4 m8n8k4 fragments) owns one tile.  The k (sample)
-// dimension is streamed in 32-row slabs through a 3-slot cp.async ring: the
+// dimension is streamed in 16-row slabs through a 3-slot cp.async ring: the
 // slab holds the tile's 64 (diagonal tile) or 128 columns of X, each column
-// 32 consecutive samples padded to 36 doubles so the fragment loads of a
+// 16 consecutive samples padded to 20 doubles so the fragment loads of a
 // half-warp (4 columns x 4 samples) hit 16 distinct bank pairs.
 #include "common.cuh"
 #include "kernels.h"
@@ -18,7 +18,8 @@ namespace h2b {
 
 namespace {
 
-constexpr int GR_T = 64, GR_KS = 32, GR_CS = 36, GR_ST = 3, GR_NT = 128;
+constexpr int GR_T = 64, GR_KS = 16, GR_CS = GR_KS + 4, GR_ST = 3, GR_NT = 128;
+constexpr int GR_KP = GR_KS / 2;  // 16-byte pairs per staged column
 constexpr int GR_SLOT = 2 * GR_T * GR_CS;  // doubles per ring slot (128 columns)
 constexpr int GR_SMEM = GR_ST * GR_SLOT * 8;
 
@@ -44,7 +45,7 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
 
 }  // namespace
 
-__global__ void __launch_bounds__(GR_NT, 2) k_gram(const GramTask* __restrict__ tasks, const int4* __restrict__ tiles) {
+__global__ void __launch_bounds__(GR_NT, 3) k_gram(const GramTask* __restrict__ tasks, const int4* __restrict__ tiles) {
   extern __shared__ __align__(16) double gsm[];
   const int4 tl = tiles[blockIdx.x];  // {task, tile row, tile col}
   const GramTask t = tasks[tl.x];
@@ -56,14 +57,14 @@ __global__ void __launch_bounds__(GR_NT, 2) k_gram(const GramTask* __restrict__ 
   const bool vec = ((reinterpret_cast<uintptr_t>(t.X) & 15) == 0) && (t.ld % 2 == 0);
   const int nslab = (t.S + GR_KS - 1) / GR_KS;
 
-  // Copies slab `sl` (samples sl*32 .. +31) into ring slot `slot`: staged
+  // Copies slab `sl` (samples sl*16 .. +15) into ring slot `slot`: staged
   // column j < 64 is X column c0 + j, column 64 + j is X column c1 + j.
   auto produce = [&](int sl, int slot) {
     if (sl < nslab) {
       double* dst = gsm + (size_t)slot * GR_SLOT;
       const int k0 = sl * GR_KS;
-      for (int c = tid; c < ncol * (GR_KS / 2); c += GR_NT) {
-        const int j = c >> 4, kk = (c & 15) * 2;
+      for (int c = tid; c < ncol * GR_KP; c += GR_NT) {
+        const int j = c / GR_KP, kk = (c % GR_KP) * 2;
         const int col = j < GR_T ? c0 + j : c1 + (j - GR_T);
         const int k = k0 + kk;
         int nk = t.S - k;
@@ -149,15 +150,16 @@ namespace h2b {
 // Segmented FP64 GEMM on the FP64 tensor cores: C_task = beta C_task + sum_e
 // alpha_e op(A_e) op(B_e) over 64 x 64 output tiles (the FP64 plans of the
 // factorization and basis completion).  Same ring and fragments as k_gram;
-// each operand slab (32 k) is staged in the orientation it has in memory:
-// k contiguous -> [row][36] (rows of 32 k, padded), rows contiguous ->
+// each operand slab (16 k) is staged in the orientation it has in memory:
+// k contiguous -> [row][20] (rows of 16 k, padded), rows contiguous ->
 // [k][68] (k-rows of 64 rows, padded), so every cp.async is a 16-byte
 // vector of consecutive elements and every fragment load of a half-warp hits
 // 16 distinct bank pairs.
 namespace {
 
-constexpr int DG_T = 64, DG_KS = 32, DG_ST = 3, DG_NT = 128;
-constexpr int DG_RK = 36;  // [row][k] stride (doubles)
+constexpr int DG_T = 64, DG_KS = 16, DG_ST = 3, DG_NT = 128;
+constexpr int DG_KP = DG_KS / 2;  // 16-byte pairs per k-contiguous row
+constexpr int DG_RK = DG_KS + 4;  // [row][k] stride (doubles)
 constexpr int DG_KR = 68;  // [k][row] stride (doubles)
 constexpr int DG_OP = DG_T * DG_RK > DG_KS * DG_KR ? DG_T * DG_RK : DG_KS * DG_KR;  // doubles per operand
 constexpr int DG_SMEM = DG_ST * 2 * DG_OP * 8;
@@ -172,8 +174,8 @@ struct DgOperand {
 
 __device__ __forceinline__ void dg_issue(const DgOperand& o, double* dst, int tid) {
   if (o.kcontig) {
-    for (int c = tid; c < DG_T * (DG_KS / 2); c += DG_NT) {
-      const int r = c >> 4, kk = (c & 15) * 2;
+    for (int c = tid; c < DG_T * DG_KP; c += DG_NT) {
+      const int r = c / DG_KP, kk = (c % DG_KP) * 2;
       const int k = o.k0 + kk;
       int nk = o.K - k;
       nk = nk < 0 ? 0 : (nk > 2 ? 2 : nk);
@@ -208,7 +210,7 @@ __device__ __forceinline__ void dg_issue(const DgOperand& o, double* dst, int ti
 
 }  // namespace
 
-__global__ void __launch_bounds__(DG_NT, 2) k_dgemm(const GemmTask<double>* __restrict__ tasks,
+__global__ void __launch_bounds__(DG_NT, 3) k_dgemm(const GemmTask<double>* __restrict__ tasks,
                                                    const GemmEntry<double>* __restrict__ ents,
                                                    const TileRef* __restrict__ tiles) {
   extern __shared__ __align__(16) double dsm[];
