@@ -466,12 +466,11 @@ constexpr size_t stream_tf32_smem() {
   return sizeof(float) * (size_t)SF_ST * SF_KS * ((BM + 8) + (NR + 8));
 }
 
+// hi: x as stored (the tensor core reads a TF32 operand from an FP32
+// container by ignoring its 13 low mantissa bits); lo = x - trunc(x), exact.
 __device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
-  uint32_t h;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
-  h &= 0xFFFFE000u;
-  hi = h;
-  lo = __float_as_uint(x - __uint_as_float(h));
+  hi = __float_as_uint(x);
+  lo = __float_as_uint(x - __uint_as_float(hi & 0xFFFFE000u));
 }
 
 __device__ __forceinline__ void mma_tf32_16x8x8(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {

@@ -96,6 +96,32 @@ def test_fp32_simt_gemm_same_bound(handle, case):
     assert worst < 1e-5, worst
 
 
+# Outputs of at most 16 columns with A and B as stored go to the streaming
+# kernels of the block-sparse applies (FP32: TF32 mma.sync with the split in
+# registers; FP64: mma.sync m8n8k4), rows in 128- and 256-row tiles; long
+# single entries are cut along k and their partials summed in order.
+SKINNY = [
+    # batch, nterms, m, n, k, opA, opB, alpha, beta, lda, ldb, ldc
+    (3, 1, 256, 16, 256, 0, 0, 1.0, 0.0, 256, 256, 256),
+    (2, 3, 300, 16, 200, 0, 0, -1.0, 1.0, 301, 203, 300),
+    (4, 2, 130, 8, 77, 0, 0, 0.5, 2.0, 131, 77, 130),
+    (2, 1, 700, 16, 900, 0, 0, 1.0, 1.0, 700, 900, 701),
+    (2, 1, 45, 3, 33, 0, 0, 1.0, 0.0, 45, 33, 45),
+]
+
+
+@pytest.mark.parametrize("case", SKINNY, ids=[str(i) for i in range(len(SKINNY))])
+def test_fp32_streaming_apply_keeps_fp32_accuracy(handle, case):
+    worst = _run(handle, _lib.FP32, *case, seed=11)
+    assert worst < 1e-5, worst
+
+
+@pytest.mark.parametrize("case", SKINNY, ids=[str(i) for i in range(len(SKINNY))])
+def test_fp64_streaming_apply(handle, case):
+    worst = _run(handle, _lib.FP64, *case, seed=12)
+    assert worst < 1e-14, worst
+
+
 @pytest.mark.parametrize("case", CASES, ids=[str(i) for i in range(len(CASES))])
 def test_fp64_tensor_core_gemm(handle, case):
     worst = _run(handle, _lib.FP64, *case, seed=9)
