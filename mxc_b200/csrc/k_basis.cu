@@ -318,20 +318,22 @@ __global__ void __launch_bounds__(256) k_basis_finish(
     return;
   }
   // T = R11^{-1} R12 in place (rows 0..rank-1, columns rank..M-1), by
-  // column chunks staged in shared memory: back substitution with the whole
-  // CTA updating the rows above the current one (one barrier per row).
+  // column chunks staged in shared memory (as many columns as fit, so
+  // usually one chunk): back substitution with the whole CTA updating the
+  // rows above the current one (one barrier per row, one reciprocal of the
+  // pivot per row).
   {
     T* X = taus + M;  // rank x nc, row-major
-    const int nc = min(32, xcap / rank);
+    const int nc = max(1, min(M - rank, xcap / rank));
     for (int c0 = rank; c0 < M; c0 += nc) {
       const int w = min(nc, M - c0);
       for (int e = tid; e < rank * w; e += nt) X[e] = W[(i64)(e / w) * M + c0 + e % w];
       __syncthreads();
       for (int i = rank - 1; i >= 0; i--) {
-        const T rii = W[(i64)i * M + i];
-        for (int e = tid; e < i * w; e += nt) {
-          const int k = e / w, c = e % w;
-          X[e] -= W[(i64)k * M + i] * (X[i * w + c] / rii);
+        const T inv = T(1) / W[(i64)i * M + i];
+        for (int k = warp; k < i; k += nw) {  // warp: row k, lanes: columns
+          const T wki = W[(i64)k * M + i] * inv;
+          for (int c = lane; c < w; c += 32) X[k * w + c] -= wki * X[i * w + c];
         }
         __syncthreads();
       }
@@ -493,8 +495,9 @@ cudaError_t launch_basis_finish(const i64* dims, const i64* krows, T* Rws, T* Q,
                                 double* pts, i64* ranks, double epi, int orth, int qin_identity, int nboxes,
                                 int maxM, cudaStream_t st, T* wy_taus) {
   if (nboxes == 0) return cudaSuccess;
-  // Back-substitution chunk: up to 32 columns of rank rows, at most 96 KB.
-  const int xcap = (int)std::min<size_t>((size_t)maxM * 32, 96 * 1024 / sizeof(T));
+  // Back-substitution chunk: columns of rank rows, at most 96 KB (all
+  // M - rank columns of a 256-box at rank >= 64 in FP64).
+  const int xcap = (int)std::min<size_t>((size_t)maxM * maxM, 96 * 1024 / sizeof(T));
   size_t smem = ((4 * (size_t)maxM + 15) / 16) * 16 + sizeof(double) * 3 * maxM + sizeof(T) * (maxM + xcap) + 64;
   auto fn = k_basis_finish<T>;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
