@@ -7,21 +7,45 @@
 namespace h2b {
 
 // Column-major blocks K(bi[r], bj[c]); grid.x = task, grid.y = chunk of
-// the block's elements.  Consecutive threads write consecutive rows.
+// the block's elements.  Consecutive threads write consecutive rows; a
+// thread finds its first (row, column) by one 32-bit division and then
+// steps by the block size without dividing (blocks hold < 2^31 elements;
+// larger ones take the 64-bit path).
 template <typename T, bool FAST>
 __global__ void __launch_bounds__(256) k_gen_blocks(KernelParams kp, const GenTask* __restrict__ tasks, T* __restrict__ out) {
-  GenTask t = tasks[blockIdx.x];
-  i64 total = (i64)t.m * t.n;
+  const GenTask t = tasks[blockIdx.x];
+  const i64 total = (i64)t.m * t.n;
   if (total == 0) return;
-  i64 per = (total + gridDim.y - 1) / gridDim.y;
-  i64 e0 = per * blockIdx.y, e1 = e0 + per < total ? e0 + per : total;
+  const i64 per = (total + gridDim.y - 1) / gridDim.y;
+  const i64 e0 = per * blockIdx.y, e1 = e0 + per < total ? e0 + per : total;
   T* o = out + t.out_off;
-  for (i64 e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-    int r = (int)(e % t.m), c = (int)(e / t.m);
+  auto value = [&](int r, int c) {
     const double* a = t.bi + 3 * r;
     const double* b = t.bj + 3 * c;
-    o[r + (i64)c * t.ld] = FAST ? (T)kernel_fast(kp, a[0] - b[0], a[1] - b[1], a[2] - b[2])
-                                : (T)kernel_exact(kp, a[0] - b[0], a[1] - b[1], a[2] - b[2]);
+    return FAST ? (T)kernel_fast(kp, a[0] - b[0], a[1] - b[1], a[2] - b[2])
+                : (T)kernel_exact(kp, a[0] - b[0], a[1] - b[1], a[2] - b[2]);
+  };
+  if (total < ((i64)1 << 31)) {
+    const int m = t.m, stride = (int)blockDim.x;
+    const int dq = stride / m, dr = stride - dq * m;
+    int e = (int)e0 + (int)threadIdx.x;
+    const int end = (int)e1;
+    if (e >= end) return;
+    int c = e / m, r = e - c * m;
+    for (; e < end; e += stride) {
+      o[r + (i64)c * t.ld] = value(r, c);
+      r += dr;
+      c += dq;
+      if (r >= m) {
+        r -= m;
+        c++;
+      }
+    }
+    return;
+  }
+  for (i64 e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    const int r = (int)(e % t.m), c = (int)(e / t.m);
+    o[r + (i64)c * t.ld] = value(r, c);
   }
 }
 
