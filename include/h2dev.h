@@ -178,7 +178,10 @@ enum { H2DEV_EXPORT_S = 0, H2DEV_EXPORT_Q = 1, H2DEV_EXPORT_R = 2, H2DEV_EXPORT_
 int h2dev_solver_export_size(h2dev_solver_t s, int64_t level, int what, int64_t* count);
 /* Copies one level's container (S: skeleton-ordered bodies, Q, R (V after
  * factorize, stored transposed), A near blocks, C couplings) in box /
- * block order, each block column-major, converted to double. */
+ * block order, each block column-major, converted to double.  After
+ * factorize, the redundant x redundant part of an off-diagonal near block
+ * keeps its pre-transform values: the factorization never forms it (the
+ * reference drops that fill and never reads it). */
 int h2dev_solver_export(h2dev_solver_t s, int64_t level, int what, double* out);
 
 /* ---- instrumentation (CUDA events on the handle's stream) ------------ */

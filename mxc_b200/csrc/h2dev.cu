@@ -1555,8 +1555,19 @@ class Solver : public SolverBase {
           T* Aij = A + lv.aoff[k];
           a.add_task(T2.p + o, Mi, Mi, Nj, T(0));
           a.add_entry(Aij, Mi, 0, Q + lv.qoff[j], Nj, 0, Nj, T(1));
-          b.add_task(Aij, Mi, Mi, Nj, T(0));
-          b.add_entry(V + lv.qoff[i], Mi, 1, T2.p + o, Mi, 0, Mi, T(1));
+          // Only the skeleton rows (ss, sr) and the rs block are formed: the
+          // redundant-redundant block of an off-diagonal A_ij is never read
+          // afterwards (Schur updates read ss / sr / rs, the substitution sr
+          // and rs, the parent level ss), as the reference ULV drops that fill.
+          const int Ms = (int)Rk[i], Ns = (int)Rk[j];
+          if (Ms > 0) {
+            b.add_task(Aij, Mi, Ms, Nj, T(0));
+            b.add_entry(V + lv.qoff[i], Mi, 1, T2.p + o, Mi, 0, Mi, T(1));
+          }
+          if (Mi > Ms && Ns > 0) {
+            b.add_task(Aij + Ms, Mi, Mi - Ms, Ns, T(0));
+            b.add_entry(V + lv.qoff[i] + (i64)Ms * Mi, Mi, 1, T2.p + o, Mi, 0, Mi, T(1));
+          }
           o += (i64)Mi * Nj;
         }
         a.name = b.name = "gemm_factor";
