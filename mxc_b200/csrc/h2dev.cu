@@ -34,18 +34,21 @@ struct CurHandle {
 struct Prof {
   h2dev_handle_s* h;
   ProfRec r;
-  Prof(const char* name, double flops, double bytes) : h(g_cur && g_cur->prof ? g_cur : nullptr) {
+  cudaStream_t s = nullptr;
+  Prof(const char* name, double flops, double bytes, cudaStream_t on = nullptr)
+      : h(g_cur && g_cur->prof ? g_cur : nullptr) {
     if (!h) return;
+    s = on ? on : h->stream;
     r.name = name;
     r.flops = flops;
     r.bytes = bytes;
     r.a = h->take();
     r.b = h->take();
-    cudaEventRecord(r.a, h->stream);
+    cudaEventRecord(r.a, s);
   }
   ~Prof() {
     if (!h) return;
-    cudaEventRecord(r.b, h->stream);
+    cudaEventRecord(r.b, s);
     h->recs.push_back(r);
   }
 };
@@ -485,7 +488,7 @@ struct GemmPlan {
   }
 
   void run(cudaStream_t st) const {
-    Prof p(name, flops, bytes);
+    Prof p(name, flops, bytes, st);
     if (skinny_nn) {
       ck(launch_skinny_nn<T>(nr, 1, d_tasks.p, d_ents.p, d_rtiles_w.p, (int)d_rtiles_w.n, st), "skinny_nn");
       ck(launch_skinny_nn<T>(nr, 0, d_tasks.p, d_ents.p, d_rtiles.p, (int)d_rtiles.n, st), "skinny_nn");
@@ -619,7 +622,7 @@ class Solver : public SolverBase {
   // per-nrhs state
   i64 cur_nrhs = -1;
   DVec<T> vin, vout;
-  GemmPlan<T> mv_leaf, mv_far;
+  GemmPlan<T> mv_leaf, mv_far, mv_qw;  // leaf: near field (A_ij x_j); qw: + U W at the leaves
   std::vector<GemmPlan<T>> mv_up, mv_down;
   std::vector<GemmPlan<T>> pc_fx, pc_fz, pc_bx, pc_by;
   std::vector<CopyPlan<T>> pc_fcopy, pc_bcopy;
@@ -1364,16 +1367,21 @@ class Solver : public SolverBase {
       GemmPlan<T>& g = mv_leaf;
       g = GemmPlan<T>();
       g.name = "gemm_matvec_near";
+      GemmPlan<T>& q = mv_qw;
+      q = GemmPlan<T>();
+      q.name = "gemm_matvec_down";
       for (i64 i = 0; i < lv.nodes; i++) {
         int M = (int)lv.dims[i], r = (int)lv.ranks[i];
         g.add_task(vout.p + lv.xoff[i], lv.lenX, M, nr, T(0));
-        g.add_entry(lv.Q.p + lv.qoff[i], M, 0, lv.vW.p + lv.zoff[i], lv.lenZ, 0, r, T(1));
         for (i64 k = lv.arow[i]; k < lv.arow[i + 1]; k++) {
           i64 j = lv.acol[k];
           g.add_entry(lv.A.p + lv.aoff[k], M, 0, vin.p + lv.xoff[j], lv.lenX, 0, (int)lv.dims[j], T(1));
         }
+        q.add_task(vout.p + lv.xoff[i], lv.lenX, M, nr, T(1));
+        q.add_entry(lv.Q.p + lv.qoff[i], M, 0, lv.vW.p + lv.zoff[i], lv.lenZ, 0, r, T(1));
       }
       g.finalize();
+      q.finalize();
     }
     mv_built = true;
   }
@@ -1400,10 +1408,28 @@ class Solver : public SolverBase {
     ensure_vectors(nrhs);
     if (!mv_built) build_matvec(nrhs);
     stage_in(nrhs, dX, ldx);
+    // The near field (reads the input, writes the output) does not depend on
+    // the upward / far / downward chain: it runs on the side stream while the
+    // chain's small upper-level launches run on the main one (serialised
+    // while per-launch profiling is on, so each launch is timed alone).
+    // The leaf U W term is added after both, so the result does not depend
+    // on the overlap.
+    const bool fork = h->stream2 && !h->prof;
+    if (fork) {
+      ck(cudaEventRecord(h->ev_fork, st()), "fork");
+      ck(cudaStreamWaitEvent(h->stream2, h->ev_fork, 0), "fork");
+      mv_leaf.run(h->stream2);
+      ck(cudaEventRecord(h->ev_join, h->stream2), "join");
+    }
     for (i64 l = levels; l >= 0; l--) mv_up[l].run(st());
     mv_far.run(st());
     for (i64 l = 0; l < levels; l++) mv_down[l].run(st());
-    mv_leaf.run(st());
+    if (fork) {
+      ck(cudaStreamWaitEvent(st(), h->ev_join, 0), "join");
+    } else {
+      mv_leaf.run(st());
+    }
+    mv_qw.run(st());
     stage_out(nrhs, dX, ldx);
   }
 
@@ -2087,8 +2113,16 @@ int h2dev_handle_create(int device, h2dev_handle_t* out) {
   ck(cudaSetDevice(device), "cudaSetDevice");
   auto* h = new h2dev_handle_s();
   h->device = device;
-  cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  int least = 0, greatest = 0;
+  ck(cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priority range");
+  cudaError_t e = cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking, greatest);
+  if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&h->stream2, cudaStreamNonBlocking, least);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming);
   if (e != cudaSuccess) {
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->stream2) cudaStreamDestroy(h->stream2);
+    if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     ck(e, "cudaStreamCreate");
   }
@@ -2108,6 +2142,10 @@ static void handle_release(h2dev_handle_s* h) {
   if (h->t0) cudaEventDestroy(h->t0);
   if (h->t1) cudaEventDestroy(h->t1);
   cache_trim(h);
+  cudaStreamSynchronize(h->stream2);
+  cudaEventDestroy(h->ev_fork);
+  cudaEventDestroy(h->ev_join);
+  cudaStreamDestroy(h->stream2);
   cudaStreamDestroy(h->stream);
   delete h;
 }

@@ -23,6 +23,14 @@ struct ProfRec {
 struct h2dev_handle_s {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // Side stream (lowest priority; `stream` has the highest) for work that is
+  // independent of the main chain inside one call: the near-field apply of
+  // an H^2 matvec runs there while the latency-bound upward / far / downward
+  // passes run on `stream`.  Every fork (ev_fork) is joined back into
+  // `stream` (ev_join) before the call returns, so all memory and cache
+  // ordering stays that of `stream`.
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool prof = false;
   int sampling_mode = 0;  // far-list cap rule for solvers created next (H2DEV_OPT_SAMPLING)
   int basis_mode = 0;  // 0: Gram + pivoted Cholesky for fixed-rank bases; 1: Householder TSQR everywhere
