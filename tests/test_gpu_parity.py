@@ -115,6 +115,27 @@ def test_operator_matvec_multi_rhs(op2048):
         assert rel(Y[:, c], y1) < 1e-14
 
 
+def test_operator_matvec_overlap_is_bitwise_serial(op2048, handle):
+    """The near field runs on a side stream, overlapping the upward / far /
+    downward passes; with per-launch profiling on, the same plans run one
+    after another on the main stream.  Same plans, same summation order:
+    the results are identical bit for bit (16 right-hand sides, the
+    tensor-core streaming path)."""
+    A, Ao, b, t, cells, L = op2048
+    N = b.shape[0]
+    X = np.asfortranarray(np.random.default_rng(5).random((N, 16)))
+    Y1 = X.copy(order="F")
+    A.matVecMul(Y1)
+    handle.profile(True)
+    try:
+        Y2 = X.copy(order="F")
+        A.matVecMul(Y2)
+    finally:
+        handle.profile(False)
+    assert np.array_equal(Y1, Y2)
+    assert rel(Y1[:, 0], m.dense_matvec(handle, m.Laplace3D(), b, X[:, 0].copy())) < 1e-10
+
+
 # ---------------------------------------------------------------- preconditioner
 
 @pytest.fixture(scope="module")
