@@ -156,7 +156,7 @@ __device__ __forceinline__ void convert_operand(const unsigned char* raw, int kc
 // Set when an mbarrier wait expired (read and cleared by the host).
 __device__ int g_tc_err = 0;
 
-// Warp-specialised variant, one CTA per SM (21 warps, 512 TMEM columns),
+// Warp-specialised variant, one CTA per SM (25 warps, 512 TMEM columns),
 // A operand in tensor memory, double-buffered accumulator.
 //
 // The tensor core reads a TF32 operand from a 32-bit container by ignoring
@@ -171,16 +171,16 @@ __device__ int g_tc_err = 0;
 //
 // Stage ring (WS_ST stages of 32 KB: A raw, B raw, B hi, B lo; TMEM A
 // buffer of 32 columns per stage at 256 + 32 s):
-//  warps 0-3   producers: wait stage_free (the MMAs of the stage's previous
+//  warps 0-7   producers: wait stage_free (the MMAs of the stage's previous
 //              slab done), cp.async the slab, cp.async.mbarrier.arrive on
 //              full.
-//  warps 4-11  converters: wait full; warp w writes A rows 32 (w & 3) ..
-//              +31, k 8 h .. +7 (h = (w - 4) >> 2) to TMEM and its share of
+//  warps 8-15  converters: wait full; warp w writes A rows 32 (w & 3) ..
+//              +31, k 8 h .. +7 (h = (w - 8) >> 2) to TMEM and its share of
 //              B lo; signal conv_full.
-//  warps 12-19 epilogue: wait acc_full, read TMEM lane quarter w & 3,
-//              columns 64 ((w - 12) >> 2) .. +63, release the accumulator
+//  warps 16-23 epilogue: wait acc_full, read TMEM lane quarter w & 3,
+//              columns 64 ((w - 16) >> 2) .. +63, release the accumulator
 //              (acc_empty), write C.
-//  warp 20     one thread: wait conv_full (and, before a tile's first slab,
+//  warp 24     one thread: wait conv_full (and, before a tile's first slab,
 //              acc_empty of its accumulator), issue the slab's MMAs, commit
 //              to stage_free and, after a tile's last slab, to acc_full.
 // Every wait is bounded; an expired wait sets a CTA-wide abort flag that
@@ -188,7 +188,9 @@ __device__ int g_tc_err = 0;
 // warp-collective instructions stay convergent; no named barrier is used
 // inside the loops.
 namespace {
-constexpr int WS_NT = 672;
+constexpr int WS_NT = 800;
+constexpr int WS_NP = 256;             // producer threads (warps 0-7)
+constexpr int WS_PCH = 512 / WS_NP;    // 16-byte chunks per operand tile per producer thread
 constexpr int WS_ST = 6;
 constexpr int WS_STAGE = 4 * TC_TILE;  // A raw, B raw, B hi, B lo
 constexpr int WS_SMEM = WS_ST * WS_STAGE;
@@ -270,19 +272,19 @@ __device__ __forceinline__ WsTile ws_tile(const GemmTask<float>* tasks, const Ge
   return w;
 }
 
-// A producer thread's four 16-byte chunks of one operand tile (the chunks
-// c = ptid + 128 j of the tile's 512), resolved once per entry: per slab only
-// the k offset changes.  k contiguous: chunk j is row (ptid >> 2) + 32 j,
-// k-chunk ptid & 3, stored in the raw layout or, with kmajor, directly in
-// the canonical K-major layout; rows contiguous: chunk j is row quad
-// ptid & 31 of k-row (ptid >> 5) + 4 j (raw layout).
+// A producer thread's 16-byte chunks of one operand tile (the chunks
+// c = ptid + WS_NP j of the tile's 512), resolved once per entry: per slab
+// only the k offset changes.  k contiguous: chunk c is row c >> 2, k-chunk
+// c & 3, stored in the raw layout or, with kmajor, directly in the
+// canonical K-major layout; rows contiguous: chunk c is row quad c & 31 of
+// k-row c >> 5 (raw layout).
 struct ProdChunks {
   const float* X;
-  const float* src[4];  // element (row, k = k0 + kofs) at src + k0 * kstep
-  uint32_t dst[4];
+  const float* src[WS_PCH];  // element (row, k = k0 + kofs) at src + k0 * kstep
+  uint32_t dst[WS_PCH];
   i64 kstep;
-  int kofs[4];
-  int nrow[4];  // k contiguous: 4 if the row is in the tile else 0; rows contiguous: valid rows of the quad
+  int kofs[WS_PCH];
+  int nrow[WS_PCH];  // k contiguous: 4 if the row is in the tile else 0; rows contiguous: valid rows of the quad
   int kcontig, vec, K;
 };
 
@@ -293,15 +295,16 @@ __device__ __forceinline__ void prod_prepare(ProdChunks& pc, const float* X, i64
   pc.kcontig = kcontig;
   pc.vec = ((reinterpret_cast<uintptr_t>(X) & 15) == 0) && (ld % 4 == 0);
 #pragma unroll
-  for (int j = 0; j < 4; j++) {
+  for (int j = 0; j < WS_PCH; j++) {
+    const int c = ptid + WS_NP * j;
     if (kcontig) {
-      const int r = (ptid >> 2) + 32 * j, kc = ptid & 3;
+      const int r = c >> 2, kc = c & 3;
       pc.kofs[j] = 4 * kc;
       pc.nrow[j] = r < rows ? 4 : 0;
       pc.src[j] = X + (i64)(r0 + r) * ld + 4 * kc;
       pc.dst[j] = base + (kmajor ? off_kmajor(r, kc) : raw_kc(r, kc));
     } else {
-      const int q = ptid & 31, k = (ptid >> 5) + 4 * j;
+      const int q = c & 31, k = c >> 5;
       int nr = rows - 4 * q;
       pc.kofs[j] = k;
       pc.nrow[j] = nr < 0 ? 0 : (nr > 4 ? 4 : nr);
@@ -312,10 +315,10 @@ __device__ __forceinline__ void prod_prepare(ProdChunks& pc, const float* X, i64
   pc.kstep = kcontig ? 1 : ld;
 }
 
-// Issues the four chunks of the slab at k0 into stage offset `stage_off`.
+// Issues the thread's chunks of the slab at k0 into stage offset `stage_off`.
 __device__ __forceinline__ void prod_issue(const ProdChunks& pc, int k0, uint32_t stage_off) {
 #pragma unroll
-  for (int j = 0; j < 4; j++) {
+  for (int j = 0; j < WS_PCH; j++) {
     const int k = k0 + pc.kofs[j];
     int n;
     if (pc.kcontig) {
@@ -348,7 +351,7 @@ __global__ void __launch_bounds__(WS_NT, 1)
 
   if (tid == 0) {
     for (int s = 0; s < WS_ST; s++) {
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 128;" ::"r"(smem_addr(&full[s])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&full[s])), "r"(WS_NP) : "memory");
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 8;" ::"r"(smem_addr(&conv_full[s])) : "memory");
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&stage_free[s])) : "memory");
     }
@@ -371,7 +374,7 @@ __global__ void __launch_bounds__(WS_NT, 1)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_slot;
 
-  if (warp < 4) {
+  if (warp < 8) {
     // ---------------------------------------------------------- producers
     int g = 0;
     bool ok = true;
@@ -399,10 +402,10 @@ __global__ void __launch_bounds__(WS_NT, 1)
       }
     }
     cp_wait<0>();
-  } else if (warp < 12) {
+  } else if (warp < 16) {
     // --------------------------------------------------------- converters
-    const int ctid = tid - 128;
-    const int q = warp & 3, kh = (warp - 4) >> 2;
+    const int ctid = tid - WS_NP;
+    const int q = warp & 3, kh = (warp - 8) >> 2;
     const int r = q * 32 + lane;  // A row (TMEM lane) of this thread
     const uint32_t tmem_row = tmem + ((uint32_t)(q * 32) << 16);
     int g = 0;
@@ -470,9 +473,9 @@ __global__ void __launch_bounds__(WS_NT, 1)
         }
       }
     }
-  } else if (warp < 20) {
+  } else if (warp < 24) {
     // ---------------------------------------------------------- epilogue
-    const int q = warp & 3, ch = (warp - 12) >> 2;
+    const int q = warp & 3, ch = (warp - 16) >> 2;
     const int row = q * 32 + lane;
     int t = 0;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
