@@ -112,14 +112,55 @@ template cudaError_t launch_seg_gemm<double>(int, const GemmTask<double>*, const
 template cudaError_t launch_seg_gemm<float>(int, const GemmTask<float>*, const GemmEntry<float>*, const TileRef*, int,
                                             cudaStream_t);
 
+// One CTA per entry: dst (m x n, ld ldd) = src or src^T (ld lds).  Plain
+// copies walk the elements column by column (consecutive threads on
+// consecutive rows, one division per thread, none per element); transposed
+// copies go through 32 x 32 shared-memory tiles so that both the reads of
+// src and the writes of dst are coalesced.
 template <typename T>
 __global__ void __launch_bounds__(256) k_batched_copy(const CopyEntry<T>* __restrict__ ents) {
   const CopyEntry<T> e = ents[blockIdx.x];
-  i64 total = (i64)e.m * e.n;
-  for (i64 x = threadIdx.x; x < total; x += blockDim.x) {
-    int r = (int)(x % e.m), c = (int)(x / e.m);
-    e.dst[r + (i64)c * e.ldd] = e.trans ? e.src[c + (i64)r * e.lds] : e.src[r + (i64)c * e.lds];
+  const int m = e.m, n = e.n;
+  if (m <= 0 || n <= 0) return;
+  if (!e.trans) {
+    if ((i64)m * n < ((i64)1 << 31)) {
+      const int stride = (int)blockDim.x, dq = stride / m, dr = stride - dq * m, total = m * n;
+      int x = (int)threadIdx.x;
+      int c = x / m, r = x - c * m;
+      for (; x < total; x += stride) {
+        e.dst[r + (i64)c * e.ldd] = e.src[r + (i64)c * e.lds];
+        r += dr;
+        c += dq;
+        if (r >= m) {
+          r -= m;
+          c++;
+        }
+      }
+    } else {
+      for (i64 x = threadIdx.x; x < (i64)m * n; x += blockDim.x) {
+        const int r = (int)(x % m), c = (int)(x / m);
+        e.dst[r + (i64)c * e.ldd] = e.src[r + (i64)c * e.lds];
+      }
+    }
+    return;
   }
+  // dst(r, c) = src(c, r): the tile at dst rows r0.., columns c0.. is the
+  // tile at src rows c0.., columns r0...
+  __shared__ T tile[32][33];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 8 rows of 32 per pass
+  for (int c0 = 0; c0 < n; c0 += 32)
+    for (int r0 = 0; r0 < m; r0 += 32) {
+      for (int i = ty; i < 32; i += 8) {
+        const int sr = c0 + tx, sc = r0 + i;  // src(sr, sc) = dst(sc, sr)
+        tile[i][tx] = (sr < n && sc < m) ? e.src[sr + (i64)sc * e.lds] : T(0);
+      }
+      __syncthreads();
+      for (int i = ty; i < 32; i += 8) {
+        const int dr = r0 + tx, dc = c0 + i;
+        if (dr < m && dc < n) e.dst[dr + (i64)dc * e.ldd] = tile[tx][i];
+      }
+      __syncthreads();
+    }
 }
 
 template <typename T>
