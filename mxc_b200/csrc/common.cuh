@@ -53,6 +53,28 @@ __device__ __forceinline__ double kernel_fast(const KernelParams& kp, double dx,
   return exp(-kp.alpha * (r2 * inv)) * inv;
 }
 
+// Calls f(r, c, e) for every element e = r + c m of an m x n column-major
+// range (m n < 2^31), consecutive threads of the CTA on consecutive rows:
+// one division per thread, then division-free stepping.
+template <typename F>
+__device__ __forceinline__ void for_each_rc(int m, int n, F f) {
+  if (m <= 0 || n <= 0) return;
+  const int stride = (int)blockDim.x, total = m * n;
+  const int dq = stride / m, dr = stride - dq * m;
+  int e = (int)threadIdx.x;
+  if (e >= total) return;
+  int c = e / m, r = e - c * m;
+  for (; e < total; e += stride) {
+    f(r, c, e);
+    r += dr;
+    c += dq;
+    if (r >= m) {
+      r -= m;
+      c++;
+    }
+  }
+}
+
 template <typename T>
 struct BlockReduce {
   // Sum over a whole CTA (blockDim.x a multiple of 32, <= 1024).

@@ -305,15 +305,13 @@ __global__ void __launch_bounds__(256) k_basis_finish(
   const int rank = s_rank;
   if (!(0 < rank && rank < M)) {
     // R = upper triangle of the incoming Q, Q = identity (h2matrix.cpp:114-117).
-    for (i64 e = tid; e < (i64)M * M; e += nt) {
-      int r = (int)(e % M), c = (int)(e / M);
+    for_each_rc(M, M, [&](int r, int c, int e) {
       Rb[e] = r <= c ? Qb[e] : T(0);
-    }
+    });
     __syncthreads();
-    for (i64 e = tid; e < (i64)M * M; e += nt) {
-      int r = (int)(e % M), c = (int)(e / M);
+    for_each_rc(M, M, [&](int r, int c, int e) {
       Qb[e] = r == c ? T(1) : T(0);
-    }
+    });
     if (tid == 0) ranks_out[box] = rank;
     return;
   }
@@ -358,22 +356,20 @@ __global__ void __launch_bounds__(256) k_basis_finish(
     // Q = P [I; T^T] padded with zero columns, R = I (h2matrix.cpp:107-112).
     for (i64 e = tid; e < (i64)M * M; e += nt) Qb[e] = T(0);
     __syncthreads();
-    for (i64 e = tid; e < (i64)M * rank; e += nt) {
-      int k = (int)(e % M), i = (int)(e / M);
+    for_each_rc(M, rank, [&](int k, int i, int e) {
       T v = k < rank ? (k == i ? T(1) : T(0)) : W[(i64)i * M + k];
       Qb[(i64)perm[k] + (i64)i * M] = v;
-    }
+    });
     for (int i = tid; i < rank; i += nt) Rb[(i64)i * M + i] = T(1);
     if (tid == 0) ranks_out[box] = rank;
     return;
   }
   // Orthogonal mode (h2matrix.cpp:100-106).  U_ID = P [I; T^T] (M x rank)
   // goes to R's slot as scratch, RX2 = triu(Qin) U_ID to W (col-major now).
-  for (i64 e = tid; e < (i64)M * rank; e += nt) {
-    int k = (int)(e % M), i = (int)(e / M);
+  for_each_rc(M, rank, [&](int k, int i, int e) {
     T v = k < rank ? (k == i ? T(1) : T(0)) : W[(i64)i * M + k];
     Rb[(i64)perm[k] + (i64)i * M] = v;
-  }
+  });
   __syncthreads();
   if (wy_taus) {
     // Blocked completion on the host side: U_ID is in R's slot, Q still
@@ -381,8 +377,7 @@ __global__ void __launch_bounds__(256) k_basis_finish(
     if (tid == 0) ranks_out[box] = rank;
     return;
   }
-  for (i64 e = tid; e < (i64)M * rank; e += nt) {
-    int p = (int)(e % M), i = (int)(e / M);
+  for_each_rc(M, rank, [&](int p, int i, int e) {
     T s;
     if (qin_identity) {
       s = Rb[e];
@@ -391,7 +386,7 @@ __global__ void __launch_bounds__(256) k_basis_finish(
       for (int l = p; l < M; l++) s += Qb[p + (i64)l * M] * Rb[l + (i64)i * M];
     }
     W[e] = s;
-  }
+  });
   __syncthreads();
   // Householder QR of RX2 (M x rank), column-major in W.  One warp per
   // column for the reflector application.
@@ -428,15 +423,13 @@ __global__ void __launch_bounds__(256) k_basis_finish(
     __syncthreads();
   }
   // R = triu(RX2[:rank, :rank]) (R's slot was scratch: clear first).
-  for (i64 e = tid; e < (i64)M * M; e += nt) {
-    int r = (int)(e % M), c = (int)(e / M);
+  for_each_rc(M, M, [&](int r, int c, int e) {
     Rb[e] = (c < rank && r <= c) ? W[r + (i64)c * M] : T(0);
-  }
+  });
   // Q = H_0 ... H_{rank-1} applied to the identity.
-  for (i64 e = tid; e < (i64)M * M; e += nt) {
-    int r = (int)(e % M), c = (int)(e / M);
+  for_each_rc(M, M, [&](int r, int c, int e) {
     Qb[e] = r == c ? T(1) : T(0);
-  }
+  });
   __syncthreads();
   for (int k = rank - 1; k >= 0; k--) {
     const T tau = taus[k];
@@ -734,10 +727,9 @@ __global__ void __launch_bounds__(256) k_qr_panel(const QrPanelTask<T>* __restri
   __shared__ T red[32];
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
   T* Wp = t.W + (i64)t.k0 + (i64)t.k0 * t.M;
-  for (i64 e = tid; e < (i64)m * nb; e += nt) {
-    int r = (int)(e % m), j = (int)(e / m);
+  for_each_rc(m, nb, [&](int r, int j, int e) {
     P[e] = Wp[r + (i64)j * t.M];
-  }
+  });
   __syncthreads();
   for (int j = 0; j < nb; j++) {
     T* cj = P + (size_t)j * m;
@@ -797,11 +789,10 @@ __global__ void __launch_bounds__(256) k_qr_panel(const QrPanelTask<T>* __restri
     }
   }
   __syncthreads();
-  for (i64 e = tid; e < (i64)m * nb; e += nt) {
-    int r = (int)(e % m), j = (int)(e / m);
+  for_each_rc(m, nb, [&](int r, int j, int e) {
     Wp[r + (i64)j * t.M] = P[e];
     t.Vp[e] = r < j ? T(0) : (r == j ? T(1) : P[e]);
-  }
+  });
   for (int e = tid; e < nb * nb; e += nt) {
     int r = e % nb, c = e / nb;
     t.Tp[e] = r <= c ? Tl[e] : T(0);
@@ -834,16 +825,14 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_qr_extract(const QrExtractTask<T>* __restrict__ tasks) {
   const QrExtractTask<T> t = tasks[blockIdx.x];
   const int M = t.M, r = t.rank;
-  for (i64 e = threadIdx.x; e < (i64)M * M; e += blockDim.x) {
-    int i = (int)(e % M), c = (int)(e / M);
+  for_each_rc(M, M, [&](int i, int c, int e) {
     t.R[e] = (c < r && i <= c) ? t.W[i + (i64)c * M] : T(0);
     t.Q[e] = i == c ? T(1) : T(0);
-  }
+  });
   __syncthreads();
-  for (i64 e = threadIdx.x; e < (i64)M * r; e += blockDim.x) {
-    int i = (int)(e % M), c = (int)(e / M);
+  for_each_rc(M, r, [&](int i, int c, int e) {
     if (i <= c) t.W[e] = i == c ? T(1) : T(0);
-  }
+  });
 }
 
 template <typename T>
