@@ -21,7 +21,11 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
          "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 
-SOURCES = ["plan.cpp", "k_gen.cu", "k_basis.cu", "k_gemm.cu", "k_tc.cu", "k_gram.cu", "k_lu.cu", "k_vec.cu", "h2dev.cu"]
+SOURCES = ["plan.cpp", "k_gen.cu", "k_basis.cu", "k_gemm.cu", "k_tc.cu", "k_gram.cu", "k_lu.cu", "k_vec.cu", "h2dev.cu",
+           "h2_solver.cpp"]
+# The reference's command-line driver on this library (C++ host code only).
+CLI_SRC = os.path.join(CSRC, "lorasp.cpp")
+CLI = os.path.join(HERE, "lorasp")
 
 
 def _compile(src: str, force: bool) -> str:
@@ -29,6 +33,7 @@ def _compile(src: str, force: bool) -> str:
     obj = os.path.join(BUILD, src + ".o")
     deps = [path] + [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".h", ".hpp", ".cuh"))]
     deps.append(os.path.join(ROOT, "include", "h2dev.h"))
+    deps.append(os.path.join(ROOT, "include", "mxc_b200", "h2_solver.hpp"))
     if not force and os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
         return obj
     cmd = [NVCC] + ARCH + FLAGS + ["-x", "cu" if src.endswith(".cu") else "c++", "-c", path, "-o", obj]
@@ -50,8 +55,15 @@ def build(jobs: int = 8, force: bool = False, verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n%s\n%s" % (" ".join(cmd), r.stderr))
+    deps = [CLI_SRC, LIB, os.path.join(ROOT, "include", "mxc_b200", "h2_solver.hpp")]
+    if force or not os.path.exists(CLI) or os.path.getmtime(CLI) < max(os.path.getmtime(d) for d in deps):
+        cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), CLI_SRC, "-o", CLI, "-L" + HERE,
+               "-lmxcb200", "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("lorasp build failed:\n%s\n%s" % (" ".join(cmd), r.stderr))
     if verbose:
-        print("built", LIB)
+        print("built", LIB, CLI)
     return LIB
 
 
