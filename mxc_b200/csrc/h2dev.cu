@@ -805,7 +805,24 @@ class Solver : public SolverBase {
       // contiguous box ranges and concatenated in box order.
       std::vector<int> sidx;
       std::vector<i64> soff(nodes + 1, 0), krows(nodes, 0);
-      {
+      // Sketch mode (H2DEV_OPT_SAMPLING = 2): every far body, as ranges of
+      // the tree-sorted body array per box (start, running count).
+      const bool sketch = sampling_mode == 2;
+      std::vector<i64> roff, rstart, rend;
+      if (sketch) {
+        roff.assign(nodes + 1, 0);
+        for (i64 i = 0; i < nodes; i++) {
+          i64 cnt = 0;
+          for (const auto& r : ranges[g0 + i]) {
+            cnt += r.second - r.first;
+            rstart.push_back(r.first);
+            rend.push_back(cnt);
+          }
+          roff[i + 1] = (i64)rstart.size();
+          soff[i + 1] = soff[i] + cnt;
+          krows[i] = std::min<i64>(lv.dims[i], cnt);
+        }
+      } else {
         const int nth = (int)std::max<i64>(1, std::min<i64>({8, (i64)std::thread::hardware_concurrency(), nodes / 16}));
         std::vector<std::vector<int>> part(nth);
         std::vector<i64> cnt(nodes, 0);
@@ -845,7 +862,7 @@ class Solver : public SolverBase {
       const bool orth = 1. <= e;
       i64 cap = -1;
       if (e >= 1.) cap = (i64)std::floor(e);
-      if (orth && h->basis_mode == 0) {
+      if (orth && h->basis_mode == 0 && !sketch) {
         basis_gram(lv, low == nullptr, soff, d_sidx, d_krows, d_perm, d_maxpiv, d_nonzero, e, cap);
       } else {
         DVec<T> Rws;
@@ -857,10 +874,36 @@ class Solver : public SolverBase {
             double S = (double)(soff[i + 1] - soff[i]), Md = (double)lv.dims[i];
             fl += S >= Md ? 2. * S * Md * Md - 2. / 3. * Md * Md * Md : 2. * Md * S * S - 2. / 3. * S * S * S;
           }
-          Prof pf("sample_tsqr", fl, (double)sidx.size() * 28.);
-          ck(launch_sample_tsqr<T>(kp, bodies.p, lv.pts.p, lv.d_xoff.p, lv.d_dims.p, d_sidx.p, d_soff.p, Rws.p,
-                                   lv.d_qoff.p, (int)nodes, (int)lv.maxM, st()),
-             "sample_tsqr");
+          if (sketch) {
+            // Y = Omega XF over the whole far list (k_sketch.cu), or XF
+            // itself where the list has at most M bodies.
+            const int tm = sketch_tile_rows(), tn = sketch_tile_cols();
+            std::vector<int4> tiles;
+            double sfl = 0.;
+            for (i64 i = 0; i < nodes; i++) {
+              const i64 M = lv.dims[i], S = soff[i + 1] - soff[i];
+              if (M == 0 || S == 0) continue;
+              const i64 rows = std::min(M, S);
+              for (i64 a = 0; a < (rows + tm - 1) / tm; a++)
+                for (i64 c = 0; c < (M + tn - 1) / tn; c++) tiles.push_back(make_int4((int)i, (int)a, (int)c, 0));
+              if (S > M) sfl += 2. * (double)M * (double)M * (double)S;
+            }
+            DVec<i64> d_roff, d_rstart, d_rend;
+            DVec<int4> d_tiles;
+            d_roff.upload(roff);
+            d_rstart.upload(rstart);
+            d_rend.upload(rend);
+            d_tiles.upload(tiles);
+            Prof pf("sketch", sfl, 24. * (double)soff[nodes]);
+            ck(launch_sketch<T>(kp, bodies.p, lv.pts.p, lv.d_xoff.p, lv.d_dims.p, lv.d_qoff.p, d_roff.p, d_rstart.p,
+                                d_rend.p, d_tiles.p, (int)tiles.size(), Rws.p, st()),
+               "sketch");
+          } else {
+            Prof pf("sample_tsqr", fl, (double)sidx.size() * 28.);
+            ck(launch_sample_tsqr<T>(kp, bodies.p, lv.pts.p, lv.d_xoff.p, lv.d_dims.p, d_sidx.p, d_soff.p, Rws.p,
+                                     lv.d_qoff.p, (int)nodes, (int)lv.maxM, st()),
+               "sample_tsqr");
+          }
         }
         {
           double fl = 0.;
@@ -2580,7 +2623,7 @@ int h2dev_set_option(h2dev_handle_t h, int option, int64_t value) {
     return H2DEV_OK;
   }
   if (option == H2DEV_OPT_SAMPLING) {
-    require(value == 0 || value == 1, "sampling option must be 0 or 1");
+    require(value >= 0 && value <= 2, "sampling option must be 0, 1 or 2");
     h->sampling_mode = (int)value;
     return H2DEV_OK;
   }

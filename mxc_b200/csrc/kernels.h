@@ -26,6 +26,15 @@ template <typename T>
 cudaError_t launch_sample_tsqr(const KernelParams& kp, const double* bodies, const double* pts, const i64* xoff,
                                const i64* dims, const int* sidx, const i64* soff, T* Rws, const i64* qoff,
                                int nboxes, int maxM, cudaStream_t st);
+// Full-far-field sketch (k_sketch.cu): Rws[box] (row-major M x M) = Omega XF
+// over every far body (ranges roff[box]..roff[box+1]-1 of rstart / rend), or
+// the first S rows = XF when S <= M.  tiles: {box, row tile, column tile}.
+template <typename T>
+cudaError_t launch_sketch(const KernelParams& kp, const double* bodies, const double* pts, const i64* xoff,
+                          const i64* dims, const i64* qoff, const i64* roff, const i64* rstart, const i64* rend,
+                          const int4* d_tiles, int ntiles, T* Rws, cudaStream_t st);
+int sketch_tile_rows();
+int sketch_tile_cols();
 template <typename T>
 cudaError_t launch_cpqr(const i64* dims, const i64* krows, T* Rws, const i64* qoff, int* perm, const i64* xoff,
                         double* maxpiv, int* nonzero, i64 step_cap, int nboxes, int maxM, cudaStream_t st);

@@ -343,13 +343,56 @@ def geometric_allocation(gsize, samples: int):
     return alloc
 
 
+SKETCH_MUL_F = np.uint64(0x9E3779B97F4A7C15)
+SKETCH_MUL_W = np.uint64(0xD1B54A32D192ED03)
+SKETCH_ADD = np.uint64(0x2545F4914F6CDD1D)
+
+
+def _mix64(z: np.ndarray) -> np.ndarray:
+    """splitmix64 finaliser (Steele, Lea and Flood 2014), uint64 wrap-around."""
+    z = z ^ (z >> np.uint64(30))
+    z = z * np.uint64(0xBF58476D1CE4E5B9)
+    z = z ^ (z >> np.uint64(27))
+    z = z * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def sketch_signs(p: int, fidx: np.ndarray) -> np.ndarray:
+    """(p, len(fidx)) random-sign matrix of the full-far-field sketch.
+
+    Entry (a, f) is -1 when bit (a mod 64) of the 64-bit word
+    mix64(body_f * MUL_F + (a div 64) * MUL_W + ADD) is set, else +1; it
+    depends only on the row and the body's index in the tree-sorted body
+    array, so the library's kernel forms the same matrix in any order.
+    """
+    fidx = np.asarray(fidx, dtype=np.int64).astype(np.uint64)
+    words = (p + 63) // 64
+    with np.errstate(over="ignore"):
+        z = (fidx[None, :] * SKETCH_MUL_F + np.arange(words, dtype=np.uint64)[:, None] * SKETCH_MUL_W
+             + SKETCH_ADD)
+        z = _mix64(z)
+    a = np.arange(p)
+    bits = (z[a >> 6, :] >> (a & 63).astype(np.uint64)[:, None]) & np.uint64(1)
+    return np.where(bits == 1, -1.0, 1.0)
+
+
+def far_indices(ranges) -> np.ndarray:
+    """Tree-sorted body indices of a box's whole far list, in list order."""
+    if not ranges:
+        return np.zeros(0, dtype=np.int64)
+    return np.concatenate([np.arange(b0, b1, dtype=np.int64) for b0, b1 in ranges])
+
+
 def far_bodies(bodies: np.ndarray, ranges, samples: int, gstart=None, mode: int = 0) -> np.ndarray:
     """Rows of a box's far list kept under ``samples``: mode 0 strided over the
-    whole list, mode 1 level-geometric (build extensions; samples <= 0 keeps all)."""
+    whole list, mode 1 level-geometric (build extensions; samples <= 0 keeps all).
+    Mode 2 (sketch) keeps every far body."""
     if not ranges:
         return np.zeros((0, 3))
     idx = np.concatenate([np.arange(b0, b1, dtype=np.int64) for b0, b1 in ranges])
     total = len(idx)
+    if mode == 2:
+        return bodies[idx]
     if mode == 0 or samples <= 0 or samples >= total:
         keep = sample_indices(total, samples)
         return bodies[idx[keep]]
@@ -461,12 +504,20 @@ def colpiv_rank(qr: np.ndarray, maxpivot: float, nonzero: int, threshold: float)
 
 
 def compute_basis(kern: Kernel, epi: float, Xbodies: np.ndarray, Fbodies: np.ndarray,
-                  a: np.ndarray, orth: bool):
+                  a: np.ndarray, orth: bool, sketch_idx: np.ndarray | None = None):
     """h2matrix.cpp:13-63.
 
     ``Xbodies`` (M, 3) is permuted in place (skeletons first).  ``a`` is the
     incoming M x M Q (identity at a leaf, children's R blocks above) and is
     replaced by the basis; returns (rank, c) with c the M x M R matrix.
+
+    ``sketch_idx`` (build extension, sampling mode 2): the body indices of
+    ``Fbodies``; when the far list is longer than M, the column-pivoted QR
+    runs on the M x M sketch S XF (S the random-sign matrix of
+    ``sketch_signs``) instead of on R of QR(XF).  Both have the column
+    geometry of XF up to the sketch's distortion, so the ID keeps the
+    whole far field's accuracy (Halko, Martinsson and Tropp 2011, randomized
+    interpolative decomposition) at the cost of one GEMM.
     """
     M = Xbodies.shape[0]
     N = Fbodies.shape[0]
@@ -475,7 +526,9 @@ def compute_basis(kern: Kernel, epi: float, Xbodies: np.ndarray, Fbodies: np.nda
     c = np.zeros((M, M))
     if K > 0:
         XF = gen_matrix(kern, Fbodies, Xbodies)  # N x M
-        if K < N:
+        if K < N and sketch_idx is not None:
+            RX = sketch_signs(M, sketch_idx) @ XF
+        elif K < N:
             RX = np.triu(householder_r(XF)[:K])
         else:
             RX = XF
@@ -654,7 +707,8 @@ class H2MatrixSolver:
             for i in range(nodes):
                 fb = far_bodies(bodies, ranges.get(g0 + i, []), samples, self.gstart.get(g0 + i, []),
                                 self.sampling)
-                rank, c = compute_basis(kern, epi, lev.S[i], fb, lev.Q[i], 1.0 <= epi)
+                sk = far_indices(ranges.get(g0 + i, [])) if self.sampling == 2 else None
+                rank, c = compute_basis(kern, epi, lev.S[i], fb, lev.Q[i], 1.0 <= epi, sk)
                 lev.R[i] = c
                 lev.DimsLr[i] = rank
 
@@ -755,7 +809,8 @@ class H2MatrixSolver:
                 if Ms > 0:
                     Aii[Ms:, :Ms] = V[Ms:] @ b[:Ms].T
                     Aii[:Ms, :Ms] -= Aii[:Ms, Ms:] @ Aii[Ms:, :Ms]
-                det = np.prod(np.diag(lu))
+                with np.errstate(over="ignore", under="ignore"):
+                    det = np.prod(np.diag(lu))  # may overflow or underflow, as Eigen's product does
                 lev.info += int(abs(det) <= DBL_MIN)
             lev.R[i] = V
             for ij in range(lev.ARows[i], lev.ARows[i + 1]):
