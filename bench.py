@@ -190,7 +190,7 @@ def rhs_matrix(n: int, nrhs: int):
     import mxc_b200 as m
 
     X = np.empty((n, nrhs), order="F")
-    X[:, 0] = m.uniform_rhs(n)  # main.cpp:358-361
+    X[:, 0] = m.uniform_rhs(n)  # main.cpp:73-76
     if nrhs > 1:
         X[:, 1:] = np.random.default_rng(20261203).random((n, nrhs - 1))
     return X

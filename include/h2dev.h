@@ -42,13 +42,13 @@ enum { H2DEV_FP64 = 0, H2DEV_FP32 = 1 };
 
 /* test_funcs.hpp:31-41 uniform_unit_cube_rnd: std::mt19937(seed) bodies. */
 int h2_uniform_unit_cube_rnd(double* bodies, int64_t nbodies, double diameter, int64_t dim, unsigned seed);
-/* main.cpp:358-361: default-seeded std::mt19937_64 uniform[0,1) vector. */
+/* main.cpp:73-76: default-seeded std::mt19937_64 uniform[0,1) vector. */
 int h2_uniform_rhs(double* x, int64_t n);
-/* build_tree.cpp:93-125 buildBinaryTree: sorts bodies (n x 3) in place and
+/* build_tree.cpp:67-99 buildBinaryTree: sorts bodies (n x 3) in place and
  * fills 2^(levels+1)-1 cells: child[2], body[2] (int64) and R[3], C[3]. */
 int h2_build_tree(double* bodies, int64_t nbodies, int64_t levels, int64_t* cell_child, int64_t* cell_body,
                   double* cell_R, double* cell_C);
-/* build_tree.cpp:67-84 CSR::CSR: kind 'N' (near) or 'F' (far) pair list over
+/* build_tree.cpp:41-58 CSR::CSR: kind 'N' (near) or 'F' (far) pair list over
  * all cells.  row receives ncells+1 offsets; col up to cap column indices;
  * *nnz the list length (call with col = NULL to size it). */
 int h2_pair_csr(char kind, int64_t ncells, const int64_t* cell_child, const int64_t* cell_body, const double* cell_R,
@@ -71,15 +71,21 @@ int h2dev_handle_trim(h2dev_handle_t h);
  * Gram matrix of the far samples with a pivoted Cholesky (same pivots and R
  * as the column-pivoted QR in exact arithmetic); 1 uses the Householder
  * sample-tile QR + Eigen-rule column-pivoted QR for every basis, the
- * reference's own sequence (h2matrix.cpp:76-89).  Threshold (operator) bases
- * always use the Householder path. */
+ * reference's own sequence (h2matrix.cpp:19-32).  Threshold (operator) bases
+ * always use the Householder path, or the sketch (H2DEV_OPT_SAMPLING = 2). */
 /* H2DEV_OPT_SKINNY_TILED: 1 makes plans built afterwards (in this process)
  * run every multi-right-hand-side apply on the tiled segmented GEMM instead
  * of the register-streaming kernel; 0 (default) restores the latter. */
 /* H2DEV_OPT_SAMPLING: how `samples` caps a box's far list.  0 (default):
  * rows floor(j * total / samples) of the whole list.  1: level-geometric —
  * the far boxes of the box's own level (the nearest) get half of the budget,
- * each level further out half of what remains, each group strided as in 0. */
+ * each level further out half of what remains, each group strided as in 0.
+ * 2: sketch — `samples` is ignored and every far body is used, as the
+ * reference does, but the column-pivoted QR runs on the M x M product of a
+ * random-sign matrix with the whole far block instead of on R of its QR
+ * (randomized interpolative decomposition; one FP64 tensor-core GEMM per box,
+ * the far block is never stored).  Boxes whose far list has at most M bodies
+ * use the far block itself, as the reference does. */
 /* H2DEV_OPT_TENSOR_CORES: 1 (default) runs the FP32 block contractions of
  * plans built afterwards (in this process) on the tcgen05 tensor cores with
  * a 3-term TF32 split (FP32 accuracy); 2 with one TF32 product (about 1e-3
@@ -89,8 +95,8 @@ int h2dev_set_option(h2dev_handle_t h, int option, int64_t value);
 
 /* ---- solver (solver.hpp:11-47 H2MatrixSolver) ------------------------ */
 
-/* H2MatrixSolver::H2MatrixSolver (solver.cpp:59-88): builds the tree lists,
- * the shared bases (compute_basis, h2matrix.cpp:70-120), near blocks and
+/* H2MatrixSolver::H2MatrixSolver (solver.cpp:12-41): builds the tree lists,
+ * the shared bases (compute_basis, h2matrix.cpp:13-63), near blocks and
  * couplings of every level on the device.  epi > 0: operator mode (ID basis
  * with relative threshold epi); epi == 0: fixed-rank orthogonal preconditioner
  * mode with rank (levels - l) * leveled_rank + rank at level l and far lists
@@ -108,20 +114,20 @@ int h2dev_solver_shape(h2dev_solver_t s, int64_t* levels, int64_t* lenX);
 /* Dims / DimsLr of one level (h2matrix.hpp:27-28), 2^level entries each. */
 int h2dev_solver_level_dims(h2dev_solver_t s, int64_t level, int64_t* dims, int64_t* ranks);
 
-/* matVecMul (solver.cpp:123-135): X <- A_H2 X, in place. */
+/* matVecMul (solver.cpp:76-88): X <- A_H2 X, in place. */
 int h2dev_matvec(h2dev_solver_t s, int64_t nrhs, double* X, int64_t ldx);
 int h2dev_matvec_device(h2dev_solver_t s, int64_t nrhs, double* dX, int64_t ldx);
 
-/* factorizeM (solver.cpp:137-147): multilevel ULV factorization.
+/* factorizeM (solver.cpp:90-100): multilevel ULV factorization.
  * info_per_level (optional, levels+1 ints) receives the singular-block
  * count of each level; returns H2DEV_ERR_SINGULAR when any is nonzero. */
 int h2dev_factorize(h2dev_solver_t s, int* info_per_level);
 
-/* solvePrecondition (solver.cpp:168-179): X <- M^{-1} X, in place. */
+/* solvePrecondition (solver.cpp:121-132): X <- M^{-1} X, in place. */
 int h2dev_solve_precondition(h2dev_solver_t s, int64_t nrhs, double* X, int64_t ldx);
 int h2dev_solve_precondition_device(h2dev_solver_t s, int64_t nrhs, double* dX, int64_t ldx);
 
-/* solveGMRES (solver.cpp:191-248), one independent restarted GMRES per
+/* solveGMRES (solver.cpp:144-201), one independent restarted GMRES per
  * right-hand side: left preconditioner M (factored), true residual with A.
  * X is the initial guess on entry and the solution on return.  resid
  * ((outer+1) x nrhs, column-major) receives the relative residual history and
@@ -134,7 +140,7 @@ int h2dev_solve_gmres_device(h2dev_solver_t A, h2dev_solver_t M, double tol, int
                              const double* dB, int64_t ld, int64_t inner, int64_t outer, int early_exit,
                              double* resid, int64_t* iters);
 
-/* H2MatrixSolver::solveRelErr (solver.cpp:276-285) for each of nrhs
+/* H2MatrixSolver::solveRelErr (solver.cpp:229-238) for each of nrhs
  * columns of device arrays X and ref (leading dimension ld):
  * err[c] = sqrt(sum (x - ref)^2 / sum ref^2), written to host memory.  The
  * per-chunk partial sums live in a device scratch buffer allocated per call. */
@@ -153,8 +159,10 @@ int h2dev_solve_rel_err_device(h2dev_handle_t h, int64_t n, int64_t nrhs, const 
  * handle's stream.  Limit: 2 * ceil(n / 16384) * nrhs <= 16384 (for example
  * n up to 134,217,728 with one column, 8,388,608 with 16); larger requests
  * return H2DEV_ERR_ARG.  The first call on a device looks up the array's
- * device address, so make it before any stream capture.  All calls share the
- * array: calls whose work overlaps on the GPU (two streams at once) race. */
+ * device address, so make it before any stream capture; the address is kept
+ * for the life of the process, so do not call this after cudaDeviceReset.
+ * All calls share the array: calls whose work overlaps on the GPU (two
+ * streams at once) race. */
 int h2dev_solve_rel_err_device_noalloc(h2dev_handle_t h, int64_t n, int64_t nrhs, const double* dX,
                                        const double* dRef, int64_t ld, double* dErr);
 

@@ -25,10 +25,22 @@ namespace h2b {
 
 static thread_local h2dev_handle_s* g_cur = nullptr;
 
+// Scope of one API call on a handle: makes the handle current for the
+// library's allocations and launches, and its device current for the CUDA
+// runtime (the caller's current device is restored on exit).
 struct CurHandle {
   h2dev_handle_s* prev;
-  explicit CurHandle(h2dev_handle_s* h) : prev(g_cur) { g_cur = h; }
-  ~CurHandle() { g_cur = prev; }
+  int prev_dev = -1;
+  explicit CurHandle(h2dev_handle_s* h) : prev(g_cur) {
+    g_cur = h;
+    int d = -1;
+    if (h && cudaGetDevice(&d) == cudaSuccess && d != h->device && cudaSetDevice(h->device) == cudaSuccess)
+      prev_dev = d;
+  }
+  ~CurHandle() {
+    g_cur = prev;
+    if (prev_dev >= 0) cudaSetDevice(prev_dev);
+  }
 };
 
 struct Prof {
@@ -277,12 +289,21 @@ static bool force_tiled() { return g_force_tiled; }
 // 0 SIMT, 1 tcgen05 with the 3-term TF32 split, 2 tcgen05 single TF32.
 static int g_tensor_cores = 1;
 
-// Throws when a tensor-core GEMM launched since the last check reported an
-// expired wait (synchronises the stream).
-static void check_tc(cudaStream_t st) {
+// Throws when a tensor-core GEMM launched on this handle since the last
+// check reported an expired wait (then its output is incomplete).  Reads and
+// clears the handle's flag; synchronises the handle's streams only when such
+// a GEMM was queued.
+static void check_tc(h2dev_handle_s* h) {
+  if (!h || !h->tc_pending) return;
   int flag = 0;
-  ck(tc_gemm_take_error(&flag, st), "tensor-core GEMM status");
-  if (flag) throw H2Error{H2DEV_ERR_CUDA, "tensor-core GEMM: an mbarrier wait expired"};
+  ck(cudaStreamSynchronize(h->stream2), "sync");
+  ck(cudaStreamSynchronize(h->stream), "sync");
+  ck(cudaMemcpy(&flag, h->d_tc_err, sizeof(int), cudaMemcpyDeviceToHost), "tensor-core GEMM status");
+  h->tc_pending = false;
+  if (flag) {
+    ck(cudaMemset(h->d_tc_err, 0, sizeof(int)), "tensor-core GEMM status");
+    throw H2Error{H2DEV_ERR_CUDA, "tensor-core GEMM: an mbarrier wait expired (the result is incomplete)"};
+  }
 }
 
 // Host-built list of segmented-GEMM tasks, uploaded once and replayed.
@@ -494,8 +515,12 @@ struct GemmPlan {
       ck(launch_skinny_nn<T>(nr, 0, d_tasks.p, d_ents.p, d_rtiles.p, (int)d_rtiles.n, st), "skinny_nn");
       if (nsums) ck(launch_sum_parts<T>(d_sums.p, nsums, sum_maxmn, st), "sum_parts");
     } else if (shape == GEMM_TC) {
-      if constexpr (std::is_same<T, float>::value)
-        ck(launch_tc_gemm(d_tasks.p, d_ents.p, d_tiles.p, ntiles, tc_mode == 1 ? 1 : 0, st), "tc_gemm");
+      if constexpr (std::is_same<T, float>::value) {
+        require(g_cur != nullptr, "tensor-core GEMM outside an API call");
+        ck(launch_tc_gemm(d_tasks.p, d_ents.p, d_tiles.p, ntiles, tc_mode == 1 ? 1 : 0, g_cur->d_tc_err, st),
+           "tc_gemm");
+        g_cur->tc_pending = true;
+      }
     } else if (std::is_same<T, double>::value && shape == GEMM_BIG && g_tensor_cores) {
       if constexpr (std::is_same<T, double>::value)
         ck(launch_dgemm(d_tasks.p, d_ents.p, d_tiles.p, ntiles, st), "dgemm");
@@ -579,7 +604,7 @@ void batched_gemm(int64_t batch, int64_t nterms, int64_t m, int64_t n, int64_t k
   }
   g.finalize();
   g.run(st);
-  check_tc(st);
+  check_tc(g_cur);
 }
 
 
@@ -692,14 +717,14 @@ class Solver : public SolverBase {
       lv.na_ld.assign(lv.acol.size(), 0);
     }
     for (i64 l = levels; l >= 0; l--) construct_level(l, ranges);
-    check_tc(st());
+    check_tc(h);
   }
 
   double level_epi(i64 l) const {
     return fix_rank ? (double)((levels - l) * leveled_rank + rank) : epi;
   }
 
-  // h2matrix.cpp:129-306 for one level.
+  // h2matrix.cpp:72-249 for one level.
   void construct_level(i64 l, const std::vector<std::vector<std::pair<i64, i64>>>& ranges) {
     Level<T>& lv = L[l];
     Level<T>* low = (l < levels) ? &L[l + 1] : nullptr;
@@ -800,7 +825,7 @@ class Solver : public SolverBase {
         acopy.run(st());
       }
 
-      // Shared basis of every box (compute_basis, h2matrix.cpp:252-257).
+      // Shared basis of every box (compute_basis, h2matrix.cpp:195-200).
       // Far-sample lists of all boxes, built by up to 8 host threads over
       // contiguous box ranges and concatenated in box order.
       std::vector<int> sidx;
@@ -947,7 +972,7 @@ class Solver : public SolverBase {
     }
     lv.C.alloc(lv.coff[nC]);
     if (lv.lenZ > 0 && nC > 0) {
-      // Couplings (h2matrix.cpp:279-299): K(S_y, S_x) on the skeletons,
+      // Couplings (h2matrix.cpp:222-242): K(S_y, S_x) on the skeletons,
       // scaled by R_y on the left and R_x^T on the right in orthogonal mode.
       const bool orth = 1. <= level_epi(l);
       DVec<T> K;
@@ -1001,7 +1026,7 @@ class Solver : public SolverBase {
   // Fixed-rank orthogonal mode: far-sample block XF generated into HBM in
   // bounded chunks, Gram matrix G = XF^T XF by the segmented GEMM (FP64),
   // pivoted Cholesky of G (the pivots and R rows of ColPivHouseholderQR in
-  // exact arithmetic, h2matrix.cpp:78-89), then the same ID / completion step
+  // exact arithmetic, h2matrix.cpp:21-32), then the same ID / completion step
   // as the Householder path, in FP64, converted to T at the end.
   void basis_gram(Level<T>& lv, bool leaf, const std::vector<i64>& soff, DVec<int>& d_sidx, DVec<i64>& d_krows,
                   DVec<int>& d_perm, DVec<double>& d_maxpiv, DVec<int>& d_nonzero, double e, i64 cap) {
@@ -1150,7 +1175,7 @@ class Solver : public SolverBase {
     }
   }
 
-  // Orthogonal completion (h2matrix.cpp:100-106) for every box with
+  // Orthogonal completion (h2matrix.cpp:43-49) for every box with
   // 0 < rank < M, after the finish kernel left U_ID = P [I; T^T] in R's slot
   // and Q_in (upper triangular) in Q: W = Q_in U_ID (M x rank, ld M), a
   // blocked Householder QR of W (panels factored in shared memory, the
@@ -1337,7 +1362,7 @@ class Solver : public SolverBase {
     pc_built = false;
   }
 
-  // H^2 matvec plans (h2matrix.cpp:308-401) for the current nrhs.
+  // H^2 matvec plans (h2matrix.cpp:251-344) for the current nrhs.
   // Multi-RHS H^2 matvec plans (h2matrix.cpp:303-344): upward pass
   // Z_l = Q_l^T X_l (from the transposed copies), one launch for the far
   // couplings of every level W_l = sum_j C_ij Z_j (all levels read finished
@@ -1477,7 +1502,7 @@ class Solver : public SolverBase {
   }
 
   // ------------------------------------------------------------ factor
-  // h2matrix.cpp:403-482 for one level, then factorizeCopyNext (484-503).
+  // h2matrix.cpp:346-425 for one level, then factorizeCopyNext (484-503).
   void factor_level(i64 l) {
     Level<T>& lv = L[l];
     const i64 nodes = lv.nodes;
@@ -1721,7 +1746,7 @@ class Solver : public SolverBase {
       factor_level(l);
       if (l > 0) copy_next(l);
     }
-    check_tc(st());
+    check_tc(h);
     // Singular-block counts per level, read once after the last level.
     for (i64 l = 0; l <= levels; l++) {
       std::vector<int> inf = L[l].info.download(st());
@@ -1733,7 +1758,7 @@ class Solver : public SolverBase {
     pc_built = false;
   }
 
-  // ULV substitution plans (h2matrix.cpp:505-594).
+  // ULV substitution plans (h2matrix.cpp:448-537).
   void build_precondition(i64 nrhs) {
     const int nr = (int)nrhs;
     pc_fx.clear(); pc_fz.clear(); pc_bx.clear(); pc_by.clear(); pc_fcopy.clear(); pc_bcopy.clear();
@@ -1898,7 +1923,7 @@ static double ls_residual(const double* Hin, int ld, int rows, int cols, double 
 }
 
 // ------------------------------------------------------------------ GMRES
-// solver.cpp:191-248 with one independent GMRES per right-hand side.
+// solver.cpp:144-201 with one independent GMRES per right-hand side.
 static int gmres(SolverBase& A, SolverBase& M, double tol, i64 nrhs, double* dX, const double* dB, i64 ld, i64 inner,
                  i64 outer, int early_exit, double* resid, i64* iters) {
   require(A.lenX() == M.lenX(), "gmres: A and M sizes differ");
@@ -1948,7 +1973,7 @@ static int gmres(SolverBase& A, SolverBase& M, double tol, i64 nrhs, double* dX,
     act[c] = (0 < outer && tol <= 1.) ? 1 : 0;
   }
   // The reference starts from the given X with R = B (not B - A X) in its
-  // first cycle (solver.cpp:204); the initial guess is zero in every caller.
+  // first cycle (solver.cpp:157); the initial guess is zero in every caller.
   i64 cycle = 0;
   while (true) {
     bool any = false;
@@ -2033,6 +2058,8 @@ static int gmres(SolverBase& A, SolverBase& M, double tol, i64 nrhs, double* dX,
   for (i64 c = 0; c < nrhs; c++)
     ck(cudaMemcpyAsync(dX + c * ld, X.p + c * N, sizeof(double) * N, cudaMemcpyDeviceToDevice, st), "copy X out");
   ck(cudaStreamSynchronize(st), "sync");
+  check_tc(A.h);
+  check_tc(M.h);
   bool conv = true;
   for (i64 c = 0; c < nrhs; c++) {
     for (i64 k = 0; k <= outer; k++) resid[c * (outer + 1) + k] = res[c * (outer + 1) + k];
@@ -2162,7 +2189,10 @@ int h2dev_handle_create(int device, h2dev_handle_t* out) {
   if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&h->stream2, cudaStreamNonBlocking, least);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&h->d_tc_err, 256);
+  if (e == cudaSuccess) e = cudaMemset(h->d_tc_err, 0, sizeof(int));
   if (e != cudaSuccess) {
+    if (h->d_tc_err) cudaFree(h->d_tc_err);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
     if (h->stream2) cudaStreamDestroy(h->stream2);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -2190,6 +2220,7 @@ static void handle_release(h2dev_handle_s* h) {
   cudaEventDestroy(h->ev_join);
   cudaStreamDestroy(h->stream2);
   cudaStreamDestroy(h->stream);
+  cudaFree(h->d_tc_err);
   delete h;
 }
 
@@ -2333,6 +2364,7 @@ int h2dev_matvec(h2dev_solver_t s, int64_t nrhs, double* X, int64_t ldx) {
   CurHandle ch(p->h);
   require(nrhs > 0 && ldx >= p->lenX(), "bad nrhs/ld");
   with_device_copy(p->h, p->lenX(), nrhs, X, ldx, [&](double* d) { p->matvec(nrhs, d, p->lenX()); });
+  check_tc(p->h);
   return H2DEV_OK;
   H2_API_END
 }
@@ -2342,6 +2374,7 @@ int h2dev_matvec_device(h2dev_solver_t s, int64_t nrhs, double* dX, int64_t ldx)
   require(s && s->impl && dX, "null argument");
   CurHandle ch(s->impl->h);
   s->impl->matvec(nrhs, dX, ldx);
+  check_tc(s->impl->h);
   return H2DEV_OK;
   H2_API_END
 }
@@ -2368,6 +2401,7 @@ int h2dev_solve_precondition(h2dev_solver_t s, int64_t nrhs, double* X, int64_t 
   CurHandle ch(p->h);
   require(nrhs > 0 && ldx >= p->lenX(), "bad nrhs/ld");
   with_device_copy(p->h, p->lenX(), nrhs, X, ldx, [&](double* d) { p->precondition(nrhs, d, p->lenX()); });
+  check_tc(p->h);
   return H2DEV_OK;
   H2_API_END
 }
@@ -2377,6 +2411,7 @@ int h2dev_solve_precondition_device(h2dev_solver_t s, int64_t nrhs, double* dX, 
   require(s && s->impl && dX, "null argument");
   CurHandle ch(s->impl->h);
   s->impl->precondition(nrhs, dX, ldx);
+  check_tc(s->impl->h);
   return H2DEV_OK;
   H2_API_END
 }
@@ -2665,7 +2700,7 @@ int h2dev_solve_rel_err_device(h2dev_handle_t h, int64_t n, int64_t nrhs, const 
   require(h && dX && dRef && err && n > 0 && nrhs > 0 && ld >= n, "bad arguments");
   CurHandle ch(h);
   DVec<double> partial, out;
-  partial.alloc((size_t)2 * relerr_chunks(n) * nrhs);
+  partial.alloc((size_t)(2 * relerr_chunks(n) * nrhs));
   out.alloc(nrhs);
   {
     Prof pf("rel_err", 3. * n * nrhs, 16. * n * nrhs);
@@ -2718,7 +2753,9 @@ static std::mutex g_noalloc_mu;
 
 // Device address of the scratch on ``dev``.  In host code the array's name
 // only stands in for the symbol; the address is looked up once per device,
-// with that device current, and cached.
+// with that device current, and cached for the life of the process (a
+// cudaDeviceReset unloads the module and leaves the cached address stale, so
+// the entry point must not be used after one).
 static cudaError_t noalloc_scratch(int dev, double** out) {
   if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
@@ -2743,7 +2780,12 @@ extern "C" int h2dev_solve_rel_err_device_noalloc(h2dev_handle_t h, int64_t n, i
                                                   const double* dRef, int64_t ld, double* dErr) {
   H2_API_BEGIN
   require(h && dX && dRef && dErr && n > 0 && nrhs > 0 && ld >= n, "bad arguments");
-  const int64_t need = 2 * (int64_t)relerr_chunks(n) * nrhs;
+  CurHandle ch(h);  // the handle's device current for the launch; allocates nothing
+  // In 64-bit arithmetic, and bounded first, so no product can wrap.
+  const int64_t chunks = relerr_chunks(n);
+  const int64_t need = (chunks > NOALLOC_SCRATCH_DOUBLES || nrhs > NOALLOC_SCRATCH_DOUBLES)
+                           ? NOALLOC_SCRATCH_DOUBLES + 1
+                           : 2 * chunks * nrhs;
   if (need > NOALLOC_SCRATCH_DOUBLES) {
     char msg[200];
     snprintf(msg, sizeof(msg),

@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(256) k_basis_finish(
   __syncthreads();
   const int rank = s_rank;
   if (!(0 < rank && rank < M)) {
-    // R = upper triangle of the incoming Q, Q = identity (h2matrix.cpp:114-117).
+    // R = upper triangle of the incoming Q, Q = identity (h2matrix.cpp:57-60).
     for_each_rc(M, M, [&](int r, int c, int e) {
       Rb[e] = r <= c ? Qb[e] : T(0);
     });
@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(256) k_basis_finish(
     bp[3 * k + 2] = sp[3 * p + 2];
   }
   if (!orth) {
-    // Q = P [I; T^T] padded with zero columns, R = I (h2matrix.cpp:107-112).
+    // Q = P [I; T^T] padded with zero columns, R = I (h2matrix.cpp:50-55).
     for (i64 e = tid; e < (i64)M * M; e += nt) Qb[e] = T(0);
     __syncthreads();
     for_each_rc(M, rank, [&](int k, int i, int e) {
@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(256) k_basis_finish(
     if (tid == 0) ranks_out[box] = rank;
     return;
   }
-  // Orthogonal mode (h2matrix.cpp:100-106).  U_ID = P [I; T^T] (M x rank)
+  // Orthogonal mode (h2matrix.cpp:43-49).  U_ID = P [I; T^T] (M x rank)
   // goes to R's slot as scratch, RX2 = triu(Qin) U_ID to W (col-major now).
   for_each_rc(M, rank, [&](int k, int i, int e) {
     T v = k < rank ? (k == i ? T(1) : T(0)) : W[(i64)i * M + k];
@@ -547,7 +547,7 @@ namespace h2b {
 // all.  The pivot is the largest remaining Schur-complement diagonal (the
 // squared column norm a column-pivoted QR of XF would pick), so pivots and
 // rows of R equal those of ColPivHouseholderQR in exact arithmetic
-// (h2matrix.cpp:84); R goes to Rws row-major in pivoted column order, where
+// (h2matrix.cpp:27); R goes to Rws row-major in pivoted column order, where
 // k_cpqr leaves it, for k_basis_finish.  Once the Schur diagonal falls to
 // rounding noise of the FP64 Gram matrix (16 eps max diag), the pivots
 // still to be taken get the row [floor, 0, ..., 0] with floor =

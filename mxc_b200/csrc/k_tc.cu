@@ -154,7 +154,6 @@ __device__ __forceinline__ void convert_operand(const unsigned char* raw, int kc
 }  // namespace
 
 // Set when an mbarrier wait expired (read and cleared by the host).
-__device__ int g_tc_err = 0;
 
 // Warp-specialised variant, one CTA per SM (25 warps, 512 TMEM columns),
 // A operand in tensor memory, double-buffered accumulator.
@@ -342,7 +341,7 @@ __device__ __forceinline__ void prod_issue(const ProdChunks& pc, int k0, uint32_
 
 __global__ void __launch_bounds__(WS_NT, 1)
     k_tc_gemm_ws(const GemmTask<float>* __restrict__ tasks, const GemmEntry<float>* __restrict__ ents,
-                 const TileRef* __restrict__ tiles, int ntiles, int split) {
+                 const TileRef* __restrict__ tiles, int ntiles, int split, int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ __align__(8) uint64_t full[WS_ST], conv_full[WS_ST], stage_free[WS_ST], acc_full[2], acc_empty[2], drain;
   __shared__ uint32_t tmem_slot;
@@ -596,7 +595,7 @@ __global__ void __launch_bounds__(WS_NT, 1)
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (tid == 0 && abort_flag) atomicExch(&g_tc_err, 1);
+  if (tid == 0 && abort_flag && err) atomicExch(err, 1);
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(WS_TMEM_COLS) : "memory");
 }
@@ -604,7 +603,7 @@ __global__ void __launch_bounds__(WS_NT, 1)
 int tc_gemm_tile() { return TC_BM; }
 
 cudaError_t launch_tc_gemm(const GemmTask<float>* d_tasks, const GemmEntry<float>* d_ents, const TileRef* d_tiles,
-                           int ntiles, int split, cudaStream_t st) {
+                           int ntiles, int split, int* err, cudaStream_t st) {
   if (ntiles == 0) return cudaSuccess;
   cudaError_t e = cudaFuncSetAttribute(k_tc_gemm_ws, cudaFuncAttributeMaxDynamicSharedMemorySize, WS_SMEM);
   if (e != cudaSuccess) return e;
@@ -617,18 +616,8 @@ cudaError_t launch_tc_gemm(const GemmTask<float>* d_tasks, const GemmEntry<float
   }
   const int grid = ntiles < sms ? ntiles : sms;
   note_launch();
-  k_tc_gemm_ws<<<grid, WS_NT, WS_SMEM, st>>>(d_tasks, d_ents, d_tiles, ntiles, split);
+  k_tc_gemm_ws<<<grid, WS_NT, WS_SMEM, st>>>(d_tasks, d_ents, d_tiles, ntiles, split, err);
   return cudaGetLastError();
-}
-
-// Reads and clears the expired-wait flag (synchronises the stream).
-cudaError_t tc_gemm_take_error(int* flag, cudaStream_t st) {
-  cudaError_t e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return e;
-  e = cudaMemcpyFromSymbol(flag, g_tc_err, sizeof(int));
-  if (e != cudaSuccess) return e;
-  const int zero = 0;
-  return cudaMemcpyToSymbol(g_tc_err, &zero, sizeof(int));
 }
 
 }  // namespace h2b

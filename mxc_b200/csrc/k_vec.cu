@@ -233,10 +233,10 @@ cudaError_t launch_fma_probe(int precision, int blocks, int iters, void* out, cu
 
 namespace h2b {
 
-// solveRelErr (solver.cpp:276-285) per column: partial sums of (x - ref)^2
+// solveRelErr (solver.cpp:229-238) per column: partial sums of (x - ref)^2
 // and ref^2 over row chunks, then a fixed-order final sum (deterministic).
 constexpr i64 RELERR_ROWS = 16384;
-int relerr_chunks(i64 n) { return (int)((n + RELERR_ROWS - 1) / RELERR_ROWS); }
+i64 relerr_chunks(i64 n) { return (n + RELERR_ROWS - 1) / RELERR_ROWS; }
 
 __global__ void __launch_bounds__(256) k_relerr_partial(const double* __restrict__ X, const double* __restrict__ ref,
                                                         i64 n, i64 ld, double* __restrict__ partial) {
@@ -272,7 +272,8 @@ __global__ void k_relerr_final(const double* __restrict__ partial, int nch, int 
 
 cudaError_t launch_relerr(const double* X, const double* ref, i64 n, i64 ld, int nrhs, double* partial, double* out,
                           cudaStream_t st) {
-  const int nch = relerr_chunks(n);
+  if (relerr_chunks(n) > 0x7fffffff || nrhs > 65535) return cudaErrorInvalidValue;
+  const int nch = (int)relerr_chunks(n);
   dim3 grid(nch, nrhs);
   note_launch();
   k_relerr_partial<<<grid, 256, 0, st>>>(X, ref, n, ld, partial);

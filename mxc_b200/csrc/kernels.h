@@ -142,11 +142,11 @@ cudaError_t launch_sum_parts(const SumTask<T>* d_tasks, int ntasks, int maxmn, c
 int gemm_tile_n(int shape);
 // FP32 segmented GEMM on the tcgen05 tensor cores, 128 x 128 output tiles
 // (TileRef over tc_gemm_tile()-sized tiles); split = 1: 3-term TF32 split
-// (FP32 accuracy), 0: one TF32 product.
+// (FP32 accuracy), 0: one TF32 product.  A CTA whose bounded wait expired
+// sets *err to 1 (err: a device int owned by the caller, may be null).
 cudaError_t launch_tc_gemm(const GemmTask<float>* d_tasks, const GemmEntry<float>* d_ents, const TileRef* d_tiles,
-                           int ntiles, int split, cudaStream_t st);
+                           int ntiles, int split, int* err, cudaStream_t st);
 int tc_gemm_tile();
-cudaError_t tc_gemm_take_error(int* flag, cudaStream_t st);
 // FP64 segmented GEMM on the FP64 tensor cores (mma.sync m8n8k4), 64 x 64
 // output tiles (TileRef over dgemm_tile()-sized tiles).
 cudaError_t launch_dgemm(const GemmTask<double>* d_tasks, const GemmEntry<double>* d_ents, const TileRef* d_tiles,
@@ -175,7 +175,7 @@ struct LuTask {
   T* invT;   // receives A^{-1} transposed (column-major, ld = ldinv)
   i64 ldinv;
   int* ipiv;  // n
-  int* info;  // 1 when |det| <= DBL_MIN (h2matrix.cpp:441)
+  int* info;  // 1 when |det| <= DBL_MIN (h2matrix.cpp:384)
 };
 template <typename T>
 cudaError_t launch_lu_inverse(const LuTask<T>* d_tasks, int ntasks, int maxn, cudaStream_t st);
@@ -196,7 +196,7 @@ cudaError_t launch_axpby(double* y, const double* x, double a, double b, i64 n, 
 cudaError_t launch_residual_norm_finish(const double* nrm2, const double* normb, double* resid, int nrhs,
                                         cudaStream_t st);
 
-int relerr_chunks(i64 n);
+i64 relerr_chunks(i64 n);
 // partial: 2 * relerr_chunks(n) * nrhs doubles of scratch; out: nrhs doubles (device)
 cudaError_t launch_relerr(const double* X, const double* ref, i64 n, i64 ld, int nrhs, double* partial, double* out,
                           cudaStream_t st);

@@ -151,8 +151,6 @@ int main(int argc, char* argv[]) {
     double h2_factor_time = now_s();
     matM.factorizeM();
     h2_factor_time = now_s() - h2_factor_time;
-    for (long long l = levels; l >= 0; l--)
-      if (matM.info[(size_t)l]) std::cout << "singularity detected at level " << l << "." << std::endl;
     X1 = X2;
 
     double h2_sub_time = now_s();
@@ -175,20 +173,10 @@ int main(int argc, char* argv[]) {
     std::cout << "GMRES Time: " << gmres_time << ", Comm: " << 0. << std::endl;
     for (long long i = 0; i <= matA.iters; i++) std::cout << "iter " << i << ": " << matA.resid[(size_t)i] << std::endl;
 
-    if (csv != nullptr) {
-      // The reference's CSV row (one process: mpi_size 1, comm times 0).
-      std::ofstream f(csv, std::ios_base::app);
-      if (f) {
-        f << 1 << ',' << Nbody << ',' << theta << ',' << leaf_size << ',' << rank << ',' << epi << ',' << mode << ',';
-        f << cerr << ',' << h2_construct_time << ',' << 0. << ',' << matvec_time << ',' << 0. << ',' << refmatvec_time
-          << ',';
-        f << m_construct_time << ',' << 0. << ',' << cerr_m << ',' << h2_factor_time << ',' << 0. << ',' << h2_sub_time
-          << ',' << 0. << ',' << serr << ',';
-        f << matA.resid[(size_t)matA.iters] << ',' << matA.iters << ',' << gmres_time << ',' << 0.;
-        for (long long i = 0; i <= matA.iters; i++) f << ',' << matA.resid[(size_t)i];
-        f << std::endl;
-      }
-    }
+    if (csv != nullptr)  // one process: mpi_size 1, comm times 0
+      write_to_csv(csv, 1, Nbody, theta, leaf_size, rank, epi, mode.data(), cerr, h2_construct_time, 0., matvec_time,
+                   0., refmatvec_time, m_construct_time, 0., cerr_m, h2_factor_time, 0., h2_sub_time, 0., serr,
+                   matA.resid[(size_t)matA.iters], (double)matA.iters, gmres_time, 0., matA.resid.data());
   } catch (const std::exception& e) {
     std::fprintf(stderr, "lorasp: %s\n", e.what());
     return 1;

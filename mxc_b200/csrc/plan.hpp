@@ -28,7 +28,7 @@ struct PairCSR {
 
 // std::mt19937 + uniform_real_distribution(0, diameter), test_funcs.hpp:31-41.
 void uniform_unit_cube_rnd(double* bodies, i64 n, double diameter, i64 dim, unsigned seed);
-// Default-seeded std::mt19937_64 + uniform_real_distribution(0,1), main.cpp:358-361.
+// Default-seeded std::mt19937_64 + uniform_real_distribution(0,1), main.cpp:73-76.
 void uniform_rhs(double* x, i64 n);
 
 // buildBinaryTree (build_tree.cpp:67-99): sorts bodies in place.

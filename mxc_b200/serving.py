@@ -15,11 +15,16 @@ their kernels overlap on the GPU.  Every batch runs at the full batch width
 system's launch plans are built once.
 
 Admission: a system's footprint is the device memory its handle holds
-after build, factorization and a warm-up solve (`Handle.memory`).  When a
-new system does not fit in the budget, idle systems are evicted in
-least-recently-used order (their solvers and handle are freed); a request
-for an evicted system rebuilds it under the same rule.  Latency is measured
-per request from `submit` to the completion of its last column.
+after build, factorization and a warm-up solve (`Handle.memory`).  Before a
+system is built, room for it is made under the budget: its footprint is
+taken from an earlier build of the same system, else from a conservative
+per-body estimate, and idle systems are evicted in least-recently-used order
+(their solvers and handle are freed) until that much is free; the room stays
+reserved while the build runs, so concurrent admissions cannot overcommit,
+and the measured footprint replaces the reservation afterwards (evicting
+more if the build came out larger).  A request for an evicted system
+rebuilds it under the same rule.  Latency is measured per request from
+`submit` to the completion of its last column.
 
 Each column's GMRES is independent of the others in its batch (the batched
 GMRES keeps one Krylov basis, Hessenberg matrix and convergence test per
@@ -75,6 +80,15 @@ class SystemSpec:
 
 class ResidentSystem:
     """A built, factored system on its own device handle."""
+
+    # Device bytes per body of a built system (operator at eps 1e-8 and an
+    # FP32 rank-100 preconditioner held about 190 KB per body at 8,192 to
+    # 262,144 bodies): the admission estimate before a first build.
+    BYTES_PER_BODY_ESTIMATE = 256 * 1024
+
+    @classmethod
+    def estimate_footprint(cls, spec: SystemSpec) -> int:
+        return int(cls.BYTES_PER_BODY_ESTIMATE * spec.points.shape[0])
 
     def __init__(self, spec: SystemSpec, max_batch: int, warm: bool = True):
         self.spec = spec
@@ -135,7 +149,8 @@ class Server:
     """Continuous-batching solve server over resident systems."""
 
     def __init__(self, hbm_budget_bytes: int, max_batch: int = 16, workers: int = 2, inner: int = 10,
-                 outer: int = 50, build_system: Optional[Callable[[SystemSpec, int], "ResidentSystem"]] = None):
+                 outer: int = 50, build_system: Optional[Callable[[SystemSpec, int], "ResidentSystem"]] = None,
+                 estimate_footprint: Optional[Callable[[SystemSpec], int]] = None):
         self.budget = int(hbm_budget_bytes)
         self.max_batch = max_batch
         self.inner, self.outer = inner, outer
@@ -154,13 +169,22 @@ class Server:
         # close(); ResidentSystem by default (other builders serve host-side tests of the scheduler).
         builder = build_system or ResidentSystem
         self._builder: Callable[[SystemSpec], ResidentSystem] = lambda s: builder(s, self.max_batch)
+        # Footprint assumed for a system never built before: ResidentSystem's
+        # per-body estimate by default; with another builder, the given
+        # estimate or none (then room is made once the build is measured).
+        if estimate_footprint is None:
+            estimate_footprint = ResidentSystem.estimate_footprint if build_system is None else (lambda spec: 0)
+        self._estimate: Callable[[SystemSpec], int] = estimate_footprint
+        self._footprint_seen: Dict[int, int] = {}  # sid -> measured footprint of its last build
+        self._reserved: Dict[int, int] = {}  # sid -> bytes held for a build in progress
         self._workers = [threading.Thread(target=self._work, daemon=True) for _ in range(workers)]
         for w in self._workers:
             w.start()
 
     # ------------------------------------------------------------ admission
     def resident_bytes(self) -> int:
-        return sum(s.footprint for s in self._sys.values())
+        """Footprints of the resident systems plus room reserved for builds in progress."""
+        return sum(s.footprint for s in self._sys.values()) + sum(self._reserved.values())
 
     def _evict_for(self, need: int, keep: int) -> None:
         """Evicts idle systems, least recently used first, until `need` more
@@ -174,8 +198,21 @@ class Server:
 
     def _admit(self, sid: int) -> ResidentSystem:
         spec = self._specs[sid]
-        system = self._builder(spec)
         with self._lock:
+            # Make room before building: the build allocates all of its
+            # device memory, so evicting afterwards would overshoot the budget.
+            need = self._footprint_seen.get(sid) or self._estimate(spec)
+            self._evict_for(need, keep=sid)
+            self._reserved[sid] = need
+        try:
+            system = self._builder(spec)
+        except BaseException:
+            with self._lock:
+                self._reserved.pop(sid, None)
+            raise
+        with self._lock:
+            self._reserved.pop(sid, None)
+            self._footprint_seen[sid] = system.footprint
             try:
                 self._evict_for(system.footprint, keep=sid)
             except MemoryError:
@@ -240,6 +277,9 @@ class Server:
                 width = 0
                 tol = None
                 for req in list(self._queue[sid]):
+                    if req.future.done():  # failed earlier: drop its remaining columns
+                        self._queue[sid].remove(req)
+                        continue
                     if width >= self.max_batch:
                         break
                     if tol is not None and req.tol != tol:
@@ -269,6 +309,9 @@ class Server:
                     self._batches += 1
                     c = 0
                     for req, c0, k in parts:
+                        if req.future.done():  # failed in another batch; its columns here are discarded
+                            c += k
+                            continue
                         req.X[:, c0:c0 + k] = X[:, c:c + k]
                         for j in range(k):
                             req.resid[c0 + j] = resid[int(iters[c + j]), c + j]
@@ -281,11 +324,16 @@ class Server:
                             finished.append((req, lat))
                     self._last_use[sid] = t_done
                 for req, lat in finished:
-                    req.future.set_result((req.X, req.resid, lat))
-            except BaseException as e:  # propagate to every request in the batch
-                for req, _, _ in parts:
                     if not req.future.done():
-                        req.future.set_exception(e)
+                        req.future.set_result((req.X, req.resid, lat))
+            except BaseException as e:  # propagate to every request in the batch
+                with self._lock:
+                    for req, _, _ in parts:
+                        if not req.future.done():
+                            req.future.set_exception(e)
+                        # a failed request's columns still queued go nowhere
+                        if req in self._queue[sid]:
+                            self._queue[sid].remove(req)
             finally:
                 with self._lock:
                     self._busy.discard(sid)

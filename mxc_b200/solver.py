@@ -21,7 +21,7 @@ def _ptr(a: np.ndarray):
 
 
 class Tree:
-    """Cells of buildBinaryTree (build_tree.cpp:93-125) as flat arrays."""
+    """Cells of buildBinaryTree (build_tree.cpp:67-99) as flat arrays."""
 
     def __init__(self, levels: int, child: np.ndarray, body: np.ndarray, R: np.ndarray, Cc: np.ndarray):
         self.levels = levels
@@ -43,7 +43,7 @@ def uniform_unit_cube_rnd(n: int, seed: int, diameter: float = 1.0, dim: int = 3
 
 
 def uniform_rhs(n: int) -> np.ndarray:
-    """main.cpp:358-361 (default-seeded std::mt19937_64, uniform[0,1))."""
+    """main.cpp:73-76 (default-seeded std::mt19937_64, uniform[0,1))."""
     x = np.empty(n, dtype=np.float64)
     L.check(L.lib().h2_uniform_rhs(_ptr(x), n), "h2_uniform_rhs")
     return x
@@ -67,7 +67,7 @@ def build_tree(bodies: np.ndarray, levels: int) -> Tree:
 
 
 def pair_csr(kind: str, tree: Tree, theta: float):
-    """CSR::CSR (build_tree.cpp:67-84): (RowIndex, ColIndex) of the near or far pairs."""
+    """CSR::CSR (build_tree.cpp:41-58): (RowIndex, ColIndex) of the near or far pairs."""
     row = np.zeros(tree.ncells + 1, dtype=np.int64)
     nnz = C.c_int64()
     args = (kind.encode(), tree.ncells, _ptr(tree.child), _ptr(tree.body), _ptr(tree.R), _ptr(tree.C), theta)
@@ -262,7 +262,7 @@ class H2MatrixSolver:
 
     @staticmethod
     def solveRelErr(X: np.ndarray, ref: np.ndarray) -> float:
-        """solver.cpp:276-285 (host-side reduction of two vectors)."""
+        """solver.cpp:229-238 (host-side reduction of two vectors)."""
         d = np.asarray(X) - np.asarray(ref)
         return math.sqrt(float(np.sum(d * d)) / float(np.sum(np.asarray(ref) ** 2)))
 
@@ -318,7 +318,7 @@ class H2MatrixSolver:
 
 
 def rel_err_device(handle: Handle, xptr: int, refptr: int, n: int, nrhs: int, ld: int) -> np.ndarray:
-    """solveRelErr (solver.cpp:276-285) of nrhs device columns; returns host values."""
+    """solveRelErr (solver.cpp:229-238) of nrhs device columns; returns host values."""
     out = np.zeros(nrhs)
     L.check(L.lib().h2dev_solve_rel_err_device(handle.h, n, nrhs, C.c_void_p(xptr), C.c_void_p(refptr), ld, _ptr(out)),
             "h2dev_solve_rel_err_device")

@@ -33,7 +33,7 @@ import numpy as np
 import scipy.linalg as sla
 
 # --------------------------------------------------------------------------
-# Random inputs (test_funcs.hpp:31-41, main.cpp:358-361)
+# Random inputs (test_funcs.hpp:31-41, main.cpp:73-76)
 # --------------------------------------------------------------------------
 
 
@@ -60,7 +60,7 @@ def uniform_unit_cube_rnd(n: int, seed: int, diameter: float = 1.0, dim: int = 3
 
 
 class _MT19937_64:
-    """std::mt19937_64 with the default seed 5489 (used by main.cpp:358)."""
+    """std::mt19937_64 with the default seed 5489 (used by main.cpp:73)."""
 
     N, M = 312, 156
     A = np.uint64(0xB5026F5AA96619E9)
@@ -105,7 +105,7 @@ class _MT19937_64:
 
 
 def xbody_uniform(n: int) -> np.ndarray:
-    """Default-seeded mt19937_64 + uniform_real_distribution(0,1): main.cpp:358-361."""
+    """Default-seeded mt19937_64 + uniform_real_distribution(0,1): main.cpp:73-76."""
     g = _MT19937_64().draws(n)
     u = g.astype(np.float64) / 18446744073709551616.0
     return np.where(u >= 1.0, np.nextafter(1.0, 0.0), u)
@@ -290,7 +290,7 @@ def far_body_lists(cells: Cells, far: CSR, levels: int):
     """Per box: the list of far body *ranges* (parent's list, then own far boxes).
 
     Returned as {cell: [(b0, b1), ...]} for every cell at levels 1..L; the
-    root (level 0) has none (its Hmatrix is never constructed, solver.cpp:78).
+    root (level 0) has none (its Hmatrix is never constructed, solver.cpp:31).
     """
     lists = {0: []}
     for l in range(1, levels + 1):
@@ -614,7 +614,7 @@ class H2MatrixSolver:
     """solver.hpp:11-47 / solver.cpp restated for one process.
 
     ``eps`` follows the reference: eps == 0 selects the fixed-rank,
-    orthogonal-basis preconditioner mode (solver.cpp:75-83) with far lists
+    orthogonal-basis preconditioner mode (solver.cpp:28-36) with far lists
     from weak admissibility; eps > 0 selects the ID operator mode.
     """
 

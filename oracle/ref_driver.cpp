@@ -7,7 +7,7 @@
 // Output layout (little-endian, all int64 unless noted):
 //   N, levels, ncells
 //   bodies    (N*3 f64, tree-sorted, as buildBinaryTree leaves them)
-//   xbody     (N f64, mt19937_64 default seed, uniform[0,1), main.cpp:358-361)
+//   xbody     (N f64, mt19937_64 default seed, uniform[0,1), main.cpp:73-76)
 //   cells     ncells x (child0, child1, body0, body1) int64, R (3 f64), C (3 f64)
 //   for each list in (Near theta, Far theta, Far 0):
 //     nrow = ncells+1, RowIndex[nrow], nnz, ColIndex[nnz]

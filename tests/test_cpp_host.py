@@ -41,7 +41,7 @@ int main() {
   for (long long i = 0; i < 3 * n; i++) std::printf("%.17g\n", b[i]);
   mesh_sphere(s.data(), 7, 2.0);
   for (int i = 0; i < 21; i++) std::printf("%.17g\n", s[i]);
-  std::printf("%.17g %.17g\n", Laplace3D(0.5)(0.), Yukawa3D(1., 2.)(0.5));
+  std::printf("%.17g %.17g\n", Laplace3D(0.5)(0.).real(), Yukawa3D(1., 2.)(0.5).real());
   return 0;
 }
 """
@@ -134,3 +134,117 @@ def test_lorasp_runs_the_reference_flow_and_matches_the_python_api(tmp_path, han
     M.close()
     assert abs(cerr - cerr_py) <= 1e-3 * cerr_py, (cerr, cerr_py)
     assert abs(serr - serr_py) <= 1e-4 * serr_py, (serr, serr_py)
+
+
+# The reference's main.cpp call sequence, written only against the
+# reference's own header names and signatures (solver.hpp, test_funcs.hpp,
+# kernel.hpp, comm-mpi.hpp): MPI_Init, a DenseZMat filled by gen_matrix,
+# H2MatrixSolver(denseA, eval, epi, rank, leveled_rank, cell, theta, body,
+# levels), matVecMul against op_Aij_mulB, the preconditioner by copy-style
+# assignment, factorizeM, solvePrecondition, solveGMRES, solveRelErr,
+# ColCommMPI::get_comm_time, write_to_csv, free_all_comms, MPI_Finalize.
+REF_PROGRAM = r"""
+#include <solver.hpp>
+#include <test_funcs.hpp>
+#include <cmath>
+#include <complex>
+#include <iostream>
+#include <random>
+#include <string>
+#include <vector>
+int main(int argc, char* argv[]) {
+  MPI_Init(&argc, &argv);
+  long long Nbody = 2048, leaf_size = 256, rank = 100, leveled_rank = 0;
+  double theta = 2., epi = 1e-10;
+  std::string mode = "h2";
+  const char* csv = argc > 1 ? argv[1] : nullptr;
+  long long levels = (long long)std::log2((double)Nbody / leaf_size);
+  long long Nleaf = (long long)1 << levels, ncells = Nleaf + Nleaf - 1;
+  Laplace3D eval(1e-4);
+  std::vector<double> body(Nbody * 3);
+  std::vector<std::complex<double>> Xbody(Nbody);
+  std::vector<Cell> cell(ncells);
+  uniform_unit_cube_rnd(&body[0], Nbody, 1, 3, 999);
+  buildBinaryTree(&cell[0], &body[0], Nbody, levels);
+  std::mt19937_64 gen;
+  std::uniform_real_distribution<double> uniform_dist(0., 1.);
+  for (auto& x : Xbody) x = std::complex<double>(uniform_dist(gen), 0.);
+  DenseZMat denseA(Nbody, Nbody);
+  gen_matrix(eval, Nbody, Nbody, &body[0], &body[0], denseA.A);
+  MPI_Barrier(MPI_COMM_WORLD);
+  double t0 = MPI_Wtime();
+  H2MatrixSolver matA(denseA, eval, epi, rank, leveled_rank, cell, theta, &body[0], levels);
+  double h2_construct_time = MPI_Wtime() - t0;
+  long long lenX = matA.local_bodies.second - matA.local_bodies.first;
+  std::vector<std::complex<double>> X1(lenX, std::complex<double>(0., 0.)), X2(lenX, std::complex<double>(0., 0.));
+  std::copy(&Xbody[matA.local_bodies.first], &Xbody[matA.local_bodies.second], &X1[0]);
+  matA.matVecMul(&X1[0]);
+  denseA.op_Aij_mulB('N', lenX, 1, Nbody, matA.local_bodies.first, 0, &Xbody[0], Nbody, &X2[0], lenX);
+  double cerr = H2MatrixSolver::solveRelErr(lenX, &X1[0], &X2[0]);
+  int mpi_rank = 0, mpi_size = 1;
+  MPI_Comm_rank(MPI_COMM_WORLD, &mpi_rank);
+  MPI_Comm_size(MPI_COMM_WORLD, &mpi_size);
+  std::cout << "Construct Err: " << cerr << std::endl;
+  H2MatrixSolver matM;
+  if (mode.compare("h2") == 0)
+    matM = H2MatrixSolver(denseA, eval, 0., rank, leveled_rank, cell, theta, &body[0], levels);
+  std::copy(&Xbody[matM.local_bodies.first], &Xbody[matM.local_bodies.second], &X1[0]);
+  matM.matVecMul(&X1[0]);
+  double cerr_m = H2MatrixSolver::solveRelErr(lenX, &X1[0], &X2[0]);
+  matM.factorizeM();
+  std::copy(X2.begin(), X2.end(), X1.begin());
+  matM.solvePrecondition(&X1[0]);
+  double serr = H2MatrixSolver::solveRelErr(lenX, &X1[0], &Xbody[matM.local_bodies.first]);
+  std::fill(X1.begin(), X1.end(), std::complex<double>(0., 0.));
+  std::cout << "H^2-Preconditioner Construct Err: " << cerr_m << std::endl;
+  std::cout << "H^2-Matrix Substitution Err: " << serr << std::endl;
+  matA.solveGMRES(epi, matM, &X1[0], &X2[0], 10, 50);
+  double xerr = H2MatrixSolver::solveRelErr(lenX, &X1[0], &Xbody[0]);
+  std::cout << "GMRES Residual: " << matA.resid[matA.iters] << ", Iters: " << matA.iters << std::endl;
+  std::cout << "Solution Err: " << xerr << std::endl;
+  std::cout << "Levels: " << matA.A.size() << " " << matA.A[levels].Dims.size() << " " << matA.A[levels].ARows.back()
+            << " " << ColCommMPI::get_comm_time() << std::endl;
+  if (csv != nullptr)
+    write_to_csv(csv, mpi_size, Nbody, theta, leaf_size, rank, epi, mode.data(), cerr, h2_construct_time, 0., 0., 0.,
+                 0., 0., 0., cerr_m, 0., 0., 0., 0., serr, matA.resid[matA.iters], matA.iters, 0., 0.,
+                 matA.resid.data());
+  matA.free_all_comms();
+  matM.free_all_comms();
+  MPI_Finalize();
+  return 0;
+}
+"""
+
+
+def _compile_ref(tmp_path):
+    src = tmp_path / "ref_main.cpp"
+    src.write_text(REF_PROGRAM)
+    exe = tmp_path / "ref_main"
+    r = subprocess.run(["g++", "-std=c++17", "-I" + os.path.join(ROOT, "include", "mxc_b200", "reference"),
+                        str(src), "-o", str(exe), "-L" + LIBDIR, "-lmxcb200", "-Wl,-rpath," + LIBDIR],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def test_reference_signature_program_compiles(tmp_path):
+    """main.cpp's calls, with only the reference's header names on the
+    include path, compile and link against the library."""
+    _compile_ref(tmp_path)
+
+
+@pytest.mark.gpu
+def test_reference_signature_program_runs(tmp_path):
+    exe = _compile_ref(tmp_path)
+    csv = tmp_path / "ref.csv"
+    r = subprocess.run([str(exe), str(csv)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    out = r.stdout
+    assert _value(out, "Construct Err:") < 1e-9
+    assert _value(out, "GMRES Residual:") < 1e-10
+    assert _value(out, "Solution Err:") < 1e-8
+    lv = re.search(r"Levels: (\d+) (\d+) (\d+) (\S+)", out)
+    assert int(lv.group(1)) == 4 and int(lv.group(2)) == 8 and int(lv.group(3)) > 8 and float(lv.group(4)) == 0.0
+    row = csv.read_text().strip().split(",")
+    iters = int(re.search(r"Iters: (\d+)", out).group(1))
+    assert len(row) == 25 + iters + 1 and row[0] == "1" and row[6] == "h2"

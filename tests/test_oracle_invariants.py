@@ -95,7 +95,7 @@ def test_colpiv_rank_zero_matrix_and_threshold_rules():
 
 
 def test_compute_basis_identity_when_full_rank():
-    """rank == M: Q = I, R = upper(Q_in) (h2matrix.cpp:114-117)."""
+    """rank == M: Q = I, R = upper(Q_in) (h2matrix.cpp:57-60)."""
     rng = np.random.default_rng(5)
     X = rng.random((8, 3))
     F = rng.random((40, 3)) + 3.0

@@ -100,6 +100,57 @@ def test_admission_evicts_least_recently_used_idle_system_and_readmits():
         srv.close()
 
 
+def test_admission_makes_room_before_building():
+    """With an estimate, idle systems are evicted before the new one is
+    built, so the build never runs on top of a full budget."""
+    FakeSystem.built = []
+    seen = []
+    holder = {}
+
+    def build(s, mb):
+        srv_ = holder["srv"]
+        seen.append(sum(x.footprint for x in srv_._sys.values()))
+        return FakeSystem(s, mb, footprint=40)
+
+    srv = S.Server(hbm_budget_bytes=100, max_batch=4, workers=1, build_system=build,
+                   estimate_footprint=lambda sp: 40)
+    holder["srv"] = srv
+    try:
+        for i in range(3):
+            srv.add_system(spec(seed=i))
+        # the third build saw at most 60 bytes resident (one system evicted first)
+        assert seen == [0, 40, 40] and srv.resident_bytes() <= 100
+    finally:
+        srv.close()
+
+
+class FailingSystem(FakeSystem):
+    def solve(self, B, tol, inner, outer):
+        if len(self.widths) == 0:
+            self.widths.append(B.shape[1])
+            raise RuntimeError("injected device failure")
+        return super().solve(B, tol, inner, outer)
+
+
+def test_failed_batch_drops_the_rest_of_its_requests():
+    """A request split over batches fails with its first batch; its queued
+    columns are dropped and later batches complete the other requests."""
+    FakeSystem.built = []
+    srv = S.Server(hbm_budget_bytes=100, max_batch=4, workers=1,
+                   build_system=lambda s, mb: FailingSystem(s, mb, delay=0.05))
+    try:
+        sid = srv.add_system(spec())
+        big = srv.submit(sid, np.ones((50, 10)))  # 3 batches; the first fails
+        others = [srv.submit(sid, np.full((50, 2), float(i))) for i in range(3)]
+        with pytest.raises(RuntimeError):
+            big.result(timeout=10)
+        for i, f in enumerate(others):
+            X, _, _ = f.result(timeout=10)
+            np.testing.assert_array_equal(X, np.full((50, 2), i / 2.0))
+    finally:
+        srv.close()
+
+
 def test_system_larger_than_budget_is_refused():
     srv = S.Server(hbm_budget_bytes=5, max_batch=4, workers=1, build_system=lambda s, mb: FakeSystem(s, mb))
     try:
