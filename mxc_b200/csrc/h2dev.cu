@@ -1502,7 +1502,7 @@ class Solver : public SolverBase {
   }
 
   // ------------------------------------------------------------ factor
-  // h2matrix.cpp:346-425 for one level, then factorizeCopyNext (484-503).
+  // h2matrix.cpp:346-425 for one level (factorizeCopyNext, 427-446, is copy_next).
   void factor_level(i64 l) {
     Level<T>& lv = L[l];
     const i64 nodes = lv.nodes;
@@ -1524,7 +1524,12 @@ class Solver : public SolverBase {
       poff[i + 1] = poff[i] + Mr;
     }
     lv.B.alloc(std::max<i64>(1, lv.boff[nodes]));
-    lv.invT.alloc(std::max<i64>(1, lv.ioff[nodes]));
+    // Global LU scratch only for redundant blocks too large for the solve
+    // kernel's shared memory; released at the end of the level.
+    i64 maxMr = 0;
+    for (i64 i = 0; i < nodes; i++) maxMr = std::max(maxMr, D[i] - Rk[i]);
+    const bool lu_in_smem = (double)sizeof(T) * maxMr * (maxMr + 1) + 8. * maxMr + 16. <= 200. * 1024.;
+    lv.invT.alloc(lu_in_smem ? 1 : std::max<i64>(1, lv.ioff[nodes]));
     lv.ipiv.alloc(std::max<i64>(1, poff[nodes]));
     lv.info.alloc(nodes);
     lv.info.zero(st());
@@ -1532,7 +1537,7 @@ class Solver : public SolverBase {
     T* Q = lv.Q.p;
     T* V = lv.R.p;  // V stored transposed: V^T column-major
     // Steps 1-2: A_ii <- U^T A_ii U.
-    GemmPlan<T> s1, s2, s5, s6, s7, s8;
+    GemmPlan<T> s1, s2, s6, s7, s8;
     CopyPlan<T> c3, c8;
     for (i64 i = 0; i < nodes; i++) {
       const int M = (int)D[i];
@@ -1549,18 +1554,25 @@ class Solver : public SolverBase {
     s2.finalize();
     s1.run(st());
     s2.run(st());
-    // Step 3: V^T[:, :Ms] = U_s.  Step 4: LU and inverse of A_rr.
-    std::vector<LuTask<T>> lt;
+    // Step 3: V^T[:, :Ms] = U_s.  Steps 4-5: PartialPivLU of A_rr and
+    // V_r = A_rr^{-1} U_r^T by its triangular solves (h2matrix.cpp:377-379);
+    // V_r is stored as V^T[:, Ms:], row r of V_r contiguous, as U_r^T is in
+    // Q[:, Ms:].
+    std::vector<LuSolveTask<T>> lt;
     for (i64 i = 0; i < nodes; i++) {
       const int M = (int)D[i], Ms = (int)Rk[i], Mr = M - Ms;
       if (M == 0) continue;
       c3.add(Q + lv.qoff[i], M, V + lv.qoff[i], M, M, Ms);
-      LuTask<T> t;
+      LuSolveTask<T> t;
       t.A = A + lv.aoff[lv.diag[i]] + Ms + (i64)Ms * M;
       t.lda = M;
       t.n = Mr;
-      t.invT = lv.invT.p + lv.ioff[i];
-      t.ldinv = Mr > 0 ? Mr : 1;
+      t.B = Q + lv.qoff[i] + (i64)Ms * M;
+      t.ldb = M;
+      t.m = M;
+      t.X = V + lv.qoff[i] + (i64)Ms * M;
+      t.ldx = M;
+      t.work = lu_in_smem ? nullptr : lv.invT.p + lv.ioff[i];
       t.ipiv = lv.ipiv.p + poff[i];
       t.info = lv.info.p + i;
       lt.push_back(t);
@@ -1568,27 +1580,15 @@ class Solver : public SolverBase {
     c3.finalize();
     c3.run(st());
     {
-      DVec<LuTask<T>> dl;
+      DVec<LuSolveTask<T>> dl;
       dl.upload(lt);
       double fl = 0.;
-      for (const auto& t : lt) fl += 8. / 3. * (double)t.n * t.n * t.n;
-      {
-        Prof pf("lu_inverse", fl, 0.);
-        int maxn = 0;
-        for (const auto& x : lt) maxn = std::max(maxn, x.n);
-        ck(launch_lu_inverse<T>(dl.p, (int)lt.size(), maxn, st()), "lu_inverse");
-      }
+      for (const auto& t : lt) fl += 2. / 3. * (double)t.n * t.n * t.n + 2. * (double)t.n * t.n * t.m;
+      Prof pf("lu_solve", fl, 0.);
+      int maxn = 0;
+      for (const auto& x : lt) maxn = std::max(maxn, x.n);
+      ck(launch_lu_solve<T>(dl.p, (int)lt.size(), maxn, st()), "lu_solve");
     }
-    // Step 5: V^T[:, Ms:] = U_r (A_rr^{-1})^T.
-    for (i64 i = 0; i < nodes; i++) {
-      const int M = (int)D[i], Ms = (int)Rk[i], Mr = M - Ms;
-      if (M == 0 || Mr == 0) continue;
-      s5.add_task(V + lv.qoff[i] + (i64)Ms * M, M, M, Mr, T(0));
-      s5.add_entry(Q + lv.qoff[i] + (i64)Ms * M, M, 0, lv.invT.p + lv.ioff[i], Mr, 0, Mr, T(1));
-    }
-    s5.name = "gemm_factor";
-    s5.finalize();
-    s5.run(st());
     // Steps 6-8.
     for (i64 i = 0; i < nodes; i++) {
       const int M = (int)D[i], Ms = (int)Rk[i], Mr = M - Ms;
@@ -1723,6 +1723,7 @@ class Solver : public SolverBase {
       s10.run(st());
       s11b.run(st());
     }
+    lv.invT.release();
   }
 
   void copy_next(i64 l) {

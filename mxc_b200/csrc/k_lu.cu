@@ -270,6 +270,172 @@ __global__ void __launch_bounds__(NP * NP / 64) k_gj_reg(const LuTask<T>* __rest
   }
 }
 
+// LU with partial pivoting of A_rr and the solve A_rr V_r = U_r^T
+// (h2matrix.cpp:377-379: PartialPivLU, then solve).  One CTA per box.
+// Factorization: the unblocked right-looking partial-pivot LU (pivot = first
+// row of largest magnitude in column k among rows k..n-1; the column below
+// the pivot divided by it; rank-1 update of the trailing block), in shared
+// memory when the block fits and otherwise in the task's global scratch.
+// Solve: the row interchanges applied to the right-hand sides, then the
+// unit-lower forward and the upper backward substitution, one warp per 32
+// right-hand-side columns (lane = column), 32 rows at a time in registers,
+// left-looking across row blocks (each earlier row block read back once).
+// Right-hand sides and solution have row r contiguous over the columns
+// (B[c + r ldb]), as U_r^T and V_r are laid out in the ULV.  info follows
+// Eigen's determinant rule (product of U's diagonal, sign of the
+// permutation, |det| <= DBL_MIN).
+template <typename T, bool SMEM>
+__global__ void __launch_bounds__(256, 2) k_lu_solve(const LuSolveTask<T>* __restrict__ tasks) {
+  const LuSolveTask<T> t = tasks[blockIdx.x];
+  const int n = t.n, m = t.m;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+  __shared__ double red_v[32];
+  __shared__ int red_i[32];
+  __shared__ double s_det;
+  __shared__ int s_swaps;
+  if (n <= 0) {
+    if (tid == 0) *t.info = 0;
+    return;
+  }
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const i64 ld = SMEM ? n + 1 : n;
+  T* a = SMEM ? reinterpret_cast<T*>(smem_raw) : t.work;
+  int* piv = SMEM ? reinterpret_cast<int*>(a + (size_t)n * ld) : reinterpret_cast<int*>(smem_raw);
+  int* prow = piv + n;  // row of the right-hand sides that lands in row i of P B
+  for (int c = warp; c < n; c += nw)
+    for (int r = lane; r < n; r += 32) a[r + (i64)c * ld] = t.A[r + (i64)c * t.lda];
+  if (!SMEM) __threadfence_block();
+  if (tid == 0) {
+    s_det = 1.;
+    s_swaps = 0;
+  }
+  __syncthreads();
+  for (int k = 0; k < n; k++) {
+    double bv = -1.;
+    int bi = 0x7fffffff;
+    for (int r = k + tid; r < n; r += nt) {
+      const double v = fabs((double)a[r + (i64)k * ld]);
+      if (v > bv) { bv = v; bi = r; }
+    }
+    argmax_first(bv, bi, red_v, red_i);
+    if (bi < k || bi >= n) bi = k;  // a column of NaNs: no swap
+    if (bi != k)
+      for (int c = tid; c < n; c += nt) {
+        const T x = a[k + (i64)c * ld];
+        a[k + (i64)c * ld] = a[bi + (i64)c * ld];
+        a[bi + (i64)c * ld] = x;
+      }
+    if (!SMEM) __threadfence_block();
+    __syncthreads();
+    const T p = a[k + (i64)k * ld];
+    if (tid == 0) {
+      piv[k] = bi;
+      s_det *= (double)p;
+      s_swaps += bi != k;
+    }
+    if (p != T(0))
+      for (int r = k + 1 + tid; r < n; r += nt) a[r + (i64)k * ld] = a[r + (i64)k * ld] / p;
+    if (!SMEM) __threadfence_block();
+    __syncthreads();
+    for (int c = k + 1 + warp; c < n; c += nw) {
+      T* ac = a + (i64)c * ld;
+      const T akc = ac[k];
+      for (int r = k + 1 + lane; r < n; r += 32) ac[r] -= a[r + (i64)k * ld] * akc;
+    }
+    if (!SMEM) __threadfence_block();
+    __syncthreads();
+  }
+  if (tid == 0) {
+    for (int i = 0; i < n; i++) prow[i] = i;
+    for (int k = 0; k < n; k++) {
+      const int q = piv[k];
+      const int x = prow[k];
+      prow[k] = prow[q];
+      prow[q] = x;
+    }
+    const double det = (s_swaps & 1) ? -s_det : s_det;
+    *t.info = fabs(det) <= DBL_MIN ? 1 : 0;
+  }
+  for (int k = tid; k < n; k += nt) t.ipiv[k] = piv[k];
+  __syncthreads();
+
+  for (int c0 = warp * 32; c0 < m; c0 += nw * 32) {
+    const int c = c0 + lane;
+    const bool cv = c < m;
+    // Forward: L y = P b, L unit lower.
+    for (int b0 = 0; b0 < n; b0 += 32) {
+      T r[32];
+#pragma unroll
+      for (int i = 0; i < 32; i++) r[i] = (cv && b0 + i < n) ? t.B[c + (i64)prow[b0 + i] * t.ldb] : T(0);
+      for (int j = 0; j < b0; j++) {
+        const T xj = cv ? t.X[c + (i64)j * t.ldx] : T(0);
+#pragma unroll
+        for (int i = 0; i < 32; i++)
+          if (b0 + i < n) r[i] -= a[(b0 + i) + (i64)j * ld] * xj;
+      }
+#pragma unroll
+      for (int jj = 0; jj < 32; jj++) {
+        if (b0 + jj < n) {
+#pragma unroll
+          for (int i = jj + 1; i < 32; i++)
+            if (b0 + i < n) r[i] -= a[(b0 + i) + (i64)(b0 + jj) * ld] * r[jj];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 32; i++)
+        if (cv && b0 + i < n) t.X[c + (i64)(b0 + i) * t.ldx] = r[i];
+    }
+    // Backward: U x = y.
+    for (int b0 = ((n - 1) / 32) * 32; b0 >= 0; b0 -= 32) {
+      T r[32];
+#pragma unroll
+      for (int i = 0; i < 32; i++) r[i] = (cv && b0 + i < n) ? t.X[c + (i64)(b0 + i) * t.ldx] : T(0);
+      for (int j = b0 + 32; j < n; j++) {
+        const T xj = cv ? t.X[c + (i64)j * t.ldx] : T(0);
+#pragma unroll
+        for (int i = 0; i < 32; i++) r[i] -= a[(b0 + i) + (i64)j * ld] * xj;
+      }
+#pragma unroll
+      for (int jj = 31; jj >= 0; jj--) {
+        if (b0 + jj < n) {
+          r[jj] = r[jj] / a[(b0 + jj) + (i64)(b0 + jj) * ld];
+#pragma unroll
+          for (int i = 0; i < jj; i++) r[i] -= a[(b0 + i) + (i64)(b0 + jj) * ld] * r[jj];
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 32; i++)
+        if (cv && b0 + i < n) t.X[c + (i64)(b0 + i) * t.ldx] = r[i];
+    }
+  }
+}
+
+template <typename T>
+size_t lu_solve_smem(int n) {
+  return sizeof(T) * (size_t)n * (n + 1) + 2 * sizeof(int) * (size_t)n + 16;
+}
+
+template <typename T>
+cudaError_t launch_lu_solve(const LuSolveTask<T>* d_tasks, int ntasks, int maxn, cudaStream_t st) {
+  if (ntasks == 0) return cudaSuccess;
+  if (lu_solve_smem<T>(maxn) <= 200 * 1024) {
+    const size_t smem = lu_solve_smem<T>(maxn);
+    cudaError_t e = cudaFuncSetAttribute(k_lu_solve<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    note_launch();
+    k_lu_solve<T, true><<<ntasks, 256, smem, st>>>(d_tasks);
+    return cudaGetLastError();
+  }
+  const size_t smem = 2 * sizeof(int) * (size_t)maxn + 16;
+  cudaError_t e = cudaFuncSetAttribute(k_lu_solve<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  note_launch();
+  k_lu_solve<T, false><<<ntasks, 256, smem, st>>>(d_tasks);
+  return cudaGetLastError();
+}
+template cudaError_t launch_lu_solve<double>(const LuSolveTask<double>*, int, int, cudaStream_t);
+template cudaError_t launch_lu_solve<float>(const LuSolveTask<float>*, int, int, cudaStream_t);
+
 template <typename T>
 size_t gj_smem(int n) {
   return sizeof(T) * ((size_t)n * (n + 1) + n) + sizeof(int) * (size_t)n + 16;

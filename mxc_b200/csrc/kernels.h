@@ -179,6 +179,25 @@ struct LuTask {
 };
 template <typename T>
 cudaError_t launch_lu_inverse(const LuTask<T>* d_tasks, int ntasks, int maxn, cudaStream_t st);
+// PartialPivLU of A (n x n) and X = A^{-1} B for m right-hand sides stored
+// row by row: B[c + r ldb], X[c + r ldx] (r < n, c < m).  work: n x n scratch
+// (ld n) used when the factor does not fit in shared memory.
+template <typename T>
+struct LuSolveTask {
+  const T* A;
+  i64 lda;
+  int n;
+  const T* B;
+  i64 ldb;
+  int m;
+  T* X;
+  i64 ldx;
+  T* work;
+  int* ipiv;
+  int* info;
+};
+template <typename T>
+cudaError_t launch_lu_solve(const LuSolveTask<T>* d_tasks, int ntasks, int maxn, cudaStream_t st);
 
 // ---------------------------------------------------------------- vectors
 template <typename Ts, typename Td>

@@ -189,7 +189,41 @@ def test_precond_factor_and_substitution(pre2048):
     z = x.copy()
     M.solvePrecondition(z)
     zo = Mo.solve_precondition(x)
-    assert rel(z, zo) < 1e-7
+    assert rel(z, zo) < 1e-10
+
+
+def test_leveled_rank_matches_oracle(handle):
+    """leveled_rank > 0: rank (levels - l) * leveled_rank + rank at level l
+    (solver.cpp:29), the reference's own basis sequence; ranks per level,
+    skeletons, the factorization's info and the substitution agree with the
+    oracle."""
+    N = 4096
+    b, t, cells, L = problem(N)
+    rank, lrank = 48, 24
+    handle.set_basis_mode(m._lib.BASIS_HOUSEHOLDER)
+    try:
+        M = m.H2MatrixSolver(handle, m.Laplace3D(), 0.0, rank, lrank, t, 2.0, b, samples=2000)
+    finally:
+        handle.set_basis_mode(m._lib.BASIS_GRAM)
+    Mo = O.H2MatrixSolver(O.Kernel(), 0.0, rank, lrank, cells, 2.0, b.copy(), L, 2000)
+    for lvl in range(L + 1):
+        d, r = M.level_dims(lvl)
+        assert np.array_equal(d, Mo.A[lvl].Dims), lvl
+        assert np.array_equal(r, Mo.A[lvl].DimsLr), lvl
+        if lvl >= 1:
+            assert r.max() <= (L - lvl) * lrank + rank
+    assert int(M.level_dims(L)[1].max()) == rank and int(M.level_dims(L - 1)[1].max()) == rank + lrank
+    S = M.export(L, m._lib.EXPORT_S).reshape(-1, 3)
+    dims, ranks = M.level_dims(L)
+    off = 0
+    for i, (dd, rr) in enumerate(zip(dims, ranks)):
+        assert np.array_equal(S[off:off + rr], Mo.A[L].S[i][:rr]), i
+        off += dd
+    assert M.factorizeM() == Mo.factorize()
+    x = m.uniform_rhs(N)
+    z = x.copy()
+    M.solvePrecondition(z)
+    assert rel(z, Mo.solve_precondition(x)) < 1e-7
 
 
 def test_precond_before_factorize_is_an_error(handle):
@@ -477,12 +511,14 @@ def test_c1_configuration_matches_oracle_fixture(handle):
     assert list(np.atleast_1d(info)) == list(g["info"])
     z = xt.copy()
     M.solvePrecondition(z)
-    # The C1 preconditioner is too ill-conditioned for a tight comparison:
-    # the oracle's own M^-1 x_true moves by 12% when its LU solve of A_rr is
-    # replaced by an explicit inverse (same matrix, other rounding), and this
-    # path inverts A_rr by Gauss-Jordan.  The bound checks agreement at the
-    # level the conditioning allows (N = 2048 agrees to 1e-7).
-    assert rel(z, g["z_pc"]) < 0.5
+    # Both sides solve with A_rr by a partial-pivot LU and triangular solves
+    # (h2matrix.cpp:377-379).  The C1 redundant blocks are so ill-conditioned
+    # that rounding alone moves M^-1 x_true by several percent (the oracle's
+    # own result moves by 12% when its LU solve is swapped for an explicit
+    # inverse of the same matrix); the device result agrees to 9.3%, at the
+    # level that conditioning allows (N = 2048 agrees to 1e-10, see
+    # test_precond_factor_and_substitution).
+    assert rel(z, g["z_pc"]) < 0.15
     B = m.dense_matvec(handle, k, b, xt)
     X = np.zeros(N)
     A.solveGMRES(1e-10, M, X, B, 10, 3)
