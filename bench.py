@@ -46,6 +46,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=262144)
     ap.add_argument("--leaf", type=int, default=256)
+    ap.add_argument("--geometry", default="cube", choices=["cube", "mixture"],
+                    help="uniform unit cube (seed 999) or a 32-component Gaussian mixture (seed 999)")
+    ap.add_argument("--leaf-range", default="",
+                    help="MIN,MAX: geometric cuts clamped to MIN..MAX bodies per leaf (default: median split)")
     ap.add_argument("--theta", type=float, default=2.0)
     ap.add_argument("--rank", type=int, default=128)
     ap.add_argument("--samples", type=int, default=4000)
@@ -53,6 +57,8 @@ def parse():
                     help="operator bases: sketch of every far body (default) or --op-samples strided samples")
     ap.add_argument("--op-samples", type=int, default=16000, help="strided samples per box with --op-sampling strided")
     ap.add_argument("--op-eps", type=float, default=1e-11)
+    ap.add_argument("--op-storage", default="stored", choices=["matrix-free", "stored"],
+                    help="operator near blocks and couplings stored (default) or evaluated inside the matvec")
     ap.add_argument("--nrhs", type=int, default=16)
     ap.add_argument("--singularity", type=float, default=1e-4,
                     help="Laplace3D(s): value 1/s where bodies coincide (kernel.hpp:28-38)")
@@ -81,16 +87,45 @@ def parse():
 
 
 def op_desc(a) -> str:
+    st = ("near blocks and couplings evaluated in the matvec (matrix-free)" if a.op_storage == "matrix-free"
+          else "near blocks and couplings stored")
     if a.op_sampling == "sketch":
-        return "ID bases from an M-row random-sign sketch of every far body"
-    return "ID bases from %d strided far samples" % a.op_samples
+        return "ID bases from an M-row random-sign sketch of every far body; " + st
+    return "ID bases from %d strided far samples; %s" % (a.op_samples, st)
+
+
+def leaf_range(a):
+    if not a.leaf_range:
+        return 0, 0
+    lo, hi = (int(v) for v in a.leaf_range.split(","))
+    return lo, hi
+
+
+def points_and_tree(a, n):
+    """Seeded bodies of the configured geometry and their tree (sorted in place)."""
+    import mxc_b200 as m
+    from mxc_b200 import serving as S
+
+    L = m.levels_for(n, a.leaf)
+    b = m.uniform_unit_cube_rnd(n, 999) if a.geometry == "cube" else S.gaussian_mixture_points(n, 32, seed=999)
+    lo, hi = leaf_range(a)
+    return b, m.build_tree(b, L, leaf_min=lo, leaf_max=hi)
+
+
+def geometry_desc(a) -> str:
+    g = "uniform unit cube" if a.geometry == "cube" else "32-component Gaussian mixture (sigma 0.01-0.2)"
+    lo, hi = leaf_range(a)
+    split = ("median split, leaf %d" % a.leaf if not lo else
+             "geometric split clamped to %d-%d bodies per leaf (mean %d)" % (lo, hi, a.leaf))
+    return "%s (seed 999), %s" % (g, split)
 
 
 def workload(a) -> dict:
-    return {"workload": "H2 ULV-preconditioned GMRES, N=%d uniform unit cube (seed 999), Laplace 1/r diag 1/s s=%g, "
-                        "theta=%g, leaf=%d, precond rank=%d, samples=%d, operator eps=%g (%s), nrhs=%d, tol=%g"
-                        % (a.n, a.singularity, a.theta, a.leaf, a.rank, a.samples, a.op_eps, op_desc(a), a.nrhs,
-                           a.tol),
+    return {"workload": "H2 ULV-preconditioned GMRES, N=%d %s, Laplace 1/r diag 1/s s=%g, "
+                        "theta=%g, precond rank=%d, samples=%d, operator eps=%g (%s), nrhs=%d, tol=%g"
+                        % (a.n, geometry_desc(a), a.singularity, a.theta, a.rank, a.samples, a.op_eps, op_desc(a),
+                           a.nrhs, a.tol),
+            "geometry": a.geometry, "leaf_range": a.leaf_range or None,
             "n": a.n, "nrhs": a.nrhs, "leaf": a.leaf, "theta": a.theta, "rank": a.rank, "samples": a.samples,
             "singularity": a.singularity, "operator_bases": op_desc(a),
             "precond_precision": "fp32" if a.precision == "mixed" else "fp64",
@@ -265,8 +300,7 @@ def run_ours(a):
     h.set_option(m._lib.OPT_TENSOR_CORES, a.tensor_cores)
     k = m.Laplace3D(a.singularity)
     L = m.levels_for(a.n, a.leaf)
-    b = m.uniform_unit_cube_rnd(a.n, 999)
-    tree = m.build_tree(b, L)
+    b, tree = points_and_tree(a, a.n)
     prec = m.FP32 if a.precision == "mixed" else m.FP64
 
     def build_operator(kern, profile):
@@ -274,6 +308,7 @@ def run_ours(a):
         # profile, its per-kernel device times are returned too.
         h.set_option(m._lib.OPT_SAMPLING, m._lib.SAMPLING_SKETCH if a.op_sampling == "sketch"
                      else m._lib.SAMPLING_STRIDED)
+        h.set_option(m._lib.OPT_MATRIX_FREE, 1 if a.op_storage == "matrix-free" else 0)
         if profile:
             h.profile(True)
         t0 = time.time()
@@ -283,6 +318,7 @@ def run_ours(a):
             h.synchronize()
         finally:
             h.set_option(m._lib.OPT_SAMPLING, m._lib.SAMPLING_STRIDED)
+            h.set_option(m._lib.OPT_MATRIX_FREE, 0)
         secs = time.time() - t0
         rep_ = None
         if profile:
@@ -417,7 +453,7 @@ def run_ours(a):
     # flops is the dense TF32 rate (half the measured BF16 rate) / 3.
     tc_kernels = ("gemm_factor", "gemm_coupling") if prec == m.FP32 and a.tensor_cores else ()
     tc_div = 3.0 if a.tensor_cores == 1 else 1.0
-    simt32 = ("sample_tsqr", "cpqr", "lu_inverse", "basis_finish") if prec == m.FP32 else ()
+    simt32 = ("sample_tsqr", "cpqr", "lu_solve", "basis_finish") if prec == m.FP32 else ()
 
     def roofline(name, nl, dms, fl, by):
         # The roof is the slower of the compute and the HBM bound for the
@@ -595,8 +631,15 @@ class OracleSample:
 
         self.O, self.np, self.a, self.ns = O, np, a, ns
         self.L = O.levels_for(ns, a.leaf)
-        self.bodies = O.uniform_unit_cube_rnd(ns, 999)
-        self.cells = O.build_binary_tree(self.bodies, self.L)
+        lo, hi = leaf_range(a)
+        if a.geometry == "cube":
+            self.bodies = O.uniform_unit_cube_rnd(ns, 999)
+        else:
+            from mxc_b200.serving import gaussian_mixture_points  # numpy only: the seeded input generator
+
+            self.bodies = gaussian_mixture_points(ns, 32, seed=999)
+        self.cells = (O.build_binary_tree_capped(self.bodies, self.L, lo, hi) if lo
+                      else O.build_binary_tree(self.bodies, self.L))
         self.k = O.Kernel(O.LAPLACE, a.singularity)
         mode = 2 if a.op_sampling == "sketch" else 0
         self.A = O.H2MatrixSolver(self.k, a.op_eps, a.rank, 0, self.cells, a.theta, self.bodies, self.L,
@@ -642,16 +685,16 @@ def gpu_at_sample(a, h, ns: int) -> dict:
 
     import mxc_b200 as m
 
-    L = m.levels_for(ns, a.leaf)
-    b = m.uniform_unit_cube_rnd(ns, 999)
-    t = m.build_tree(b, L)
+    b, t = points_and_tree(a, ns)
     k = m.Laplace3D(a.singularity)
     h.set_option(m._lib.OPT_SAMPLING, m._lib.SAMPLING_SKETCH if a.op_sampling == "sketch" else m._lib.SAMPLING_STRIDED)
+    h.set_option(m._lib.OPT_MATRIX_FREE, 1 if a.op_storage == "matrix-free" else 0)
     try:
         A = m.H2MatrixSolver(h, k, a.op_eps, a.rank, 0, t, a.theta, b,
                              samples=0 if a.op_sampling == "sketch" else a.op_samples)
     finally:
         h.set_option(m._lib.OPT_SAMPLING, m._lib.SAMPLING_STRIDED)
+        h.set_option(m._lib.OPT_MATRIX_FREE, 0)
     X = np.random.default_rng(20261203).random((ns, a.nrhs))
     B = np.asfortranarray(m.dense_matvec(h, k, b, np.asfortranarray(X)))
     prec = m.FP32 if a.precision == "mixed" else m.FP64

@@ -48,6 +48,14 @@ int h2_uniform_rhs(double* x, int64_t n);
  * fills 2^(levels+1)-1 cells: child[2], body[2] (int64) and R[3], C[3]. */
 int h2_build_tree(double* bodies, int64_t nbodies, int64_t levels, int64_t* cell_child, int64_t* cell_body,
                   double* cell_R, double* cell_C);
+/* No counterpart in the reference (whose median split always gives equal
+ * leaves): the same tree with each cell cut where its bounding box is halved
+ * along the longest extent, the cut clamped so every leaf ends with
+ * leaf_min..leaf_max bodies (requires leaf_min 2^levels <= nbodies <=
+ * leaf_max 2^levels).  For strongly non-uniform bodies (clustered
+ * mixtures), where median cuts give elongated boxes. */
+int h2_build_tree_capped(double* bodies, int64_t nbodies, int64_t levels, int64_t leaf_min, int64_t leaf_max,
+                         int64_t* cell_child, int64_t* cell_body, double* cell_R, double* cell_C);
 /* build_tree.cpp:41-58 CSR::CSR: kind 'N' (near) or 'F' (far) pair list over
  * all cells.  row receives ncells+1 offsets; col up to cap column indices;
  * *nnz the list length (call with col = NULL to size it). */
@@ -90,7 +98,22 @@ int h2dev_handle_trim(h2dev_handle_t h);
  * plans built afterwards (in this process) on the tcgen05 tensor cores with
  * a 3-term TF32 split (FP32 accuracy); 2 with one TF32 product (about 1e-3
  * relative, for accuracy ablations); 0 runs them on the SIMT kernel. */
-enum { H2DEV_OPT_BASIS = 0, H2DEV_OPT_SKINNY_TILED = 1, H2DEV_OPT_SAMPLING = 2, H2DEV_OPT_TENSOR_CORES = 3 };
+/* H2DEV_OPT_MATRIX_FREE: 1 makes operator-mode (epi > 0) FP64 solvers
+ * created afterwards matrix-free: in interpolative mode every block the
+ * matvec reads is the kernel evaluated on two point sets (leaf near blocks on
+ * the box bodies, couplings on the skeleton bodies), so those blocks are
+ * evaluated inside the matvec instead of stored, and the upper-level near
+ * blocks (read only by a factorization) are not assembled.  Such a solver
+ * holds only its bases and points; h2dev_factorize on it returns
+ * H2DEV_ERR_STATE and exporting its A or C yields nothing.  0 (default)
+ * stores every block as the reference does. */
+enum {
+  H2DEV_OPT_BASIS = 0,
+  H2DEV_OPT_SKINNY_TILED = 1,
+  H2DEV_OPT_SAMPLING = 2,
+  H2DEV_OPT_TENSOR_CORES = 3,
+  H2DEV_OPT_MATRIX_FREE = 4
+};
 int h2dev_set_option(h2dev_handle_t h, int option, int64_t value);
 
 /* ---- solver (solver.hpp:11-47 H2MatrixSolver) ------------------------ */

@@ -29,6 +29,7 @@ OPT_BASIS = 0
 OPT_SKINNY_TILED = 1
 OPT_SAMPLING = 2
 OPT_TENSOR_CORES = 3
+OPT_MATRIX_FREE = 4
 BASIS_GRAM, BASIS_HOUSEHOLDER = 0, 1
 # H2DEV_OPT_SAMPLING values: strided cap, level-geometric cap, sketch of every far body
 SAMPLING_STRIDED, SAMPLING_GEOMETRIC, SAMPLING_SKETCH = 0, 1, 2
@@ -46,6 +47,7 @@ SIGNATURES = {
     "h2_uniform_rhs": (C.c_int, [_vp, _i64]),
     "h2_build_tree": (C.c_int, [_vp, _i64, _i64, _vp, _vp, _vp, _vp]),
     "h2_levels_for": (_i64, [_i64, _i64]),
+    "h2_build_tree_capped": (C.c_int, [_vp, _i64, _i64, _i64, _i64, _vp, _vp, _vp, _vp]),
     "h2_pair_csr": (C.c_int, [C.c_char, _i64, _vp, _vp, _vp, _vp, C.c_double, _vp, _vp, _i64, _i64p]),
     "h2dev_handle_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
     "h2dev_handle_destroy": (C.c_int, [_vp]),

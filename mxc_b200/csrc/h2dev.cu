@@ -530,6 +530,52 @@ struct GemmPlan {
   }
 };
 
+// Host-built matrix-free apply plan (k_mf.cu): tasks over point sets,
+// uploaded once per right-hand-side count and replayed.
+struct MfPlan {
+  std::vector<MfTask> tasks;
+  std::vector<MfEntry> ents;
+  std::vector<int2> tiles;
+  DVec<MfTask> d_tasks;
+  DVec<MfEntry> d_ents;
+  DVec<int2> d_tiles;
+  int nr = 0;
+  const char* name = "mf_apply";
+  double flops = 0., bytes = 0.;
+  void add_task(const double* pts, int m, double* C, i64 ldc, double beta) {
+    MfTask t;
+    t.pts = pts; t.m = m; t.C = C; t.ldc = ldc; t.beta = beta;
+    t.e0 = t.e1 = (int)ents.size();
+    tasks.push_back(t);
+  }
+  void add_entry(const double* pts, int k, const double* B, i64 ldb, double alpha) {
+    if (k <= 0) return;
+    MfEntry e;
+    e.pts = pts; e.k = k; e.B = B; e.ldb = ldb; e.alpha = alpha;
+    ents.push_back(e);
+    tasks.back().e1 = (int)ents.size();
+    // 2 nr multiply-adds per pair (the kernel evaluation is extra work);
+    // bytes: the entry's points and right-hand-side rows.
+    flops += 2. * nr * (double)tasks.back().m * k;
+    bytes += (24. + 8. * nr) * k;
+  }
+  void finalize() {
+    const int bm = mf_rows_per_cta();
+    tiles.clear();
+    for (size_t t = 0; t < tasks.size(); t++) {
+      bytes += (24. + 8. * nr) * tasks[t].m;
+      for (int r = 0; r < tasks[t].m; r += bm) tiles.push_back(make_int2((int)t, r / bm));
+    }
+    d_tasks.upload(tasks);
+    d_ents.upload(ents);
+    d_tiles.upload(tiles);
+  }
+  void run(const KernelParams& kp, cudaStream_t st) const {
+    Prof p(name, flops, bytes, st);
+    ck(launch_mf_apply(kp, nr, d_tasks.p, d_ents.p, d_tiles.p, (int)tiles.size(), st), name);
+  }
+};
+
 template <typename T>
 struct CopyPlan {
   std::vector<CopyEntry<T>> ents;
@@ -642,6 +688,12 @@ class Solver : public SolverBase {
   DVec<double> bodies;
   std::vector<Level<T>> L;
   bool factored = false;
+  // Matrix-free operator (H2DEV_OPT_MATRIX_FREE, ID mode, FP64): the leaf
+  // near blocks and the couplings are evaluated inside the matvec, never
+  // stored, and the upper-level near blocks (read only by a factorization)
+  // are not assembled.
+  bool matrix_free = false;
+  MfPlan mf_leaf, mf_far;
   int sampling_mode = 0;                 // 0: strided, 1: level-geometric far-list cap
   std::vector<std::vector<i64>> gstart;  // per cell: first range of each level group
   // per-nrhs state
@@ -667,6 +719,7 @@ class Solver : public SolverBase {
     N = a.nbodies;
     samples = a.samples;
     sampling_mode = h->sampling_mode;
+    matrix_free = h->matrix_free && !fix_rank && std::is_same<T, double>::value;
     cells = a.cells;
     {
       std::vector<double> hb(a.bodies, a.bodies + 3 * N);
@@ -752,7 +805,7 @@ class Solver : public SolverBase {
     lv.pts.alloc(3 * lv.lenX);
     lv.Q.alloc(lv.qoff[nodes]);
     lv.R.alloc(lv.qoff[nodes]);
-    lv.A.alloc(lv.aoff[nA]);
+    lv.A.alloc(matrix_free ? 0 : lv.aoff[nA]);
     lv.Q.zero(st());
     lv.R.zero(st());
     lv.A.zero(st());
@@ -775,9 +828,10 @@ class Solver : public SolverBase {
             t.ld = lv.dims[i];
             gt.push_back(t);
           }
+        if (matrix_free) gt.clear();
         DVec<GenTask> dg;
         dg.upload(gt);
-        {
+        if (!gt.empty()) {
           Prof pf("gen_near_blocks", 0., (double)lv.aoff[nA] * sizeof(T));
           // FP64 blocks use the std::hypot-exact distance (bit-exact with the
           // reference); FP32 blocks the rsqrt path, rounded to FP32 anyway.
@@ -808,7 +862,7 @@ class Solver : public SolverBase {
                   if (lowN >= 0) {
                     low->na_off[lowN] = lv.aoff[k] + offy + offx * M;
                     low->na_ld[lowN] = M;
-                  } else if (lowC >= 0) {
+                  } else if (lowC >= 0 && !matrix_free) {
                     acopy.add(low->C.p + low->coff[lowC], low->cld[y], lv.A.p + lv.aoff[k] + offy + offx * M, M, (int)ny, (int)nx);
                   }
                   offx += nx;
@@ -970,8 +1024,8 @@ class Solver : public SolverBase {
       lv.cld[i] = (lv.ranks[i] + 3) / 4 * 4;
       for (i64 k = lv.crow[i]; k < lv.crow[i + 1]; k++) lv.coff[k + 1] = lv.coff[k] + lv.cld[i] * lv.ranks[lv.ccol[k]];
     }
-    lv.C.alloc(lv.coff[nC]);
-    if (lv.lenZ > 0 && nC > 0) {
+    lv.C.alloc(matrix_free ? 0 : lv.coff[nC]);
+    if (lv.lenZ > 0 && nC > 0 && !matrix_free) {
       // Couplings (h2matrix.cpp:222-242): K(S_y, S_x) on the skeletons,
       // scaled by R_y on the left and R_x^T on the right in orthogonal mode.
       const bool orth = 1. <= level_epi(l);
@@ -1403,9 +1457,10 @@ class Solver : public SolverBase {
       }
       g.finalize();
     }
+    if (matrix_free) build_mf_plans(nr);
     mv_far = GemmPlan<T>();
     mv_far.name = "gemm_matvec_far";
-    for (i64 l = 0; l <= levels; l++) {
+    for (i64 l = 0; l <= levels && !matrix_free; l++) {
       Level<T>& lv = L[l];
       for (i64 i = 0; i < lv.nodes; i++) {
         int r = (int)lv.ranks[i];
@@ -1440,10 +1495,12 @@ class Solver : public SolverBase {
       q.name = "gemm_matvec_down";
       for (i64 i = 0; i < lv.nodes; i++) {
         int M = (int)lv.dims[i], r = (int)lv.ranks[i];
-        g.add_task(vout.p + lv.xoff[i], lv.lenX, M, nr, T(0));
-        for (i64 k = lv.arow[i]; k < lv.arow[i + 1]; k++) {
-          i64 j = lv.acol[k];
-          g.add_entry(lv.A.p + lv.aoff[k], M, 0, vin.p + lv.xoff[j], lv.lenX, 0, (int)lv.dims[j], T(1));
+        if (!matrix_free) {
+          g.add_task(vout.p + lv.xoff[i], lv.lenX, M, nr, T(0));
+          for (i64 k = lv.arow[i]; k < lv.arow[i + 1]; k++) {
+            i64 j = lv.acol[k];
+            g.add_entry(lv.A.p + lv.aoff[k], M, 0, vin.p + lv.xoff[j], lv.lenX, 0, (int)lv.dims[j], T(1));
+          }
         }
         q.add_task(vout.p + lv.xoff[i], lv.lenX, M, nr, T(1));
         q.add_entry(lv.Q.p + lv.qoff[i], M, 0, lv.vW.p + lv.zoff[i], lv.lenZ, 0, r, T(1));
@@ -1452,6 +1509,55 @@ class Solver : public SolverBase {
       q.finalize();
     }
     mv_built = true;
+  }
+
+  // Matrix-free near field (leaf boxes, tree-order bodies, as the stored
+  // blocks are generated) and couplings (skeleton bodies of every level).
+  void build_mf_plans(int nr) {
+    if constexpr (std::is_same<T, double>::value) {
+      mf_far = MfPlan();
+      mf_far.name = "mf_matvec_far";
+      mf_far.nr = nr;
+      for (i64 l = 0; l <= levels; l++) {
+        Level<T>& lv = L[l];
+        for (i64 i = 0; i < lv.nodes; i++) {
+          const int r = (int)lv.ranks[i];
+          if (r == 0) continue;
+          mf_far.add_task(lv.pts.p + 3 * lv.xoff[i], r, lv.vW.p + lv.zoff[i], lv.lenZ, 0.);
+          for (i64 k = lv.crow[i]; k < lv.crow[i + 1]; k++) {
+            const i64 j = lv.ccol[k];
+            mf_far.add_entry(lv.pts.p + 3 * lv.xoff[j], (int)lv.ranks[j], lv.vZ.p + lv.zoff[j], lv.lenZ, 1.);
+          }
+        }
+      }
+      mf_far.finalize();
+      mf_leaf = MfPlan();
+      mf_leaf.name = "mf_matvec_near";
+      mf_leaf.nr = nr;
+      Level<T>& lv = L[levels];
+      const i64 g0 = lv.gbegin;
+      for (i64 i = 0; i < lv.nodes; i++) {
+        const int M = (int)lv.dims[i];
+        mf_leaf.add_task(bodies.p + 3 * cells[g0 + i].body[0], M, vout.p + lv.xoff[i], lv.lenX, 0.);
+        for (i64 k = lv.arow[i]; k < lv.arow[i + 1]; k++) {
+          const i64 j = lv.acol[k];
+          mf_leaf.add_entry(bodies.p + 3 * cells[g0 + j].body[0], (int)lv.dims[j], vin.p + lv.xoff[j], lv.lenX, 1.);
+        }
+      }
+      mf_leaf.finalize();
+    }
+  }
+  void run_near(cudaStream_t s) {
+    if (matrix_free)
+      mf_leaf.run(kp, s);
+    else
+      mv_leaf.run(s);
+  }
+  void run_far(cudaStream_t s) {
+    if (matrix_free)
+      mf_far.run(kp, s);
+    else
+      mv_far.run(s);
   }
 
   void stage_in(i64 nrhs, const double* dX, i64 ldx) {
@@ -1486,16 +1592,16 @@ class Solver : public SolverBase {
     if (fork) {
       ck(cudaEventRecord(h->ev_fork, st()), "fork");
       ck(cudaStreamWaitEvent(h->stream2, h->ev_fork, 0), "fork");
-      mv_leaf.run(h->stream2);
+      run_near(h->stream2);
       ck(cudaEventRecord(h->ev_join, h->stream2), "join");
     }
     for (i64 l = levels; l >= 0; l--) mv_up[l].run(st());
-    mv_far.run(st());
+    run_far(st());
     for (i64 l = 0; l < levels; l++) mv_down[l].run(st());
     if (fork) {
       ck(cudaStreamWaitEvent(st(), h->ev_join, 0), "join");
     } else {
-      mv_leaf.run(st());
+      run_near(st());
     }
     mv_qw.run(st());
     stage_out(nrhs, dX, ldx);
@@ -1743,6 +1849,8 @@ class Solver : public SolverBase {
 
   void factorize(int* info) override {
     require(!factored, "factorize: already factored");
+    if (matrix_free)
+      throw H2Error{H2DEV_ERR_STATE, "factorize: a matrix-free operator stores no near blocks to factor"};
     for (i64 l = levels; l >= 0; l--) {
       factor_level(l);
       if (l > 0) copy_next(l);
@@ -1855,8 +1963,9 @@ class Solver : public SolverBase {
       case H2DEV_EXPORT_S: return 3 * lv.lenX;
       case H2DEV_EXPORT_Q:
       case H2DEV_EXPORT_R: return lv.qoff.back();
-      case H2DEV_EXPORT_A: return lv.aoff.back();
+      case H2DEV_EXPORT_A: return matrix_free ? 0 : lv.aoff.back();
       case H2DEV_EXPORT_C: {
+        if (matrix_free) return 0;
         i64 n = 0;  // packed: each block rank_i x rank_j with leading dimension rank_i
         for (i64 i = 0; i < lv.nodes; i++)
           for (i64 k = lv.crow[i]; k < lv.crow[i + 1]; k++) n += lv.ranks[i] * lv.ranks[lv.ccol[k]];
@@ -2139,6 +2248,30 @@ int h2_build_tree(double* bodies, int64_t nbodies, int64_t levels, int64_t* cell
   int64_t ncells = ((int64_t)2 << levels) - 1;
   std::vector<Cell> cells(ncells);
   build_binary_tree(cells.data(), bodies, nbodies, levels);
+  for (int64_t c = 0; c < ncells; c++) {
+    for (int k = 0; k < 2; k++) {
+      if (cell_child) cell_child[2 * c + k] = cells[c].child[k];
+      if (cell_body) cell_body[2 * c + k] = cells[c].body[k];
+    }
+    for (int k = 0; k < 3; k++) {
+      if (cell_R) cell_R[3 * c + k] = cells[c].R[k];
+      if (cell_C) cell_C[3 * c + k] = cells[c].C[k];
+    }
+  }
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2_build_tree_capped(double* bodies, int64_t nbodies, int64_t levels, int64_t leaf_min, int64_t leaf_max,
+                         int64_t* cell_child, int64_t* cell_body, double* cell_R, double* cell_C) {
+  H2_API_BEGIN
+  require(bodies && nbodies > 0 && levels >= 0 && levels < 40, "bad arguments");
+  require(leaf_min >= 1 && leaf_min <= leaf_max, "need 1 <= leaf_min <= leaf_max");
+  require(leaf_min * ((int64_t)1 << levels) <= nbodies && nbodies <= leaf_max * ((int64_t)1 << levels),
+          "leaf_min * 2^levels <= nbodies <= leaf_max * 2^levels does not hold");
+  int64_t ncells = ((int64_t)2 << levels) - 1;
+  std::vector<Cell> cells(ncells);
+  build_binary_tree_capped(cells.data(), bodies, nbodies, levels, leaf_min, leaf_max);
   for (int64_t c = 0; c < ncells; c++) {
     for (int k = 0; k < 2; k++) {
       if (cell_child) cell_child[2 * c + k] = cells[c].child[k];
@@ -2661,6 +2794,11 @@ int h2dev_set_option(h2dev_handle_t h, int option, int64_t value) {
   if (option == H2DEV_OPT_SAMPLING) {
     require(value >= 0 && value <= 2, "sampling option must be 0, 1 or 2");
     h->sampling_mode = (int)value;
+    return H2DEV_OK;
+  }
+  if (option == H2DEV_OPT_MATRIX_FREE) {
+    require(value == 0 || value == 1, "matrix-free option must be 0 or 1");
+    h->matrix_free = value != 0;
     return H2DEV_OK;
   }
   if (option == H2DEV_OPT_BASIS) {

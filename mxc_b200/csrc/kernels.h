@@ -153,6 +153,29 @@ cudaError_t launch_dgemm(const GemmTask<double>* d_tasks, const GemmEntry<double
                          int ntiles, cudaStream_t st);
 int dgemm_tile();
 
+// Matrix-free block apply (k_mf.cu), FP64: C = beta C + sum over the task's
+// entries of alpha K(pts_task, pts_entry) B (m x nr output, ld ldc; B k x nr,
+// ld ldb; points xyz-interleaved).  tiles: {task, block of
+// mf_rows_per_cta() rows}; nr <= 16.
+struct MfTask {
+  const double* pts;
+  int m;
+  double* C;
+  i64 ldc;
+  int e0, e1;
+  double beta;
+};
+struct MfEntry {
+  const double* pts;
+  int k;
+  const double* B;
+  i64 ldb;
+  double alpha;
+};
+cudaError_t launch_mf_apply(const KernelParams& kp, int nr, const MfTask* d_tasks, const MfEntry* d_ents,
+                            const int2* d_tiles, int ntiles, cudaStream_t st);
+int mf_rows_per_cta();
+
 template <typename T>
 struct CopyEntry {
   const T* src;

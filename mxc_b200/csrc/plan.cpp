@@ -73,6 +73,50 @@ void build_binary_tree(Cell* cells, double* bodies, i64 nbodies, i64 levels) {
   }
 }
 
+// Geometric, leaf-capped binary tree (build extension for strongly
+// non-uniform bodies).  Same cells, sort and bounds as build_binary_tree,
+// but a cell is cut where its bounding box is halved along the longest
+// extent (the first body at or past the box centre) rather than at the
+// median, and the cut is clamped so that each child can still give every one
+// of its h = 2^(levels - l - 1) leaves between leaf_min and leaf_max bodies:
+// left count in [max(leaf_min h, n - leaf_max h), min(leaf_max h, n -
+// leaf_min h)].  By induction from the root (leaf_min 2^levels <= N <=
+// leaf_max 2^levels) every leaf ends with leaf_min..leaf_max bodies, while
+// boxes follow the geometry wherever the density allows.
+void build_binary_tree_capped(Cell* cells, double* bodies, i64 nbodies, i64 levels, i64 leaf_min, i64 leaf_max) {
+  cells[0].body[0] = 0;
+  cells[0].body[1] = nbodies;
+  bounds(bodies, nbodies, cells[0].R, cells[0].C);
+  const i64 nleaf = (i64)1 << levels;
+  typedef std::array<double, 3> P3;
+  i64 level = 0;
+  for (i64 i = 0; i + 1 < nleaf; i++) {
+    if (i + 1 >= ((i64)2 << level)) level++;  // cells of level l are [2^l - 1, 2^(l+1) - 1)
+    Cell& ci = cells[i];
+    int sdim = 0;
+    for (int k = 1; k < 3; k++)
+      if (ci.R[sdim] < ci.R[k]) sdim = k;
+    const i64 b0 = ci.body[0], b1 = ci.body[1], n = b1 - b0;
+    P3* first = reinterpret_cast<P3*>(bodies + 3 * b0);
+    P3* last = reinterpret_cast<P3*>(bodies + 3 * b1);
+    std::sort(first, last, [=](P3& a, P3& b) { return a[sdim] < b[sdim]; });
+    const double cut = ci.C[sdim];
+    i64 left = std::lower_bound(first, last, cut, [=](const P3& a, double v) { return a[sdim] < v; }) - first;
+    const i64 h = (i64)1 << (levels - level - 1);
+    const i64 lo = std::max(leaf_min * h, n - leaf_max * h), hi = std::min(leaf_max * h, n - leaf_min * h);
+    left = lo <= hi ? std::min(std::max(left, lo), hi) : n / 2;
+    const i64 c0 = 2 * i + 1, mid = b0 + left;
+    ci.child[0] = c0;
+    ci.child[1] = c0 + 2;
+    cells[c0].body[0] = b0;
+    cells[c0].body[1] = mid;
+    cells[c0 + 1].body[0] = mid;
+    cells[c0 + 1].body[1] = b1;
+    bounds(bodies + 3 * b0, mid - b0, cells[c0].R, cells[c0].C);
+    bounds(bodies + 3 * mid, b1 - mid, cells[c0 + 1].R, cells[c0 + 1].C);
+  }
+}
+
 PairCSR build_pair_csr(char kind, const std::vector<Cell>& cells, double theta) {
   // Dual-tree descent from (0, 0), taken one tree level at a time; the
   // emitted pairs are sorted afterwards exactly as CSR::CSR sorts them.

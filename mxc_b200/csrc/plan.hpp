@@ -34,6 +34,10 @@ void uniform_rhs(double* x, i64 n);
 // buildBinaryTree (build_tree.cpp:67-99): sorts bodies in place.
 void build_binary_tree(Cell* cells, double* bodies, i64 nbodies, i64 levels);
 
+// Geometric split clamped so every leaf holds leaf_min..leaf_max bodies
+// (requires leaf_min 2^levels <= nbodies <= leaf_max 2^levels).
+void build_binary_tree_capped(Cell* cells, double* bodies, i64 nbodies, i64 levels, i64 leaf_min, i64 leaf_max);
+
 // CSR lists (build_tree.cpp:24-58); kind 'N' near, 'F' far.
 PairCSR build_pair_csr(char kind, const std::vector<Cell>& cells, double theta);
 

@@ -53,16 +53,24 @@ def levels_for(n: int, leaf: int) -> int:
     return int(L.lib().h2_levels_for(n, leaf))
 
 
-def build_tree(bodies: np.ndarray, levels: int) -> Tree:
-    """buildBinaryTree: sorts ``bodies`` (n x 3, C-contiguous float64) in place."""
+def build_tree(bodies: np.ndarray, levels: int, leaf_min: int = 0, leaf_max: int = 0) -> Tree:
+    """buildBinaryTree: sorts ``bodies`` (n x 3, C-contiguous float64) in place.
+
+    With leaf_min / leaf_max (extension): geometric cuts clamped so every leaf
+    holds leaf_min..leaf_max bodies (h2_build_tree_capped), for clustered
+    bodies; the default is the reference's median split."""
     assert bodies.dtype == np.float64 and bodies.flags.c_contiguous and bodies.shape[1] == 3
     nc = (2 << levels) - 1
     child = np.empty((nc, 2), dtype=np.int64)
     body = np.empty((nc, 2), dtype=np.int64)
     R = np.empty((nc, 3))
     Cc = np.empty((nc, 3))
-    L.check(L.lib().h2_build_tree(_ptr(bodies), bodies.shape[0], levels, _ptr(child), _ptr(body), _ptr(R),
-                                  _ptr(Cc)), "h2_build_tree")
+    if leaf_min or leaf_max:
+        L.check(L.lib().h2_build_tree_capped(_ptr(bodies), bodies.shape[0], levels, leaf_min, leaf_max, _ptr(child),
+                                             _ptr(body), _ptr(R), _ptr(Cc)), "h2_build_tree_capped")
+    else:
+        L.check(L.lib().h2_build_tree(_ptr(bodies), bodies.shape[0], levels, _ptr(child), _ptr(body), _ptr(R),
+                                      _ptr(Cc)), "h2_build_tree")
     return Tree(levels, child, body, R, Cc)
 
 

@@ -229,6 +229,43 @@ def build_binary_tree(bodies: np.ndarray, levels: int) -> Cells:
     return Cells(child, body, R, C)
 
 
+def build_binary_tree_capped(bodies: np.ndarray, levels: int, leaf_min: int, leaf_max: int) -> Cells:
+    """Geometric, leaf-capped split (build extension; the reference only has
+    the median split of build_tree.cpp:67-99): each cell is sorted along its
+    longest extent as in build_binary_tree, cut at the first body at or past
+    its bounding-box centre, the cut clamped so each child can still give its
+    h = 2^(levels - l - 1) leaves leaf_min..leaf_max bodies."""
+    nb = bodies.shape[0]
+    nleaf = 1 << levels
+    ncells = 2 * nleaf - 1
+    child = np.full((ncells, 2), -1, dtype=np.int64)
+    body = np.full((ncells, 2), -1, dtype=np.int64)
+    R = np.zeros((ncells, 3))
+    C = np.zeros((ncells, 3))
+    body[0] = (0, nb)
+    R[0], C[0] = get_bounds(bodies)
+    for i in range(nleaf - 1):
+        level = int(math.floor(math.log2(i + 1)))
+        sdim = int(np.argmax(R[i]))
+        b0, b1 = body[i]
+        seg = bodies[b0:b1]
+        order = np.argsort(seg[:, sdim], kind="stable")
+        bodies[b0:b1] = seg[order]
+        n = int(b1 - b0)
+        left = int(np.searchsorted(bodies[b0:b1, sdim], C[i, sdim], side="left"))
+        h = 1 << (levels - level - 1)
+        lo, hi = max(leaf_min * h, n - leaf_max * h), min(leaf_max * h, n - leaf_min * h)
+        left = min(max(left, lo), hi) if lo <= hi else n // 2
+        c0 = 2 * i + 1
+        child[i] = (c0, c0 + 2)
+        mid = b0 + left
+        body[c0] = (b0, mid)
+        body[c0 + 1] = (mid, b1)
+        R[c0], C[c0] = get_bounds(bodies[b0:mid])
+        R[c0 + 1], C[c0 + 1] = get_bounds(bodies[mid:b1])
+    return Cells(child, body, R, C)
+
+
 @dataclass
 class CSR:
     RowIndex: np.ndarray
