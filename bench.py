@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--tensor-cores", type=int, default=1, choices=[0, 1, 2],
                     help="FP32 contractions: 1 tcgen05 3-term TF32 split (default), 2 one TF32 product, 0 SIMT")
     ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--graph-solve", type=int, default=0, choices=[0, 1],
+                    help="run each GMRES solve as one captured CUDA graph (H2DEV_OPT_GRAPH_SOLVE)")
     ap.add_argument("--diag1-outer", type=int, default=8,
                     help="restarts of the diagonal-1 variant (Laplace3D(1), the reference's own diagonal; 0: skip)")
     ap.add_argument("--serving-requests", type=int, default=120,
@@ -80,7 +82,7 @@ def parse():
     ap.add_argument("--serving-budget-gb", type=float, default=140.0, help="HBM budget of the serving phase")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="one profiled step, no timing (for ncu)")
-    ap.add_argument("--profile-phase", default="step", choices=["step", "build", "factor", "solve"],
+    ap.add_argument("--profile-phase", default="step", choices=["step", "build", "factor", "solve", "operator"],
                     help="with --profile-only: the part of the step bracketed by cudaProfilerStart/Stop "
                          "(for ncu --profile-from-start off)")
     return ap.parse_args()
@@ -131,7 +133,9 @@ def workload(a) -> dict:
             "precond_precision": "fp32" if a.precision == "mixed" else "fp64",
             "fp32_contractions": {0: "simt fp32", 1: "tcgen05 3-term tf32 split", 2: "tcgen05 single tf32"}[
                 getattr(a, "tensor_cores", 1)],
-            "gmres": "fp64, inner %d, outer <= %d, early exit %d" % (a.inner, a.outer, a.early_exit),
+            "gmres": "fp64, inner %d, outer <= %d, early exit %d%s" % (a.inner, a.outer, a.early_exit,
+                                                                       ", one CUDA graph per solve" if a.graph_solve
+                                                                       else ""),
             "l2": "inputs (HBM working set of GBs) exceed the 126 MB L2 every step"}
 
 
@@ -298,6 +302,7 @@ def run_ours(a):
     torch.cuda.set_device(local)
     h = m.Handle(local)
     h.set_option(m._lib.OPT_TENSOR_CORES, a.tensor_cores)
+    h.set_option(m._lib.OPT_GRAPH_SOLVE, a.graph_solve)
     k = m.Laplace3D(a.singularity)
     L = m.levels_for(a.n, a.leaf)
     b, tree = points_and_tree(a, a.n)
@@ -326,7 +331,15 @@ def run_ours(a):
             h.profile(False)
         return Aop, secs, rep_
 
+    if a.profile_only and a.profile_phase == "operator":
+        import torch.cuda.profiler as prof_api
+
+        torch.cuda.synchronize()
+        prof_api.start()
     A, op_build_s, op_rep = build_operator(k, not a.profile_only)
+    if a.profile_only and a.profile_phase == "operator":
+        h.synchronize()
+        prof_api.stop()
     Xt = rhs_matrix(a.n, a.nrhs)
     dXt = torch.from_numpy(Xt.T.copy()).cuda()  # (nrhs, n) row-major == column-major n x nrhs
     dB = torch.empty_like(dXt)
@@ -346,7 +359,7 @@ def run_ours(a):
             h.synchronize()
             (torch.cuda.profiler.start if on else torch.cuda.profiler.stop)()
 
-    def step(precision, profile=False, Aop=None, kern=None, dBv=None, outer=None):
+    def step(precision, profile=False, Aop=None, kern=None, dBv=None, outer=None, bf16=False):
         Aop = A if Aop is None else Aop
         kern = k if kern is None else kern
         dBv = dB if dBv is None else dBv
@@ -357,7 +370,12 @@ def run_ours(a):
             h.profile(True)
         bracket("build", True)
         h.timer_start()
-        M = m.H2MatrixSolver(h, kern, 0.0, a.rank, 0, tree, a.theta, b, samples=a.samples, precision=precision)
+        if bf16:
+            h.set_option(m._lib.OPT_PRECOND_BF16, 1)
+        try:
+            M = m.H2MatrixSolver(h, kern, 0.0, a.rank, 0, tree, a.theta, b, samples=a.samples, precision=precision)
+        finally:
+            h.set_option(m._lib.OPT_PRECOND_BF16, 0)
         t_build = h.timer_stop()
         bracket("build", False)
         bracket("factor", True)
@@ -434,6 +452,39 @@ def run_ours(a):
                                              for c in range(a.nrhs))),
                 "x_mixed_vs_fp64_rel_max": float(max(np.linalg.norm(X64[:, c] - Xs[:, c]) / np.linalg.norm(X64[:, c])
                                                      for c in range(a.nrhs)))}
+
+    # The solve phase launched step by step against captured as one CUDA
+    # graph (same kernels, same order, same result).
+    graph = None
+    if not a.no_fp64_compare:
+        gm = {}
+        for mode in (0, 1):
+            h.set_option(m._lib.OPT_GRAPH_SOLVE, mode)
+            step(prec)
+            gm[mode] = step(prec)
+        h.set_option(m._lib.OPT_GRAPH_SOLVE, a.graph_solve)
+        graph = {"solve_ms_step_by_step": gm[0]["solve_ms"], "solve_ms_graph": gm[1]["solve_ms"],
+                 "iters_equal": gm[0]["iters"] == gm[1]["iters"],
+                 "note": "GMRES solve phase of one step: kernels launched one by one with the host reading the "
+                         "device's convergence flags, against the whole solve captured once (WHILE over cycles, "
+                         "IF per Arnoldi step) and launched as one graph; capture and instantiation included"}
+
+    # Ablation: the FP32 preconditioner's substitution applied from BF16
+    # copies of its blocks (per-block power-of-two scale, FP32 arithmetic).
+    bf16 = None
+    if a.precision == "mixed" and not a.no_fp64_compare:
+        step(m.FP32, bf16=True)
+        rb = step(m.FP32, bf16=True)
+        Xb = np.asfortranarray(dX.cpu().numpy().T)
+        Rb = m.dense_matvec(h, k, b, Xb)
+        bf16 = {"ms_per_step": rb["total_ms"], "build_ms": rb["build_ms"], "factor_ms": rb["factor_ms"],
+                "solve_ms": rb["solve_ms"], "iters": rb["iters"], "converged": rb["rc"] == 0,
+                "dense_resid_max": float(max(np.linalg.norm(Bh[:, c] - Rb[:, c]) / np.linalg.norm(Bh[:, c])
+                                             for c in range(a.nrhs))),
+                "x_vs_fp32_apply_rel_max": float(max(np.linalg.norm(Xb[:, c] - Xs[:, c]) / np.linalg.norm(Xs[:, c])
+                                                     for c in range(a.nrhs))),
+                "note": "same step with the substitution streamed from BF16 blocks; GMRES cycles and time "
+                        "against the FP32 apply (iters / phases_ms of the main line)"}
 
     # Profiled step: per-kernel device time, algorithmic work, launch count.
     step(prec, profile=True)
@@ -596,6 +647,8 @@ def run_ours(a):
             "roofline": roof,
             "kernels": kernels,
             "fp64_factor": fp64,
+            "bf16_apply_ablation": bf16,
+            "graph_solve": graph,
             "diag1": diag1,
             "gpu_at_cpu_sample": small,
             "serving": serving,

@@ -107,12 +107,26 @@ int h2dev_handle_trim(h2dev_handle_t h);
  * holds only its bases and points; h2dev_factorize on it returns
  * H2DEV_ERR_STATE and exporting its A or C yields nothing.  0 (default)
  * stores every block as the reference does. */
+/* H2DEV_OPT_PRECOND_BF16: 1 makes FP32 solvers created afterwards apply
+ * their ULV substitution (solvePrecondition) from BF16 copies of the blocks
+ * it streams, each scaled by a power of two so its entries lie in [-1, 1],
+ * with FP32 arithmetic: half the bytes of the FP32 apply, 8 significand
+ * bits instead of 24.  The factorization itself stays FP32.  0 (default):
+ * FP32 blocks. */
+/* H2DEV_OPT_GRAPH_SOLVE: 1 runs every GMRES solve on this handle as one
+ * CUDA graph: the solve is captured once per call (a WHILE node over restart
+ * cycles, an IF node around each Arnoldi step, the convergence decisions made
+ * by kernels on the device) and launched once, with no host round trip until
+ * it ends.  0 (default): the same kernels launched step by step, the host
+ * reading the device's convergence flags between steps. */
 enum {
   H2DEV_OPT_BASIS = 0,
   H2DEV_OPT_SKINNY_TILED = 1,
   H2DEV_OPT_SAMPLING = 2,
   H2DEV_OPT_TENSOR_CORES = 3,
-  H2DEV_OPT_MATRIX_FREE = 4
+  H2DEV_OPT_MATRIX_FREE = 4,
+  H2DEV_OPT_PRECOND_BF16 = 5,
+  H2DEV_OPT_GRAPH_SOLVE = 6
 };
 int h2dev_set_option(h2dev_handle_t h, int option, int64_t value);
 

@@ -30,6 +30,8 @@ OPT_SKINNY_TILED = 1
 OPT_SAMPLING = 2
 OPT_TENSOR_CORES = 3
 OPT_MATRIX_FREE = 4
+OPT_PRECOND_BF16 = 5
+OPT_GRAPH_SOLVE = 6
 BASIS_GRAM, BASIS_HOUSEHOLDER = 0, 1
 # H2DEV_OPT_SAMPLING values: strided cap, level-geometric cap, sketch of every far body
 SAMPLING_STRIDED, SAMPLING_GEOMETRIC, SAMPLING_SKETCH = 0, 1, 2

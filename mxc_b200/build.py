@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
          "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 
-SOURCES = ["plan.cpp", "k_gen.cu", "k_basis.cu", "k_gemm.cu", "k_tc.cu", "k_gram.cu", "k_sketch.cu", "k_mf.cu", "k_lu.cu", "k_vec.cu", "h2dev.cu",
+SOURCES = ["plan.cpp", "k_gen.cu", "k_basis.cu", "k_gemm.cu", "k_tc.cu", "k_gram.cu", "k_sketch.cu", "k_mf.cu", "k_bf16.cu", "k_lu.cu", "k_vec.cu", "h2dev.cu",
            "h2_solver.cpp"]
 # The reference's command-line driver on this library (C++ host code only).
 CLI_SRC = os.path.join(CSRC, "lorasp.cpp")

@@ -576,6 +576,33 @@ struct MfPlan {
   }
 };
 
+// BF16 substitution plan: the tasks of one FP32 GemmPlan with each entry's
+// block packed to BF16 (per-block power-of-two scale), applied by
+// k_stream_bf16.
+struct BfPlan {
+  std::vector<GemmTask<float>> tasks;
+  std::vector<BfEntry> ents;
+  std::vector<int2> tiles;
+  DVec<GemmTask<float>> d_tasks;
+  DVec<BfEntry> d_ents;
+  DVec<int2> d_tiles;
+  int nr = 0;
+  double flops = 0., bytes = 0.;
+  void finalize() {
+    const int bm = bf16_rows_per_cta();
+    tiles.clear();
+    for (size_t t = 0; t < tasks.size(); t++)
+      for (int r = 0; r < tasks[t].m; r += bm) tiles.push_back(make_int2((int)t, r / bm));
+    d_tasks.upload(tasks);
+    d_ents.upload(ents);
+    d_tiles.upload(tiles);
+  }
+  void run(cudaStream_t st) const {
+    Prof p("bf16_precond", flops, bytes, st);
+    ck(launch_stream_bf16(nr, d_tasks.p, d_ents.p, d_tiles.p, (int)tiles.size(), st), "bf16_precond");
+  }
+};
+
 template <typename T>
 struct CopyPlan {
   std::vector<CopyEntry<T>> ents;
@@ -662,6 +689,9 @@ class SolverBase {
   virtual void matvec(i64 nrhs, double* dX, i64 ldx) = 0;
   virtual void factorize(int* info) = 0;
   virtual void precondition(i64 nrhs, double* dX, i64 ldx) = 0;
+  // Builds the per-nrhs vectors and the matvec / substitution plans now, so
+  // that later applies only launch (required before a graph capture).
+  virtual void prepare(i64 nrhs) = 0;
   virtual void level_dims(i64 l, i64* dims, i64* ranks) const = 0;
   virtual i64 export_size(i64 l, int what) const = 0;
   virtual void export_to(i64 l, int what, double* out) = 0;
@@ -702,6 +732,12 @@ class Solver : public SolverBase {
   GemmPlan<T> mv_leaf, mv_far, mv_qw;  // leaf: near field (A_ij x_j); qw: + U W at the leaves
   std::vector<GemmPlan<T>> mv_up, mv_down;
   std::vector<GemmPlan<T>> pc_fx, pc_fz, pc_bx, pc_by;
+  // BF16 substitution (H2DEV_OPT_PRECOND_BF16, FP32 solvers): packed
+  // copies of the streamed blocks and the plans that read them.
+  bool precond_bf16 = false;
+  DVec<__nv_bfloat16> bf_pool;
+  DVec<float> bf_scales;
+  std::vector<BfPlan> bf_fx, bf_fz, bf_bx, bf_by;
   std::vector<CopyPlan<T>> pc_fcopy, pc_bcopy;
   bool mv_built = false, pc_built = false;
 
@@ -720,6 +756,7 @@ class Solver : public SolverBase {
     samples = a.samples;
     sampling_mode = h->sampling_mode;
     matrix_free = h->matrix_free && !fix_rank && std::is_same<T, double>::value;
+    precond_bf16 = h->precond_bf16 && std::is_same<T, float>::value;
     cells = a.cells;
     {
       std::vector<double> hb(a.bodies, a.bodies + 3 * N);
@@ -1577,6 +1614,12 @@ class Solver : public SolverBase {
     }
   }
 
+  void prepare(i64 nrhs) override {
+    ensure_vectors(nrhs);
+    if (!mv_built) build_matvec(nrhs);
+    if (factored && !pc_built) build_precondition(nrhs);
+  }
+
   void matvec(i64 nrhs, double* dX, i64 ldx) override {
     require(nrhs > 0 && ldx >= N, "matvec: bad nrhs/ld");
     ensure_vectors(nrhs);
@@ -1923,10 +1966,85 @@ class Solver : public SolverBase {
         pc_by[l].add_entry(lv.Q.p + lv.qoff[i], M, 0, X + lv.xoff[i], ldx, 0, M, T(1));
       }
       pc_fx[l].name = pc_fz[l].name = pc_bx[l].name = pc_by[l].name = "gemm_precond";
+      if (precond_bf16) continue;  // the BF16 plans below replace them
       pc_fx[l].finalize(); pc_fz[l].finalize(); pc_bx[l].finalize(); pc_by[l].finalize();
-      pc_fcopy[l].finalize(); pc_bcopy[l].finalize();
     }
+    for (i64 l = 0; l <= levels; l++) {
+      pc_fcopy[l].finalize();
+      pc_bcopy[l].finalize();
+    }
+    if (precond_bf16) build_bf16_plans(nr);
     pc_built = true;
+  }
+
+  // Packs every block the substitution plans stream into one BF16 pool
+  // (columns padded to multiples of 8 elements, so each block and column
+  // starts on a 16-byte boundary) and builds the BF16 plans over it.
+  void build_bf16_plans(int nr) {
+    if constexpr (std::is_same<T, float>::value) {
+      std::vector<GemmPlan<T>>* srcs[4] = {&pc_fx, &pc_fz, &pc_bx, &pc_by};
+      std::vector<BfPlan>* dsts[4] = {&bf_fx, &bf_fz, &bf_bx, &bf_by};
+      i64 total = 0, nblk = 0;
+      for (auto* sp : srcs)
+        for (auto& g : *sp)
+          for (const auto& t : g.tasks)
+            for (int e = t.e0; e < t.e1; e++) {
+              total += (i64)((t.m + 7) / 8 * 8) * g.ents[e].k;
+              nblk++;
+            }
+      bf_pool.alloc(std::max<i64>(8, total));
+      bf_scales.alloc(std::max<i64>(1, nblk));
+      std::vector<BfPackTask> packs;
+      i64 off = 0, sb = 0;
+      for (int q = 0; q < 4; q++) {
+        dsts[q]->clear();
+        dsts[q]->resize(levels + 1);
+        for (i64 l = 0; l <= levels; l++) {
+          const GemmPlan<T>& g = (*srcs[q])[l];
+          BfPlan& b = (*dsts[q])[l];
+          b.nr = nr;
+          for (const auto& t : g.tasks) {
+            GemmTask<float> bt = t;
+            bt.e0 = (int)b.ents.size();
+            const i64 ldd = (t.m + 7) / 8 * 8;
+            for (int e = t.e0; e < t.e1; e++) {
+              const GemmEntry<float>& en = g.ents[e];
+              if (en.k <= 0) continue;
+              BfPackTask pk;
+              pk.src = en.A;
+              pk.lds = en.lda;
+              pk.m = t.m;
+              pk.k = en.k;
+              pk.dst = bf_pool.p + off;
+              pk.ldd = ldd;
+              pk.scale = bf_scales.p + sb;
+              packs.push_back(pk);
+              BfEntry be;
+              be.A = pk.dst;
+              be.lda = ldd;
+              be.B = en.B;
+              be.ldb = en.ldb;
+              be.k = en.k;
+              be.alpha = en.alpha;
+              be.scale = pk.scale;
+              b.ents.push_back(be);
+              b.flops += 2. * nr * (double)t.m * en.k;
+              b.bytes += 2. * (double)t.m * en.k + 4. * (double)nr * en.k;
+              off += ldd * en.k;
+              sb++;
+            }
+            bt.e1 = (int)b.ents.size();
+            b.bytes += 8. * (double)nr * t.m;
+            b.tasks.push_back(bt);
+          }
+          b.finalize();
+        }
+      }
+      DVec<BfPackTask> dp;
+      dp.upload(packs);
+      Prof pf("bf16_pack", 0., 6. * (double)off);
+      ck(launch_bf16_pack(dp.p, (int)packs.size(), st()), "bf16_pack");
+    }
   }
 
   void precondition(i64 nrhs, double* dX, i64 ldx) override {
@@ -1935,6 +2053,22 @@ class Solver : public SolverBase {
     ensure_vectors(nrhs);
     if (!pc_built) build_precondition(nrhs);
     stage_in(nrhs, dX, ldx);
+    if constexpr (std::is_same<T, float>::value) {
+      if (precond_bf16) {
+        for (i64 l = levels; l >= 0; l--) {
+          bf_fx[l].run(st());
+          pc_fcopy[l].run(st());
+          bf_fz[l].run(st());
+        }
+        for (i64 l = 0; l <= levels; l++) {
+          pc_bcopy[l].run(st());
+          bf_bx[l].run(st());
+          bf_by[l].run(st());
+        }
+        stage_out(nrhs, dX, ldx);
+        return;
+      }
+    }
     for (i64 l = levels; l >= 0; l--) {
       pc_fx[l].run(st());
       pc_fcopy[l].run(st());
@@ -2008,166 +2142,248 @@ class Solver : public SolverBase {
   }
 };
 
-// Residual norm of min || beta e1 - H y || for an (rows x cols) Hessenberg
-// block of a column-major array with leading dimension ld.
-static double ls_residual(const double* Hin, int ld, int rows, int cols, double beta) {
-  std::vector<double> H((size_t)rows * cols), s(rows, 0.);
-  for (int j = 0; j < cols; j++)
-    for (int r = 0; r < rows; r++) H[r + (size_t)j * rows] = Hin[r + (size_t)j * ld];
-  s[0] = beta;
-  for (int k = 0; k < cols; k++) {
-    double a = H[k + (size_t)k * rows], b = H[k + 1 + (size_t)k * rows];
-    double r = std::hypot(a, b);
-    if (r == 0.) continue;
-    double c = a / r, sn = b / r;
-    for (int j = k; j < cols; j++) {
-      double x = H[k + (size_t)j * rows], y = H[k + 1 + (size_t)j * rows];
-      H[k + (size_t)j * rows] = c * x + sn * y;
-      H[k + 1 + (size_t)j * rows] = -sn * x + c * y;
-    }
-    double x = s[k], y = s[k + 1];
-    s[k] = c * x + sn * y;
-    s[k + 1] = -sn * x + c * y;
-  }
-  return std::fabs(s[cols]);
+// ------------------------------------------------------------------ GMRES
+// solver.cpp:144-201 with one independent GMRES per right-hand side.  The
+// control flow is on the device (k_vec.cu: k_gmres_init / cycle_begin /
+// estimate / cycle_end): which columns are active, when a cycle's Arnoldi
+// loop may stop early, the residual history.  Launched step by step (the
+// host reads one flag after each Arnoldi step when early exit is on, and the
+// active flags after each cycle), or, with the handle's graph option, the
+// whole solve is captured once as a CUDA graph -- a WHILE node over restart
+// cycles, an IF node around each Arnoldi step -- and runs as one launch with
+// no host round trip until the end.
+struct GmresState {
+  i64 N = 0, nrhs = 0, inner = 0, outer = 0, vstride = 0;
+  int ldh = 0, nch = 0;
+  double tol = 0.;
+  int early = 0;
+  DVec<double> V, w, R, Bc, X, H, y, beta, nrm2, partial, normb, rvec, resh;
+  DVec<int> act, it, ctl;  // ctl: used, stop, cycles
+};
+
+static void gmres_prologue(SolverBase& M, GmresState& g, int graph, cudaGraphConditionalHandle hs,
+                           cudaStream_t st) {
+  const int nr = (int)g.nrhs;
+  ck(launch_gmres_cycle_begin(g.ctl.p, g.ctl.p + 1, (int)g.inner, graph, hs, st), "cycle begin");
+  M.precondition(g.nrhs, g.R.p, g.N);
+  ck(launch_dots(g.R.p, 0, 1, g.R.p, g.N, nr, g.partial.p, g.nch, g.nrm2.p, st), "dots");
+  ck(launch_scale_by_norm(g.R.p, g.V.p, g.nrm2.p, g.beta.p, 1, g.N, nr, st), "v0");
+  ck(cudaMemsetAsync(g.H.p, 0, sizeof(double) * g.H.n, st), "H=0");
 }
 
-// ------------------------------------------------------------------ GMRES
-// solver.cpp:144-201 with one independent GMRES per right-hand side.
+static void gmres_step(SolverBase& A, SolverBase& M, GmresState& g, i64 i, int graph, cudaGraphConditionalHandle hs,
+                       cudaStream_t st) {
+  const int nr = (int)g.nrhs, kv = (int)i + 1;
+  const i64 hstride = (i64)g.ldh * g.inner;
+  ck(cudaMemcpyAsync(g.w.p, g.V.p + i * g.vstride, sizeof(double) * g.vstride, cudaMemcpyDeviceToDevice, st), "w=v");
+  A.matvec(g.nrhs, g.w.p, g.N);
+  M.precondition(g.nrhs, g.w.p, g.N);
+  double* hcol = g.H.p + i * g.ldh;  // H[:, i] of rhs c at hcol + c * hstride
+  {
+    Prof pf("gmres_dots", 2. * g.N * kv * nr, 8. * (kv + 1) * g.N * nr);
+    ck(launch_dots_strided(g.V.p, g.vstride, kv, g.w.p, g.N, nr, g.partial.p, g.nch, hcol, hstride, st), "dots");
+  }
+  {
+    Prof pf("gmres_gs_update", 2. * g.N * kv * nr, 8. * (kv + 2) * g.N * nr);
+    ck(launch_gs_update(g.w.p, g.V.p, g.vstride, hcol, hstride, kv, g.N, nr, -1.0, nullptr, st), "gs");
+  }
+  ck(launch_dots(g.w.p, 0, 1, g.w.p, g.N, nr, g.partial.p, g.nch, g.nrm2.p, st), "dots");
+  ck(launch_scale_by_norm(g.w.p, g.V.p + (i + 1) * g.vstride, g.nrm2.p, hcol + i + 1, hstride, g.N, nr, st), "scale");
+  if (g.early)
+    ck(launch_gmres_estimate(g.H.p, g.ldh, (int)g.inner, (int)i, g.beta.p, g.normb.p, g.act.p, nr, g.tol, g.ctl.p,
+                             g.ctl.p + 1, graph, hs, st),
+       "estimate");
+}
+
+static void gmres_epilogue(SolverBase& A, GmresState& g, int graph, cudaGraphConditionalHandle hw, cudaStream_t st) {
+  const int nr = (int)g.nrhs;
+  ck(launch_gmres_ls(g.H.p, g.ldh, (int)g.inner, g.beta.p, g.y.p, nr, st, g.ctl.p), "ls");
+  ck(launch_gs_update(g.X.p, g.V.p, g.vstride, g.y.p, g.inner, (int)g.inner, g.N, nr, 1.0, g.act.p, st, g.ctl.p),
+     "x update");
+  ck(cudaMemcpyAsync(g.R.p, g.X.p, sizeof(double) * g.vstride, cudaMemcpyDeviceToDevice, st), "R=X");
+  A.matvec(g.nrhs, g.R.p, g.N);
+  ck(launch_axpby(g.R.p, g.Bc.p, -1.0, 1.0, g.vstride, st), "R=B-AX");
+  ck(launch_dots(g.R.p, 0, 1, g.R.p, g.N, nr, g.partial.p, g.nch, g.nrm2.p, st), "dots");
+  ck(launch_residual_norm_finish(g.nrm2.p, g.normb.p, g.rvec.p, nr, st), "resid");
+  ck(launch_gmres_cycle_end(g.rvec.p, g.act.p, g.it.p, g.resh.p, (int)g.outer, g.tol, nr, g.ctl.p + 2, graph, hw, st),
+     "cycle end");
+}
+
+// The whole solve as one graph: init kernel, then WHILE(any column active)
+// { prologue; IF(step enabled) { Arnoldi step i } for i < inner; epilogue }.
+// Library launches go to h->stream, which is pointed at each body's capture
+// stream in turn (the side stream of the matvec joins and leaves every
+// capture by its events, so the bodies hold kernels and copies only).
+static void gmres_graph(SolverBase& A, SolverBase& M, GmresState& g) {
+  h2dev_handle_s* h = A.h;
+  cudaStream_t s0 = h->stream;
+  cudaStream_t sb = nullptr, ss = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  struct Restore {
+    h2dev_handle_s* h;
+    cudaStream_t s0, sb, ss;
+    cudaGraph_t* g;
+    cudaGraphExec_t* e;
+    ~Restore() {
+      h->stream = s0;
+      if (*e) cudaGraphExecDestroy(*e);
+      if (*g) cudaGraphDestroy(*g);
+      if (sb) cudaStreamDestroy(sb);
+      if (ss) cudaStreamDestroy(ss);
+    }
+  } restore{h, s0, nullptr, nullptr, &graph, &exec};
+  ck(cudaStreamCreateWithFlags(&sb, cudaStreamNonBlocking), "stream");
+  restore.sb = sb;
+  ck(cudaStreamCreateWithFlags(&ss, cudaStreamNonBlocking), "stream");
+  restore.ss = ss;
+  ck(cudaStreamBeginCapture(s0, cudaStreamCaptureModeRelaxed), "capture");
+  try {
+    cudaGraph_t g0 = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaStreamCaptureStatus cs;
+    ck(cudaStreamGetCaptureInfo(s0, &cs, nullptr, &g0, &deps, &ndeps), "capture info");
+    cudaGraphConditionalHandle hw;
+    ck(cudaGraphConditionalHandleCreate(&hw, g0, 0, 0), "conditional handle");
+    ck(launch_gmres_init(g.act.p, g.it.p, g.resh.p, (int)g.outer, g.tol, (int)g.nrhs, g.ctl.p + 2, 1, hw, s0),
+       "init");
+    ck(cudaStreamGetCaptureInfo(s0, &cs, nullptr, &g0, &deps, &ndeps), "capture info");
+    cudaGraphNodeParams wp = {};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = hw;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    ck(cudaGraphAddNode(&wnode, g0, deps, ndeps, &wp), "while node");
+    ck(cudaStreamUpdateCaptureDependencies(s0, &wnode, 1, cudaStreamSetCaptureDependencies), "capture deps");
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    cudaGraphConditionalHandle hs;
+    ck(cudaGraphConditionalHandleCreate(&hs, body, 1, cudaGraphCondAssignDefault), "conditional handle");
+    h->stream = sb;
+    ck(cudaStreamBeginCaptureToGraph(sb, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed), "body capture");
+    gmres_prologue(M, g, 1, hs, sb);
+    for (i64 i = 0; i < g.inner; i++) {
+      cudaGraph_t bg = nullptr;
+      ck(cudaStreamGetCaptureInfo(sb, &cs, nullptr, &bg, &deps, &ndeps), "capture info");
+      cudaGraphNodeParams ip = {};
+      ip.type = cudaGraphNodeTypeConditional;
+      ip.conditional.handle = hs;
+      ip.conditional.type = cudaGraphCondTypeIf;
+      ip.conditional.size = 1;
+      cudaGraphNode_t inode;
+      ck(cudaGraphAddNode(&inode, bg, deps, ndeps, &ip), "if node");
+      ck(cudaStreamUpdateCaptureDependencies(sb, &inode, 1, cudaStreamSetCaptureDependencies), "capture deps");
+      h->stream = ss;
+      ck(cudaStreamBeginCaptureToGraph(ss, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                       cudaStreamCaptureModeRelaxed),
+         "step capture");
+      gmres_step(A, M, g, i, 1, hs, ss);
+      cudaGraph_t done = nullptr;
+      ck(cudaStreamEndCapture(ss, &done), "step capture end");
+      h->stream = sb;
+    }
+    gmres_epilogue(A, g, 1, hw, sb);
+    cudaGraph_t bdone = nullptr;
+    ck(cudaStreamEndCapture(sb, &bdone), "body capture end");
+    h->stream = s0;
+  } catch (...) {
+    h->stream = s0;
+    cudaGraph_t junk = nullptr;
+    cudaStreamEndCapture(s0, &junk);
+    if (junk) cudaGraphDestroy(junk);
+    cudaGetLastError();
+    throw;
+  }
+  ck(cudaStreamEndCapture(s0, &graph), "capture end");
+  ck(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+  ck(cudaGraphLaunch(exec, s0), "graph launch");
+  ck(cudaStreamSynchronize(s0), "sync");
+}
+
 static int gmres(SolverBase& A, SolverBase& M, double tol, i64 nrhs, double* dX, const double* dB, i64 ld, i64 inner,
                  i64 outer, int early_exit, double* resid, i64* iters) {
   require(A.lenX() == M.lenX(), "gmres: A and M sizes differ");
   require(inner >= 1 && inner <= 16 && outer >= 0 && nrhs >= 1, "gmres: inner must be in [1,16]");
   cudaStream_t st = A.h->stream;
-  const i64 N = A.lenX();
+  GmresState g;
+  g.N = A.lenX();
+  g.nrhs = nrhs;
+  g.inner = inner;
+  g.outer = outer;
+  g.ldh = (int)inner + 1;
+  g.vstride = g.N * nrhs;
+  g.tol = tol;
+  g.early = early_exit ? 1 : 0;
+  g.nch = dots_chunks(g.N);
   const int nr = (int)nrhs;
-  const int ldh = (int)inner + 1;
-  const i64 vstride = N * nrhs;
-  DVec<double> V, w, R, Bc, X, H, y, beta, nrm2, partial, normb, rvec, hcol;
-  DVec<int> active;
-  V.alloc((size_t)(inner + 1) * vstride);
-  w.alloc(vstride);
-  R.alloc(vstride);
-  Bc.alloc(vstride);
-  X.alloc(vstride);
-  H.alloc((size_t)ldh * inner * nrhs);
-  y.alloc((size_t)inner * nrhs);
-  beta.alloc(nrhs);
-  nrm2.alloc(nrhs);
-  normb.alloc(nrhs);
-  rvec.alloc(nrhs);
-  hcol.alloc((size_t)(inner + 1) * nrhs);
-  active.alloc(nrhs);
-  const int nch = dots_chunks(N);
-  partial.alloc((size_t)nch * (inner + 1) * nrhs);
+  g.V.alloc((size_t)(inner + 1) * g.vstride);
+  g.w.alloc(g.vstride);
+  g.R.alloc(g.vstride);
+  g.Bc.alloc(g.vstride);
+  g.X.alloc(g.vstride);
+  g.H.alloc((size_t)g.ldh * inner * nrhs);
+  g.y.alloc((size_t)inner * nrhs);
+  g.beta.alloc(nrhs);
+  g.nrm2.alloc(nrhs);
+  g.normb.alloc(nrhs);
+  g.rvec.alloc(nrhs);
+  g.resh.alloc((size_t)(outer + 1) * nrhs);
+  g.act.alloc(nrhs);
+  g.it.alloc(nrhs);
+  g.ctl.alloc(4);
+  g.partial.alloc((size_t)g.nch * (inner + 1) * nrhs);
+  g.resh.zero(st);
+  g.y.zero(st);
   for (i64 c = 0; c < nrhs; c++) {
-    ck(cudaMemcpyAsync(Bc.p + c * N, dB + c * ld, sizeof(double) * N, cudaMemcpyDeviceToDevice, st), "copy B");
-    ck(cudaMemcpyAsync(X.p + c * N, dX + c * ld, sizeof(double) * N, cudaMemcpyDeviceToDevice, st), "copy X");
+    ck(cudaMemcpyAsync(g.Bc.p + c * g.N, dB + c * ld, sizeof(double) * g.N, cudaMemcpyDeviceToDevice, st), "copy B");
+    ck(cudaMemcpyAsync(g.X.p + c * g.N, dX + c * ld, sizeof(double) * g.N, cudaMemcpyDeviceToDevice, st), "copy X");
   }
-  ck(launch_dots(Bc.p, 0, 1, Bc.p, N, nr, partial.p, nch, nrm2.p, st), "dots");
-  std::vector<double> hn(nrhs);
+  ck(launch_dots(g.Bc.p, 0, 1, g.Bc.p, g.N, nr, g.partial.p, g.nch, g.nrm2.p, st), "dots");
   {
-    std::vector<double> n2 = nrm2.download(st);
+    std::vector<double> n2 = g.nrm2.download(st), hn(nrhs);
     for (i64 c = 0; c < nrhs; c++) {
       hn[c] = std::sqrt(n2[c]);
       if (hn[c] == 0.) hn[c] = 1.;
     }
-    ck(cudaMemcpy(normb.p, hn.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice), "normb");
-  }
-  ck(cudaMemcpyAsync(R.p, Bc.p, sizeof(double) * vstride, cudaMemcpyDeviceToDevice, st), "R=B");
-  std::vector<double> res((size_t)(outer + 1) * nrhs, 0.);
-  std::vector<i64> it(nrhs, 0);
-  std::vector<int> act(nrhs, 1);
-  for (i64 c = 0; c < nrhs; c++) {
-    res[c * (outer + 1)] = 1.;
-    act[c] = (0 < outer && tol <= 1.) ? 1 : 0;
+    g.normb.upload(hn);
   }
   // The reference starts from the given X with R = B (not B - A X) in its
   // first cycle (solver.cpp:157); the initial guess is zero in every caller.
-  i64 cycle = 0;
-  while (true) {
-    bool any = false;
-    for (i64 c = 0; c < nrhs; c++) any |= act[c] != 0;
-    if (!any) break;
-    ck(cudaMemcpy(active.p, act.data(), sizeof(int) * nrhs, cudaMemcpyHostToDevice), "active");
-    M.precondition(nrhs, R.p, N);
-    ck(launch_dots(R.p, 0, 1, R.p, N, nr, partial.p, nch, nrm2.p, st), "dots");
-    ck(launch_scale_by_norm(R.p, V.p, nrm2.p, beta.p, 1, N, nr, st), "v0");
-    ck(cudaMemsetAsync(H.p, 0, sizeof(double) * H.n, st), "H=0");
-    i64 used = inner;
-    for (i64 i = 0; i < inner; i++) {
-      ck(cudaMemcpyAsync(w.p, V.p + i * vstride, sizeof(double) * vstride, cudaMemcpyDeviceToDevice, st), "w=v");
-      A.matvec(nrhs, w.p, N);
-      M.precondition(nrhs, w.p, N);
-      const int kv = (int)i + 1;
-      { Prof pf("gmres_dots", 2. * N * kv * nr, 8. * (kv + 1) * N * nr); ck(launch_dots(V.p, vstride, kv, w.p, N, nr, partial.p, nch, hcol.p, st), "dots"); }
-      // H[:kv, i] for every rhs (rhs c block of H has stride ldh*inner)
-      { Prof pf("gmres_gs_update", 2. * N * kv * nr, 8. * (kv + 2) * N * nr); ck(launch_gs_update(w.p, V.p, vstride, hcol.p, kv, kv, N, nr, -1.0, nullptr, st), "gs"); }
-      {
-        // scatter hcol into H column i
-        CopyPlan<double> cp;
-        for (int c = 0; c < nr; c++) cp.add(hcol.p + (i64)c * kv, kv, H.p + (i64)c * ldh * inner + i * ldh, ldh, kv, 1);
-        cp.finalize();
-        cp.run(st);
-        ck(launch_dots(w.p, 0, 1, w.p, N, nr, partial.p, nch, nrm2.p, st), "dots");
-        // H[i+1, i] and v_{i+1}; hout stride is per rhs block
-        DVec<double> hv;
-        hv.alloc(nrhs);
-        ck(launch_scale_by_norm(w.p, V.p + (i + 1) * vstride, nrm2.p, hv.p, 1, N, nr, st), "scale");
-        CopyPlan<double> cp2;
-        for (int c = 0; c < nr; c++) cp2.add(hv.p + c, 1, H.p + (i64)c * ldh * inner + i * ldh + i + 1, 1, 1, 1);
-        cp2.finalize();
-        cp2.run(st);
-      }
-      if (early_exit) {
-        // Hessenberg least-squares residual of the first i+1 steps, on the
-        // host (H is at most 17 x 16 per right-hand side).
-        std::vector<double> hh = H.download(st), bb = beta.download(st);
-        bool done = true;
-        for (i64 c = 0; c < nrhs && done; c++) {
-          if (!act[c]) continue;
-          double est = ls_residual(hh.data() + c * ldh * inner, ldh, (int)i + 2, (int)i + 1, bb[c]);
-          if (!(est / hn[c] < tol * 0.5)) done = false;
-        }
-        if (done) {
-          used = i + 1;
-          break;
+  ck(cudaMemcpyAsync(g.R.p, g.Bc.p, sizeof(double) * g.vstride, cudaMemcpyDeviceToDevice, st), "R=B");
+  const bool use_graph = A.h->graph_solve && !A.h->prof && A.h == M.h;
+  if (use_graph) {
+    // Everything a capture must not do (plan builds, uploads, allocations)
+    // happens here, once.
+    A.prepare(nrhs);
+    M.prepare(nrhs);
+    gmres_graph(A, M, g);
+  } else {
+    ck(launch_gmres_init(g.act.p, g.it.p, g.resh.p, (int)outer, tol, nr, g.ctl.p + 2, 0, 0, st), "init");
+    bool any = 0 < outer && tol <= 1.;
+    while (any) {
+      gmres_prologue(M, g, 0, 0, st);
+      for (i64 i = 0; i < inner; i++) {
+        gmres_step(A, M, g, i, 0, 0, st);
+        if (g.early) {
+          int stop = 0;
+          ck(cudaStreamSynchronize(st), "sync");
+          ck(cudaMemcpy(&stop, g.ctl.p + 1, sizeof(int), cudaMemcpyDeviceToHost), "stop flag");
+          if (stop) break;
         }
       }
+      gmres_epilogue(A, g, 0, 0, st);
+      std::vector<int> a = g.act.download(st), cyc(1);
+      ck(cudaMemcpy(cyc.data(), g.ctl.p + 2, sizeof(int), cudaMemcpyDeviceToHost), "cycles");
+      any = false;
+      for (int v : a) any |= v != 0;
+      if (cyc[0] >= outer) any = false;
     }
-    if (used == inner) {
-      ck(launch_gmres_ls(H.p, ldh, (int)inner, beta.p, y.p, nr, st), "ls");
-    } else {
-      // Compact the leading used x used block per rhs for the final solve.
-      DVec<double> Hs;
-      Hs.alloc((size_t)(used + 1) * used * nrhs);
-      CopyPlan<double> cp;
-      for (int c = 0; c < nr; c++)
-        cp.add(H.p + (i64)c * ldh * inner, ldh, Hs.p + (i64)c * (used + 1) * used, used + 1, (int)used + 1, (int)used);
-      cp.finalize();
-      cp.run(st);
-      ck(launch_gmres_ls(Hs.p, (int)used + 1, (int)used, beta.p, y.p, nr, st), "ls");
-    }
-    ck(launch_gs_update(X.p, V.p, vstride, y.p, used, (int)used, N, nr, 1.0, active.p, st), "x update");
-    ck(cudaMemcpyAsync(R.p, X.p, sizeof(double) * vstride, cudaMemcpyDeviceToDevice, st), "R=X");
-    A.matvec(nrhs, R.p, N);
-    ck(launch_axpby(R.p, Bc.p, -1.0, 1.0, vstride, st), "R=B-AX");
-    ck(launch_dots(R.p, 0, 1, R.p, N, nr, partial.p, nch, nrm2.p, st), "dots");
-    ck(launch_residual_norm_finish(nrm2.p, normb.p, rvec.p, nr, st), "resid");
-    std::vector<double> rv = rvec.download(st);
-    cycle++;
-    for (i64 c = 0; c < nrhs; c++) {
-      if (!act[c]) continue;
-      it[c]++;
-      res[c * (outer + 1) + it[c]] = rv[c];
-      if (!(it[c] < outer && tol <= rv[c])) act[c] = 0;
-    }
-    // Columns that stopped keep their X; columns still running restart from
-    // the true residual.  Converged columns keep R (unused).
   }
   for (i64 c = 0; c < nrhs; c++)
-    ck(cudaMemcpyAsync(dX + c * ld, X.p + c * N, sizeof(double) * N, cudaMemcpyDeviceToDevice, st), "copy X out");
-  ck(cudaStreamSynchronize(st), "sync");
+    ck(cudaMemcpyAsync(dX + c * ld, g.X.p + c * g.N, sizeof(double) * g.N, cudaMemcpyDeviceToDevice, st), "copy X out");
+  std::vector<double> res = g.resh.download(st);
+  std::vector<int> it = g.it.download(st);
   check_tc(A.h);
   check_tc(M.h);
   bool conv = true;
@@ -2794,6 +3010,16 @@ int h2dev_set_option(h2dev_handle_t h, int option, int64_t value) {
   if (option == H2DEV_OPT_SAMPLING) {
     require(value >= 0 && value <= 2, "sampling option must be 0, 1 or 2");
     h->sampling_mode = (int)value;
+    return H2DEV_OK;
+  }
+  if (option == H2DEV_OPT_GRAPH_SOLVE) {
+    require(value == 0 || value == 1, "graph option must be 0 or 1");
+    h->graph_solve = value != 0;
+    return H2DEV_OK;
+  }
+  if (option == H2DEV_OPT_PRECOND_BF16) {
+    require(value == 0 || value == 1, "BF16 substitution option must be 0 or 1");
+    h->precond_bf16 = value != 0;
     return H2DEV_OK;
   }
   if (option == H2DEV_OPT_MATRIX_FREE) {

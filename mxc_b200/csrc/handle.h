@@ -39,7 +39,9 @@ struct h2dev_handle_s {
   int* d_tc_err = nullptr;
   bool tc_pending = false;
   int sampling_mode = 0;  // far-list cap rule for solvers created next (H2DEV_OPT_SAMPLING)
-  bool matrix_free = false;  // operator-mode solvers created next keep no near blocks or couplings (H2DEV_OPT_MATRIX_FREE)
+  bool matrix_free = false;
+  bool precond_bf16 = false;
+  bool graph_solve = false;  // GMRES solves on this handle run as one captured CUDA graph (H2DEV_OPT_GRAPH_SOLVE)  // FP32 solvers created next apply their substitution from BF16 copies (H2DEV_OPT_PRECOND_BF16)  // operator-mode solvers created next keep no near blocks or couplings (H2DEV_OPT_MATRIX_FREE)
   int basis_mode = 0;  // 0: Gram + pivoted Cholesky for fixed-rank bases; 1: Householder TSQR everywhere
   // One reference held by the caller plus one per live solver: the stream
   // (and the stream-ordered memory freed on it) outlives every solver.

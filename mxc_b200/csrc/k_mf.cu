@@ -14,9 +14,10 @@
 // column bodies and the 32 x NR right-hand-side values go to shared memory
 // (row-contiguous, so each is read by a broadcast vector load), then every
 // thread evaluates its two rows against the 32 columns and updates its
-// accumulators.  FP64 throughout, one rsqrt per pair (kernel_fast, a few ulp
-// from the reference's std::hypot form); the summation order is fixed by the
-// plan, so results are deterministic.  Bound: FP64 FMA throughput (2 NR
+// accumulators.  FP64 throughout, one reciprocal square root per pair
+// (rsqrt_newton: an FP32 seed refined by two FP64 Newton steps, about 1 ulp;
+// the whole entry is a few ulp from the reference's std::hypot form); the
+// summation order is fixed by the plan, so results are deterministic.  Bound: FP64 FMA throughput (2 NR
 // multiply-adds plus one kernel evaluation per pair), not HBM.
 #include "common.cuh"
 #include "kernels.h"
@@ -27,7 +28,7 @@ namespace {
 
 constexpr int MF_NT = 128, MF_RPT = 2, MF_BM = MF_NT * MF_RPT, MF_KS = 32;
 
-template <int NR>
+template <int NR, int KIND>
 __global__ void __launch_bounds__(MF_NT, 4)
     k_mf_apply(KernelParams kp, const MfTask* __restrict__ tasks, const MfEntry* __restrict__ ents,
                const int2* __restrict__ tiles, int nr) {
@@ -67,8 +68,8 @@ __global__ void __launch_bounds__(MF_NT, 4)
       __syncthreads();
       for (int b = 0; b < kn; b++) {
         const double cx = cs[3 * b], cy = cs[3 * b + 1], cz = cs[3 * b + 2];
-        const double k0v = kernel_fast(kp, p0x - cx, p0y - cy, p0z - cz);
-        const double k1v = kernel_fast(kp, p1x - cx, p1y - cy, p1z - cz);
+        const double k0v = kernel_eval<KIND>(kp, p0x - cx, p0y - cy, p0z - cz);
+        const double k1v = kernel_eval<KIND>(kp, p1x - cx, p1y - cy, p1z - cz);
         const double* br = bs + b * NRP;
         if constexpr (NR == 1) {
           const double x = br[0];
@@ -105,24 +106,31 @@ __global__ void __launch_bounds__(MF_NT, 4)
 
 int mf_rows_per_cta() { return MF_BM; }
 
+template <int KIND>
+static cudaError_t mf_go(const KernelParams& kp, int nr, const MfTask* d_tasks, const MfEntry* d_ents,
+                         const int2* d_tiles, int ntiles, cudaStream_t st) {
+  switch (nr) {
+    case 1: k_mf_apply<1, KIND><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr); break;
+    case 2: k_mf_apply<2, KIND><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr); break;
+    case 3:
+    case 4: k_mf_apply<4, KIND><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr); break;
+    case 5:
+    case 6:
+    case 7:
+    case 8: k_mf_apply<8, KIND><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr); break;
+    default: k_mf_apply<16, KIND><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr);
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_mf_apply(const KernelParams& kp, int nr, const MfTask* d_tasks, const MfEntry* d_ents,
                             const int2* d_tiles, int ntiles, cudaStream_t st) {
   if (ntiles == 0) return cudaSuccess;
   if (nr < 1 || nr > 16) return cudaErrorInvalidValue;
   note_launch();
-  switch (nr) {
-    case 1: k_mf_apply<1><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr); break;
-    case 2: k_mf_apply<2><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr); break;
-    case 3:
-    case 4: k_mf_apply<4><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr); break;
-    case 5:
-    case 6:
-    case 7:
-    case 8: k_mf_apply<8><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr); break;
-    default:
-      k_mf_apply<16><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr);
-  }
-  return cudaGetLastError();
+  if (kp.kind == KERNEL_LAPLACE) return mf_go<KERNEL_LAPLACE>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
+  if (kp.kind == KERNEL_YUKAWA) return mf_go<KERNEL_YUKAWA>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
+  return mf_go<KERNEL_QUADRATIC>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
 }
 
 }  // namespace h2b

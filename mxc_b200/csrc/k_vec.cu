@@ -54,32 +54,40 @@ __global__ void __launch_bounds__(DOT_THREADS) k_dots_partial(const double* __re
   }
 }
 
-__global__ void k_dots_final(const double* __restrict__ partial, int nchunks, int kvec, int nrhs, double* __restrict__ out) {
+__global__ void k_dots_final(const double* __restrict__ partial, int nchunks, int kvec, int nrhs, double* __restrict__ out,
+                             i64 ostride) {
   int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= kvec * nrhs) return;
   int j = idx / nrhs, c = idx % nrhs;
   double s = 0.;
   for (int g = 0; g < nchunks; g++) s += partial[((i64)g * kvec + j) * nrhs + c];
-  out[(i64)c * kvec + j] = s;  // column c holds the kvec dots of rhs c
+  out[(i64)c * ostride + j] = s;  // rhs c's kvec dots at out + c * ostride
 }
 
-cudaError_t launch_dots(const double* V, i64 vstride, int kvec, const double* w, i64 n, int nrhs, double* partial,
-                        int nchunks, double* out, cudaStream_t st) {
+cudaError_t launch_dots_strided(const double* V, i64 vstride, int kvec, const double* w, i64 n, int nrhs,
+                                double* partial, int nchunks, double* out, i64 ostride, cudaStream_t st) {
   dim3 grid(nchunks, nrhs);
   note_launch();
   k_dots_partial<<<grid, DOT_THREADS, 0, st>>>(V, vstride, kvec, w, n, nrhs, partial);
   int tot = kvec * nrhs;
   note_launch();
-  k_dots_final<<<(tot + 127) / 128, 128, 0, st>>>(partial, nchunks, kvec, nrhs, out);
+  k_dots_final<<<(tot + 127) / 128, 128, 0, st>>>(partial, nchunks, kvec, nrhs, out, ostride);
   return cudaGetLastError();
 }
 
-// w[:, c] += sign * sum_j V_j[:, c] * h[c * hstride + j]   (active[c] != 0)
+cudaError_t launch_dots(const double* V, i64 vstride, int kvec, const double* w, i64 n, int nrhs, double* partial,
+                        int nchunks, double* out, cudaStream_t st) {
+  return launch_dots_strided(V, vstride, kvec, w, n, nrhs, partial, nchunks, out, kvec, st);
+}
+
+// w[:, c] += sign * sum_j V_j[:, c] * h[c * hstride + j]   (active[c] != 0;
+// j < *kdev when kdev is given, else j < kvec)
 __global__ void k_gs_update(double* __restrict__ w, const double* __restrict__ V, i64 vstride,
                             const double* __restrict__ h, i64 hstride, int kvec, i64 n, int nrhs, double sign,
-                            const int* __restrict__ active) {
+                            const int* __restrict__ active, const int* __restrict__ kdev) {
   const int c = blockIdx.y;
   if (active && !active[c]) return;
+  if (kdev) kvec = *kdev;
   const double* hc = h + (i64)c * hstride;
   for (i64 r = (i64)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (i64)gridDim.x * blockDim.x) {
     double s = 0.;
@@ -89,12 +97,12 @@ __global__ void k_gs_update(double* __restrict__ w, const double* __restrict__ V
 }
 
 cudaError_t launch_gs_update(double* w, const double* V, i64 vstride, const double* h, i64 hstride, int kvec, i64 n,
-                             int nrhs, double sign, const int* active, cudaStream_t st) {
+                             int nrhs, double sign, const int* active, cudaStream_t st, const int* kdev) {
   int gx = (int)((n + 255) / 256);
   gx = gx > 1024 ? 1024 : gx;
   dim3 grid(gx, nrhs);
   note_launch();
-  k_gs_update<<<grid, 256, 0, st>>>(w, V, vstride, h, hstride, kvec, n, nrhs, sign, active);
+  k_gs_update<<<grid, 256, 0, st>>>(w, V, vstride, h, hstride, kvec, n, nrhs, sign, active, kdev);
   return cudaGetLastError();
 }
 
@@ -123,13 +131,18 @@ cudaError_t launch_scale_by_norm(const double* w, double* vout, const double* nr
 // stride ld * inner); Householder QR in one thread per rhs (the reference
 // solves the same problem with HouseholderQR::solve, solver.cpp:190).
 __global__ void k_gmres_ls(const double* __restrict__ Hall, int ld, int inner, const double* __restrict__ beta,
-                           double* __restrict__ yall, int nrhs) {
+                           double* __restrict__ yall, int nrhs, const int* __restrict__ used) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nrhs) return;
+  const i64 hstride = (i64)ld * inner;
+  // With `used`: the leading (used + 1) x used block of each ld x inner H
+  // (rows below used + 1 of those columns are zero, so the reflections and
+  // sums equal those of the compacted block).
+  if (used) inner = *used;
   double H[17 * 16];
   double s[17];
   if (ld > 17 || inner > 16) return;
-  const double* Hc = Hall + (i64)c * ld * inner;
+  const double* Hc = Hall + (i64)c * hstride;
   for (int i = 0; i < ld * inner; i++) H[i] = Hc[i];
   for (int i = 0; i < ld; i++) s[i] = 0.;
   s[0] = beta[c];
@@ -158,7 +171,7 @@ __global__ void k_gmres_ls(const double* __restrict__ Hall, int ld, int inner, c
     d = 2. * d / vn;
     for (int r = k; r < ld; r++) s[r] -= d * v[r];
   }
-  double* y = yall + (i64)c * inner;
+  double* y = yall + (i64)c * (hstride / ld);
   for (int i = inner - 1; i >= 0; i--) {
     double t = s[i];
     for (int j = i + 1; j < inner; j++) t -= H[i + j * ld] * y[j];
@@ -167,9 +180,134 @@ __global__ void k_gmres_ls(const double* __restrict__ Hall, int ld, int inner, c
 }
 
 cudaError_t launch_gmres_ls(const double* H, int ld, int inner, const double* beta, double* y, int nrhs,
-                            cudaStream_t st) {
+                            cudaStream_t st, const int* used) {
   note_launch();
-  k_gmres_ls<<<(nrhs + 31) / 32, 32, 0, st>>>(H, ld, inner, beta, y, nrhs);
+  k_gmres_ls<<<(nrhs + 31) / 32, 32, 0, st>>>(H, ld, inner, beta, y, nrhs, used);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ device-side GMRES control
+// The convergence logic of the batched GMRES (solver.cpp:162-200 per column,
+// plus the early exit inside a cycle) kept on the device, so a whole solve
+// runs without host round trips; with `graph` set, the decisions also drive
+// the conditional nodes of a captured CUDA graph (the WHILE over restart
+// cycles, the IF around each Arnoldi step).
+
+// Start of the solve: resid[c][0] = 1, act[c] = (outer > 0 && tol <= 1),
+// it[c] = 0; the WHILE condition = any column active.
+__global__ void k_gmres_init(int* __restrict__ act, int* __restrict__ it, double* __restrict__ resh, int outer,
+                             double tol, int nrhs, int* __restrict__ cycles, int graph,
+                             cudaGraphConditionalHandle hw) {
+  int any = 0;
+  for (int c = threadIdx.x; c < nrhs; c += blockDim.x) {
+    act[c] = (0 < outer && tol <= 1.) ? 1 : 0;
+    it[c] = 0;
+    resh[(i64)c * (outer + 1)] = 1.;
+    any |= act[c];
+  }
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) {
+    *cycles = 0;
+    if (graph) cudaGraphSetConditional(hw, any ? 1u : 0u);
+  }
+}
+
+// Start of a cycle: every Arnoldi step enabled, `used` = inner.
+__global__ void k_gmres_cycle_begin(int* __restrict__ used, int* __restrict__ stop, int inner, int graph,
+                                    cudaGraphConditionalHandle hs) {
+  *used = inner;
+  *stop = 0;
+  if (graph) cudaGraphSetConditional(hs, 1u);
+}
+
+// After Arnoldi step i: the Givens residual estimate of every active column
+// (min || beta e1 - H y || over the first i + 1 steps); when all are below
+// tol / 2 relative to ||b||, the cycle ends here (used = i + 1).
+__global__ void k_gmres_estimate(const double* __restrict__ Hall, int ldh, int inner, int i,
+                                 const double* __restrict__ beta, const double* __restrict__ normb,
+                                 const int* __restrict__ act, int nrhs, double tol, int* __restrict__ used,
+                                 int* __restrict__ stop, int graph, cudaGraphConditionalHandle hs) {
+  int ok = 1;
+  for (int c = threadIdx.x; c < nrhs; c += blockDim.x) {
+    if (!act[c]) continue;
+    const double* Hc = Hall + (i64)c * ldh * inner;
+    const int rows = i + 2, cols = i + 1;
+    double H[17 * 16], s[17];
+    for (int j = 0; j < cols; j++)
+      for (int r = 0; r < rows; r++) H[r + j * rows] = Hc[r + (i64)j * ldh];
+    for (int r = 0; r < rows; r++) s[r] = 0.;
+    s[0] = beta[c];
+    for (int k = 0; k < cols; k++) {
+      const double a = H[k + k * rows], b = H[k + 1 + k * rows];
+      const double r = hypot(a, b);
+      if (r == 0.) continue;
+      const double cs = a / r, sn = b / r;
+      for (int j = k; j < cols; j++) {
+        const double x = H[k + j * rows], y = H[k + 1 + j * rows];
+        H[k + j * rows] = cs * x + sn * y;
+        H[k + 1 + j * rows] = -sn * x + cs * y;
+      }
+      const double x = s[k], y = s[k + 1];
+      s[k] = cs * x + sn * y;
+      s[k + 1] = -sn * x + cs * y;
+    }
+    const double est = fabs(s[cols]) / normb[c];
+    if (!(est < tol * 0.5)) ok = 0;
+  }
+  ok = __syncthreads_and(ok);
+  if (threadIdx.x == 0 && ok && !*stop) {
+    *used = i + 1;
+    *stop = 1;
+    if (graph) cudaGraphSetConditional(hs, 0u);
+  }
+}
+
+// End of a cycle: record the true residual of every active column, retire
+// columns that converged or ran out of cycles; WHILE condition = any active
+// (and fewer than `outer` cycles done).
+__global__ void k_gmres_cycle_end(const double* __restrict__ rvec, int* __restrict__ act, int* __restrict__ it,
+                                  double* __restrict__ resh, int outer, double tol, int nrhs, int* __restrict__ cycles,
+                                  int graph, cudaGraphConditionalHandle hw) {
+  int any = 0;
+  for (int c = threadIdx.x; c < nrhs; c += blockDim.x) {
+    if (act[c]) {
+      const int k = ++it[c];
+      resh[(i64)c * (outer + 1) + k] = rvec[c];
+      if (!(k < outer && tol <= rvec[c])) act[c] = 0;
+    }
+    any |= act[c];
+  }
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) {
+    const int cy = ++*cycles;
+    if (graph) cudaGraphSetConditional(hw, (any && cy < outer) ? 1u : 0u);
+  }
+}
+
+cudaError_t launch_gmres_init(int* act, int* it, double* resh, int outer, double tol, int nrhs, int* cycles,
+                              int graph, cudaGraphConditionalHandle hw, cudaStream_t st) {
+  note_launch();
+  k_gmres_init<<<1, 128, 0, st>>>(act, it, resh, outer, tol, nrhs, cycles, graph, hw);
+  return cudaGetLastError();
+}
+cudaError_t launch_gmres_cycle_begin(int* used, int* stop, int inner, int graph, cudaGraphConditionalHandle hs,
+                                     cudaStream_t st) {
+  note_launch();
+  k_gmres_cycle_begin<<<1, 1, 0, st>>>(used, stop, inner, graph, hs);
+  return cudaGetLastError();
+}
+cudaError_t launch_gmres_estimate(const double* H, int ldh, int inner, int i, const double* beta, const double* normb,
+                                  const int* act, int nrhs, double tol, int* used, int* stop, int graph,
+                                  cudaGraphConditionalHandle hs, cudaStream_t st) {
+  if (ldh > 17 || i + 2 > 17) return cudaErrorInvalidValue;
+  note_launch();
+  k_gmres_estimate<<<1, 32, 0, st>>>(H, ldh, inner, i, beta, normb, act, nrhs, tol, used, stop, graph, hs);
+  return cudaGetLastError();
+}
+cudaError_t launch_gmres_cycle_end(const double* rvec, int* act, int* it, double* resh, int outer, double tol,
+                                   int nrhs, int* cycles, int graph, cudaGraphConditionalHandle hw, cudaStream_t st) {
+  note_launch();
+  k_gmres_cycle_end<<<1, 128, 0, st>>>(rvec, act, it, resh, outer, tol, nrhs, cycles, graph, hw);
   return cudaGetLastError();
 }
 

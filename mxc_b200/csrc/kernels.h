@@ -1,6 +1,7 @@
 // Launch interfaces of the device kernels (host-callable, no torch types).
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -176,6 +177,33 @@ cudaError_t launch_mf_apply(const KernelParams& kp, int nr, const MfTask* d_task
                             const int2* d_tiles, int ntiles, cudaStream_t st);
 int mf_rows_per_cta();
 
+// BF16 substitution blocks (k_bf16.cu).  Pack: dst (m x k, ld ldd, a
+// multiple of 8) = bf16(src / s), s = 2^ceil(log2 max |src|) written to
+// *scale.  Apply: GemmTask<float> tasks with BfEntry entries, C = beta C +
+// sum_e (alpha_e *scale_e) A_e B_e (A_e BF16 packed, B_e FP32 k x n);
+// tiles {task, block of bf16_rows_per_cta() rows}; n <= 16.
+struct BfPackTask {
+  const float* src;
+  i64 lds;
+  int m, k;
+  __nv_bfloat16* dst;
+  i64 ldd;
+  float* scale;
+};
+struct BfEntry {
+  const __nv_bfloat16* A;
+  i64 lda;
+  const float* B;
+  i64 ldb;
+  int k;
+  float alpha;
+  const float* scale;
+};
+cudaError_t launch_bf16_pack(const BfPackTask* d_tasks, int ntasks, cudaStream_t st);
+cudaError_t launch_stream_bf16(int nr, const GemmTask<float>* d_tasks, const BfEntry* d_ents, const int2* d_tiles,
+                               int ntiles, cudaStream_t st);
+int bf16_rows_per_cta();
+
 template <typename T>
 struct CopyEntry {
   const T* src;
@@ -229,11 +257,24 @@ cudaError_t launch_dots(const double* V, i64 vstride, int kvec, const double* w,
                         int nchunks, double* out, cudaStream_t st);
 int dots_chunks(i64 n);
 cudaError_t launch_gs_update(double* w, const double* V, i64 vstride, const double* h, i64 hstride, int kvec, i64 n,
-                             int nrhs, double sign, const int* active, cudaStream_t st);
+                             int nrhs, double sign, const int* active, cudaStream_t st, const int* kdev = nullptr);
+cudaError_t launch_dots_strided(const double* V, i64 vstride, int kvec, const double* w, i64 n, int nrhs,
+                                double* partial, int nchunks, double* out, i64 ostride, cudaStream_t st);
+// Device-side GMRES control (k_vec.cu); graph != 0 also sets the given
+// conditional handles of a captured graph.
+cudaError_t launch_gmres_init(int* act, int* it, double* resh, int outer, double tol, int nrhs, int* cycles,
+                              int graph, cudaGraphConditionalHandle hw, cudaStream_t st);
+cudaError_t launch_gmres_cycle_begin(int* used, int* stop, int inner, int graph, cudaGraphConditionalHandle hs,
+                                     cudaStream_t st);
+cudaError_t launch_gmres_estimate(const double* H, int ldh, int inner, int i, const double* beta, const double* normb,
+                                  const int* act, int nrhs, double tol, int* used, int* stop, int graph,
+                                  cudaGraphConditionalHandle hs, cudaStream_t st);
+cudaError_t launch_gmres_cycle_end(const double* rvec, int* act, int* it, double* resh, int outer, double tol,
+                                   int nrhs, int* cycles, int graph, cudaGraphConditionalHandle hw, cudaStream_t st);
 cudaError_t launch_scale_by_norm(const double* w, double* vout, const double* nrm2, double* hout, i64 hstride,
                                  i64 n, int nrhs, cudaStream_t st);
 cudaError_t launch_gmres_ls(const double* H, int ld, int inner, const double* beta, double* y, int nrhs,
-                            cudaStream_t st);
+                            cudaStream_t st, const int* used = nullptr);
 cudaError_t launch_axpby(double* y, const double* x, double a, double b, i64 n, cudaStream_t st);
 cudaError_t launch_residual_norm_finish(const double* nrm2, const double* normb, double* resid, int nrhs,
                                         cudaStream_t st);
