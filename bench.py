@@ -55,7 +55,9 @@ def parse():
     ap.add_argument("--samples", type=int, default=4000)
     ap.add_argument("--op-sampling", default="sketch", choices=["sketch", "strided"],
                     help="operator bases: sketch of every far body (default) or --op-samples strided samples")
-    ap.add_argument("--op-samples", type=int, default=16000, help="strided samples per box with --op-sampling strided")
+    ap.add_argument("--op-samples", type=int, default=4000,
+                    help="sketch: strided samples of the far list beyond the nearest three levels (0: every far "
+                         "body); strided: samples per box")
     ap.add_argument("--op-eps", type=float, default=1e-11)
     ap.add_argument("--op-storage", default="stored", choices=["matrix-free", "stored"],
                     help="operator near blocks and couplings stored (default) or evaluated inside the matvec")
@@ -91,8 +93,11 @@ def parse():
 def op_desc(a) -> str:
     st = ("near blocks and couplings evaluated in the matvec (matrix-free)" if a.op_storage == "matrix-free"
           else "near blocks and couplings stored")
-    if a.op_sampling == "sketch":
+    if a.op_sampling == "sketch" and a.op_samples <= 0:
         return "ID bases from an M-row random-sign sketch of every far body; " + st
+    if a.op_sampling == "sketch":
+        return ("ID bases from an M-row random-sign sketch of the far bodies of the nearest three levels plus %d "
+                "strided farther ones; %s" % (a.op_samples, st))
     return "ID bases from %d strided far samples; %s" % (a.op_samples, st)
 
 
@@ -318,8 +323,8 @@ def run_ours(a):
             h.profile(True)
         t0 = time.time()
         try:
-            Aop = m.H2MatrixSolver(h, kern, a.op_eps, a.rank, 0, tree, a.theta, b,
-                                   samples=0 if a.op_sampling == "sketch" else a.op_samples, precision=m.FP64)
+            Aop = m.H2MatrixSolver(h, kern, a.op_eps, a.rank, 0, tree, a.theta, b, samples=a.op_samples,
+                                   precision=m.FP64)
             h.synchronize()
         finally:
             h.set_option(m._lib.OPT_SAMPLING, m._lib.SAMPLING_STRIDED)
@@ -696,7 +701,7 @@ class OracleSample:
         self.k = O.Kernel(O.LAPLACE, a.singularity)
         mode = 2 if a.op_sampling == "sketch" else 0
         self.A = O.H2MatrixSolver(self.k, a.op_eps, a.rank, 0, self.cells, a.theta, self.bodies, self.L,
-                                  0 if mode == 2 else a.op_samples, mode)
+                                  a.op_samples, mode)
         X = np.random.default_rng(20261203).random((ns, a.nrhs))
         self.B = O.dense_matvec(self.k, self.bodies, X)
 
@@ -743,8 +748,7 @@ def gpu_at_sample(a, h, ns: int) -> dict:
     h.set_option(m._lib.OPT_SAMPLING, m._lib.SAMPLING_SKETCH if a.op_sampling == "sketch" else m._lib.SAMPLING_STRIDED)
     h.set_option(m._lib.OPT_MATRIX_FREE, 1 if a.op_storage == "matrix-free" else 0)
     try:
-        A = m.H2MatrixSolver(h, k, a.op_eps, a.rank, 0, t, a.theta, b,
-                             samples=0 if a.op_sampling == "sketch" else a.op_samples)
+        A = m.H2MatrixSolver(h, k, a.op_eps, a.rank, 0, t, a.theta, b, samples=a.op_samples)
     finally:
         h.set_option(m._lib.OPT_SAMPLING, m._lib.SAMPLING_STRIDED)
         h.set_option(m._lib.OPT_MATRIX_FREE, 0)

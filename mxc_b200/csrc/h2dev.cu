@@ -926,13 +926,32 @@ class Solver : public SolverBase {
       const bool sketch = sampling_mode == 2;
       std::vector<i64> roff, rstart, rend;
       if (sketch) {
+        // samples <= 0: every far body.  samples > 0: the far boxes of this
+        // level and the two above it in full (they hold the numerical rank)
+        // plus `samples` strided bodies of the farther list, whose
+        // interactions are smooth -- the whole far field's accuracy at a
+        // cost that no longer grows with N.
         roff.assign(nodes + 1, 0);
+        std::vector<int> tmp;
         for (i64 i = 0; i < nodes; i++) {
+          const auto& rl = ranges[g0 + i];
+          const auto& gs = gstart[g0 + i];
+          size_t cut = 0;
+          if (samples > 0 && gs.size() >= 3) cut = (size_t)gs[gs.size() - 3];
           i64 cnt = 0;
-          for (const auto& r : ranges[g0 + i]) {
-            cnt += r.second - r.first;
-            rstart.push_back(r.first);
+          for (size_t q = cut; q < rl.size(); q++) {
+            cnt += rl[q].second - rl[q].first;
+            rstart.push_back(rl[q].first);
             rend.push_back(cnt);
+          }
+          if (cut > 0) {
+            std::vector<std::pair<i64, i64>> farther(rl.begin(), rl.begin() + cut);
+            sample_far_list(farther, samples, tmp);
+            for (int b : tmp) {
+              cnt += 1;
+              rstart.push_back(b);
+              rend.push_back(cnt);
+            }
           }
           roff[i + 1] = (i64)rstart.size();
           soff[i + 1] = soff[i] + cnt;
@@ -2161,18 +2180,16 @@ struct GmresState {
   DVec<int> act, it, ctl;  // ctl: used, stop, cycles
 };
 
-static void gmres_prologue(SolverBase& M, GmresState& g, int graph, cudaGraphConditionalHandle hs,
-                           cudaStream_t st) {
+static void gmres_prologue(SolverBase& M, GmresState& g, cudaStream_t st) {
   const int nr = (int)g.nrhs;
-  ck(launch_gmres_cycle_begin(g.ctl.p, g.ctl.p + 1, (int)g.inner, graph, hs, st), "cycle begin");
+  ck(launch_gmres_cycle_begin(g.ctl.p, (int)g.inner, st), "cycle begin");
   M.precondition(g.nrhs, g.R.p, g.N);
   ck(launch_dots(g.R.p, 0, 1, g.R.p, g.N, nr, g.partial.p, g.nch, g.nrm2.p, st), "dots");
   ck(launch_scale_by_norm(g.R.p, g.V.p, g.nrm2.p, g.beta.p, 1, g.N, nr, st), "v0");
   ck(cudaMemsetAsync(g.H.p, 0, sizeof(double) * g.H.n, st), "H=0");
 }
 
-static void gmres_step(SolverBase& A, SolverBase& M, GmresState& g, i64 i, int graph, cudaGraphConditionalHandle hs,
-                       cudaStream_t st) {
+static void gmres_step(SolverBase& A, SolverBase& M, GmresState& g, i64 i, cudaStream_t st) {
   const int nr = (int)g.nrhs, kv = (int)i + 1;
   const i64 hstride = (i64)g.ldh * g.inner;
   ck(cudaMemcpyAsync(g.w.p, g.V.p + i * g.vstride, sizeof(double) * g.vstride, cudaMemcpyDeviceToDevice, st), "w=v");
@@ -2191,7 +2208,7 @@ static void gmres_step(SolverBase& A, SolverBase& M, GmresState& g, i64 i, int g
   ck(launch_scale_by_norm(g.w.p, g.V.p + (i + 1) * g.vstride, g.nrm2.p, hcol + i + 1, hstride, g.N, nr, st), "scale");
   if (g.early)
     ck(launch_gmres_estimate(g.H.p, g.ldh, (int)g.inner, (int)i, g.beta.p, g.normb.p, g.act.p, nr, g.tol, g.ctl.p,
-                             g.ctl.p + 1, graph, hs, st),
+                             st),
        "estimate");
 }
 
@@ -2205,99 +2222,107 @@ static void gmres_epilogue(SolverBase& A, GmresState& g, int graph, cudaGraphCon
   ck(launch_axpby(g.R.p, g.Bc.p, -1.0, 1.0, g.vstride, st), "R=B-AX");
   ck(launch_dots(g.R.p, 0, 1, g.R.p, g.N, nr, g.partial.p, g.nch, g.nrm2.p, st), "dots");
   ck(launch_residual_norm_finish(g.nrm2.p, g.normb.p, g.rvec.p, nr, st), "resid");
-  ck(launch_gmres_cycle_end(g.rvec.p, g.act.p, g.it.p, g.resh.p, (int)g.outer, g.tol, nr, g.ctl.p + 2, graph, hw, st),
+  ck(launch_gmres_cycle_end(g.rvec.p, g.act.p, g.it.p, g.resh.p, (int)g.outer, g.tol, nr, g.ctl.p, st),
      "cycle end");
+  if (graph) ck(launch_graph_condition(hw, g.ctl.p + 3, 0, st), "cycle condition");
 }
 
-// The whole solve as one graph: init kernel, then WHILE(any column active)
-// { prologue; IF(step enabled) { Arnoldi step i } for i < inner; epilogue }.
-// Library launches go to h->stream, which is pointed at each body's capture
-// stream in turn (the side stream of the matvec joins and leaves every
-// capture by its events, so the bodies hold kernels and copies only).
+// The whole solve as one graph: init kernel, then WHILE(another cycle)
+// { prologue; [IF(not stopped) { Arnoldi step i }] for i < inner; epilogue }.
+// A conditional handle belongs to one node, so each IF node has its own,
+// set from the stop flag by a small kernel just before it.  Library launches
+// go to h->stream, pointed at each body's capture stream in turn; the matvec
+// keeps its near field on that stream while capturing (no side-stream fork),
+// so the bodies hold kernels, copies and memsets only.
 static void gmres_graph(SolverBase& A, SolverBase& M, GmresState& g) {
   h2dev_handle_s* h = A.h;
   cudaStream_t s0 = h->stream;
+  cudaStream_t side = h->stream2;
   cudaStream_t sb = nullptr, ss = nullptr;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  struct Restore {
+  // Restores the handle and releases the capture streams and graphs on every
+  // exit; captures still open (after an error) are ended first, innermost
+  // first, so no stream is destroyed mid-capture.
+  struct Scope {
     h2dev_handle_s* h;
-    cudaStream_t s0, sb, ss;
-    cudaGraph_t* g;
-    cudaGraphExec_t* e;
-    ~Restore() {
+    cudaStream_t s0, side, sb = nullptr, ss = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~Scope() {
+      for (cudaStream_t s : {ss, sb, s0}) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (s && cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+          cudaGraph_t junk = nullptr;
+          cudaStreamEndCapture(s, &junk);
+          if (junk && s == s0) cudaGraphDestroy(junk);
+        }
+      }
+      cudaGetLastError();
       h->stream = s0;
-      if (*e) cudaGraphExecDestroy(*e);
-      if (*g) cudaGraphDestroy(*g);
+      h->stream2 = side;
+      if (exec) cudaGraphExecDestroy(exec);
+      if (graph) cudaGraphDestroy(graph);
       if (sb) cudaStreamDestroy(sb);
       if (ss) cudaStreamDestroy(ss);
     }
-  } restore{h, s0, nullptr, nullptr, &graph, &exec};
+  } scope{h, s0, side};
+  h->stream2 = nullptr;
   ck(cudaStreamCreateWithFlags(&sb, cudaStreamNonBlocking), "stream");
-  restore.sb = sb;
+  scope.sb = sb;
   ck(cudaStreamCreateWithFlags(&ss, cudaStreamNonBlocking), "stream");
-  restore.ss = ss;
+  scope.ss = ss;
   ck(cudaStreamBeginCapture(s0, cudaStreamCaptureModeRelaxed), "capture");
-  try {
-    cudaGraph_t g0 = nullptr;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t ndeps = 0;
-    cudaStreamCaptureStatus cs;
-    ck(cudaStreamGetCaptureInfo(s0, &cs, nullptr, &g0, &deps, &ndeps), "capture info");
-    cudaGraphConditionalHandle hw;
-    ck(cudaGraphConditionalHandleCreate(&hw, g0, 0, 0), "conditional handle");
-    ck(launch_gmres_init(g.act.p, g.it.p, g.resh.p, (int)g.outer, g.tol, (int)g.nrhs, g.ctl.p + 2, 1, hw, s0),
-       "init");
-    ck(cudaStreamGetCaptureInfo(s0, &cs, nullptr, &g0, &deps, &ndeps), "capture info");
-    cudaGraphNodeParams wp = {};
-    wp.type = cudaGraphNodeTypeConditional;
-    wp.conditional.handle = hw;
-    wp.conditional.type = cudaGraphCondTypeWhile;
-    wp.conditional.size = 1;
-    cudaGraphNode_t wnode;
-    ck(cudaGraphAddNode(&wnode, g0, deps, ndeps, &wp), "while node");
-    ck(cudaStreamUpdateCaptureDependencies(s0, &wnode, 1, cudaStreamSetCaptureDependencies), "capture deps");
-    cudaGraph_t body = wp.conditional.phGraph_out[0];
-    cudaGraphConditionalHandle hs;
-    ck(cudaGraphConditionalHandleCreate(&hs, body, 1, cudaGraphCondAssignDefault), "conditional handle");
+  cudaGraph_t g0 = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  cudaStreamCaptureStatus cs;
+  ck(cudaStreamGetCaptureInfo(s0, &cs, nullptr, &g0, &deps, &ndeps), "capture info");
+  cudaGraphConditionalHandle hw;
+  ck(cudaGraphConditionalHandleCreate(&hw, g0, 0, 0), "conditional handle");
+  ck(launch_gmres_init(g.act.p, g.it.p, g.resh.p, (int)g.outer, g.tol, (int)g.nrhs, g.ctl.p, s0), "init");
+  ck(launch_graph_condition(hw, g.ctl.p + 3, 0, s0), "cycle condition");
+  ck(cudaStreamGetCaptureInfo(s0, &cs, nullptr, &g0, &deps, &ndeps), "capture info");
+  cudaGraphNodeParams wp = {};
+  wp.type = cudaGraphNodeTypeConditional;
+  wp.conditional.handle = hw;
+  wp.conditional.type = cudaGraphCondTypeWhile;
+  wp.conditional.size = 1;
+  cudaGraphNode_t wnode;
+  ck(cudaGraphAddNode(&wnode, g0, deps, ndeps, &wp), "while node");
+  ck(cudaStreamUpdateCaptureDependencies(s0, &wnode, 1, cudaStreamSetCaptureDependencies), "capture deps");
+  cudaGraph_t body = wp.conditional.phGraph_out[0];
+  h->stream = sb;
+  ck(cudaStreamBeginCaptureToGraph(sb, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed), "body capture");
+  gmres_prologue(M, g, sb);
+  for (i64 i = 0; i < g.inner; i++) {
+    cudaGraphConditionalHandle hi;
+    ck(cudaGraphConditionalHandleCreate(&hi, body, 0, 0), "conditional handle");
+    ck(launch_graph_condition(hi, g.ctl.p + 1, 1, sb), "step condition");  // step i runs unless stopped
+    cudaGraph_t bg = nullptr;
+    ck(cudaStreamGetCaptureInfo(sb, &cs, nullptr, &bg, &deps, &ndeps), "capture info");
+    cudaGraphNodeParams ip = {};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = hi;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    cudaGraphNode_t inode;
+    ck(cudaGraphAddNode(&inode, bg, deps, ndeps, &ip), "if node");
+    ck(cudaStreamUpdateCaptureDependencies(sb, &inode, 1, cudaStreamSetCaptureDependencies), "capture deps");
+    h->stream = ss;
+    ck(cudaStreamBeginCaptureToGraph(ss, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeRelaxed),
+       "step capture");
+    gmres_step(A, M, g, i, ss);
+    cudaGraph_t done = nullptr;
+    ck(cudaStreamEndCapture(ss, &done), "step capture end");
     h->stream = sb;
-    ck(cudaStreamBeginCaptureToGraph(sb, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed), "body capture");
-    gmres_prologue(M, g, 1, hs, sb);
-    for (i64 i = 0; i < g.inner; i++) {
-      cudaGraph_t bg = nullptr;
-      ck(cudaStreamGetCaptureInfo(sb, &cs, nullptr, &bg, &deps, &ndeps), "capture info");
-      cudaGraphNodeParams ip = {};
-      ip.type = cudaGraphNodeTypeConditional;
-      ip.conditional.handle = hs;
-      ip.conditional.type = cudaGraphCondTypeIf;
-      ip.conditional.size = 1;
-      cudaGraphNode_t inode;
-      ck(cudaGraphAddNode(&inode, bg, deps, ndeps, &ip), "if node");
-      ck(cudaStreamUpdateCaptureDependencies(sb, &inode, 1, cudaStreamSetCaptureDependencies), "capture deps");
-      h->stream = ss;
-      ck(cudaStreamBeginCaptureToGraph(ss, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                       cudaStreamCaptureModeRelaxed),
-         "step capture");
-      gmres_step(A, M, g, i, 1, hs, ss);
-      cudaGraph_t done = nullptr;
-      ck(cudaStreamEndCapture(ss, &done), "step capture end");
-      h->stream = sb;
-    }
-    gmres_epilogue(A, g, 1, hw, sb);
-    cudaGraph_t bdone = nullptr;
-    ck(cudaStreamEndCapture(sb, &bdone), "body capture end");
-    h->stream = s0;
-  } catch (...) {
-    h->stream = s0;
-    cudaGraph_t junk = nullptr;
-    cudaStreamEndCapture(s0, &junk);
-    if (junk) cudaGraphDestroy(junk);
-    cudaGetLastError();
-    throw;
   }
-  ck(cudaStreamEndCapture(s0, &graph), "capture end");
-  ck(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
-  ck(cudaGraphLaunch(exec, s0), "graph launch");
+  gmres_epilogue(A, g, 1, hw, sb);
+  cudaGraph_t bdone = nullptr;
+  ck(cudaStreamEndCapture(sb, &bdone), "body capture end");
+  h->stream = s0;
+  ck(cudaStreamEndCapture(s0, &scope.graph), "capture end");
+  ck(cudaGraphInstantiate(&scope.exec, scope.graph, 0), "graph instantiate");
+  ck(cudaGraphLaunch(scope.exec, s0), "graph launch");
   ck(cudaStreamSynchronize(s0), "sync");
 }
 
@@ -2359,12 +2384,12 @@ static int gmres(SolverBase& A, SolverBase& M, double tol, i64 nrhs, double* dX,
     M.prepare(nrhs);
     gmres_graph(A, M, g);
   } else {
-    ck(launch_gmres_init(g.act.p, g.it.p, g.resh.p, (int)outer, tol, nr, g.ctl.p + 2, 0, 0, st), "init");
+    ck(launch_gmres_init(g.act.p, g.it.p, g.resh.p, (int)outer, tol, nr, g.ctl.p, st), "init");
     bool any = 0 < outer && tol <= 1.;
     while (any) {
-      gmres_prologue(M, g, 0, 0, st);
+      gmres_prologue(M, g, st);
       for (i64 i = 0; i < inner; i++) {
-        gmres_step(A, M, g, i, 0, 0, st);
+        gmres_step(A, M, g, i, st);
         if (g.early) {
           int stop = 0;
           ck(cudaStreamSynchronize(st), "sync");
@@ -2373,21 +2398,20 @@ static int gmres(SolverBase& A, SolverBase& M, double tol, i64 nrhs, double* dX,
         }
       }
       gmres_epilogue(A, g, 0, 0, st);
-      std::vector<int> a = g.act.download(st), cyc(1);
-      ck(cudaMemcpy(cyc.data(), g.ctl.p + 2, sizeof(int), cudaMemcpyDeviceToHost), "cycles");
-      any = false;
-      for (int v : a) any |= v != 0;
-      if (cyc[0] >= outer) any = false;
+      std::vector<int> c4 = g.ctl.download(st);
+      any = c4[3] != 0;
     }
   }
   for (i64 c = 0; c < nrhs; c++)
     ck(cudaMemcpyAsync(dX + c * ld, g.X.p + c * g.N, sizeof(double) * g.N, cudaMemcpyDeviceToDevice, st), "copy X out");
   std::vector<double> res = g.resh.download(st);
   std::vector<int> it = g.it.download(st);
+  ck(cudaGetLastError(), "gmres");
   check_tc(A.h);
   check_tc(M.h);
   bool conv = true;
   for (i64 c = 0; c < nrhs; c++) {
+    require(it[c] >= 0 && it[c] <= outer, "gmres: cycle count out of range (device control state)");
     for (i64 k = 0; k <= outer; k++) resid[c * (outer + 1) + k] = res[c * (outer + 1) + k];
     if (iters) iters[c] = it[c];
     if (!(res[c * (outer + 1) + it[c]] < tol)) conv = false;

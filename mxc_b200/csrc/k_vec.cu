@@ -186,18 +186,45 @@ cudaError_t launch_gmres_ls(const double* H, int ld, int inner, const double* be
   return cudaGetLastError();
 }
 
+// y = a * y + b * x
+__global__ void k_axpby(double* __restrict__ y, const double* __restrict__ x, double a, double b, i64 n) {
+  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
+    y[i] = a * y[i] + b * x[i];
+}
+cudaError_t launch_axpby(double* y, const double* x, double a, double b, i64 n, cudaStream_t st) {
+  int grid = (int)((n + 255) / 256);
+  grid = grid > 148 * 16 ? 148 * 16 : grid;
+  note_launch();
+  k_axpby<<<grid, 256, 0, st>>>(y, x, a, b, n);
+  return cudaGetLastError();
+}
+
+__global__ void k_resid_finish(const double* __restrict__ nrm2, const double* __restrict__ normb, double* __restrict__ resid,
+                               int nrhs) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < nrhs) resid[c] = sqrt(nrm2[c]) / normb[c];
+}
+cudaError_t launch_residual_norm_finish(const double* nrm2, const double* normb, double* resid, int nrhs,
+                                        cudaStream_t st) {
+  note_launch();
+  k_resid_finish<<<(nrhs + 127) / 128, 128, 0, st>>>(nrm2, normb, resid, nrhs);
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------------ device-side GMRES control
 // The convergence logic of the batched GMRES (solver.cpp:162-200 per column,
 // plus the early exit inside a cycle) kept on the device, so a whole solve
-// runs without host round trips; with `graph` set, the decisions also drive
-// the conditional nodes of a captured CUDA graph (the WHILE over restart
-// cycles, the IF around each Arnoldi step).
+// needs no host round trip: the kernels below keep the active flags, the
+// residual history and two control words (ctl[0] = Arnoldi steps used in the
+// cycle, ctl[1] = stop flag, ctl[2] = cycles done, ctl[3] = "another cycle"
+// flag).  A captured graph turns the control words into the values of its
+// conditional nodes with k_graph_condition (the only kernel that touches a
+// graph handle).
 
 // Start of the solve: resid[c][0] = 1, act[c] = (outer > 0 && tol <= 1),
-// it[c] = 0; the WHILE condition = any column active.
+// it[c] = 0; ctl[3] = any column active.
 __global__ void k_gmres_init(int* __restrict__ act, int* __restrict__ it, double* __restrict__ resh, int outer,
-                             double tol, int nrhs, int* __restrict__ cycles, int graph,
-                             cudaGraphConditionalHandle hw) {
+                             double tol, int nrhs, int* __restrict__ ctl) {
   int any = 0;
   for (int c = threadIdx.x; c < nrhs; c += blockDim.x) {
     act[c] = (0 < outer && tol <= 1.) ? 1 : 0;
@@ -207,26 +234,23 @@ __global__ void k_gmres_init(int* __restrict__ act, int* __restrict__ it, double
   }
   any = __syncthreads_or(any);
   if (threadIdx.x == 0) {
-    *cycles = 0;
-    if (graph) cudaGraphSetConditional(hw, any ? 1u : 0u);
+    ctl[2] = 0;
+    ctl[3] = any ? 1 : 0;
   }
 }
 
 // Start of a cycle: every Arnoldi step enabled, `used` = inner.
-__global__ void k_gmres_cycle_begin(int* __restrict__ used, int* __restrict__ stop, int inner, int graph,
-                                    cudaGraphConditionalHandle hs) {
-  *used = inner;
-  *stop = 0;
-  if (graph) cudaGraphSetConditional(hs, 1u);
+__global__ void k_gmres_cycle_begin(int* __restrict__ ctl, int inner) {
+  ctl[0] = inner;
+  ctl[1] = 0;
 }
 
 // After Arnoldi step i: the Givens residual estimate of every active column
 // (min || beta e1 - H y || over the first i + 1 steps); when all are below
-// tol / 2 relative to ||b||, the cycle ends here (used = i + 1).
+// tol / 2 relative to ||b||, the cycle ends here (used = i + 1, stop = 1).
 __global__ void k_gmres_estimate(const double* __restrict__ Hall, int ldh, int inner, int i,
                                  const double* __restrict__ beta, const double* __restrict__ normb,
-                                 const int* __restrict__ act, int nrhs, double tol, int* __restrict__ used,
-                                 int* __restrict__ stop, int graph, cudaGraphConditionalHandle hs) {
+                                 const int* __restrict__ act, int nrhs, double tol, int* __restrict__ ctl) {
   int ok = 1;
   for (int c = threadIdx.x; c < nrhs; c += blockDim.x) {
     if (!act[c]) continue;
@@ -255,19 +279,17 @@ __global__ void k_gmres_estimate(const double* __restrict__ Hall, int ldh, int i
     if (!(est < tol * 0.5)) ok = 0;
   }
   ok = __syncthreads_and(ok);
-  if (threadIdx.x == 0 && ok && !*stop) {
-    *used = i + 1;
-    *stop = 1;
-    if (graph) cudaGraphSetConditional(hs, 0u);
+  if (threadIdx.x == 0 && ok && !ctl[1]) {
+    ctl[0] = i + 1;
+    ctl[1] = 1;
   }
 }
 
 // End of a cycle: record the true residual of every active column, retire
-// columns that converged or ran out of cycles; WHILE condition = any active
-// (and fewer than `outer` cycles done).
+// columns that converged or ran out of cycles; ctl[3] = another cycle
+// (any column active and fewer than `outer` cycles done).
 __global__ void k_gmres_cycle_end(const double* __restrict__ rvec, int* __restrict__ act, int* __restrict__ it,
-                                  double* __restrict__ resh, int outer, double tol, int nrhs, int* __restrict__ cycles,
-                                  int graph, cudaGraphConditionalHandle hw) {
+                                  double* __restrict__ resh, int outer, double tol, int nrhs, int* __restrict__ ctl) {
   int any = 0;
   for (int c = threadIdx.x; c < nrhs; c += blockDim.x) {
     if (act[c]) {
@@ -279,60 +301,45 @@ __global__ void k_gmres_cycle_end(const double* __restrict__ rvec, int* __restri
   }
   any = __syncthreads_or(any);
   if (threadIdx.x == 0) {
-    const int cy = ++*cycles;
-    if (graph) cudaGraphSetConditional(hw, (any && cy < outer) ? 1u : 0u);
+    const int cy = ++ctl[2];
+    ctl[3] = (any && cy < outer) ? 1 : 0;
   }
 }
 
-cudaError_t launch_gmres_init(int* act, int* it, double* resh, int outer, double tol, int nrhs, int* cycles,
-                              int graph, cudaGraphConditionalHandle hw, cudaStream_t st) {
+// Sets a conditional node's value from a control word: *word != 0 (or == 0
+// with invert).
+__global__ void k_graph_condition(cudaGraphConditionalHandle handle, const int* __restrict__ word, int invert) {
+  const int v = *word != 0;
+  cudaGraphSetConditional(handle, (unsigned)(invert ? !v : v));
+}
+
+cudaError_t launch_gmres_init(int* act, int* it, double* resh, int outer, double tol, int nrhs, int* ctl,
+                              cudaStream_t st) {
   note_launch();
-  k_gmres_init<<<1, 128, 0, st>>>(act, it, resh, outer, tol, nrhs, cycles, graph, hw);
+  k_gmres_init<<<1, 128, 0, st>>>(act, it, resh, outer, tol, nrhs, ctl);
   return cudaGetLastError();
 }
-cudaError_t launch_gmres_cycle_begin(int* used, int* stop, int inner, int graph, cudaGraphConditionalHandle hs,
-                                     cudaStream_t st) {
+cudaError_t launch_gmres_cycle_begin(int* ctl, int inner, cudaStream_t st) {
   note_launch();
-  k_gmres_cycle_begin<<<1, 1, 0, st>>>(used, stop, inner, graph, hs);
+  k_gmres_cycle_begin<<<1, 1, 0, st>>>(ctl, inner);
   return cudaGetLastError();
 }
 cudaError_t launch_gmres_estimate(const double* H, int ldh, int inner, int i, const double* beta, const double* normb,
-                                  const int* act, int nrhs, double tol, int* used, int* stop, int graph,
-                                  cudaGraphConditionalHandle hs, cudaStream_t st) {
+                                  const int* act, int nrhs, double tol, int* ctl, cudaStream_t st) {
   if (ldh > 17 || i + 2 > 17) return cudaErrorInvalidValue;
   note_launch();
-  k_gmres_estimate<<<1, 32, 0, st>>>(H, ldh, inner, i, beta, normb, act, nrhs, tol, used, stop, graph, hs);
+  k_gmres_estimate<<<1, 32, 0, st>>>(H, ldh, inner, i, beta, normb, act, nrhs, tol, ctl);
   return cudaGetLastError();
 }
 cudaError_t launch_gmres_cycle_end(const double* rvec, int* act, int* it, double* resh, int outer, double tol,
-                                   int nrhs, int* cycles, int graph, cudaGraphConditionalHandle hw, cudaStream_t st) {
+                                   int nrhs, int* ctl, cudaStream_t st) {
   note_launch();
-  k_gmres_cycle_end<<<1, 128, 0, st>>>(rvec, act, it, resh, outer, tol, nrhs, cycles, graph, hw);
+  k_gmres_cycle_end<<<1, 128, 0, st>>>(rvec, act, it, resh, outer, tol, nrhs, ctl);
   return cudaGetLastError();
 }
-
-// y = a * y + b * x
-__global__ void k_axpby(double* __restrict__ y, const double* __restrict__ x, double a, double b, i64 n) {
-  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
-    y[i] = a * y[i] + b * x[i];
-}
-cudaError_t launch_axpby(double* y, const double* x, double a, double b, i64 n, cudaStream_t st) {
-  int grid = (int)((n + 255) / 256);
-  grid = grid > 148 * 16 ? 148 * 16 : grid;
+cudaError_t launch_graph_condition(cudaGraphConditionalHandle handle, const int* word, int invert, cudaStream_t st) {
   note_launch();
-  k_axpby<<<grid, 256, 0, st>>>(y, x, a, b, n);
-  return cudaGetLastError();
-}
-
-__global__ void k_resid_finish(const double* __restrict__ nrm2, const double* __restrict__ normb, double* __restrict__ resid,
-                               int nrhs) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c < nrhs) resid[c] = sqrt(nrm2[c]) / normb[c];
-}
-cudaError_t launch_residual_norm_finish(const double* nrm2, const double* normb, double* resid, int nrhs,
-                                        cudaStream_t st) {
-  note_launch();
-  k_resid_finish<<<(nrhs + 127) / 128, 128, 0, st>>>(nrm2, normb, resid, nrhs);
+  k_graph_condition<<<1, 1, 0, st>>>(handle, word, invert);
   return cudaGetLastError();
 }
 

@@ -260,17 +260,16 @@ cudaError_t launch_gs_update(double* w, const double* V, i64 vstride, const doub
                              int nrhs, double sign, const int* active, cudaStream_t st, const int* kdev = nullptr);
 cudaError_t launch_dots_strided(const double* V, i64 vstride, int kvec, const double* w, i64 n, int nrhs,
                                 double* partial, int nchunks, double* out, i64 ostride, cudaStream_t st);
-// Device-side GMRES control (k_vec.cu); graph != 0 also sets the given
-// conditional handles of a captured graph.
-cudaError_t launch_gmres_init(int* act, int* it, double* resh, int outer, double tol, int nrhs, int* cycles,
-                              int graph, cudaGraphConditionalHandle hw, cudaStream_t st);
-cudaError_t launch_gmres_cycle_begin(int* used, int* stop, int inner, int graph, cudaGraphConditionalHandle hs,
-                                     cudaStream_t st);
+// Device-side GMRES control (k_vec.cu); ctl = {used, stop, cycles, again}.
+cudaError_t launch_gmres_init(int* act, int* it, double* resh, int outer, double tol, int nrhs, int* ctl,
+                              cudaStream_t st);
+cudaError_t launch_gmres_cycle_begin(int* ctl, int inner, cudaStream_t st);
 cudaError_t launch_gmres_estimate(const double* H, int ldh, int inner, int i, const double* beta, const double* normb,
-                                  const int* act, int nrhs, double tol, int* used, int* stop, int graph,
-                                  cudaGraphConditionalHandle hs, cudaStream_t st);
+                                  const int* act, int nrhs, double tol, int* ctl, cudaStream_t st);
 cudaError_t launch_gmres_cycle_end(const double* rvec, int* act, int* it, double* resh, int outer, double tol,
-                                   int nrhs, int* cycles, int graph, cudaGraphConditionalHandle hw, cudaStream_t st);
+                                   int nrhs, int* ctl, cudaStream_t st);
+// Conditional node value of a captured graph = (*word != 0) xor invert.
+cudaError_t launch_graph_condition(cudaGraphConditionalHandle handle, const int* word, int invert, cudaStream_t st);
 cudaError_t launch_scale_by_norm(const double* w, double* vout, const double* nrm2, double* hout, i64 hstride,
                                  i64 n, int nrhs, cudaStream_t st);
 cudaError_t launch_gmres_ls(const double* H, int ld, int inner, const double* beta, double* y, int nrhs,

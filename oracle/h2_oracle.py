@@ -413,11 +413,20 @@ def sketch_signs(p: int, fidx: np.ndarray) -> np.ndarray:
     return np.where(bits == 1, -1.0, 1.0)
 
 
-def far_indices(ranges) -> np.ndarray:
-    """Tree-sorted body indices of a box's whole far list, in list order."""
+def far_indices(ranges, samples: int = 0, gstart=None) -> np.ndarray:
+    """Tree-sorted body indices of the far list the sketch mode uses: every
+    far body when ``samples <= 0``; otherwise the far boxes of the box's own
+    level and the two above it in full, then ``samples`` strided bodies
+    (sample_indices) of the farther part of the list."""
     if not ranges:
         return np.zeros(0, dtype=np.int64)
-    return np.concatenate([np.arange(b0, b1, dtype=np.int64) for b0, b1 in ranges])
+    cut = gstart[-3] if (samples > 0 and gstart is not None and len(gstart) >= 3) else 0
+    near = [np.arange(b0, b1, dtype=np.int64) for b0, b1 in ranges[cut:]]
+    parts = near
+    if cut > 0:
+        farther = np.concatenate([np.arange(b0, b1, dtype=np.int64) for b0, b1 in ranges[:cut]])
+        parts = near + [farther[sample_indices(len(farther), samples)]]
+    return np.concatenate(parts) if parts else np.zeros(0, dtype=np.int64)
 
 
 def far_bodies(bodies: np.ndarray, ranges, samples: int, gstart=None, mode: int = 0) -> np.ndarray:
@@ -429,7 +438,7 @@ def far_bodies(bodies: np.ndarray, ranges, samples: int, gstart=None, mode: int 
     idx = np.concatenate([np.arange(b0, b1, dtype=np.int64) for b0, b1 in ranges])
     total = len(idx)
     if mode == 2:
-        return bodies[idx]
+        return bodies[far_indices(ranges, samples, gstart)]
     if mode == 0 or samples <= 0 or samples >= total:
         keep = sample_indices(total, samples)
         return bodies[idx[keep]]
@@ -744,7 +753,8 @@ class H2MatrixSolver:
             for i in range(nodes):
                 fb = far_bodies(bodies, ranges.get(g0 + i, []), samples, self.gstart.get(g0 + i, []),
                                 self.sampling)
-                sk = far_indices(ranges.get(g0 + i, [])) if self.sampling == 2 else None
+                sk = (far_indices(ranges.get(g0 + i, []), samples, self.gstart.get(g0 + i, []))
+                      if self.sampling == 2 else None)
                 rank, c = compute_basis(kern, epi, lev.S[i], fb, lev.Q[i], 1.0 <= epi, sk)
                 lev.R[i] = c
                 lev.DimsLr[i] = rank

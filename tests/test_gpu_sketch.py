@@ -20,10 +20,10 @@ def rel(a, b):
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b)))
 
 
-def sketch_solver(handle, k, eps, t, b, theta=2.0):
+def sketch_solver(handle, k, eps, t, b, theta=2.0, samples=0):
     handle.set_option(m._lib.OPT_SAMPLING, m._lib.SAMPLING_SKETCH)
     try:
-        return m.H2MatrixSolver(handle, k, eps, 100, 0, t, theta, b, samples=0)
+        return m.H2MatrixSolver(handle, k, eps, 100, 0, t, theta, b, samples=samples)
     finally:
         handle.set_option(m._lib.OPT_SAMPLING, m._lib.SAMPLING_STRIDED)
 
@@ -103,3 +103,32 @@ def test_sketch_beats_strided_sampling(handle):
     A2.close()
     e1, e2 = rel(y1, yd), rel(y2, yd)
     assert e2 < 1e-11 and e2 < e1 / 10, (e1, e2)
+
+
+def test_sketch_near_levels_plus_samples_matches_oracle(handle):
+    """samples > 0 in sketch mode: the far boxes of the box's level and the
+    two above in full, plus strided samples of the farther list; same set of
+    bodies and signs as the oracle, so the same ranks (to rounding), and the
+    operator as accurate as with every far body."""
+    N = 16384
+    L = m.levels_for(N, 256)
+    b = m.uniform_unit_cube_rnd(N, 999)
+    t = m.build_tree(b, L)
+    cells = O.build_binary_tree(O.uniform_unit_cube_rnd(N, 999), L)
+    k = m.Laplace3D(1e-4)
+    A = sketch_solver(handle, k, 1e-11, t, b, samples=1000)
+    Afull = sketch_solver(handle, k, 1e-11, t, b, samples=0)
+    Ao = O.H2MatrixSolver(O.Kernel(O.LAPLACE, 1e-4), 1e-11, 100, 0, cells, 2.0, b.copy(), L, 1000, 2)
+    for lvl in range(L + 1):
+        d, r = A.level_dims(lvl)
+        assert np.array_equal(d, Ao.A[lvl].Dims), lvl
+        diff = np.abs(r - Ao.A[lvl].DimsLr)
+        assert diff.max() <= 1 and (diff > 0).sum() <= max(1, len(r) // 8), (lvl, r, Ao.A[lvl].DimsLr)
+    x = np.random.default_rng(2).random(N)
+    yd = m.dense_matvec(handle, k, b, x)
+    y = x.copy()
+    A.matVecMul(y)
+    yf = x.copy()
+    Afull.matVecMul(yf)
+    assert rel(y, Ao.matvec(x)) < 1e-11
+    assert rel(y, yd) < 3 * max(rel(yf, yd), 1e-13)
