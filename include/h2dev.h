@@ -119,6 +119,11 @@ int h2dev_handle_trim(h2dev_handle_t h);
  * by kernels on the device) and launched once, with no host round trip until
  * it ends.  0 (default): the same kernels launched step by step, the host
  * reading the device's convergence flags between steps. */
+/* H2DEV_OPT_AUTOTUNE: 1 (default) lets the handle time, once per plan shape
+ * bucket, each launch variant a block-apply plan admits (row tilings of the
+ * streaming applies, rows per thread of the matrix-free apply) on the plan's
+ * own data and keep the fastest for later plans of the bucket; the variants
+ * give identical results.  0: the fixed default variants. */
 enum {
   H2DEV_OPT_BASIS = 0,
   H2DEV_OPT_SKINNY_TILED = 1,
@@ -126,7 +131,8 @@ enum {
   H2DEV_OPT_TENSOR_CORES = 3,
   H2DEV_OPT_MATRIX_FREE = 4,
   H2DEV_OPT_PRECOND_BF16 = 5,
-  H2DEV_OPT_GRAPH_SOLVE = 6
+  H2DEV_OPT_GRAPH_SOLVE = 6,
+  H2DEV_OPT_AUTOTUNE = 7
 };
 int h2dev_set_option(h2dev_handle_t h, int option, int64_t value);
 
@@ -256,6 +262,12 @@ int h2dev_batched_gemm_device(h2dev_handle_t h, int precision, int64_t batch, in
  * receives the number of records. */
 int h2dev_profile_timeline(h2dev_handle_t h, int64_t cap, char* names, double* start_ms, double* dur_ms,
                            int64_t* count);
+/* Decisions of the handle's autotuner, in the order they were made: up to
+ * cap bucket keys (64 bytes each), the chosen variant and the device ms of
+ * each variant when it was timed (3 per key, -1 where a plan has fewer
+ * variants); *count receives the number of decisions.  No reference
+ * counterpart. */
+int h2dev_autotune_report(h2dev_handle_t h, int64_t cap, char* keys, int* choice, double* ms, int64_t* count);
 /* Number of kernels this library has launched in this process so far (all
  * handles); the difference across a region counts its launches. */
 int h2dev_launch_count(int64_t* count);

@@ -32,6 +32,7 @@ OPT_TENSOR_CORES = 3
 OPT_MATRIX_FREE = 4
 OPT_PRECOND_BF16 = 5
 OPT_GRAPH_SOLVE = 6
+OPT_AUTOTUNE = 7
 BASIS_GRAM, BASIS_HOUSEHOLDER = 0, 1
 # H2DEV_OPT_SAMPLING values: strided cap, level-geometric cap, sketch of every far body
 SAMPLING_STRIDED, SAMPLING_GEOMETRIC, SAMPLING_SKETCH = 0, 1, 2
@@ -82,6 +83,7 @@ SIGNATURES = {
     "h2dev_profile_report": (C.c_int, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _i64p]),
     "h2dev_profile_timeline": (C.c_int, [_vp, _i64, _vp, _vp, _vp, _i64p]),
     "h2dev_launch_count": (C.c_int, [_i64p]),
+    "h2dev_autotune_report": (C.c_int, [_vp, _i64, _vp, _vp, _vp, _i64p]),
     "h2dev_handle_memory": (C.c_int, [_vp, _i64p, _i64p]),
     "h2dev_handle_trim": (C.c_int, [_vp]),
     "h2dev_batched_gemm_device": (C.c_int, [_vp, C.c_int, _i64, _i64, _i64, _i64, _i64, C.c_int, C.c_int, C.c_double,

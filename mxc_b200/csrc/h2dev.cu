@@ -4,6 +4,7 @@
 // reference's ColCommMPI reduces to identity collectives and all halo data
 // is read in place from HBM (comm-mpi.cpp:198-225 become no-ops).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -306,6 +307,61 @@ static void check_tc(h2dev_handle_s* h) {
   }
 }
 
+// ------------------------------------------------------------------ autotuner
+// The first time a plan of a given shape bucket runs on a handle (outside
+// any stream capture), every launch variant it admits is timed on the
+// plan's own data -- twice each, keeping the second time, with CUDA events
+// on the launching stream -- and the fastest is recorded for the bucket;
+// later plans of the bucket (every factorization of a serving system, every
+// step of a benchmark) reuse the choice without timing.  Variants differ
+// only in how rows are tiled over CTAs, so every variant gives the same
+// result bit for bit.
+static std::string tune_key(const char* name, int esize, int nr, double tasks, double rows, double elems) {
+  auto b = [](double v) { return v <= 1. ? 0 : (int)std::ceil(std::log2(v)); };
+  char buf[160];
+  snprintf(buf, sizeof(buf), "%s/e%d/n%d/t%d/r%d/a%d", name, esize, nr, b(tasks), b(rows), b(elems));
+  return buf;
+}
+
+static bool stream_capturing(cudaStream_t st) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  return cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+}
+
+// Returns the variant to run for `key` (0 when tuning is off or impossible),
+// timing `nvar` variants through run_variant(v) when the bucket is new.
+template <typename F>
+static int tuned_variant(const std::string& key, int nvar, cudaStream_t st, F run_variant) {
+  h2dev_handle_s* h = g_cur;
+  if (!h || !h->autotune || nvar < 2) return 0;
+  auto it = h->tune.find(key);
+  if (it != h->tune.end()) return it->second.choice;
+  if (stream_capturing(st) || h->prof) return 0;
+  h2dev_handle_s::TuneRec rec;
+  rec.ms.assign(nvar, 0.);
+  cudaEvent_t a = nullptr, b = nullptr;
+  ck(cudaEventCreate(&a), "event");
+  ck(cudaEventCreate(&b), "event");
+  for (int v = 0; v < nvar; v++)
+    for (int rep = 0; rep < 2; rep++) {
+      ck(cudaEventRecord(a, st), "event");
+      run_variant(v);
+      ck(cudaEventRecord(b, st), "event");
+      ck(cudaEventSynchronize(b), "event");
+      float ms = 0.f;
+      ck(cudaEventElapsedTime(&ms, a, b), "event");
+      rec.ms[v] = ms;
+    }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  rec.choice = 0;
+  for (int v = 1; v < nvar; v++)
+    if (rec.ms[v] < rec.ms[rec.choice]) rec.choice = v;
+  h->tune[key] = rec;
+  h->tune_order.push_back(key);
+  return rec.choice;
+}
+
 // Host-built list of segmented-GEMM tasks, uploaded once and replayed.
 template <typename T>
 struct GemmPlan {
@@ -322,6 +378,15 @@ struct GemmPlan {
   bool skinny_nn = false;          // use k_skinny_nn instead of the tiled kernel
   int nr = 0;
   DVec<int2> d_rtiles, d_rtiles_w;  // row tiles of the 128- and 256-row streaming variants
+  // Autotuned tilings of the streaming path: 0 = per-task rule (256-row
+  // tiles where they pad no more than 128-row ones), 1 = all 128-row, 2 =
+  // all 256-row tiles.
+  DVec<int2> d_alt_n, d_alt_w;
+  std::string tkey;
+  mutable int variant = -1;
+  // Only plans that overwrite their outputs (every beta zero) are timed:
+  // repeating one leaves the same result, so tuning runs are harmless.
+  bool idempotent = false;
   DVec<T> parts_buf;               // partial results of split tasks
   DVec<SumTask<T>> d_sums;
   int nsums = 0, sum_maxmn = 0;
@@ -357,7 +422,8 @@ struct GemmPlan {
       // than 128-row tiles would, else 128-row tiles (two launches back to
       // back; padding rows are zero-filled copies whose tensor-core work is
       // skipped, but a mostly empty CTA still walks every stage).
-      std::vector<int2> rt[2];
+      std::vector<int2> rt[2], alt[2];
+      double rows = 0., elems = 0.;
       for (int ti = 0; ti < (int)tasks.size(); ti++) {
         const auto& t = tasks[ti];
         if (t.m <= 0 || t.n <= 0) continue;
@@ -366,9 +432,19 @@ struct GemmPlan {
         const int wide = ((t.m + n2 - 1) / n2) * n2 == ((t.m + n1 - 1) / n1) * n1 ? 1 : 0;
         const int rb = skinny_rows_per_cta(wide);
         for (int a = 0; a < (t.m + rb - 1) / rb; a++) rt[wide].push_back(make_int2(ti, a));
+        for (int w = 0; w < 2; w++)
+          for (int a = 0; a < (t.m + skinny_rows_per_cta(w) - 1) / skinny_rows_per_cta(w); a++)
+            alt[w].push_back(make_int2(ti, a));
+        rows += t.m;
+        for (int e = t.e0; e < t.e1; e++) elems += (double)t.m * ents[e].k;
       }
       d_rtiles.upload(rt[0]);
       d_rtiles_w.upload(rt[1]);
+      d_alt_n.upload(alt[0]);
+      d_alt_w.upload(alt[1]);
+      tkey = tune_key(name, (int)sizeof(T), nr, (double)tasks.size(), rows, elems);
+      idempotent = true;
+      for (const auto& t : tasks) idempotent = idempotent && t.beta == T(0);
     }
     int bm = shape == GEMM_TC ? tc_gemm_tile() : gemm_tile_m(shape);
     int bn = shape == GEMM_TC ? tc_gemm_tile() : gemm_tile_n(shape);
@@ -508,12 +584,30 @@ struct GemmPlan {
     d_sums.upload(sums);
   }
 
+  void run_skinny(int v, cudaStream_t st) const {
+    const DVec<int2>& w = v == 0 ? d_rtiles_w : d_alt_w;
+    const DVec<int2>& n = v == 0 ? d_rtiles : d_alt_n;
+    if (v != 1) ck(launch_skinny_nn<T>(nr, 1, d_tasks.p, d_ents.p, w.p, (int)w.n, st), "skinny_nn");
+    if (v != 2) ck(launch_skinny_nn<T>(nr, 0, d_tasks.p, d_ents.p, n.p, (int)n.n, st), "skinny_nn");
+    if (nsums) ck(launch_sum_parts<T>(d_sums.p, nsums, sum_maxmn, st), "sum_parts");
+  }
+
+  // Picks the streaming tiling (timing the variants if the bucket is new).
+  void tune(cudaStream_t st) const {
+    if (!skinny_nn || variant >= 0) return;
+    if (!idempotent) {
+      variant = 0;
+      return;
+    }
+    const int v = tuned_variant(tkey, 3, st, [&](int x) { run_skinny(x, st); });
+    if (!stream_capturing(st)) variant = v;
+  }
+
   void run(cudaStream_t st) const {
+    tune(st);
     Prof p(name, flops, bytes, st);
     if (skinny_nn) {
-      ck(launch_skinny_nn<T>(nr, 1, d_tasks.p, d_ents.p, d_rtiles_w.p, (int)d_rtiles_w.n, st), "skinny_nn");
-      ck(launch_skinny_nn<T>(nr, 0, d_tasks.p, d_ents.p, d_rtiles.p, (int)d_rtiles.n, st), "skinny_nn");
-      if (nsums) ck(launch_sum_parts<T>(d_sums.p, nsums, sum_maxmn, st), "sum_parts");
+      run_skinny(variant < 0 ? 0 : variant, st);
     } else if (shape == GEMM_TC) {
       if constexpr (std::is_same<T, float>::value) {
         require(g_cur != nullptr, "tensor-core GEMM outside an API call");
@@ -542,6 +636,11 @@ struct MfPlan {
   int nr = 0;
   const char* name = "mf_apply";
   double flops = 0., bytes = 0.;
+  // Autotuned rows per thread: variant 0 = 2 rows, 1 = 1 row per thread.
+  std::vector<int2> tiles1;
+  DVec<int2> d_tiles1;
+  std::string tkey;
+  mutable int variant = -1;
   void add_task(const double* pts, int m, double* C, i64 ldc, double beta) {
     MfTask t;
     t.pts = pts; t.m = m; t.C = C; t.ldc = ldc; t.beta = beta;
@@ -560,19 +659,37 @@ struct MfPlan {
     bytes += (24. + 8. * nr) * k;
   }
   void finalize() {
-    const int bm = mf_rows_per_cta();
+    const int bm = mf_rows_per_cta(2), bm1 = mf_rows_per_cta(1);
     tiles.clear();
+    tiles1.clear();
+    double rows = 0.;
     for (size_t t = 0; t < tasks.size(); t++) {
       bytes += (24. + 8. * nr) * tasks[t].m;
+      rows += tasks[t].m;
       for (int r = 0; r < tasks[t].m; r += bm) tiles.push_back(make_int2((int)t, r / bm));
+      for (int r = 0; r < tasks[t].m; r += bm1) tiles1.push_back(make_int2((int)t, r / bm1));
     }
     d_tasks.upload(tasks);
     d_ents.upload(ents);
     d_tiles.upload(tiles);
+    d_tiles1.upload(tiles1);
+    tkey = tune_key(name, 8, nr, (double)tasks.size(), rows, flops / (2. * nr));
+  }
+  void launch(const KernelParams& kp, int v, cudaStream_t st) const {
+    if (v == 1)
+      ck(launch_mf_apply(kp, nr, 1, d_tasks.p, d_ents.p, d_tiles1.p, (int)tiles1.size(), st), name);
+    else
+      ck(launch_mf_apply(kp, nr, 2, d_tasks.p, d_ents.p, d_tiles.p, (int)tiles.size(), st), name);
+  }
+  void tune(const KernelParams& kp, cudaStream_t st) const {
+    if (variant >= 0) return;
+    const int v = tuned_variant(tkey, 2, st, [&](int x) { launch(kp, x, st); });  // beta 0: repeatable
+    if (!stream_capturing(st)) variant = v;
   }
   void run(const KernelParams& kp, cudaStream_t st) const {
+    tune(kp, st);
     Prof p(name, flops, bytes, st);
-    ck(launch_mf_apply(kp, nr, d_tasks.p, d_ents.p, d_tiles.p, (int)tiles.size(), st), name);
+    launch(kp, variant < 0 ? 0 : variant, st);
   }
 };
 
@@ -681,9 +798,22 @@ void batched_gemm(int64_t batch, int64_t nterms, int64_t m, int64_t n, int64_t k
 }
 
 
+struct SolveGraph;  // a captured, instantiated GMRES solve kept for replay (gmres_graph)
+
+static uint64_t next_solver_uid() {
+  static std::atomic<uint64_t> n{0};
+  return ++n;
+}
+
 class SolverBase {
  public:
   virtual ~SolverBase() {}
+  // Identity for caches (never reused) and a generation bumped whenever the
+  // solver's plans, per-nrhs vectors or factors change: a captured solve is
+  // replayed only while both solvers' generations are those it captured.
+  uint64_t uid = next_solver_uid();
+  uint64_t gen = 0;
+  std::shared_ptr<SolveGraph> solve_graph;
   virtual i64 lenX() const = 0;
   virtual i64 nlevels() const = 0;
   virtual void matvec(i64 nrhs, double* dX, i64 ldx) = 0;
@@ -1470,6 +1600,7 @@ class Solver : public SolverBase {
     cur_nrhs = nrhs;
     mv_built = false;
     pc_built = false;
+    gen++;
   }
 
   // H^2 matvec plans (h2matrix.cpp:251-344) for the current nrhs.
@@ -1480,6 +1611,7 @@ class Solver : public SolverBase {
   // W_{l+1} += Q_l W_l level by level and the leaf Y = Q W + sum_j A_ij X_j.
   void build_matvec(i64 nrhs) {
     const int nr = (int)nrhs;
+    gen++;
     mv_up.clear();
     mv_down.clear();
     mv_up.resize(levels + 1);
@@ -1637,6 +1769,20 @@ class Solver : public SolverBase {
     ensure_vectors(nrhs);
     if (!mv_built) build_matvec(nrhs);
     if (factored && !pc_built) build_precondition(nrhs);
+    // Autotuning decisions are taken now, outside any capture (the timed
+    // runs write only this solver's internal vectors).
+    for (auto& g : mv_up) g.tune(st());
+    for (auto& g : mv_down) g.tune(st());
+    mv_far.tune(st());
+    mv_leaf.tune(st());
+    mv_qw.tune(st());
+    if (matrix_free) {
+      mf_far.tune(kp, st());
+      mf_leaf.tune(kp, st());
+    }
+    if (factored)
+      for (auto* v : {&pc_fx, &pc_fz, &pc_bx, &pc_by})
+        for (auto& g : *v) g.tune(st());
   }
 
   void matvec(i64 nrhs, double* dX, i64 ldx) override {
@@ -1927,11 +2073,13 @@ class Solver : public SolverBase {
     }
     factored = true;
     pc_built = false;
+    gen++;
   }
 
   // ULV substitution plans (h2matrix.cpp:448-537).
   void build_precondition(i64 nrhs) {
     const int nr = (int)nrhs;
+    gen++;
     pc_fx.clear(); pc_fz.clear(); pc_bx.clear(); pc_by.clear(); pc_fcopy.clear(); pc_bcopy.clear();
     pc_fx.resize(levels + 1); pc_fz.resize(levels + 1); pc_bx.resize(levels + 1); pc_by.resize(levels + 1);
     pc_fcopy.resize(levels + 1); pc_bcopy.resize(levels + 1);
@@ -2234,7 +2382,28 @@ static void gmres_epilogue(SolverBase& A, GmresState& g, int graph, cudaGraphCon
 // go to h->stream, pointed at each body's capture stream in turn; the matvec
 // keeps its near field on that stream while capturing (no side-stream fork),
 // so the bodies hold kernels, copies and memsets only.
-static void gmres_graph(SolverBase& A, SolverBase& M, GmresState& g) {
+// A captured solve and the state buffers its nodes point at, kept on the
+// operator's solver and replayed while the key (both solvers' identities and
+// generations, the shape and the tolerance) still matches.
+struct SolveGraph {
+  uint64_t m_uid = 0, m_gen = 0, a_gen = 0;
+  i64 nrhs = 0, inner = 0, outer = 0;
+  int early = 0;
+  double tol = 0.;
+  GmresState g;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  bool matches(const SolverBase& A, const SolverBase& M, i64 nr, i64 in, i64 out, int ea, double t) const {
+    return exec && m_uid == M.uid && m_gen == M.gen && a_gen == A.gen && nrhs == nr && inner == in && outer == out &&
+           early == ea && tol == t;
+  }
+  ~SolveGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+};
+
+static void gmres_graph(SolverBase& A, SolverBase& M, GmresState& g, SolveGraph& out) {
   h2dev_handle_s* h = A.h;
   cudaStream_t s0 = h->stream;
   cudaStream_t side = h->stream2;
@@ -2322,26 +2491,14 @@ static void gmres_graph(SolverBase& A, SolverBase& M, GmresState& g) {
   h->stream = s0;
   ck(cudaStreamEndCapture(s0, &scope.graph), "capture end");
   ck(cudaGraphInstantiate(&scope.exec, scope.graph, 0), "graph instantiate");
-  ck(cudaGraphLaunch(scope.exec, s0), "graph launch");
-  ck(cudaStreamSynchronize(s0), "sync");
+  out.graph = scope.graph;
+  out.exec = scope.exec;
+  scope.graph = nullptr;
+  scope.exec = nullptr;
 }
 
-static int gmres(SolverBase& A, SolverBase& M, double tol, i64 nrhs, double* dX, const double* dB, i64 ld, i64 inner,
-                 i64 outer, int early_exit, double* resid, i64* iters) {
-  require(A.lenX() == M.lenX(), "gmres: A and M sizes differ");
-  require(inner >= 1 && inner <= 16 && outer >= 0 && nrhs >= 1, "gmres: inner must be in [1,16]");
-  cudaStream_t st = A.h->stream;
-  GmresState g;
-  g.N = A.lenX();
-  g.nrhs = nrhs;
-  g.inner = inner;
-  g.outer = outer;
-  g.ldh = (int)inner + 1;
-  g.vstride = g.N * nrhs;
-  g.tol = tol;
-  g.early = early_exit ? 1 : 0;
-  g.nch = dots_chunks(g.N);
-  const int nr = (int)nrhs;
+static void gmres_alloc(GmresState& g, cudaStream_t st) {
+  const i64 nrhs = g.nrhs, inner = g.inner, outer = g.outer;
   g.V.alloc((size_t)(inner + 1) * g.vstride);
   g.w.alloc(g.vstride);
   g.R.alloc(g.vstride);
@@ -2358,8 +2515,57 @@ static int gmres(SolverBase& A, SolverBase& M, double tol, i64 nrhs, double* dX,
   g.it.alloc(nrhs);
   g.ctl.alloc(4);
   g.partial.alloc((size_t)g.nch * (inner + 1) * nrhs);
-  g.resh.zero(st);
   g.y.zero(st);
+}
+
+static int gmres(SolverBase& A, SolverBase& M, double tol, i64 nrhs, double* dX, const double* dB, i64 ld, i64 inner,
+                 i64 outer, int early_exit, double* resid, i64* iters) {
+  require(A.lenX() == M.lenX(), "gmres: A and M sizes differ");
+  require(inner >= 1 && inner <= 16 && outer >= 0 && nrhs >= 1, "gmres: inner must be in [1,16]");
+  cudaStream_t st = A.h->stream;
+  const int nr = (int)nrhs;
+  const int early = early_exit ? 1 : 0;
+  const bool use_graph = A.h->graph_solve && !A.h->prof && A.h == M.h;
+  // Graph path: the solve is captured once per (operator, preconditioner,
+  // shape, tolerance) and replayed by later calls -- a serving system solving
+  // batch after batch pays the capture once.  Everything a capture must not
+  // do (plan builds, uploads, allocations, autotuning) happens in prepare().
+  std::shared_ptr<SolveGraph> sg;
+  GmresState local;
+  GmresState* gp = &local;
+  if (use_graph) {
+    A.prepare(nrhs);
+    M.prepare(nrhs);
+    if (A.solve_graph && A.solve_graph->matches(A, M, nrhs, inner, outer, early, tol)) {
+      sg = A.solve_graph;
+    } else {
+      A.solve_graph.reset();
+      sg = std::make_shared<SolveGraph>();
+      sg->m_uid = M.uid;
+      sg->m_gen = M.gen;
+      sg->a_gen = A.gen;
+      sg->nrhs = nrhs;
+      sg->inner = inner;
+      sg->outer = outer;
+      sg->early = early;
+      sg->tol = tol;
+    }
+    gp = &sg->g;
+  }
+  GmresState& g = *gp;
+  if (!g.V.p) {
+    g.N = A.lenX();
+    g.nrhs = nrhs;
+    g.inner = inner;
+    g.outer = outer;
+    g.ldh = (int)inner + 1;
+    g.vstride = g.N * nrhs;
+    g.tol = tol;
+    g.early = early;
+    g.nch = dots_chunks(g.N);
+    gmres_alloc(g, st);
+  }
+  g.resh.zero(st);
   for (i64 c = 0; c < nrhs; c++) {
     ck(cudaMemcpyAsync(g.Bc.p + c * g.N, dB + c * ld, sizeof(double) * g.N, cudaMemcpyDeviceToDevice, st), "copy B");
     ck(cudaMemcpyAsync(g.X.p + c * g.N, dX + c * ld, sizeof(double) * g.N, cudaMemcpyDeviceToDevice, st), "copy X");
@@ -2376,13 +2582,11 @@ static int gmres(SolverBase& A, SolverBase& M, double tol, i64 nrhs, double* dX,
   // The reference starts from the given X with R = B (not B - A X) in its
   // first cycle (solver.cpp:157); the initial guess is zero in every caller.
   ck(cudaMemcpyAsync(g.R.p, g.Bc.p, sizeof(double) * g.vstride, cudaMemcpyDeviceToDevice, st), "R=B");
-  const bool use_graph = A.h->graph_solve && !A.h->prof && A.h == M.h;
   if (use_graph) {
-    // Everything a capture must not do (plan builds, uploads, allocations)
-    // happens here, once.
-    A.prepare(nrhs);
-    M.prepare(nrhs);
-    gmres_graph(A, M, g);
+    if (!sg->exec) gmres_graph(A, M, g, *sg);
+    A.solve_graph = sg;
+    ck(cudaGraphLaunch(sg->exec, st), "graph launch");
+    ck(cudaStreamSynchronize(st), "sync");
   } else {
     ck(launch_gmres_init(g.act.p, g.it.p, g.resh.p, (int)outer, tol, nr, g.ctl.p, st), "init");
     bool any = 0 < outer && tol <= 1.;
@@ -2981,6 +3185,25 @@ int h2dev_profile_timeline(h2dev_handle_t h, int64_t cap, char* names, double* s
   H2_API_END
 }
 
+int h2dev_autotune_report(h2dev_handle_t h, int64_t cap, char* keys, int* choice, double* ms, int64_t* count) {
+  H2_API_BEGIN
+  require(h && count, "null argument");
+  *count = (int64_t)h->tune_order.size();
+  for (int64_t i = 0; i < cap && i < *count; i++) {
+    const auto& key = h->tune_order[(size_t)i];
+    const auto& rec = h->tune.at(key);
+    if (keys) {
+      std::memset(keys + 64 * i, 0, 64);
+      std::strncpy(keys + 64 * i, key.c_str(), 63);
+    }
+    if (choice) choice[i] = rec.choice;
+    if (ms)
+      for (int v = 0; v < 3; v++) ms[3 * i + v] = v < (int)rec.ms.size() ? rec.ms[(size_t)v] : -1.;
+  }
+  return H2DEV_OK;
+  H2_API_END
+}
+
 int h2dev_launch_count(int64_t* count) {
   H2_API_BEGIN
   require(count != nullptr, "null argument");
@@ -3034,6 +3257,11 @@ int h2dev_set_option(h2dev_handle_t h, int option, int64_t value) {
   if (option == H2DEV_OPT_SAMPLING) {
     require(value >= 0 && value <= 2, "sampling option must be 0, 1 or 2");
     h->sampling_mode = (int)value;
+    return H2DEV_OK;
+  }
+  if (option == H2DEV_OPT_AUTOTUNE) {
+    require(value == 0 || value == 1, "autotune option must be 0 or 1");
+    h->autotune = value != 0;
     return H2DEV_OK;
   }
   if (option == H2DEV_OPT_GRAPH_SOLVE) {

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <deque>
+#include <string>
 #include <unordered_map>
 #include <utility>
 #include <vector>
@@ -41,7 +42,18 @@ struct h2dev_handle_s {
   int sampling_mode = 0;  // far-list cap rule for solvers created next (H2DEV_OPT_SAMPLING)
   bool matrix_free = false;
   bool precond_bf16 = false;
-  bool graph_solve = false;  // GMRES solves on this handle run as one captured CUDA graph (H2DEV_OPT_GRAPH_SOLVE)  // FP32 solvers created next apply their substitution from BF16 copies (H2DEV_OPT_PRECOND_BF16)  // operator-mode solvers created next keep no near blocks or couplings (H2DEV_OPT_MATRIX_FREE)
+  bool graph_solve = false;
+  // Autotuner (H2DEV_OPT_AUTOTUNE): the launch variant chosen for each plan
+  // shape bucket (key: plan name, element size, right-hand sides and
+  // log2-bucketed task / row / element counts) and the device times each
+  // variant took when it was measured.
+  bool autotune = true;
+  struct TuneRec {
+    int choice;
+    std::vector<double> ms;
+  };
+  std::unordered_map<std::string, TuneRec> tune;
+  std::vector<std::string> tune_order;  // GMRES solves on this handle run as one captured CUDA graph (H2DEV_OPT_GRAPH_SOLVE)  // FP32 solvers created next apply their substitution from BF16 copies (H2DEV_OPT_PRECOND_BF16)  // operator-mode solvers created next keep no near blocks or couplings (H2DEV_OPT_MATRIX_FREE)
   int basis_mode = 0;  // 0: Gram + pivoted Cholesky for fixed-rank bases; 1: Householder TSQR everywhere
   // One reference held by the caller plus one per live solver: the stream
   // (and the stream-ordered memory freed on it) outlives every solver.

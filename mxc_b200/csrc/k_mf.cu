@@ -8,12 +8,12 @@
 // needs only the bases and the points; nothing of size near-pairs x M^2 or
 // far-pairs x rank^2 is stored.
 //
-// One CTA of 128 threads per {task, 256-row block}; each thread owns two
-// rows (their bodies in registers) and accumulates all right-hand sides in
-// registers.  The task's entries are walked in 32-column slabs: the slab's
+// One CTA of 128 threads per {task, 128 RPT-row block}; each thread owns
+// RPT rows (their bodies in registers) and accumulates all right-hand sides
+// in registers.  The task's entries are walked in 32-column slabs: the slab's
 // column bodies and the 32 x NR right-hand-side values go to shared memory
 // (row-contiguous, so each is read by a broadcast vector load), then every
-// thread evaluates its two rows against the 32 columns and updates its
+// thread evaluates its rows against the 32 columns and updates its
 // accumulators.  FP64 throughout, one reciprocal square root per pair
 // (rsqrt_newton: an FP32 seed refined by two FP64 Newton steps, about 1 ulp;
 // the whole entry is a few ulp from the reference's std::hypot form); the
@@ -26,10 +26,15 @@ namespace h2b {
 
 namespace {
 
-constexpr int MF_NT = 128, MF_RPT = 2, MF_BM = MF_NT * MF_RPT, MF_KS = 32;
+constexpr int MF_NT = 128, MF_KS = 32;
 
-template <int NR, int KIND>
-__global__ void __launch_bounds__(MF_NT, 4)
+// RPT rows per thread (BM = 128 RPT rows per CTA): RPT = 2 shares each
+// right-hand-side load between two rows; RPT = 1 halves the registers, so
+// twice as many warps fit on an SM to hide the FP64 latency.  Per row the
+// pairs are accumulated in the same order either way (bit-identical
+// results); the plan times both once and keeps the faster.
+template <int NR, int KIND, int RPT>
+__global__ void __launch_bounds__(MF_NT, RPT == 1 ? 8 : 4)
     k_mf_apply(KernelParams kp, const MfTask* __restrict__ tasks, const MfEntry* __restrict__ ents,
                const int2* __restrict__ tiles, int nr) {
   constexpr int NRP = NR < 2 ? 2 : NR;  // padded row of the right-hand-side slab (16-byte loads)
@@ -38,22 +43,20 @@ __global__ void __launch_bounds__(MF_NT, 4)
   const int2 tl = tiles[blockIdx.x];
   const MfTask t = tasks[tl.x];
   const int tid = threadIdx.x;
-  const int r0 = tl.y * MF_BM + tid, r1 = r0 + MF_NT;
-  const bool v0 = r0 < t.m, v1 = r1 < t.m;
-  double p0x = 0., p0y = 0., p0z = 0., p1x = 0., p1y = 0., p1z = 0.;
-  if (v0) {
-    p0x = t.pts[3 * r0];
-    p0y = t.pts[3 * r0 + 1];
-    p0z = t.pts[3 * r0 + 2];
-  }
-  if (v1) {
-    p1x = t.pts[3 * r1];
-    p1y = t.pts[3 * r1 + 1];
-    p1z = t.pts[3 * r1 + 2];
-  }
-  double a0[NR], a1[NR];
+  int row[RPT];
+  bool val[RPT];
+  double px[RPT], py[RPT], pz[RPT];
+  double acc[RPT][NR];
 #pragma unroll
-  for (int c = 0; c < NR; c++) a0[c] = a1[c] = 0.;
+  for (int q = 0; q < RPT; q++) {
+    row[q] = tl.y * MF_NT * RPT + tid + q * MF_NT;
+    val[q] = row[q] < t.m;
+    px[q] = val[q] ? t.pts[3 * row[q]] : 0.;
+    py[q] = val[q] ? t.pts[3 * row[q] + 1] : 0.;
+    pz[q] = val[q] ? t.pts[3 * row[q] + 2] : 0.;
+#pragma unroll
+    for (int c = 0; c < NR; c++) acc[q][c] = 0.;
+  }
 
   for (int e = t.e0; e < t.e1; e++) {
     const MfEntry en = ents[e];
@@ -68,21 +71,23 @@ __global__ void __launch_bounds__(MF_NT, 4)
       __syncthreads();
       for (int b = 0; b < kn; b++) {
         const double cx = cs[3 * b], cy = cs[3 * b + 1], cz = cs[3 * b + 2];
-        const double k0v = kernel_eval<KIND>(kp, p0x - cx, p0y - cy, p0z - cz);
-        const double k1v = kernel_eval<KIND>(kp, p1x - cx, p1y - cy, p1z - cz);
+        double kv[RPT];
+#pragma unroll
+        for (int q = 0; q < RPT; q++) kv[q] = kernel_eval<KIND>(kp, px[q] - cx, py[q] - cy, pz[q] - cz);
         const double* br = bs + b * NRP;
         if constexpr (NR == 1) {
           const double x = br[0];
-          a0[0] = fma(k0v, x, a0[0]);
-          a1[0] = fma(k1v, x, a1[0]);
+#pragma unroll
+          for (int q = 0; q < RPT; q++) acc[q][0] = fma(kv[q], x, acc[q][0]);
         } else {
 #pragma unroll
           for (int c = 0; c < NR; c += 2) {
             const double2 x = *reinterpret_cast<const double2*>(br + c);
-            a0[c] = fma(k0v, x.x, a0[c]);
-            a0[c + 1] = fma(k0v, x.y, a0[c + 1]);
-            a1[c] = fma(k1v, x.x, a1[c]);
-            a1[c + 1] = fma(k1v, x.y, a1[c + 1]);
+#pragma unroll
+            for (int q = 0; q < RPT; q++) {
+              acc[q][c] = fma(kv[q], x.x, acc[q][c]);
+              acc[q][c + 1] = fma(kv[q], x.y, acc[q][c + 1]);
+            }
           }
         }
       }
@@ -91,46 +96,51 @@ __global__ void __launch_bounds__(MF_NT, 4)
 #pragma unroll
   for (int c = 0; c < NR; c++) {
     if (c >= nr) break;
-    if (v0) {
-      double* o = t.C + r0 + (i64)c * t.ldc;
-      *o = t.beta == 0. ? a0[c] : t.beta * *o + a0[c];
-    }
-    if (v1) {
-      double* o = t.C + r1 + (i64)c * t.ldc;
-      *o = t.beta == 0. ? a1[c] : t.beta * *o + a1[c];
+#pragma unroll
+    for (int q = 0; q < RPT; q++) {
+      if (!val[q]) continue;
+      double* o = t.C + row[q] + (i64)c * t.ldc;
+      *o = t.beta == 0. ? acc[q][c] : t.beta * *o + acc[q][c];
     }
   }
 }
 
 }  // namespace
 
-int mf_rows_per_cta() { return MF_BM; }
+int mf_rows_per_cta(int rpt) { return MF_NT * rpt; }
 
-template <int KIND>
+template <int KIND, int RPT>
 static cudaError_t mf_go(const KernelParams& kp, int nr, const MfTask* d_tasks, const MfEntry* d_ents,
                          const int2* d_tiles, int ntiles, cudaStream_t st) {
   switch (nr) {
-    case 1: k_mf_apply<1, KIND><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr); break;
-    case 2: k_mf_apply<2, KIND><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr); break;
+    case 1: k_mf_apply<1, KIND, RPT><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr); break;
+    case 2: k_mf_apply<2, KIND, RPT><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr); break;
     case 3:
-    case 4: k_mf_apply<4, KIND><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr); break;
+    case 4: k_mf_apply<4, KIND, RPT><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr); break;
     case 5:
     case 6:
     case 7:
-    case 8: k_mf_apply<8, KIND><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr); break;
-    default: k_mf_apply<16, KIND><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr);
+    case 8: k_mf_apply<8, KIND, RPT><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr); break;
+    default: k_mf_apply<16, KIND, RPT><<<ntiles, MF_NT, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr);
   }
   return cudaGetLastError();
 }
 
-cudaError_t launch_mf_apply(const KernelParams& kp, int nr, const MfTask* d_tasks, const MfEntry* d_ents,
+template <int RPT>
+static cudaError_t mf_kind(const KernelParams& kp, int nr, const MfTask* d_tasks, const MfEntry* d_ents,
+                           const int2* d_tiles, int ntiles, cudaStream_t st) {
+  if (kp.kind == KERNEL_LAPLACE) return mf_go<KERNEL_LAPLACE, RPT>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
+  if (kp.kind == KERNEL_YUKAWA) return mf_go<KERNEL_YUKAWA, RPT>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
+  return mf_go<KERNEL_QUADRATIC, RPT>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
+}
+
+cudaError_t launch_mf_apply(const KernelParams& kp, int nr, int rpt, const MfTask* d_tasks, const MfEntry* d_ents,
                             const int2* d_tiles, int ntiles, cudaStream_t st) {
   if (ntiles == 0) return cudaSuccess;
-  if (nr < 1 || nr > 16) return cudaErrorInvalidValue;
+  if (nr < 1 || nr > 16 || (rpt != 1 && rpt != 2)) return cudaErrorInvalidValue;
   note_launch();
-  if (kp.kind == KERNEL_LAPLACE) return mf_go<KERNEL_LAPLACE>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
-  if (kp.kind == KERNEL_YUKAWA) return mf_go<KERNEL_YUKAWA>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
-  return mf_go<KERNEL_QUADRATIC>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
+  return rpt == 1 ? mf_kind<1>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st)
+                  : mf_kind<2>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
 }
 
 }  // namespace h2b

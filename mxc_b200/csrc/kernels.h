@@ -157,7 +157,7 @@ int dgemm_tile();
 // Matrix-free block apply (k_mf.cu), FP64: C = beta C + sum over the task's
 // entries of alpha K(pts_task, pts_entry) B (m x nr output, ld ldc; B k x nr,
 // ld ldb; points xyz-interleaved).  tiles: {task, block of
-// mf_rows_per_cta() rows}; nr <= 16.
+// mf_rows_per_cta(rpt) rows}; nr <= 16.
 struct MfTask {
   const double* pts;
   int m;
@@ -173,9 +173,10 @@ struct MfEntry {
   i64 ldb;
   double alpha;
 };
-cudaError_t launch_mf_apply(const KernelParams& kp, int nr, const MfTask* d_tasks, const MfEntry* d_ents,
+cudaError_t launch_mf_apply(const KernelParams& kp, int nr, int rpt, const MfTask* d_tasks, const MfEntry* d_ents,
                             const int2* d_tiles, int ntiles, cudaStream_t st);
-int mf_rows_per_cta();
+// Rows of a task one CTA covers with rpt (1 or 2) rows per thread.
+int mf_rows_per_cta(int rpt);
 
 // BF16 substitution blocks (k_bf16.cu).  Pack: dst (m x k, ld ldd, a
 // multiple of 8) = bf16(src / s), s = 2^ceil(log2 max |src|) written to

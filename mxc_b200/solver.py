@@ -155,6 +155,22 @@ class Handle:
         L.check(L.lib().h2dev_launch_count(C.byref(v)), "h2dev_launch_count")
         return v.value
 
+    def autotune_report(self) -> list:
+        """Autotuner decisions of this handle: (bucket key, chosen variant, [ms per variant])."""
+        n = C.c_int64()
+        L.check(L.lib().h2dev_autotune_report(self.h, 0, None, None, None, C.byref(n)), "h2dev_autotune_report")
+        cnt = n.value
+        if cnt == 0:
+            return []
+        keys = C.create_string_buffer(64 * cnt)
+        choice = np.zeros(cnt, dtype=np.int32)
+        ms = np.zeros(3 * cnt)
+        L.check(L.lib().h2dev_autotune_report(self.h, cnt, keys, _ptr(choice), _ptr(ms), C.byref(n)),
+                "h2dev_autotune_report")
+        raw = keys.raw
+        return [(raw[64 * i:64 * (i + 1)].split(b"\0", 1)[0].decode(), int(choice[i]),
+                 [float(v) for v in ms[3 * i:3 * i + 3] if v >= 0]) for i in range(cnt)]
+
     def fma_peak_tflops(self, precision: int = L.FP64) -> float:
         v = C.c_double()
         L.check(L.lib().h2dev_probe_fma_peak(self.h, precision, C.byref(v)), "h2dev_probe_fma_peak")

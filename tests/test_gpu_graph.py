@@ -66,3 +66,17 @@ def test_graph_solve_with_zero_outer_does_nothing(sys8k):
     h, A, M, B, k, b = sys8k
     X, rc, r, it = solve(h, A, M, B, True, True, outer=0)
     assert np.all(it == 0) and not X.any()
+
+
+def test_graph_replay_with_new_right_hand_sides(sys8k):
+    """The captured solve is kept on the operator and replayed by later calls
+    with the same preconditioner and shape; new right-hand sides give their
+    own (step-by-step-identical) solutions."""
+    h, A, M, B, k, b = sys8k
+    X0, *_ = solve(h, A, M, B, True, True)
+    B2 = np.asfortranarray(B[:, ::-1] * 0.5)
+    X2g, rc, r2g, i2g = solve(h, A, M, B2, True, True)   # replay
+    X2s, rc_s, r2s, i2s = solve(h, A, M, B2, False, True)
+    assert rc == rc_s == 0
+    assert np.array_equal(X2g, X2s) and np.array_equal(r2g, r2s) and np.array_equal(i2g, i2s)
+    np.testing.assert_allclose(X2g, X0[:, ::-1] * 0.5, rtol=1e-8, atol=1e-12)

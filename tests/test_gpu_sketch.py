@@ -131,4 +131,6 @@ def test_sketch_near_levels_plus_samples_matches_oracle(handle):
     yf = x.copy()
     Afull.matVecMul(yf)
     assert rel(y, Ao.matvec(x)) < 1e-11
-    assert rel(y, yd) < 3 * max(rel(yf, yd), 1e-13)
+    # Cheaper than the whole far field, and less accurate (at 16,384 bodies
+    # about 7x the full sketch's error, still well inside the threshold).
+    assert rel(yf, yd) < 1e-12 and rel(y, yd) < 1e-11
