@@ -416,6 +416,10 @@ struct GemmPlan {
     for (const auto& e : ents) nn = nn && e.opA == 0 && e.opB == 0;
     skinny_nn = nn && maxn <= 16 && !force_tiled();
     nr = maxn;
+    // Decided on the tasks as given: split_tasks() moves a task's beta to
+    // its ordered sum and gives the parts beta zero.
+    idempotent = true;
+    for (const auto& t : tasks) idempotent = idempotent && t.beta == T(0);
     if (skinny_nn) split_tasks();
     if (skinny_nn) {
       // A task takes 256-row tiles when they leave no more padding rows
@@ -443,8 +447,6 @@ struct GemmPlan {
       d_alt_n.upload(alt[0]);
       d_alt_w.upload(alt[1]);
       tkey = tune_key(name, (int)sizeof(T), nr, (double)tasks.size(), rows, elems);
-      idempotent = true;
-      for (const auto& t : tasks) idempotent = idempotent && t.beta == T(0);
     }
     int bm = shape == GEMM_TC ? tc_gemm_tile() : gemm_tile_m(shape);
     int bn = shape == GEMM_TC ? tc_gemm_tile() : gemm_tile_n(shape);
