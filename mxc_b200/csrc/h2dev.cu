@@ -303,7 +303,8 @@ static void check_tc(h2dev_handle_s* h) {
   h->tc_pending = false;
   if (flag) {
     ck(cudaMemset(h->d_tc_err, 0, sizeof(int)), "tensor-core GEMM status");
-    throw H2Error{H2DEV_ERR_CUDA, "tensor-core GEMM: an mbarrier wait expired (the result is incomplete)"};
+    throw H2Error{H2DEV_ERR_CUDA,
+                  "tensor-core GEMM or bulk-copy apply: an mbarrier wait expired (the result is incomplete)"};
   }
 }
 
@@ -387,6 +388,9 @@ struct GemmPlan {
   // Only plans that overwrite their outputs (every beta zero) are timed:
   // repeating one leaves the same result, so tuning runs are harmless.
   bool idempotent = false;
+  // FP64 streaming plans whose A columns all start on 16-byte boundaries run
+  // the bulk-copy kernel.
+  bool bulk_ok = false;
   DVec<T> parts_buf;               // partial results of split tasks
   DVec<SumTask<T>> d_sums;
   int nsums = 0, sum_maxmn = 0;
@@ -447,6 +451,9 @@ struct GemmPlan {
       d_alt_n.upload(alt[0]);
       d_alt_w.upload(alt[1]);
       tkey = tune_key(name, (int)sizeof(T), nr, (double)tasks.size(), rows, elems);
+      bulk_ok = sizeof(T) == 8 && nr > 4;
+      for (const auto& e : ents)
+        bulk_ok = bulk_ok && (reinterpret_cast<uintptr_t>(e.A) & 15) == 0 && (e.lda & 1) == 0;
     }
     int bm = shape == GEMM_TC ? tc_gemm_tile() : gemm_tile_m(shape);
     int bn = shape == GEMM_TC ? tc_gemm_tile() : gemm_tile_n(shape);
@@ -589,8 +596,10 @@ struct GemmPlan {
   void run_skinny(int v, cudaStream_t st) const {
     const DVec<int2>& w = v == 0 ? d_rtiles_w : d_alt_w;
     const DVec<int2>& n = v == 0 ? d_rtiles : d_alt_n;
-    if (v != 1) ck(launch_skinny_nn<T>(nr, 1, d_tasks.p, d_ents.p, w.p, (int)w.n, st), "skinny_nn");
-    if (v != 2) ck(launch_skinny_nn<T>(nr, 0, d_tasks.p, d_ents.p, n.p, (int)n.n, st), "skinny_nn");
+    int* be = (bulk_ok && g_cur) ? g_cur->d_tc_err : nullptr;
+    if (be) g_cur->tc_pending = true;
+    if (v != 1) ck(launch_skinny_nn<T>(nr, 1, d_tasks.p, d_ents.p, w.p, (int)w.n, st, be), "skinny_nn");
+    if (v != 2) ck(launch_skinny_nn<T>(nr, 0, d_tasks.p, d_ents.p, n.p, (int)n.n, st, be), "skinny_nn");
     if (nsums) ck(launch_sum_parts<T>(d_sums.p, nsums, sum_maxmn, st), "sum_parts");
   }
 
@@ -2587,6 +2596,7 @@ static int gmres(SolverBase& A, SolverBase& M, double tol, i64 nrhs, double* dX,
   if (use_graph) {
     if (!sg->exec) gmres_graph(A, M, g, *sg);
     A.solve_graph = sg;
+    A.h->tc_pending = true;  // the graph may hold mbarrier-pipelined kernels
     ck(cudaGraphLaunch(sg->exec, st), "graph launch");
     ck(cudaStreamSynchronize(st), "sync");
   } else {

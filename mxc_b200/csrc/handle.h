@@ -33,10 +33,10 @@ struct h2dev_handle_s {
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool prof = false;
-  // Expired-wait flag of the tensor-core GEMM (one int in device memory,
-  // owned by this handle): set by any k_tc_gemm_ws launched on this handle's
-  // streams, read and cleared by check_tc.  tc_pending says such a launch
-  // was queued since the last check.
+  // Expired-wait flag of the mbarrier-pipelined kernels (one int in device
+  // memory, owned by this handle): set by any k_tc_gemm_ws or k_stream_dtma
+  // launched on this handle's streams, read and cleared by check_tc.
+  // tc_pending says such a launch was queued since the last check.
   int* d_tc_err = nullptr;
   bool tc_pending = false;
   int sampling_mode = 0;  // far-list cap rule for solvers created next (H2DEV_OPT_SAMPLING)

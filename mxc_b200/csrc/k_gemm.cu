@@ -493,6 +493,257 @@ __global__ void __launch_bounds__(BM, BM == 256 ? 3 : 6)
   }
 }
 
+// FP64 streaming apply, warp-specialised: one producer warp moves the A
+// slabs with bulk asynchronous copies (cp.async.bulk, one per column of the
+// tile, completion counted in bytes on the stage's mbarrier) and the B slabs
+// with cp.async; BM / 32 consumer warps each own 32 rows x NR columns and
+// only read shared memory and issue mma.sync m16n8k16 FP64.  Stages are
+// handed over by mbarriers (full: the copies landed; empty: every active
+// consumer warp is done with the stage), so no block barrier runs inside
+// the loop.
+//
+// MMA row and k orders are chosen for 16-byte fragment loads: MMA row g
+// (g + 8) of a 16-row block is tile row 2g (2g + 1), so a lane's two A rows
+// are one 16-byte pair of the column-major slab; MMA k index t + 4j is slab
+// column t + 4j.  A columns are stored BM + 4 doubles apart and B rows NR + 4
+// apart, which puts the 8 lanes of an A quarter-warp load (and the 16 lanes
+// of a B half-warp load) on distinct banks.
+//
+// Columns whose start is not 16-byte aligned (odd leading dimension or
+// base) are copied element by element with cp.async by the producer lanes.
+// A slab columns past the entry's K are not copied: their B rows are zero
+// and the stale A values there are finite (the ring is zeroed at start), so
+// they add nothing; rows past the tile's last row produce outputs that are
+// not stored.  Every wait is bounded: an expired wait sets the CTA's abort
+// flag and the error word, the loops end, and the producer waits (bounded)
+// for its last stages' copies before the CTA exits.
+constexpr int DT_KS = 16;
+
+template <int NR, int BM, int ST>
+constexpr size_t stream_dtma_smem() {
+  return sizeof(double) * (size_t)ST * DT_KS * ((BM + 4) + (NR + 4)) + 16 * (size_t)(2 * ST + 2);
+}
+
+__device__ __forceinline__ void dt_arrive_expect(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void dt_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void dt_bulk(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+      "l"(src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ bool dt_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity), "r"(100000u)
+      : "memory");
+  return ok != 0;
+}
+// About two seconds of SM clock cycles.
+constexpr long long DT_WAIT_CYCLES = 4000000000LL;
+// Lane 0 waits for the phase (bounded; the abort flag ends the wait early),
+// the warp learns the outcome.
+__device__ __forceinline__ bool dt_warp_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag, int lane) {
+  int ok = 1;
+  if (lane == 0) {
+    if (!dt_try(bar, parity)) {
+      const long long t0 = clock64();
+      while (!dt_try(bar, parity)) {
+        if (*abort_flag) {
+          ok = 0;
+          break;
+        }
+        if (clock64() - t0 > DT_WAIT_CYCLES) {
+          *abort_flag = 1;
+          ok = 0;
+          break;
+        }
+      }
+    }
+  }
+  return __shfl_sync(0xffffffffu, ok, 0) != 0;
+}
+
+template <int NR, int BM, int ST>
+__global__ void __launch_bounds__(BM + 32) k_stream_dtma(const GemmTask<double>* __restrict__ tasks,
+                                                         const GemmEntry<double>* __restrict__ ents,
+                                                         const int2* __restrict__ tiles, int* __restrict__ err) {
+  constexpr int NC = BM / 32, AS = BM + 4, BS = NR + 4, NF = NR / 8;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* As = reinterpret_cast<double*>(smem_raw);   // [ST][KS][AS]
+  double* Bs = As + (size_t)ST * DT_KS * AS;          // [ST][KS][BS]
+  uint64_t* full = reinterpret_cast<uint64_t*>(Bs + (size_t)ST * DT_KS * BS);
+  uint64_t* empty = full + ST;
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(empty + ST);
+
+  const int2 tl = tiles[blockIdx.x];
+  const GemmTask<double> task = tasks[tl.x];
+  const int m0 = tl.y * BM;
+  const int mrows = min(BM, task.m - m0);
+  const int nact = (mrows + 31) / 32;  // consumer warps with rows
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+
+  for (int i = tid * 2; i < ST * DT_KS * AS; i += 2 * blockDim.x)
+    *reinterpret_cast<double2*>(As + i) = make_double2(0., 0.);
+  // The zeros (generic proxy) are ordered before the bulk copies (async proxy).
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  if (tid == 0) {
+    for (int s = 0; s < ST; s++) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 33;\n" ::"r"(smem_u32(&full[s])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(&empty[s])), "r"(nact) : "memory");
+    }
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+
+  if (warp == NC) {
+    // ---- producer warp
+    int pe = task.e0, pk = 0, g = 0;
+    while (pe < task.e1 && ents[pe].k <= 0) pe++;
+    const int rows2 = (mrows + 1) & ~1;
+    while (pe < task.e1) {
+      const int s = g % ST;
+      if (g >= ST && !dt_warp_wait(smem_u32(&empty[s]), (uint32_t)(((g / ST) - 1) & 1), abort_flag, lane)) break;
+      const GemmEntry<double> en = ents[pe];
+      const int kv = min(DT_KS, en.k - pk);
+      double* as = As + (size_t)s * DT_KS * AS;
+      double* bs = Bs + (size_t)s * DT_KS * BS;
+      const uint32_t fb = smem_u32(&full[s]);
+      const bool aligned = ((reinterpret_cast<uintptr_t>(en.A) & 15) == 0) && ((en.lda & 1) == 0);
+      if (aligned) {
+        if (lane == 0) dt_arrive_expect(fb, (uint32_t)(kv * rows2 * 8));
+        __syncwarp();
+        if (lane < kv) dt_bulk(smem_u32(as + lane * AS), en.A + m0 + (i64)(pk + lane) * en.lda, (uint32_t)rows2 * 8, fb);
+      } else {
+        if (lane == 0) dt_arrive(fb);
+        for (int c = 0; c < kv; c++)
+          for (int r = lane; r < mrows; r += 32) cp_async_ca<8>(as + c * AS + r, en.A + m0 + r + (i64)(pk + c) * en.lda, 8);
+      }
+      for (int idx = lane; idx < DT_KS * NR; idx += 32) {
+        const int k = idx % DT_KS, j = idx / DT_KS;
+        const bool ok = k < kv && j < task.n;
+        const double* src = ok ? en.B + (i64)(pk + k) + (i64)j * en.ldb : en.B;
+        cp_async_ca<8>(bs + k * BS + j, src, ok ? 8 : 0);
+      }
+      asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(fb) : "memory");
+      g++;
+      pk += DT_KS;
+      if (pk >= en.k) {
+        pk = 0;
+        pe++;
+        while (pe < task.e1 && ents[pe].k <= 0) pe++;
+      }
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    if (*abort_flag) {
+      // Let the copies of the stages still in flight land before the CTA's
+      // shared memory is released.
+      for (int q = max(0, g - ST); q < g; q++) {
+        if (lane == 0) {
+          const long long t0 = clock64();
+          while (!dt_try(smem_u32(&full[q % ST]), (uint32_t)((q / ST) & 1)) && clock64() - t0 < DT_WAIT_CYCLES) {
+          }
+        }
+      }
+      if (lane == 0 && err) atomicExch(err, 1);
+    }
+    return;
+  }
+  if (warp >= nact) return;
+
+  // ---- consumer warp: rows m0 + 32 warp .. + 31
+  double acc[2][NF][4];
+#pragma unroll
+  for (int rb = 0; rb < 2; rb++)
+#pragma unroll
+    for (int cb = 0; cb < NF; cb++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[rb][cb][q] = 0.;
+  const int g8 = lane >> 2, t4 = lane & 3;
+  const int wr = warp * 32;
+  const int nrb = min(2, (mrows - wr + 15) / 16);  // 16-row blocks with rows
+  int ce = task.e0, ck = 0, g = 0;
+  while (ce < task.e1 && ents[ce].k <= 0) ce++;
+  bool ok = true;
+  while (ce < task.e1) {
+    const int s = g % ST;
+    if (!dt_warp_wait(smem_u32(&full[s]), (uint32_t)((g / ST) & 1), abort_flag, lane)) {
+      ok = false;
+      break;
+    }
+    const double alpha = ents[ce].alpha;
+    const double* as = As + (size_t)s * DT_KS * AS + wr + 2 * g8;
+    const double* bs = Bs + (size_t)s * DT_KS * BS + g8;
+    double a[2][8], b[NF][4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+#pragma unroll
+      for (int rb = 0; rb < 2; rb++) {
+        const double2 v = *reinterpret_cast<const double2*>(as + (t4 + 4 * j) * AS + 16 * rb);
+        a[rb][2 * j] = v.x;
+        a[rb][2 * j + 1] = v.y;
+      }
+#pragma unroll
+      for (int cb = 0; cb < NF; cb++) b[cb][j] = bs[(t4 + 4 * j) * BS + cb * 8];
+    }
+    if (alpha != 1.) {
+#pragma unroll
+      for (int cb = 0; cb < NF; cb++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) b[cb][j] *= alpha;
+    }
+#pragma unroll
+    for (int rb = 0; rb < 2; rb++)
+      if (rb < nrb)
+#pragma unroll
+        for (int cb = 0; cb < NF; cb++)
+          asm volatile(
+              "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+              "{%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+              : "+d"(acc[rb][cb][0]), "+d"(acc[rb][cb][1]), "+d"(acc[rb][cb][2]), "+d"(acc[rb][cb][3])
+              : "d"(a[rb][0]), "d"(a[rb][1]), "d"(a[rb][2]), "d"(a[rb][3]), "d"(a[rb][4]), "d"(a[rb][5]),
+                "d"(a[rb][6]), "d"(a[rb][7]), "d"(b[cb][0]), "d"(b[cb][1]), "d"(b[cb][2]), "d"(b[cb][3]));
+    __syncwarp();
+    if (lane == 0) dt_arrive(smem_u32(&empty[s]));
+    g++;
+    ck += DT_KS;
+    if (ck >= ents[ce].k) {
+      ck = 0;
+      ce++;
+      while (ce < task.e1 && ents[ce].k <= 0) ce++;
+    }
+  }
+  if (!ok) return;
+  // D fragment of 16-row block rb: c[2h + q] is MMA row g8 + 8h (tile row
+  // 2 g8 + h of the block), column 2 t4 + q of the column block.
+#pragma unroll
+  for (int rb = 0; rb < 2; rb++)
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int r = wr + 16 * rb + 2 * g8 + h;
+      if (r >= mrows) continue;
+#pragma unroll
+      for (int cb = 0; cb < NF; cb++)
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+          const int c = cb * 8 + 2 * t4 + q;
+          if (c < task.n) {
+            double* p = task.C + (m0 + r) + (i64)c * task.ldc;
+            *p = (task.beta == 0.) ? acc[rb][cb][2 * h + q] : task.beta * (*p) + acc[rb][cb][2 * h + q];
+          }
+        }
+    }
+}
+
 // FP32 variant of the streaming apply on the tensor cores through warp-level
 // mma.sync m16n8k8 TF32 with the 3-term split (hi*hi + hi*lo + lo*hi, FP32
 // accumulation: FP32 accuracy) for 8 or 16 right-hand sides.  Same ring and
@@ -704,8 +955,15 @@ int skinny_rows_per_cta(int wide) { return wide ? 256 : 128; }
 
 template <typename T>
 cudaError_t launch_skinny_nn(int nr, int wide, const GemmTask<T>* d_tasks, const GemmEntry<T>* d_ents,
-                             const int2* d_tiles, int ntiles, cudaStream_t st) {
+                             const int2* d_tiles, int ntiles, cudaStream_t st, int* bulk_err) {
   if (ntiles == 0) return cudaSuccess;
+  auto go_bulk = [&](auto kern, size_t smem, int threads) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    note_launch();
+    kern<<<ntiles, threads, smem, st>>>(d_tasks, d_ents, d_tiles, bulk_err);
+    return cudaGetLastError();
+  };
   auto go = [&](auto kern, size_t smem, int threads) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -725,7 +983,17 @@ cudaError_t launch_skinny_nn(int nr, int wide, const GemmTask<T>* d_tasks, const
     }
   }
   if constexpr (sizeof(T) == 8) {
-    // FP64 with 5..16 right-hand sides: tensor-core variant, BM threads.
+    // FP64 with 5..16 right-hand sides on the FP64 tensor cores: the
+    // warp-specialised bulk-copy kernel (BM + 32 threads, three stages, two
+    // CTAs per SM), or the cp.async ring (BM threads).
+    if (bulk_err && nr > 4 && nr <= 16) {
+      if (nr <= 8) {
+        if (wide) return go_bulk(k_stream_dtma<8, 256, 3>, stream_dtma_smem<8, 256, 3>(), 288);
+        return go_bulk(k_stream_dtma<8, 128, 3>, stream_dtma_smem<8, 128, 3>(), 160);
+      }
+      if (wide) return go_bulk(k_stream_dtma<16, 256, 3>, stream_dtma_smem<16, 256, 3>(), 288);
+      return go_bulk(k_stream_dtma<16, 128, 3>, stream_dtma_smem<16, 128, 3>(), 160);
+    }
     if (nr > 4 && nr <= 8) {
       if (wide) return go(k_stream_dmma<8, 256>, stream_dmma_smem<8, 256>(), 256);
       return go(k_stream_dmma<8, 128>, stream_dmma_smem<8, 128>(), 128);
@@ -749,8 +1017,8 @@ cudaError_t launch_skinny_nn(int nr, int wide, const GemmTask<T>* d_tasks, const
   return cudaErrorInvalidValue;
 }
 template cudaError_t launch_skinny_nn<double>(int, int, const GemmTask<double>*, const GemmEntry<double>*, const int2*,
-                                              int, cudaStream_t);
+                                              int, cudaStream_t, int*);
 template cudaError_t launch_skinny_nn<float>(int, int, const GemmTask<float>*, const GemmEntry<float>*, const int2*,
-                                             int, cudaStream_t);
+                                             int, cudaStream_t, int*);
 
 }  // namespace h2b

@@ -121,12 +121,16 @@ cudaError_t launch_seg_gemm(int shape, const GemmTask<T>* d_tasks, const GemmEnt
                             int ntiles, cudaStream_t st);
 int gemm_tile_m(int shape);
 // Plans whose entries all use A and B as stored and whose outputs have at
-// most 16 columns: A streamed from HBM through a cp.async shared-memory
-// ring, one CTA per skinny_rows_per_cta(wide) rows of a task (tile = {task,
-// row block}); wide = 0 for tasks of at most 128 rows, 1 otherwise.
+// most 16 columns: A streamed from HBM through a shared-memory ring, one CTA
+// per skinny_rows_per_cta(wide) rows of a task (tile = {task, row block});
+// wide = 0 for tasks of at most 128 rows, 1 otherwise.  FP64 plans with 5-16
+// columns given bulk_err (a device int) run the warp-specialised bulk-copy
+// kernel, which wants every A column start 16-byte aligned for full speed
+// and sets *bulk_err when one of its mbarrier waits expires; without
+// bulk_err they run the cp.async ring.
 template <typename T>
 cudaError_t launch_skinny_nn(int nr, int wide, const GemmTask<T>* d_tasks, const GemmEntry<T>* d_ents,
-                             const int2* d_tiles, int ntiles, cudaStream_t st);
+                             const int2* d_tiles, int ntiles, cudaStream_t st, int* bulk_err = nullptr);
 int skinny_rows_per_cta(int wide);
 // Reduction of a split task: dst (m x n, ld ldd) = beta dst + sum of `parts`
 // consecutive m x n partial results at src.
