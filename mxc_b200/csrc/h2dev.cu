@@ -694,13 +694,17 @@ struct MfPlan {
   }
   void tune(const KernelParams& kp, cudaStream_t st) const {
     if (variant >= 0) return;
+    if (nr > 4) {  // one kernel (tensor cores, 128-row tiles): nothing to choose
+      variant = 1;
+      return;
+    }
     const int v = tuned_variant(tkey, 2, st, [&](int x) { launch(kp, x, st); });  // beta 0: repeatable
     if (!stream_capturing(st)) variant = v;
   }
   void run(const KernelParams& kp, cudaStream_t st) const {
     tune(kp, st);
     Prof p(name, flops, bytes, st);
-    launch(kp, variant < 0 ? 0 : variant, st);
+    launch(kp, variant < 0 ? (nr > 4 ? 1 : 0) : variant, st);
   }
 };
 

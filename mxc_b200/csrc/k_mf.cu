@@ -105,6 +105,96 @@ __global__ void __launch_bounds__(MF_NT, RPT == 1 ? 8 : 4)
   }
 }
 
+// Tensor-core variant for 5-16 right-hand sides: the kernel block is
+// generated straight into mma.sync m16n8k16 FP64 fragments and multiplied
+// by the right-hand sides on the FP64 tensor cores; no shared memory and
+// no block barriers.  Each warp owns 32 rows of a task (its lane holds rows
+// g, g + 8, g + 16, g + 24 with their bodies in registers) and walks the
+// task's entries in 16-column steps: a lane evaluates K for its 4 rows x 4
+// columns (t, t + 4, t + 8, t + 12 of the step; bodies and right-hand sides
+// read through L1, where the CTA's other warps find them again) and the warp
+// issues 2 x NR / 8 MMAs.  Rows past m evaluate against a copy of row 0 and
+// are not stored; columns past the entry's k contribute zero.  Per row the
+// pairs are summed by the MMAs in k order, a fixed order for a given plan.
+constexpr int MFD_WARPS = 4;
+
+template <int NR, int KIND>
+__global__ void __launch_bounds__(32 * MFD_WARPS) k_mf_dmma(KernelParams kp, const MfTask* __restrict__ tasks,
+                                                             const MfEntry* __restrict__ ents,
+                                                             const int2* __restrict__ tiles, int nr) {
+  constexpr int NF = NR / 8;
+  const int2 tl = tiles[blockIdx.x];
+  const MfTask t = tasks[tl.x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g8 = lane >> 2, t4 = lane & 3;
+  const int r0 = tl.y * 32 * MFD_WARPS + warp * 32;
+  if (r0 >= t.m) return;
+  double px[4], py[4], pz[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int r = r0 + g8 + 8 * q;
+    const int rr = r < t.m ? r : 0;
+    px[q] = t.pts[3 * rr];
+    py[q] = t.pts[3 * rr + 1];
+    pz[q] = t.pts[3 * rr + 2];
+  }
+  double acc[2][NF][4];
+#pragma unroll
+  for (int rb = 0; rb < 2; rb++)
+#pragma unroll
+    for (int cb = 0; cb < NF; cb++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[rb][cb][q] = 0.;
+  for (int e = t.e0; e < t.e1; e++) {
+    const MfEntry en = ents[e];
+    for (int k0 = 0; k0 < en.k; k0 += 16) {
+      double a[2][8], b[NF][4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int c = k0 + t4 + 4 * j;
+        const bool cv = c < en.k;
+        const double* cp = en.pts + 3 * (i64)(cv ? c : 0);
+        const double cx = __ldg(cp), cy = __ldg(cp + 1), cz = __ldg(cp + 2);
+#pragma unroll
+        for (int cb = 0; cb < NF; cb++)
+          b[cb][j] = (cv && cb * 8 + g8 < nr) ? en.alpha * __ldg(en.B + c + (i64)(cb * 8 + g8) * en.ldb) : 0.;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          // row g8 + 8q: block q >> 1, fragment half q & 1
+          const double v = kernel_eval<KIND>(kp, px[q] - cx, py[q] - cy, pz[q] - cz);
+          a[q >> 1][2 * j + (q & 1)] = cv ? v : 0.;
+        }
+      }
+#pragma unroll
+      for (int rb = 0; rb < 2; rb++)
+#pragma unroll
+        for (int cb = 0; cb < NF; cb++)
+          asm volatile(
+              "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, "
+              "{%4,%5,%6,%7,%8,%9,%10,%11}, {%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+              : "+d"(acc[rb][cb][0]), "+d"(acc[rb][cb][1]), "+d"(acc[rb][cb][2]), "+d"(acc[rb][cb][3])
+              : "d"(a[rb][0]), "d"(a[rb][1]), "d"(a[rb][2]), "d"(a[rb][3]), "d"(a[rb][4]), "d"(a[rb][5]),
+                "d"(a[rb][6]), "d"(a[rb][7]), "d"(b[cb][0]), "d"(b[cb][1]), "d"(b[cb][2]), "d"(b[cb][3]));
+    }
+  }
+  // c[2h + q] of block rb: row 16 rb + g8 + 8h, column cb * 8 + 2 t4 + q.
+#pragma unroll
+  for (int rb = 0; rb < 2; rb++)
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int r = r0 + 16 * rb + g8 + 8 * h;
+      if (r >= t.m) continue;
+#pragma unroll
+      for (int cb = 0; cb < NF; cb++)
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+          const int c = cb * 8 + 2 * t4 + q;
+          if (c >= nr) continue;
+          double* o = t.C + r + (i64)c * t.ldc;
+          *o = t.beta == 0. ? acc[rb][cb][2 * h + q] : t.beta * *o + acc[rb][cb][2 * h + q];
+        }
+    }
+}
+
 }  // namespace
 
 int mf_rows_per_cta(int rpt) { return MF_NT * rpt; }
@@ -126,9 +216,24 @@ static cudaError_t mf_go(const KernelParams& kp, int nr, const MfTask* d_tasks, 
   return cudaGetLastError();
 }
 
+template <int KIND>
+static cudaError_t mf_dmma_go(const KernelParams& kp, int nr, const MfTask* d_tasks, const MfEntry* d_ents,
+                              const int2* d_tiles, int ntiles, cudaStream_t st) {
+  if (nr <= 8)
+    k_mf_dmma<8, KIND><<<ntiles, 32 * MFD_WARPS, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr);
+  else
+    k_mf_dmma<16, KIND><<<ntiles, 32 * MFD_WARPS, 0, st>>>(kp, d_tasks, d_ents, d_tiles, nr);
+  return cudaGetLastError();
+}
+
 template <int RPT>
 static cudaError_t mf_kind(const KernelParams& kp, int nr, const MfTask* d_tasks, const MfEntry* d_ents,
                            const int2* d_tiles, int ntiles, cudaStream_t st) {
+  if (RPT == 1 && nr > 4) {
+    if (kp.kind == KERNEL_LAPLACE) return mf_dmma_go<KERNEL_LAPLACE>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
+    if (kp.kind == KERNEL_YUKAWA) return mf_dmma_go<KERNEL_YUKAWA>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
+    return mf_dmma_go<KERNEL_QUADRATIC>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
+  }
   if (kp.kind == KERNEL_LAPLACE) return mf_go<KERNEL_LAPLACE, RPT>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
   if (kp.kind == KERNEL_YUKAWA) return mf_go<KERNEL_YUKAWA, RPT>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
   return mf_go<KERNEL_QUADRATIC, RPT>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);

@@ -161,7 +161,9 @@ int dgemm_tile();
 // Matrix-free block apply (k_mf.cu), FP64: C = beta C + sum over the task's
 // entries of alpha K(pts_task, pts_entry) B (m x nr output, ld ldc; B k x nr,
 // ld ldb; points xyz-interleaved).  tiles: {task, block of
-// mf_rows_per_cta(rpt) rows}; nr <= 16.
+// mf_rows_per_cta(rpt) rows}; nr <= 16.  With rpt 1 and nr > 4 the block is
+// generated into FP64 tensor-core fragments (k_mf_dmma), otherwise each
+// thread accumulates rpt rows on the FP64 FMA pipe.
 struct MfTask {
   const double* pts;
   int m;
