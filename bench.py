@@ -72,15 +72,27 @@ def parse():
     ap.add_argument("--tensor-cores", type=int, default=1, choices=[0, 1, 2],
                     help="FP32 contractions: 1 tcgen05 3-term TF32 split (default), 2 one TF32 product, 0 SIMT")
     ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--no-graph-compare", action="store_true", help="skip the step-by-step vs CUDA-graph solve timing")
+    ap.add_argument("--no-bf16-ablation", action="store_true", help="skip the BF16 substitution ablation")
     ap.add_argument("--graph-solve", type=int, default=0, choices=[0, 1],
                     help="run each GMRES solve as one captured CUDA graph (H2DEV_OPT_GRAPH_SOLVE)")
     ap.add_argument("--diag1-outer", type=int, default=8,
                     help="restarts of the diagonal-1 variant (Laplace3D(1), the reference's own diagonal; 0: skip)")
-    ap.add_argument("--serving-requests", type=int, default=120,
-                    help="requests of the serving phase (0: skip); Poisson arrivals over resident systems")
-    ap.add_argument("--serving-rate", type=float, default=200.0, help="mean arrival rate, requests / s")
-    ap.add_argument("--serving-systems", default="8192c,8192m,32768c,32768m,131072c,131072m,262144c",
-                    help="resident systems: size + c (uniform cube) or m (32-component Gaussian mixture)")
+    ap.add_argument("--c3-n", type=int, default=1048576,
+                    help="bodies of the uneven-batching sub-run (Gaussian mixture, geometric leaf-capped split, "
+                         "matrix-free operator; 0: skip)")
+    ap.add_argument("--c3-fp64-n", type=int, default=524288,
+                    help="bodies of the sub-run's mixed-vs-FP64 comparison (the FP64 preconditioner does not fit "
+                         "in HBM at 1,048,576; 0: skip)")
+    ap.add_argument("--serving-requests", type=int, default=60,
+                    help="requests per arrival rate of the serving phase (0: skip); Poisson arrivals over resident "
+                         "systems")
+    ap.add_argument("--serving-rates", default="4,8,16,200",
+                    help="mean arrival rates swept, requests / s (200: the serving configuration's offered load)")
+    ap.add_argument("--serving-systems",
+                    default="8192c,8192m,32768c,32768m,131072c,131072m,262144c:mf,262144m:mf",
+                    help="resident systems: size + c (uniform cube) or m (32-component Gaussian mixture), "
+                         "':mf' for a matrix-free operator")
     ap.add_argument("--serving-budget-gb", type=float, default=140.0, help="HBM budget of the serving phase")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="one profiled step, no timing (for ncu)")
@@ -197,6 +209,14 @@ class ClockSampler:
         return {"sm_mhz": med, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def log(msg: str) -> None:
+    """Progress on stderr (the JSON line alone goes to stdout)."""
+    print("[bench %.1fs] %s" % (time.perf_counter() - T_START, msg), file=sys.stderr, flush=True)
+
+
+T_START = time.perf_counter()
+
+
 def dist_setup(a):
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -242,11 +262,15 @@ def rhs_matrix(n: int, nrhs: int):
 
 def run_serving(a, local: int) -> dict:
     """Continuous-batching serving phase: resident systems of the given sizes
-    (uniform cube and 32-component Gaussian mixture each; Laplace with the
-    bench's diagonal, operator eps 1e-8, preconditioner rank 100, 4000
-    samples), a seeded Poisson stream of requests with 1-64 uniform[0,1)
-    right-hand sides each, target residual 1e-10.  Latency is submit to
-    completion; throughput counts completed requests (solves) and columns."""
+    (uniform cube or 32-component Gaussian mixture; Laplace with the bench's
+    diagonal, operator eps 1e-8, preconditioner rank 100, 4000 samples; a
+    system name ending in ":mf" keeps its operator matrix-free), then seeded
+    Poisson streams of requests with 1-64 uniform[0,1) right-hand sides each,
+    target residual 1e-10, at each arrival rate of --serving-rates in turn.
+    Latency is submit to completion; throughput counts completed requests
+    (solves) and columns.  A rate is sustained when the last request
+    completes within a second of its arrival window, i.e. the queue did not
+    grow without bound."""
     import numpy as np
 
     import mxc_b200 as m
@@ -254,11 +278,15 @@ def run_serving(a, local: int) -> dict:
 
     names = [x for x in a.serving_systems.split(",") if x]
     k = m.Laplace3D(a.singularity)
-    specs = []
+    specs, labels = [], []
     for i, nm in enumerate(names):
-        n = int(nm[:-1])
-        pts = m.uniform_unit_cube_rnd(n, 1000 + i) if nm[-1] == "c" else S.gaussian_mixture_points(n, 32, seed=2000 + i)
-        specs.append(S.SystemSpec(points=pts, kernel=k, op_eps=1e-8, rank=100, samples=4000, device=local))
+        mf = nm.endswith(":mf")
+        base = nm[:-3] if mf else nm
+        n = int(base[:-1])
+        pts = m.uniform_unit_cube_rnd(n, 1000 + i) if base[-1] == "c" else S.gaussian_mixture_points(n, 32, seed=2000 + i)
+        specs.append(S.SystemSpec(points=pts, kernel=k, op_eps=1e-8, rank=100, samples=4000, device=local,
+                                  matrix_free=mf))
+        labels.append("%d %s%s" % (n, "cube" if base[-1] == "c" else "mixture", ", matrix-free operator" if mf else ""))
     srv = S.Server(hbm_budget_bytes=int(a.serving_budget_gb * 1e9), max_batch=16, workers=4, inner=a.inner,
                    outer=a.outer)
     try:
@@ -266,35 +294,178 @@ def run_serving(a, local: int) -> dict:
         sids = [srv.add_system(sp) for sp in specs]
         build_s = time.perf_counter() - t0
         resident = srv.resident_bytes()
+        log("serving: %d systems resident (%.1f GB) after %.1f s" % (len(sids), resident / 1e9, build_s))
+        sweep = []
         rng = np.random.default_rng(20261203)
-        gaps = rng.exponential(1.0 / a.serving_rate, a.serving_requests)
-        which = rng.integers(0, len(sids), a.serving_requests)
-        widths = rng.integers(1, 65, a.serving_requests)
-        srv.reset_stats()
-        futs = []
-        t_start = time.perf_counter()
-        t_next = t_start
-        for g, w_, k_ in zip(gaps, which, widths):
-            t_next += g
-            dt = t_next - time.perf_counter()
-            if dt > 0:
-                time.sleep(dt)
-            futs.append(srv.submit(sids[w_], rng.random((specs[w_].points.shape[0], int(k_))), 1e-10))
-        res = [f.result() for f in futs]
-        t_end = time.perf_counter()
-        st = srv.stats()
-        worst = float(max(float(r[1].max()) for r in res))
-        return {"systems": ["%s %s" % (nm[:-1], "cube" if nm[-1] == "c" else "mixture") for nm in names],
-                "requests": a.serving_requests, "arrival_rate_req_s": a.serving_rate, "rhs_per_request": "1-64",
-                "seconds": t_end - t_start, "solves_per_s": a.serving_requests / (t_end - t_start),
-                "rhs_per_s": st["columns"] / (t_end - t_start), "p50_s": st["p50_s"], "p99_s": st["p99_s"],
-                "batches": st["batches"], "max_final_resid": worst, "resident_gb": resident / 1e9,
-                "budget_gb": a.serving_budget_gb,
-                "build_s": build_s, "workers": 4, "batch_width": 16,
+        for rate in [float(x) for x in a.serving_rates.split(",") if x]:
+            gaps = rng.exponential(1.0 / rate, a.serving_requests)
+            which = rng.integers(0, len(sids), a.serving_requests)
+            widths = rng.integers(1, 65, a.serving_requests)
+            srv.reset_stats()
+            futs = []
+            t_start = time.perf_counter()
+            t_next = t_start
+            for g, w_, k_ in zip(gaps, which, widths):
+                t_next += g
+                dt = t_next - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                futs.append(srv.submit(sids[w_], rng.random((specs[w_].points.shape[0], int(k_))), 1e-10))
+            t_last_arrival = time.perf_counter()
+            res = [f.result() for f in futs]
+            t_end = time.perf_counter()
+            st = srv.stats()
+            worst = float(max(float(r[1].max()) for r in res))
+            row = {"arrival_rate_req_s": rate, "requests": a.serving_requests, "seconds": t_end - t_start,
+                   "solves_per_s": a.serving_requests / (t_end - t_start),
+                   "rhs_per_s": st["columns"] / (t_end - t_start), "p50_s": st["p50_s"], "p99_s": st["p99_s"],
+                   "batches": st["batches"], "drain_s": t_end - t_last_arrival,
+                   "sustained": (t_end - t_last_arrival) < 1.0, "max_final_resid": worst}
+            log("serving at %.1f req/s: %.1f solves/s, p50 %.3f s, p99 %.3f s, drain %.2f s"
+                % (rate, row["solves_per_s"], row["p50_s"], row["p99_s"], row["drain_s"]))
+            sweep.append(row)
+        ok = [r for r in sweep if r["sustained"]]
+        best = max(ok, key=lambda r: r["arrival_rate_req_s"]) if ok else None
+        return {"systems": labels, "rhs_per_request": "1-64", "resident_gb": resident / 1e9,
+                "budget_gb": a.serving_budget_gb, "build_s": build_s, "workers": 4, "batch_width": 16,
+                "sweep": sweep,
+                "highest_sustained_rate_req_s": best["arrival_rate_req_s"] if best else None,
+                "p50_s_at_highest_sustained": best["p50_s"] if best else None,
+                "p99_s_at_highest_sustained": best["p99_s"] if best else None,
+                "solves_per_s_at_highest_sustained": best["solves_per_s"] if best else None,
                 "note": "operator eps 1e-8, preconditioner rank 100 / 4000 samples, FP32 preconditioner, "
-                        "FP64 GMRES(%d) to 1e-10; arrivals seeded (numpy default_rng 20261203)" % a.inner}
+                        "FP64 GMRES(%d) to 1e-10; arrivals seeded (numpy default_rng 20261203); sustained = the "
+                        "last request done within 1 s of the last arrival" % a.inner}
     finally:
         srv.close()
+
+
+def run_c3(a, h) -> dict:
+    """Uneven-batching configuration as a sub-run: Gaussian-mixture bodies
+    (32 components, sigma 0.01-0.2, seed 999) in a geometric tree whose cuts
+    are clamped to 32-256 bodies per leaf (mean 128), Laplace with diagonal
+    1/s, s = 1e-6, theta 2, a matrix-free FP64 operator (eps 1e-8, bases from
+    a sketch of the nearest three levels' far bodies plus 4000 strided
+    farther ones), an FP32 preconditioner of rank 128 / 4000 samples and FP64
+    GMRES to 1e-10 for 16 right-hand sides.  Mixed precision at --c3-n (1
+    warm-up + 2 timed steps); the FP64-factor path on the same inputs where
+    it fits (--c3-fp64-n).  The diagonal: clusters with sigma 0.01 hold about
+    32,000 bodies within a few hundredths, so their kernel row sums reach
+    ~1e6; with the benchmark's diagonal 1e4 the reference method's dropped
+    near-field fill leaves GMRES stagnating near 1e-6 (measured), with 1e6 it
+    converges in three restarts."""
+    import numpy as np
+    import torch
+
+    import mxc_b200 as m
+    from mxc_b200 import serving as S
+
+    s_c3, leaf, lo, hi, rank, nrhs = 1e-6, 128, 32, 256, 128, 16
+    k = m.Laplace3D(s_c3)
+
+    def setup(n):
+        L = m.levels_for(n, leaf)
+        b = S.gaussian_mixture_points(n, 32, seed=999)
+        t = m.build_tree(b, L, leaf_min=lo, leaf_max=hi)
+        h.set_option(m._lib.OPT_SAMPLING, m._lib.SAMPLING_SKETCH)
+        h.set_option(m._lib.OPT_MATRIX_FREE, 1)
+        t0 = time.time()
+        try:
+            A = m.H2MatrixSolver(h, k, 1e-8, rank, 0, t, 2.0, b, samples=4000, precision=m.FP64)
+            h.synchronize()
+        finally:
+            h.set_option(m._lib.OPT_SAMPLING, m._lib.SAMPLING_STRIDED)
+            h.set_option(m._lib.OPT_MATRIX_FREE, 0)
+        op_s = time.time() - t0
+        Xt = np.random.default_rng(20261203).random((n, nrhs))
+        B = np.asfortranarray(m.dense_matvec(h, k, b, np.asfortranarray(Xt)))
+        dB = torch.from_numpy(B.T.copy()).cuda()
+        dX = torch.zeros_like(dB)
+        torch.cuda.synchronize()
+        return A, b, t, Xt, B, dB, dX, op_s
+
+    def one(A, b, t, dB, dX, n, prec):
+        dX.zero_()
+        torch.cuda.synchronize()
+        h.timer_start()
+        M = m.H2MatrixSolver(h, k, 0.0, rank, 0, t, 2.0, b, samples=4000, precision=prec)
+        tb = h.timer_stop()
+        h.timer_start()
+        M.factorizeM()
+        tf = h.timer_stop()
+        h.timer_start()
+        rc, resid, iters = A.gmres_device(M, a.tol, dX.data_ptr(), dB.data_ptr(), nrhs, n, a.inner, a.outer, True)
+        ts = h.timer_stop()
+        M.close()
+        return {"build_ms": tb, "factor_ms": tf, "solve_ms": ts, "total_ms": tb + tf + ts, "converged": rc == 0,
+                "cycles": [int(v) for v in iters], "h2_resid_max": float(max(resid[int(iters[c]), c] for c in range(nrhs)))}
+
+    def check(b, Xt, B, dX):
+        X = np.asfortranarray(dX.cpu().numpy().T)
+        R = m.dense_matvec(h, k, b, X)
+        return (X, float(max(np.linalg.norm(B[:, c] - R[:, c]) / np.linalg.norm(B[:, c]) for c in range(nrhs))),
+                float(max(np.linalg.norm(X[:, c] - Xt[:, c]) / np.linalg.norm(Xt[:, c]) for c in range(nrhs))))
+
+    out = {"workload": "N=%d 32-component Gaussian mixture (sigma 0.01-0.2, seed 999), geometric split clamped to "
+                       "%d-%d bodies per leaf (mean %d), Laplace 1/r diag 1/s s=%g, theta=2, operator eps 1e-8 "
+                       "matrix-free (sketch: nearest three levels' far bodies + 4000 strided), FP32 preconditioner "
+                       "rank %d / 4000 samples, FP64 GMRES(%d) to %g, nrhs=%d"
+                       % (a.c3_n, lo, hi, leaf, s_c3, rank, a.inner, a.tol, nrhs)}
+    h.trim()
+    h.memory_peak(reset=True)
+    A, b, t, Xt, B, dB, dX, op_s = setup(a.c3_n)
+    out["operator_build_s"] = op_s
+    one(A, b, t, dB, dX, a.c3_n, m.FP32)
+    runs = [one(A, b, t, dB, dX, a.c3_n, m.FP32) for _ in range(2)]
+    X, dres, xerr = check(b, Xt, B, dX)
+    ms = sum(r["total_ms"] for r in runs) / len(runs)
+    d0, r0 = A.level_dims(A.levels)
+    out.update({"ms_per_step": ms, "value": a.c3_n * nrhs / (ms / 1e3), "unit": UNIT,
+                "phases_ms": {p: sum(r[p + "_ms"] for r in runs) / len(runs) for p in ("build", "factor", "solve")},
+                "gmres_cycles": runs[-1]["cycles"], "converged": all(r["converged"] for r in runs),
+                "h2_resid_max": runs[-1]["h2_resid_max"], "dense_resid_max": dres, "x_true_err_max": xerr,
+                "leaf_bodies": {"min": int(d0.min()), "max": int(d0.max()), "mean": float(d0.mean())},
+                "operator_leaf_ranks": {"min": int(r0.min()), "max": int(r0.max()), "mean": float(r0.mean())},
+                "peak_device_gb": h.memory_peak() / 1e9,
+                "dense_resid_note": "bounded by the operator's eps 1e-8 (GMRES reaches the H2 residual)"})
+    log("c3: %.1f ms/step %s, cycles %s, dense residual %.2e, peak %.1f GB"
+        % (ms, out["phases_ms"], runs[-1]["cycles"], dres, out["peak_device_gb"]))
+    try:
+        h.trim()
+        one(A, b, t, dB, dX, a.c3_n, m.FP64)
+        out["fp64_factor"] = "ran"
+    except m._lib.H2DevError as e:
+        if e.code != 3:
+            raise
+        out["fp64_factor"] = {"unavailable": "the FP64 preconditioner does not fit in HBM at N=%d next to the "
+                                             "operator (%s); the mixed-vs-FP64 ratio is measured at N=%d"
+                                             % (a.c3_n, e, a.c3_fp64_n)}
+    A.close()
+    del dB, dX
+    h.trim()
+    if a.c3_fp64_n > 0:
+        A, b, t, Xt, B, dB, dX, _ = setup(a.c3_fp64_n)
+        one(A, b, t, dB, dX, a.c3_fp64_n, m.FP32)
+        rm = one(A, b, t, dB, dX, a.c3_fp64_n, m.FP32)
+        Xm, dres_m, _ = check(b, Xt, B, dX)
+        h.trim()
+        one(A, b, t, dB, dX, a.c3_fp64_n, m.FP64)
+        r64 = one(A, b, t, dB, dX, a.c3_fp64_n, m.FP64)
+        X64, dres_64, _ = check(b, Xt, B, dX)
+        out["mixed_vs_fp64"] = {
+            "n": a.c3_fp64_n, "mixed_ms": rm["total_ms"], "fp64_ms": r64["total_ms"],
+            "speedup_mixed_vs_fp64": r64["total_ms"] / rm["total_ms"],
+            "mixed_phases_ms": {p: rm[p + "_ms"] for p in ("build", "factor", "solve")},
+            "fp64_phases_ms": {p: r64[p + "_ms"] for p in ("build", "factor", "solve")},
+            "cycles_mixed": rm["cycles"], "cycles_fp64": r64["cycles"],
+            "dense_resid_mixed": dres_m, "dense_resid_fp64": dres_64,
+            "x_mixed_vs_fp64_rel_max": float(max(np.linalg.norm(X64[:, c] - Xm[:, c]) / np.linalg.norm(X64[:, c])
+                                                 for c in range(nrhs)))}
+        log("c3 at N=%d: mixed %.1f ms, FP64 %.1f ms" % (a.c3_fp64_n, rm["total_ms"], r64["total_ms"]))
+        A.close()
+        del dB, dX
+        h.trim()
+    return out
 
 
 def run_ours(a):
@@ -342,6 +513,8 @@ def run_ours(a):
         torch.cuda.synchronize()
         prof_api.start()
     A, op_build_s, op_rep = build_operator(k, not a.profile_only)
+    log("operator built in %.1f s; device memory (live, cached) %s, peak live %.1f GB"
+        % (op_build_s, h.memory(), h.memory_peak(reset=True) / 1e9))
     if a.profile_only and a.profile_phase == "operator":
         h.synchronize()
         prof_api.stop()
@@ -418,6 +591,9 @@ def run_ours(a):
     ck = clocks.stop()
     dist_barrier(ws)
     ms = [r["total_ms"] for r in runs]
+    log("timed steps (build, factor, solve ms): %s; cycles %s; memory %s, peak live %.1f GB"
+        % ([[round(r["build_ms"], 1), round(r["factor_ms"], 1), round(r["solve_ms"], 1)] for r in runs],
+           runs[-1]["iters"], h.memory(), h.memory_peak(reset=True) / 1e9))
     ms_step = sum(ms) / len(ms)
     ms_step_max = dist_max(ms_step, ws)
 
@@ -444,10 +620,21 @@ def run_ours(a):
 
     # FP64-factor comparison (BASELINE: mixed vs FP64 on the same GPU): its
     # solution is the FP64 reference solution the mixed one is held to.
+    log("e2e %.1f ms/step; dense residual %.3e, x error %.3e" % (e2e_step, max(dense_res), max(xerr)))
     fp64 = None
     if a.precision == "mixed" and not a.no_fp64_compare:
-        step(m.FP64)  # warm-up: the FP64 path's first step also sizes its memory cache
-        r64 = step(m.FP64)
+        h.trim()  # the FP32 steps' cached blocks go back before the larger FP64 preconditioner is built
+        try:
+            step(m.FP64)  # warm-up: the FP64 path's first step also sizes its memory cache
+            r64 = step(m.FP64)
+        except m._lib.H2DevError as e:
+            if e.code != 3:
+                raise
+            r64 = None
+            fp64 = {"unavailable": "FP64 preconditioner does not fit next to the operator: %s" % e}
+            log(fp64["unavailable"])
+            h.trim()
+    if a.precision == "mixed" and not a.no_fp64_compare and r64 is not None:
         X64 = np.asfortranarray(dX.cpu().numpy().T)
         R64 = m.dense_matvec(h, k, b, X64)
         fp64 = {"ms_per_step": r64["total_ms"], "build_ms": r64["build_ms"], "factor_ms": r64["factor_ms"],
@@ -460,8 +647,10 @@ def run_ours(a):
 
     # The solve phase launched step by step against captured as one CUDA
     # graph (same kernels, same order, same result).
+    if fp64 and "speedup_mixed_vs_fp64" in fp64:
+        log("FP64-factor step %.1f ms (mixed %.1f ms)" % (fp64["ms_per_step"], ms_step_max))
     graph = None
-    if not a.no_fp64_compare:
+    if not a.no_fp64_compare and not a.no_graph_compare:
         # One factored preconditioner, solved against repeatedly (as a
         # serving system is): step by step, then as a graph -- the first
         # graph solve captures and instantiates, later ones replay.
@@ -492,7 +681,7 @@ def run_ours(a):
     # Ablation: the FP32 preconditioner's substitution applied from BF16
     # copies of its blocks (per-block power-of-two scale, FP32 arithmetic).
     bf16_ab = None
-    if a.precision == "mixed" and not a.no_fp64_compare:
+    if a.precision == "mixed" and not a.no_fp64_compare and not a.no_bf16_ablation:
         step(m.FP32, bf16=True)
         rb = step(m.FP32, bf16=True)
         Xb = np.asfortranarray(dX.cpu().numpy().T)
@@ -616,12 +805,26 @@ def run_ours(a):
                          % a.diag1_outer}
         A1.close()
 
-    serving = None
-    if a.serving_requests > 0:
-        del dX, dXt, dB, dbod
+    del dX, dXt, dB, dbod
+    h.trim()
+    torch.cuda.empty_cache()
+    c3 = None
+    if a.c3_n > 0 and rank == 0:
+        try:
+            c3 = run_c3(a, h)
+        except Exception as e:  # recorded, the headline line still prints
+            c3 = {"error": "%s: %s" % (type(e).__name__, e)}
+            log("c3 failed: %s" % c3["error"])
         h.trim()
         torch.cuda.empty_cache()
-        serving = run_serving(a, local)
+
+    serving = None
+    if a.serving_requests > 0:
+        try:
+            serving = run_serving(a, local)
+        except Exception as e:
+            serving = {"error": "%s: %s" % (type(e).__name__, e)}
+            log("serving failed: %s" % serving["error"])
 
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
@@ -670,6 +873,7 @@ def run_ours(a):
             "bf16_apply_ablation": bf16_ab,
             "graph_solve": graph,
             "diag1": diag1,
+            "uneven_batching_c3": c3,
             "gpu_at_cpu_sample": small,
             "serving": serving,
             "cpu_baseline": cpu,

@@ -74,6 +74,11 @@ int h2dev_handle_synchronize(h2dev_handle_t h);
 int h2dev_handle_memory(h2dev_handle_t h, int64_t* live_bytes, int64_t* cached_bytes);
 /* Returns the handle's cached (free) device blocks to the driver. */
 int h2dev_handle_trim(h2dev_handle_t h);
+/* High-water mark of the live bytes (blocks handed out by the handle's
+ * cache) since the handle was created or the mark last reset; reset != 0
+ * restarts it from the current live bytes.  No reference counterpart
+ * (memory planning for resident systems). */
+int h2dev_handle_memory_peak(h2dev_handle_t h, int64_t* peak_live_bytes, int reset);
 /* Handle options (apply to solvers created afterwards on this handle).
  * H2DEV_OPT_BASIS: 0 (default) forms fixed-rank orthogonal bases from the
  * Gram matrix of the far samples with a pivoted Cholesky (same pivots and R

@@ -86,6 +86,7 @@ SIGNATURES = {
     "h2dev_autotune_report": (C.c_int, [_vp, _i64, _vp, _vp, _vp, _i64p]),
     "h2dev_handle_memory": (C.c_int, [_vp, _i64p, _i64p]),
     "h2dev_handle_trim": (C.c_int, [_vp]),
+    "h2dev_handle_memory_peak": (C.c_int, [_vp, _i64p, C.c_int]),
     "h2dev_batched_gemm_device": (C.c_int, [_vp, C.c_int, _i64, _i64, _i64, _i64, _i64, C.c_int, C.c_int, C.c_double,
                                             _vp, _i64, _i64, _vp, _i64, _i64, C.c_double, _vp, _i64, _i64]),
     "h2dev_probe_fma_peak": (C.c_int, [_vp, C.c_int, _dp]),

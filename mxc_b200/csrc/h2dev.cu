@@ -195,6 +195,7 @@ static void* cache_alloc(h2dev_handle_s* h, size_t cls) {
     it->second.pop_back();
     h->cached_bytes -= cls;
     h->live_bytes += cls;
+    h->peak_live_bytes = std::max(h->peak_live_bytes, h->live_bytes);
     return p;
   }
   void* p = nullptr;
@@ -206,6 +207,7 @@ static void* cache_alloc(h2dev_handle_s* h, size_t cls) {
   }
   ck(e, "cudaMalloc");
   h->live_bytes += cls;
+  h->peak_live_bytes = std::max(h->peak_live_bytes, h->live_bytes);
   return p;
 }
 
@@ -2830,6 +2832,15 @@ int h2dev_handle_memory(h2dev_handle_t h, int64_t* live_bytes, int64_t* cached_b
   require(h != nullptr, "null handle");
   if (live_bytes) *live_bytes = (int64_t)h->live_bytes;
   if (cached_bytes) *cached_bytes = (int64_t)h->cached_bytes;
+  return H2DEV_OK;
+  H2_API_END
+}
+
+int h2dev_handle_memory_peak(h2dev_handle_t h, int64_t* peak_live_bytes, int reset) {
+  H2_API_BEGIN
+  require(h != nullptr && peak_live_bytes != nullptr, "null argument");
+  *peak_live_bytes = (int64_t)h->peak_live_bytes;
+  if (reset) h->peak_live_bytes = h->live_bytes;
   return H2DEV_OK;
   H2_API_END
 }

@@ -77,6 +77,7 @@ struct h2dev_handle_s {
   std::unordered_map<size_t, std::vector<void*>> cache;
   size_t cached_bytes = 0;
   size_t live_bytes = 0;  // blocks handed out (solvers, plans, temporaries)
+  size_t peak_live_bytes = 0;  // high-water mark of live_bytes since the last reset
   std::vector<ProfRec> recs;
   std::vector<cudaEvent_t> pool;
   cudaEvent_t t0 = nullptr, t1 = nullptr;

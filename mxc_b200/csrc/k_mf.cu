@@ -15,10 +15,10 @@
 // (row-contiguous, so each is read by a broadcast vector load), then every
 // thread evaluates its rows against the 32 columns and updates its
 // accumulators.  FP64 throughout, one reciprocal square root per pair
-// (rsqrt_newton: an FP32 seed refined by two FP64 Newton steps, about 1 ulp;
-// the whole entry is a few ulp from the reference's std::hypot form); the
-// summation order is fixed by the plan, so results are deterministic.  Bound: FP64 FMA throughput (2 NR
-// multiply-adds plus one kernel evaluation per pair), not HBM.
+// (about 1 ulp; the whole entry is a few ulp from the reference's std::hypot
+// form); the summation order is fixed by the plan, so results are
+// deterministic.  Bound: FP64 FMA throughput (2 NR multiply-adds plus one
+// kernel evaluation per pair), not HBM.
 #include "common.cuh"
 #include "kernels.h"
 

@@ -76,6 +76,10 @@ class SystemSpec:
     leaf: int = 256
     precision: int = L.FP32  # preconditioner precision; the operator is FP64
     device: int = 0
+    # Operator near blocks and couplings stored in HBM, or evaluated inside
+    # each matvec (H2DEV_OPT_MATRIX_FREE): a fraction of the memory, slower
+    # matvecs; lets more large systems stay resident under one budget.
+    matrix_free: bool = False
 
 
 class ResidentSystem:
@@ -83,12 +87,15 @@ class ResidentSystem:
 
     # Device bytes per body of a built system (operator at eps 1e-8 and an
     # FP32 rank-100 preconditioner held about 190 KB per body at 8,192 to
-    # 262,144 bodies): the admission estimate before a first build.
+    # 262,144 bodies; with a matrix-free operator the preconditioner is most
+    # of it): the admission estimate before a first build.
     BYTES_PER_BODY_ESTIMATE = 256 * 1024
+    BYTES_PER_BODY_ESTIMATE_MATRIX_FREE = 128 * 1024
 
     @classmethod
     def estimate_footprint(cls, spec: SystemSpec) -> int:
-        return int(cls.BYTES_PER_BODY_ESTIMATE * spec.points.shape[0])
+        per = cls.BYTES_PER_BODY_ESTIMATE_MATRIX_FREE if spec.matrix_free else cls.BYTES_PER_BODY_ESTIMATE
+        return int(per * spec.points.shape[0])
 
     def __init__(self, spec: SystemSpec, max_batch: int, warm: bool = True):
         self.spec = spec
@@ -100,8 +107,12 @@ class ResidentSystem:
         self.bodies = np.ascontiguousarray(spec.points, dtype=np.float64).copy()
         self.tree = build_tree(self.bodies, levels)
         ops = spec.op_samples or spec.samples
-        self.A = H2MatrixSolver(self.handle, spec.kernel, spec.op_eps, spec.rank, 0, self.tree, spec.theta,
-                                self.bodies, samples=ops, precision=L.FP64)
+        self.handle.set_option(L.OPT_MATRIX_FREE, 1 if spec.matrix_free else 0)
+        try:
+            self.A = H2MatrixSolver(self.handle, spec.kernel, spec.op_eps, spec.rank, 0, self.tree, spec.theta,
+                                    self.bodies, samples=ops, precision=L.FP64)
+        finally:
+            self.handle.set_option(L.OPT_MATRIX_FREE, 0)
         self.M = H2MatrixSolver(self.handle, spec.kernel, 0.0, spec.rank, 0, self.tree, spec.theta, self.bodies,
                                 samples=spec.samples, precision=spec.precision)
         self.M.factorizeM()

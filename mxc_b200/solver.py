@@ -144,6 +144,12 @@ class Handle:
         L.check(L.lib().h2dev_handle_memory(self.h, C.byref(live), C.byref(cached)), "h2dev_handle_memory")
         return live.value, cached.value
 
+    def memory_peak(self, reset: bool = False) -> int:
+        """High-water mark of the live bytes since creation or the last reset."""
+        v = C.c_int64()
+        L.check(L.lib().h2dev_handle_memory_peak(self.h, C.byref(v), 1 if reset else 0), "h2dev_handle_memory_peak")
+        return v.value
+
     def trim(self) -> None:
         """Return the handle's cached device blocks to the driver."""
         L.check(L.lib().h2dev_handle_trim(self.h), "h2dev_handle_trim")
