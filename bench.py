@@ -84,10 +84,16 @@ def parse():
     ap.add_argument("--c3-fp64-n", type=int, default=524288,
                     help="bodies of the sub-run's mixed-vs-FP64 comparison (the FP64 preconditioner does not fit "
                          "in HBM at 1,048,576; 0: skip)")
-    ap.add_argument("--serving-requests", type=int, default=60,
+    ap.add_argument("--c5-n", type=int, default=2097152,
+                    help="bodies of the scale-up sub-run (unit-sphere surface, Yukawa, theta 3, rank 160, BF16 "
+                         "substitution; halved until it fits in HBM; 0: skip)")
+    ap.add_argument("--c5-singularity", type=float, default=1e-6,
+                    help="diagonal 1/s of the scale-up sub-run's kernel")
+    ap.add_argument("--c5-outer", type=int, default=20, help="GMRES restart limit of the scale-up sub-run")
+    ap.add_argument("--serving-requests", type=int, default=48,
                     help="requests per arrival rate of the serving phase (0: skip); Poisson arrivals over resident "
                          "systems")
-    ap.add_argument("--serving-rates", default="4,8,16,200",
+    ap.add_argument("--serving-rates", default="3,4,6,8,200",
                     help="mean arrival rates swept, requests / s (200: the serving configuration's offered load)")
     ap.add_argument("--serving-systems",
                     default="8192c,8192m,32768c,32768m,131072c,131072m,262144c:mf,262144m:mf",
@@ -468,6 +474,114 @@ def run_c3(a, h) -> dict:
     return out
 
 
+def run_c5(a, h) -> dict:
+    """Scale-up configuration as a sub-run: bodies uniform on the unit
+    sphere's surface (seed 999), Yukawa exp(-r)/r with diagonal 1/s
+    (--c5-singularity, 1e-6: the surface's kernel row sums reach ~1e6, and
+    with diagonal 1e4 GMRES stagnates near 1e-3 at N = 2,097,152, measured),
+    theta 3, leaf 256, a matrix-free FP64 operator (eps 1e-8, sketch:
+    nearest three levels plus 6000 strided farther bodies), an FP32
+    preconditioner of rank 160 / 6000 samples whose substitution streams BF16
+    blocks with one power-of-two scale each (FP32 accumulation), FP64 GMRES to
+    1e-10 for 8 right-hand sides; one warm-up and one timed step with the
+    BF16 substitution and one with the FP32 substitution (the ablation).
+    Starts at --c5-n bodies and halves while the preconditioner does not fit
+    in HBM."""
+    import numpy as np
+    import torch
+
+    import mxc_b200 as m
+    from mxc_b200 import serving as S
+
+    s_c5, alpha, theta, leaf, rank, samples, nrhs = a.c5_singularity, 1.0, 3.0, 256, 160, 6000, 8
+    k = m.Yukawa3D(s_c5, alpha)
+    n = a.c5_n
+    tried = []
+    while n >= 65536:
+        h.trim()
+        h.memory_peak(reset=True)
+        L = m.levels_for(n, leaf)
+        b = S.unit_sphere_points(n, seed=999)
+        t = m.build_tree(b, L)
+        h.set_option(m._lib.OPT_SAMPLING, m._lib.SAMPLING_SKETCH)
+        h.set_option(m._lib.OPT_MATRIX_FREE, 1)
+        t0 = time.time()
+        try:
+            A = m.H2MatrixSolver(h, k, 1e-8, rank, 0, t, theta, b, samples=samples, precision=m.FP64)
+            h.synchronize()
+        finally:
+            h.set_option(m._lib.OPT_SAMPLING, m._lib.SAMPLING_STRIDED)
+            h.set_option(m._lib.OPT_MATRIX_FREE, 0)
+        op_s = time.time() - t0
+        Xt = np.random.default_rng(20261203).random((n, nrhs))
+        B = np.asfortranarray(m.dense_matvec(h, k, b, np.asfortranarray(Xt)))
+        dB = torch.from_numpy(B.T.copy()).cuda()
+        dX = torch.zeros_like(dB)
+        torch.cuda.synchronize()
+
+        def one(bf16, verify=True):
+            dX.zero_()
+            torch.cuda.synchronize()
+            h.timer_start()
+            h.set_option(m._lib.OPT_PRECOND_BF16, 1 if bf16 else 0)
+            try:
+                M = m.H2MatrixSolver(h, k, 0.0, rank, 0, t, theta, b, samples=samples, precision=m.FP32)
+            finally:
+                h.set_option(m._lib.OPT_PRECOND_BF16, 0)
+            tb = h.timer_stop()
+            h.timer_start()
+            M.factorizeM()
+            tf = h.timer_stop()
+            h.timer_start()
+            rc, resid, iters = A.gmres_device(M, a.tol, dX.data_ptr(), dB.data_ptr(), nrhs, n, a.inner, a.c5_outer,
+                                              True)
+            ts = h.timer_stop()
+            M.close()
+            r = {"build_ms": tb, "factor_ms": tf, "solve_ms": ts, "total_ms": tb + tf + ts, "converged": rc == 0,
+                 "cycles": [int(v) for v in iters],
+                 "h2_resid_max": float(max(resid[int(iters[c]), c] for c in range(nrhs)))}
+            if not verify:
+                return r, None
+            X = np.asfortranarray(dX.cpu().numpy().T)
+            R = m.dense_matvec(h, k, b, X)
+            r["dense_resid_max"] = float(max(np.linalg.norm(B[:, c] - R[:, c]) / np.linalg.norm(B[:, c])
+                                             for c in range(nrhs)))
+            r["x_true_err_max"] = float(max(np.linalg.norm(X[:, c] - Xt[:, c]) / np.linalg.norm(Xt[:, c])
+                                            for c in range(nrhs)))
+            return r, X
+
+        try:
+            one(True, verify=False)
+            rb, Xb = one(True)
+            rf, Xf = one(False)
+        except m._lib.H2DevError as e:
+            A.close()
+            del dB, dX
+            if e.code != 3:
+                raise
+            tried.append({"n": n, "unavailable": "out of device memory: %s" % e})
+            log("c5 at N=%d does not fit: %s" % (n, e))
+            n //= 2
+            continue
+        A.close()
+        del dB, dX
+        h.trim()
+        out = {"workload": "N=%d uniform on the unit sphere surface (seed 999), Yukawa exp(-r)/r diag 1/s s=%g, "
+                           "theta=%g, leaf %d, operator eps 1e-8 matrix-free (sketch: nearest three levels' far "
+                           "bodies + %d strided), FP32 preconditioner rank %d / %d samples with BF16 per-block-"
+                           "scaled substitution, FP64 GMRES(%d) to %g, nrhs=%d"
+                           % (n, s_c5, theta, leaf, samples, rank, samples, a.inner, a.tol, nrhs),
+               "n": n, "operator_build_s": op_s, "bf16_substitution": rb, "fp32_substitution": rf,
+               "x_bf16_vs_fp32_rel_max": float(max(np.linalg.norm(Xb[:, c] - Xf[:, c]) / np.linalg.norm(Xf[:, c])
+                                                   for c in range(nrhs))),
+               "value": n * nrhs / (rb["total_ms"] / 1e3), "unit": UNIT,
+               "peak_device_gb": h.memory_peak() / 1e9, "larger_sizes_tried": tried}
+        log("c5 at N=%d: BF16 %.1f ms (cycles %s), FP32 %.1f ms, dense residual %.2e"
+            % (n, rb["total_ms"], rb["cycles"], rf["total_ms"], rb["dense_resid_max"]))
+        return out
+    return {"unavailable": "no size from %d down to 65536 fits" % a.c5_n, "larger_sizes_tried": tried}
+
+
 def run_ours(a):
     import numpy as np
     import torch
@@ -818,6 +932,16 @@ def run_ours(a):
         h.trim()
         torch.cuda.empty_cache()
 
+    c5 = None
+    if a.c5_n > 0 and rank == 0:
+        try:
+            c5 = run_c5(a, h)
+        except Exception as e:
+            c5 = {"error": "%s: %s" % (type(e).__name__, e)}
+            log("c5 failed: %s" % c5["error"])
+        h.trim()
+        torch.cuda.empty_cache()
+
     serving = None
     if a.serving_requests > 0:
         try:
@@ -874,6 +998,7 @@ def run_ours(a):
             "graph_solve": graph,
             "diag1": diag1,
             "uneven_batching_c3": c3,
+            "scale_up_c5": c5,
             "gpu_at_cpu_sample": small,
             "serving": serving,
             "cpu_baseline": cpu,

@@ -722,7 +722,13 @@ struct BfPlan {
   DVec<int2> d_tiles;
   int nr = 0;
   double flops = 0., bytes = 0.;
+  // Split tasks (as GemmPlan::split_tasks): partials in parts_buf, summed
+  // in order into the task's output by k_sum_parts.
+  DVec<float> parts_buf;
+  DVec<SumTask<float>> d_sums;
+  int nsums = 0, sum_maxmn = 0;
   void finalize() {
+    split();
     const int bm = bf16_rows_per_cta();
     tiles.clear();
     for (size_t t = 0; t < tasks.size(); t++)
@@ -731,9 +737,97 @@ struct BfPlan {
     d_ents.upload(ents);
     d_tiles.upload(tiles);
   }
+  // Plans with fewer 256-row tiles than about four CTAs per SM (the upper
+  // tree levels: few large boxes) cut their entries along k into pieces of
+  // a multiple of 32 columns and spread each task over several CTAs.
+  void split() {
+    double rowtiles = 0., total = 0.;
+    for (const auto& t : tasks) {
+      rowtiles += (t.m + 255) / 256;
+      for (int e = t.e0; e < t.e1; e++) total += (double)std::min(t.m, 256) * ents[e].k;
+    }
+    constexpr double kCtaTarget = 4. * 148.;
+    if (rowtiles >= kCtaTarget || tasks.empty()) return;
+    const double cap = std::max(total / kCtaTarget, 16384.);
+    std::vector<GemmTask<float>> out;
+    std::vector<BfEntry> cut;
+    std::vector<SumTask<float>> sums;
+    i64 scratch = 0;
+    std::vector<std::pair<size_t, i64>> scr;  // (first part index in out, scratch offset) per split task
+    for (const auto& t : tasks) {
+      const int mw = std::min(t.m, 256);
+      // pieces of this task's entries
+      std::vector<BfEntry> pcs;
+      for (int e = t.e0; e < t.e1; e++) {
+        const BfEntry& en = ents[e];
+        if (en.k <= 0) continue;
+        const int kc = std::max(32, (int)(cap / mw) / 32 * 32);
+        for (int k0 = 0; k0 < en.k; k0 += kc) {
+          BfEntry p = en;
+          p.A = en.A + (i64)k0 * en.lda;
+          p.B = en.B + k0;
+          p.k = std::min(kc, en.k - k0);
+          pcs.push_back(p);
+        }
+      }
+      double w = 0.;
+      for (const auto& p : pcs) w += (double)mw * p.k;
+      if (w <= cap || pcs.size() < 2 || t.m <= 0 || t.n <= 0) {
+        GemmTask<float> nt = t;
+        nt.e0 = (int)cut.size();
+        cut.insert(cut.end(), pcs.begin(), pcs.end());
+        nt.e1 = (int)cut.size();
+        out.push_back(nt);
+        continue;
+      }
+      const size_t first = out.size();
+      int parts = 0;
+      size_t q = 0;
+      while (q < pcs.size()) {
+        GemmTask<float> part = t;
+        part.e0 = (int)cut.size();
+        double wp = 0.;
+        while (q < pcs.size() && (wp == 0. || wp + (double)mw * pcs[q].k <= cap)) {
+          wp += (double)mw * pcs[q].k;
+          cut.push_back(pcs[q++]);
+        }
+        part.e1 = (int)cut.size();
+        part.beta = 0.f;
+        part.ldc = t.m;
+        part.C = nullptr;  // set once the scratch exists
+        out.push_back(part);
+        parts++;
+      }
+      SumTask<float> sm;
+      sm.dst = t.C;
+      sm.ldd = t.ldc;
+      sm.src = nullptr;
+      sm.m = t.m;
+      sm.n = t.n;
+      sm.parts = parts;
+      sm.beta = t.beta;
+      sums.push_back(sm);
+      scr.emplace_back(first, scratch);
+      scratch += (i64)parts * t.m * t.n;
+      sum_maxmn = std::max(sum_maxmn, t.m * t.n);
+      bytes += (double)(parts + 1) * t.m * t.n * sizeof(float);
+    }
+    if (sums.empty()) return;
+    parts_buf.alloc(scratch);
+    for (size_t i = 0; i < sums.size(); i++) {
+      const i64 mn = (i64)sums[i].m * sums[i].n;
+      sums[i].src = parts_buf.p + scr[i].second;
+      for (int p = 0; p < sums[i].parts; p++) out[scr[i].first + p].C = parts_buf.p + scr[i].second + p * mn;
+    }
+    tasks.swap(out);
+    ents.swap(cut);
+    nsums = (int)sums.size();
+    d_sums.upload(sums);
+  }
   void run(cudaStream_t st) const {
     Prof p("bf16_precond", flops, bytes, st);
     ck(launch_stream_bf16(nr, d_tasks.p, d_ents.p, d_tiles.p, (int)tiles.size(), st), "bf16_precond");
+    if (nsums) ck(launch_sum_parts<float>(d_sums.p, nsums, sum_maxmn, st), "sum_parts");
   }
 };
 

@@ -207,6 +207,8 @@ struct BfEntry {
   const float* scale;
 };
 cudaError_t launch_bf16_pack(const BfPackTask* d_tasks, int ntasks, cudaStream_t st);
+// 5-16 right-hand sides run on the BF16 tensor cores (k_stream_bf16_mma),
+// 1-4 on the FMA pipe.
 cudaError_t launch_stream_bf16(int nr, const GemmTask<float>* d_tasks, const BfEntry* d_ents, const int2* d_tiles,
                                int ntiles, cudaStream_t st);
 int bf16_rows_per_cta();

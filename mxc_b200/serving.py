@@ -62,6 +62,15 @@ def gaussian_mixture_points(n: int, ncomp: int = 32, seed: int = 0, sigma=(0.01,
     return np.ascontiguousarray(pts)
 
 
+def unit_sphere_points(n: int, seed: int = 0) -> np.ndarray:
+    """n points uniform on the unit sphere's surface (seeded): normalised
+    standard-normal 3-vectors (the scale-up configuration's inputs)."""
+    rng = np.random.default_rng(seed)
+    v = rng.standard_normal((n, 3))
+    v /= np.linalg.norm(v, axis=1)[:, None]
+    return np.ascontiguousarray(v)
+
+
 @dataclass
 class SystemSpec:
     """What a resident system is built from (kept so an evicted system can
@@ -80,6 +89,10 @@ class SystemSpec:
     # each matvec (H2DEV_OPT_MATRIX_FREE): a fraction of the memory, slower
     # matvecs; lets more large systems stay resident under one budget.
     matrix_free: bool = False
+    # Each batched solve as one CUDA graph (H2DEV_OPT_GRAPH_SOLVE), captured
+    # at the warm-up and replayed: no host round trip per Arnoldi step, so
+    # systems served by concurrent workers do not wait on each other's syncs.
+    graph_solve: bool = True
 
 
 class ResidentSystem:
@@ -97,7 +110,8 @@ class ResidentSystem:
         per = cls.BYTES_PER_BODY_ESTIMATE_MATRIX_FREE if spec.matrix_free else cls.BYTES_PER_BODY_ESTIMATE
         return int(per * spec.points.shape[0])
 
-    def __init__(self, spec: SystemSpec, max_batch: int, warm: bool = True):
+    def __init__(self, spec: SystemSpec, max_batch: int, warm: bool = True, inner: int = 10, outer: int = 50,
+                 tol: float = 1e-10):
         self.spec = spec
         self.handle = Handle(spec.device)
         n = spec.points.shape[0]
@@ -121,11 +135,14 @@ class ResidentSystem:
         self.handle.trim()
         self.n = n
         self.max_batch = max_batch
+        self.handle.set_option(L.OPT_GRAPH_SOLVE, 1 if spec.graph_solve else 0)
         if warm:
-            # Builds the batch-width plans once (and measures them in the footprint).
+            # Builds the batch-width plans once, and with graph solves captures
+            # the solve at the serving shape and tolerance (all measured in the
+            # footprint).
             B = np.ones((n, max_batch), order="F")
             X = np.zeros((n, max_batch), order="F")
-            self.A.solveGMRES(1e-6, self.M, X, B, 2, 1)
+            self.A.solveGMRES(tol, self.M, X, B, inner, outer, early_exit=True)
         self.handle.synchronize()
         live, cached = self.handle.memory()
         self.footprint = live + cached
@@ -178,8 +195,11 @@ class Server:
         self._t0 = time.perf_counter()
         # build_system(spec, max_batch) -> an object with n, footprint, solve(B, tol, inner, outer) and
         # close(); ResidentSystem by default (other builders serve host-side tests of the scheduler).
-        builder = build_system or ResidentSystem
-        self._builder: Callable[[SystemSpec], ResidentSystem] = lambda s: builder(s, self.max_batch)
+        if build_system is None:
+            self._builder: Callable[[SystemSpec], ResidentSystem] = lambda s: ResidentSystem(
+                s, self.max_batch, inner=self.inner, outer=self.outer)
+        else:
+            self._builder = lambda s: build_system(s, self.max_batch)
         # Footprint assumed for a system never built before: ResidentSystem's
         # per-body estimate by default; with another builder, the given
         # estimate or none (then room is made once the build is measured).
