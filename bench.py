@@ -484,7 +484,8 @@ def run_c5(a, h) -> dict:
     preconditioner of rank 160 / 6000 samples whose substitution streams BF16
     blocks with one power-of-two scale each (FP32 accumulation), FP64 GMRES to
     1e-10 for 8 right-hand sides; one warm-up and one timed step with the
-    BF16 substitution and one with the FP32 substitution (the ablation).
+    BF16 substitution, then the same with the FP32 substitution (the
+    ablation).
     Starts at --c5-n bodies and halves while the preconditioner does not fit
     in HBM."""
     import numpy as np
@@ -553,6 +554,7 @@ def run_c5(a, h) -> dict:
         try:
             one(True, verify=False)
             rb, Xb = one(True)
+            one(False, verify=False)
             rf, Xf = one(False)
         except m._lib.H2DevError as e:
             A.close()

@@ -4,11 +4,13 @@
 //
 // Only the upper-triangle 64 x 64 tiles of each G are computed; each
 // off-diagonal tile is also written transposed.  One CTA (4 warps, each a
-// 32 x 32 quadrant as 4 x 4 m8n8k4 fragments) owns one tile.  The k (sample)
-// dimension is streamed in 16-row slabs through a 3-slot cp.async ring: the
-// slab holds the tile's 64 (diagonal tile) or 128 columns of X, each column
-// 16 consecutive samples padded to 20 doubles so the fragment loads of a
-// half-warp (4 columns x 4 samples) hit 16 distinct bank pairs.
+// 32 x 32 quadrant as 2 x 4 mma.sync m16n8k16 FP64 fragments) owns one tile.
+// The k (sample) dimension is streamed in 16-row slabs through a 3-slot
+// cp.async ring: the slab holds the tile's 64 (diagonal tile) or 128 columns
+// of X, each column 16 consecutive samples padded to 18 doubles.  MMA k index
+// t + 4j is slab sample 4t + j, so a lane's fragment values of one row (or
+// column) are 4 consecutive samples: two 16-byte loads, which the 18-double
+// column stride puts on distinct banks for each quarter warp.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -18,7 +20,7 @@ namespace h2b {
 
 namespace {
 
-constexpr int GR_T = 64, GR_KS = 16, GR_CS = GR_KS + 4, GR_ST = 3, GR_NT = 128;
+constexpr int GR_T = 64, GR_KS = 16, GR_CS = GR_KS + 2, GR_ST = 3, GR_NT = 128;
 constexpr int GR_KP = GR_KS / 2;  // 16-byte pairs per staged column
 constexpr int GR_SLOT = 2 * GR_T * GR_CS;  // doubles per ring slot (128 columns)
 constexpr int GR_SMEM = GR_ST * GR_SLOT * 8;
@@ -41,6 +43,15 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
                : "+d"(d[0]), "+d"(d[1])
                : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void dmma16(double (&d)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+        "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
 }  // namespace
@@ -83,53 +94,73 @@ __global__ void __launch_bounds__(GR_NT, 3) k_gram(const GramTask* __restrict__ 
     gcommit();
   };
 
-  double acc[4][4][2];
+  double acc[2][4][4];
 #pragma unroll
-  for (int i = 0; i < 4; i++)
+  for (int i = 0; i < 2; i++)
 #pragma unroll
-    for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.;
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[i][j][q] = 0.;
 
 #pragma unroll
   for (int s = 0; s < GR_ST - 1; s++) produce(s, s);
-  const int fr = lane >> 2, fk = lane & 3;  // fragment row / column within m8n8k4
+  const int g8 = lane >> 2, t4 = lane & 3;
   for (int sl = 0; sl < nslab; sl++) {
     gwait<GR_ST - 2>();
     __syncthreads();
     produce(sl + GR_ST - 1, (sl + GR_ST - 1) % GR_ST);
     const double* base = gsm + (size_t)(sl % GR_ST) * GR_SLOT;
-    const double* as = base + (wm * 32 + fr) * GR_CS + fk;
-    const double* bs = base + ((diag ? 0 : GR_T) + wn * 32 + fr) * GR_CS + fk;
+    // A row (G row) c0 + wm 32 + 16 i + g8 + 8 h, samples 4 t4 .. 4 t4 + 3:
+    // a[2 j + h] is sample 4 t4 + j (MMA row g8 + 8 h, MMA k t4 + 4 j).
+    const double* as = base + (wm * 32 + g8) * GR_CS + 4 * t4;
+    const double* bs = base + ((diag ? 0 : GR_T) + wn * 32 + g8) * GR_CS + 4 * t4;
+    double a[2][8], b[4][4];
 #pragma unroll
-    for (int ks = 0; ks < GR_KS; ks += 4) {
-      double a[4], b[4];
+    for (int i = 0; i < 2; i++)
 #pragma unroll
-      for (int i = 0; i < 4; i++) a[i] = as[i * 8 * GR_CS + ks];
+      for (int h = 0; h < 2; h++) {
+        const double* p = as + (16 * i + 8 * h) * GR_CS;
+        const double2 x0 = *reinterpret_cast<const double2*>(p);
+        const double2 x1 = *reinterpret_cast<const double2*>(p + 2);
+        a[i][h] = x0.x;
+        a[i][2 + h] = x0.y;
+        a[i][4 + h] = x1.x;
+        a[i][6 + h] = x1.y;
+      }
 #pragma unroll
-      for (int j = 0; j < 4; j++) b[j] = bs[j * 8 * GR_CS + ks];
-#pragma unroll
-      for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) dmma(acc[i][j], a[i], b[j]);
+    for (int j = 0; j < 4; j++) {
+      const double* p = bs + 8 * j * GR_CS;
+      const double2 x0 = *reinterpret_cast<const double2*>(p);
+      const double2 x1 = *reinterpret_cast<const double2*>(p + 2);
+      b[j][0] = x0.x;
+      b[j][1] = x0.y;
+      b[j][2] = x1.x;
+      b[j][3] = x1.y;
     }
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 4; j++) dmma16(acc[i][j], a[i], b[j]);
   }
   gwait<0>();
 
-  // D fragment of m8n8k4: lane holds row lane >> 2, columns 2 (lane & 3) + {0, 1}.
+  // D fragment of m16n8: c[2 h + q] is row g8 + 8 h, column 2 t4 + q.
 #pragma unroll
-  for (int i = 0; i < 4; i++) {
-    const int r = c0 + wm * 32 + i * 8 + fr;
+  for (int i = 0; i < 2; i++)
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
+    for (int h = 0; h < 2; h++) {
+      const int r = c0 + wm * 32 + 16 * i + g8 + 8 * h;
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const int c = c1 + wn * 32 + j * 8 + 2 * fk + h;
-        if (r < t.M && c < t.M) {
-          t.G[(i64)r + (i64)c * t.ldg] = acc[i][j][h];
-          if (!diag) t.G[(i64)c + (i64)r * t.ldg] = acc[i][j][h];
+      for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+          const int c = c1 + wn * 32 + 8 * j + 2 * t4 + q;
+          if (r < t.M && c < t.M) {
+            t.G[(i64)r + (i64)c * t.ldg] = acc[i][j][2 * h + q];
+            if (!diag) t.G[(i64)c + (i64)r * t.ldg] = acc[i][j][2 * h + q];
+          }
         }
-      }
     }
-  }
 }
 
 int gram_tile() { return GR_T; }
