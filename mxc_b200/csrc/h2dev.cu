@@ -649,7 +649,9 @@ struct MfPlan {
   int nr = 0;
   const char* name = "mf_apply";
   double flops = 0., bytes = 0.;
-  // Autotuned rows per thread: variant 0 = 2 rows, 1 = 1 row per thread.
+  // Autotuned rows per thread (at most 4 right-hand sides): variant 0 = 2
+  // rows, 1 = 1 row per thread; with more, variant 1 is the tensor-core
+  // kernel over 32-row tiles.
   std::vector<int2> tiles1;
   DVec<int2> d_tiles1;
   std::string tkey;
@@ -672,7 +674,7 @@ struct MfPlan {
     bytes += (24. + 8. * nr) * k;
   }
   void finalize() {
-    const int bm = mf_rows_per_cta(2), bm1 = mf_rows_per_cta(1);
+    const int bm = mf_rows_per_cta(2), bm1 = nr > 4 ? mf_dmma_rows_per_cta() : mf_rows_per_cta(1);
     tiles.clear();
     tiles1.clear();
     double rows = 0.;

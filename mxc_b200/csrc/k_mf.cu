@@ -108,7 +108,10 @@ __global__ void __launch_bounds__(MF_NT, RPT == 1 ? 8 : 4)
 // Tensor-core variant for 5-16 right-hand sides: the kernel block is
 // generated straight into mma.sync m16n8k16 FP64 fragments and multiplied
 // by the right-hand sides on the FP64 tensor cores; no shared memory and
-// no block barriers.  Each warp owns 32 rows of a task (its lane holds rows
+// no block barriers.  Four warps per CTA share the column bodies and
+// right-hand sides through L1 (one-warp CTAs, which idle no warp beside
+// short tasks, measured 5-10% slower).  Each warp owns 32 rows of a task
+// (its lane holds rows
 // g, g + 8, g + 16, g + 24 with their bodies in registers) and walks the
 // task's entries in 16-column steps: a lane evaluates K for its 4 rows x 4
 // columns (t, t + 4, t + 8, t + 12 of the step; bodies and right-hand sides
@@ -198,6 +201,7 @@ __global__ void __launch_bounds__(32 * MFD_WARPS) k_mf_dmma(KernelParams kp, con
 }  // namespace
 
 int mf_rows_per_cta(int rpt) { return MF_NT * rpt; }
+int mf_dmma_rows_per_cta() { return 32 * MFD_WARPS; }
 
 template <int KIND, int RPT>
 static cudaError_t mf_go(const KernelParams& kp, int nr, const MfTask* d_tasks, const MfEntry* d_ents,
@@ -229,7 +233,7 @@ static cudaError_t mf_dmma_go(const KernelParams& kp, int nr, const MfTask* d_ta
 template <int RPT>
 static cudaError_t mf_kind(const KernelParams& kp, int nr, const MfTask* d_tasks, const MfEntry* d_ents,
                            const int2* d_tiles, int ntiles, cudaStream_t st) {
-  if (RPT == 1 && nr > 4) {
+  if (RPT == 1 && nr > 4) {  // tiles of mf_dmma_rows_per_cta() rows
     if (kp.kind == KERNEL_LAPLACE) return mf_dmma_go<KERNEL_LAPLACE>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
     if (kp.kind == KERNEL_YUKAWA) return mf_dmma_go<KERNEL_YUKAWA>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
     return mf_dmma_go<KERNEL_QUADRATIC>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);

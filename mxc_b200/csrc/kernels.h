@@ -162,8 +162,9 @@ int dgemm_tile();
 // entries of alpha K(pts_task, pts_entry) B (m x nr output, ld ldc; B k x nr,
 // ld ldb; points xyz-interleaved).  tiles: {task, block of
 // mf_rows_per_cta(rpt) rows}; nr <= 16.  With rpt 1 and nr > 4 the block is
-// generated into FP64 tensor-core fragments (k_mf_dmma), otherwise each
-// thread accumulates rpt rows on the FP64 FMA pipe.
+// generated into FP64 tensor-core fragments (k_mf_dmma, tiles of
+// mf_dmma_rows_per_cta() rows), otherwise each thread accumulates rpt rows
+// on the FP64 FMA pipe.
 struct MfTask {
   const double* pts;
   int m;
@@ -183,6 +184,7 @@ cudaError_t launch_mf_apply(const KernelParams& kp, int nr, int rpt, const MfTas
                             const int2* d_tiles, int ntiles, cudaStream_t st);
 // Rows of a task one CTA covers with rpt (1 or 2) rows per thread.
 int mf_rows_per_cta(int rpt);
+int mf_dmma_rows_per_cta();
 
 // BF16 substitution blocks (k_bf16.cu).  Pack: dst (m x k, ld ldd, a
 // multiple of 8) = bf16(src / s), s = 2^ceil(log2 max |src|) written to
