@@ -310,6 +310,21 @@ static void check_tc(h2dev_handle_s* h) {
   }
 }
 
+// Largest row count of a generation task list (one CTA per 256 rows).
+static i64 gen_max_rows(const std::vector<GenTask>& gt) {
+  i64 m = 0;
+  for (const auto& t : gt) m = std::max<i64>(m, t.m);
+  return m;
+}
+
+// The current handle's error word for the bulk-copy staging of the
+// generation kernel (checked with the other mbarrier-pipelined kernels').
+static int* gen_err() {
+  if (!g_cur) return nullptr;
+  g_cur->tc_pending = true;
+  return g_cur->d_tc_err;
+}
+
 // ------------------------------------------------------------------ autotuner
 // The first time a plan of a given shape bucket runs on a handle (outside
 // any stream capture), every launch variant it admits is timed on the
@@ -1115,7 +1130,9 @@ class Solver : public SolverBase {
           Prof pf("gen_near_blocks", 0., (double)lv.aoff[nA] * sizeof(T));
           // FP64 blocks use the std::hypot-exact distance (bit-exact with the
           // reference); FP32 blocks the rsqrt path, rounded to FP32 anyway.
-          ck(launch_gen_blocks<T>(kp, dg.p, (int)gt.size(), 1, lv.A.p, st(), sizeof(T) == 4 ? 1 : 0), "gen near");
+          ck(launch_gen_blocks<T>(kp, dg.p, (int)gt.size(), gen_max_rows(gt), lv.A.p, st(), sizeof(T) == 4 ? 1 : 0,
+                                  gen_err()),
+             "gen near");
         }
       } else {
         CopyPlan<double> pcopy;
@@ -1351,7 +1368,9 @@ class Solver : public SolverBase {
       dg.upload(gt);
       {
         Prof pf("gen_couplings", 0., (double)lv.coff[nC] * sizeof(T));
-        ck(launch_gen_blocks<T>(kp, dg.p, (int)gt.size(), 1, kout, st(), sizeof(T) == 4 ? 1 : 0), "gen couplings");
+        ck(launch_gen_blocks<T>(kp, dg.p, (int)gt.size(), gen_max_rows(gt), kout, st(), sizeof(T) == 4 ? 1 : 0,
+                                gen_err()),
+           "gen couplings");
       }
       if (orth) {
         DVec<T> T1;
@@ -1445,7 +1464,8 @@ class Solver : public SolverBase {
       dg.upload(gt);
       {
         Prof pf("gen_samples", 0., 8. * o);
-        ck(launch_gen_blocks<double>(kp, dg.p, (int)gt.size(), 4, XF.p, st(), 1), "gen samples");
+        ck(launch_gen_blocks<double>(kp, dg.p, (int)gt.size(), gen_max_rows(gt), XF.p, st(), 1, gen_err()),
+           "gen samples");
       }
       DVec<GramTask> dgm;
       DVec<int4> dtl;
@@ -3172,8 +3192,7 @@ int h2dev_gen_block(h2dev_handle_t h, int kernel, double singularity, double alp
   gt[0].ld = m;
   DVec<GenTask> dg;
   dg.upload(gt);
-  int chunks = (int)std::min<int64_t>(4096, (m * n + 65535) / 65536);
-  ck(launch_gen_blocks<double>(kp, dg.p, 1, chunks, dout.p, h->stream), "gen");
+  ck(launch_gen_blocks<double>(kp, dg.p, 1, m, dout.p, h->stream, 0, gen_err()), "gen");
   ck(cudaStreamSynchronize(h->stream), "sync");
   ck(cudaMemcpy(out, dout.p, sizeof(double) * m * n, cudaMemcpyDeviceToHost), "D2H");
   return H2DEV_OK;

@@ -6,67 +6,141 @@
 
 namespace h2b {
 
-// Column-major blocks K(bi[r], bj[c]); grid.x = task, grid.y = chunk of
-// the block's elements.  Consecutive threads write consecutive rows; a
-// thread finds its first (row, column) by one 32-bit division and then
-// steps by the block size without dividing (blocks hold < 2^31 elements;
-// larger ones take the 64-bit path).
-template <typename T, bool FAST>
-__global__ void __launch_bounds__(256) k_gen_blocks(KernelParams kp, const GenTask* __restrict__ tasks, T* __restrict__ out) {
+// Column-major blocks K(bi[r], bj[c]); grid.x = task, grid.y = tile of 256
+// rows.  The task's column bodies are staged in shared memory 256 at a time
+// -- by one cp.async.bulk copy completing on an mbarrier when the tile starts
+// on a 16-byte boundary, by coalesced loads otherwise -- and every thread
+// keeps its row's body in registers, so each element costs one kernel
+// evaluation (kind fixed at compile time) and one store; consecutive threads
+// write consecutive rows of a column.  The wait on the bulk copy is bounded:
+// an expired wait sets *err and the CTA falls back to plain loads.
+constexpr int GEN_ROWS = 256, GEN_COLS = 256;
+constexpr long long GEN_WAIT_CYCLES = 2000000000LL;  // about one second
+
+template <int KIND>
+__device__ __forceinline__ double gen_exact(const KernelParams& kp, double dx, double dy, double dz) {
+  const double d = hypot3_exact(dx, dy, dz);
+  if (d == 0.) return kp.diag;
+  if constexpr (KIND == KERNEL_LAPLACE) return __ddiv_rn(1., d);
+  if constexpr (KIND == KERNEL_QUADRATIC) return __dadd_rn(__dmul_rn(d, d), kp.alpha);
+  return __ddiv_rn(exp(__dmul_rn(-kp.alpha, d)), d);
+}
+
+template <int KIND>
+__device__ __forceinline__ double gen_fast(const KernelParams& kp, double dx, double dy, double dz) {
+  const double r2 = dx * dx + dy * dy + dz * dz;
+  if (r2 == 0.) return kp.diag;
+  if constexpr (KIND == KERNEL_QUADRATIC) return r2 + kp.alpha;
+  const double inv = rsqrt(r2);
+  if constexpr (KIND == KERNEL_LAPLACE) return inv;
+  return exp(-kp.alpha * (r2 * inv)) * inv;
+}
+
+template <typename T, bool FAST, int KIND>
+__global__ void __launch_bounds__(GEN_ROWS) k_gen_blocks(KernelParams kp, const GenTask* __restrict__ tasks,
+                                                         T* __restrict__ out, int* __restrict__ err) {
+  __shared__ __align__(16) double cpts[GEN_COLS * 3];
+  __shared__ __align__(8) uint64_t bar;
   const GenTask t = tasks[blockIdx.x];
-  const i64 total = (i64)t.m * t.n;
-  if (total == 0) return;
-  const i64 per = (total + gridDim.y - 1) / gridDim.y;
-  const i64 e0 = per * blockIdx.y, e1 = e0 + per < total ? e0 + per : total;
+  const int r0 = blockIdx.y * GEN_ROWS;
+  if (r0 >= t.m || t.n <= 0) return;
+  const int r = r0 + (int)threadIdx.x;
+  const bool live = r < t.m;
+  double px = 0., py = 0., pz = 0.;
+  if (live) {
+    px = t.bi[3 * (i64)r];
+    py = t.bi[3 * (i64)r + 1];
+    pz = t.bi[3 * (i64)r + 2];
+  }
+  const uint32_t bar_s = (uint32_t)__cvta_generic_to_shared(&bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar_s) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
   T* o = out + t.out_off;
-  auto value = [&](int r, int c) {
-    const double* a = t.bi + 3 * r;
-    const double* b = t.bj + 3 * c;
-    return FAST ? (T)kernel_fast(kp, a[0] - b[0], a[1] - b[1], a[2] - b[2])
-                : (T)kernel_exact(kp, a[0] - b[0], a[1] - b[1], a[2] - b[2]);
-  };
-  if (total < ((i64)1 << 31)) {
-    const int m = t.m, stride = (int)blockDim.x;
-    const int dq = stride / m, dr = stride - dq * m;
-    int e = (int)e0 + (int)threadIdx.x;
-    const int end = (int)e1;
-    if (e >= end) return;
-    int c = e / m, r = e - c * m;
-    for (; e < end; e += stride) {
-      o[r + (i64)c * t.ld] = value(r, c);
-      r += dr;
-      c += dq;
-      if (r >= m) {
-        r -= m;
-        c++;
+  uint32_t phase = 0;
+  bool bulk_ok = true;  // cleared for good after an expired wait
+  for (int c0 = 0; c0 < t.n; c0 += GEN_COLS) {
+    const int nc = min(GEN_COLS, t.n - c0);
+    const double* src = t.bj + 3 * (i64)c0;
+    const uint32_t bytes = (uint32_t)(24 * nc);
+    const bool bulk = bulk_ok && ((reinterpret_cast<uintptr_t>(src) & 15) == 0) && (bytes % 16 == 0);
+    __syncthreads();  // the previous chunk's readers are done with cpts
+    bool staged = false;
+    if (bulk) {
+      if (threadIdx.x == 0) {
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar_s), "r"(bytes) : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                (uint32_t)__cvta_generic_to_shared(cpts)),
+            "l"(src), "r"(bytes), "r"(bar_s)
+            : "memory");
+      }
+      uint32_t ok = 0;
+      const long long tw = clock64();
+      while (true) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok)
+            : "r"(bar_s), "r"(phase)
+            : "memory");
+        if (ok || clock64() - tw > GEN_WAIT_CYCLES) break;
+      }
+      phase ^= 1;
+      staged = __syncthreads_and((int)ok) != 0;
+      if (!staged) {
+        bulk_ok = false;
+        if (threadIdx.x == 0 && err) atomicExch(err, 1);
       }
     }
-    return;
-  }
-  for (i64 e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-    const int r = (int)(e % t.m), c = (int)(e / t.m);
-    o[r + (i64)c * t.ld] = value(r, c);
+    if (!staged) {
+      __syncthreads();
+      for (int i = threadIdx.x; i < 3 * nc; i += GEN_ROWS) cpts[i] = src[i];
+      __syncthreads();
+    }
+    if (live) {
+      T* oc = o + r + (i64)c0 * t.ld;
+#pragma unroll 4
+      for (int c = 0; c < nc; c++) {
+        const double dx = px - cpts[3 * c], dy = py - cpts[3 * c + 1], dz = pz - cpts[3 * c + 2];
+        oc[(i64)c * t.ld] = (T)(FAST ? gen_fast<KIND>(kp, dx, dy, dz) : gen_exact<KIND>(kp, dx, dy, dz));
+      }
+    }
   }
 }
 
+template <typename T, bool FAST>
+static void gen_launch(const KernelParams& kp, dim3 grid, const GenTask* d_tasks, T* out, int* err, cudaStream_t st) {
+  if (kp.kind == KERNEL_LAPLACE)
+    k_gen_blocks<T, FAST, KERNEL_LAPLACE><<<grid, GEN_ROWS, 0, st>>>(kp, d_tasks, out, err);
+  else if (kp.kind == KERNEL_YUKAWA)
+    k_gen_blocks<T, FAST, KERNEL_YUKAWA><<<grid, GEN_ROWS, 0, st>>>(kp, d_tasks, out, err);
+  else
+    k_gen_blocks<T, FAST, KERNEL_QUADRATIC><<<grid, GEN_ROWS, 0, st>>>(kp, d_tasks, out, err);
+}
+
 template <typename T>
-cudaError_t launch_gen_blocks(const KernelParams& kp, const GenTask* d_tasks, int ntasks, int chunks, T* out,
-                              cudaStream_t st, int fast) {
-  if (ntasks == 0) return cudaSuccess;
-  dim3 grid(ntasks, chunks < 1 ? 1 : chunks);
-  if (fast) {
-    note_launch();
-    k_gen_blocks<T, true><<<grid, 256, 0, st>>>(kp, d_tasks, out);
-  } else {
-    note_launch();
-    k_gen_blocks<T, false><<<grid, 256, 0, st>>>(kp, d_tasks, out);
-  }
+cudaError_t launch_gen_blocks(const KernelParams& kp, const GenTask* d_tasks, int ntasks, i64 max_m, T* out,
+                              cudaStream_t st, int fast, int* err) {
+  if (ntasks == 0 || max_m <= 0) return cudaSuccess;
+  const i64 ty = (max_m + GEN_ROWS - 1) / GEN_ROWS;
+  if (ty > 65535) return cudaErrorInvalidValue;
+  dim3 grid(ntasks, (unsigned)ty);
+  note_launch();
+  if (fast)
+    gen_launch<T, true>(kp, grid, d_tasks, out, err, st);
+  else
+    gen_launch<T, false>(kp, grid, d_tasks, out, err, st);
   return cudaGetLastError();
 }
-template cudaError_t launch_gen_blocks<double>(const KernelParams&, const GenTask*, int, int, double*, cudaStream_t,
-                                               int);
-template cudaError_t launch_gen_blocks<float>(const KernelParams&, const GenTask*, int, int, float*, cudaStream_t,
-                                              int);
+template cudaError_t launch_gen_blocks<double>(const KernelParams&, const GenTask*, int, i64, double*, cudaStream_t,
+                                               int, int*);
+template cudaError_t launch_gen_blocks<float>(const KernelParams&, const GenTask*, int, i64, float*, cudaStream_t,
+                                              int, int*);
 
 // Y = A_dense X for up to NR right-hand sides per pass.  Each thread owns a
 // row; columns stream through shared memory in tiles of 256 bodies.

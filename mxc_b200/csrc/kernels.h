@@ -16,9 +16,13 @@ struct GenTask {
   i64 out_off;  // element offset of the column-major m x n output
   i64 ld;
 };
+// max_m: the largest task row count (one CTA per 256 rows of a task); fast:
+// rsqrt of the squared distance instead of the std::hypot-exact form; err:
+// device int set if a CTA's bounded wait on its bulk copy expired (then the
+// CTA fell back to plain loads, and the result is still complete).
 template <typename T>
-cudaError_t launch_gen_blocks(const KernelParams& kp, const GenTask* d_tasks, int ntasks, int chunks, T* out,
-                              cudaStream_t st, int fast = 0);
+cudaError_t launch_gen_blocks(const KernelParams& kp, const GenTask* d_tasks, int ntasks, i64 max_m, T* out,
+                              cudaStream_t st, int fast = 0, int* err = nullptr);
 cudaError_t launch_dense_matvec(const KernelParams& kp, const double* bodies, i64 n, const double* X, i64 ldx,
                                 double* Y, i64 ldy, int nrhs, cudaStream_t st);
 
