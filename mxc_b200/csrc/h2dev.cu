@@ -12,6 +12,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <future>
 #include <thread>
 #include <type_traits>
 #include <vector>
@@ -1064,7 +1065,41 @@ class Solver : public SolverBase {
       lv.na_off.assign(lv.acol.size(), -1);
       lv.na_ld.assign(lv.acol.size(), 0);
     }
+    // Sample lists of every level, leaves first, on one background thread
+    // (each level's list is itself built by up to 8 threads), so that the
+    // host computes level l-1's lists while the device works on level l.
+    // The futures are taken (or, on an error, drained) before this returns.
+    std::thread ahead;
+    std::vector<std::promise<LevelSamples>> prom;
+    if (sampling_mode != 2) {
+      prom.resize(levels + 1);
+      sample_ahead.resize(levels + 1);
+      for (i64 l = 0; l <= levels; l++) sample_ahead[l] = prom[l].get_future();
+      ahead = std::thread([this, &prom, &ranges]() {
+        for (i64 l = levels; l >= 0; l--) {
+          try {
+            prom[l].set_value(level_samples(l, ranges));
+          } catch (...) {
+            prom[l].set_exception(std::current_exception());
+          }
+        }
+      });
+    }
+    struct Join {
+      std::thread& t;
+      std::vector<std::future<LevelSamples>>& f;
+      ~Join() {
+        if (t.joinable()) t.join();
+        f.clear();
+      }
+    } join{ahead, sample_ahead};
     for (i64 l = levels; l >= 0; l--) construct_level(l, ranges);
+    if (fix_rank) {
+      // The host-side rank rule must agree with the ranks the device chose
+      // (plans and offsets were sized from it).
+      for (i64 l = 0; l <= levels; l++)
+        if (L[l].d_ranks.n) require(L[l].d_ranks.download(st()) == L[l].ranks, "fixed-rank rule disagrees with the device");
+    }
     check_tc(h);
   }
 
@@ -1073,6 +1108,64 @@ class Solver : public SolverBase {
   }
 
   // h2matrix.cpp:72-249 for one level.
+  // Ranks of fixed-rank bases (epi >= 1), by the rule k_basis_finish
+  // applies on the device: min(K, M, floor(epi)) with K the box's sample
+  // rows (0 when K or M is 0).  Knowing them on the host spares the level a
+  // device-to-host synchronisation before its completion plans are built.
+  static std::vector<i64> fixed_rank_rule(const std::vector<i64>& dims, const std::vector<i64>& krows, double e) {
+    std::vector<i64> r(dims.size(), 0);
+    const i64 cap = (i64)std::floor(e);
+    for (size_t i = 0; i < dims.size(); i++) {
+      if (dims[i] == 0 || krows[i] == 0) continue;
+      r[i] = std::min(std::min(krows[i], dims[i]), cap);
+    }
+    return r;
+  }
+
+  // Far-sample index lists of one level (strided or level-geometric cap):
+  // every box's list concatenated in box order, and the per-box counts;
+  // host work that depends only on the tree, so build() computes all levels
+  // ahead on a background thread while the device constructs the levels
+  // below.
+  struct LevelSamples {
+    std::vector<int> sidx;
+    std::vector<i64> cnt;
+  };
+  std::vector<std::future<LevelSamples>> sample_ahead;
+
+  LevelSamples level_samples(i64 l, const std::vector<std::vector<std::pair<i64, i64>>>& ranges) const {
+    const i64 nodes = (i64)1 << l, g0 = nodes - 1;
+    LevelSamples out;
+    out.cnt.assign(nodes, 0);
+    const int nth = (int)std::max<i64>(1, std::min<i64>({8, (i64)std::thread::hardware_concurrency(), nodes / 16}));
+    std::vector<std::vector<int>> part(nth);
+    auto work = [&](int t) {
+      std::vector<int> tmp;
+      for (i64 i = nodes * t / nth; i < nodes * (t + 1) / nth; i++) {
+        if (sampling_mode == 1)
+          sample_far_list_geometric(ranges[g0 + i], gstart[g0 + i], samples, tmp);
+        else
+          sample_far_list(ranges[g0 + i], samples, tmp);
+        part[t].insert(part[t].end(), tmp.begin(), tmp.end());
+        out.cnt[i] = (i64)tmp.size();
+      }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < nth; t++) th.emplace_back(work, t);
+    work(0);
+    for (auto& x : th) x.join();
+    size_t tot = 0;
+    for (auto& v : part) tot += v.size();
+    out.sidx.reserve(tot);
+    for (auto& v : part) out.sidx.insert(out.sidx.end(), v.begin(), v.end());
+    return out;
+  }
+
+  LevelSamples take_samples(i64 l, const std::vector<std::vector<std::pair<i64, i64>>>& ranges) {
+    if ((i64)sample_ahead.size() > l && sample_ahead[l].valid()) return sample_ahead[l].get();
+    return level_samples(l, ranges);
+  }
+
   void construct_level(i64 l, const std::vector<std::vector<std::pair<i64, i64>>>& ranges) {
     Level<T>& lv = L[l];
     Level<T>* low = (l < levels) ? &L[l + 1] : nullptr;
@@ -1218,30 +1311,14 @@ class Solver : public SolverBase {
           krows[i] = std::min<i64>(lv.dims[i], cnt);
         }
       } else {
-        const int nth = (int)std::max<i64>(1, std::min<i64>({8, (i64)std::thread::hardware_concurrency(), nodes / 16}));
-        std::vector<std::vector<int>> part(nth);
-        std::vector<i64> cnt(nodes, 0);
-        auto work = [&](int t) {
-          std::vector<int> tmp;
-          for (i64 i = nodes * t / nth; i < nodes * (t + 1) / nth; i++) {
-            if (sampling_mode == 1)
-              sample_far_list_geometric(ranges[g0 + i], gstart[g0 + i], samples, tmp);
-            else
-              sample_far_list(ranges[g0 + i], samples, tmp);
-            part[t].insert(part[t].end(), tmp.begin(), tmp.end());
-            cnt[i] = (i64)tmp.size();
-          }
-        };
-        std::vector<std::thread> th;
-        for (int t = 1; t < nth; t++) th.emplace_back(work, t);
-        work(0);
-        for (auto& x : th) x.join();
+        // Computed ahead by the background thread started in build() (or
+        // here, when none runs).
+        LevelSamples ls = take_samples(l, ranges);
         for (i64 i = 0; i < nodes; i++) {
-          soff[i + 1] = soff[i] + cnt[i];
-          krows[i] = std::min<i64>(lv.dims[i], cnt[i]);
+          soff[i + 1] = soff[i] + ls.cnt[i];
+          krows[i] = std::min<i64>(lv.dims[i], ls.cnt[i]);
         }
-        sidx.reserve(soff[nodes]);
-        for (auto& v : part) sidx.insert(sidx.end(), v.begin(), v.end());
+        sidx.swap(ls.sidx);
       }
       DVec<int> d_sidx, d_perm, d_nonzero;
       DVec<i64> d_soff, d_krows;
@@ -1322,9 +1399,9 @@ class Solver : public SolverBase {
                                     low ? 0 : 1, (int)nodes, (int)lv.maxM, st(), orth ? taus.p : nullptr),
              "basis_finish");
         }
-        if (orth) blocked_orth_qr<T>(lv, Rws.p, lv.Q.p, lv.R.p, taus.p, lv.d_ranks.download(st()), low == nullptr);
+        if (orth) blocked_orth_qr<T>(lv, Rws.p, lv.Q.p, lv.R.p, taus.p, fixed_rank_rule(lv.dims, krows, e), low == nullptr);
       }
-      lv.ranks = lv.d_ranks.download(st());
+      lv.ranks = orth ? fixed_rank_rule(lv.dims, krows, e) : lv.d_ranks.download(st());
     } else {
       lv.d_ranks.alloc(nodes);
       lv.d_ranks.zero(st());
@@ -1403,6 +1480,8 @@ class Solver : public SolverBase {
   void basis_gram(Level<T>& lv, bool leaf, const std::vector<i64>& soff, DVec<int>& d_sidx, DVec<i64>& d_krows,
                   DVec<int>& d_perm, DVec<double>& d_maxpiv, DVec<int>& d_nonzero, double e, i64 cap) {
     const i64 nodes = lv.nodes;
+    std::vector<i64> gram_krows(nodes);
+    for (i64 i = 0; i < nodes; i++) gram_krows[i] = std::min<i64>(lv.dims[i], soff[i + 1] - soff[i]);
     DVec<double> spts, G, XF, Rws;
     spts.alloc(std::max<i64>(3, 3 * soff[nodes]));
     ck(launch_gather_points(bodies.p, d_sidx.p, soff[nodes], spts.p, st()), "gather samples");
@@ -1496,14 +1575,15 @@ class Solver : public SolverBase {
       DVec<double> state;
       d_steps.upload(steps);
       state.alloc(3 * nodes);
-      Prof pf("pivchol", fl, 0.);
-      for (i64 k0 = 0; k0 < maxsteps; k0 += nb) {
-        ck(launch_pivchol_panel(lv.d_dims.p, d_steps.p, G.p, Rws.p, lv.d_qoff.p, d_perm.p, lv.d_xoff.p, state.p,
-                                (int)k0, nb, (int)nodes, (int)lv.maxM, st()),
-           "pivchol panel");
+      // The trailing-update plans depend only on the sizes: all are built
+      // (and uploaded) before the first panel, so the device does not wait
+      // for host planning between panels.
+      std::vector<GemmPlan<double>> ups;
+      ups.reserve((size_t)std::max<i64>(0, (maxsteps - 1) / nb));
+      for (i64 k0 = 0; k0 + nb < maxsteps; k0 += nb) {
         const i64 k1 = k0 + nb;
-        if (k1 >= maxsteps) break;
-        GemmPlan<double> up;
+        ups.emplace_back();
+        GemmPlan<double>& up = ups.back();
         up.name = "gemm_pivchol_update";
         for (i64 i = 0; i < nodes; i++) {
           const i64 M = lv.dims[i];
@@ -1513,7 +1593,14 @@ class Solver : public SolverBase {
           up.add_entry(Rb + k0 * M + k1, M, 0, Rb + k0 * M + k1, M, 1, nb, -1.);
         }
         up.finalize();
-        up.run(st());
+      }
+      Prof pf("pivchol", fl, 0.);
+      for (i64 k0 = 0, p = 0; k0 < maxsteps; k0 += nb, p++) {
+        ck(launch_pivchol_panel(lv.d_dims.p, d_steps.p, G.p, Rws.p, lv.d_qoff.p, d_perm.p, lv.d_xoff.p, state.p,
+                                (int)k0, nb, (int)nodes, (int)lv.maxM, st()),
+           "pivchol panel");
+        if (k0 + nb >= maxsteps) break;
+        ups[p].run(st());
       }
     }
     DVec<double> taus;
@@ -1528,7 +1615,7 @@ class Solver : public SolverBase {
            "basis_finish");
       }
       blocked_orth_qr<double>(lv, Rws.p, reinterpret_cast<double*>(lv.Q.p), reinterpret_cast<double*>(lv.R.p),
-                              taus.p, lv.d_ranks.download(st()), leaf);
+                              taus.p, fixed_rank_rule(lv.dims, gram_krows, e), leaf);
     } else {
       DVec<double> Qd, Rd;
       Qd.alloc(lv.qoff[nodes]);
@@ -1542,7 +1629,7 @@ class Solver : public SolverBase {
                                        leaf ? 1 : 0, (int)nodes, (int)lv.maxM, st(), taus.p),
            "basis_finish");
       }
-      blocked_orth_qr<double>(lv, Rws.p, Qd.p, Rd.p, taus.p, lv.d_ranks.download(st()), leaf);
+      blocked_orth_qr<double>(lv, Rws.p, Qd.p, Rd.p, taus.p, fixed_rank_rule(lv.dims, gram_krows, e), leaf);
       ck(launch_convert<double, T>(Qd.p, lv.Q.p, lv.qoff[nodes], st()), "convert");
       ck(launch_convert<double, T>(Rd.p, lv.R.p, lv.qoff[nodes], st()), "convert");
     }
