@@ -672,24 +672,76 @@ namespace h2b {
 // T of the compact-WY form Q = H_0 ... H_{r-1} = I - V T V^T (forward,
 // column by column: T[i][i] = tau_i, T[0:i, i] = -tau_i T[0:i,0:i] S[0:i, i]
 // with S = V^T V), one CTA per box, r x r column-major at Tb + toff[box].
+// Blocked: the 32 x 32 diagonal blocks are independent and are formed one
+// per warp with the recurrence (lane j keeps row j of its block in
+// registers, the column -tau_i S[0:i, i] is shared by shuffles; no barrier);
+// the blocks above the diagonal follow from the product rule of compact-WY
+// factors, T[A, B] = -T[A, A] S[A, B] T[B, B], for the leading columns A of
+// each column block B in turn (two barriers per block instead of two per
+// column).
+constexpr int WY_B = 32;
+
+template <typename T>
+__device__ __forceinline__ void wy_diag_block(const WyTask<T>& t, int off, int bs, int lane) {
+  const int r = t.r;
+  T row[WY_B];
+#pragma unroll
+  for (int l = 0; l < WY_B; l++) row[l] = T(0);
+#pragma unroll
+  for (int i = 0; i < WY_B; i++) {
+    if (i < bs) {
+      const T tau = t.taus[off + i];
+      const T c = lane < i ? -tau * t.S[(off + lane) + (i64)(off + i) * r] : T(0);
+      T v = T(0);
+#pragma unroll
+      for (int l = 0; l < WY_B; l++) {
+        const T cl = __shfl_sync(0xffffffffu, c, l);
+        if (l < i) v += row[l] * cl;
+      }
+      if (lane < i) row[i] = v;
+      if (lane == i) row[i] = tau;
+    }
+  }
+  if (lane < bs) {
+#pragma unroll
+    for (int l = 0; l < WY_B; l++)
+      if (l < bs) t.Tm[(off + lane) + (i64)(off + l) * r] = row[l];
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_wy_t(const WyTask<T>* __restrict__ tasks) {
   const WyTask<T> t = tasks[blockIdx.x];
   const int r = t.r;
+  if (r <= 0) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* col = reinterpret_cast<T*>(smem_raw);  // r
-  for (i64 e = threadIdx.x; e < (i64)r * r; e += blockDim.x) t.Tm[e] = T(0);
+  T* X = reinterpret_cast<T*>(smem_raw);  // (r - 32) x 32, column-major, ld r
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int nb = (r + WY_B - 1) / WY_B;
+  // Zero the strictly lower triangle (the blocks below write only the upper part).
+  for (i64 e = threadIdx.x; e < (i64)r * r; e += blockDim.x) {
+    const int row = (int)(e % r), colm = (int)(e / r);
+    if (row > colm) t.Tm[e] = T(0);
+  }
+  for (int b = warp; b < nb; b += nw) wy_diag_block(t, b * WY_B, min(WY_B, r - b * WY_B), lane);
   __syncthreads();
-  for (int i = 0; i < r; i++) {
-    const T tau = t.taus[i];
-    for (int j = threadIdx.x; j < i; j += blockDim.x) col[j] = -tau * t.S[j + (i64)i * r];
-    __syncthreads();
-    for (int j = threadIdx.x; j < i; j += blockDim.x) {
+  for (int b = 1; b < nb; b++) {
+    const int off = b * WY_B, bs = min(WY_B, r - off), p = off;
+    // X = S[0:p, B] T[B, B]  (T[B, B] upper triangular)
+    for (int e = threadIdx.x; e < p * bs; e += blockDim.x) {
+      const int j = e % p, c = e / p;
       T v = T(0);
-      for (int l = j; l < i; l++) v += t.Tm[j + (i64)l * r] * col[l];
-      t.Tm[j + (i64)i * r] = v;
+      for (int k = 0; k <= c; k++) v += t.S[j + (i64)(off + k) * r] * t.Tm[(off + k) + (i64)(off + c) * r];
+      X[j + c * p] = v;
     }
-    if (threadIdx.x == 0) t.Tm[i + (i64)i * r] = tau;
+    __syncthreads();
+    // T[0:p, B] = -T[0:p, 0:p] X  (T[0:p, 0:p] upper triangular)
+    for (int e = threadIdx.x; e < p * bs; e += blockDim.x) {
+      const int j = e % p, c = e / p;
+      T v = T(0);
+      for (int k = j; k < p; k++) v += t.Tm[j + (i64)k * r] * X[k + c * p];
+      t.Tm[j + (i64)(off + c) * r] = -v;
+    }
     __syncthreads();
   }
 }
@@ -697,8 +749,14 @@ __global__ void __launch_bounds__(256) k_wy_t(const WyTask<T>* __restrict__ task
 template <typename T>
 cudaError_t launch_wy_t(const WyTask<T>* d_tasks, int ntasks, int maxr, cudaStream_t st) {
   if (ntasks == 0) return cudaSuccess;
+  const size_t smem = sizeof(T) * (size_t)std::max(1, maxr - WY_B) * WY_B;
+  if (smem > 200 * 1024) return cudaErrorInvalidValue;
+  if (smem > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(k_wy_t<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
   note_launch();
-  k_wy_t<T><<<ntasks, 256, sizeof(T) * (size_t)(maxr + 2), st>>>(d_tasks);
+  k_wy_t<T><<<ntasks, 256, smem, st>>>(d_tasks);
   return cudaGetLastError();
 }
 template cudaError_t launch_wy_t<double>(const WyTask<double>*, int, int, cudaStream_t);
