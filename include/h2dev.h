@@ -34,8 +34,22 @@ enum {
 /* Laplace3D 1/d and Yukawa3D exp(-alpha d)/d (kernel.hpp:28-50); QUADRATIC
  * d^2 + alpha has exactly low-rank off-diagonal blocks (no counterpart in the
  * reference: used to verify that the ULV factorization is an exact inverse
- * when no fill is dropped).  Every kernel takes the value 1/s at d == 0. */
-enum { H2DEV_KERNEL_LAPLACE = 0, H2DEV_KERNEL_YUKAWA = 1, H2DEV_KERNEL_QUADRATIC = 2 };
+ * when no fill is dropped).  Every kernel takes the value 1/s at d == 0.
+ *
+ * HELMHOLTZ is Helmholtz3D exp(-i alpha d)/d (kernel.hpp:63-74, the
+ * reference's default, main.cpp:62), complex valued.  Its vectors are
+ * complex: each column holds n complex values as 2n doubles with real and
+ * imaginary parts interleaved (the std::complex<double> layout), so lenX,
+ * ld and every vector length count 2 doubles per body.  The solver stores the
+ * real symmetric form S = [[Re K, Im K], [Im K, -Re K]] over two real
+ * unknowns per body (S conj(x) = K x) and runs every kernel of the real
+ * path on it; matvec, precondition, GMRES and the dense matvec conjugate
+ * their vectors so that callers see K itself.  rank, leveled_rank and
+ * samples are given per body as for the reference (complex degrees of
+ * freedom) and doubled for the real form; level dims and ranks report real
+ * unknowns.  Bodies' x coordinates are used with bit 0 cleared (a change of
+ * at most one ulp), which carries the component tag internally. */
+enum { H2DEV_KERNEL_LAPLACE = 0, H2DEV_KERNEL_YUKAWA = 1, H2DEV_KERNEL_QUADRATIC = 2, H2DEV_KERNEL_HELMHOLTZ = 3 };
 enum { H2DEV_FP64 = 0, H2DEV_FP32 = 1 };
 
 /* ---- host helpers (no device work) ---------------------------------- */
@@ -217,10 +231,12 @@ int h2dev_solve_rel_err_device_noalloc(h2dev_handle_t h, int64_t n, int64_t nrhs
 /* ---- dense kernel access (kernel.cpp:71-85 gen_matrix; main.cpp:83-84) */
 
 /* out (m x n column-major) = K(bi, bj), bodies xyz-interleaved host arrays;
- * distances formed exactly as the reference's std::hypot. */
+ * distances formed exactly as the reference's std::hypot.  HELMHOLTZ: the
+ * complex block, 2m doubles per column (interleaved real/imaginary parts). */
 int h2dev_gen_block(h2dev_handle_t h, int kernel, double singularity, double alpha, const double* bi, int64_t m,
                     const double* bj, int64_t n, double* out);
-/* Y = A_dense X without storing A (host arrays, FP64). */
+/* Y = A_dense X without storing A (host arrays, FP64).  HELMHOLTZ: X and Y
+ * complex, 2n doubles per column (ld >= 2n). */
 int h2dev_dense_matvec(h2dev_handle_t h, int kernel, double singularity, double alpha, const double* bodies,
                        int64_t n, int64_t nrhs, const double* X, double* Y, int64_t ld);
 int h2dev_dense_matvec_device(h2dev_handle_t h, int kernel, double singularity, double alpha,

@@ -12,12 +12,15 @@
 //  * The dense-matrix Accessor argument of the constructor is accepted and
 //    not read (in the reference it only fed the randomized SVD of
 //    Hmatrix::construct, h-matrix.cpp:103-116, whose result is never used).
-//  * Kernels run on the device, so only Laplace3D and Yukawa3D are accepted
-//    by the solver (the complex Helmholtz3D is not implemented; a
-//    MatrixAccessor subclass of the caller's own works on the host, for
-//    gen_matrix, but the solver rejects it); std::complex<double> vector
-//    overloads take and return zero imaginary parts and throw if an input
-//    has a nonzero one.
+//  * Kernels run on the device, so the solver accepts Laplace3D, Yukawa3D
+//    and Helmholtz3D (a MatrixAccessor subclass of the caller's own works on
+//    the host, for gen_matrix, but the solver rejects it).  With a real
+//    kernel the std::complex<double> vector overloads take and return zero
+//    imaginary parts and throw if an input has a nonzero one.  With
+//    Helmholtz3D the vectors are complex and only the std::complex<double>
+//    overloads are accepted; the device holds the real symmetric form of the
+//    complex matrix (two real unknowns per body), so A[l].Dims / DimsLr count
+//    real unknowns, twice the reference's complex box dimensions.
 //  * The *Device methods (factorizeDeviceM, solvePreconditionDevice,
 //    solveGMRESDevice, matVecMulSp) are the same device computations as the
 //    plain ones: every method here runs on the GPU.
@@ -77,10 +80,19 @@ public:
   Yukawa3D(double s, double a) : MatrixAccessor(H2DEV_KERNEL_YUKAWA, s, a), singularity(1. / s) {}
 };
 
+// Helmholtz3D (kernel.hpp:63-74): exp(-i k d) / d, 1/s at d == 0.
+class Helmholtz3D : public MatrixAccessor {
+public:
+  double k;
+  double singularity;
+  Helmholtz3D(double wave_number, double s)
+      : MatrixAccessor(H2DEV_KERNEL_HELMHOLTZ, s, wave_number), k(wave_number), singularity(1. / s) {}
+};
+
 // gen_matrix (kernel.cpp:71-85): Aij (m x n, column-major) = K(|bi_y - bj_x|)
-// with the distance of the 3-argument std::hypot.  Laplace3D / Yukawa3D
-// blocks are generated on the device (Laplace bit for bit as the reference's
-// host loop); other MatrixAccessor kinds by the host loop.
+// with the distance of the 3-argument std::hypot.  Laplace3D / Yukawa3D /
+// Helmholtz3D blocks are generated on the device (Laplace bit for bit as the
+// reference's host loop); other MatrixAccessor kinds by the host loop.
 void gen_matrix(const MatrixAccessor& eval, long long m, long long n, const double* bi, const double* bj,
                 std::complex<double> Aij[]);
 
@@ -227,8 +239,11 @@ private:
   void fill_levels(const std::vector<Cell>& cells, double theta);
   h2dev_solver_t s_ = nullptr;
   h2dev_handle_t h_ = nullptr;
+  bool complex_ = false;  // Helmholtz3D: complex vectors
 };
 
-// Y = A_dense X (matrix-free on the GPU, FP64) for nrhs columns.
+// Y = A_dense X (matrix-free on the GPU, FP64) for nrhs columns.  With
+// Helmholtz3D, X and Y hold complex columns as interleaved real/imaginary
+// parts (2n doubles each, ld >= 2n).
 void dense_matvec(const MatrixAccessor& eval, const double bodies[], long long n, long long nrhs, const double X[],
                   double Y[], long long ld, h2dev_handle_t handle = nullptr);

@@ -3,6 +3,7 @@
 A drop-in for delta-leader/mxc's solver path: the C ABI in include/h2dev.h
 (libmxcb200.so) plus this Python mirror of solver.hpp's H2MatrixSolver.
 """
-from ._lib import (FP32, FP64, KERNEL_LAPLACE, KERNEL_QUADRATIC, KERNEL_YUKAWA, H2DevError, LIB_PATH, lib)  # noqa: F401
-from .solver import (H2MatrixSolver, Handle, Kernel, Laplace3D, Quadratic, Tree, Yukawa3D, build_tree,  # noqa: F401
-                     dense_matvec, gen_block, levels_for, pair_csr, rel_err_device, uniform_rhs, uniform_unit_cube_rnd)
+from ._lib import (FP32, FP64, KERNEL_HELMHOLTZ, KERNEL_LAPLACE, KERNEL_QUADRATIC, KERNEL_YUKAWA, H2DevError,  # noqa: F401
+                   LIB_PATH, lib)
+from .solver import (H2MatrixSolver, Handle, Helmholtz3D, Kernel, Laplace3D, Quadratic, Tree, Yukawa3D, build_tree,  # noqa: F401
+                     dense_matvec, gen_block, levels_for, mesh_sphere, pair_csr, rel_err_device, uniform_rhs, uniform_unit_cube_rnd)

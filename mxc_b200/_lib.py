@@ -22,6 +22,7 @@ H2DEV_ERR_NOCONV = 6
 KERNEL_LAPLACE = 0
 KERNEL_YUKAWA = 1
 KERNEL_QUADRATIC = 2
+KERNEL_HELMHOLTZ = 3
 FP64 = 0
 FP32 = 1
 

@@ -11,7 +11,17 @@ typedef int64_t i64;
 // KERNEL_QUADRATIC, K(d) = d^2 + alpha, has exactly low-rank (<= 6)
 // off-diagonal blocks; with it the ULV factorization has no dropped fill and
 // must reproduce the inverse, which is how the multilevel logic is verified.
-enum KernelKind { KERNEL_LAPLACE = 0, KERNEL_YUKAWA = 1, KERNEL_QUADRATIC = 2 };
+//
+// KERNEL_HELMHOLTZ is the complex kernel exp(-i k d)/d (kernel.hpp:63-74)
+// solved in its real symmetric form: every body appears twice, as its real
+// (component 0) and imaginary (component 1) unknown, and the real matrix
+// entry between component p of body a and component q of body b is
+//   p == q == 0: Re K(a, b);   p != q: Im K(a, b);   p == q == 1: -Re K(a, b).
+// This form is symmetric because K is complex symmetric, and it maps y =
+// conj(x) to K x (Re and Im interleaved, the std::complex<double> layout).
+// The component travels with the body's coordinates as bit 0 of x (see
+// helm_tag), so every copy and permutation of the body arrays keeps it.
+enum KernelKind { KERNEL_LAPLACE = 0, KERNEL_YUKAWA = 1, KERNEL_QUADRATIC = 2, KERNEL_HELMHOLTZ = 3 };
 
 // K(d) for d != 0, and the value used where two bodies coincide
 // (kernel.hpp:28-50: Laplace 1/d, Yukawa exp(-alpha d)/d, diagonal 1/s).
@@ -53,6 +63,58 @@ __device__ __forceinline__ double kernel_fast(const KernelParams& kp, double dx,
   return exp(-kp.alpha * (r2 * inv)) * inv;
 }
 
+// Helmholtz real form.  Component tag of a body coordinate (bit 0 of x) and
+// the coordinate with the tag cleared; distances are always taken between
+// cleared coordinates, so the two components of one body coincide.
+__device__ __forceinline__ int helm_tag(double x) { return (int)(__double_as_longlong(x) & 1LL); }
+__device__ __forceinline__ double helm_clear(double x) { return __longlong_as_double(__double_as_longlong(x) & ~1LL); }
+
+// Real-form entry for a pair of tagged bodies (wave number kp.alpha, value
+// 1/s at d == 0 as Helmholtz3D::operator()).  EXACT: distance by the
+// separately rounded hypot and a correctly rounded division, as the FP64
+// stored blocks use; otherwise one rsqrt of the squared distance.
+template <bool EXACT>
+__device__ __forceinline__ double helm_entry(const KernelParams& kp, double xi, double yi, double zi, double xj,
+                                             double yj, double zj) {
+  const int ti = helm_tag(xi), tj = helm_tag(xj);
+  const double dx = helm_clear(xi) - helm_clear(xj), dy = yi - yj, dz = zi - zj;
+  double re, im;
+  if (EXACT) {
+    const double d = hypot3_exact(dx, dy, dz);
+    if (d == 0.) {
+      re = kp.diag;
+      im = 0.;
+    } else {
+      double s, c;
+      sincos(kp.alpha * d, &s, &c);
+      re = __ddiv_rn(c, d);
+      im = -__ddiv_rn(s, d);
+    }
+  } else {
+    const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+    if (r2 == 0.) {
+      re = kp.diag;
+      im = 0.;
+    } else {
+      const double inv = rsqrt(r2);
+      double s, c;
+      sincos(kp.alpha * (r2 * inv), &s, &c);
+      re = c * inv;
+      im = -s * inv;
+    }
+  }
+  return ti != tj ? im : (ti ? -re : re);
+}
+
+// kernel_fast for a pair of bodies given by their coordinates (kind chosen
+// at run time): the real kernels take the differences exactly as
+// kernel_fast does; Helmholtz reads the component tags.
+__device__ __forceinline__ double kernel_fast_pair(const KernelParams& kp, double xi, double yi, double zi,
+                                                   double xj, double yj, double zj) {
+  if (kp.kind == KERNEL_HELMHOLTZ) return helm_entry<false>(kp, xi, yi, zi, xj, yj, zj);
+  return kernel_fast(kp, xi - xj, yi - yj, zi - zj);
+}
+
 // K(d) with the kernel kind fixed at compile time (no per-pair dispatch),
 // for the matrix-free applies: one reciprocal square root per pair (the
 // library's FP64 rsqrt measured faster on B200 than an FP32 seed refined by
@@ -65,6 +127,14 @@ __device__ __forceinline__ double kernel_eval(const KernelParams& kp, double dx,
   const double inv = rsqrt(r2);
   if constexpr (KIND == KERNEL_LAPLACE) return inv;
   return exp(-kp.alpha * (r2 * inv)) * inv;
+}
+
+// kernel_eval for a pair of bodies given by their coordinates.
+template <int KIND>
+__device__ __forceinline__ double kernel_eval_pair(const KernelParams& kp, double xi, double yi, double zi, double xj,
+                                                   double yj, double zj) {
+  if constexpr (KIND == KERNEL_HELMHOLTZ) return helm_entry<false>(kp, xi, yi, zi, xj, yj, zj);
+  return kernel_eval<KIND>(kp, xi - xj, yi - yj, zi - zj);
 }
 
 // Calls f(r, c, e) for every element e = r + c m of an m x n column-major

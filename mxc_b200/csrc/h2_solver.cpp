@@ -59,13 +59,15 @@ std::complex<double> MatrixAccessor::operator()(double d) const {
   if (d == 0.) return 1. / s;
   if (kind == H2DEV_KERNEL_YUKAWA) return std::exp(-alpha * d) / d;
   if (kind == H2DEV_KERNEL_QUADRATIC) return d * d + alpha;
+  if (kind == H2DEV_KERNEL_HELMHOLTZ) return std::exp(std::complex<double>(0., -alpha * d)) / d;
   return 1. / d;
 }
 
 void gen_matrix(const MatrixAccessor& eval, long long m, long long n, const double* bi, const double* bj,
                 std::complex<double> Aij[]) {
   if (m <= 0 || n <= 0) return;
-  const bool device = eval.kind == H2DEV_KERNEL_LAPLACE || eval.kind == H2DEV_KERNEL_YUKAWA;
+  const bool device =
+      eval.kind == H2DEV_KERNEL_LAPLACE || eval.kind == H2DEV_KERNEL_YUKAWA || eval.kind == H2DEV_KERNEL_HELMHOLTZ;
   if (!device) {
     for (long long x = 0; x < n; x++)
       for (long long y = 0; y < m; y++) {
@@ -74,15 +76,19 @@ void gen_matrix(const MatrixAccessor& eval, long long m, long long n, const doub
       }
     return;
   }
-  // Column panels of at most 2^26 doubles through the device generator.
-  const long long cols = std::max<long long>(1, ((long long)1 << 26) / m);
-  std::vector<double> buf((size_t)(m * std::min(cols, n)));
+  // Column panels of at most 2^26 doubles through the device generator (a
+  // Helmholtz panel holds interleaved real and imaginary parts).
+  const long long w = eval.kind == H2DEV_KERNEL_HELMHOLTZ ? 2 : 1;
+  const long long cols = std::max<long long>(1, ((long long)1 << 26) / (w * m));
+  std::vector<double> buf((size_t)(w * m * std::min(cols, n)));
   for (long long x0 = 0; x0 < n; x0 += cols) {
     const long long nc = std::min(cols, n - x0);
     check(h2dev_gen_block(H2MatrixSolver::default_handle(), eval.kind, eval.s, eval.alpha, bi, m, bj + 3 * x0, nc,
                           buf.data()),
           "h2dev_gen_block");
-    for (long long e = 0; e < m * nc; e++) Aij[x0 * m + e] = std::complex<double>(buf[(size_t)e], 0.);
+    for (long long e = 0; e < m * nc; e++)
+      Aij[x0 * m + e] = w == 2 ? std::complex<double>(buf[(size_t)(2 * e)], buf[(size_t)(2 * e + 1)])
+                               : std::complex<double>(buf[(size_t)e], 0.);
   }
 }
 
@@ -190,8 +196,10 @@ H2MatrixSolver::H2MatrixSolver(const MatrixAccessor& eval, double epi, long long
 void H2MatrixSolver::create(const MatrixAccessor& eval, double epi, long long rank, long long leveled_rank,
                             const std::vector<Cell>& cells, double theta, const double bodies[], long long samples,
                             int precision) {
-  if (eval.kind != H2DEV_KERNEL_LAPLACE && eval.kind != H2DEV_KERNEL_YUKAWA && eval.kind != H2DEV_KERNEL_QUADRATIC)
-    throw std::invalid_argument("H2MatrixSolver: the device evaluates Laplace3D and Yukawa3D kernels only");
+  if (eval.kind != H2DEV_KERNEL_LAPLACE && eval.kind != H2DEV_KERNEL_YUKAWA && eval.kind != H2DEV_KERNEL_QUADRATIC &&
+      eval.kind != H2DEV_KERNEL_HELMHOLTZ)
+    throw std::invalid_argument("H2MatrixSolver: the device evaluates Laplace3D, Yukawa3D and Helmholtz3D kernels only");
+  complex_ = eval.kind == H2DEV_KERNEL_HELMHOLTZ;
   const long long nc = (long long)cells.size();
   if (nc < (2LL << levels) - 1) throw std::invalid_argument("cells: fewer than 2^(levels+1) - 1 cells");
   std::vector<int64_t> child((size_t)nc * 2), body((size_t)nc * 2);
@@ -274,6 +282,7 @@ H2MatrixSolver& H2MatrixSolver::operator=(H2MatrixSolver&& o) noexcept {
     info = std::move(o.info);
     s_ = o.s_;
     h_ = o.h_;
+    complex_ = o.complex_;
     o.s_ = nullptr;
   }
   return *this;
@@ -284,11 +293,19 @@ H2MatrixSolver::~H2MatrixSolver() {
 }
 
 void H2MatrixSolver::matVecMul(double X[]) {
+  if (complex_) throw std::invalid_argument("matVecMul: Helmholtz3D takes complex vectors");
   const long long n = local_bodies.second - local_bodies.first;
   check(h2dev_matvec(s_, 1, X, n), "h2dev_matvec");
 }
 
+// Complex vectors of a Helmholtz3D solver go to the device as interleaved
+// real/imaginary parts (the std::complex<double> layout).
 void H2MatrixSolver::matVecMul(std::complex<double> X[]) {
+  if (complex_) {
+    const long long n = local_bodies.second - local_bodies.first;
+    check(h2dev_matvec(s_, 1, reinterpret_cast<double*>(X), 2 * n), "h2dev_matvec");
+    return;
+  }
   std::vector<double> r = real_parts(X, local_bodies.second - local_bodies.first);
   matVecMul(r.data());
   put_real(X, r);
@@ -305,11 +322,17 @@ void H2MatrixSolver::factorizeM() {
 }
 
 void H2MatrixSolver::solvePrecondition(double X[]) {
+  if (complex_) throw std::invalid_argument("solvePrecondition: Helmholtz3D takes complex vectors");
   const long long n = local_bodies.second - local_bodies.first;
   check(h2dev_solve_precondition(s_, 1, X, n), "h2dev_solve_precondition");
 }
 
 void H2MatrixSolver::solvePrecondition(std::complex<double> X[]) {
+  if (complex_) {
+    const long long n = local_bodies.second - local_bodies.first;
+    check(h2dev_solve_precondition(s_, 1, reinterpret_cast<double*>(X), 2 * n), "h2dev_solve_precondition");
+    return;
+  }
   std::vector<double> r = real_parts(X, local_bodies.second - local_bodies.first);
   solvePrecondition(r.data());
   put_real(X, r);
@@ -317,6 +340,7 @@ void H2MatrixSolver::solvePrecondition(std::complex<double> X[]) {
 
 void H2MatrixSolver::solveGMRES(double tol, H2MatrixSolver& M, double X[], const double B[], long long nrhs,
                                 long long ld, long long inner_iters, long long outer_iters, bool early_exit) {
+  if (complex_) throw std::invalid_argument("solveGMRES: Helmholtz3D takes complex vectors");
   resid.assign((size_t)((outer_iters + 1) * nrhs), 0.);
   std::vector<int64_t> it((size_t)nrhs, 0);
   const int rc = h2dev_solve_gmres(s_, M.s_, tol, nrhs, X, B, ld, inner_iters, outer_iters, early_exit ? 1 : 0,
@@ -334,6 +358,16 @@ void H2MatrixSolver::solveGMRES(double tol, H2MatrixSolver& M, double X[], const
 void H2MatrixSolver::solveGMRES(double tol, H2MatrixSolver& M, std::complex<double> X[],
                                 const std::complex<double> B[], long long inner_iters, long long outer_iters) {
   const long long n = local_bodies.second - local_bodies.first;
+  if (complex_) {
+    if (!M.complex_) throw std::invalid_argument("solveGMRES: operator and preconditioner kernels differ");
+    resid.assign((size_t)(outer_iters + 1), 0.);
+    int64_t it = 0;
+    const int rc = h2dev_solve_gmres(s_, M.s_, tol, 1, reinterpret_cast<double*>(X), reinterpret_cast<const double*>(B),
+                                     2 * n, inner_iters, outer_iters, 0, resid.data(), &it);
+    if (rc != H2DEV_ERR_NOCONV) check(rc, "h2dev_solve_gmres");
+    iters = it;
+    return;
+  }
   std::vector<double> x = real_parts(X, n), b = real_parts(B, n);
   solveGMRES(tol, M, x.data(), b.data(), 1, n, inner_iters, outer_iters, false);
   put_real(X, x);

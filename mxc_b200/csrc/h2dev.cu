@@ -955,6 +955,10 @@ class SolverBase {
   virtual i64 export_size(i64 l, int what) const = 0;
   virtual void export_to(i64 l, int what, double* out) = 0;
   h2dev_handle_s* h = nullptr;
+  // Helmholtz: the solver holds the real symmetric form S of the complex
+  // matrix K over two unknowns per body (KERNEL_HELMHOLTZ), S conj(x) = K x.
+  // The entry points conjugate their vectors so that callers see K itself.
+  bool complex_form = false;
 };
 
 struct BuildArgs {
@@ -2869,7 +2873,8 @@ using namespace h2b;
   }
 
 static KernelParams make_kp(int kernel, double singularity, double alpha) {
-  require(kernel == H2DEV_KERNEL_LAPLACE || kernel == H2DEV_KERNEL_YUKAWA || kernel == H2DEV_KERNEL_QUADRATIC,
+  require(kernel == H2DEV_KERNEL_LAPLACE || kernel == H2DEV_KERNEL_YUKAWA || kernel == H2DEV_KERNEL_QUADRATIC ||
+              kernel == H2DEV_KERNEL_HELMHOLTZ,
           "unknown kernel");
   require(singularity != 0., "singularity must be nonzero");
   KernelParams kp;
@@ -3098,6 +3103,35 @@ int h2dev_solver_create(h2dev_handle_t h, int kernel, double singularity, double
     }
   }
   require(a.cells[0].body[0] == 0 && a.cells[0].body[1] == nbodies, "root cell must span all bodies");
+  // Helmholtz: body i becomes unknowns 2i (real part) and 2i + 1 (imaginary
+  // part) of the real form, tagged in bit 0 of x; every cell keeps its
+  // geometry and owns the unknowns of its bodies; ranks and far samples
+  // count real unknowns, two per complex degree of freedom.
+  std::vector<double> helm_bodies;
+  const bool helm = kernel == H2DEV_KERNEL_HELMHOLTZ;
+  if (helm) {
+    require(nbodies < ((int64_t)1 << 40), "too many bodies");
+    helm_bodies.resize((size_t)6 * nbodies);
+    for (int64_t i = 0; i < nbodies; i++) {
+      int64_t xb;
+      std::memcpy(&xb, &bodies[3 * i], sizeof(xb));
+      for (int t = 0; t < 2; t++) {
+        const int64_t xt = (xb & ~(int64_t)1) | t;
+        std::memcpy(&helm_bodies[6 * i + 3 * t], &xt, sizeof(xt));
+        helm_bodies[6 * i + 3 * t + 1] = bodies[3 * i + 1];
+        helm_bodies[6 * i + 3 * t + 2] = bodies[3 * i + 2];
+      }
+    }
+    a.bodies = helm_bodies.data();
+    a.nbodies = 2 * nbodies;
+    a.rank = 2 * rank;
+    a.leveled_rank = 2 * leveled_rank;
+    a.samples = samples > 0 ? 2 * samples : samples;
+    for (auto& c : a.cells) {
+      c.body[0] *= 2;
+      c.body[1] *= 2;
+    }
+  }
   std::unique_ptr<h2dev_solver_s> s(new h2dev_solver_s());
   if (precision == H2DEV_FP64) {
     auto* p = new Solver<double>();
@@ -3110,6 +3144,7 @@ int h2dev_solver_create(h2dev_handle_t h, int kernel, double singularity, double
     p->h = h;
     p->build(a);
   }
+  s->impl->complex_form = helm;
   h->refs++;
   *out = s.release();
   return H2DEV_OK;
@@ -3171,7 +3206,10 @@ int h2dev_matvec(h2dev_solver_t s, int64_t nrhs, double* X, int64_t ldx) {
   SolverBase* p = s->impl.get();
   CurHandle ch(p->h);
   require(nrhs > 0 && ldx >= p->lenX(), "bad nrhs/ld");
-  with_device_copy(p->h, p->lenX(), nrhs, X, ldx, [&](double* d) { p->matvec(nrhs, d, p->lenX()); });
+  with_device_copy(p->h, p->lenX(), nrhs, X, ldx, [&](double* d) {
+    if (p->complex_form) ck(launch_conj_interleaved(d, p->lenX(), p->lenX(), (int)nrhs, p->h->stream), "conj");
+    p->matvec(nrhs, d, p->lenX());
+  });
   check_tc(p->h);
   return H2DEV_OK;
   H2_API_END
@@ -3181,6 +3219,8 @@ int h2dev_matvec_device(h2dev_solver_t s, int64_t nrhs, double* dX, int64_t ldx)
   H2_API_BEGIN
   require(s && s->impl && dX, "null argument");
   CurHandle ch(s->impl->h);
+  if (s->impl->complex_form)
+    ck(launch_conj_interleaved(dX, s->impl->lenX(), ldx, (int)nrhs, s->impl->h->stream), "conj");
   s->impl->matvec(nrhs, dX, ldx);
   check_tc(s->impl->h);
   return H2DEV_OK;
@@ -3208,7 +3248,10 @@ int h2dev_solve_precondition(h2dev_solver_t s, int64_t nrhs, double* X, int64_t 
   SolverBase* p = s->impl.get();
   CurHandle ch(p->h);
   require(nrhs > 0 && ldx >= p->lenX(), "bad nrhs/ld");
-  with_device_copy(p->h, p->lenX(), nrhs, X, ldx, [&](double* d) { p->precondition(nrhs, d, p->lenX()); });
+  with_device_copy(p->h, p->lenX(), nrhs, X, ldx, [&](double* d) {
+    p->precondition(nrhs, d, p->lenX());
+    if (p->complex_form) ck(launch_conj_interleaved(d, p->lenX(), p->lenX(), (int)nrhs, p->h->stream), "conj");
+  });
   check_tc(p->h);
   return H2DEV_OK;
   H2_API_END
@@ -3219,6 +3262,8 @@ int h2dev_solve_precondition_device(h2dev_solver_t s, int64_t nrhs, double* dX, 
   require(s && s->impl && dX, "null argument");
   CurHandle ch(s->impl->h);
   s->impl->precondition(nrhs, dX, ldx);
+  if (s->impl->complex_form)
+    ck(launch_conj_interleaved(dX, s->impl->lenX(), ldx, (int)nrhs, s->impl->h->stream), "conj");
   check_tc(s->impl->h);
   return H2DEV_OK;
   H2_API_END
@@ -3230,8 +3275,15 @@ int h2dev_solve_gmres_device(h2dev_solver_t A, h2dev_solver_t M, double tol, int
   H2_API_BEGIN
   require(A && A->impl && M && M->impl && dX && dB && resid, "null argument");
   require(ld >= A->impl->lenX(), "bad ld");
+  require(A->impl->complex_form == M->impl->complex_form, "operator and preconditioner kernels differ in kind");
   CurHandle ch(A->impl->h);
-  return gmres(*A->impl, *M->impl, tol, nrhs, dX, dB, ld, inner, outer, early_exit, resid, iters);
+  // Helmholtz: GMRES on S y = B with y = conj(X) (S conj(x) = K x).
+  const bool cf = A->impl->complex_form;
+  cudaStream_t st = A->impl->h->stream;
+  if (cf) ck(launch_conj_interleaved(dX, A->impl->lenX(), ld, (int)nrhs, st), "conj");
+  int rc = gmres(*A->impl, *M->impl, tol, nrhs, dX, dB, ld, inner, outer, early_exit, resid, iters);
+  if (cf) ck(launch_conj_interleaved(dX, A->impl->lenX(), ld, (int)nrhs, st), "conj");
+  return rc;
   H2_API_END
 }
 
@@ -3243,6 +3295,7 @@ int h2dev_solve_gmres(h2dev_solver_t A, h2dev_solver_t M, double tol, int64_t nr
   CurHandle ch(a->h);
   const int64_t n = a->lenX();
   require(nrhs > 0 && ld >= n, "bad nrhs/ld");
+  require(a->complex_form == M->impl->complex_form, "operator and preconditioner kernels differ in kind");
   cudaStream_t st = a->h->stream;
   DVec<double> dX, dB;
   dX.alloc((size_t)n * nrhs);
@@ -3251,7 +3304,9 @@ int h2dev_solve_gmres(h2dev_solver_t A, h2dev_solver_t M, double tol, int64_t nr
                        cudaMemcpyHostToDevice, st), "H2D");
   ck(cudaMemcpy2DAsync(dB.p, sizeof(double) * n, B, sizeof(double) * ld, sizeof(double) * n, nrhs,
                        cudaMemcpyHostToDevice, st), "H2D");
+  if (a->complex_form) ck(launch_conj_interleaved(dX.p, n, n, (int)nrhs, st), "conj");
   int rc = gmres(*a, *M->impl, tol, nrhs, dX.p, dB.p, n, inner, outer, early_exit, resid, iters);
+  if (a->complex_form) ck(launch_conj_interleaved(dX.p, n, n, (int)nrhs, st), "conj");
   ck(cudaMemcpy2DAsync(X, sizeof(double) * ld, dX.p, sizeof(double) * n, sizeof(double) * n, nrhs,
                        cudaMemcpyDeviceToHost, st), "D2H");
   ck(cudaStreamSynchronize(st), "sync");
@@ -3266,9 +3321,24 @@ int h2dev_gen_block(h2dev_handle_t h, int kernel, double singularity, double alp
   require(m * n < ((int64_t)1 << 31), "block too large");
   KernelParams kp = make_kp(kernel, singularity, alpha);
   if (m == 0 || n == 0) return H2DEV_OK;
+  CurHandle ch(h);
   DVec<double> di, dj, dout;
   di.upload(std::vector<double>(bi, bi + 3 * m));
   dj.upload(std::vector<double>(bj, bj + 3 * n));
+  if (kernel == H2DEV_KERNEL_HELMHOLTZ) {
+    // Rows: both components of each bi body; columns: the real part of each
+    // bj body.  The 2m x n real block is the m x n complex block with its
+    // real and imaginary parts interleaved.
+    require(2 * m * n < ((int64_t)1 << 31), "block too large");
+    DVec<double> ei, ej;
+    ei.alloc((size_t)6 * m);
+    ej.alloc((size_t)3 * n);
+    ck(launch_helm_expand(di.p, m, 2, ei.p, h->stream), "expand");
+    ck(launch_helm_expand(dj.p, n, 1, ej.p, h->stream), "expand");
+    std::swap(di, ei);
+    std::swap(dj, ej);
+    m *= 2;
+  }
   dout.alloc((size_t)m * n);
   std::vector<GenTask> gt(1);
   gt[0].bi = di.p;
@@ -3289,9 +3359,24 @@ int h2dev_gen_block(h2dev_handle_t h, int kernel, double singularity, double alp
 int h2dev_dense_matvec_device(h2dev_handle_t h, int kernel, double singularity, double alpha, const double* dbodies,
                               int64_t n, int64_t nrhs, const double* dX, double* dY, int64_t ld) {
   H2_API_BEGIN
-  require(h && dbodies && dX && dY && n > 0 && nrhs > 0 && ld >= n, "bad arguments");
   KernelParams kp = make_kp(kernel, singularity, alpha);
+  const bool helm = kernel == H2DEV_KERNEL_HELMHOLTZ;
+  require(h && dbodies && dX && dY && n > 0 && nrhs > 0 && ld >= (helm ? 2 * n : n), "bad arguments");
   CurHandle ch(h);
+  if (helm) {
+    // K X = S conj(X) over the tagged real-form bodies (2n unknowns).
+    DVec<double> eb, cx;
+    eb.alloc((size_t)6 * n);
+    cx.alloc((size_t)2 * n * nrhs);
+    ck(launch_helm_expand(dbodies, n, 2, eb.p, h->stream), "expand");
+    ck(cudaMemcpy2DAsync(cx.p, sizeof(double) * 2 * n, dX, sizeof(double) * ld, sizeof(double) * 2 * n, nrhs,
+                         cudaMemcpyDeviceToDevice, h->stream),
+       "copy");
+    ck(launch_conj_interleaved(cx.p, 2 * n, 2 * n, (int)nrhs, h->stream), "conj");
+    Prof pf("dense_matvec", 8. * (double)n * n * nrhs, 32. * n * nrhs);
+    ck(launch_dense_matvec(kp, eb.p, 2 * n, cx.p, 2 * n, dY, ld, (int)nrhs, h->stream), "dense_matvec");
+    return H2DEV_OK;
+  }
   Prof pf("dense_matvec", 2. * (double)n * n * nrhs, 16. * n * nrhs);
   ck(launch_dense_matvec(kp, dbodies, n, dX, ld, dY, ld, (int)nrhs, h->stream), "dense_matvec");
   return H2DEV_OK;
@@ -3301,17 +3386,29 @@ int h2dev_dense_matvec_device(h2dev_handle_t h, int kernel, double singularity, 
 int h2dev_dense_matvec(h2dev_handle_t h, int kernel, double singularity, double alpha, const double* bodies,
                        int64_t n, int64_t nrhs, const double* X, double* Y, int64_t ld) {
   H2_API_BEGIN
-  require(h && bodies && X && Y && n > 0 && nrhs > 0 && ld >= n, "bad arguments");
   KernelParams kp = make_kp(kernel, singularity, alpha);
+  const bool helm = kernel == H2DEV_KERNEL_HELMHOLTZ;
+  const int64_t len = helm ? 2 * n : n;  // doubles per column
+  require(h && bodies && X && Y && n > 0 && nrhs > 0 && ld >= len, "bad arguments");
+  CurHandle ch(h);
   DVec<double> db, dx, dy;
   db.upload(std::vector<double>(bodies, bodies + 3 * n));
-  dx.alloc((size_t)n * nrhs);
-  dy.alloc((size_t)n * nrhs);
-  ck(cudaMemcpy2D(dx.p, sizeof(double) * n, X, sizeof(double) * ld, sizeof(double) * n, nrhs,
+  dx.alloc((size_t)len * nrhs);
+  dy.alloc((size_t)len * nrhs);
+  ck(cudaMemcpy2D(dx.p, sizeof(double) * len, X, sizeof(double) * ld, sizeof(double) * len, nrhs,
                   cudaMemcpyHostToDevice), "H2D");
-  ck(launch_dense_matvec(kp, db.p, n, dx.p, n, dy.p, n, (int)nrhs, h->stream), "dense_matvec");
+  if (helm) {
+    // K X = S conj(X) over the tagged real-form bodies (2n unknowns).
+    DVec<double> eb;
+    eb.alloc((size_t)6 * n);
+    ck(launch_helm_expand(db.p, n, 2, eb.p, h->stream), "expand");
+    ck(launch_conj_interleaved(dx.p, len, len, (int)nrhs, h->stream), "conj");
+    ck(launch_dense_matvec(kp, eb.p, len, dx.p, len, dy.p, len, (int)nrhs, h->stream), "dense_matvec");
+  } else {
+    ck(launch_dense_matvec(kp, db.p, n, dx.p, n, dy.p, n, (int)nrhs, h->stream), "dense_matvec");
+  }
   ck(cudaStreamSynchronize(h->stream), "sync");
-  ck(cudaMemcpy2D(Y, sizeof(double) * ld, dy.p, sizeof(double) * n, sizeof(double) * n, nrhs,
+  ck(cudaMemcpy2D(Y, sizeof(double) * ld, dy.p, sizeof(double) * len, sizeof(double) * len, nrhs,
                   cudaMemcpyDeviceToHost), "D2H");
   return H2DEV_OK;
   H2_API_END

@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(TS_THREADS) k_sample_tsqr(
       int c = tid + k * TS_THREADS;
       if (c < M)
         for (int r = 0; r < TR; r++)
-          tile[r * M + c] = r < nrows ? (T)kernel_fast(kp, sp[3 * r] - px[k], sp[3 * r + 1] - py[k], sp[3 * r + 2] - pz[k]) : T(0);
+          tile[r * M + c] = r < nrows ? (T)kernel_fast_pair(kp, sp[3 * r], sp[3 * r + 1], sp[3 * r + 2], px[k], py[k], pz[k]) : T(0);
     }
     __syncthreads();
     const int jend = (rows + nrows) < M ? (rows + nrows) : M;

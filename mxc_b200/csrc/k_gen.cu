@@ -36,6 +36,16 @@ __device__ __forceinline__ double gen_fast(const KernelParams& kp, double dx, do
   return exp(-kp.alpha * (r2 * inv)) * inv;
 }
 
+// One element from the two bodies' coordinates (Helmholtz reads the
+// component tags; the real kernels take the differences as above).
+template <bool FAST, int KIND>
+__device__ __forceinline__ double gen_pair(const KernelParams& kp, double xi, double yi, double zi, double xj,
+                                           double yj, double zj) {
+  if constexpr (KIND == KERNEL_HELMHOLTZ) return helm_entry<!FAST>(kp, xi, yi, zi, xj, yj, zj);
+  const double dx = xi - xj, dy = yi - yj, dz = zi - zj;
+  return FAST ? gen_fast<KIND>(kp, dx, dy, dz) : gen_exact<KIND>(kp, dx, dy, dz);
+}
+
 template <typename T, bool FAST, int KIND>
 __global__ void __launch_bounds__(GEN_ROWS) k_gen_blocks(KernelParams kp, const GenTask* __restrict__ tasks,
                                                          T* __restrict__ out, int* __restrict__ err) {
@@ -106,8 +116,7 @@ __global__ void __launch_bounds__(GEN_ROWS) k_gen_blocks(KernelParams kp, const 
       T* oc = o + r + (i64)c0 * t.ld;
 #pragma unroll 4
       for (int c = 0; c < nc; c++) {
-        const double dx = px - cpts[3 * c], dy = py - cpts[3 * c + 1], dz = pz - cpts[3 * c + 2];
-        oc[(i64)c * t.ld] = (T)(FAST ? gen_fast<KIND>(kp, dx, dy, dz) : gen_exact<KIND>(kp, dx, dy, dz));
+        oc[(i64)c * t.ld] = (T)gen_pair<FAST, KIND>(kp, px, py, pz, cpts[3 * c], cpts[3 * c + 1], cpts[3 * c + 2]);
       }
     }
   }
@@ -119,6 +128,8 @@ static void gen_launch(const KernelParams& kp, dim3 grid, const GenTask* d_tasks
     k_gen_blocks<T, FAST, KERNEL_LAPLACE><<<grid, GEN_ROWS, 0, st>>>(kp, d_tasks, out, err);
   else if (kp.kind == KERNEL_YUKAWA)
     k_gen_blocks<T, FAST, KERNEL_YUKAWA><<<grid, GEN_ROWS, 0, st>>>(kp, d_tasks, out, err);
+  else if (kp.kind == KERNEL_HELMHOLTZ)
+    k_gen_blocks<T, FAST, KERNEL_HELMHOLTZ><<<grid, GEN_ROWS, 0, st>>>(kp, d_tasks, out, err);
   else
     k_gen_blocks<T, FAST, KERNEL_QUADRATIC><<<grid, GEN_ROWS, 0, st>>>(kp, d_tasks, out, err);
 }
@@ -141,6 +152,29 @@ template cudaError_t launch_gen_blocks<double>(const KernelParams&, const GenTas
                                                int, int*);
 template cudaError_t launch_gen_blocks<float>(const KernelParams&, const GenTask*, int, i64, float*, cudaStream_t,
                                               int, int*);
+
+// Helmholtz real form: body i of b (n x 3) becomes rows 2i + t of out
+// (2n x 3), with bit 0 of x set to the component t (t = 0 real part, 1
+// imaginary part).  comps = 1 writes only the t = 0 rows (n x 3 out).
+__global__ void k_helm_expand(const double* __restrict__ b, i64 n, int comps, double* __restrict__ out) {
+  for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x) {
+    const long long xb = __double_as_longlong(b[3 * i]) & ~1LL;
+    const double y = b[3 * i + 1], z = b[3 * i + 2];
+    for (int t = 0; t < comps; t++) {
+      double* o = out + 3 * (comps * i + t);
+      o[0] = __longlong_as_double(xb | t);
+      o[1] = y;
+      o[2] = z;
+    }
+  }
+}
+cudaError_t launch_helm_expand(const double* bodies, i64 n, int comps, double* out, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const i64 g = (n + 255) / 256;
+  note_launch();
+  k_helm_expand<<<(int)(g > 148 * 8 ? 148 * 8 : g), 256, 0, st>>>(bodies, n, comps, out);
+  return cudaGetLastError();
+}
 
 // Y = A_dense X for up to NR right-hand sides per pass.  Each thread owns a
 // row; columns stream through shared memory in tiles of 256 bodies.
@@ -173,7 +207,7 @@ __global__ void __launch_bounds__(DM_THREADS) k_dense_mv(KernelParams kp, const 
     __syncthreads();
     int jn = (n - j0) < DM_THREADS ? (int)(n - j0) : DM_THREADS;
     for (int jj = 0; jj < jn; jj++) {
-      double k = kernel_fast(kp, xi - sp[3 * jj], yi - sp[3 * jj + 1], zi - sp[3 * jj + 2]);
+      double k = kernel_fast_pair(kp, xi, yi, zi, sp[3 * jj], sp[3 * jj + 1], sp[3 * jj + 2]);
 #pragma unroll
       for (int c = 0; c < NR; c++) acc[c] += k * sx[jj * NR + c];
     }

@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(MF_NT, RPT == 1 ? 8 : 4)
         const double cx = cs[3 * b], cy = cs[3 * b + 1], cz = cs[3 * b + 2];
         double kv[RPT];
 #pragma unroll
-        for (int q = 0; q < RPT; q++) kv[q] = kernel_eval<KIND>(kp, px[q] - cx, py[q] - cy, pz[q] - cz);
+        for (int q = 0; q < RPT; q++) kv[q] = kernel_eval_pair<KIND>(kp, px[q], py[q], pz[q], cx, cy, cz);
         const double* br = bs + b * NRP;
         if constexpr (NR == 1) {
           const double x = br[0];
@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(32 * MFD_WARPS) k_mf_dmma(KernelParams kp, con
 #pragma unroll
         for (int q = 0; q < 4; q++) {
           // row g8 + 8q: block q >> 1, fragment half q & 1
-          const double v = kernel_eval<KIND>(kp, px[q] - cx, py[q] - cy, pz[q] - cz);
+          const double v = kernel_eval_pair<KIND>(kp, px[q], py[q], pz[q], cx, cy, cz);
           a[q >> 1][2 * j + (q & 1)] = cv ? v : 0.;
         }
       }
@@ -236,10 +236,13 @@ static cudaError_t mf_kind(const KernelParams& kp, int nr, const MfTask* d_tasks
   if (RPT == 1 && nr > 4) {  // tiles of mf_dmma_rows_per_cta() rows
     if (kp.kind == KERNEL_LAPLACE) return mf_dmma_go<KERNEL_LAPLACE>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
     if (kp.kind == KERNEL_YUKAWA) return mf_dmma_go<KERNEL_YUKAWA>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
+    if (kp.kind == KERNEL_HELMHOLTZ)
+      return mf_dmma_go<KERNEL_HELMHOLTZ>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
     return mf_dmma_go<KERNEL_QUADRATIC>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
   }
   if (kp.kind == KERNEL_LAPLACE) return mf_go<KERNEL_LAPLACE, RPT>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
   if (kp.kind == KERNEL_YUKAWA) return mf_go<KERNEL_YUKAWA, RPT>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
+  if (kp.kind == KERNEL_HELMHOLTZ) return mf_go<KERNEL_HELMHOLTZ, RPT>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
   return mf_go<KERNEL_QUADRATIC, RPT>(kp, nr, d_tasks, d_ents, d_tiles, ntiles, st);
 }
 

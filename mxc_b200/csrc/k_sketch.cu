@@ -98,8 +98,8 @@ __global__ void __launch_bounds__(SK_NT, 2)
       const int a = a0 + e / SK_TN, c = c0 + e % SK_TN;
       if ((i64)a >= S || c >= M) continue;
       const i64 body = sk_body(a, r0, r0, rstart, rend);
-      W[(i64)a * M + c] = (T)kernel_fast(kp, bodies[3 * body] - X[3 * c], bodies[3 * body + 1] - X[3 * c + 1],
-                                         bodies[3 * body + 2] - X[3 * c + 2]);
+      W[(i64)a * M + c] = (T)kernel_fast_pair(kp, bodies[3 * body], bodies[3 * body + 1], bodies[3 * body + 2],
+                                              X[3 * c], X[3 * c + 1], X[3 * c + 2]);
     }
     return;
   }
@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(SK_NT, 2)
       const int fl = e * 4 + (lane & 3);
       double v = 0.;
       if (cv && fb[b][fl] >= 0)
-        v = kernel_fast(kp, fc[b][3 * fl] - x0, fc[b][3 * fl + 1] - x1, fc[b][3 * fl + 2] - x2);
+        v = kernel_fast_pair(kp, fc[b][3 * fl], fc[b][3 * fl + 1], fc[b][3 * fl + 2], x0, x1, x2);
       xf[b][cl * SK_CS + fl] = v;
     }
     if (tid >= 32 && tid < 64) {

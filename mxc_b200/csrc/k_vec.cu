@@ -32,6 +32,26 @@ template cudaError_t launch_convert<double, float>(const double*, float*, i64, c
 template cudaError_t launch_convert<float, double>(const float*, double*, i64, cudaStream_t);
 template cudaError_t launch_convert<double, double>(const double*, double*, i64, cudaStream_t);
 
+// Complex conjugate of n/2 interleaved (re, im) pairs per column of a
+// column-major n x nrhs array (leading dimension ld): negates the odd rows.
+__global__ void k_conj_interleaved(double* __restrict__ X, i64 half, i64 ld, int nrhs) {
+  const i64 total = half * nrhs;
+  for (i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (i64)gridDim.x * blockDim.x) {
+    const i64 c = e / half, i = e - c * half;
+    double* p = X + c * ld + 2 * i + 1;
+    *p = -*p;
+  }
+}
+cudaError_t launch_conj_interleaved(double* X, i64 n, i64 ld, int nrhs, cudaStream_t st) {
+  const i64 half = n / 2;
+  if (half == 0 || nrhs <= 0) return cudaSuccess;
+  i64 g = (half * nrhs + 255) / 256;
+  const int grid = (int)(g > 148 * 16 ? 148 * 16 : g);
+  note_launch();
+  k_conj_interleaved<<<grid, 256, 0, st>>>(X, half, ld, nrhs);
+  return cudaGetLastError();
+}
+
 constexpr int DOT_THREADS = 256;
 constexpr i64 DOT_ROWS = 8192;  // rows per chunk
 int dots_chunks(i64 n) { return (int)((n + DOT_ROWS - 1) / DOT_ROWS); }

@@ -289,6 +289,10 @@ cudaError_t launch_scale_by_norm(const double* w, double* vout, const double* nr
                                  i64 n, int nrhs, cudaStream_t st);
 cudaError_t launch_gmres_ls(const double* H, int ld, int inner, const double* beta, double* y, int nrhs,
                             cudaStream_t st, const int* used = nullptr);
+// Helmholtz real form: tagged bodies (comps = 2: 2n x 3, both components; 1: n x 3, real part only).
+cudaError_t launch_helm_expand(const double* bodies, i64 n, int comps, double* out, cudaStream_t st);
+// Complex conjugate of a column-major array of interleaved (re, im) pairs (n doubles per column).
+cudaError_t launch_conj_interleaved(double* X, i64 n, i64 ld, int nrhs, cudaStream_t st);
 cudaError_t launch_axpby(double* y, const double* x, double a, double b, i64 n, cudaStream_t st);
 cudaError_t launch_residual_norm_finish(const double* nrm2, const double* normb, double* resid, int nrhs,
                                         cudaStream_t st);

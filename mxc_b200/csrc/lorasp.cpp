@@ -8,10 +8,10 @@
 //
 // The reference fixes its kernel and geometry in the source; here they are
 // options (the default geometry is the reference's: mesh_sphere of radius
-// sqrt(N / 4 pi)).  Its default kernel, the complex Helmholtz3D, is not
-// implemented; the default here is Laplace3D with the same diagonal 1/s,
-// s = 0.1.
-//   --kernel laplace|yukawa   --singularity S   --alpha A (Yukawa decay)
+// sqrt(N / 4 pi)) and its kernel (Helmholtz3D with wave number 1 and
+// s = 0.1, main.cpp:62), on complex vectors as the reference's.
+//   --kernel helmholtz|laplace|yukawa   --singularity S
+//   --alpha A (Helmholtz wave number or Yukawa decay, 1)
 //   --geometry sphere|cube    --seed K (cube: std::mt19937 seed, 999)
 //   --samples S   far-list cap of the basis construction (0: every far body)
 //   --precision fp64|fp32     storage of the preconditioner
@@ -19,6 +19,7 @@
 // matrix-free FP64 device matvec (same products, no N^2 memory).
 #include <algorithm>
 #include <chrono>
+#include <complex>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -40,15 +41,33 @@ double now_s() {
 void usage() {
   std::printf(
       "usage: lorasp [N [theta [leaf [rank [leveled_rank [epi [mode [csv]]]]]]]]\n"
-      "              [--kernel laplace|yukawa] [--singularity S] [--alpha A]\n"
+      "              [--kernel helmholtz|laplace|yukawa] [--singularity S] [--alpha A]\n"
       "              [--geometry sphere|cube] [--seed K] [--samples S] [--precision fp64|fp32]\n");
+}
+
+typedef std::complex<double> cplx;
+
+// Y = K X with the matrix-free FP64 device matvec (main.cpp:83-84 multiplies
+// by the dense matrix): complex columns as interleaved parts for
+// Helmholtz3D, real parts for the real kernels.
+void dense_apply(const MatrixAccessor& eval, const double* body, long long n, const std::vector<cplx>& X,
+                 std::vector<cplx>& Y) {
+  if (eval.kind == H2DEV_KERNEL_HELMHOLTZ) {
+    dense_matvec(eval, body, n, 1, reinterpret_cast<const double*>(X.data()), reinterpret_cast<double*>(Y.data()),
+                 2 * n);
+    return;
+  }
+  std::vector<double> x((size_t)n), y((size_t)n);
+  for (long long i = 0; i < n; i++) x[(size_t)i] = X[(size_t)i].real();
+  dense_matvec(eval, body, n, 1, x.data(), y.data(), n);
+  for (long long i = 0; i < n; i++) Y[(size_t)i] = cplx(y[(size_t)i], 0.);
 }
 
 }  // namespace
 
 int main(int argc, char* argv[]) {
   std::vector<std::string> pos;
-  std::string kernel = "laplace", geometry = "sphere", precision = "fp64";
+  std::string kernel = "helmholtz", geometry = "sphere", precision = "fp64";
   double singularity = 0.1, alpha = 1.;
   unsigned seed = 999;
   long long samples = 0;
@@ -95,7 +114,7 @@ int main(int argc, char* argv[]) {
   const double epi = arg(5) ? std::atof(arg(5)) : 1e-10;
   const std::string mode = arg(6) ? std::string(arg(6)) : "h2";
   const char* csv = arg(7);
-  if (Nbody < 2 || leaf_size < 1 || (mode != "h2" && mode != "hss") || (kernel != "laplace" && kernel != "yukawa") ||
+  if (Nbody < 2 || leaf_size < 1 || (mode != "h2" && mode != "hss") || (kernel != "helmholtz" && kernel != "laplace" && kernel != "yukawa") ||
       (geometry != "sphere" && geometry != "cube") || (precision != "fp64" && precision != "fp32")) {
     usage();
     return 2;
@@ -105,32 +124,37 @@ int main(int argc, char* argv[]) {
     leaf_size = Nbody < leaf_size ? Nbody : leaf_size;
     const long long levels = h2_levels_for(Nbody, leaf_size);
     const long long ncells = (2LL << levels) - 1;
-    const MatrixAccessor eval = kernel == "yukawa" ? (MatrixAccessor)Yukawa3D(singularity, alpha)
-                                                   : (MatrixAccessor)Laplace3D(singularity);
+    const MatrixAccessor eval = kernel == "yukawa"    ? (MatrixAccessor)Yukawa3D(singularity, alpha)
+                                : kernel == "laplace" ? (MatrixAccessor)Laplace3D(singularity)
+                                                      : (MatrixAccessor)Helmholtz3D(alpha, singularity);
     const int pc_precision = precision == "fp32" ? H2DEV_FP32 : H2DEV_FP64;
 
     std::vector<double> body((size_t)Nbody * 3);
-    std::vector<double> Xbody((size_t)Nbody);
+    std::vector<cplx> Xbody((size_t)Nbody);
     std::vector<Cell> cell((size_t)ncells);
     if (geometry == "sphere")
       mesh_sphere(body.data(), Nbody, std::sqrt((double)Nbody / (4. * M_PI)));
     else
       uniform_unit_cube_rnd(body.data(), Nbody, 1., 3, seed);
     buildBinaryTree(cell.data(), body.data(), Nbody, levels);
-    if (h2_uniform_rhs(Xbody.data(), Nbody) != H2DEV_OK) throw std::runtime_error("h2_uniform_rhs failed");
+    {  // main.cpp:73-76: real parts from the default-seeded std::mt19937_64
+      std::vector<double> xr((size_t)Nbody);
+      if (h2_uniform_rhs(xr.data(), Nbody) != H2DEV_OK) throw std::runtime_error("h2_uniform_rhs failed");
+      for (long long i = 0; i < Nbody; i++) Xbody[(size_t)i] = cplx(xr[(size_t)i], 0.);
+    }
 
     double h2_construct_time = now_s();
     H2MatrixSolver matA(eval, epi, rank, leveled_rank, cell, theta, body.data(), levels, samples, H2DEV_FP64);
     h2_construct_time = now_s() - h2_construct_time;
 
     const long long lenX = matA.local_bodies.second - matA.local_bodies.first;
-    std::vector<double> X1(Xbody), X2((size_t)lenX, 0.);
+    std::vector<cplx> X1(Xbody), X2((size_t)lenX, 0.);
     double matvec_time = now_s();
     matA.matVecMul(X1.data());
     matvec_time = now_s() - matvec_time;
 
     double refmatvec_time = now_s();
-    dense_matvec(eval, body.data(), Nbody, 1, Xbody.data(), X2.data(), Nbody);
+    dense_apply(eval, body.data(), Nbody, Xbody, X2);
     refmatvec_time = now_s() - refmatvec_time;
     const double cerr = H2MatrixSolver::solveRelErr(lenX, X1.data(), X2.data());
 
@@ -157,7 +181,7 @@ int main(int argc, char* argv[]) {
     matM.solvePrecondition(X1.data());
     h2_sub_time = now_s() - h2_sub_time;
     const double serr = H2MatrixSolver::solveRelErr(lenX, X1.data(), Xbody.data());
-    std::fill(X1.begin(), X1.end(), 0.);
+    std::fill(X1.begin(), X1.end(), cplx(0., 0.));
 
     std::cout << "H^2-Preconditioner Construct Time: " << m_construct_time << ", " << 0. << std::endl;
     std::cout << "H^2-Preconditioner Construct Err: " << cerr_m << std::endl;

@@ -42,6 +42,20 @@ def uniform_unit_cube_rnd(n: int, seed: int, diameter: float = 1.0, dim: int = 3
     return b
 
 
+def mesh_sphere(n: int, r: float) -> np.ndarray:
+    """test_funcs.hpp:43-61 mesh_sphere, the reference's default geometry:
+    golden-angle spiral of n bodies on a sphere of radius r (the reference
+    uses r = sqrt(n / 4 pi), one body per unit area); the same formula as the
+    C++ API's mesh_sphere."""
+    golden = math.pi * (3.0 - math.sqrt(5.0))
+    i = np.arange(n, dtype=np.float64)
+    t = i / (n - 1) if n > 1 else np.zeros(n)
+    y = r - 2.0 * r * t
+    ring = np.sqrt(r * r - y * y)
+    a = golden * i
+    return np.ascontiguousarray(np.stack([ring * np.cos(a), y, ring * np.sin(a)], axis=1))
+
+
 def uniform_rhs(n: int) -> np.ndarray:
     """main.cpp:73-76 (default-seeded std::mt19937_64, uniform[0,1))."""
     x = np.empty(n, dtype=np.float64)
@@ -203,7 +217,7 @@ class Handle:
 
 
 class Kernel:
-    """Laplace3D(s) / Yukawa3D(s, alpha) of kernel.hpp:28-50."""
+    """Laplace3D(s) / Yukawa3D(s, alpha) / Helmholtz3D(k, s) of kernel.hpp:28-74."""
 
     def __init__(self, kind: int = L.KERNEL_LAPLACE, singularity: float = 1.0, alpha: float = 1.0):
         self.kind = kind
@@ -219,17 +233,35 @@ def Yukawa3D(s: float = 1.0, a: float = 1.0) -> Kernel:
     return Kernel(L.KERNEL_YUKAWA, s, a)
 
 
+def Helmholtz3D(wave_number: float = 1.0, s: float = 1.0) -> Kernel:
+    """exp(-i k d) / d, 1/s at d == 0 (kernel.hpp:63-74): complex matrices and vectors.
+
+    The device holds the real symmetric form of the complex matrix (two real
+    unknowns per body); vectors passed to a Helmholtz solver are complex128
+    arrays, and level dims / ranks count real unknowns."""
+    return Kernel(L.KERNEL_HELMHOLTZ, s, wave_number)
+
+
 def Quadratic(s: float = 1.0, a: float = 1.0) -> Kernel:
     """d^2 + a off the diagonal: exactly low-rank off-diagonal blocks (ULV exactness checks)."""
     return Kernel(L.KERNEL_QUADRATIC, s, a)
 
 
-def _as_cols(X: np.ndarray):
-    """(n,) or (n, nrhs) float64 -> Fortran-ordered 2-D view + nrhs + ld."""
+def _as_cols(X: np.ndarray, cplx: bool = False):
+    """(n,) or (n, nrhs) float64 -> Fortran-ordered 2-D view + nrhs + ld.
+
+    cplx: complex128 arrays, whose columns the library reads as 2n doubles
+    (interleaved real and imaginary parts); ld then counts doubles."""
+    if cplx:
+        assert X.dtype == np.complex128, "a Helmholtz solver takes complex128 vectors"
+    else:
+        assert X.dtype == np.float64, "a real-kernel solver takes float64 vectors"
+    w = 2 if cplx else 1
     if X.ndim == 1:
-        return X.reshape(-1, 1, order="F"), 1, X.shape[0]
+        assert X.flags.c_contiguous
+        return X.reshape(-1, 1, order="F"), 1, w * X.shape[0]
     assert X.flags.f_contiguous, "multi-RHS arrays must be column-major (order='F')"
-    return X, X.shape[1], X.shape[0]
+    return X, X.shape[1], w * X.shape[0]
 
 
 class H2MatrixSolver:
@@ -252,6 +284,7 @@ class H2MatrixSolver:
                                             _ptr(tree.R), _ptr(tree.C), theta, _ptr(bodies), n, tree.levels,
                                             samples, precision, C.byref(s)), "h2dev_solver_create")
         self.s = s
+        self.complex = kernel.kind == L.KERNEL_HELMHOLTZ
         self.local_bodies = (0, n)
         self.resid = None
         self.iters = 0
@@ -259,7 +292,7 @@ class H2MatrixSolver:
 
     # ------------------------------------------------------------ reference API
     def matVecMul(self, X: np.ndarray) -> None:
-        A, nrhs, ld = _as_cols(X)
+        A, nrhs, ld = _as_cols(X, self.complex)
         L.check(L.lib().h2dev_matvec(self.s, nrhs, _ptr(A), ld), "h2dev_matvec")
 
     def factorizeM(self) -> list:
@@ -273,13 +306,14 @@ class H2MatrixSolver:
         return self.info
 
     def solvePrecondition(self, X: np.ndarray) -> None:
-        A, nrhs, ld = _as_cols(X)
+        A, nrhs, ld = _as_cols(X, self.complex)
         L.check(L.lib().h2dev_solve_precondition(self.s, nrhs, _ptr(A), ld), "h2dev_solve_precondition")
 
     def solveGMRES(self, tol: float, M: "H2MatrixSolver", X: np.ndarray, B: np.ndarray, inner_iters: int,
                    outer_iters: int, early_exit: bool = False) -> int:
-        Xa, nrhs, ld = _as_cols(X)
-        Ba, nb, ldb = _as_cols(np.asarray(B, dtype=np.float64, order="F"))
+        dt = np.complex128 if self.complex else np.float64
+        Xa, nrhs, ld = _as_cols(X, self.complex)
+        Ba, nb, ldb = _as_cols(np.asarray(B, dtype=dt, order="F"), self.complex)
         assert nb == nrhs and ldb == ld
         resid = np.zeros((outer_iters + 1, nrhs), order="F")
         iters = np.zeros(nrhs, dtype=np.int64)
@@ -292,9 +326,11 @@ class H2MatrixSolver:
 
     @staticmethod
     def solveRelErr(X: np.ndarray, ref: np.ndarray) -> float:
-        """solver.cpp:229-238 (host-side reduction of two vectors)."""
-        d = np.asarray(X) - np.asarray(ref)
-        return math.sqrt(float(np.sum(d * d)) / float(np.sum(np.asarray(ref) ** 2)))
+        """solver.cpp:229-238 (host-side reduction of two vectors; of complex
+        vectors only the real parts enter, as in the reference)."""
+        d = np.real(np.asarray(X) - np.asarray(ref))
+        r = np.real(np.asarray(ref))
+        return math.sqrt(float(np.sum(d * d)) / float(np.sum(r * r)))
 
     # ------------------------------------------------------------ device-pointer API
     def matvec_device(self, ptr: int, nrhs: int, ld: int) -> None:
@@ -356,20 +392,23 @@ def rel_err_device(handle: Handle, xptr: int, refptr: int, n: int, nrhs: int, ld
 
 
 def gen_block(handle: Handle, kernel: Kernel, bi: np.ndarray, bj: np.ndarray) -> np.ndarray:
-    """gen_matrix (kernel.cpp:71-85) on the device; returns an (m, n) array."""
+    """gen_matrix (kernel.cpp:71-85) on the device; returns an (m, n) array
+    (complex128 for Helmholtz3D)."""
     bi = np.ascontiguousarray(bi, dtype=np.float64)
     bj = np.ascontiguousarray(bj, dtype=np.float64)
     m, n = bi.shape[0], bj.shape[0]
-    out = np.zeros((m, n), order="F")
+    cplx = kernel.kind == L.KERNEL_HELMHOLTZ
+    out = np.zeros((m, n), dtype=np.complex128 if cplx else np.float64, order="F")
     L.check(L.lib().h2dev_gen_block(handle.h, kernel.kind, kernel.singularity, kernel.alpha, _ptr(bi), m, _ptr(bj),
                                     n, _ptr(out)), "h2dev_gen_block")
     return out
 
 
 def dense_matvec(handle: Handle, kernel: Kernel, bodies: np.ndarray, X: np.ndarray) -> np.ndarray:
-    """Y = A_dense X (FP64, matrix-free on the device)."""
+    """Y = A_dense X (FP64, matrix-free on the device; complex for Helmholtz3D)."""
     bodies = np.ascontiguousarray(bodies, dtype=np.float64)
-    Xa, nrhs, ld = _as_cols(np.asarray(X, dtype=np.float64, order="F"))
+    cplx = kernel.kind == L.KERNEL_HELMHOLTZ
+    Xa, nrhs, ld = _as_cols(np.asarray(X, dtype=np.complex128 if cplx else np.float64, order="F"), cplx)
     Y = np.zeros_like(Xa, order="F")
     L.check(L.lib().h2dev_dense_matvec(handle.h, kernel.kind, kernel.singularity, kernel.alpha, _ptr(bodies),
                                        bodies.shape[0], nrhs, _ptr(Xa), _ptr(Y), ld), "h2dev_dense_matvec")

@@ -115,18 +115,25 @@ def xbody_uniform(n: int) -> np.ndarray:
 # Kernels (kernel.hpp:28-50, kernel.cpp:71-85)
 # --------------------------------------------------------------------------
 
-LAPLACE, YUKAWA, QUADRATIC = 0, 1, 2
+LAPLACE, YUKAWA, QUADRATIC, HELMHOLTZ = 0, 1, 2, 3
 
 
 @dataclass
 class Kernel:
     kind: int = LAPLACE
     singularity: float = 1.0  # ctor argument s; the diagonal value is 1/s
-    alpha: float = 1.0        # Yukawa decay
+    alpha: float = 1.0        # Yukawa decay, Helmholtz wave number
+
+    @property
+    def dtype(self):
+        """complex128 for Helmholtz3D (kernel.hpp:63-74), float64 otherwise."""
+        return np.complex128 if self.kind == HELMHOLTZ else np.float64
 
     def eval_d(self, d: np.ndarray) -> np.ndarray:
         with np.errstate(divide="ignore", invalid="ignore"):
-            if self.kind == LAPLACE:
+            if self.kind == HELMHOLTZ:
+                v = np.exp(-1j * self.alpha * d) / d
+            elif self.kind == LAPLACE:
                 v = 1.0 / d
             elif self.kind == YUKAWA:
                 v = np.exp(-self.alpha * d) / d
@@ -165,7 +172,7 @@ def dense_matvec(kern: Kernel, bodies: np.ndarray, x: np.ndarray, chunk: int = 2
     """y = A_dense x with A generated block-row by block-row (never stored whole)."""
     n = bodies.shape[0]
     x2 = x.reshape(n, -1)
-    y = np.zeros_like(x2)
+    y = np.zeros(x2.shape, dtype=np.result_type(x2, kern.dtype))
     for s in range(0, n, chunk):
         e = min(n, s + chunk)
         y[s:e] = gen_matrix(kern, bodies[s:e], bodies) @ x2
@@ -469,18 +476,22 @@ DBL_MIN = np.finfo(np.float64).tiny
 def householder_r(X: np.ndarray) -> np.ndarray:
     """R of a Householder QR (HouseholderQR::matrixQR upper part)."""
     if X.shape[0] == 0 or X.shape[1] == 0:
-        return np.zeros((min(X.shape), X.shape[1]))
+        return np.zeros((min(X.shape), X.shape[1]), dtype=X.dtype)
     return sla.qr(X, mode="r", check_finite=False)[0]
 
 
 def colpiv_qr(Xin: np.ndarray):
-    """Eigen 3.4 ColPivHouseholderQR::computeInPlace restated (real case).
+    """Eigen 3.4 ColPivHouseholderQR::computeInPlace restated.
 
     Returns (qr, perm, maxpivot, nonzero_pivots).  ``qr`` holds R in its
     upper triangle; ``perm[k]`` is the original index of pivoted column k
-    (A P = Q R, (A P)[:, k] = A[:, perm[k]]).
+    (A P = Q R, (A P)[:, k] = A[:, perm[k]]).  Complex input follows
+    makeHouseholderInPlace's complex rules: beta real with the sign opposite
+    to Re c0, tau = conj((beta - c0) / beta), H = I - tau v v^* applied on
+    the left (H maps the pivot column to beta e1).
     """
-    qr = np.array(Xin, dtype=np.float64, copy=True)
+    cplx = np.iscomplexobj(Xin)
+    qr = np.array(Xin, dtype=np.complex128 if cplx else np.float64, copy=True)
     rows, cols = qr.shape
     size = min(rows, cols)
     perm = np.arange(cols)
@@ -505,17 +516,30 @@ def colpiv_qr(Xin: np.ndarray):
         # makeHouseholderInPlace on qr[k:, k]
         c0 = qr[k, k]
         tail_v = qr[k + 1:, k]
-        tsq = float(tail_v @ tail_v)
-        if tsq <= DBL_MIN:
-            tau = 0.0
-            beta = c0
-            ess = np.zeros_like(tail_v)
+        if cplx:
+            tsq = float(np.vdot(tail_v, tail_v).real)
+            if tsq <= DBL_MIN and c0.imag * c0.imag <= DBL_MIN:
+                tau = 0.0
+                beta = c0.real
+                ess = np.zeros_like(tail_v)
+            else:
+                beta = math.sqrt(c0.real * c0.real + c0.imag * c0.imag + tsq)
+                if c0.real >= 0:
+                    beta = -beta
+                ess = tail_v / (c0 - beta)
+                tau = np.conj((beta - c0) / beta)
         else:
-            beta = math.sqrt(c0 * c0 + tsq)
-            if c0 >= 0:
-                beta = -beta
-            ess = tail_v / (c0 - beta)
-            tau = (beta - c0) / beta
+            tsq = float(tail_v @ tail_v)
+            if tsq <= DBL_MIN:
+                tau = 0.0
+                beta = c0
+                ess = np.zeros_like(tail_v)
+            else:
+                beta = math.sqrt(c0 * c0 + tsq)
+                if c0 >= 0:
+                    beta = -beta
+                ess = tail_v / (c0 - beta)
+                tau = (beta - c0) / beta
         qr[k + 1:, k] = ess
         qr[k, k] = beta
         if abs(beta) > maxpivot:
@@ -523,7 +547,7 @@ def colpiv_qr(Xin: np.ndarray):
         # applyHouseholderOnTheLeft to qr[k:, k+1:]
         if tau != 0.0 and k + 1 < cols:
             blk = qr[k:, k + 1:]
-            w = blk[0] + ess @ blk[1:]
+            w = blk[0] + (np.conj(ess) if cplx else ess) @ blk[1:]
             blk[0] -= tau * w
             blk[1:] -= tau * np.outer(ess, w)
         # norm downdate
@@ -569,7 +593,8 @@ def compute_basis(kern: Kernel, epi: float, Xbodies: np.ndarray, Fbodies: np.nda
     N = Fbodies.shape[0]
     K = min(M, N)
     rank = 0
-    c = np.zeros((M, M))
+    dt = kern.dtype
+    c = np.zeros((M, M), dtype=dt)
     if K > 0:
         XF = gen_matrix(kern, Fbodies, Xbodies)  # N x M
         if K < N and sketch_idx is not None:
@@ -587,7 +612,7 @@ def compute_basis(kern: Kernel, epi: float, Xbodies: np.ndarray, Fbodies: np.nda
             T = sla.solve_triangular(R11, qr[:rank, rank:], lower=False, check_finite=False)
             top = np.hstack([np.eye(rank), T])       # rank x M, pivoted order
             Xbodies[:] = Xbodies[perm]
-            PCt = np.zeros((M, rank))
+            PCt = np.zeros((M, rank), dtype=dt)
             PCt[perm, :] = top.T
             if orth:
                 RX2 = np.triu(a) @ PCt
@@ -664,9 +689,12 @@ class H2MatrixSolver:
     from weak admissibility; eps > 0 selects the ID operator mode.
     """
 
+    dt = np.float64  # element type of every block and vector; complex128 for Helmholtz3D
+
     def __init__(self, kern: Kernel, epi: float, rank: int, leveled_rank: int, cells: Cells,
                  theta: float, bodies: np.ndarray, levels: int, samples: int = 0, sampling: int = 0):
         self.kern = kern
+        self.dt = kern.dtype  # complex128 for Helmholtz3D: the reference's complex arithmetic
         self.levels = levels
         self.cells = cells
         self.bodies = bodies
@@ -707,16 +735,17 @@ class H2MatrixSolver:
             Dims = np.array([low.DimsLr[2 * i] + low.DimsLr[2 * i + 1] for i in range(nodes)], dtype=np.int64)
         lev.Dims = Dims
         lev.DimsLr = np.zeros(nodes, dtype=np.int64)
-        lev.Q = [np.zeros((d, d)) for d in Dims]
-        lev.R = [np.zeros((d, d)) for d in Dims]
+        dt = self.dt
+        lev.Q = [np.zeros((d, d), dtype=dt) for d in Dims]
+        lev.R = [np.zeros((d, d), dtype=dt) for d in Dims]
         lev.S = [np.zeros((d, 3)) for d in Dims]
         nA = int(lev.ARows[-1])
         lev.A = [None] * nA
         for i in range(nodes):
             for ij in range(lev.ARows[i], lev.ARows[i + 1]):
-                lev.A[ij] = np.zeros((Dims[i], Dims[lev.ACols[ij]]))
-        lev.X = [np.zeros(d) for d in Dims]
-        lev.Y = [np.zeros(d) for d in Dims]
+                lev.A[ij] = np.zeros((Dims[i], Dims[lev.ACols[ij]]), dtype=dt)
+        lev.X = [np.zeros(d, dtype=dt) for d in Dims]
+        lev.Y = [np.zeros(d, dtype=dt) for d in Dims]
 
         if Dims.sum():
             for i in range(nodes):
@@ -762,8 +791,8 @@ class H2MatrixSolver:
         nC = int(lev.CRows[-1])
         lev.C = [None] * nC
         lev.NA = [None] * nA
-        lev.Z = [np.zeros(r) for r in lev.DimsLr]
-        lev.W = [np.zeros(r) for r in lev.DimsLr]
+        lev.Z = [np.zeros(r, dtype=self.dt) for r in lev.DimsLr]
+        lev.W = [np.zeros(r, dtype=self.dt) for r in lev.DimsLr]
         if lev.DimsLr.sum():
             for i in range(nodes):
                 My = int(lev.DimsLr[i])
@@ -789,12 +818,13 @@ class H2MatrixSolver:
     def matvec(self, x: np.ndarray) -> np.ndarray:
         L = self.levels
         A = self.A
-        xin = np.asarray(x, dtype=np.float64)
+        xin = np.asarray(x, dtype=self.dt)
         for l in range(L, -1, -1):
             lev = A[l]
-            src = xin if l == L else np.concatenate(A[l + 1].Z) if len(A[l + 1].Z) else np.zeros(0)
+            src = xin if l == L else np.concatenate(A[l + 1].Z) if len(A[l + 1].Z) else np.zeros(0, dtype=self.dt)
             lev.X = self._split(lev, src, lev.Dims)
-            lev.Z = [lev.Q[i][:, :lev.DimsLr[i]].T @ lev.X[i] if lev.DimsLr[i] > 0 else np.zeros(0)
+            # h2matrix.cpp:266: z = q^T x (transpose, no conjugate)
+            lev.Z = [lev.Q[i][:, :lev.DimsLr[i]].T @ lev.X[i] if lev.DimsLr[i] > 0 else np.zeros(0, dtype=self.dt)
                      for i in range(lev.nodes)]
         for l in range(0, L):
             lev = A[l]
@@ -806,7 +836,7 @@ class H2MatrixSolver:
                         w = w + lev.C[ij] @ lev.Z[lev.CCols[ij]]
                     lev.W[i] = w
                     lev.Y[i] = lev.Q[i][:, :K] @ w
-            nxt = np.concatenate(lev.Y) if lev.nodes else np.zeros(0)
+            nxt = np.concatenate(lev.Y) if lev.nodes else np.zeros(0, dtype=self.dt)
             A[l + 1].W = self._split(A[l + 1], nxt, A[l + 1].DimsLr)
         lev = A[L]
         lev.X = self._split(lev, xin, lev.Dims)
@@ -814,7 +844,7 @@ class H2MatrixSolver:
         for i in range(lev.nodes):
             M = lev.Dims[i]
             K = lev.DimsLr[i]
-            yi = np.zeros(M)
+            yi = np.zeros(M, dtype=self.dt)
             if K > 0:
                 w = lev.W[i]
                 for ij in range(lev.CRows[i], lev.CRows[i + 1]):
@@ -845,14 +875,15 @@ class H2MatrixSolver:
             Ms = int(lev.DimsLr[i])
             Mr = M - Ms
             U = lev.Q[i]
+            Uh = U.conj().T  # Ui.adjoint() (h2matrix.cpp:373-379); U^T for real kernels
             Aii = lev.A[d]
-            b = U.T @ Aii.T
-            Aii[:] = U.T @ b.T
-            V = np.zeros((M, M))
-            V[:Ms] = U[:, :Ms].T
+            b = Uh @ Aii.T
+            Aii[:] = Uh @ b.T
+            V = np.zeros((M, M), dtype=self.dt)
+            V[:Ms] = Uh[:Ms]
             if Mr > 0:
                 lu, piv = sla.lu_factor(Aii[Ms:, Ms:], check_finite=False)
-                V[Ms:] = sla.lu_solve((lu, piv), U[:, Ms:].T, check_finite=False)
+                V[Ms:] = sla.lu_solve((lu, piv), Uh[Ms:], check_finite=False)
                 if Ms > 0:
                     Aii[Ms:, :Ms] = V[Ms:] @ b[:Ms].T
                     Aii[:Ms, :Ms] -= Aii[:Ms, Ms:] @ Aii[Ms:, :Ms]
@@ -865,9 +896,9 @@ class H2MatrixSolver:
                     j = int(lev.ACols[ij])
                     Uj = lev.Q[j]
                     Aij = lev.A[ij]
-                    bj = Uj.T @ Aij.T
+                    bj = Uj.conj().T @ Aij.T
                     Aij[:] = V @ bj.T
-            Bi = np.zeros((Mr, M))
+            Bi = np.zeros((Mr, M), dtype=self.dt)
             Bi[:, :Ms] = Aii[Ms:, :Ms]
             Bi[:, Ms:] = V[Ms:] @ U[:, Ms:]
             B[i] = Bi
@@ -905,9 +936,9 @@ class H2MatrixSolver:
         A = self.A
         for l in range(L, -1, -1):
             lev = A[l]
-            src = np.asarray(x, dtype=np.float64) if l == L else np.concatenate(A[l + 1].Z)
+            src = np.asarray(x, dtype=self.dt) if l == L else np.concatenate(A[l + 1].Z)
             lev.Y = self._split(lev, src, lev.Dims)
-            lev.X = [lev.R[i] @ lev.Y[i] if lev.Dims[i] > 0 else np.zeros(0) for i in range(lev.nodes)]
+            lev.X = [lev.R[i] @ lev.Y[i] if lev.Dims[i] > 0 else np.zeros(0, dtype=self.dt) for i in range(lev.nodes)]
             Z = []
             for i in range(lev.nodes):
                 Ms = int(lev.DimsLr[i])
@@ -924,7 +955,7 @@ class H2MatrixSolver:
         for l in range(0, L + 1):
             lev = A[l]
             if l == 0:
-                W = [np.zeros(int(r)) for r in lev.DimsLr]
+                W = [np.zeros(int(r), dtype=self.dt) for r in lev.DimsLr]
             else:
                 W = self._split(lev, np.concatenate(A[l - 1].Y), lev.DimsLr)
             lev.W = W
@@ -943,7 +974,9 @@ class H2MatrixSolver:
                             xi[Ms:] -= lev.A[ij][Ms:, :Ns] @ W[j]
                 Xn.append(xi)
             lev.X = Xn
-            lev.Y = [lev.Q[i] @ lev.X[i] if lev.Dims[i] > 0 else np.zeros(0) for i in range(lev.nodes)]
+            # h2matrix.cpp:532: y = conj(q) x
+            lev.Y = [lev.Q[i].conj() @ lev.X[i] if lev.Dims[i] > 0 else np.zeros(0, dtype=self.dt)
+                     for i in range(lev.nodes)]
         return np.concatenate(A[L].Y)
 
     # ---- GMRES (solver.cpp:144-201) ----
@@ -951,9 +984,10 @@ class H2MatrixSolver:
                     inner: int, outer: int, early_exit: bool = False):
         N = self.lenX
         ld = inner + 1
-        B = np.asarray(b, dtype=np.float64)
-        X = np.array(x, dtype=np.float64, copy=True)
-        normb = math.sqrt(float(B @ B))
+        dt = self.dt
+        B = np.asarray(b, dtype=dt)
+        X = np.array(x, dtype=dt, copy=True)
+        normb = math.sqrt(float(np.vdot(B, B).real))
         if normb == 0.0:
             normb = 1.0
         Rv = B.copy()
@@ -961,18 +995,18 @@ class H2MatrixSolver:
         iters = 0
         while iters < outer and tol <= resid[iters]:
             Rv = Msolver.solve_precondition(Rv)
-            beta = math.sqrt(float(Rv @ Rv))
-            H = np.zeros((ld, inner))
-            v = np.zeros((N, ld))
+            beta = math.sqrt(float(np.vdot(Rv, Rv).real))
+            H = np.zeros((ld, inner), dtype=dt)
+            v = np.zeros((N, ld), dtype=dt)
             v[:, 0] = Rv * (1.0 / beta)
             for i in range(inner):
                 Rv = self.matvec(v[:, i])
                 Rv = Msolver.solve_precondition(Rv)
-                H[:i + 1, i] = v[:, :i + 1].T @ Rv
+                H[:i + 1, i] = v[:, :i + 1].conj().T @ Rv
                 Rv = Rv - v[:, :i + 1] @ H[:i + 1, i]
-                H[i + 1, i] = math.sqrt(float(Rv @ Rv))
+                H[i + 1, i] = math.sqrt(float(np.vdot(Rv, Rv).real))
                 v[:, i + 1] = Rv * (1.0 / H[i + 1, i])
-            s = np.zeros(ld)
+            s = np.zeros(ld, dtype=dt)
             s[0] = beta
             y = np.linalg.lstsq(H, s, rcond=None)[0]
             X = X + v[:, :inner] @ y
@@ -980,14 +1014,15 @@ class H2MatrixSolver:
             Rv = self.matvec(Rv)
             Rv = Rv + B
             iters += 1
-            resid.append(math.sqrt(float(Rv @ Rv)) / normb)
+            resid.append(math.sqrt(float(np.vdot(Rv, Rv).real)) / normb)
         return X, np.array(resid), iters
 
 
 def solve_rel_err(x: np.ndarray, ref: np.ndarray) -> float:
-    """solver.cpp:229-238 (real parts)."""
-    d = x - ref
-    return math.sqrt(float(d @ d) / float(ref @ ref))
+    """solver.cpp:229-238 (real parts only, also for complex vectors)."""
+    d = np.real(x - ref)
+    r = np.real(ref)
+    return math.sqrt(float(d @ d) / float(r @ r))
 
 
 def levels_for(N: int, leaf: int) -> int:

@@ -12,6 +12,9 @@
 //   for each list in (Near theta, Far theta, Far 0):
 //     nrow = ncells+1, RowIndex[nrow], nnz, ColIndex[nnz]
 //   kernel probe: npairs, then for each pair (i, j, laplace f64, yukawa f64)
+//   Helmholtz probe (the same pairs): npairs, then for each pair the real
+//   and imaginary part (f64) of Helmholtz3D(1, 0.1), main.cpp:62
+//   sphere: N, then mesh_sphere(N, sqrt(N / 4 pi)) (N*3 f64), main.cpp:68
 #include <build_tree.hpp>
 #include <kernel.hpp>
 #include <test_funcs.hpp>
@@ -88,6 +91,20 @@ int main(int argc, char** argv) {
       put_i(f, i); put_i(f, j);
       put_d(f, lap(d).real()); put_d(f, yuk(d).real());
     }
+  Helmholtz3D helm(1., 1e-1);
+  put_i(f, np);
+  for (long long a = 0; a < 64; a++)
+    for (long long b = 0; b < 64; b++) {
+      long long i = a % N, j = (b * 7919) % N;
+      const double* bi = &body[3 * i];
+      const double* bj = &body[3 * j];
+      std::complex<double> v = helm(std::hypot(bi[0] - bj[0], bi[1] - bj[1], bi[2] - bj[2]));
+      put_d(f, v.real()); put_d(f, v.imag());
+    }
+  std::vector<double> sphere(N * 3);
+  mesh_sphere(&sphere[0], N, std::sqrt(N / (4 * M_PI)));
+  put_i(f, N);
+  fwrite(sphere.data(), sizeof(double), sphere.size(), f);
   fclose(f);
   return 0;
 }

@@ -2,8 +2,8 @@
 
 Runs oracle/_ref/ref_driver (the reference's own build_tree.cpp compiled from
 its source tree by oracle/Makefile, plus its header-only test_funcs.hpp and
-kernel.hpp) and stores its points, right-hand side, tree, Near/Far lists and
-kernel values as .npz files.  Needs the reference source tree, so it runs in
+kernel.hpp) and stores its points, right-hand side, tree, Near/Far lists,
+kernel values (Laplace, Yukawa, Helmholtz) and mesh_sphere points as .npz files.  Needs the reference source tree, so it runs in
 the development container only; the fixtures it writes are committed.
 
     make -C oracle && python tests/golden/make_fixtures.py
@@ -75,6 +75,11 @@ def read_dump(path: str) -> dict:
     out["probe_ij"] = ij
     out["probe_laplace"] = vals[:, 0]
     out["probe_yukawa"] = vals[:, 1]
+    nh = int(ints(1)[0])
+    hv = dbls(2 * nh).reshape(nh, 2)
+    out["probe_helmholtz"] = hv[:, 0] + 1j * hv[:, 1]
+    ns = int(ints(1)[0])
+    out["mesh_sphere"] = dbls(3 * ns).reshape(ns, 3)
     return out
 
 

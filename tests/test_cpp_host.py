@@ -83,7 +83,7 @@ def test_lorasp_help_and_bad_arguments():
     r = subprocess.run([LORASP, "--help"], capture_output=True, text=True)
     assert r.returncode == 0 and "usage: lorasp" in r.stdout
     assert subprocess.run([LORASP, "1000", "2", "256", "50", "0", "1e-10", "bogus"], capture_output=True).returncode == 2
-    assert subprocess.run([LORASP, "--kernel", "helmholtz"], capture_output=True).returncode == 2
+    assert subprocess.run([LORASP, "--kernel", "gaussian"], capture_output=True).returncode == 2
     assert subprocess.run([LORASP, "--no-such-option"], capture_output=True).returncode == 2
 
 
@@ -96,7 +96,7 @@ def test_lorasp_runs_the_reference_flow_and_matches_the_python_api(tmp_path, han
     n, theta, leaf, rank, eps, samples = 4096, 2.0, 256, 100, 1e-10, 2000
     csv = tmp_path / "run.csv"
     r = subprocess.run([LORASP, str(n), str(theta), str(leaf), str(rank), "0", str(eps), "h2", str(csv),
-                        "--geometry", "cube", "--singularity", "0.1", "--samples", str(samples)],
+                        "--kernel", "laplace", "--geometry", "cube", "--singularity", "0.1", "--samples", str(samples)],
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
     out = r.stdout

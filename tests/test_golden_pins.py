@@ -5,6 +5,8 @@ kernel.hpp compiled under oracle/_ref (tests/golden/make_fixtures.py).
 Everything here is bit-exact except Yukawa, whose exp() may differ by an ulp
 between numpy and glibc.
 """
+import math
+
 import numpy as np
 import pytest
 
@@ -55,6 +57,23 @@ def test_oracle_kernel_values(gold):
     vy = np.array([O.gen_matrix(yuk, b[i:i + 1], b[j:j + 1])[0, 0] for i, j in ij])
     assert np.array_equal(vl, gold["probe_laplace"])
     np.testing.assert_allclose(vy, gold["probe_yukawa"], rtol=4e-16, atol=0)
+    # Helmholtz3D(1, 0.1), the reference's default kernel (complex): numpy's
+    # complex exp against glibc's, within an ulp or so of the magnitude
+    helm = O.Kernel(O.HELMHOLTZ, 0.1, 1.0)
+    vh = np.array([O.gen_matrix(helm, b[i:i + 1], b[j:j + 1])[0, 0] for i, j in ij])
+    assert np.max(np.abs(vh - gold["probe_helmholtz"]) / np.abs(gold["probe_helmholtz"])) < 6e-16
+
+
+def test_mesh_sphere(gold):
+    """mesh_sphere(N, sqrt(N / 4 pi)) of the reference (main.cpp:68) against
+    the Python API's restatement (cos/sin of numpy vs glibc: within an ulp)."""
+    import mxc_b200 as m
+
+    ref = gold["mesh_sphere"]
+    n = ref.shape[0]
+    got = m.mesh_sphere(n, math.sqrt(n / (4 * math.pi)))
+    assert np.array_equal(got[:, 1], ref[:, 1])
+    np.testing.assert_allclose(got, ref, rtol=0, atol=4e-16 * math.sqrt(n))
 
 
 def test_library_host_plan(gold):
