@@ -90,6 +90,11 @@ def parse():
     ap.add_argument("--c5-singularity", type=float, default=1e-6,
                     help="diagonal 1/s of the scale-up sub-run's kernel")
     ap.add_argument("--c5-outer", type=int, default=20, help="GMRES restart limit of the scale-up sub-run")
+    ap.add_argument("--helm-n", type=int, default=8192,
+                    help="bodies of the Helmholtz sub-run (the reference's default run scaled up; 0 skips it)")
+    ap.add_argument("--helm-theta", type=float, default=1.0, help="admissibility of the Helmholtz sub-run")
+    ap.add_argument("--helm-samples", type=int, default=0,
+                    help="far samples per box of the Helmholtz sub-run's preconditioner (0: every far body)")
     ap.add_argument("--serving-requests", type=int, default=48,
                     help="requests per arrival rate of the serving phase (0: skip); Poisson arrivals over resident "
                          "systems")
@@ -584,6 +589,93 @@ def run_c5(a, h) -> dict:
     return {"unavailable": "no size from %d down to 65536 fits" % a.c5_n, "larger_sizes_tried": tried}
 
 
+def run_helmholtz(a, h) -> dict:
+    """The reference's default run (main.cpp:45-76: Helmholtz3D(1, 0.1) on
+    mesh_sphere of radius sqrt(N / 4 pi), theta 1, leaf 256, rank 50, eps
+    1e-10) scaled to --helm-n bodies, as a sub-run: complex system solved
+    through its real symmetric form (two real unknowns per body), operator
+    with ID bases from a sketch of every far body, preconditioner with
+    --helm-samples far samples (0: every far body, as the reference), 8
+    complex right-hand sides, GMRES(10) to 1e-10.  Sizes are bounded by the
+    box-dimension limit of 2048 real unknowns: at eps 1e-10 the Helmholtz
+    ranks barely compress at the upper levels (65,536 bodies exceed it).  One warm-up and one timed step each with the FP32 and the FP64
+    preconditioner; dense-checked residual and error against x_true."""
+    import numpy as np
+    import torch
+
+    import mxc_b200 as m
+
+    n, theta, leaf, rank, eps, nrhs, samples = a.helm_n, a.helm_theta, 256, 50, 1e-10, 8, a.helm_samples
+    k = m.Helmholtz3D(1.0, 0.1)
+    L = m.levels_for(n, leaf)
+    b = m.mesh_sphere(n, math.sqrt(n / (4 * math.pi)))
+    t = m.build_tree(b, L)
+    h.set_option(m._lib.OPT_SAMPLING, m._lib.SAMPLING_SKETCH)
+    t0 = time.time()
+    try:
+        A = m.H2MatrixSolver(h, k, eps, rank, 0, t, theta, b, samples=0, precision=m.FP64)
+        h.synchronize()
+    finally:
+        h.set_option(m._lib.OPT_SAMPLING, m._lib.SAMPLING_STRIDED)
+    op_s = time.time() - t0
+    rng = np.random.default_rng(20261203)
+    Xt = np.asfortranarray(rng.random((n, nrhs)) + 1j * rng.random((n, nrhs)))
+    B = np.asfortranarray(m.dense_matvec(h, k, b, Xt))
+    # device columns of 2n doubles (interleaved real/imaginary parts)
+    dB = torch.from_numpy(B.T.copy().view(np.float64)).cuda()
+    dX = torch.zeros_like(dB)
+    ld = 2 * n
+    torch.cuda.synchronize()
+
+    def one(precision, verify=True):
+        dX.zero_()
+        torch.cuda.synchronize()
+        h.timer_start()
+        M = m.H2MatrixSolver(h, k, 0.0, rank, 0, t, theta, b, samples=samples, precision=precision)
+        tb = h.timer_stop()
+        h.timer_start()
+        M.factorizeM()
+        tf = h.timer_stop()
+        h.timer_start()
+        rc, resid, iters = A.gmres_device(M, a.tol, dX.data_ptr(), dB.data_ptr(), nrhs, ld, a.inner, a.outer, True)
+        ts = h.timer_stop()
+        M.close()
+        r = {"build_ms": tb, "factor_ms": tf, "solve_ms": ts, "total_ms": tb + tf + ts, "converged": rc == 0,
+             "cycles": [int(v) for v in iters],
+             "h2_resid_max": float(max(resid[int(iters[c]), c] for c in range(nrhs)))}
+        if not verify:
+            return r, None
+        X = np.asfortranarray(dX.cpu().numpy().view(np.complex128).T)
+        R = m.dense_matvec(h, k, b, X)
+        r["dense_resid_max"] = float(max(np.linalg.norm(B[:, c] - R[:, c]) / np.linalg.norm(B[:, c])
+                                         for c in range(nrhs)))
+        r["x_true_err_max"] = float(max(np.linalg.norm(X[:, c] - Xt[:, c]) / np.linalg.norm(Xt[:, c])
+                                        for c in range(nrhs)))
+        return r, X
+
+    one(m.FP32, verify=False)
+    rm, Xm = one(m.FP32)
+    one(m.FP64, verify=False)
+    rd, Xd = one(m.FP64)
+    ranks = [int(A.level_dims(l)[1].max()) for l in range(L + 1)]
+    A.close()
+    del dB, dX
+    h.trim()
+    out = {"workload": "N=%d bodies on mesh_sphere of radius sqrt(N/4pi), Helmholtz exp(-i d)/d diag 1/s s=0.1, "
+                       "theta=%g, leaf %d, operator eps %g (ID bases from a sketch of every far body, stored), "
+                       "preconditioner rank %d (complex) / %d samples, complex nrhs=%d, GMRES(%d) to %g; real "
+                       "symmetric form, 2N real unknowns" % (n, theta, leaf, eps, rank, samples, nrhs, a.inner, a.tol),
+           "n": n, "operator_build_s": op_s, "operator_max_rank_per_level_real": ranks,
+           "mixed_fp32_preconditioner": rm, "fp64_preconditioner": rd,
+           "mixed_vs_fp64_speedup": rd["total_ms"] / rm["total_ms"],
+           "x_mixed_vs_fp64_rel_max": float(max(np.linalg.norm(Xm[:, c] - Xd[:, c]) / np.linalg.norm(Xd[:, c])
+                                                for c in range(nrhs))),
+           "value": n * nrhs / (rm["total_ms"] / 1e3), "unit": "complex unknowns/s"}
+    log("helmholtz at N=%d: mixed %.1f ms (cycles %s), FP64 %.1f ms, dense residual %.2e"
+        % (n, rm["total_ms"], rm["cycles"], rd["total_ms"], rm["dense_resid_max"]))
+    return out
+
+
 def run_ours(a):
     import numpy as np
     import torch
@@ -944,6 +1036,16 @@ def run_ours(a):
         h.trim()
         torch.cuda.empty_cache()
 
+    helm = None
+    if a.helm_n > 0 and rank == 0:
+        try:
+            helm = run_helmholtz(a, h)
+        except Exception as e:
+            helm = {"error": "%s: %s" % (type(e).__name__, e)}
+            log("helmholtz failed: %s" % helm["error"])
+        h.trim()
+        torch.cuda.empty_cache()
+
     serving = None
     if a.serving_requests > 0:
         try:
@@ -1001,6 +1103,7 @@ def run_ours(a):
             "diag1": diag1,
             "uneven_batching_c3": c3,
             "scale_up_c5": c5,
+            "helmholtz_default_scaled": helm,
             "gpu_at_cpu_sample": small,
             "serving": serving,
             "cpu_baseline": cpu,
