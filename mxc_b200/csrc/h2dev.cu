@@ -272,8 +272,12 @@ struct DVec {
     if (v.empty()) return;
     if (owner && g_cur == owner)
       stage_copy(g_cur, p, v.data(), v.size() * sizeof(T));
-    else
+    else {
+      // From pageable memory cudaMemcpy may return before its DMA lands;
+      // wait for it so that work on any stream sees the data.
       ck(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+      ck(cudaStreamSynchronize(cudaStreamLegacy), "upload sync");
+    }
   }
   std::vector<T> download(cudaStream_t st) const {
     std::vector<T> v(n);
@@ -2579,7 +2583,8 @@ static void gmres_step(SolverBase& A, SolverBase& M, GmresState& g, i64 i, cudaS
   ck(launch_dots(g.w.p, 0, 1, g.w.p, g.N, nr, g.partial.p, g.nch, g.nrm2.p, st), "dots");
   ck(launch_scale_by_norm(g.w.p, g.V.p + (i + 1) * g.vstride, g.nrm2.p, hcol + i + 1, hstride, g.N, nr, st), "scale");
   if (g.early)
-    ck(launch_gmres_estimate(g.H.p, g.ldh, (int)g.inner, (int)i, g.beta.p, g.normb.p, g.act.p, nr, g.tol, g.ctl.p,
+    ck(launch_gmres_estimate(g.H.p, g.ldh, (int)g.inner, (int)i, g.beta.p, g.resh.p, g.it.p, (int)g.outer, g.act.p,
+                             nr, g.tol, g.ctl.p,
                              st),
        "estimate");
 }
@@ -3395,8 +3400,11 @@ int h2dev_dense_matvec(h2dev_handle_t h, int kernel, double singularity, double 
   db.upload(std::vector<double>(bodies, bodies + 3 * n));
   dx.alloc((size_t)len * nrhs);
   dy.alloc((size_t)len * nrhs);
-  ck(cudaMemcpy2D(dx.p, sizeof(double) * len, X, sizeof(double) * ld, sizeof(double) * len, nrhs,
-                  cudaMemcpyHostToDevice), "H2D");
+  // On the handle's (non-blocking) stream: a plain cudaMemcpy from pageable
+  // memory may return before its DMA lands, so the kernels below would not be
+  // ordered after it.
+  ck(cudaMemcpy2DAsync(dx.p, sizeof(double) * len, X, sizeof(double) * ld, sizeof(double) * len, nrhs,
+                       cudaMemcpyHostToDevice, h->stream), "H2D");
   if (helm) {
     // K X = S conj(X) over the tagged real-form bodies (2n unknowns).
     DVec<double> eb;

@@ -279,8 +279,9 @@ cudaError_t launch_dots_strided(const double* V, i64 vstride, int kvec, const do
 cudaError_t launch_gmres_init(int* act, int* it, double* resh, int outer, double tol, int nrhs, int* ctl,
                               cudaStream_t st);
 cudaError_t launch_gmres_cycle_begin(int* ctl, int inner, cudaStream_t st);
-cudaError_t launch_gmres_estimate(const double* H, int ldh, int inner, int i, const double* beta, const double* normb,
-                                  const int* act, int nrhs, double tol, int* ctl, cudaStream_t st);
+cudaError_t launch_gmres_estimate(const double* H, int ldh, int inner, int i, const double* beta, const double* resh,
+                                  const int* it, int outer, const int* act, int nrhs, double tol, int* ctl,
+                                  cudaStream_t st);
 cudaError_t launch_gmres_cycle_end(const double* rvec, int* act, int* it, double* resh, int outer, double tol,
                                    int nrhs, int* ctl, cudaStream_t st);
 // Conditional node value of a captured graph = (*word != 0) xor invert.
