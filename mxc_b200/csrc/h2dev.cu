@@ -2552,6 +2552,11 @@ struct GmresState {
   int ldh = 0, nch = 0;
   double tol = 0.;
   int early = 0;
+  // Complex GMRES (Helmholtz): vectors of N / 2 complex entries (interleaved),
+  // complex H and y; the operator and preconditioner act on the real form,
+  // so a vector is conjugated before each matvec and after each
+  // preconditioner solve (S conj(x) = K x, S_M^-1 y = conj(M^-1 y)).
+  int cplx = 0;
   DVec<double> V, w, R, Bc, X, H, y, beta, nrm2, partial, normb, rvec, resh;
   DVec<int> act, it, ctl;  // ctl: used, stop, cycles
 };
@@ -2560,6 +2565,7 @@ static void gmres_prologue(SolverBase& M, GmresState& g, cudaStream_t st) {
   const int nr = (int)g.nrhs;
   ck(launch_gmres_cycle_begin(g.ctl.p, (int)g.inner, st), "cycle begin");
   M.precondition(g.nrhs, g.R.p, g.N);
+  if (g.cplx) ck(launch_conj_interleaved(g.R.p, g.N, g.N, nr, st), "conj");
   ck(launch_dots(g.R.p, 0, 1, g.R.p, g.N, nr, g.partial.p, g.nch, g.nrm2.p, st), "dots");
   ck(launch_scale_by_norm(g.R.p, g.V.p, g.nrm2.p, g.beta.p, 1, g.N, nr, st), "v0");
   ck(cudaMemsetAsync(g.H.p, 0, sizeof(double) * g.H.n, st), "H=0");
@@ -2567,34 +2573,60 @@ static void gmres_prologue(SolverBase& M, GmresState& g, cudaStream_t st) {
 
 static void gmres_step(SolverBase& A, SolverBase& M, GmresState& g, i64 i, cudaStream_t st) {
   const int nr = (int)g.nrhs, kv = (int)i + 1;
-  const i64 hstride = (i64)g.ldh * g.inner;
+  const int cw = g.cplx ? 2 : 1;  // doubles per H entry
+  const i64 hstride = (i64)cw * g.ldh * g.inner;
   ck(cudaMemcpyAsync(g.w.p, g.V.p + i * g.vstride, sizeof(double) * g.vstride, cudaMemcpyDeviceToDevice, st), "w=v");
+  if (g.cplx) ck(launch_conj_interleaved(g.w.p, g.N, g.N, nr, st), "conj");
   A.matvec(g.nrhs, g.w.p, g.N);
   M.precondition(g.nrhs, g.w.p, g.N);
-  double* hcol = g.H.p + i * g.ldh;  // H[:, i] of rhs c at hcol + c * hstride
+  if (g.cplx) ck(launch_conj_interleaved(g.w.p, g.N, g.N, nr, st), "conj");
+  double* hcol = g.H.p + (i64)cw * i * g.ldh;  // H[:, i] of rhs c at hcol + c * hstride
   {
     Prof pf("gmres_dots", 2. * g.N * kv * nr, 8. * (kv + 1) * g.N * nr);
-    ck(launch_dots_strided(g.V.p, g.vstride, kv, g.w.p, g.N, nr, g.partial.p, g.nch, hcol, hstride, st), "dots");
+    if (g.cplx)
+      ck(launch_cdots_strided(g.V.p, g.vstride, kv, g.w.p, g.N / 2, nr, g.partial.p, cdots_chunks(g.N / 2), hcol,
+                              hstride, st),
+         "dots");
+    else
+      ck(launch_dots_strided(g.V.p, g.vstride, kv, g.w.p, g.N, nr, g.partial.p, g.nch, hcol, hstride, st), "dots");
   }
   {
     Prof pf("gmres_gs_update", 2. * g.N * kv * nr, 8. * (kv + 2) * g.N * nr);
-    ck(launch_gs_update(g.w.p, g.V.p, g.vstride, hcol, hstride, kv, g.N, nr, -1.0, nullptr, st), "gs");
+    if (g.cplx)
+      ck(launch_cgs_update(g.w.p, g.V.p, g.vstride, hcol, hstride, kv, g.N / 2, nr, -1.0, nullptr, st), "gs");
+    else
+      ck(launch_gs_update(g.w.p, g.V.p, g.vstride, hcol, hstride, kv, g.N, nr, -1.0, nullptr, st), "gs");
   }
   ck(launch_dots(g.w.p, 0, 1, g.w.p, g.N, nr, g.partial.p, g.nch, g.nrm2.p, st), "dots");
-  ck(launch_scale_by_norm(g.w.p, g.V.p + (i + 1) * g.vstride, g.nrm2.p, hcol + i + 1, hstride, g.N, nr, st), "scale");
-  if (g.early)
-    ck(launch_gmres_estimate(g.H.p, g.ldh, (int)g.inner, (int)i, g.beta.p, g.resh.p, g.it.p, (int)g.outer, g.act.p,
-                             nr, g.tol, g.ctl.p,
-                             st),
-       "estimate");
+  // H[i + 1][i] = ||w|| (real; its imaginary part stays zero from the cycle's memset)
+  ck(launch_scale_by_norm(g.w.p, g.V.p + (i + 1) * g.vstride, g.nrm2.p, hcol + cw * (i + 1), hstride, g.N, nr, st),
+     "scale");
+  if (g.early) {
+    if (g.cplx)
+      ck(launch_cgmres_estimate(g.H.p, g.ldh, (int)g.inner, (int)i, g.beta.p, g.resh.p, g.it.p, (int)g.outer,
+                                g.act.p, nr, g.tol, g.ctl.p, st),
+         "estimate");
+    else
+      ck(launch_gmres_estimate(g.H.p, g.ldh, (int)g.inner, (int)i, g.beta.p, g.resh.p, g.it.p, (int)g.outer, g.act.p,
+                               nr, g.tol, g.ctl.p, st),
+         "estimate");
+  }
 }
 
 static void gmres_epilogue(SolverBase& A, GmresState& g, int graph, cudaGraphConditionalHandle hw, cudaStream_t st) {
   const int nr = (int)g.nrhs;
-  ck(launch_gmres_ls(g.H.p, g.ldh, (int)g.inner, g.beta.p, g.y.p, nr, st, g.ctl.p), "ls");
-  ck(launch_gs_update(g.X.p, g.V.p, g.vstride, g.y.p, g.inner, (int)g.inner, g.N, nr, 1.0, g.act.p, st, g.ctl.p),
-     "x update");
+  if (g.cplx) {
+    ck(launch_cgmres_ls(g.H.p, g.ldh, (int)g.inner, g.beta.p, g.y.p, nr, st, g.ctl.p), "ls");
+    ck(launch_cgs_update(g.X.p, g.V.p, g.vstride, g.y.p, 2 * g.inner, (int)g.inner, g.N / 2, nr, 1.0, g.act.p, st,
+                         g.ctl.p),
+       "x update");
+  } else {
+    ck(launch_gmres_ls(g.H.p, g.ldh, (int)g.inner, g.beta.p, g.y.p, nr, st, g.ctl.p), "ls");
+    ck(launch_gs_update(g.X.p, g.V.p, g.vstride, g.y.p, g.inner, (int)g.inner, g.N, nr, 1.0, g.act.p, st, g.ctl.p),
+       "x update");
+  }
   ck(cudaMemcpyAsync(g.R.p, g.X.p, sizeof(double) * g.vstride, cudaMemcpyDeviceToDevice, st), "R=X");
+  if (g.cplx) ck(launch_conj_interleaved(g.R.p, g.N, g.N, nr, st), "conj");
   A.matvec(g.nrhs, g.R.p, g.N);
   ck(launch_axpby(g.R.p, g.Bc.p, -1.0, 1.0, g.vstride, st), "R=B-AX");
   ck(launch_dots(g.R.p, 0, 1, g.R.p, g.N, nr, g.partial.p, g.nch, g.nrm2.p, st), "dots");
@@ -2733,8 +2765,9 @@ static void gmres_alloc(GmresState& g, cudaStream_t st) {
   g.R.alloc(g.vstride);
   g.Bc.alloc(g.vstride);
   g.X.alloc(g.vstride);
-  g.H.alloc((size_t)g.ldh * inner * nrhs);
-  g.y.alloc((size_t)inner * nrhs);
+  const size_t cw = g.cplx ? 2 : 1;
+  g.H.alloc(cw * g.ldh * inner * nrhs);
+  g.y.alloc(cw * inner * nrhs);
   g.beta.alloc(nrhs);
   g.nrm2.alloc(nrhs);
   g.normb.alloc(nrhs);
@@ -2743,13 +2776,14 @@ static void gmres_alloc(GmresState& g, cudaStream_t st) {
   g.act.alloc(nrhs);
   g.it.alloc(nrhs);
   g.ctl.alloc(4);
-  g.partial.alloc((size_t)g.nch * (inner + 1) * nrhs);
+  g.partial.alloc(cw * g.nch * (inner + 1) * nrhs);
   g.y.zero(st);
 }
 
 static int gmres(SolverBase& A, SolverBase& M, double tol, i64 nrhs, double* dX, const double* dB, i64 ld, i64 inner,
                  i64 outer, int early_exit, double* resid, i64* iters) {
   require(A.lenX() == M.lenX(), "gmres: A and M sizes differ");
+  require(A.complex_form == M.complex_form, "gmres: operator and preconditioner kernels differ in kind");
   require(inner >= 1 && inner <= 16 && outer >= 0 && nrhs >= 1, "gmres: inner must be in [1,16]");
   cudaStream_t st = A.h->stream;
   const int nr = (int)nrhs;
@@ -2791,6 +2825,7 @@ static int gmres(SolverBase& A, SolverBase& M, double tol, i64 nrhs, double* dX,
     g.vstride = g.N * nrhs;
     g.tol = tol;
     g.early = early;
+    g.cplx = A.complex_form ? 1 : 0;
     g.nch = dots_chunks(g.N);
     gmres_alloc(g, st);
   }
@@ -3282,13 +3317,9 @@ int h2dev_solve_gmres_device(h2dev_solver_t A, h2dev_solver_t M, double tol, int
   require(ld >= A->impl->lenX(), "bad ld");
   require(A->impl->complex_form == M->impl->complex_form, "operator and preconditioner kernels differ in kind");
   CurHandle ch(A->impl->h);
-  // Helmholtz: GMRES on S y = B with y = conj(X) (S conj(x) = K x).
-  const bool cf = A->impl->complex_form;
-  cudaStream_t st = A->impl->h->stream;
-  if (cf) ck(launch_conj_interleaved(dX, A->impl->lenX(), ld, (int)nrhs, st), "conj");
-  int rc = gmres(*A->impl, *M->impl, tol, nrhs, dX, dB, ld, inner, outer, early_exit, resid, iters);
-  if (cf) ck(launch_conj_interleaved(dX, A->impl->lenX(), ld, (int)nrhs, st), "conj");
-  return rc;
+  // Helmholtz: complex GMRES on K x = B (vectors conjugated around each
+  // real-form matvec and preconditioner solve inside).
+  return gmres(*A->impl, *M->impl, tol, nrhs, dX, dB, ld, inner, outer, early_exit, resid, iters);
   H2_API_END
 }
 
@@ -3309,9 +3340,7 @@ int h2dev_solve_gmres(h2dev_solver_t A, h2dev_solver_t M, double tol, int64_t nr
                        cudaMemcpyHostToDevice, st), "H2D");
   ck(cudaMemcpy2DAsync(dB.p, sizeof(double) * n, B, sizeof(double) * ld, sizeof(double) * n, nrhs,
                        cudaMemcpyHostToDevice, st), "H2D");
-  if (a->complex_form) ck(launch_conj_interleaved(dX.p, n, n, (int)nrhs, st), "conj");
   int rc = gmres(*a, *M->impl, tol, nrhs, dX.p, dB.p, n, inner, outer, early_exit, resid, iters);
-  if (a->complex_form) ck(launch_conj_interleaved(dX.p, n, n, (int)nrhs, st), "conj");
   ck(cudaMemcpy2DAsync(X, sizeof(double) * ld, dX.p, sizeof(double) * n, sizeof(double) * n, nrhs,
                        cudaMemcpyDeviceToHost, st), "D2H");
   ck(cudaStreamSynchronize(st), "sync");

@@ -206,6 +206,173 @@ cudaError_t launch_gmres_ls(const double* H, int ld, int inner, const double* be
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------ complex GMRES
+// The same Arnoldi process on complex vectors (Helmholtz), each column n
+// complex values stored as 2n interleaved doubles: inner products are
+// v^H w (the reference's adjoint, solver.cpp:177), the Hessenberg matrix and
+// its least-squares solution are complex (interleaved pairs), norms are the
+// real norms of the 2n doubles.
+
+// partial[((g * kvec + j) * nrhs + c) * 2 + {0, 1}] = Re / Im of sum over the
+// chunk's complex rows of conj(V_j[:, c]) * w[:, c]
+__global__ void __launch_bounds__(DOT_THREADS) k_cdots_partial(const double* __restrict__ V, i64 vstride, int kvec,
+                                                               const double* __restrict__ w, i64 nc, int nrhs,
+                                                               double* __restrict__ partial) {
+  __shared__ double red[32];
+  const int g = blockIdx.x, c = blockIdx.y;
+  const i64 r0 = (i64)g * DOT_ROWS;
+  const i64 r1 = r0 + DOT_ROWS < nc ? r0 + DOT_ROWS : nc;
+  const double2* wc = reinterpret_cast<const double2*>(w) + (i64)c * nc;
+  for (int j = 0; j < kvec; j++) {
+    const double2* vc = reinterpret_cast<const double2*>(V + (i64)j * vstride) + (i64)c * nc;
+    double sr = 0., si = 0.;
+    for (i64 r = r0 + threadIdx.x; r < r1; r += DOT_THREADS) {
+      const double2 a = vc[r], b = wc[r];
+      sr += a.x * b.x + a.y * b.y;
+      si += a.x * b.y - a.y * b.x;
+    }
+    sr = BlockReduce<double>::sum(sr, red);
+    si = BlockReduce<double>::sum(si, red);
+    if (threadIdx.x == 0) {
+      partial[(((i64)g * kvec + j) * nrhs + c) * 2] = sr;
+      partial[(((i64)g * kvec + j) * nrhs + c) * 2 + 1] = si;
+    }
+  }
+}
+
+__global__ void k_cdots_final(const double* __restrict__ partial, int nchunks, int kvec, int nrhs,
+                              double* __restrict__ out, i64 ostride) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= kvec * nrhs) return;
+  int j = idx / nrhs, c = idx % nrhs;
+  double sr = 0., si = 0.;
+  for (int g = 0; g < nchunks; g++) {
+    sr += partial[(((i64)g * kvec + j) * nrhs + c) * 2];
+    si += partial[(((i64)g * kvec + j) * nrhs + c) * 2 + 1];
+  }
+  out[(i64)c * ostride + 2 * j] = sr;  // rhs c's kvec complex dots at out + c * ostride
+  out[(i64)c * ostride + 2 * j + 1] = si;
+}
+
+int cdots_chunks(i64 nc) { return (int)((nc + DOT_ROWS - 1) / DOT_ROWS); }
+
+cudaError_t launch_cdots_strided(const double* V, i64 vstride, int kvec, const double* w, i64 nc, int nrhs,
+                                 double* partial, int nchunks, double* out, i64 ostride, cudaStream_t st) {
+  if ((reinterpret_cast<uintptr_t>(V) | reinterpret_cast<uintptr_t>(w)) & 15 || vstride % 2) return cudaErrorInvalidValue;
+  dim3 grid(nchunks, nrhs);
+  note_launch();
+  k_cdots_partial<<<grid, DOT_THREADS, 0, st>>>(V, vstride, kvec, w, nc, nrhs, partial);
+  int tot = kvec * nrhs;
+  note_launch();
+  k_cdots_final<<<(tot + 127) / 128, 128, 0, st>>>(partial, nchunks, kvec, nrhs, out, ostride);
+  return cudaGetLastError();
+}
+
+// w[:, c] += sign * sum_j V_j[:, c] * h_j  (complex; h_j at h + c * hstride + 2 j)
+__global__ void k_cgs_update(double* __restrict__ w, const double* __restrict__ V, i64 vstride,
+                             const double* __restrict__ h, i64 hstride, int kvec, i64 nc, int nrhs, double sign,
+                             const int* __restrict__ active, const int* __restrict__ kdev) {
+  const int c = blockIdx.y;
+  if (active && !active[c]) return;
+  if (kdev) kvec = *kdev;
+  const double* hc = h + (i64)c * hstride;
+  double2* wc = reinterpret_cast<double2*>(w) + (i64)c * nc;
+  for (i64 r = (i64)blockIdx.x * blockDim.x + threadIdx.x; r < nc; r += (i64)gridDim.x * blockDim.x) {
+    double sr = 0., si = 0.;
+    for (int j = 0; j < kvec; j++) {
+      const double2 v = reinterpret_cast<const double2*>(V + (i64)j * vstride)[(i64)c * nc + r];
+      const double hr = hc[2 * j], hi = hc[2 * j + 1];
+      sr += v.x * hr - v.y * hi;
+      si += v.x * hi + v.y * hr;
+    }
+    double2 o = wc[r];
+    o.x += sign * sr;
+    o.y += sign * si;
+    wc[r] = o;
+  }
+}
+
+cudaError_t launch_cgs_update(double* w, const double* V, i64 vstride, const double* h, i64 hstride, int kvec, i64 nc,
+                              int nrhs, double sign, const int* active, cudaStream_t st, const int* kdev) {
+  if ((reinterpret_cast<uintptr_t>(V) | reinterpret_cast<uintptr_t>(w)) & 15 || vstride % 2) return cudaErrorInvalidValue;
+  int gx = (int)((nc + 255) / 256);
+  gx = gx > 1024 ? 1024 : gx;
+  dim3 grid(gx, nrhs);
+  note_launch();
+  k_cgs_update<<<grid, 256, 0, st>>>(w, V, vstride, h, hstride, kvec, nc, nrhs, sign, active, kdev);
+  return cudaGetLastError();
+}
+
+// Complex Givens reduction of the (cols + 1) x cols upper Hessenberg H
+// (interleaved, leading dimension ldh) against beta e1: rotation k maps
+// (a, b) = (H[k][k], H[k+1][k]) to (r a / |a|, 0) with c = |a| / r real and
+// s = (a / |a|) conj(b) / r.  Leaves R in H, the rotated right-hand side in
+// s (cols + 1 entries; |s[cols]| is the residual norm of the least-squares
+// problem min || beta e1 - H y ||).
+__device__ void cgivens_reduce(double2* H, int ldh, int cols, double beta, double2* s) {
+  for (int r = 0; r <= cols; r++) s[r] = make_double2(0., 0.);
+  s[0].x = beta;
+  for (int k = 0; k < cols; k++) {
+    const double2 a = H[k + k * ldh], b = H[k + 1 + k * ldh];
+    const double na = hypot(a.x, a.y), nb = hypot(b.x, b.y);
+    const double r = hypot(na, nb);
+    if (r == 0.) continue;
+    double cs;
+    double2 sn;
+    if (na == 0.) {
+      cs = 0.;
+      sn = make_double2(b.x / nb, -b.y / nb);  // conj(b) / |b|
+    } else {
+      cs = na / r;
+      const double2 u = make_double2(a.x / na, a.y / na);  // a / |a|
+      // u * conj(b) / r
+      sn = make_double2((u.x * b.x + u.y * b.y) / r, (u.y * b.x - u.x * b.y) / r);
+    }
+    auto rot = [&](double2& x, double2& y) {
+      // x' = c x + s y;  y' = -conj(s) x + c y
+      const double2 xs = make_double2(cs * x.x + sn.x * y.x - sn.y * y.y, cs * x.y + sn.x * y.y + sn.y * y.x);
+      const double2 ys = make_double2(-(sn.x * x.x + sn.y * x.y) + cs * y.x, -(sn.x * x.y - sn.y * x.x) + cs * y.y);
+      x = xs;
+      y = ys;
+    };
+    for (int j = k; j < cols; j++) rot(H[k + j * ldh], H[k + 1 + j * ldh]);
+    rot(s[k], s[k + 1]);
+  }
+}
+
+// min || beta e1 - H y || per rhs (complex H, inner columns, or *used).
+__global__ void k_cgmres_ls(const double* __restrict__ Hall, int ld, int inner, const double* __restrict__ beta,
+                            double* __restrict__ yall, int nrhs, const int* __restrict__ used) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nrhs) return;
+  const i64 hstride = 2 * (i64)ld * inner;
+  if (used) inner = *used;
+  if (ld > 17 || inner > 16) return;
+  double2 H[17 * 16], s[17];
+  const double2* Hc = reinterpret_cast<const double2*>(Hall + (i64)c * hstride);
+  for (int i = 0; i < ld * inner; i++) H[i] = Hc[i];
+  cgivens_reduce(H, ld, inner, beta[c], s);
+  double2* y = reinterpret_cast<double2*>(yall + (i64)c * (hstride / ld));
+  for (int i = inner - 1; i >= 0; i--) {
+    double2 t = s[i];
+    for (int j = i + 1; j < inner; j++) {
+      const double2 h = H[i + j * ld], v = y[j];
+      t.x -= h.x * v.x - h.y * v.y;
+      t.y -= h.x * v.y + h.y * v.x;
+    }
+    const double2 d = H[i + i * ld];
+    const double dn = d.x * d.x + d.y * d.y;
+    y[i] = dn != 0. ? make_double2((t.x * d.x + t.y * d.y) / dn, (t.y * d.x - t.x * d.y) / dn) : make_double2(0., 0.);
+  }
+}
+
+cudaError_t launch_cgmres_ls(const double* H, int ld, int inner, const double* beta, double* y, int nrhs,
+                             cudaStream_t st, const int* used) {
+  note_launch();
+  k_cgmres_ls<<<(nrhs + 31) / 32, 32, 0, st>>>(H, ld, inner, beta, y, nrhs, used);
+  return cudaGetLastError();
+}
+
 // y = a * y + b * x
 __global__ void k_axpby(double* __restrict__ y, const double* __restrict__ x, double a, double b, i64 n) {
   for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (i64)gridDim.x * blockDim.x)
@@ -313,6 +480,31 @@ __global__ void k_gmres_estimate(const double* __restrict__ Hall, int ldh, int i
   }
 }
 
+// k_gmres_estimate for complex H (interleaved pairs).
+__global__ void k_cgmres_estimate(const double* __restrict__ Hall, int ldh, int inner, int i,
+                                  const double* __restrict__ beta, const double* __restrict__ resh,
+                                  const int* __restrict__ it, int outer, const int* __restrict__ act, int nrhs,
+                                  double tol, int* __restrict__ ctl) {
+  int ok = 1;
+  for (int c = threadIdx.x; c < nrhs; c += blockDim.x) {
+    if (!act[c]) continue;
+    const double2* Hc = reinterpret_cast<const double2*>(Hall + (i64)c * 2 * ldh * inner);
+    const int rows = i + 2, cols = i + 1;
+    double2 H[17 * 16], s[17];
+    for (int j = 0; j < cols; j++)
+      for (int r = 0; r < rows; r++) H[r + j * rows] = Hc[r + (i64)j * ldh];
+    cgivens_reduce(H, rows, cols, beta[c], s);
+    const double r0 = resh[(i64)c * (outer + 1) + it[c]];
+    const double est = beta[c] > 0. ? hypot(s[cols].x, s[cols].y) / beta[c] * r0 : 0.;
+    if (!(est < tol * 0.5)) ok = 0;
+  }
+  ok = __syncthreads_and(ok);
+  if (threadIdx.x == 0 && ok && !ctl[1]) {
+    ctl[0] = i + 1;
+    ctl[1] = 1;
+  }
+}
+
 // End of a cycle: record the true residual of every active column, retire
 // columns that converged or ran out of cycles; ctl[3] = another cycle
 // (any column active and fewer than `outer` cycles done).
@@ -358,6 +550,14 @@ cudaError_t launch_gmres_estimate(const double* H, int ldh, int inner, int i, co
   if (ldh > 17 || i + 2 > 17) return cudaErrorInvalidValue;
   note_launch();
   k_gmres_estimate<<<1, 32, 0, st>>>(H, ldh, inner, i, beta, resh, it, outer, act, nrhs, tol, ctl);
+  return cudaGetLastError();
+}
+cudaError_t launch_cgmres_estimate(const double* H, int ldh, int inner, int i, const double* beta, const double* resh,
+                                   const int* it, int outer, const int* act, int nrhs, double tol, int* ctl,
+                                   cudaStream_t st) {
+  if (ldh > 17 || i + 2 > 17) return cudaErrorInvalidValue;
+  note_launch();
+  k_cgmres_estimate<<<1, 32, 0, st>>>(H, ldh, inner, i, beta, resh, it, outer, act, nrhs, tol, ctl);
   return cudaGetLastError();
 }
 cudaError_t launch_gmres_cycle_end(const double* rvec, int* act, int* it, double* resh, int outer, double tol,

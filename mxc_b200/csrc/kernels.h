@@ -294,6 +294,17 @@ cudaError_t launch_gmres_ls(const double* H, int ld, int inner, const double* be
 cudaError_t launch_helm_expand(const double* bodies, i64 n, int comps, double* out, cudaStream_t st);
 // Complex conjugate of a column-major array of interleaved (re, im) pairs (n doubles per column).
 cudaError_t launch_conj_interleaved(double* X, i64 n, i64 ld, int nrhs, cudaStream_t st);
+// Complex GMRES (interleaved vectors of nc complex entries per column; H and y complex pairs).
+int cdots_chunks(i64 nc);
+cudaError_t launch_cdots_strided(const double* V, i64 vstride, int kvec, const double* w, i64 nc, int nrhs,
+                                 double* partial, int nchunks, double* out, i64 ostride, cudaStream_t st);
+cudaError_t launch_cgs_update(double* w, const double* V, i64 vstride, const double* h, i64 hstride, int kvec, i64 nc,
+                              int nrhs, double sign, const int* active, cudaStream_t st, const int* kdev = nullptr);
+cudaError_t launch_cgmres_ls(const double* H, int ld, int inner, const double* beta, double* y, int nrhs,
+                             cudaStream_t st, const int* used = nullptr);
+cudaError_t launch_cgmres_estimate(const double* H, int ldh, int inner, int i, const double* beta, const double* resh,
+                                   const int* it, int outer, const int* act, int nrhs, double tol, int* ctl,
+                                   cudaStream_t st);
 cudaError_t launch_axpby(double* y, const double* x, double a, double b, i64 n, cudaStream_t st);
 cudaError_t launch_residual_norm_finish(const double* nrm2, const double* normb, double* resid, int nrhs,
                                         cudaStream_t st);
