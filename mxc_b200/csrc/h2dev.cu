@@ -2603,12 +2603,12 @@ static void gmres_step(SolverBase& A, SolverBase& M, GmresState& g, i64 i, cudaS
      "scale");
   if (g.early) {
     if (g.cplx)
-      ck(launch_cgmres_estimate(g.H.p, g.ldh, (int)g.inner, (int)i, g.beta.p, g.resh.p, g.it.p, (int)g.outer,
-                                g.act.p, nr, g.tol, g.ctl.p, st),
+      ck(launch_cgmres_estimate(g.H.p, g.ldh, (int)g.inner, (int)i, g.beta.p, g.normb.p, g.act.p, nr, g.tol,
+                                g.ctl.p, st),
          "estimate");
     else
-      ck(launch_gmres_estimate(g.H.p, g.ldh, (int)g.inner, (int)i, g.beta.p, g.resh.p, g.it.p, (int)g.outer, g.act.p,
-                               nr, g.tol, g.ctl.p, st),
+      ck(launch_gmres_estimate(g.H.p, g.ldh, (int)g.inner, (int)i, g.beta.p, g.normb.p, g.act.p, nr, g.tol,
+                               g.ctl.p, st),
          "estimate");
   }
 }

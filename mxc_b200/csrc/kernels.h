@@ -279,9 +279,8 @@ cudaError_t launch_dots_strided(const double* V, i64 vstride, int kvec, const do
 cudaError_t launch_gmres_init(int* act, int* it, double* resh, int outer, double tol, int nrhs, int* ctl,
                               cudaStream_t st);
 cudaError_t launch_gmres_cycle_begin(int* ctl, int inner, cudaStream_t st);
-cudaError_t launch_gmres_estimate(const double* H, int ldh, int inner, int i, const double* beta, const double* resh,
-                                  const int* it, int outer, const int* act, int nrhs, double tol, int* ctl,
-                                  cudaStream_t st);
+cudaError_t launch_gmres_estimate(const double* H, int ldh, int inner, int i, const double* beta, const double* normb,
+                                  const int* act, int nrhs, double tol, int* ctl, cudaStream_t st);
 cudaError_t launch_gmres_cycle_end(const double* rvec, int* act, int* it, double* resh, int outer, double tol,
                                    int nrhs, int* ctl, cudaStream_t st);
 // Conditional node value of a captured graph = (*word != 0) xor invert.
@@ -302,9 +301,8 @@ cudaError_t launch_cgs_update(double* w, const double* V, i64 vstride, const dou
                               int nrhs, double sign, const int* active, cudaStream_t st, const int* kdev = nullptr);
 cudaError_t launch_cgmres_ls(const double* H, int ld, int inner, const double* beta, double* y, int nrhs,
                              cudaStream_t st, const int* used = nullptr);
-cudaError_t launch_cgmres_estimate(const double* H, int ldh, int inner, int i, const double* beta, const double* resh,
-                                   const int* it, int outer, const int* act, int nrhs, double tol, int* ctl,
-                                   cudaStream_t st);
+cudaError_t launch_cgmres_estimate(const double* H, int ldh, int inner, int i, const double* beta, const double* normb,
+                                   const int* act, int nrhs, double tol, int* ctl, cudaStream_t st);
 cudaError_t launch_axpby(double* y, const double* x, double a, double b, i64 n, cudaStream_t st);
 cudaError_t launch_residual_norm_finish(const double* nrm2, const double* normb, double* resid, int nrhs,
                                         cudaStream_t st);
