@@ -2557,13 +2557,20 @@ struct GmresState {
   // so a vector is conjugated before each matvec and after each
   // preconditioner solve (S conj(x) = K x, S_M^-1 y = conj(M^-1 y)).
   int cplx = 0;
-  DVec<double> V, w, R, Bc, X, H, y, beta, nrm2, partial, normb, rvec, resh;
-  DVec<int> act, it, ctl;  // ctl: used, stop, cycles
+  // With early exit: residual by recurrence.  A v_i is kept for every
+  // Arnoldi vector (AV) and the cycle's starting residual (Rr), so the new
+  // residual is Rr - AV y without a matvec; the true residual B - A X is
+  // computed only to certify a column below tol (or on its last cycle), and
+  // a column that fails it continues from the true residual.
+  int rec = 0;
+  DVec<double> V, w, R, Bc, X, H, y, beta, nrm2, partial, normb, rvec, resh, AV, Rr;
+  DVec<int> act, it, ctl;  // ctl: used, stop, cycles, another cycle, need true residual
 };
 
 static void gmres_prologue(SolverBase& M, GmresState& g, cudaStream_t st) {
   const int nr = (int)g.nrhs;
   ck(launch_gmres_cycle_begin(g.ctl.p, (int)g.inner, st), "cycle begin");
+  if (g.rec) ck(cudaMemcpyAsync(g.Rr.p, g.R.p, sizeof(double) * g.vstride, cudaMemcpyDeviceToDevice, st), "Rr=R");
   M.precondition(g.nrhs, g.R.p, g.N);
   if (g.cplx) ck(launch_conj_interleaved(g.R.p, g.N, g.N, nr, st), "conj");
   ck(launch_dots(g.R.p, 0, 1, g.R.p, g.N, nr, g.partial.p, g.nch, g.nrm2.p, st), "dots");
@@ -2578,6 +2585,9 @@ static void gmres_step(SolverBase& A, SolverBase& M, GmresState& g, i64 i, cudaS
   ck(cudaMemcpyAsync(g.w.p, g.V.p + i * g.vstride, sizeof(double) * g.vstride, cudaMemcpyDeviceToDevice, st), "w=v");
   if (g.cplx) ck(launch_conj_interleaved(g.w.p, g.N, g.N, nr, st), "conj");
   A.matvec(g.nrhs, g.w.p, g.N);
+  if (g.rec)
+    ck(cudaMemcpyAsync(g.AV.p + i * g.vstride, g.w.p, sizeof(double) * g.vstride, cudaMemcpyDeviceToDevice, st),
+       "AV");
   M.precondition(g.nrhs, g.w.p, g.N);
   if (g.cplx) ck(launch_conj_interleaved(g.w.p, g.N, g.N, nr, st), "conj");
   double* hcol = g.H.p + (i64)cw * i * g.ldh;  // H[:, i] of rhs c at hcol + c * hstride
@@ -2613,7 +2623,21 @@ static void gmres_step(SolverBase& A, SolverBase& M, GmresState& g, i64 i, cudaS
   }
 }
 
-static void gmres_epilogue(SolverBase& A, GmresState& g, int graph, cudaGraphConditionalHandle hw, cudaStream_t st) {
+// rvec = || B - A X || / || B || per column (the reference's restart
+// residual, solver.cpp:192-200).
+static void gmres_true_residual(SolverBase& A, GmresState& g, cudaStream_t st) {
+  const int nr = (int)g.nrhs;
+  ck(cudaMemcpyAsync(g.R.p, g.X.p, sizeof(double) * g.vstride, cudaMemcpyDeviceToDevice, st), "R=X");
+  if (g.cplx) ck(launch_conj_interleaved(g.R.p, g.N, g.N, nr, st), "conj");
+  A.matvec(g.nrhs, g.R.p, g.N);
+  ck(launch_axpby(g.R.p, g.Bc.p, -1.0, 1.0, g.vstride, st), "R=B-AX");
+  ck(launch_dots(g.R.p, 0, 1, g.R.p, g.N, nr, g.partial.p, g.nch, g.nrm2.p, st), "dots");
+  ck(launch_residual_norm_finish(g.nrm2.p, g.normb.p, g.rvec.p, nr, st), "resid");
+}
+
+// child: a stream for capturing the true-residual IF node (graph mode).
+static void gmres_epilogue(SolverBase& A, GmresState& g, int graph, cudaGraphConditionalHandle hw, cudaStream_t st,
+                           cudaStream_t child = nullptr) {
   const int nr = (int)g.nrhs;
   if (g.cplx) {
     ck(launch_cgmres_ls(g.H.p, g.ldh, (int)g.inner, g.beta.p, g.y.p, nr, st, g.ctl.p), "ls");
@@ -2625,12 +2649,54 @@ static void gmres_epilogue(SolverBase& A, GmresState& g, int graph, cudaGraphCon
     ck(launch_gs_update(g.X.p, g.V.p, g.vstride, g.y.p, g.inner, (int)g.inner, g.N, nr, 1.0, g.act.p, st, g.ctl.p),
        "x update");
   }
-  ck(cudaMemcpyAsync(g.R.p, g.X.p, sizeof(double) * g.vstride, cudaMemcpyDeviceToDevice, st), "R=X");
-  if (g.cplx) ck(launch_conj_interleaved(g.R.p, g.N, g.N, nr, st), "conj");
-  A.matvec(g.nrhs, g.R.p, g.N);
-  ck(launch_axpby(g.R.p, g.Bc.p, -1.0, 1.0, g.vstride, st), "R=B-AX");
-  ck(launch_dots(g.R.p, 0, 1, g.R.p, g.N, nr, g.partial.p, g.nch, g.nrm2.p, st), "dots");
-  ck(launch_residual_norm_finish(g.nrm2.p, g.normb.p, g.rvec.p, nr, st), "resid");
+  if (!g.rec) {
+    gmres_true_residual(A, g, st);
+  } else {
+    // R = Rr - AV y (the columns that are done keep whatever R holds)
+    ck(cudaMemcpyAsync(g.R.p, g.Rr.p, sizeof(double) * g.vstride, cudaMemcpyDeviceToDevice, st), "R=Rr");
+    if (g.cplx)
+      ck(launch_cgs_update(g.R.p, g.AV.p, g.vstride, g.y.p, 2 * g.inner, (int)g.inner, g.N / 2, nr, -1.0, g.act.p, st,
+                           g.ctl.p),
+         "R update");
+    else
+      ck(launch_gs_update(g.R.p, g.AV.p, g.vstride, g.y.p, g.inner, (int)g.inner, g.N, nr, -1.0, g.act.p, st,
+                          g.ctl.p),
+         "R update");
+    ck(launch_dots(g.R.p, 0, 1, g.R.p, g.N, nr, g.partial.p, g.nch, g.nrm2.p, st), "dots");
+    ck(launch_residual_norm_finish(g.nrm2.p, g.normb.p, g.rvec.p, nr, st), "resid");
+    ck(launch_gmres_need_true(g.rvec.p, g.act.p, g.it.p, (int)g.outer, nr, g.tol, g.ctl.p, st), "need true");
+    if (graph) {
+      h2dev_handle_s* h = A.h;
+      cudaStreamCaptureStatus cs;
+      cudaGraph_t bg = nullptr;
+      const cudaGraphNode_t* deps = nullptr;
+      size_t ndeps = 0;
+      ck(cudaStreamGetCaptureInfo(st, &cs, nullptr, &bg, &deps, &ndeps), "capture info");
+      cudaGraphConditionalHandle hc;
+      ck(cudaGraphConditionalHandleCreate(&hc, bg, 0, 0), "conditional handle");
+      ck(launch_graph_condition(hc, g.ctl.p + 4, 0, st), "certify condition");
+      ck(cudaStreamGetCaptureInfo(st, &cs, nullptr, &bg, &deps, &ndeps), "capture info");
+      cudaGraphNodeParams ip = {};
+      ip.type = cudaGraphNodeTypeConditional;
+      ip.conditional.handle = hc;
+      ip.conditional.type = cudaGraphCondTypeIf;
+      ip.conditional.size = 1;
+      cudaGraphNode_t inode;
+      ck(cudaGraphAddNode(&inode, bg, deps, ndeps, &ip), "if node");
+      ck(cudaStreamUpdateCaptureDependencies(st, &inode, 1, cudaStreamSetCaptureDependencies), "capture deps");
+      h->stream = child;
+      ck(cudaStreamBeginCaptureToGraph(child, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                       cudaStreamCaptureModeRelaxed),
+         "certify capture");
+      gmres_true_residual(A, g, child);
+      cudaGraph_t done = nullptr;
+      ck(cudaStreamEndCapture(child, &done), "certify capture end");
+      h->stream = st;
+    } else {
+      std::vector<int> c5 = g.ctl.download(st);
+      if (c5[4]) gmres_true_residual(A, g, st);
+    }
+  }
   ck(launch_gmres_cycle_end(g.rvec.p, g.act.p, g.it.p, g.resh.p, (int)g.outer, g.tol, nr, g.ctl.p, st),
      "cycle end");
   if (graph) ck(launch_graph_condition(hw, g.ctl.p + 3, 0, st), "cycle condition");
@@ -2746,7 +2812,7 @@ static void gmres_graph(SolverBase& A, SolverBase& M, GmresState& g, SolveGraph&
     ck(cudaStreamEndCapture(ss, &done), "step capture end");
     h->stream = sb;
   }
-  gmres_epilogue(A, g, 1, hw, sb);
+  gmres_epilogue(A, g, 1, hw, sb, ss);
   cudaGraph_t bdone = nullptr;
   ck(cudaStreamEndCapture(sb, &bdone), "body capture end");
   h->stream = s0;
@@ -2775,7 +2841,11 @@ static void gmres_alloc(GmresState& g, cudaStream_t st) {
   g.resh.alloc((size_t)(outer + 1) * nrhs);
   g.act.alloc(nrhs);
   g.it.alloc(nrhs);
-  g.ctl.alloc(4);
+  g.ctl.alloc(5);
+  if (g.rec) {
+    g.AV.alloc((size_t)inner * g.vstride);
+    g.Rr.alloc(g.vstride);
+  }
   g.partial.alloc(cw * g.nch * (inner + 1) * nrhs);
   g.y.zero(st);
 }
@@ -2826,6 +2896,7 @@ static int gmres(SolverBase& A, SolverBase& M, double tol, i64 nrhs, double* dX,
     g.tol = tol;
     g.early = early;
     g.cplx = A.complex_form ? 1 : 0;
+    g.rec = early;
     g.nch = dots_chunks(g.N);
     gmres_alloc(g, st);
   }

@@ -525,6 +525,24 @@ __global__ void k_gmres_cycle_end(const double* __restrict__ rvec, int* __restri
   }
 }
 
+// ctl[4] = 1 when some active column's recurrence residual is below tol or
+// the column is on its last cycle: its true residual must be computed, to
+// certify convergence or to report the final residual.
+__global__ void k_gmres_need_true(const double* __restrict__ rvec, const int* __restrict__ act,
+                                  const int* __restrict__ it, int outer, int nrhs, double tol, int* __restrict__ ctl) {
+  int any = 0;
+  for (int c = threadIdx.x; c < nrhs; c += blockDim.x)
+    if (act[c] && (rvec[c] < tol || it[c] + 1 >= outer)) any = 1;
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) ctl[4] = any;
+}
+cudaError_t launch_gmres_need_true(const double* rvec, const int* act, const int* it, int outer, int nrhs, double tol,
+                                   int* ctl, cudaStream_t st) {
+  note_launch();
+  k_gmres_need_true<<<1, 128, 0, st>>>(rvec, act, it, outer, nrhs, tol, ctl);
+  return cudaGetLastError();
+}
+
 // Sets a conditional node's value from a control word: *word != 0 (or == 0
 // with invert).
 __global__ void k_graph_condition(cudaGraphConditionalHandle handle, const int* __restrict__ word, int invert) {

@@ -283,6 +283,9 @@ cudaError_t launch_gmres_estimate(const double* H, int ldh, int inner, int i, co
                                   const int* act, int nrhs, double tol, int* ctl, cudaStream_t st);
 cudaError_t launch_gmres_cycle_end(const double* rvec, int* act, int* it, double* resh, int outer, double tol,
                                    int nrhs, int* ctl, cudaStream_t st);
+// ctl[4] = some active column needs its true residual (recurrence residual below tol, or last cycle).
+cudaError_t launch_gmres_need_true(const double* rvec, const int* act, const int* it, int outer, int nrhs, double tol,
+                                   int* ctl, cudaStream_t st);
 // Conditional node value of a captured graph = (*word != 0) xor invert.
 cudaError_t launch_graph_condition(cudaGraphConditionalHandle handle, const int* word, int invert, cudaStream_t st);
 cudaError_t launch_scale_by_norm(const double* w, double* vout, const double* nrm2, double* hout, i64 hstride,
