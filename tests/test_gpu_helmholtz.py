@@ -175,3 +175,33 @@ def test_lorasp_default_run_is_helmholtz(tmp_path):
     res = float(re.search(r"GMRES Residual: ([-+0-9.eE]+)", out).group(1))
     assert cerr < 1e-9 and res < 1e-10
     assert len(csv.read_text().strip().split(",")) >= 26
+
+
+@pytest.mark.parametrize("theta_m, lrank", [(0.0, 0), (1.0, 10)])
+def test_hss_and_leveled_rank_vs_oracle(handle, helm_case, theta_m, lrank):
+    """The reference's HSS mode (preconditioner with theta 0, main.cpp:139-140)
+    and leveled ranks ((levels - l) * leveled_rank + rank, solver.cpp:29) with
+    the Helmholtz kernel: the preconditioner's ranks are twice the oracle's
+    complex ranks (real form), and GMRES reaches the oracle's solution in
+    about its restarts."""
+    c = helm_case
+    N = c["b"].shape[0]
+    k = m.Helmholtz3D(1.0, 0.1)
+    ko = O.Kernel(O.HELMHOLTZ, 0.1, 1.0)
+    cells = O.build_binary_tree(c["b"].copy(), c["L"])
+    Mo = O.H2MatrixSolver(ko, 0.0, c["rank"], lrank, cells, theta_m, clear_x_bit0(c["b"]), c["L"])
+    Mo.factorize()
+    xo, res_o, it_o = c["Ao"].solve_gmres(c["eps"], Mo, np.zeros(N, np.complex128), c["B"], 10, 50)
+    A = m.H2MatrixSolver(handle, k, c["eps"], c["rank"], 0, c["t"], c["theta"], c["b"])
+    M = m.H2MatrixSolver(handle, k, 0.0, c["rank"], lrank, c["t"], theta_m, c["b"])
+    for lvl in range(c["L"] + 1):
+        d, r = M.level_dims(lvl)
+        assert np.array_equal(r, np.minimum(2 * Mo.A[lvl].DimsLr, d)), lvl
+    M.factorizeM()
+    X = np.zeros(N, np.complex128)
+    rc = A.solveGMRES(c["eps"], M, X, c["B"], 10, 50)
+    assert rc == 0 and A.iters <= it_o + 1, (A.iters, it_o)
+    assert rel(X, xo) < 1e-8
+    assert rel(m.dense_matvec(handle, k, c["b"], X), c["B"]) <= 1e-10
+    A.close()
+    M.close()
