@@ -2562,79 +2562,17 @@ struct GmresState {
   // residual is Rr - AV y without a matvec; the true residual B - A X is
   // computed only to certify a column below tol (or on its last cycle), and
   // a column that fails it continues from the true residual.
-  //
-  // The next cycle's preconditioned residual then also comes without a
-  // preconditioner solve: M^-1 A V_k = V_{k+1} H_k, so M^-1 (Rr - AV y) =
-  // V_{k+1} (beta e1 - H y) (Zp); only a cycle that follows a true residual
-  // preconditions it.
   int rec = 0;
-  DVec<double> V, w, R, Bc, X, H, y, beta, nrm2, partial, normb, rvec, resh, AV, Rr, Zp, S;
-  DVec<int> act, it, ctl;  // ctl: used, stop, cycles, another cycle, true residual taken, used + 1
+  DVec<double> V, w, R, Bc, X, H, y, beta, nrm2, partial, normb, rvec, resh, AV, Rr;
+  DVec<int> act, it, ctl;  // ctl: used, stop, cycles, another cycle, need true residual
 };
 
-// Captures body(child) as the body of an IF node on *word (or !*word with
-// invert) of the graph st is capturing; the handle's stream points at the
-// child capture stream meanwhile.
-static void capture_if(h2dev_handle_s* h, cudaStream_t st, cudaStream_t child, const int* word, int invert,
-                       const std::function<void(cudaStream_t)>& body) {
-  cudaStreamCaptureStatus cs;
-  cudaGraph_t bg = nullptr;
-  const cudaGraphNode_t* deps = nullptr;
-  size_t ndeps = 0;
-  ck(cudaStreamGetCaptureInfo(st, &cs, nullptr, &bg, &deps, &ndeps), "capture info");
-  cudaGraphConditionalHandle hc;
-  ck(cudaGraphConditionalHandleCreate(&hc, bg, 0, 0), "conditional handle");
-  ck(launch_graph_condition(hc, word, invert, st), "condition");
-  ck(cudaStreamGetCaptureInfo(st, &cs, nullptr, &bg, &deps, &ndeps), "capture info");
-  cudaGraphNodeParams ip = {};
-  ip.type = cudaGraphNodeTypeConditional;
-  ip.conditional.handle = hc;
-  ip.conditional.type = cudaGraphCondTypeIf;
-  ip.conditional.size = 1;
-  cudaGraphNode_t inode;
-  ck(cudaGraphAddNode(&inode, bg, deps, ndeps, &ip), "if node");
-  ck(cudaStreamUpdateCaptureDependencies(st, &inode, 1, cudaStreamSetCaptureDependencies), "capture deps");
-  h->stream = child;
-  ck(cudaStreamBeginCaptureToGraph(child, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                   cudaStreamCaptureModeRelaxed),
-     "if capture");
-  body(child);
-  cudaGraph_t done = nullptr;
-  ck(cudaStreamEndCapture(child, &done), "if capture end");
-  h->stream = st;
-}
-
-// R <- M^-1 R (complex: conjugated back, S_M^-1 y = conj(M^-1 y)).
-static void gmres_precondition_r(SolverBase& M, GmresState& g, cudaStream_t st) {
-  M.precondition(g.nrhs, g.R.p, g.N);
-  if (g.cplx) ck(launch_conj_interleaved(g.R.p, g.N, g.N, (int)g.nrhs, st), "conj");
-}
-
-// child: a stream for capturing IF nodes (graph mode, recurrence on).
-static void gmres_prologue(SolverBase& M, GmresState& g, cudaStream_t st, int graph = 0,
-                           cudaStream_t child = nullptr) {
+static void gmres_prologue(SolverBase& M, GmresState& g, cudaStream_t st) {
   const int nr = (int)g.nrhs;
   ck(launch_gmres_cycle_begin(g.ctl.p, (int)g.inner, st), "cycle begin");
-  if (!g.rec) {
-    gmres_precondition_r(M, g, st);
-  } else {
-    ck(cudaMemcpyAsync(g.Rr.p, g.R.p, sizeof(double) * g.vstride, cudaMemcpyDeviceToDevice, st), "Rr=R");
-    // After a true residual (and in the first cycle) precondition it;
-    // otherwise the previous cycle left M^-1 R in Zp.
-    auto from_krylov = [&](cudaStream_t s) {
-      ck(cudaMemcpyAsync(g.R.p, g.Zp.p, sizeof(double) * g.vstride, cudaMemcpyDeviceToDevice, s), "R=Zp");
-    };
-    if (graph) {
-      capture_if(M.h, st, child, g.ctl.p + 4, 0, [&](cudaStream_t s) { gmres_precondition_r(M, g, s); });
-      capture_if(M.h, st, child, g.ctl.p + 4, 1, from_krylov);
-    } else {
-      std::vector<int> c = g.ctl.download(st);
-      if (c[4])
-        gmres_precondition_r(M, g, st);
-      else
-        from_krylov(st);
-    }
-  }
+  if (g.rec) ck(cudaMemcpyAsync(g.Rr.p, g.R.p, sizeof(double) * g.vstride, cudaMemcpyDeviceToDevice, st), "Rr=R");
+  M.precondition(g.nrhs, g.R.p, g.N);
+  if (g.cplx) ck(launch_conj_interleaved(g.R.p, g.N, g.N, nr, st), "conj");
   ck(launch_dots(g.R.p, 0, 1, g.R.p, g.N, nr, g.partial.p, g.nch, g.nrm2.p, st), "dots");
   ck(launch_scale_by_norm(g.R.p, g.V.p, g.nrm2.p, g.beta.p, 1, g.N, nr, st), "v0");
   ck(cudaMemsetAsync(g.H.p, 0, sizeof(double) * g.H.n, st), "H=0");
@@ -2726,21 +2664,34 @@ static void gmres_epilogue(SolverBase& A, GmresState& g, int graph, cudaGraphCon
          "R update");
     ck(launch_dots(g.R.p, 0, 1, g.R.p, g.N, nr, g.partial.p, g.nch, g.nrm2.p, st), "dots");
     ck(launch_residual_norm_finish(g.nrm2.p, g.normb.p, g.rvec.p, nr, st), "resid");
-    // Zp = V_{k+1} (beta e1 - H y): the next cycle's preconditioned residual
-    const int cw = g.cplx ? 2 : 1;
-    ck(launch_gmres_resvec(g.H.p, g.ldh, (int)g.inner, g.beta.p, g.y.p, g.act.p, nr, g.S.p, g.ctl.p, g.cplx, st),
-       "resvec");
-    ck(cudaMemsetAsync(g.Zp.p, 0, sizeof(double) * g.vstride, st), "Zp=0");
-    if (g.cplx)
-      ck(launch_cgs_update(g.Zp.p, g.V.p, g.vstride, g.S.p, (i64)cw * g.ldh, g.ldh, g.N / 2, nr, 1.0, g.act.p, st,
-                           g.ctl.p + 5),
-         "Zp");
-    else
-      ck(launch_gs_update(g.Zp.p, g.V.p, g.vstride, g.S.p, g.ldh, g.ldh, g.N, nr, 1.0, g.act.p, st, g.ctl.p + 5),
-         "Zp");
     ck(launch_gmres_need_true(g.rvec.p, g.act.p, g.it.p, (int)g.outer, nr, g.tol, g.ctl.p, st), "need true");
     if (graph) {
-      capture_if(A.h, st, child, g.ctl.p + 4, 0, [&](cudaStream_t s) { gmres_true_residual(A, g, s); });
+      h2dev_handle_s* h = A.h;
+      cudaStreamCaptureStatus cs;
+      cudaGraph_t bg = nullptr;
+      const cudaGraphNode_t* deps = nullptr;
+      size_t ndeps = 0;
+      ck(cudaStreamGetCaptureInfo(st, &cs, nullptr, &bg, &deps, &ndeps), "capture info");
+      cudaGraphConditionalHandle hc;
+      ck(cudaGraphConditionalHandleCreate(&hc, bg, 0, 0), "conditional handle");
+      ck(launch_graph_condition(hc, g.ctl.p + 4, 0, st), "certify condition");
+      ck(cudaStreamGetCaptureInfo(st, &cs, nullptr, &bg, &deps, &ndeps), "capture info");
+      cudaGraphNodeParams ip = {};
+      ip.type = cudaGraphNodeTypeConditional;
+      ip.conditional.handle = hc;
+      ip.conditional.type = cudaGraphCondTypeIf;
+      ip.conditional.size = 1;
+      cudaGraphNode_t inode;
+      ck(cudaGraphAddNode(&inode, bg, deps, ndeps, &ip), "if node");
+      ck(cudaStreamUpdateCaptureDependencies(st, &inode, 1, cudaStreamSetCaptureDependencies), "capture deps");
+      h->stream = child;
+      ck(cudaStreamBeginCaptureToGraph(child, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                       cudaStreamCaptureModeRelaxed),
+         "certify capture");
+      gmres_true_residual(A, g, child);
+      cudaGraph_t done = nullptr;
+      ck(cudaStreamEndCapture(child, &done), "certify capture end");
+      h->stream = st;
     } else {
       std::vector<int> c5 = g.ctl.download(st);
       if (c5[4]) gmres_true_residual(A, g, st);
@@ -2837,7 +2788,7 @@ static void gmres_graph(SolverBase& A, SolverBase& M, GmresState& g, SolveGraph&
   cudaGraph_t body = wp.conditional.phGraph_out[0];
   h->stream = sb;
   ck(cudaStreamBeginCaptureToGraph(sb, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed), "body capture");
-  gmres_prologue(M, g, sb, 1, ss);
+  gmres_prologue(M, g, sb);
   for (i64 i = 0; i < g.inner; i++) {
     cudaGraphConditionalHandle hi;
     ck(cudaGraphConditionalHandleCreate(&hi, body, 0, 0), "conditional handle");
@@ -2890,12 +2841,10 @@ static void gmres_alloc(GmresState& g, cudaStream_t st) {
   g.resh.alloc((size_t)(outer + 1) * nrhs);
   g.act.alloc(nrhs);
   g.it.alloc(nrhs);
-  g.ctl.alloc(6);
+  g.ctl.alloc(5);
   if (g.rec) {
     g.AV.alloc((size_t)inner * g.vstride);
     g.Rr.alloc(g.vstride);
-    g.Zp.alloc(g.vstride);
-    g.S.alloc(cw * g.ldh * nrhs);
   }
   g.partial.alloc(cw * g.nch * (inner + 1) * nrhs);
   g.y.zero(st);

@@ -132,7 +132,7 @@ __global__ void k_scale_by_norm(const double* __restrict__ w, double* __restrict
   const int c = blockIdx.y;
   const double nv = sqrt(nrm2[c]);
   if (blockIdx.x == 0 && threadIdx.x == 0 && hout) hout[(i64)c * hstride] = nv;
-  const double inv = nv > 0. ? 1. / nv : 0.;
+  const double inv = 1. / nv;
   for (i64 r = (i64)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (i64)gridDim.x * blockDim.x)
     vout[(i64)c * n + r] = w[(i64)c * n + r] * inv;
 }
@@ -423,7 +423,6 @@ __global__ void k_gmres_init(int* __restrict__ act, int* __restrict__ it, double
   if (threadIdx.x == 0) {
     ctl[2] = 0;
     ctl[3] = any ? 1 : 0;
-    ctl[4] = 1;  // the first cycle preconditions B
   }
 }
 
@@ -524,49 +523,6 @@ __global__ void k_gmres_cycle_end(const double* __restrict__ rvec, int* __restri
     const int cy = ++ctl[2];
     ctl[3] = (any && cy < outer) ? 1 : 0;
   }
-}
-
-// Coefficients of the preconditioned residual in the Krylov basis: with
-// M^-1 A V_k = V_{k+1} H_k (left-preconditioned Arnoldi), M^-1 (r - A V_k y)
-// = V_{k+1} (beta e1 - H_k y), so s = beta e1 - H_k y (k = used = ctl[0],
-// k + 1 entries per column at s + c * ld, CPLX: interleaved pairs) and
-// ctl[5] = k + 1.
-template <bool CPLX>
-__global__ void k_gmres_resvec(const double* __restrict__ Hall, int ld, int inner, const double* __restrict__ beta,
-                               const double* __restrict__ yall, const int* __restrict__ act, int nrhs,
-                               double* __restrict__ sall, int* __restrict__ ctl) {
-  const int used = ctl[0];
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nrhs; c += gridDim.x * blockDim.x) {
-    if (!act[c]) continue;
-    const int w = CPLX ? 2 : 1;
-    const double* H = Hall + (i64)c * w * ld * inner;
-    const double* y = yall + (i64)c * w * inner;
-    double* s = sall + (i64)c * w * ld;
-    for (int i = 0; i <= used; i++) {
-      double re = i == 0 ? beta[c] : 0., im = 0.;
-      for (int j = 0; j < used; j++) {
-        if (CPLX) {
-          const double hr = H[2 * (i + j * ld)], hi = H[2 * (i + j * ld) + 1], yr = y[2 * j], yi = y[2 * j + 1];
-          re -= hr * yr - hi * yi;
-          im -= hr * yi + hi * yr;
-        } else {
-          re -= H[i + j * ld] * y[j];
-        }
-      }
-      s[w * i] = re;
-      if (CPLX) s[2 * i + 1] = im;
-    }
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) ctl[5] = used + 1;
-}
-cudaError_t launch_gmres_resvec(const double* H, int ld, int inner, const double* beta, const double* y,
-                                const int* act, int nrhs, double* s, int* ctl, int cplx, cudaStream_t st) {
-  note_launch();
-  if (cplx)
-    k_gmres_resvec<true><<<1, 32, 0, st>>>(H, ld, inner, beta, y, act, nrhs, s, ctl);
-  else
-    k_gmres_resvec<false><<<1, 32, 0, st>>>(H, ld, inner, beta, y, act, nrhs, s, ctl);
-  return cudaGetLastError();
 }
 
 // ctl[4] = 1 when some active column's recurrence residual is below tol or

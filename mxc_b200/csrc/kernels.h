@@ -283,10 +283,6 @@ cudaError_t launch_gmres_estimate(const double* H, int ldh, int inner, int i, co
                                   const int* act, int nrhs, double tol, int* ctl, cudaStream_t st);
 cudaError_t launch_gmres_cycle_end(const double* rvec, int* act, int* it, double* resh, int outer, double tol,
                                    int nrhs, int* ctl, cudaStream_t st);
-// s = beta e1 - H y per column (ld entries, k = ctl[0] + 1 used), ctl[5] = k: the preconditioned
-// residual's coefficients in the Krylov basis.
-cudaError_t launch_gmres_resvec(const double* H, int ld, int inner, const double* beta, const double* y,
-                                const int* act, int nrhs, double* s, int* ctl, int cplx, cudaStream_t st);
 // ctl[4] = some active column needs its true residual (recurrence residual below tol, or last cycle).
 cudaError_t launch_gmres_need_true(const double* rvec, const int* act, const int* it, int outer, int nrhs, double tol,
                                    int* ctl, cudaStream_t st);
