@@ -119,3 +119,74 @@ def test_small_gmres_converges_and_matches_dense():
     assert res[it] < 1e-10 and it <= 5
     r = B - O.dense_matvec(k, b, x)
     assert np.linalg.norm(r) / np.linalg.norm(B) < 1e-10
+
+
+def test_ulv_exact_two_boxes_synthetic_complex():
+    """Complex symmetric version (Helmholtz arithmetic): left transforms by
+    U^H, right ones by conj(U) (h2matrix.cpp:373-396, 532); with the
+    off-diagonal block U0[:, :k] S U1[:, :k]^T in the skeleton spans the ULV is
+    exact."""
+    rng = np.random.default_rng(1)
+    n, k = 20, 6
+
+    def cplx(*shape):
+        return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+
+    U = [np.linalg.qr(cplx(n, n))[0] for _ in range(2)]
+    S12 = cplx(k, k)
+    G1, G2 = cplx(n, n), cplx(n, n)
+    A11 = G1 + G1.T + 8 * np.eye(n)
+    A22 = G2 + G2.T + 8 * np.eye(n)
+    A12 = U[0][:, :k] @ S12 @ U[1][:, :k].T
+    Ad = np.block([[A11, A12], [A12.T, A22]])
+    assert np.allclose(Ad, Ad.T)
+
+    def lvl(l, nodes, ar, ac):
+        return O.Level(l, (1 << l) - 1, nodes, np.array(ar), np.array(ac), np.zeros(nodes + 1, dtype=np.int64),
+                       np.array([], dtype=np.int64))
+
+    s = O.H2MatrixSolver.__new__(O.H2MatrixSolver)
+    s.dt = np.complex128
+    s.levels = 1
+    leaf = lvl(1, 2, [0, 2, 4], [0, 1, 0, 1])
+    root = lvl(0, 1, [0, 1], [0])
+    z = lambda m: np.zeros((m, m), dtype=np.complex128)
+    leaf.Dims = np.array([n, n]); leaf.DimsLr = np.array([k, k])
+    leaf.Q = [U[0].copy(), U[1].copy()]; leaf.R = [z(n), z(n)]
+    leaf.A = [A11.copy(), A12.copy(), A12.T.copy(), A22.copy()]
+    leaf.NA = [(0, 0, 0), (0, 0, k), (0, k, 0), (0, k, k)]
+    root.Dims = np.array([2 * k]); root.DimsLr = np.array([0])
+    root.Q = [np.eye(2 * k, dtype=np.complex128)]; root.R = [z(2 * k)]; root.A = [z(2 * k)]
+    s.A = [root, leaf]
+    s.lenX = 2 * n
+    s.factorize()
+    b = cplx(2 * n)
+    x = s.solve_precondition(b)
+    xe = np.linalg.solve(Ad, b)
+    assert np.linalg.norm(x - xe) / np.linalg.norm(xe) < 1e-12
+
+
+def test_hss_mode_is_exact_inverse_of_its_h2_matrix_complex():
+    """Helmholtz3D(1, 0.1) on the reference's sphere: in HSS mode (theta 0)
+    the complex ULV of the fixed-rank H^2 matrix inverts that matrix, and the
+    operator (ID, eps 1e-10) reproduces the dense complex product."""
+    import math
+
+    N = 1024
+    L = O.levels_for(N, 128)
+    g = math.pi * (3.0 - math.sqrt(5.0))
+    i = np.arange(N)
+    r = math.sqrt(N / (4 * math.pi))
+    y = r - 2.0 * r * (i / (N - 1))
+    ring = np.sqrt(r * r - y * y)
+    b = np.ascontiguousarray(np.stack([ring * np.cos(g * i), y, ring * np.sin(g * i)], 1))
+    cells = O.build_binary_tree(b, L)
+    k = O.Kernel(O.HELMHOLTZ, 0.1, 1.0)
+    x = O.xbody_uniform(N).astype(np.complex128) * (1 + 0.5j)
+    A = O.H2MatrixSolver(k, 1e-10, 50, 0, cells, 1.0, b.copy(), L)
+    assert O.solve_rel_err(A.matvec(x), O.dense_matvec(k, b, x)) < 1e-9
+    M = O.H2MatrixSolver(k, 0.0, 40, 0, cells, 0.0, b.copy(), L)
+    yv = M.matvec(x)
+    M.factorize()
+    z = M.solve_precondition(yv)
+    assert np.linalg.norm(z - x) / np.linalg.norm(x) < 1e-9
