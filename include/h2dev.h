@@ -43,8 +43,9 @@ enum {
  * ld and every vector length count 2 doubles per body.  The solver stores the
  * real symmetric form S = [[Re K, Im K], [Im K, -Re K]] over two real
  * unknowns per body (S conj(x) = K x) and runs every kernel of the real
- * path on it; matvec, precondition, GMRES and the dense matvec conjugate
- * their vectors so that callers see K itself.  rank, leveled_rank and
+ * path on it; matvec, precondition and the dense matvec conjugate their
+ * vectors, and GMRES runs in complex arithmetic (as solver.cpp:144-201), so
+ * that callers see K itself.  rank, leveled_rank and
  * samples are given per body as for the reference (complex degrees of
  * freedom) and doubled for the real form; level dims and ranks report real
  * unknowns.  Bodies' x coordinates are used with bit 0 cleared (a change of
