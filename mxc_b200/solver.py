@@ -252,15 +252,17 @@ def _as_cols(X: np.ndarray, cplx: bool = False):
 
     cplx: complex128 arrays, whose columns the library reads as 2n doubles
     (interleaved real and imaginary parts); ld then counts doubles."""
-    if cplx:
-        assert X.dtype == np.complex128, "a Helmholtz solver takes complex128 vectors"
-    else:
-        assert X.dtype == np.float64, "a real-kernel solver takes float64 vectors"
+    if cplx and X.dtype != np.complex128:
+        raise TypeError("a Helmholtz solver takes complex128 vectors, got %s" % X.dtype)
+    if not cplx and X.dtype != np.float64:
+        raise TypeError("a real-kernel solver takes float64 vectors, got %s" % X.dtype)
     w = 2 if cplx else 1
     if X.ndim == 1:
-        assert X.flags.c_contiguous
+        if not X.flags.c_contiguous:
+            raise ValueError("vectors must be contiguous")
         return X.reshape(-1, 1, order="F"), 1, w * X.shape[0]
-    assert X.flags.f_contiguous, "multi-RHS arrays must be column-major (order='F')"
+    if not X.flags.f_contiguous:
+        raise ValueError("multi-RHS arrays must be column-major (order='F')")
     return X, X.shape[1], w * X.shape[0]
 
 

@@ -4,10 +4,14 @@ TEST INFRASTRUCTURE ONLY.  Nothing in the product (``mxc_b200``) imports this
 module; only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s
 CPU-baseline / reference arm use it, and only as the checker.
 
-Every matrix of the reference is ``std::complex<double>``; for the real
+Every matrix of the reference is ``std::complex<double>``.  For the real
 kernels on this path (Laplace3D, Yukawa3D) every imaginary part stays zero,
 so ``adjoint`` reduces to ``transpose`` and ``conjugate`` to the identity and
-this restatement works in real FP64.
+this restatement works in real FP64.  For Helmholtz3D (kernel.hpp:63-74, the
+reference's default) it works in complex128 with the reference's own
+``adjoint`` / ``transpose`` / ``conjugate`` placements (h2matrix.cpp:266,
+373-396, 532), Eigen's complex Householder rules and GMRES with adjoint inner
+products (solver.cpp:151-197).
 
 Pinning: the point generator, tree, Near/Far lists and kernel values are
 checked bit-for-bit against the reference's own build_tree.cpp /
