@@ -782,8 +782,13 @@ def run_ours(a):
                 "resid": final}
 
     if a.profile_only:
-        r = step(prec, profile=False)
-        print(json.dumps({"profile_only": True, **{k_: v for k_, v in r.items() if k_ != "resid"}}))
+        r = step(prec, profile=True)
+        # the library's per-kernel algorithmic counts of the profiled step
+        # (launches, ms, flops, bytes), to scale an ncu traffic capture by
+        rep = {k_: v for k_, v in h.profile_report().items()}
+        print(json.dumps({"profile_only": True, **{k_: v for k_, v in r.items() if k_ != "resid"},
+                          "kernels": {k_: {"launches": v[0], "ms": round(v[1], 3), "gflop": round(v[2] / 1e9, 3),
+                                           "bytes": v[3]} for k_, v in rep.items()}}))
         return
 
     for _ in range(a.warmup):
