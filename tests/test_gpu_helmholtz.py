@@ -205,3 +205,34 @@ def test_hss_and_leveled_rank_vs_oracle(handle, helm_case, theta_m, lrank):
     assert rel(m.dense_matvec(handle, k, c["b"], X), c["B"]) <= 1e-10
     A.close()
     M.close()
+
+
+@pytest.mark.parametrize("early", [True, False])
+def test_complex_graph_solve_equals_step_by_step(handle, helm_case, early):
+    """Complex GMRES as one captured CUDA graph (WHILE over cycles, IF per
+    Arnoldi step, IF around the certifying true residual) launches the same
+    kernels as the step-by-step path: identical solutions and histories, for
+    several complex right-hand sides at once."""
+    c = helm_case
+    k = m.Helmholtz3D(1.0, 0.1)
+    A = m.H2MatrixSolver(handle, k, c["eps"], c["rank"], 0, c["t"], c["theta"], c["b"])
+    M = m.H2MatrixSolver(handle, k, 0.0, c["rank"], 0, c["t"], c["theta"], c["b"], precision=m.FP32)
+    M.factorizeM()
+    B = np.asfortranarray(np.stack([c["B"], 1j * c["B"], c["B"].conj()], 1))
+    out = []
+    for graph in (False, True):
+        handle.set_option(m._lib.OPT_GRAPH_SOLVE, 1 if graph else 0)
+        try:
+            X = np.zeros_like(B, order="F")
+            rc = A.solveGMRES(c["eps"], M, X, B, 10, 50, early_exit=early)
+            out.append((X, rc, np.array(A.resid, copy=True), np.array(A.iters, copy=True)))
+        finally:
+            handle.set_option(m._lib.OPT_GRAPH_SOLVE, 0)
+    (X1, rc1, r1, i1), (X2, rc2, r2, i2) = out
+    assert rc1 == rc2 == 0
+    assert np.array_equal(i1, i2) and np.array_equal(r1, r2) and np.array_equal(X1, X2)
+    assert rel(X2[:, 0], c["x_true"]) < 1e-8 and rel(X2[:, 1], 1j * c["x_true"]) < 1e-8
+    R = B - m.dense_matvec(handle, k, c["b"], X2)
+    assert max(np.linalg.norm(R[:, j]) / np.linalg.norm(B[:, j]) for j in range(3)) <= 1e-10
+    A.close()
+    M.close()
