@@ -107,9 +107,10 @@ def parse():
     ap.add_argument("--serving-budget-gb", type=float, default=140.0, help="HBM budget of the serving phase")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-only", action="store_true", help="one profiled step, no timing (for ncu)")
-    ap.add_argument("--profile-phase", default="step", choices=["step", "build", "factor", "solve", "operator"],
+    ap.add_argument("--profile-phase", default="step",
+                    choices=["step", "build", "factor", "solve", "operator", "helmholtz"],
                     help="with --profile-only: the part of the step bracketed by cudaProfilerStart/Stop "
-                         "(for ncu --profile-from-start off)")
+                         "(for ncu --profile-from-start off); helmholtz: one mixed step of the Helmholtz sub-run")
     return ap.parse_args()
 
 
@@ -589,7 +590,7 @@ def run_c5(a, h) -> dict:
     return {"unavailable": "no size from %d down to 65536 fits" % a.c5_n, "larger_sizes_tried": tried}
 
 
-def run_helmholtz(a, h) -> dict:
+def run_helmholtz(a, h, profile: bool = False) -> dict:
     """The reference's default run (main.cpp:45-76: Helmholtz3D(1, 0.1) on
     mesh_sphere of radius sqrt(N / 4 pi), theta 1, leaf 256, rank 50, eps
     1e-10) scaled to --helm-n bodies, as a sub-run: complex system solved
@@ -654,6 +655,18 @@ def run_helmholtz(a, h) -> dict:
         return r, X
 
     one(m.FP32, verify=False)
+    if profile:
+        # one mixed step bracketed for ncu, with the library's per-kernel counts
+        torch.cuda.synchronize()
+        h.profile(True)
+        torch.cuda.profiler.start()
+        r, _ = one(m.FP32, verify=False)
+        h.synchronize()
+        torch.cuda.profiler.stop()
+        rep = h.profile_report()
+        h.profile(False)
+        A.close()
+        return {"n": n, **r, "kernels": {k_: {"launches": v[0], "ms": round(v[1], 3)} for k_, v in rep.items()}}
     rm, Xm = one(m.FP32)
     one(m.FP64, verify=False)
     rd, Xd = one(m.FP64)
@@ -687,6 +700,9 @@ def run_ours(a):
     h = m.Handle(local)
     h.set_option(m._lib.OPT_TENSOR_CORES, a.tensor_cores)
     h.set_option(m._lib.OPT_GRAPH_SOLVE, a.graph_solve)
+    if a.profile_only and a.profile_phase == "helmholtz":
+        print(json.dumps({"profile_only": True, "helmholtz": run_helmholtz(a, h, profile=True)}))
+        return
     k = m.Laplace3D(a.singularity)
     L = m.levels_for(a.n, a.leaf)
     b, tree = points_and_tree(a, a.n)
