@@ -190,3 +190,31 @@ def test_hss_mode_is_exact_inverse_of_its_h2_matrix_complex():
     M.factorize()
     z = M.solve_precondition(yv)
     assert np.linalg.norm(z - x) / np.linalg.norm(x) < 1e-9
+
+
+def test_complex_gmres_reaches_dense_solution():
+    """The reference's default run at N = 1024 (Helmholtz3D(1, 0.1) on the
+    sphere, theta 1, rank 50): complex GMRES with the complex ULV
+    preconditioner reaches 1e-10 and the dense solution."""
+    import math
+
+    N = 1024
+    L = O.levels_for(N, 256)
+    g = math.pi * (3.0 - math.sqrt(5.0))
+    i = np.arange(N)
+    r = math.sqrt(N / (4 * math.pi))
+    y = r - 2.0 * r * (i / (N - 1))
+    ring = np.sqrt(r * r - y * y)
+    b = np.ascontiguousarray(np.stack([ring * np.cos(g * i), y, ring * np.sin(g * i)], 1))
+    cells = O.build_binary_tree(b, L)
+    k = O.Kernel(O.HELMHOLTZ, 0.1, 1.0)
+    A = O.H2MatrixSolver(k, 1e-10, 50, 0, cells, 1.0, b.copy(), L)
+    M = O.H2MatrixSolver(k, 0.0, 50, 0, cells, 1.0, b.copy(), L)
+    M.factorize()
+    x = O.xbody_uniform(N).astype(np.complex128)
+    Kd = O.gen_matrix(k, b, b)
+    B = Kd @ x
+    X, res, it = A.solve_gmres(1e-10, M, np.zeros(N, np.complex128), B, 10, 50)
+    assert res[it] < 1e-10 and it <= 5
+    assert np.linalg.norm(Kd @ X - B) / np.linalg.norm(B) < 1e-9
+    assert np.linalg.norm(X - np.linalg.solve(Kd, B)) / np.linalg.norm(x) < 1e-8
