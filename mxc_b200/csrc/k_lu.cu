@@ -272,10 +272,11 @@ __global__ void __launch_bounds__(NP * NP / 64) k_gj_reg(const LuTask<T>* __rest
 
 // LU with partial pivoting of A_rr and the solve A_rr V_r = U_r^T
 // (h2matrix.cpp:377-379: PartialPivLU, then solve).  One CTA per box.
-// Factorization: the unblocked right-looking partial-pivot LU (pivot = first
-// row of largest magnitude in column k among rows k..n-1; the column below
-// the pivot divided by it; rank-1 update of the trailing block), in shared
-// memory when the block fits and otherwise in the task's global scratch.
+// Factorization: the right-looking partial-pivot LU (pivot = first row of
+// largest magnitude in column k among rows k..n-1; the column below the
+// pivot divided by it; rank-1 update of the trailing block), unblocked in
+// shared memory when the block fits, otherwise in the task's global scratch
+// blocked by panels of LU_NB columns (the trailing update as a tiled product).
 // Solve: the row interchanges applied to the right-hand sides, then the
 // unit-lower forward and the upper backward substitution, one warp per 32
 // right-hand-side columns (lane = column), 32 rows at a time in registers,
@@ -284,6 +285,15 @@ __global__ void __launch_bounds__(NP * NP / 64) k_gj_reg(const LuTask<T>* __rest
 // (B[c + r ldb]), as U_r^T and V_r are laid out in the ULV.  info follows
 // Eigen's determinant rule (product of U's diagonal, sign of the
 // permutation, |det| <= DBL_MIN).
+constexpr int LU_NB = 32;  // panel width of the blocked LU in global scratch
+// Byte offset of the trailing-update tiles in the global variant's dynamic
+// shared memory (after the pivot arrays, 16-byte aligned).
+__host__ __device__ constexpr size_t lu_tile_offset(int n) { return ((2 * sizeof(int) * (size_t)n + 15) / 16) * 16; }
+template <typename T>
+constexpr size_t lu_tile_bytes() {
+  return sizeof(T) * (size_t)(64 * (LU_NB + 1) + LU_NB * 65);
+}
+
 template <typename T, bool SMEM>
 __global__ void __launch_bounds__(256, 2) k_lu_solve(const LuSolveTask<T>* __restrict__ tasks) {
   const LuSolveTask<T> t = tasks[blockIdx.x];
@@ -310,7 +320,10 @@ __global__ void __launch_bounds__(256, 2) k_lu_solve(const LuSolveTask<T>* __res
     s_swaps = 0;
   }
   __syncthreads();
-  for (int k = 0; k < n; k++) {
+  // One pivot step of the partial-pivot LU: pivot search in column k among
+  // rows k..n-1, row interchange over all n columns, the column below the
+  // pivot divided by it, and the rank-1 update of columns k+1 .. c_end-1.
+  auto pivot_step = [&](int k, int c_end) {
     double bv = -1.;
     int bi = 0x7fffffff;
     for (int r = k + tid; r < n; r += nt) {
@@ -337,13 +350,82 @@ __global__ void __launch_bounds__(256, 2) k_lu_solve(const LuSolveTask<T>* __res
       for (int r = k + 1 + tid; r < n; r += nt) a[r + (i64)k * ld] = a[r + (i64)k * ld] / p;
     if (!SMEM) __threadfence_block();
     __syncthreads();
-    for (int c = k + 1 + warp; c < n; c += nw) {
+    for (int c = k + 1 + warp; c < c_end; c += nw) {
       T* ac = a + (i64)c * ld;
       const T akc = ac[k];
       for (int r = k + 1 + lane; r < n; r += 32) ac[r] -= a[r + (i64)k * ld] * akc;
     }
     if (!SMEM) __threadfence_block();
     __syncthreads();
+  };
+  if constexpr (SMEM) {
+    for (int k = 0; k < n; k++) pivot_step(k, n);
+  } else {
+    // In global scratch: blocked right-looking LU (panels of LU_NB columns,
+    // the same pivots as the unblocked form up to rounding), so the trailing
+    // matrix is read and written once per panel instead of once per pivot.
+    // The trailing update runs in 64 x 64 tiles with the panel's L rows and
+    // U columns staged in shared memory after the pivot arrays.
+    T* Ls = reinterpret_cast<T*>(smem_raw + lu_tile_offset(n));  // [64][LU_NB + 1]
+    T* Us = Ls + 64 * (LU_NB + 1);                               // [LU_NB][65]
+    const int tx = tid & 15, ty = tid >> 4;                      // 4 x 4 outputs per thread
+    for (int k0 = 0; k0 < n; k0 += LU_NB) {
+      const int kb = min(LU_NB, n - k0), j0 = k0 + kb;
+      for (int k = k0; k < j0; k++) pivot_step(k, j0);
+      if (j0 >= n) break;
+      // U12 = L11^-1 A12 (L11 unit lower), one column per thread
+      for (int c = j0 + tid; c < n; c += nt) {
+        T* ac = a + (i64)c * ld;
+        for (int i = 0; i < kb; i++) {
+          const T x = ac[k0 + i];
+          for (int r = i + 1; r < kb; r++) ac[k0 + r] -= a[(k0 + r) + (i64)(k0 + i) * ld] * x;
+        }
+      }
+      __threadfence_block();
+      __syncthreads();
+      // A22 -= L21 U12
+      for (int tr = j0; tr < n; tr += 64)
+        for (int tc = j0; tc < n; tc += 64) {
+          for (int e = tid; e < 64 * LU_NB; e += nt) {
+            const int rr = e % 64, i = e / 64;
+            Ls[rr * (LU_NB + 1) + i] = (tr + rr < n && i < kb) ? a[(tr + rr) + (i64)(k0 + i) * ld] : T(0);
+          }
+          for (int e = tid; e < 64 * LU_NB; e += nt) {
+            const int i = e % LU_NB, cc = e / LU_NB;
+            Us[i * 65 + cc] = (tc + cc < n && i < kb) ? a[(k0 + i) + (i64)(tc + cc) * ld] : T(0);
+          }
+          __syncthreads();
+          T acc[4][4];
+#pragma unroll
+          for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int v = 0; v < 4; v++) acc[u][v] = T(0);
+          for (int i = 0; i < kb; i++) {
+            T lv[4], uv[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) lv[u] = Ls[(ty * 4 + u) * (LU_NB + 1) + i];
+#pragma unroll
+            for (int v = 0; v < 4; v++) uv[v] = Us[i * 65 + tx * 4 + v];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+              for (int v = 0; v < 4; v++) acc[u][v] += lv[u] * uv[v];
+          }
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            const int r = tr + ty * 4 + u;
+            if (r >= n) continue;
+#pragma unroll
+            for (int v = 0; v < 4; v++) {
+              const int c = tc + tx * 4 + v;
+              if (c < n) a[r + (i64)c * ld] -= acc[u][v];
+            }
+          }
+          __syncthreads();  // the tiles are restaged by the next (tr, tc)
+        }
+      __threadfence_block();
+      __syncthreads();
+    }
   }
   if (tid == 0) {
     for (int i = 0; i < n; i++) prow[i] = i;
@@ -426,7 +508,7 @@ cudaError_t launch_lu_solve(const LuSolveTask<T>* d_tasks, int ntasks, int maxn,
     k_lu_solve<T, true><<<ntasks, 256, smem, st>>>(d_tasks);
     return cudaGetLastError();
   }
-  const size_t smem = 2 * sizeof(int) * (size_t)maxn + 16;
+  const size_t smem = lu_tile_offset(maxn) + lu_tile_bytes<T>() + 16;
   cudaError_t e = cudaFuncSetAttribute(k_lu_solve<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   note_launch();
