@@ -276,7 +276,8 @@ __global__ void __launch_bounds__(NP * NP / 64) k_gj_reg(const LuTask<T>* __rest
 // largest magnitude in column k among rows k..n-1; the column below the
 // pivot divided by it; rank-1 update of the trailing block), unblocked in
 // shared memory when the block fits, otherwise in the task's global scratch
-// blocked by panels of LU_NB columns (the trailing update as a tiled product).
+// (FP32: blocked by panels of LU_NB columns, the trailing update as a tiled
+// product).
 // Solve: the row interchanges applied to the right-hand sides, then the
 // unit-lower forward and the upper backward substitution, one warp per 32
 // right-hand-side columns (lane = column), 32 rows at a time in registers,
@@ -358,12 +359,16 @@ __global__ void __launch_bounds__(256, 2) k_lu_solve(const LuSolveTask<T>* __res
     if (!SMEM) __threadfence_block();
     __syncthreads();
   };
-  if constexpr (SMEM) {
+  if constexpr (SMEM || sizeof(T) == 8) {
+    // FP64 keeps the unblocked order in global scratch too: it is the path
+    // held to the oracle on the ill-conditioned reference configuration,
+    // whose substitution moves by tens of percent with the rounding order.
     for (int k = 0; k < n; k++) pivot_step(k, n);
   } else {
-    // In global scratch: blocked right-looking LU (panels of LU_NB columns,
-    // the same pivots as the unblocked form up to rounding), so the trailing
-    // matrix is read and written once per panel instead of once per pivot.
+    // FP32 (the mixed preconditioner) in global scratch: blocked
+    // right-looking LU (panels of LU_NB columns, the same pivots as the
+    // unblocked form up to rounding), so the trailing matrix is read and
+    // written once per panel instead of once per pivot.
     // The trailing update runs in 64 x 64 tiles with the panel's L rows and
     // U columns staged in shared memory after the pivot arrays.
     T* Ls = reinterpret_cast<T*>(smem_raw + lu_tile_offset(n));  // [64][LU_NB + 1]
