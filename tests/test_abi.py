@@ -39,3 +39,24 @@ def test_host_entry_points_validate_arguments():
         m.build_tree(b, 5)  # more leaves than bodies
     assert m.levels_for(20000, 256) == 6
     assert m.levels_for(100, 256) == 0
+
+
+def test_vector_argument_validation():
+    """The Python mirror rejects vectors of the wrong element type or layout
+    before any device call: complex128 for a Helmholtz solver, float64 for
+    the real kernels, column-major multi-RHS arrays."""
+    import numpy as np
+    import pytest
+    from mxc_b200 import solver as S
+
+    x = np.zeros(8)
+    Xf = np.zeros((8, 3), order="F")
+    assert S._as_cols(x)[1:] == (1, 8)
+    assert S._as_cols(Xf)[1:] == (3, 8)
+    assert S._as_cols(np.zeros((8, 3), dtype=np.complex128, order="F"), True)[1:] == (3, 16)
+    with pytest.raises(TypeError):
+        S._as_cols(np.zeros(8, dtype=np.complex128))
+    with pytest.raises(TypeError):
+        S._as_cols(x, True)
+    with pytest.raises(ValueError):
+        S._as_cols(np.zeros((8, 3)))  # row-major
